@@ -1,0 +1,424 @@
+"""Benchmark: BEM solves/s (dense Burton-Miller TBEM: assembly + GMRES) on B200.
+
+Workload (default): rigid sphere, icosphere level 5 (N = 20480 flat triangles, constant panels
+collocated at centroids), k = 10, incident plane wave exp(i k z), beta = i/k. One step = one
+solve: re-assembly of the dense system on the device, the incident right-hand side, and GMRES.
+
+  * `value`  -- the mixed-precision solver (complex128 matrix + complex64 copy written by one
+                assembly epilogue; FP32 inner GMRES(50) to 1e-5 inside FP64 refinement to 1e-8),
+                inputs resident in HBM, device time by CUDA events on the operator's stream.
+                Its relative error against the plain FP64 solution is measured and reported.
+  * `plain_fp64` -- the same solve with complex128 only and FP64 GMRES(50) to 1e-8.
+  * `e2e`    -- the mixed solve through the C ABI with host buffers: mesh upload, assembly,
+                host RHS, solve with host b / x (all copies inside the timed region).
+  * `cpu_baseline` / `--impl reference` -- the CPU restatement of the reference path (oracle),
+                timed on a bounded sample (assembly rows + a CPU matvec) and scaled to one solve.
+
+With torchrun (N > 1 ranks) every rank solves its own copy of the workload (replicas: the path
+has no exchange step); value = all ranks' solves / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import ctypes as ct
+import io
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RADIUS = 1.0
+LEVEL = 5
+K = 10.0
+RESTART = 50
+TOL = 1e-8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--level", type=int, default=LEVEL)
+    ap.add_argument("--k", type=float, default=K)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 timing")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing (only used when launched by torchrun)
+# ---------------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in csv.reader(io.StringIO(out)):
+            if len(row) < 9:
+                continue
+            try:
+                sm.append(float(row[1]))
+                smax.append(float(row[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, row[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline (oracle restatement of the reference CPU path), bounded sample
+# ---------------------------------------------------------------------------------------------
+def cpu_baseline(level: int, k: float, fp64_matvecs: int, budget_s: float = 12.0):
+    from oracle import oracle as O
+
+    O.build()
+    nodes, tris = O.icosphere(RADIUS, level)
+    n = tris.shape[0]
+    ph = O.physics_for_k(k)
+    beta = O.bm_beta(ph)
+    # assembly: time a block of rows, grow it until ~budget/2 seconds
+    rows, t_rows = 8, 0.0
+    while True:
+        r0 = min(n // 3, n - rows)
+        t0 = time.perf_counter()
+        O.assemble(nodes, tris, ph, beta, rows=(r0, r0 + rows))
+        t_rows = time.perf_counter() - t0
+        if t_rows > budget_s / 4 or rows >= n:
+            break
+        rows = min(n, rows * 4)
+    t_asm = t_rows * n / rows
+    # dense complex128 matvec on a sample matrix, scaled by bytes (16 n^2)
+    ns = 4096
+    rng = np.random.default_rng(0x5EED)
+    A = (rng.standard_normal((ns, ns)) + 1j * rng.standard_normal((ns, ns))).astype(np.complex128)
+    x = rng.standard_normal(ns) + 0j
+    O.matvec(A, x)
+    reps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s / 4:
+        O.matvec(A, x)
+        reps += 1
+    t_mv_s = (time.perf_counter() - t0) / reps
+    t_mv = t_mv_s * (n / ns) ** 2
+    t_solve = t_asm + fp64_matvecs * t_mv
+    return {
+        "value": 1.0 / t_solve, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+        "sample": (f"oracle (C++ restatement, OpenMP {os.cpu_count()} threads): assembly of {rows} of {n} rows "
+                   f"({t_rows:.2f} s, scaled x{n / rows:.0f}) + complex128 matvec at n={ns} "
+                   f"({t_mv_s * 1e3:.1f} ms, scaled by bytes to n={n}) x {fp64_matvecs} matvecs of the FP64 GMRES"),
+        "assembly_s": t_asm, "matvec_s": t_mv,
+    }
+
+
+def reference_arm(a, dist: Dist):
+    """--impl reference: the CPU restatement of the reference path on this host, bounded samples."""
+    if dist.rank != 0:
+        return
+    res = []
+    for _ in range(a.warmup + a.steps):
+        res.append(cpu_baseline(a.level, a.k, fp64_matvecs=40, budget_s=8.0))
+    timed = res[a.warmup:]
+    v = float(np.mean([r["value"] for r in timed]))
+    line = {
+        "impl": "reference", "metric": "BEM solves/s (dense Burton-Miller TBEM assembly + GMRES)",
+        "value": v, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128", "data": "synthetic (icosphere geometry, analytic plane wave)",
+        "config": {"workload": f"rigid sphere icosphere L{a.level} (N={20 * 4 ** a.level}), k={a.k}, "
+                               f"Burton-Miller beta=i/k, GMRES({RESTART}) rtol {TOL}"},
+        "cpu_baseline": {k: timed[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the Rust reference cannot be built here (no rustc/cargo); this arm times its C++ "
+                "restatement (oracle/) and assumes 40 FP64 matvecs per solve",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------------
+def main():
+    a = parse()
+    dist = Dist()
+    if a.impl == "reference":
+        reference_arm(a, dist)
+        dist.close()
+        return
+    import sonium_b200 as sb
+    from sonium_b200 import _lib as L
+
+    from sonium_b200 import build as sb_build
+
+    sb_build.build()
+    lib = L.load()
+    dev = dist.local
+    n_dev = sb.device_count()
+    assert n_dev > dev, "no CUDA device for this rank"
+
+    nodes, tris = sb.icosphere(RADIUS, a.level)
+    n = tris.shape[0]
+    ph = sb.PhysicsParams.for_wavenumber(a.k)
+    beta = ph.burton_miller_beta()
+    mesh = sb.Mesh(nodes, tris, device=dev)
+    op = sb.build_tbem_system_with_beta(mesh, ph, beta, sb.SB_PRECISION_FP64_FP32)
+    dirs = np.array([[0.0, 0.0, 1.0]])
+    # device-resident b and x (caller-owned device memory, as the *_device entry points take)
+    rt = _cudart()
+    b_d = _dev_alloc(rt, 16 * n)
+    x_d = _dev_alloc(rt, 16 * n)
+    phys = ph._struct()
+    bta = L.SbComplex(beta.real, beta.imag)
+    ir = L.SbIrConfig(20, TOL, RESTART, 20, 1e-5)
+    gc = L.SbGmresConfig(100, RESTART, TOL, 1)
+    st = L.SbGmresStats()
+
+    def step_mixed():
+        L.check(lib.sb_assemble_into(op.handle, ct.byref(phys), bta))
+        L.check(lib.sb_rhs_plane_wave_device(op.handle, dirs.ctypes.data, None, 1, b_d))
+        L.check(lib.sb_gmres_mixed_device(op.handle, b_d, x_d, 0, ct.byref(ir), ct.byref(st)))
+        return st
+
+    def step_plain(op64):
+        L.check(lib.sb_assemble_into(op64.handle, ct.byref(phys), bta))
+        L.check(lib.sb_rhs_plane_wave_device(op64.handle, dirs.ctypes.data, None, 1, b_d))
+        L.check(lib.sb_gmres_device(op64.handle, b_d, x_d, 0, ct.byref(gc), 0, ct.byref(st)))
+        return st
+
+    ev0, ev1 = ct.c_void_p(), ct.c_void_p()
+    L.check(lib.sb_event_create(ct.byref(ev0)))
+    L.check(lib.sb_event_create(ct.byref(ev1)))
+
+    def timed(fn, handle, steps):
+        dist.barrier()
+        rt.cudaDeviceSynchronize()
+        L.check(lib.sb_event_record(ev0, handle))
+        stats = [fn() for _ in range(steps)]
+        L.check(lib.sb_event_record(ev1, handle))
+        ms = ct.c_float()
+        L.check(lib.sb_event_elapsed_ms(ev0, ev1, ct.byref(ms)))
+        rt.cudaDeviceSynchronize()
+        dist.barrier()
+        return dist.max(ms.value / 1e3), stats
+
+    # ---- mixed (headline) ----
+    for _ in range(a.warmup):
+        step_mixed()
+    clocks = Clocks(dev)
+    prof = L.SbProfile()
+    L.check(lib.sb_profile_read(ct.byref(prof), 1))
+    L.check(lib.sb_profile_enable(1))
+    clocks.start()
+    t_mixed, _ = timed(step_mixed, op.handle, a.steps)
+    clk = clocks.stop()
+    L.check(lib.sb_profile_enable(0))
+    L.check(lib.sb_profile_read(ct.byref(prof), 1))
+    mixed_stats = L.SbGmresStats.from_buffer_copy(st)
+    x_mixed = _to_host(rt, x_d, n)
+
+    # ---- plain FP64 ----
+    plain = None
+    x_plain = None
+    plain_stats = None
+    op64 = sb.build_tbem_system_with_beta(mesh, ph, beta, sb.SB_PRECISION_FP64)
+    step_plain(op64)
+    plain_stats = L.SbGmresStats.from_buffer_copy(st)
+    x_plain = _to_host(rt, x_d, n)
+    if not a.no_plain:
+        for _ in range(max(1, a.warmup - 1)):
+            step_plain(op64)
+        t_plain, _ = timed(lambda: step_plain(op64), op64.handle, a.steps)
+        plain = dist.world * a.steps / t_plain
+    op64.close()
+    err_vs_fp64 = float(np.linalg.norm(x_mixed - x_plain) / np.linalg.norm(x_plain))
+
+    # ---- e2e through the C ABI with host buffers ----
+    e2e = None
+    if not a.no_e2e:
+        op.close()
+        mesh.close()
+        ts = []
+        for i in range(1 + a.steps):
+            rt.cudaDeviceSynchronize()
+            dist.barrier()
+            t0 = time.perf_counter()
+            m2 = sb.Mesh(nodes, tris, device=dev)
+            o2 = sb.build_tbem_system_with_beta(m2, ph, beta, sb.SB_PRECISION_FP64_FP32)
+            bh = sb.rhs_plane_wave(m2, ph, beta, dirs)[:, 0]
+            s2 = sb.gmres_mixed(o2, bh, sb.IrConfig(20, TOL, RESTART, 20, 1e-5))
+            o2.close()
+            m2.close()
+            rt.cudaDeviceSynchronize()
+            dt = time.perf_counter() - t0
+            dist.barrier()
+            if i > 0:
+                ts.append(dist.max(dt))
+        h2d = nodes.nbytes + tris.nbytes + 16 * n + 24  # nodes, tris, b, direction
+        d2h = 16 * n + 16 * n                           # RHS and solution
+        e2e = {"value": dist.world * len(ts) / sum(ts), "unit": "solves/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    # ---- roofline of the dominant kernel ----
+    pk, pk_kind = peaks()
+    names = L.PROF_NAMES
+    ms = {names[i]: prof.ms[i] for i in range(L.SB_PROF_KINDS)}
+    launches = {names[i]: prof.launches[i] for i in range(L.SB_PROF_KINDS)}
+    total_ms = sum(ms.values())
+    # HBM-bound matvecs: complex64 (8 N^2 bytes) and complex128 (16 N^2 bytes) per launch
+    bytes_mv = {"gemv32": 8.0 * n * n, "gemv64": 16.0 * n * n}
+    hbm_kind = max(("gemv32", "gemv64"), key=lambda kk: ms[kk])
+    avg = ms[hbm_kind] / max(launches[hbm_kind], 1) / 1e3
+    achieved = bytes_mv[hbm_kind] / avg / 1e9
+    roof = {"kernel": "k_gemv_n_c64 (complex64 matvec, FP32 vectors)" if hbm_kind == "gemv32"
+            else "k_gemv_n_c128 (complex128 matvec)",
+            "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_kind,
+            "bytes_per_launch": bytes_mv[hbm_kind], "avg_launch_ms": avg * 1e3}
+    # assembly: evaluations per second (13-point far leaves) and FP64 rate at 90 flop / evaluation
+    evals = 13.0 * n * (n - 1)
+    far_avg = ms["far"] / max(launches["far"], 1) / 1e3
+    assembly = {"far_kernel_ms": far_avg * 1e3, "evals_per_s": evals / far_avg,
+                "fp64_tflops_nominal90": 90 * evals / far_avg / 1e12,
+                "share_of_step": (ms["far"] + ms["near"] + ms["self"]) / max(total_ms, 1e-9)}
+
+    cpu = None
+    if not a.no_cpu and dist.rank == 0:
+        cpu = cpu_baseline(a.level, a.k, int(plain_stats.matvecs))
+    value = dist.world * a.steps / t_mixed
+    line = {
+        "metric": "BEM solves/s at <=1e-5 rel err vs FP64 (mixed-precision solve, dense Burton-Miller TBEM)",
+        "value": value, "unit": "solves/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * t_mixed / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128+c64",
+        "data": "synthetic (icosphere geometry, analytic incident plane wave)",
+        "config": {"workload": f"rigid sphere icosphere L{a.level} (N={n}), k={a.k}, beta=i/k, plane wave +z; "
+                               f"assembly + GMRES({RESTART}) FP32-inner / FP64-refined to rtol {TOL}",
+                   "N": n, "l2": "inputs larger than L2 (matrix %.1f GB)" % (24 * n * n / 1e9),
+                   "parallelism": f"replicas x{dist.world}"},
+        "error_vs_fp64": err_vs_fp64,
+        "plain_fp64": {"value": plain, "unit": "solves/s",
+                       "iterations": int(plain_stats.iterations), "matvecs": int(plain_stats.matvecs)},
+        "mixed": {"iterations": int(mixed_stats.iterations), "matvecs": int(mixed_stats.matvecs),
+                  "matvecs_fp32": int(mixed_stats.matvecs_fp32), "refinements": int(mixed_stats.refinements),
+                  "residual": mixed_stats.residual},
+        "roofline": roof,
+        "assembly": assembly,
+        "kernel_ms_per_step": {kk: v / a.steps for kk, v in ms.items() if v > 0},
+        "gpu_launches": int(prof.kernels),
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": None if cpu is None else {kk: cpu[kk] for kk in ("value", "unit", "cores", "kind", "sample")},
+    }
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    rt.cudaFree(b_d)
+    rt.cudaFree(x_d)
+    dist.close()
+
+
+def _cudart():
+    for name in ("libcudart.so.12", "libcudart.so", "/usr/local/cuda/lib64/libcudart.so.12"):
+        try:
+            rt = ct.CDLL(name)
+            break
+        except OSError:
+            continue
+    else:
+        raise RuntimeError("libcudart not found")
+    rt.cudaMalloc.argtypes = [ct.POINTER(ct.c_void_p), ct.c_size_t]
+    rt.cudaFree.argtypes = [ct.c_void_p]
+    rt.cudaMemcpy.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_int]
+    return rt
+
+
+def _dev_alloc(rt, nbytes):
+    p = ct.c_void_p()
+    if rt.cudaMalloc(ct.byref(p), nbytes) != 0:
+        raise RuntimeError("cudaMalloc failed")
+    return p
+
+
+def _to_host(rt, p, n):
+    out = np.zeros(n, np.complex128)
+    rt.cudaDeviceSynchronize()
+    if rt.cudaMemcpy(out.ctypes.data, p, 16 * n, 2) != 0:
+        raise RuntimeError("cudaMemcpy failed")
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,278 @@
+/*
+ * sonium-b200 C ABI: dense constant-panel Burton-Miller TBEM on one NVIDIA B200 (sm_100a).
+ *
+ * The entry points below are what the reference's Rust side would bind over FFI to replace
+ * its dense collocation path: the assembly entry points of crates/sonium-bem/src/core/
+ * assembly/tbem.rs, the incident-field right-hand side of crates/sonium-bem/src/core/
+ * incident.rs, the LinearOperator / Preconditioner surface of crates/sonium-solvers/crates/
+ * sonium-solvers-core/src/traits.rs and the restarted GMRES of crates/sonium-solvers/crates/
+ * sonium-solvers-iterative/src/gmres.rs. Citations are relative to the sonium workspace root.
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, POD structs. Complex numbers are interleaved
+ *    (re, im) doubles (sb_complex) or floats (sb_complex32), layout-compatible with
+ *    num_complex::Complex64 / Complex32.
+ *  - Matrices are row-major (row = source/collocation DOF, column = field DOF), as
+ *    DenseMatrix<Complex64> in tbem.rs:135.
+ *  - Constant panels: element e owns DOF e (the dof_addresses = [e] numbering that
+ *    generate_icosphere_mesh produces, generators.rs:700-712).
+ *  - Every function returns an int status (SB_OK = 0). On failure sb_last_error() returns a
+ *    message. Errors are never silently replaced by a CPU computation: there is no CPU
+ *    fallback in this library, and a missing or unusable GPU is SB_ERR_CUDA.
+ *  - Host pointers are caller-owned and only read/written during the call. Handles are
+ *    thread-safe per handle, not across handles that share a mesh.
+ */
+#ifndef SONIUM_B200_H
+#define SONIUM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SB_API __attribute__((visibility("default")))
+#else
+#define SB_API
+#endif
+
+/* ---- status codes: CudaTbemAssemblyError (tbem.rs:3693-3718) + MissingSourceDof (:108-129) ---- */
+#define SB_OK 0
+#define SB_ERR_INVALID_ARGUMENT 1   /* InvalidInput { reason } */
+#define SB_ERR_UNSUPPORTED_ELEMENT 2 /* UnsupportedElement (degenerate Tri3) */
+#define SB_ERR_OUT_OF_MEMORY 3
+#define SB_ERR_CUDA 4               /* Backend(..): launch / runtime failure, no device */
+#define SB_ERR_DEVICE_CHECK 5       /* a kernel reported a bounded failure in its status word */
+#define SB_ERR_INJECTED 6           /* host-side fault injection (sb_inject_failure) */
+#define SB_ERR_NOT_FINITE 7         /* non-finite input or output (try_apply contract) */
+
+/* ---- basic types ---- */
+typedef struct sb_complex {
+    double re, im;
+} sb_complex;
+
+typedef struct sb_complex32 {
+    float re, im;
+} sb_complex32;
+
+/* PhysicsParams (crates/sonium-bem/src/core/types.rs:34-53). */
+typedef struct sb_physics {
+    double frequency, speed_of_sound, density, wave_number, omega, wave_length;
+    double harmonic_factor, pressure_factor, tau;
+} sb_physics;
+
+/* Message of the last failure on this thread (empty when none). Returns the message length. */
+SB_API int sb_last_error(char* buf, size_t len);
+SB_API int sb_version(int* major, int* minor, int* patch);
+/* Number of visible CUDA devices (0 when none); never falls back. */
+SB_API int sb_device_count(int* count);
+
+/* PhysicsParams::new / try_new (types.rs:120-160,165-190): k = 2 pi f / c, harmonic factor +1
+ * (conventions.rs:308-313), pressure_factor = rho * omega, tau = +1 exterior / -1 interior. */
+SB_API int sb_physics_new(double frequency, double speed_of_sound, double density,
+                          int is_internal, sb_physics* out);
+/* PhysicsParams::validate (types.rs:238-300). */
+SB_API int sb_physics_validate(const sb_physics* p);
+/* burton_miller_beta_scaled (types.rs:314-320, 418): i * harmonic_factor * scale / k for
+ * exterior problems, 0 for interior ones. */
+SB_API int sb_burton_miller_beta(const sb_physics* p, double scale, sb_complex* beta);
+
+/* ---- mesh ---- */
+/* generate_icosphere_mesh (crates/sonium-bem/src/core/mesh/generators.rs:309-397) on the host,
+ * vertices scaled per axis by scale[3] (NULL = sphere) after the radius. */
+SB_API int sb_icosphere_counts(int level, int64_t* n_nodes, int64_t* n_tris);
+SB_API int sb_icosphere(double radius, int level, const double* scale, double* nodes,
+                        uint32_t* tris);
+
+typedef struct sb_mesh sb_mesh;
+
+typedef struct sb_mesh_info {
+    int64_t n_nodes, n_elements, n_near_pairs;
+    int32_t device;
+    int32_t reserved;
+} sb_mesh_info;
+
+/* Upload a Tri3 constant-panel mesh to `device` (validate_cuda_tbem_inputs, tbem.rs:4659-4798:
+ * finite coordinates, in-range connectivity, non-degenerate triangles) and precompute the
+ * element geometry (compute_element_geometry, generators.rs:771-830), the far-field quadrature
+ * points and the near-pair list. The default boundary condition is rigid (velocity 0). */
+SB_API int sb_mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris,
+                          int64_t n_tris, int device, sb_mesh** out);
+SB_API int sb_mesh_destroy(sb_mesh* mesh);
+SB_API int sb_mesh_info_get(const sb_mesh* mesh, sb_mesh_info* info);
+/* Element centroid (collocation point), unit normal and area, each n_elements long. */
+SB_API int sb_mesh_element_geometry(const sb_mesh* mesh, double* centers, double* normals,
+                                    double* areas);
+
+/* Boundary conditions per element (BoundaryCondition, types.rs:582-640; get_bc_type_and_value,
+ * crates/sonium-bem/src/core/assembly/common.rs:283-293): kind 0 = velocity (Neumann),
+ * 1 = pressure (Dirichlet); value = the element's averaged prescribed value; has_admittance /
+ * admittance = VelocityWithAdmittance. Any pointer may be NULL (0 / none). */
+#define SB_BC_VELOCITY 0
+#define SB_BC_PRESSURE 1
+SB_API int sb_mesh_set_bc(sb_mesh* mesh, const int32_t* kind, const sb_complex* value,
+                          const uint8_t* has_admittance, const sb_complex* admittance);
+
+/* ---- assembly ---- */
+#define SB_PRECISION_FP64 0      /* complex128 matrix only */
+#define SB_PRECISION_FP64_FP32 1 /* complex128 matrix plus a complex64 copy from one epilogue */
+
+typedef struct sb_operator sb_operator;
+
+typedef struct sb_operator_info {
+    int64_t n;
+    int32_t precision;
+    int32_t device;
+    double assembly_ms;          /* device time of the last assembly */
+    uint64_t bytes_fp64, bytes_fp32;
+} sb_operator_info;
+
+/* build_tbem_system_with_beta (tbem.rs:1196-1203 -> build_tbem_system_with_beta_parallel
+ * :1284-1466): dense Burton-Miller collocation matrix (G, H, H^T, E channels; adaptive
+ * regular quadrature regular.rs:124-321 with generate_subelements singular.rs:1372-1540;
+ * self term singular.rs:297-614) plus the boundary-condition RHS, resident on the device. */
+SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta,
+                       int precision, sb_operator** out);
+/* Re-assemble an existing operator for a new frequency / beta in place
+ * (CudaTbemAssemblyWorkspace::assemble, tbem.rs:4230-4389). */
+SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_complex beta);
+SB_API int sb_operator_destroy(sb_operator* op);
+SB_API int sb_operator_info_get(const sb_operator* op, sb_operator_info* info);
+/* TbemSystem { matrix, rhs } (tbem.rs:134-150) copied to host; either pointer may be NULL. */
+SB_API int sb_operator_copy_to_host(const sb_operator* op, sb_complex* matrix, sb_complex* rhs);
+SB_API int sb_operator_copy_rows_to_host(const sb_operator* op, int64_t row0, int64_t row1,
+                                         sb_complex* rows);
+SB_API int sb_operator_copy_to_host_c64(const sb_operator* op, sb_complex32* matrix);
+
+/* LinearOperator<Complex64> (traits.rs:2949-3120) over DenseMatrixOperator
+ * (crates/sonium-bem/src/core/bem_solver.rs:6548-6590): apply_into (y = A x),
+ * apply_transpose_into (y = A^T x), Hermitian (y = A^H x) and apply_block (Y = A X, X/Y row-major
+ * n x r). Host buffers; non-finite input or output returns SB_ERR_NOT_FINITE (try_apply). */
+#define SB_OP_N 0
+#define SB_OP_T 1
+#define SB_OP_C 2
+SB_API int sb_operator_apply(const sb_operator* op, int trans, const sb_complex* x,
+                             sb_complex* y);
+SB_API int sb_operator_apply_block(const sb_operator* op, const sb_complex* X, sb_complex* Y,
+                                   int64_t r);
+/* Same on device pointers (n complex128 each), on the operator's stream, synchronised. */
+SB_API int sb_operator_apply_device(const sb_operator* op, int trans, const sb_complex* x_dev,
+                                    sb_complex* y_dev);
+
+/* Preconditioner<Complex64>::apply_into (traits.rs:3645-3720): identity or Jacobi (A_ii^-1). */
+#define SB_PRECOND_IDENTITY 0
+#define SB_PRECOND_JACOBI 1
+SB_API int sb_preconditioner_apply(const sb_operator* op, int precond, const sb_complex* x,
+                                   sb_complex* y);
+
+/* IncidentField::compute_rhs_with_beta for plane waves (incident.rs:216-245,315-331,807-833):
+ * rhs[i*r+q] = -(gamma p_inc + beta tau dp_inc/dn) at the element centroids, for r directions
+ * dirs[q] (unit vectors) with amplitudes amps[q] (NULL = 1). */
+SB_API int sb_rhs_plane_wave(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta,
+                             const double* dirs, const sb_complex* amps, int64_t r,
+                             sb_complex* rhs);
+
+/* ---- GMRES ---- */
+/* GmresConfig (gmres.rs:26-47): max_iterations counts restart cycles, restart is the Krylov
+ * dimension, tolerance is relative to ||b||. */
+typedef struct sb_gmres_config {
+    int64_t max_iterations;
+    int64_t restart;
+    double tolerance;
+    int64_t convergence_check_interval;
+} sb_gmres_config;
+
+/* GmresSolution (gmres.rs:93-118). status: SB_SOLVER_* below. */
+#define SB_SOLVER_CONVERGED 0
+#define SB_SOLVER_MAX_ITERATIONS 1
+#define SB_SOLVER_BREAKDOWN 2
+#define SB_SOLVER_NUMERICAL_ERROR 3
+typedef struct sb_gmres_stats {
+    int64_t iterations;         /* Krylov steps (outer + inner for the mixed solver) */
+    int64_t restarts;
+    int64_t matvecs;            /* all operator applications incl. residual checks */
+    int64_t matvecs_fp32;       /* of which on the complex64 copy (mixed solver) */
+    int64_t refinements;        /* FP64 refinement steps (mixed solver) */
+    double residual;            /* ||b - A x|| / ||b|| with the complex128 operator */
+    double estimated_residual;
+    double backward_error;
+    double device_ms;           /* device time of the solve */
+    int32_t converged;
+    int32_t status;
+} sb_gmres_stats;
+
+/* gmres / gmres_preconditioned (gmres.rs:286-305, 631-1047, finalize 159-247) with CGS + one
+ * DGKS pass (0.707), Givens on the host in FP64. b, x0 (NULL = 0) and x are host buffers. */
+SB_API int sb_gmres(const sb_operator* op, const sb_complex* b, const sb_complex* x0,
+                    const sb_gmres_config* cfg, int precond, sb_complex* x, sb_gmres_stats* stats);
+/* Same with device-resident b / x (x holds x0 on entry when x0_given != 0). */
+SB_API int sb_gmres_device(const sb_operator* op, const sb_complex* b_dev, sb_complex* x_dev,
+                           int x0_given, const sb_gmres_config* cfg, int precond,
+                           sb_gmres_stats* stats);
+
+/* Mixed-precision iterative refinement (the FGMRES-IR precedent of crates/sonium-compute/src/
+ * gmres_ir.rs:1-80, 665): an FP64 outer loop r = b - A x on the complex128 matrix, an inner
+ * GMRES on the complex64 copy with FP32 vectors and FP32-accumulated products (Hessenberg /
+ * Givens in FP64), x += d in FP64. Needs an SB_PRECISION_FP64_FP32 operator. */
+typedef struct sb_ir_config {
+    int64_t max_refinements;
+    double tolerance;            /* outer relative residual target */
+    int64_t inner_restart;
+    int64_t inner_max_iterations;
+    double inner_tolerance;
+} sb_ir_config;
+SB_API int sb_gmres_mixed(const sb_operator* op, const sb_complex* b, const sb_complex* x0,
+                          const sb_ir_config* cfg, sb_complex* x, sb_gmres_stats* stats);
+SB_API int sb_gmres_mixed_device(const sb_operator* op, const sb_complex* b_dev,
+                                 sb_complex* x_dev, int x0_given, const sb_ir_config* cfg,
+                                 sb_gmres_stats* stats);
+
+/* Plane-wave RHS written to device memory (n x r complex128) on the operator's stream. */
+SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs,
+                                    const sb_complex* amps, int64_t r, sb_complex* rhs_dev);
+
+/* ---- timing (no reference counterpart: instrumentation, the PerfModel / runtime-stats role of
+ * crates/sonium-compute/src/perf.rs:1-30) ---- */
+/* Kernel classes timed by CUDA events recorded on their launching stream when profiling is on. */
+#define SB_PROF_FAR 0        /* far-field assembly tiles */
+#define SB_PROF_NEAR 1       /* near-pair subdivision kernel */
+#define SB_PROF_SELF 2       /* self (singular) kernel */
+#define SB_PROF_GEMV64 3     /* complex128 matvec (incl. fused residual) */
+#define SB_PROF_GEMV32 4     /* complex64 matvec (FP32 or FP64 vectors) */
+#define SB_PROF_ARNOLDI 5    /* Gram-Schmidt dots / projections / basis updates */
+#define SB_PROF_OTHER 6      /* geometry, coefficients, RHS reductions, plane waves */
+#define SB_PROF_KINDS 8
+typedef struct sb_profile {
+    double ms[SB_PROF_KINDS];
+    int64_t launches[SB_PROF_KINDS];
+    int64_t kernels; /* all kernels launched by the library (counted whether profiling is on or not) */
+} sb_profile;
+SB_API int sb_profile_enable(int on);
+/* Totals since the last reset (synchronises the recorded events); reset != 0 clears them. */
+SB_API int sb_profile_read(sb_profile* out, int reset);
+/* CUDA event helpers on an operator's stream, for timing whole solves on the device. */
+SB_API int sb_event_create(void** event);
+SB_API int sb_event_destroy(void* event);
+SB_API int sb_event_record(void* event, const sb_operator* op);
+SB_API int sb_event_elapsed_ms(void* start, void* stop, float* ms);
+
+/* ---- diagnostics ---- */
+/* The device sine/cosine used by every kernel phase exp(i k r) (the reference's exp_i,
+ * crates/sonium-fastmath/src/api.rs:450-456): s[i] = sin(x[i]), c[i] = cos(x[i]) computed on
+ * `device`, for testing it against golden values. */
+SB_API int sb_math_sincos(int device, const double* x, int64_t n, double* s, double* c);
+
+/* ---- fault injection (tbem.rs:6740-6794, injection point crates/sonium-compute/src/cuda/
+ * cublas.rs:3128): the next library call that reaches `point` fails with SB_ERR_INJECTED
+ * before any device work, releasing its transient buffers. ---- */
+#define SB_INJECT_NONE 0
+#define SB_INJECT_ALLOC 1
+#define SB_INJECT_LAUNCH 2
+SB_API int sb_inject_failure(int point);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

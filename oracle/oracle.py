@@ -1,0 +1,263 @@
+"""ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+The oracle is a plain C++ restatement of the reference (sonium-bem) CPU path, built from
+``oracle/tbem_oracle.cpp`` by ``oracle/Makefile``. Only the tests, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py`` import this module; the product library never does.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libtbem_oracle.so")
+_lib = None
+
+
+class OrC128(ct.Structure):
+    _fields_ = [("re", ct.c_double), ("im", ct.c_double)]
+
+
+class OrPhysics(ct.Structure):
+    _fields_ = [(n, ct.c_double) for n in (
+        "frequency", "speed_of_sound", "density", "wave_number", "omega", "wave_length",
+        "harmonic_factor", "pressure_factor", "tau")]
+
+
+class OrBc(ct.Structure):
+    _fields_ = [("kind", ct.c_void_p), ("value", ct.c_void_p), ("has_adm", ct.c_void_p),
+                ("adm", ct.c_void_p)]
+
+
+class OrGmresResult(ct.Structure):
+    _fields_ = [("iterations", ct.c_int64), ("restarts", ct.c_int64), ("matvecs", ct.c_int64),
+                ("residual", ct.c_double), ("estimated_residual", ct.c_double),
+                ("backward_error", ct.c_double), ("converged", ct.c_int32),
+                ("status", ct.c_int32)]
+
+
+def build() -> str:
+    """Compile the oracle library with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ct.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    P = ct.c_void_p
+    L.or_physics_new.argtypes = [ct.c_double, ct.c_double, ct.c_double, ct.c_int,
+                                 ct.POINTER(OrPhysics)]
+    L.or_icosphere_counts.argtypes = [ct.c_int, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]
+    L.or_icosphere.argtypes = [ct.c_double, ct.c_int, ct.c_double, ct.c_double, ct.c_double, P, P]
+    L.or_element_geometry.argtypes = [ct.c_int64, P, P, P, P, P]
+    L.or_assemble_rows.argtypes = [ct.c_int64, P, ct.c_int64, P, ct.POINTER(OrBc),
+                                   ct.POINTER(OrPhysics), OrC128, ct.c_int64, ct.c_int64,
+                                   ct.c_int, P, P]
+    L.or_regular_pair.argtypes = [P, P, P, ct.c_double, ct.POINTER(OrPhysics), P]
+    L.or_singular_pair.argtypes = [P, P, P, ct.POINTER(OrPhysics), P]
+    L.or_subelements.argtypes = [P, P, ct.c_double, P, ct.c_int]
+    L.or_rhs_plane_wave.argtypes = [ct.c_int64, P, P, ct.POINTER(OrPhysics), OrC128,
+                                    ct.c_int64, P, P, P]
+    L.or_gmres.argtypes = [ct.c_int64, P, P, P, ct.c_int64, ct.c_int64, ct.c_double, ct.c_int,
+                           P, ct.POINTER(OrGmresResult)]
+    L.or_matvec.argtypes = [ct.c_int64, P, P, P, ct.c_int]
+    L.or_sph_j.argtypes = [ct.c_int, ct.c_double]
+    L.or_sph_j.restype = ct.c_double
+    L.or_sph_y.argtypes = [ct.c_int, ct.c_double]
+    L.or_sph_y.restype = ct.c_double
+    L.or_mie_rigid_coefficients.argtypes = [ct.c_double, ct.c_int, P]
+    L.or_mie_rigid_field.argtypes = [ct.c_double, ct.c_double, ct.c_int, ct.c_double,
+                                     ct.c_int64, P, P]
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ct.c_void_p)
+
+
+def physics(frequency: float, speed_of_sound: float = 343.0, density: float = 1.21,
+            internal: bool = False) -> OrPhysics:
+    out = OrPhysics()
+    lib().or_physics_new(frequency, speed_of_sound, density, int(internal), ct.byref(out))
+    return out
+
+
+def physics_for_k(k: float, speed_of_sound: float = 343.0, density: float = 1.21) -> OrPhysics:
+    return physics(k * speed_of_sound / (2.0 * np.pi), speed_of_sound, density)
+
+
+def bm_beta(ph: OrPhysics, scale: float = 1.0) -> complex:
+    """burton_miller_beta (crates/sonium-bem/src/core/types.rs:314-320), times ``scale``."""
+    if ph.tau > 0.0:
+        return complex(0.0, scale * ph.harmonic_factor / ph.wave_number)
+    return 0j
+
+
+def icosphere(radius: float, level: int, scale=(1.0, 1.0, 1.0)):
+    nn, nt = ct.c_int64(), ct.c_int64()
+    if lib().or_icosphere_counts(level, ct.byref(nn), ct.byref(nt)):
+        raise ValueError("bad icosphere level")
+    nodes = np.zeros((nn.value, 3), np.float64)
+    tris = np.zeros((nt.value, 3), np.uint32)
+    rc = lib().or_icosphere(radius, level, scale[0], scale[1], scale[2], _p(nodes), _p(tris))
+    if rc:
+        raise RuntimeError("icosphere failed")
+    return nodes, tris
+
+
+def element_geometry(nodes: np.ndarray, tris: np.ndarray):
+    m = tris.shape[0]
+    c = np.zeros((m, 3)); n = np.zeros((m, 3)); a = np.zeros(m)
+    lib().or_element_geometry(m, _p(np.ascontiguousarray(nodes, np.float64)),
+                              _p(np.ascontiguousarray(tris, np.uint32)), _p(c), _p(n), _p(a))
+    return c, n, a
+
+
+def _bc_struct(m, bc_kind=None, bc_value=None, admittance=None, keep=None):
+    b = OrBc()
+    if bc_kind is not None:
+        k = np.ascontiguousarray(bc_kind, np.int32); keep.append(k); b.kind = k.ctypes.data
+    if bc_value is not None:
+        v = np.ascontiguousarray(bc_value, np.complex128); keep.append(v); b.value = v.ctypes.data
+    if admittance is not None:
+        adm = np.asarray(admittance, np.complex128)
+        has = np.ascontiguousarray(~np.isnan(adm.real), np.uint8)
+        adm = np.ascontiguousarray(np.nan_to_num(adm), np.complex128)
+        keep += [has, adm]
+        b.has_adm = has.ctypes.data
+        b.adm = adm.ctypes.data
+    return b
+
+
+def assemble(nodes, tris, ph: OrPhysics, beta: complex, rows=None, bc_kind=None, bc_value=None,
+             admittance=None, threads: int = 0):
+    """Rows [r0, r1) of the dense TBEM matrix and RHS (build_tbem_system_with_beta_parallel).
+
+    ``admittance`` holds NaN for elements without admittance."""
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    tris = np.ascontiguousarray(tris, np.uint32)
+    m = tris.shape[0]
+    r0, r1 = (0, m) if rows is None else rows
+    A = np.zeros((r1 - r0, m), np.complex128)
+    rhs = np.zeros(r1 - r0, np.complex128)
+    keep = []
+    b = _bc_struct(m, bc_kind, bc_value, admittance, keep)
+    rc = lib().or_assemble_rows(nodes.shape[0], _p(nodes), m, _p(tris), ct.byref(b),
+                                ct.byref(ph), OrC128(beta.real, beta.imag), r0, r1, threads,
+                                _p(A), _p(rhs))
+    if rc:
+        raise ValueError("oracle assembly rejected its input")
+    return A, rhs
+
+
+def regular_pair(x, nx, coords, area, ph):
+    out = np.zeros(4, np.complex128)
+    lib().or_regular_pair(_p(np.ascontiguousarray(x, np.float64)),
+                          _p(np.ascontiguousarray(nx, np.float64)),
+                          _p(np.ascontiguousarray(coords, np.float64)), area, ct.byref(ph),
+                          _p(out))
+    return out
+
+
+def singular_pair(x, nx, coords, ph):
+    out = np.zeros(4, np.complex128)
+    lib().or_singular_pair(_p(np.ascontiguousarray(x, np.float64)),
+                           _p(np.ascontiguousarray(nx, np.float64)),
+                           _p(np.ascontiguousarray(coords, np.float64)), ct.byref(ph), _p(out))
+    return out
+
+
+def subelements(x, coords, area, cap=256):
+    leaves = np.zeros((cap, 8))
+    n = lib().or_subelements(_p(np.ascontiguousarray(x, np.float64)),
+                             _p(np.ascontiguousarray(coords, np.float64)), area, _p(leaves), cap)
+    return leaves[:min(n, cap)]
+
+
+def rhs_plane_wave(centers, normals, ph, beta, dirs, amps=None):
+    centers = np.ascontiguousarray(centers, np.float64)
+    normals = np.ascontiguousarray(normals, np.float64)
+    dirs = np.ascontiguousarray(np.atleast_2d(dirs), np.float64)
+    n, r = centers.shape[0], dirs.shape[0]
+    out = np.zeros((n, r), np.complex128)
+    a = None if amps is None else np.ascontiguousarray(amps, np.complex128)
+    lib().or_rhs_plane_wave(n, _p(centers), _p(normals), ct.byref(ph),
+                            OrC128(beta.real, beta.imag), r, _p(dirs),
+                            None if a is None else _p(a), _p(out))
+    return out
+
+
+def gmres(A, b, restart=30, max_iterations=100, tol=1e-8, x0=None, threads=0):
+    A = np.ascontiguousarray(A, np.complex128)
+    b = np.ascontiguousarray(b, np.complex128)
+    n = b.shape[0]
+    x = np.zeros(n, np.complex128)
+    res = OrGmresResult()
+    x0a = None if x0 is None else np.ascontiguousarray(x0, np.complex128)
+    lib().or_gmres(n, _p(A), _p(b), None if x0a is None else _p(x0a), max_iterations, restart,
+                   tol, threads, _p(x), ct.byref(res))
+    return x, res
+
+
+def matvec(A, x, threads=0):
+    A = np.ascontiguousarray(A, np.complex128)
+    x = np.ascontiguousarray(x, np.complex128)
+    y = np.zeros(A.shape[0], np.complex128)
+    lib().or_matvec(A.shape[0], _p(A), _p(x), _p(y), threads)
+    return y
+
+
+def sph_j(n, x):
+    return lib().or_sph_j(n, x)
+
+
+def sph_y(n, x):
+    return lib().or_sph_y(n, x)
+
+
+def mie_coefficients(ka, num_terms):
+    out = np.zeros(num_terms, np.complex128)
+    lib().or_mie_rigid_coefficients(ka, num_terms, _p(out))
+    return out
+
+
+def mie_field(k, radius, num_terms, r, theta):
+    theta = np.ascontiguousarray(theta, np.float64)
+    out = np.zeros(theta.shape[0], np.complex128)
+    lib().or_mie_rigid_field(k, radius, num_terms, r, theta.shape[0], _p(theta), _p(out))
+    return out
+
+
+def suggested_sphere_terms(ka: float) -> int:
+    """suggested_sphere_terms (crates/sonium-wave/src/analytical/solutions_3d.rs:241-249)."""
+    if np.isfinite(ka) and ka > 0:
+        return max(int(np.ceil(ka)) * 4 + 16, 17)
+    return 16
+
+
+def weighted_relative_l2(computed, reference, weights):
+    """weighted_relative_l2_error (crates/sonium-qa/src/lib.rs:264-311)."""
+    d = np.sum(weights * np.abs(computed - reference) ** 2)
+    r = np.sum(weights * np.abs(reference) ** 2)
+    return float(np.sqrt(d / r))
+
+
+def rigid_sphere_surface_error(x, centers, areas, k, radius, num_terms=None):
+    """rigid_sphere_surface_relative_l2_error (crates/sonium-qa/src/lib.rs:319-358)."""
+    if num_terms is None:
+        num_terms = suggested_sphere_terms(k * radius)
+    rad = np.linalg.norm(centers, axis=1)
+    theta = np.arccos(np.clip(centers[:, 2] / rad, -1.0, 1.0))
+    ref = mie_field(k, radius, num_terms, radius, theta)
+    return weighted_relative_l2(x, ref, areas)

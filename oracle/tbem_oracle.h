@@ -1,0 +1,114 @@
+/*
+ * CPU oracle for the dense Burton-Miller TBEM path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * This library is the checker the CUDA product is compared against. It is a
+ * plain C++ restatement of the reference (sonium-bem, Rust) CPU algorithms;
+ * only tests, the smoke check and the CPU-baseline leg of the benchmark may
+ * load it. Nothing in the product library links or calls it.
+ *
+ * Parity pins: the Mie/spherical-Bessel parts are pinned by the reference's
+ * golden fixtures (crates/sonium-wave/fixtures/scattering-golden-v1.json and
+ * special-golden-wolfram-v1.json, extracted into tests/golden/). The TBEM
+ * matrix itself has no golden vector in the reference; it is pinned through
+ * the reference's own invariants (thread-count independence, RHS-only ==
+ * full, partial rows == full) and the Mie convergence of the solved field.
+ *
+ * Every function cites the reference file:line it restates.
+ */
+#ifndef SONIUM_TBEM_ORACLE_H
+#define SONIUM_TBEM_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_c128 {
+    double re, im;
+} or_c128;
+
+/* Mirrors PhysicsParams (crates/sonium-bem/src/core/types.rs:34-53,165-190). */
+typedef struct or_physics {
+    double frequency, speed_of_sound, density, wave_number, omega, wave_length;
+    double harmonic_factor, pressure_factor, tau;
+} or_physics;
+
+void or_physics_new(double frequency, double speed_of_sound, double density, int is_internal,
+                    or_physics* out);
+
+/* generate_icosphere_mesh (crates/sonium-bem/src/core/mesh/generators.rs:309-397) with an
+ * optional per-axis vertex scale applied after the radius (ellipsoid configs). */
+int or_icosphere_counts(int level, int64_t* n_nodes, int64_t* n_tris);
+int or_icosphere(double radius, int level, double sx, double sy, double sz, double* nodes,
+                 uint32_t* tris);
+
+/* compute_element_geometry (generators.rs:771-830): centroid, unit normal, area. */
+void or_element_geometry(int64_t n_tris, const double* nodes, const uint32_t* tris,
+                         double* centers, double* normals, double* areas);
+
+/* Boundary condition per element: kind 0 = velocity (Neumann), 1 = pressure (Dirichlet);
+ * value = the element's (averaged) prescribed value; has_adm/adm = surface admittance.
+ * Null pointers mean rigid (velocity 0, no admittance). */
+typedef struct or_bc {
+    const int32_t* kind;
+    const or_c128* value;
+    const uint8_t* has_adm;
+    const or_c128* adm;
+} or_bc;
+
+/* build_tbem_system_with_beta_parallel (crates/sonium-bem/src/core/assembly/tbem.rs:1284-1466)
+ * for source rows [row0, row1). A is (row1-row0) x n_tris row-major, rhs has row1-row0 entries.
+ * threads <= 0 uses all OpenMP threads. */
+int or_assemble_rows(int64_t n_nodes, const double* nodes, int64_t n_tris, const uint32_t* tris,
+                     const or_bc* bc, const or_physics* phys, or_c128 beta, int64_t row0,
+                     int64_t row1, int threads, or_c128* A, or_c128* rhs);
+
+/* Single-pair channel integrals (G, H, H^T, E) as 4 complex numbers, for unit tests.
+ * regular_integration (crates/sonium-bem/src/core/integration/regular.rs:124-321) and
+ * singular_integration (crates/sonium-bem/src/core/integration/singular.rs:297-614). */
+void or_regular_pair(const double* x, const double* nx, const double* coords9, double area,
+                     const or_physics* phys, or_c128* out4);
+void or_singular_pair(const double* x, const double* nx, const double* coords9,
+                      const or_physics* phys, or_c128* out4);
+
+/* generate_subelements (singular.rs:1372-1540): returns the leaf count, writes up to cap
+ * leaves as [v0x v0y v1x v1y v2x v2y factor order]. */
+int or_subelements(const double* x, const double* coords9, double area, double* leaves, int cap);
+
+/* IncidentField::compute_rhs_with_beta for a plane wave (crates/sonium-bem/src/core/incident.rs:
+ * 216-245, 315-331, 807-833). dirs: r x 3, amps: r; rhs: n x r row-major. */
+void or_rhs_plane_wave(int64_t n, const double* centers, const double* normals,
+                       const or_physics* phys, or_c128 beta, int64_t r, const double* dirs,
+                       const or_c128* amps, or_c128* rhs);
+
+/* Restarted GMRES (crates/sonium-solvers/crates/sonium-solvers-iterative/src/gmres.rs:631-1047,
+ * finalize 159-247), dense row-major operator, identity preconditioner. */
+typedef struct or_gmres_result {
+    int64_t iterations, restarts, matvecs;
+    double residual, estimated_residual, backward_error;
+    int32_t converged, status; /* status: 0 converged, 1 max iterations, 2 breakdown, 3 numerical */
+} or_gmres_result;
+
+int or_gmres(int64_t n, const or_c128* A, const or_c128* b, const or_c128* x0,
+             int64_t max_iterations, int64_t restart, double tolerance, int threads,
+             or_c128* x, or_gmres_result* res);
+
+/* Dense complex matvec y = A x (row-major), the reference CPU GEMV
+ * (crates/sonium-solvers/crates/sonium-solvers-core/src/dense.rs:416-427). */
+void or_matvec(int64_t n, const or_c128* A, const or_c128* x, or_c128* y, int threads);
+
+/* Spherical Bessel j_n, y_n (crates/sonium-wave/src/analytical/solutions_3d.rs:808-900),
+ * rigid-sphere Mie coefficients (solutions_3d.rs:769-806) and the surface field
+ * (solutions_3d.rs:315-366). */
+double or_sph_j(int n, double x);
+double or_sph_y(int n, double x);
+void or_mie_rigid_coefficients(double ka, int num_terms, or_c128* out);
+void or_mie_rigid_field(double k, double radius, int num_terms, double r, int64_t n_theta,
+                        const double* theta, or_c128* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,20 @@
+"""sonium-b200: dense Burton-Miller TBEM (assembly, matvec, GMRES) on NVIDIA B200 (sm_100a).
+
+The compute path is the CUDA shared library built from ``sonium_b200/csrc`` (C ABI in
+``include/sonium_b200.h``); this package is its Python binding. There is no CPU fallback.
+"""
+from ._lib import (SB_BC_PRESSURE, SB_BC_VELOCITY, SB_INJECT_ALLOC, SB_INJECT_LAUNCH, SB_INJECT_NONE,
+                   SB_OP_C, SB_OP_N, SB_OP_T, SB_PRECISION_FP64, SB_PRECISION_FP64_FP32,
+                   SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI, SoniumError)
+from .tbem import (GmresConfig, GmresSolution, IrConfig, JacobiPreconditioner, LinearOperator, Mesh,
+                   PhysicsParams, TbemOperator, build_tbem_system, build_tbem_system_with_beta,
+                   device_count, gmres, gmres_mixed, icosphere, inject_failure, rhs_plane_wave)
+
+__all__ = [
+    "GmresConfig", "GmresSolution", "IrConfig", "JacobiPreconditioner", "LinearOperator", "Mesh",
+    "PhysicsParams", "TbemOperator", "build_tbem_system", "build_tbem_system_with_beta", "device_count",
+    "gmres", "gmres_mixed", "icosphere", "inject_failure", "rhs_plane_wave", "SoniumError",
+    "SB_BC_PRESSURE", "SB_BC_VELOCITY", "SB_INJECT_ALLOC", "SB_INJECT_LAUNCH", "SB_INJECT_NONE",
+    "SB_OP_C", "SB_OP_N", "SB_OP_T", "SB_PRECISION_FP64", "SB_PRECISION_FP64_FP32",
+    "SB_PRECOND_IDENTITY", "SB_PRECOND_JACOBI",
+]

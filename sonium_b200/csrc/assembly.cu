@@ -1,0 +1,1240 @@
+// Dense Burton-Miller TBEM assembly on sm_100a: mesh precompute, near-pair classification and
+// the far / near / self kernels.
+//
+// Reference (paths relative to the sonium workspace root):
+//   build_tbem_system_with_beta_parallel  crates/sonium-bem/src/core/assembly/tbem.rs:1284-1466
+//   regular_integration                   crates/sonium-bem/src/core/integration/regular.rs:124-321
+//   generate_subelements                  crates/sonium-bem/src/core/integration/singular.rs:1372-1540
+//   singular_integration                  crates/sonium-bem/src/core/integration/singular.rs:297-614
+//
+// Work split. A pair (source i, field j) whose level-0 subdivision test passes
+// (dist(centre_j, x_i) >= 3 sqrt(area_j)) is a single 13-point leaf: the far kernel evaluates
+// those with field-element quadrature points staged in shared memory by a bulk async copy and
+// one thread per (row, column) so that the complex stores of a warp are contiguous. Pairs that
+// may fail the test (a superset with a 1e-9 relative margin, decided with correctly rounded
+// operations so every kernel agrees) go to the near kernel, one warp per pair, which replays
+// the reference subdivision tree exactly (level order, the 15-split and 110-leaf limits) and
+// reduces the leaf points with warp shuffles. The diagonal goes to the self kernel, one warp per
+// element (regularised edge integral + Duffy sub-triangles).
+
+#include <mutex>
+
+#include "sb_device.cuh"
+#include "sb_internal.cuh"
+#include "sb_profile.cuh"
+
+namespace sb {
+
+// ---------------------------------------------------------------------------------------------
+// Quadrature tables
+// ---------------------------------------------------------------------------------------------
+__constant__ double c_gl_x[kGLTotal];
+__constant__ double c_gl_w[kGLTotal];
+__constant__ double c_tri_xi[kTriTotal];
+__constant__ double c_tri_eta[kTriTotal];
+__constant__ double c_tri_w[kTriTotal];
+__constant__ int c_tri_off[kTriOrders];
+__constant__ int c_tri_cnt[kTriOrders];
+
+// Gauss-Legendre on [-1, 1] by Newton iteration on the Legendre three-term recurrence.
+void host_gauss_legendre(int n, double* x, double* w) {
+    const int half = (n + 1) / 2;
+    const double nf = n;
+    for (int i = 0; i < half; ++i) {
+        double root = std::cos(3.14159265358979323846 * (i + 0.75) / (nf + 0.5));
+        for (int it = 0; it < 32; ++it) {
+            double p0 = 1.0, p1 = root;
+            for (int d = 2; d <= n; ++d) {
+                double p2 = ((2 * d - 1) * root * p1 - (d - 1) * p0) / d;
+                p0 = p1;
+                p1 = p2;
+            }
+            double dp = nf * (root * p1 - p0) / (root * root - 1.0);
+            double next = root - p1 / dp;
+            bool done = std::fabs(next - root) <= 8.9e-16 * std::fmax(std::fabs(next), 1.0);
+            root = next;
+            if (done) break;
+        }
+        double p0 = 1.0, p1 = root;
+        for (int d = 2; d <= n; ++d) {
+            double p2 = ((2 * d - 1) * root * p1 - (d - 1) * p0) / d;
+            p0 = p1;
+            p1 = p2;
+        }
+        double dp = nf * (root * p1 - p0) / (root * root - 1.0);
+        double wt = 2.0 / ((1.0 - root * root) * dp * dp);
+        if (n == 1) {
+            root = 0.0;
+            wt = 2.0;
+        }
+        x[i] = -root;
+        x[n - 1 - i] = root;
+        w[i] = wt;
+        w[n - 1 - i] = wt;
+    }
+}
+
+// The published 13-point degree-7 symmetric triangle rule on the unit simplex, with the
+// 15-digit constants the reference table carries (crates/sonium-bem/src/core/integration/
+// gauss.rs:524-538) so that leaf quadratures agree with it to rounding.
+static const double kRule13[13][3] = {
+    {0.333333333333333, 0.333333333333333, -0.149570044467682},
+    {0.260345966079040, 0.260345966079040, 0.175615257433208},
+    {0.260345966079040, 0.479308067841920, 0.175615257433208},
+    {0.479308067841920, 0.260345966079040, 0.175615257433208},
+    {0.065130102902216, 0.065130102902216, 0.053347235608838},
+    {0.065130102902216, 0.869739794195568, 0.053347235608838},
+    {0.869739794195568, 0.065130102902216, 0.053347235608838},
+    {0.638444188569810, 0.048690315425316, 0.077113760890257},
+    {0.048690315425316, 0.638444188569810, 0.077113760890257},
+    {0.638444188569810, 0.312865496004874, 0.077113760890257},
+    {0.312865496004874, 0.638444188569810, 0.077113760890257},
+    {0.048690315425316, 0.312865496004874, 0.077113760890257},
+    {0.312865496004874, 0.048690315425316, 0.077113760890257}};
+
+// triangle_quadrature (gauss.rs:110-156) for leaf orders 4..7: order 4 is the 13-point rule,
+// higher orders the Duffy-collapsed Gauss-Legendre product; weights sum to 0.5.
+int host_triangle_rule(int order, double* xi, double* eta, double* w) {
+    if (order == 4) {
+        for (int i = 0; i < 13; ++i) {
+            xi[i] = kRule13[i][0];
+            eta[i] = kRule13[i][1];
+            w[i] = kRule13[i][2] * 0.5;
+        }
+        return 13;
+    }
+    double gx[16], gw[16];
+    host_gauss_legendre(order, gx, gw);
+    int c = 0;
+    for (int a = 0; a < order; ++a) {
+        double u = 0.5 * (gx[a] + 1.0), uw = 0.5 * gw[a];
+        for (int b = 0; b < order; ++b) {
+            double v = 0.5 * (gx[b] + 1.0), vw = 0.5 * gw[b];
+            xi[c] = u;
+            eta[c] = (1.0 - u) * v;
+            w[c] = uw * vw * (1.0 - u);
+            ++c;
+        }
+    }
+    return c;
+}
+
+void ensure_tables(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    SB_REQUIRE(device >= 0 && device < 64, SB_ERR_INVALID_ARGUMENT, "device index out of range");
+    if (done[device]) return;
+    double gx[kGLTotal], gw[kGLTotal];
+    for (int n = 1; n <= kMaxGL; ++n) host_gauss_legendre(n, gx + n * (n - 1) / 2, gw + n * (n - 1) / 2);
+    double tx[kTriTotal], te[kTriTotal], tw[kTriTotal];
+    int off[kTriOrders], cnt[kTriOrders], c = 0;
+    for (int o = 4; o <= 7; ++o) {
+        off[o - 4] = c;
+        cnt[o - 4] = host_triangle_rule(o, tx + c, te + c, tw + c);
+        c += cnt[o - 4];
+    }
+    SB_CUDA(cudaMemcpyToSymbol(c_gl_x, gx, sizeof(gx)));
+    SB_CUDA(cudaMemcpyToSymbol(c_gl_w, gw, sizeof(gw)));
+    SB_CUDA(cudaMemcpyToSymbol(c_tri_xi, tx, sizeof(tx)));
+    SB_CUDA(cudaMemcpyToSymbol(c_tri_eta, te, sizeof(te)));
+    SB_CUDA(cudaMemcpyToSymbol(c_tri_w, tw, sizeof(tw)));
+    SB_CUDA(cudaMemcpyToSymbol(c_tri_off, off, sizeof(off)));
+    SB_CUDA(cudaMemcpyToSymbol(c_tri_cnt, cnt, sizeof(cnt)));
+    done[device] = true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mesh precompute
+// ---------------------------------------------------------------------------------------------
+#define E(f, e) elem[(int64_t)(f) * ld + (e)]
+
+// compute_element_geometry (generators.rs:771-830) and the level-0 subdivision centre
+// local_to_global(1/3, 1/3) (singular.rs:1409-1418, 1580-1606), with explicitly rounded
+// operations so the host-visible geometry does not depend on multiply-add contraction.
+__global__ void k_element_geometry(const double* __restrict__ nodes,
+                                   const uint32_t* __restrict__ tris, int64_t n, int64_t ld,
+                                   double* __restrict__ elem) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ld) return;
+    if (e >= n) {
+        for (int f = 0; f < EFIELDS; ++f) E(f, e) = 0.0;
+        return;
+    }
+    double v[3][3];
+    for (int a = 0; a < 3; ++a) {
+        uint32_t t = tris[3 * e + a];
+        for (int j = 0; j < 3; ++j) v[a][j] = nodes[3 * (int64_t)t + j];
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 3; ++j) E(EV0X + 3 * a + j, e) = v[a][j];
+    for (int j = 0; j < 3; ++j) {
+        double s = __dadd_rn(__dadd_rn(__dadd_rn(0.0, v[0][j]), v[1][j]), v[2][j]);
+        E(ECX + j, e) = __ddiv_rn(s, 3.0);
+    }
+    double a1[3], a2[3];
+    for (int j = 0; j < 3; ++j) {
+        a1[j] = __dsub_rn(v[1][j], v[0][j]);
+        a2[j] = __dsub_rn(v[2][j], v[0][j]);
+    }
+    double c0 = __dsub_rn(__dmul_rn(a1[1], a2[2]), __dmul_rn(a1[2], a2[1]));
+    double c1 = __dsub_rn(__dmul_rn(a1[2], a2[0]), __dmul_rn(a1[0], a2[2]));
+    double c2 = __dsub_rn(__dmul_rn(a1[0], a2[1]), __dmul_rn(a1[1], a2[0]));
+    double len = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(c0, c0), __dmul_rn(c1, c1)), __dmul_rn(c2, c2)));
+    E(EAREA, e) = __ddiv_rn(len, 2.0);
+    E(EJAC, e) = len;
+    if (len > 1e-15) {
+        E(ENX, e) = __ddiv_rn(c0, len);
+        E(ENY, e) = __ddiv_rn(c1, len);
+        E(ENZ, e) = __ddiv_rn(c2, len);
+    } else {
+        E(ENX, e) = E(ENY, e) = E(ENZ, e) = 0.0;
+    }
+    const double third = __ddiv_rn(1.0, 3.0);
+    const double sf0 = __dsub_rn(__dsub_rn(1.0, third), third);
+    for (int j = 0; j < 3; ++j) {
+        double g = __dadd_rn(0.0, __dmul_rn(sf0, v[0][j]));
+        g = __dadd_rn(g, __dmul_rn(third, v[1][j]));
+        g = __dadd_rn(g, __dmul_rn(third, v[2][j]));
+        E(EGX + j, e) = g;
+    }
+    E(ESQA, e) = __dsqrt_rn(E(EAREA, e));
+}
+
+// Far-field leaf points of every element: position of the 13-point rule on the flat triangle
+// (compute_parameters, regular.rs:636-714) and weight * Jacobian, in tile-blocked SoA
+// qp[((tile * 13 + q) * 4 + c) * kFarTile + lane] so one contiguous block feeds a column tile.
+__global__ void k_far_points(const double* __restrict__ elem, int64_t n, int64_t ld,
+                             double* __restrict__ qp) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ld) return;
+    const int64_t tile = e / kFarTile;
+    const int lane = static_cast<int>(e % kFarTile);
+    const int o = c_tri_off[0];
+    for (int q = 0; q < kFarPoints; ++q) {
+        double* dst = qp + ((tile * kFarPoints + q) * 4) * kFarTile + lane;
+        if (e >= n) {
+            dst[0] = dst[kFarTile] = dst[2 * kFarTile] = dst[3 * kFarTile] = 0.0;
+            continue;
+        }
+        const double s = c_tri_xi[o + q], t = c_tri_eta[o + q];
+        const double sf0 = 1.0 - s - t;
+        for (int j = 0; j < 3; ++j)
+            dst[j * kFarTile] = sf0 * E(EV0X + j, e) + s * E(EV1X + j, e) + t * E(EV2X + j, e);
+        dst[3 * kFarTile] = c_tri_w[o + q] * E(EJAC, e);
+    }
+}
+
+// Superset of the reference's level-0 "must subdivide" test ratdis < 3 (singular.rs:1431):
+// dist^2 < 9 (1 + 1e-9) area, evaluated with correctly rounded operations so that the
+// classifier and the far kernel make bitwise-identical decisions.
+__device__ __forceinline__ bool near_superset(double gx, double gy, double gz, double thr,
+                                              double x, double y, double z) {
+    double dx = __dsub_rn(gx, x), dy = __dsub_rn(gy, y), dz = __dsub_rn(gz, z);
+    double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return d2 < thr;
+}
+__device__ __forceinline__ double near_threshold(double area) {
+    return __dmul_rn(9.000000009, area);
+}
+
+constexpr int kNearRows = 32;
+
+// Near-pair classification, one CTA per 32 source rows. pass 0 counts per row, pass 1 writes
+// the column indices in increasing order (row_ptr from the host-side scan).
+__global__ void __launch_bounds__(256) k_near_pass(const double* __restrict__ elem, int64_t n,
+                                                   int64_t ld, int pass,
+                                                   int64_t* __restrict__ counts,
+                                                   const int64_t* __restrict__ row_ptr,
+                                                   int32_t* __restrict__ cols) {
+    __shared__ double sx[kNearRows][3];
+    __shared__ unsigned sball[8][kNearRows];
+    __shared__ int64_t sbase[kNearRows];
+    __shared__ int scount[kNearRows];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t row0 = blockIdx.x * (int64_t)kNearRows;
+    if (tid < kNearRows) {
+        int64_t i = row0 + tid;
+        for (int c = 0; c < 3; ++c) sx[tid][c] = (i < n) ? E(ECX + c, i) : 1e300;
+        scount[tid] = 0;
+        sbase[tid] = (pass == 1 && i < n) ? row_ptr[i] : 0;
+    }
+    __syncthreads();
+    for (int64_t c0 = 0; c0 < n; c0 += 256) {
+        const int64_t j = c0 + tid;
+        double gx = 0, gy = 0, gz = 0, thr = -1.0;
+        if (j < n) {
+            gx = E(EGX, j);
+            gy = E(EGY, j);
+            gz = E(EGZ, j);
+            thr = near_threshold(E(EAREA, j));
+        }
+        for (int r = 0; r < kNearRows; ++r) {
+            const int64_t i = row0 + r;
+            bool p = (j < n) && (i < n) && (j != i) &&
+                     near_superset(gx, gy, gz, thr, sx[r][0], sx[r][1], sx[r][2]);
+            unsigned b = __ballot_sync(0xffffffffu, p);
+            if (pass == 0) {
+                if (lane == 0 && b) atomicAdd(&scount[r], __popc(b));
+            } else {
+                if (lane == 0) sball[warp][r] = b;
+            }
+        }
+        if (pass == 1) {
+            __syncthreads();
+            for (int r = 0; r < kNearRows; ++r) {
+                const unsigned b = sball[warp][r];
+                if (b & (1u << lane)) {
+                    int64_t pos = sbase[r];
+                    for (int w = 0; w < warp; ++w) pos += __popc(sball[w][r]);
+                    pos += __popc(b & ((1u << lane) - 1u));
+                    cols[pos] = static_cast<int32_t>(j);
+                }
+            }
+            __syncthreads();
+            if (tid < kNearRows) {
+                int64_t t = 0;
+                for (int w = 0; w < 8; ++w) t += __popc(sball[w][tid]);
+                sbase[tid] += t;
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    if (pass == 0 && tid < kNearRows && row0 + tid < n) counts[row0 + tid] = scount[tid];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Per-assembly element coefficients
+// ---------------------------------------------------------------------------------------------
+// coef[f * ld + e], f: 0-7 = (cG, cH, cHt, cE) complex matrix weights of the field element,
+// 8-15 = (dG, dH, dHt, dE) complex RHS weights (nonzero only for a nonzero prescribed value),
+// 16-17 = diagonal free term, 18-19 = RHS free term. From the coefficient / RHS formulas of
+// build_tbem_system_with_beta_parallel (tbem.rs:1344-1358, 1404-1444) with gamma = 1.
+enum { CF_CG = 0, CF_CH = 2, CF_CHT = 4, CF_CE = 6, CF_DG = 8, CF_DH = 10, CF_DHT = 12,
+       CF_DE = 14, CF_DIAG = 16, CF_RHS = 18, CF_FIELDS = 20 };
+
+__global__ void k_coefficients(int64_t n, int64_t ld, const int32_t* __restrict__ kind,
+                               const double2* __restrict__ value,
+                               const uint8_t* __restrict__ has_adm,
+                               const double2* __restrict__ adm, double tau, double pf,
+                               double2 beta, double* __restrict__ coef) {
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ld) return;
+    double2 out[10];
+    for (int f = 0; f < 10; ++f) out[f] = make_double2(0.0, 0.0);
+    if (e < n) {
+        const int k = kind ? kind[e] : 0;
+        const double2 v = value ? value[e] : make_double2(0.0, 0.0);
+        const bool hv = sqrt(v.x * v.x + v.y * v.y) > 1e-15;  // has_nonzero_bc, tbem.rs:1239
+        const bool ha = has_adm && has_adm[e];
+        const double2 Y = (ha && adm) ? adm[e] : make_double2(0.0, 0.0);
+        const double2 gt = make_double2(tau, 0.0);   // gamma * tau
+        const double2 iwr = make_double2(0.0, pf);   // i omega rho
+        const double2 bt = cscale(beta, tau);        // beta * tau
+        if (k == SB_BC_VELOCITY) {
+            out[1] = gt;    // H
+            out[3] = beta;  // E
+            if (ha) {
+                const double2 yi = cmul(Y, iwr);
+                out[0] = make_double2(-cmul(gt, yi).x, -cmul(gt, yi).y);
+                out[2] = make_double2(-cmul(beta, yi).x, -cmul(beta, yi).y);
+            }
+            if (hv) {
+                const double2 vi = cmul(v, iwr);
+                out[4] = cmul(gt, vi);
+                out[6] = cmul(beta, vi);
+            }
+            double2 d = make_double2(-0.5, 0.0);
+            if (ha) {
+                const double2 t = cscale(cmul(cmul(Y, iwr), bt), 0.5);
+                d = make_double2(d.x - t.x, d.y - t.y);
+            }
+            out[8] = d;
+            out[9] = cscale(cmul(cmul(v, iwr), bt), 0.5);
+        } else if (k == SB_BC_PRESSURE) {
+            out[0] = make_double2(-gt.x, -gt.y);
+            out[2] = make_double2(-beta.x, -beta.y);
+            if (hv) {
+                out[5] = cmul(gt, v);
+                out[7] = cmul(beta, v);
+            }
+            out[8] = cscale(bt, 0.5);
+            out[9] = make_double2(-0.5 * v.x, -0.5 * v.y);
+        }
+    }
+    for (int f = 0; f < 10; ++f) {
+        coef[(int64_t)(2 * f) * ld + e] = out[f].x;
+        coef[(int64_t)(2 * f + 1) * ld + e] = out[f].y;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Channel accumulation shared by all kernels: one quadrature point of regular.rs:229-281.
+// ---------------------------------------------------------------------------------------------
+struct Acc {
+    double gr = 0, gi = 0, hr = 0, hi = 0, tr = 0, ti = 0, er = 0, ei = 0;
+};
+
+// Adds the (G, H, H^T, E) contribution of a point at offset d = y - x (distance r, inverse
+// rinv) with weight * Jacobian `wga`, field normal ny and source normal nx.
+__device__ __forceinline__ void point_channels(Acc& a, double dx, double dy, double dz,
+                                               double r, double rinv, double wga, double nyx,
+                                               double nyy, double nyz, double nxx, double nxy,
+                                               double nxz, double k, double k2) {
+    double s, c;
+    sb_sincos(k * r, &s, &c);
+    const double gs = wga * kInv4Pi * rinv;
+    const double g_r = c * gs, g_i = s * gs;
+    const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+    const double rny = ux * nyx + uy * nyy + uz * nyz;
+    const double rnx = -(ux * nxx + uy * nxy + uz * nxz);
+    // zhh_base = G * (-1/r + i k)
+    const double b_r = -g_r * rinv - g_i * k;
+    const double b_i = g_r * k - g_i * rinv;
+    a.gr += g_r;
+    a.gi += g_i;
+    a.hr = fma(b_r, rny, a.hr);
+    a.hi = fma(b_i, rny, a.hi);
+    a.tr = fma(b_r, rnx, a.tr);
+    a.ti = fma(b_i, rnx, a.ti);
+    const double rq = rny * rnx;
+    const double nxny = nxx * nyx + nxy * nyy + nxz * nyz;
+    const double ri2 = rinv * rinv;
+    const double f_r = (3.0 * ri2 - k2) * rq + nxny * ri2;
+    const double f_i = -k * rinv * (3.0 * rq + nxny);
+    a.er += g_r * f_r - g_i * f_i;
+    a.ei += g_r * f_i + g_i * f_r;
+}
+
+__device__ __forceinline__ double2 combine(const Acc& a, const double* __restrict__ coef,
+                                           int64_t ld, int64_t j, int base) {
+    const double cgr = coef[(int64_t)(base + 0) * ld + j], cgi = coef[(int64_t)(base + 1) * ld + j];
+    const double chr = coef[(int64_t)(base + 2) * ld + j], chi = coef[(int64_t)(base + 3) * ld + j];
+    const double ctr = coef[(int64_t)(base + 4) * ld + j], cti = coef[(int64_t)(base + 5) * ld + j];
+    const double cer = coef[(int64_t)(base + 6) * ld + j], cei = coef[(int64_t)(base + 7) * ld + j];
+    double2 v;
+    v.x = a.gr * cgr - a.gi * cgi + a.hr * chr - a.hi * chi + a.tr * ctr - a.ti * cti + a.er * cer - a.ei * cei;
+    v.y = a.gr * cgi + a.gi * cgr + a.hr * chi + a.hi * chr + a.tr * cti + a.ti * ctr + a.er * cei + a.ei * cer;
+    return v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Far kernel
+// ---------------------------------------------------------------------------------------------
+constexpr int kFarRows = 32;
+constexpr int kQpTileDoubles = kFarPoints * 4 * kFarTile;
+constexpr long kWaitLimit = 1L << 26;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Bounded wait on an mbarrier phase. Returns false when the iteration limit is hit.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <bool kWithRhs, bool kWithF32>
+__global__ void __launch_bounds__(kFarTile) k_far(const double* __restrict__ qp,
+                                                  const double* __restrict__ elem, int64_t n,
+                                                  int64_t ld, const double* __restrict__ coef,
+                                                  double k, double2* __restrict__ A64,
+                                                  float2* __restrict__ A32, int64_t lda32,
+                                                  double2* __restrict__ far_part,
+                                                  int64_t n_tiles, int* __restrict__ status) {
+    extern __shared__ __align__(128) double smem[];
+    double* sq = smem;                              // [13][4][kFarTile]
+    double* sr = smem + kQpTileDoubles;             // [kFarRows][6]
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ double sred[kFarTile / 32][2];
+    const int tid = threadIdx.x;
+    const int64_t tile = blockIdx.x;
+    const int64_t j = tile * kFarTile + tid;
+    const int64_t row0 = blockIdx.y * (int64_t)kFarRows;
+    const double k2 = k * k;
+
+    // Stage this column tile's quadrature points with one bulk async copy (TMA engine).
+    const uint32_t bar_a = smem_addr(&bar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = kQpTileDoubles * sizeof(double);
+        const double* src = qp + tile * (int64_t)kQpTileDoubles;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_addr(sq)),
+            "l"(src), "r"(bytes), "r"(bar_a)
+            : "memory");
+    }
+    // Source rows (collocation point and normal) with plain loads meanwhile.
+    for (int t = tid; t < kFarRows * 6; t += kFarTile) {
+        const int r = t / 6, f = t % 6;
+        const int64_t i = row0 + r;
+        sr[t] = (i < n) ? E(ECX + f, i) : 0.0;  // ECX..ECZ then ENX..ENZ are contiguous fields
+    }
+    // Column constants in registers.
+    double nyx = 0, nyy = 0, nyz = 0, gx = 0, gy = 0, gz = 0, thr = -1;
+    if (j < n) {
+        nyx = E(ENX, j);
+        nyy = E(ENY, j);
+        nyz = E(ENZ, j);
+        gx = E(EGX, j);
+        gy = E(EGY, j);
+        gz = E(EGZ, j);
+        thr = near_threshold(E(EAREA, j));
+    }
+    const bool ok = mbar_wait(bar_a, 0);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) atomicExch(status, 1);
+        return;
+    }
+
+    const int64_t rows_here = (n - row0 < kFarRows) ? (n - row0) : kFarRows;
+    for (int r = 0; r < rows_here; ++r) {
+        const int64_t i = row0 + r;
+        const double xx = sr[r * 6 + 0], xy = sr[r * 6 + 1], xz = sr[r * 6 + 2];
+        const double nxx = sr[r * 6 + 3], nxy = sr[r * 6 + 4], nxz = sr[r * 6 + 5];
+        const bool active = (j < n) && (j != i) && !near_superset(gx, gy, gz, thr, xx, xy, xz);
+        double2 rhs_c = make_double2(0.0, 0.0);
+        if (active) {
+            Acc a;
+#pragma unroll
+            for (int q = 0; q < kFarPoints; ++q) {
+                const double* p = sq + q * 4 * kFarTile + tid;
+                const double dx = p[0] - xx, dy = p[kFarTile] - xy, dz = p[2 * kFarTile] - xz;
+                const double w = p[3 * kFarTile];
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                const double rinv = sb_rsqrt(d2);
+                point_channels(a, dx, dy, dz, d2 * rinv, rinv, w, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
+            }
+            const double2 v = combine(a, coef, ld, j, CF_CG);
+            A64[i * n + j] = v;
+            if (kWithF32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+            if (kWithRhs) rhs_c = combine(a, coef, ld, j, CF_DG);
+        }
+        if (kWithRhs) {
+            double sx = warp_sum(rhs_c.x), sy = warp_sum(rhs_c.y);
+            if ((tid & 31) == 0) {
+                sred[tid >> 5][0] = sx;
+                sred[tid >> 5][1] = sy;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                double tx = 0, ty = 0;
+                for (int w = 0; w < kFarTile / 32; ++w) {
+                    tx += sred[w][0];
+                    ty += sred[w][1];
+                }
+                far_part[i * n_tiles + tile] = make_double2(tx, ty);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Near kernel: one warp per near pair, exact replay of generate_subelements + regular leaves.
+// ---------------------------------------------------------------------------------------------
+constexpr int kNearWarps = 4;
+constexpr int kMaxNse = 60;
+constexpr int kMaxLeaves = 110;
+
+struct NearWarpSmem {
+    double xs[2][kMaxNse][3];
+    double es[2][kMaxNse][3];
+    double lv[kMaxNse][6];   // kept leaves of the current level: local vertices
+    int lorder[kMaxNse];
+    int loff[kMaxNse + 1];
+};
+
+// compute_gauss_order (singular.rs:1543-1573).
+__device__ __forceinline__ int gauss_order(double disfac) {
+    for (int o = 4; o <= 7; ++o) {
+        const double b = disfac / (2.0 * o + 1.0);
+        double p = 1.0;
+        for (int t = 0; t < 2 * o + 1; ++t) p *= b;
+        const double eg = p, eh = p * b, ee = p * b * b;
+        if (eg < 0.0005 && eh < 0.0005 && ee < 0.0005) return o;
+    }
+    return 7;
+}
+
+// Evaluates the regular-integration channels of pair (i, j) into lane-partial sums.
+__device__ void near_pair_channels(Acc& a, NearWarpSmem& S, const double* __restrict__ elem,
+                                   int64_t ld, int64_t i, int64_t j, double k, double k2,
+                                   int lane) {
+    const double x0 = E(ECX, i), x1 = E(ECY, i), x2 = E(ECZ, i);
+    const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
+    double V[3][3];
+    for (int t = 0; t < 3; ++t)
+        for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, j);
+    const double nyx = E(ENX, j), nyy = E(ENY, j), nyz = E(ENZ, j);
+    const double area = E(EAREA, j), jac = E(EJAC, j);
+
+    if (lane == 0) {
+        S.xs[0][0][0] = 0.0; S.xs[0][0][1] = 1.0; S.xs[0][0][2] = 0.0;
+        S.es[0][0][0] = 0.0; S.es[0][0][1] = 0.0; S.es[0][0][2] = 1.0;
+    }
+    __syncwarp();
+    int cur = 0, nsel = 1, total = 0;
+    double faclin = 2.0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int level = 0; level < 64; ++level) {
+        faclin *= 0.5;
+        const double arels = __dmul_rn(__dmul_rn(area, faclin), faclin);
+        const double sqa = __dsqrt_rn(arels);
+        bool sub[2] = {false, false};
+        double rat[2] = {0.0, 0.0};
+        for (int h = 0; h < 2; ++h) {
+            const int s = lane + 32 * h;
+            if (s < nsel) {
+                const double* xp = S.xs[cur][s];
+                const double* ep = S.es[cur][s];
+                const double sc = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(0.0, xp[0]), xp[1]), xp[2]), 3.0);
+                const double tc = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(0.0, ep[0]), ep[1]), ep[2]), 3.0);
+                const double sf0 = __dsub_rn(__dsub_rn(1.0, sc), tc);
+                double g[3];
+                for (int c = 0; c < 3; ++c) {
+                    double v = __dadd_rn(0.0, __dmul_rn(sf0, V[0][c]));
+                    v = __dadd_rn(v, __dmul_rn(sc, V[1][c]));
+                    v = __dadd_rn(v, __dmul_rn(tc, V[2][c]));
+                    g[c] = v;
+                }
+                const double dx = __dsub_rn(g[0], x0), dy = __dsub_rn(g[1], x1), dz = __dsub_rn(g[2], x2);
+                const double dist = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+                rat[h] = __ddiv_rn(dist, sqa);
+                sub[h] = rat[h] < 3.0;
+            }
+        }
+        const unsigned m0 = __ballot_sync(0xffffffffu, sub[0]);
+        const unsigned m1 = __ballot_sync(0xffffffffu, sub[1]);
+        const int nsub = __popc(m0) + __popc(m1);
+        // Position of the 16th subdivision, which ends the level (singular.rs:1432-1436).
+        int breakpos = nsel;
+        if (nsub >= 16) {
+            if (__popc(m0) >= 16) {
+                unsigned m = m0;
+                for (int t = 0; t < 15; ++t) m &= m - 1;
+                breakpos = __ffs(m) - 1;
+            } else {
+                unsigned m = m1;
+                for (int t = 0; t < 15 - __popc(m0); ++t) m &= m - 1;
+                breakpos = 32 + __ffs(m) - 1;
+            }
+        }
+        const unsigned valid0 = breakpos >= 32 ? 0xffffffffu : ((1u << breakpos) - 1u);
+        const unsigned valid1 = breakpos >= 64 ? 0xffffffffu : (breakpos <= 32 ? 0u : ((1u << (breakpos - 32)) - 1u));
+        const unsigned nsel0 = nsel >= 32 ? 0xffffffffu : ((1u << nsel) - 1u);
+        const unsigned nsel1 = nsel >= 64 ? 0xffffffffu : (nsel <= 32 ? 0u : ((1u << (nsel - 32)) - 1u));
+        const unsigned l0 = ~m0 & valid0 & nsel0;
+        const unsigned l1 = ~m1 & valid1 & nsel1;
+        const int nleaf = __popc(l0) + __popc(l1);
+        const int keep = min(nleaf, kMaxLeaves - total);
+        const int nxt = cur ^ 1;
+        // Kept leaves and children of this level.
+        for (int h = 0; h < 2; ++h) {
+            const int s = lane + 32 * h;
+            if (s >= nsel) continue;
+            const unsigned lm = h == 0 ? l0 : l1;
+            if (lm & (1u << lane)) {
+                const int rank = (h == 0) ? __popc(l0 & lt) : __popc(l0) + __popc(l1 & lt);
+                if (rank < keep) {
+                    for (int t = 0; t < 3; ++t) {
+                        S.lv[rank][2 * t] = S.xs[cur][s][t];
+                        S.lv[rank][2 * t + 1] = S.es[cur][s][t];
+                    }
+                    S.lorder[rank] = gauss_order(0.5 / rat[h]);
+                }
+            }
+            const unsigned sm = h == 0 ? m0 : m1;
+            if (sm & (1u << lane)) {
+                const int rank = (h == 0) ? __popc(m0 & lt) : __popc(m0) + __popc(m1 & lt);
+                if (rank < 15) {
+                    const double* xp = S.xs[cur][s];
+                    const double* ep = S.es[cur][s];
+                    double xm[6], em[6];
+                    for (int t = 0; t < 3; ++t) {
+                        const int t1 = (t + 1) % 3;
+                        xm[t] = xp[t];
+                        xm[t + 3] = (xp[t] + xp[t1]) / 2.0;
+                        em[t] = ep[t];
+                        em[t + 3] = (ep[t] + ep[t1]) / 2.0;
+                    }
+                    const int b = 4 * rank;
+                    for (int t = 0; t < 3; ++t) {
+                        const int t2 = (t == 0) ? 5 : t + 2;
+                        S.xs[nxt][b + t][0] = xm[t];
+                        S.xs[nxt][b + t][1] = xm[t + 3];
+                        S.xs[nxt][b + t][2] = xm[t2];
+                        S.es[nxt][b + t][0] = em[t];
+                        S.es[nxt][b + t][1] = em[t + 3];
+                        S.es[nxt][b + t][2] = em[t2];
+                    }
+                    S.xs[nxt][b + 3][0] = xm[3];
+                    S.xs[nxt][b + 3][1] = xm[4];
+                    S.xs[nxt][b + 3][2] = xm[5];
+                    S.es[nxt][b + 3][0] = em[3];
+                    S.es[nxt][b + 3][1] = em[4];
+                    S.es[nxt][b + 3][2] = em[5];
+                }
+            }
+        }
+        __syncwarp();
+        // Point offsets of the kept leaves (serial scan by lane 0: at most 60 leaves).
+        if (lane == 0) {
+            int o = 0;
+            for (int l = 0; l < keep; ++l) {
+                S.loff[l] = o;
+                o += c_tri_cnt[S.lorder[l] - 4];
+            }
+            S.loff[keep] = o;
+        }
+        __syncwarp();
+        const int npts = S.loff[keep];
+        const bool iforie = fabs(fabs(faclin) - 1.0) < 1e-10;
+        for (int f = lane; f < npts; f += 32) {
+            int lo = 0, hi = keep - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (S.loff[mid] <= f) lo = mid; else hi = mid - 1;
+            }
+            const int l = lo;
+            const int q = f - S.loff[l];
+            const int ti = c_tri_off[S.lorder[l] - 4] + q;
+            const double xi = c_tri_xi[ti], et = c_tri_eta[ti], wq = c_tri_w[ti];
+            double xio, eto, weih2;
+            if (iforie) {
+                xio = xi;
+                eto = et;
+                weih2 = wq;
+            } else {
+                const double* lv = S.lv[l];
+                const double lam = 1.0 - xi - et;
+                xio = lv[0] * lam + lv[2] * xi + lv[4] * et;
+                eto = lv[1] * lam + lv[3] * xi + lv[5] * et;
+                const double det = fabs((lv[2] - lv[0]) * (lv[5] - lv[1]) - (lv[4] - lv[0]) * (lv[3] - lv[1]));
+                weih2 = wq * det;
+            }
+            const double sf0 = 1.0 - xio - eto;
+            const double px = sf0 * V[0][0] + xio * V[1][0] + eto * V[2][0];
+            const double py = sf0 * V[0][1] + xio * V[1][1] + eto * V[2][1];
+            const double pz = sf0 * V[0][2] + xio * V[1][2] + eto * V[2][2];
+            const double dx = px - x0, dy = py - x1, dz = pz - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            point_channels(a, dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
+        }
+        total += keep;
+        __syncwarp();
+        if (total >= kMaxLeaves || nsub == 0) break;
+        nsel = min(nsub, 15) * 4;
+        cur = nxt;
+    }
+}
+
+__device__ __forceinline__ Acc warp_reduce(const Acc& a) {
+    Acc r;
+    r.gr = warp_sum(a.gr); r.gi = warp_sum(a.gi);
+    r.hr = warp_sum(a.hr); r.hi = warp_sum(a.hi);
+    r.tr = warp_sum(a.tr); r.ti = warp_sum(a.ti);
+    r.er = warp_sum(a.er); r.ei = warp_sum(a.ei);
+    return r;
+}
+
+template <bool kWithF32>
+__global__ void __launch_bounds__(32 * kNearWarps) k_near(const double* __restrict__ elem,
+                                                          int64_t n, int64_t ld,
+                                                          const int64_t* __restrict__ row_ptr,
+                                                          const int32_t* __restrict__ cols,
+                                                          int64_t nnz,
+                                                          const double* __restrict__ coef,
+                                                          double k, double2* __restrict__ A64,
+                                                          float2* __restrict__ A32, int64_t lda32,
+                                                          double2* __restrict__ near_rhs) {
+    __shared__ NearWarpSmem smem[kNearWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t p = blockIdx.x * (int64_t)kNearWarps + warp;
+    if (p >= nnz) return;
+    // Row of pair p by binary search in row_ptr.
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (row_ptr[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    const int64_t i = lo, j = cols[p];
+    Acc a;
+    near_pair_channels(a, smem[warp], elem, ld, i, j, k, k * k, lane);
+    const Acc t = warp_reduce(a);
+    if (lane == 0) {
+        const double2 v = combine(t, coef, ld, j, CF_CG);
+        A64[i * n + j] = v;
+        if (kWithF32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+        if (near_rhs) near_rhs[p] = combine(t, coef, ld, j, CF_DG);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Self kernel: one warp per element (singular_integration_with_params_mode, singular.rs:297-614).
+// ---------------------------------------------------------------------------------------------
+template <bool kWithF32>
+__global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, int64_t n,
+                                              int64_t ld, const double* __restrict__ coef,
+                                              double k, double2* __restrict__ A64,
+                                              float2* __restrict__ A32, int64_t lda32,
+                                              double2* __restrict__ self_rhs,
+                                              double2* __restrict__ diag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp;
+    if (i >= n) return;
+    const double k2 = k * k;
+    const double x0 = E(ECX, i), x1 = E(ECY, i), x2 = E(ECZ, i);
+    const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
+    const double nyx = nxx, nyy = nxy, nyz = nxz;
+    const double jac = E(EJAC, i);
+    double V[3][3];
+    for (int t = 0; t < 3; ++t)
+        for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, i);
+    // QuadratureParams::for_ka with estimate_element_size = max(sqrt(area), 1e-10).
+    const double ka = k * fmax(sqrt(E(EAREA, i)), 1e-10);
+    int ngpo1, nsub, nsec1, nsec2;
+    if (ka < 0.3) { ngpo1 = 3; nsub = 4; nsec1 = 4; nsec2 = 2; }
+    else if (ka < 1.0) { ngpo1 = 4; nsub = 5; nsec1 = 6; nsec2 = 2; }
+    else if (ka < 2.0) { ngpo1 = 5; nsub = 6; nsec1 = 8; nsec2 = 3; }
+    else { ngpo1 = 6; nsub = 7; nsec1 = 10; nsec2 = 4; }
+    const int ego = ngpo1 * (ngpo1 - 1) / 2, sgo = nsub * (nsub - 1) / 2;
+    const int n_edge = nsec1 * ngpo1, n_bulk = nsec2 * nsub * nsub;
+    const int per_edge = n_edge + n_bulk;
+    const double csi6[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+    const double eta6[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
+    Acc a;
+    double edge_r = 0.0, edge_i = 0.0;
+    for (int f = lane; f < 3 * per_edge; f += 32) {
+        const int ieg = f / per_edge, rem = f % per_edge;
+        const int ig1 = (ieg + 1) % 3, ig2 = ieg + 3;
+        if (rem < n_edge) {
+            // Regularised hypersingular edge term: ((grad G x t) . n_x) w.
+            const int isec = rem / ngpo1, ig = rem % ngpo1;
+            double dp[3], leneg = 0.0;
+            for (int c = 0; c < 3; ++c) {
+                dp[c] = V[ig1][c] - V[ieg][c];
+                leneg += dp[c] * dp[c];
+            }
+            leneg = sqrt(leneg);
+            const double to0 = dp[0] / leneg, to1 = dp[1] / leneg, to2 = dp[2] / leneg;
+            const double leneg_scaled = leneg / (2.0 * nsec1);
+            const double delsec = 2.0 / nsec1;
+            double secmid = -1.0 - delsec / 2.0;
+            for (int s = 0; s <= isec; ++s) secmid += delsec;
+            const double sga = secmid + c_gl_x[ego + ig] / nsec1;
+            const double wga = c_gl_w[ego + ig] * leneg_scaled;
+            const double dx = V[ieg][0] + dp[0] * (sga + 1.0) / 2.0 - x0;
+            const double dy = V[ieg][1] + dp[1] * (sga + 1.0) / 2.0 - x1;
+            const double dz = V[ieg][2] + dp[2] * (sga + 1.0) / 2.0 - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            double s, c;
+            sb_sincos(k * dis, &s, &c);
+            const double g_r = c * kInv4Pi * rinv, g_i = s * kInv4Pi * rinv;
+            const double f_r = -g_r * rinv - g_i * k, f_i = g_r * k - g_i * rinv;
+            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+            // (u x t) . n_x
+            const double cr = (uy * to2 - uz * to1) * nxx + (uz * to0 - ux * to2) * nxy +
+                              (ux * to1 - uy * to0) * nxz;
+            edge_r += f_r * cr * wga;
+            edge_i += f_i * cr * wga;
+        } else {
+            // Duffy sub-triangle (centroid, vertex, edge midpoint) with an nsub x nsub GL rule.
+            const int r2 = rem - n_edge;
+            const int isec = r2 / (nsub * nsub), ab = r2 % (nsub * nsub);
+            const int ia = ab / nsub, ib = ab % nsub;
+            const double aresub = 1.0 / 24.0 / nsec2;
+            double ss[3], ts[3];
+            ss[0] = ts[0] = 1.0 / 3.0;
+            if (isec == 0) {
+                ss[1] = csi6[ieg]; ss[2] = csi6[ig2]; ts[1] = eta6[ieg]; ts[2] = eta6[ig2];
+            } else {
+                ss[1] = csi6[ig2]; ss[2] = csi6[ig1]; ts[1] = eta6[ig2]; ts[2] = eta6[ig1];
+            }
+            const double sga = c_gl_x[sgo + ia], tga = c_gl_x[sgo + ib];
+            const double wei = c_gl_w[sgo + ia] * c_gl_w[sgo + ib];
+            const double sgg = 0.5 * (1.0 - sga) * ss[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ss[1] + (1.0 + tga) * ss[2]);
+            const double tgg = 0.5 * (1.0 - sga) * ts[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ts[1] + (1.0 + tga) * ts[2]);
+            const double sf0 = 1.0 - sgg - tgg;
+            const double dx = sf0 * V[0][0] + sgg * V[1][0] + tgg * V[2][0] - x0;
+            const double dy = sf0 * V[0][1] + sgg * V[1][1] + tgg * V[2][1] - x1;
+            const double dz = sf0 * V[0][2] + sgg * V[1][2] + tgg * V[2][2] - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            const double wga = wei * (1.0 + sga) * aresub * jac;
+            double s, c;
+            sb_sincos(k * dis, &s, &c);
+            const double gs = wga * kInv4Pi * rinv;
+            const double g_r = c * gs, g_i = s * gs;
+            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+            const double rny = ux * nyx + uy * nyy + uz * nyz;
+            const double rnx = -(ux * nxx + uy * nxy + uz * nxz);
+            const double b_r = -g_r * rinv - g_i * k, b_i = g_r * k - g_i * rinv;
+            a.gr += g_r; a.gi += g_i;
+            a.hr += b_r * rny; a.hi += b_i * rny;
+            a.tr += b_r * rnx; a.ti += b_i * rnx;
+            const double nd = nxx * nyx + nxy * nyy + nxz * nyz;
+            a.er += g_r * k2 * nd;
+            a.ei += g_i * k2 * nd;
+        }
+    }
+    a.er += edge_r;
+    a.ei += edge_i;
+    const Acc t = warp_reduce(a);
+    if (lane == 0) {
+        double2 v = combine(t, coef, ld, i, CF_CG);
+        v.x += coef[(int64_t)(CF_DIAG) * ld + i];
+        v.y += coef[(int64_t)(CF_DIAG + 1) * ld + i];
+        A64[i * n + i] = v;
+        if (kWithF32) A32[i * lda32 + i] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+        diag[i] = v;
+        double2 r = make_double2(coef[(int64_t)(CF_RHS) * ld + i], coef[(int64_t)(CF_RHS + 1) * ld + i]);
+        if (self_rhs) {
+            const double2 c = combine(t, coef, ld, i, CF_DG);
+            r.x += c.x;
+            r.y += c.y;
+        }
+        self_rhs ? (void)(self_rhs[i] = r) : (void)0;
+    }
+}
+
+// rhs_i = free term + self + far tiles + near pairs (BC-induced RHS of tbem.rs:1421-1444).
+__global__ void k_rhs_reduce(int64_t n, int64_t ld, const double* __restrict__ coef,
+                             const double2* __restrict__ self_rhs,
+                             const double2* __restrict__ far_part, int64_t n_tiles,
+                             const int64_t* __restrict__ row_ptr,
+                             const double2* __restrict__ near_rhs, double2* __restrict__ rhs) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!self_rhs) {
+        rhs[i] = make_double2(coef[(int64_t)CF_RHS * ld + i], coef[(int64_t)(CF_RHS + 1) * ld + i]);
+        return;
+    }
+    double2 r = self_rhs[i];
+    for (int64_t t = 0; t < n_tiles; ++t) r = cadd(r, far_part[i * n_tiles + t]);
+    for (int64_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) r = cadd(r, near_rhs[p]);
+    rhs[i] = r;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Incident plane-wave RHS (incident.rs:216-245, 315-331, 807-833).
+// ---------------------------------------------------------------------------------------------
+__global__ void k_plane_wave(const double* __restrict__ elem, int64_t n, int64_t ld,
+                             const double* __restrict__ dirs, const double2* __restrict__ amps,
+                             int64_t r, double k, double hf, double tau, double2 beta,
+                             double2* __restrict__ rhs, int accumulate) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n * r) return;
+    const int64_t i = t / r, q = t % r;
+    const double d0 = dirs[3 * q], d1 = dirs[3 * q + 1], d2 = dirs[3 * q + 2];
+    const double2 A = amps ? amps[q] : make_double2(1.0, 0.0);
+    const double kdx = hf * k * (d0 * E(ECX, i) + d1 * E(ECY, i) + d2 * E(ECZ, i));
+    const double kdn = hf * k * (d0 * E(ENX, i) + d1 * E(ENY, i) + d2 * E(ENZ, i));
+    double s, c;
+    sb_sincos(kdx, &s, &c);
+    const double2 p = cmul(A, make_double2(c, s));
+    const double2 dpdn = make_double2(-kdn * p.y, kdn * p.x);  // i kdn p
+    const double2 bt = cscale(beta, tau);
+    const double2 v = make_double2(-(p.x + bt.x * dpdn.x - bt.y * dpdn.y),
+                                   -(p.y + bt.x * dpdn.y + bt.y * dpdn.x));
+    if (accumulate) {
+        rhs[t] = cadd(rhs[t], v);
+    } else {
+        rhs[t] = v;
+    }
+}
+
+__global__ void k_sincos(const double* __restrict__ x, int64_t n, double* __restrict__ s,
+                         double* __restrict__ c) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) sb_sincos(x[i], s + i, c + i);
+}
+
+#undef E
+
+// ---------------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------------
+static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, int64_t n_tris,
+                  int device) {
+    SB_REQUIRE(nodes && tris, SB_ERR_INVALID_ARGUMENT, "mesh: null nodes or connectivity");
+    SB_REQUIRE(n_nodes >= 3 && n_tris >= 1, SB_ERR_INVALID_ARGUMENT, "mesh: empty mesh");
+    SB_REQUIRE(n_tris < (int64_t(1) << 31), SB_ERR_INVALID_ARGUMENT, "mesh: too many elements");
+    for (int64_t a = 0; a < 3 * n_nodes; ++a)
+        SB_REQUIRE(std::isfinite(nodes[a]), SB_ERR_INVALID_ARGUMENT, "mesh: non-finite node coordinate");
+    for (int64_t a = 0; a < 3 * n_tris; ++a)
+        SB_REQUIRE(tris[a] < static_cast<uint64_t>(n_nodes), SB_ERR_INVALID_ARGUMENT,
+                   "mesh: connectivity index out of range");
+    std::vector<double> c(3 * n_tris), nr(3 * n_tris), ar(n_tris);
+    host_element_geometry(nodes, tris, n_tris, c.data(), nr.data(), ar.data());
+    for (int64_t e = 0; e < n_tris; ++e)
+        SB_REQUIRE(ar[e] > 1e-300 && std::isfinite(ar[e]), SB_ERR_UNSUPPORTED_ELEMENT,
+                   "mesh: degenerate triangle " + std::to_string(e));
+    int ndev = 0;
+    SB_CUDA(cudaGetDeviceCount(&ndev));
+    SB_REQUIRE(device >= 0 && device < ndev, SB_ERR_CUDA, "mesh: CUDA device not available");
+    SB_CUDA(cudaSetDevice(device));
+    ensure_tables(device);
+    maybe_inject(SB_INJECT_ALLOC);
+    Mesh* m = new Mesh();
+    try {
+        m->device = device;
+        m->n = n_tris;
+        m->n_nodes = n_nodes;
+        m->n_tiles = cdiv(n_tris, kFarTile);
+        m->ld = m->n_tiles * kFarTile;
+        m->h_nodes.assign(nodes, nodes + 3 * n_nodes);
+        m->h_tris.assign(tris, tris + 3 * n_tris);
+        m->nodes.alloc(sizeof(double) * 3 * n_nodes);
+        m->tris.alloc(sizeof(uint32_t) * 3 * n_tris);
+        m->elem.alloc(sizeof(double) * EFIELDS * m->ld);
+        m->qp.alloc(sizeof(double) * kQpTileDoubles * m->n_tiles);
+        SB_CUDA(cudaMemcpy(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes, cudaMemcpyHostToDevice));
+        SB_CUDA(cudaMemcpy(m->tris.p, tris, sizeof(uint32_t) * 3 * n_tris, cudaMemcpyHostToDevice));
+        const int64_t nb = cdiv(m->ld, 256);
+        k_element_geometry<<<nb, 256>>>(m->nodes.as<double>(), m->tris.as<uint32_t>(), m->n, m->ld, m->elem.as<double>()); count_launch();
+        SB_CUDA(cudaGetLastError());
+        k_far_points<<<nb, 256>>>(m->elem.as<double>(), m->n, m->ld, m->qp.as<double>()); count_launch();
+        SB_CUDA(cudaGetLastError());
+        // Near-pair CSR.
+        DevBuf counts;
+        counts.alloc(sizeof(int64_t) * (m->n + 1));
+        const int64_t nblk = cdiv(m->n, kNearRows);
+        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 0, counts.as<int64_t>(), nullptr, nullptr); count_launch();
+        SB_CUDA(cudaGetLastError());
+        std::vector<int64_t> cnt(m->n), ptr(m->n + 1);
+        SB_CUDA(cudaMemcpy(cnt.data(), counts.p, sizeof(int64_t) * m->n, cudaMemcpyDeviceToHost));
+        ptr[0] = 0;
+        for (int64_t i = 0; i < m->n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
+        m->nnz = ptr[m->n];
+        m->near_ptr.alloc(sizeof(int64_t) * (m->n + 1));
+        SB_CUDA(cudaMemcpy(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1), cudaMemcpyHostToDevice));
+        m->near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m->nnz, 1));
+        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 1, nullptr, m->near_ptr.as<int64_t>(), m->near_col.as<int32_t>()); count_launch();
+        SB_CUDA(cudaGetLastError());
+        m->h_elem.resize(static_cast<size_t>(EFIELDS) * m->ld);
+        SB_CUDA(cudaMemcpy(m->h_elem.data(), m->elem.p, sizeof(double) * m->h_elem.size(), cudaMemcpyDeviceToHost));
+        SB_CUDA(cudaDeviceSynchronize());
+        m->h_bc_kind.assign(m->n, SB_BC_VELOCITY);
+        m->h_bc_value.assign(2 * m->n, 0.0);
+        m->h_adm.assign(2 * m->n, 0.0);
+        m->h_has_adm.assign(m->n, 0);
+    } catch (...) {
+        delete m;
+        throw;
+    }
+    return m;
+}
+
+void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const uint8_t* has_adm,
+                 const sb_complex* adm) {
+    for (int64_t e = 0; e < m.n; ++e) {
+        const int k = kind ? kind[e] : SB_BC_VELOCITY;
+        SB_REQUIRE(k == SB_BC_VELOCITY || k == SB_BC_PRESSURE, SB_ERR_INVALID_ARGUMENT,
+                   "bc: kind must be velocity (0) or pressure (1)");
+        if (value) SB_REQUIRE(std::isfinite(value[e].re) && std::isfinite(value[e].im),
+                              SB_ERR_INVALID_ARGUMENT, "bc: non-finite value");
+        if (adm && has_adm && has_adm[e])
+            SB_REQUIRE(std::isfinite(adm[e].re) && std::isfinite(adm[e].im),
+                       SB_ERR_INVALID_ARGUMENT, "bc: non-finite admittance");
+    }
+    SB_CUDA(cudaSetDevice(m.device));
+    m.any_bc_value = false;
+    m.any_adm = false;
+    for (int64_t e = 0; e < m.n; ++e) {
+        m.h_bc_kind[e] = kind ? kind[e] : SB_BC_VELOCITY;
+        m.h_bc_value[2 * e] = value ? value[e].re : 0.0;
+        m.h_bc_value[2 * e + 1] = value ? value[e].im : 0.0;
+        m.h_has_adm[e] = (has_adm && has_adm[e]) ? 1 : 0;
+        m.h_adm[2 * e] = (adm && m.h_has_adm[e]) ? adm[e].re : 0.0;
+        m.h_adm[2 * e + 1] = (adm && m.h_has_adm[e]) ? adm[e].im : 0.0;
+        if (std::hypot(m.h_bc_value[2 * e], m.h_bc_value[2 * e + 1]) > 1e-15) m.any_bc_value = true;
+        if (m.h_has_adm[e]) m.any_adm = true;
+    }
+    if (!m.bc_kind.p) {
+        m.bc_kind.alloc(sizeof(int32_t) * m.n);
+        m.bc_value.alloc(sizeof(double2) * m.n);
+        m.has_adm.alloc(m.n);
+        m.adm.alloc(sizeof(double2) * m.n);
+    }
+    SB_CUDA(cudaMemcpy(m.bc_kind.p, m.h_bc_kind.data(), sizeof(int32_t) * m.n, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemcpy(m.bc_value.p, m.h_bc_value.data(), sizeof(double2) * m.n, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemcpy(m.has_adm.p, m.h_has_adm.data(), m.n, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemcpy(m.adm.p, m.h_adm.data(), sizeof(double2) * m.n, cudaMemcpyHostToDevice));
+}
+
+void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
+    Mesh& m = *op.mesh;
+    SB_CUDA(cudaSetDevice(m.device));
+    maybe_inject(SB_INJECT_LAUNCH);
+    const int64_t n = m.n, ld = m.ld;
+    const bool with_rhs = m.any_bc_value;
+    if (!op.coef.p) op.coef.alloc(sizeof(double) * CF_FIELDS * ld);
+    if (with_rhs) {
+        if (!op.far_part.p) op.far_part.alloc(sizeof(double2) * n * m.n_tiles);
+        if (!op.near_rhs.p) op.near_rhs.alloc(sizeof(double2) * std::max<int64_t>(m.nnz, 1));
+        if (!op.self_rhs.p) op.self_rhs.alloc(sizeof(double2) * n);
+    }
+    if (!op.rhs.p) op.rhs.alloc(sizeof(double2) * n);
+    if (!op.diag.p) op.diag.alloc(sizeof(double2) * n);
+    DevBuf status;
+    status.alloc(sizeof(int));
+    SB_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int), op.stream));
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, op.stream));
+    const double2 beta = make_double2(beta_re, beta_im);
+    k_coefficients<<<cdiv(ld, 256), 256, 0, op.stream>>>(
+        n, ld, m.bc_kind.as<int32_t>(), m.bc_value.as<double2>(), m.has_adm.as<uint8_t>(),
+        m.adm.as<double2>(), ph.tau, ph.pressure_factor, beta, op.coef.as<double>()); count_launch();
+    SB_CUDA(cudaGetLastError());
+    const double k = ph.harmonic_factor * ph.wave_number;
+    const bool f32 = op.precision == SB_PRECISION_FP64_FP32;
+    double2* A64 = op.A64.as<double2>();
+    float2* A32 = f32 ? op.A32.as<float2>() : nullptr;
+    {
+        ProfScope prof(SB_PROF_FAR, op.stream);
+        dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFarRows)));
+        const size_t sm = sizeof(double) * (kQpTileDoubles + kFarRows * 6);
+        auto launch = [&](auto kern) {
+            SB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+            kern<<<grid, kFarTile, sm, op.stream>>>(m.qp.as<double>(), m.elem.as<double>(), n, ld,
+                                                    op.coef.as<double>(), k, A64, A32, op.lda32,
+                                                    with_rhs ? op.far_part.as<double2>() : nullptr,
+                                                    m.n_tiles, status.as<int>()); count_launch();
+        };
+        if (with_rhs) {
+            if (f32) launch(k_far<true, true>); else launch(k_far<true, false>);
+        } else {
+            if (f32) launch(k_far<false, true>); else launch(k_far<false, false>);
+        }
+        SB_CUDA(cudaGetLastError());
+    }
+    if (m.nnz > 0) {
+        ProfScope prof(SB_PROF_NEAR, op.stream);
+        const int64_t nb = cdiv(m.nnz, kNearWarps);
+        auto kern = f32 ? k_near<true> : k_near<false>;
+        kern<<<nb, 32 * kNearWarps, 0, op.stream>>>(m.elem.as<double>(), n, ld, m.near_ptr.as<int64_t>(),
+                                                     m.near_col.as<int32_t>(), m.nnz, op.coef.as<double>(), k,
+                                                     A64, A32, op.lda32, with_rhs ? op.near_rhs.as<double2>() : nullptr); count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    {
+        ProfScope prof(SB_PROF_SELF, op.stream);
+        auto kern = f32 ? k_self<true> : k_self<false>;
+        kern<<<cdiv(n, 4), 128, 0, op.stream>>>(m.elem.as<double>(), n, ld, op.coef.as<double>(), k, A64, A32, op.lda32,
+                                                 with_rhs ? op.self_rhs.as<double2>() : nullptr,
+                                                 op.diag.as<double2>()); count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    k_rhs_reduce<<<cdiv(n, 256), 256, 0, op.stream>>>(n, ld, op.coef.as<double>(),
+                                                       with_rhs ? op.self_rhs.as<double2>() : nullptr,
+                                                       with_rhs ? op.far_part.as<double2>() : nullptr,
+                                                       m.n_tiles, m.near_ptr.as<int64_t>(),
+                                                       with_rhs ? op.near_rhs.as<double2>() : nullptr,
+                                                       op.rhs.as<double2>()); count_launch();
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaEventRecord(e1, op.stream));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    op.last_assembly_ms = ms;
+    int st = 0;
+    SB_CUDA(cudaMemcpy(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    SB_REQUIRE(st == 0, SB_ERR_DEVICE_CHECK, "assembly: shared-memory staging did not complete");
+    op.phys = ph;
+    op.beta_re = beta_re;
+    op.beta_im = beta_im;
+}
+
+void incident_plane_wave(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im,
+                         const double* dirs_host, const double* amps_host, int64_t r,
+                         double2* rhs_dev, cudaStream_t s, bool accumulate) {
+    SB_CUDA(cudaSetDevice(m.device));
+    DevBuf dd, da;
+    dd.alloc(sizeof(double) * 3 * r);
+    SB_CUDA(cudaMemcpyAsync(dd.p, dirs_host, sizeof(double) * 3 * r, cudaMemcpyHostToDevice, s));
+    if (amps_host) {
+        da.alloc(sizeof(double2) * r);
+        SB_CUDA(cudaMemcpyAsync(da.p, amps_host, sizeof(double2) * r, cudaMemcpyHostToDevice, s));
+    }
+    const int64_t tot = m.n * r;
+    ProfScope prof(SB_PROF_OTHER, s);
+    k_plane_wave<<<cdiv(tot, 256), 256, 0, s>>>(m.elem.as<double>(), m.n, m.ld, dd.as<double>(),
+                                                 amps_host ? da.as<double2>() : nullptr, r,
+                                                 ph.wave_number, ph.harmonic_factor, ph.tau,
+                                                 make_double2(beta_re, beta_im), rhs_dev, accumulate ? 1 : 0); count_launch();
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(s));
+}
+
+void device_sincos(int device, const double* x, int64_t n, double* s, double* c) {
+    SB_CUDA(cudaSetDevice(device));
+    DevBuf dx, ds, dc;
+    dx.alloc(sizeof(double) * n);
+    ds.alloc(sizeof(double) * n);
+    dc.alloc(sizeof(double) * n);
+    SB_CUDA(cudaMemcpy(dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice));
+    k_sincos<<<cdiv(n, 256), 256>>>(dx.as<double>(), n, ds.as<double>(), dc.as<double>()); count_launch();
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaMemcpy(s, ds.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    SB_CUDA(cudaMemcpy(c, dc.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+}
+
+// compute_element_geometry (generators.rs:771-830) on the host, for input validation.
+void host_element_geometry(const double* nodes, const uint32_t* tris, int64_t n, double* c,
+                           double* nrm, double* area) {
+    for (int64_t e = 0; e < n; ++e) {
+        const uint32_t* t = tris + 3 * e;
+        for (int j = 0; j < 3; ++j)
+            c[3 * e + j] = (((0.0 + nodes[3 * t[0] + j]) + nodes[3 * t[1] + j]) + nodes[3 * t[2] + j]) / 3.0;
+        double a1[3], a2[3];
+        for (int j = 0; j < 3; ++j) {
+            a1[j] = nodes[3 * t[1] + j] - nodes[3 * t[0] + j];
+            a2[j] = nodes[3 * t[2] + j] - nodes[3 * t[0] + j];
+        }
+        const double c0 = a1[1] * a2[2] - a1[2] * a2[1];
+        const double c1 = a1[2] * a2[0] - a1[0] * a2[2];
+        const double c2 = a1[0] * a2[1] - a1[1] * a2[0];
+        const double len = std::sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+        area[e] = len / 2.0;
+        if (len > 1e-15) {
+            nrm[3 * e] = c0 / len;
+            nrm[3 * e + 1] = c1 / len;
+            nrm[3 * e + 2] = c2 / len;
+        } else {
+            nrm[3 * e] = nrm[3 * e + 1] = nrm[3 * e + 2] = 0.0;
+        }
+    }
+}
+
+}  // namespace sb

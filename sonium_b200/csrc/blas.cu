@@ -1,0 +1,532 @@
+// Dense complex matvec and Arnoldi building blocks on sm_100a.
+//
+// Reference: DenseMatrix::matvec_into -> gemv_c64 (crates/sonium-solvers/crates/sonium-solvers-core/
+// src/dense.rs:416-427, traits.rs:1430-1452) on the CPU and cublasZgemv / cublasCgemv
+// (crates/sonium-compute/src/cuda/cublas_blas23.rs:126,165) on the GPU; the Arnoldi helpers follow
+// batched_dots_flat_into / batched_project_flat / fused_basis_update_flat (crates/sonium-solvers/
+// crates/sonium-solvers-iterative/src/cgs_orth.rs:180-300) and the fused CUDA multi-dot / axpy
+// kernels (crates/sonium-compute/src/cuda/kernels/multi_dot_kernels.cu:173-306).
+//
+// The matvec is HBM-bound (16 N^2 bytes per complex128 product): each CTA owns a few rows and
+// streams them with 128-bit evict-first loads, several loads in flight per thread, reusing each
+// x element across its rows.
+
+#include "sb_blas.cuh"
+#include "sb_device.cuh"
+#include "sb_internal.cuh"
+#include "sb_profile.cuh"
+
+namespace sb {
+
+static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+__device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
+__device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
+
+// Block-wide sum of NV doubles held per thread; result valid in thread 0.
+template <int NV, int THREADS>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int t = 0; t < NV; ++t) v[t] = warp_sum(v[t]);
+    if (lane == 0) {
+#pragma unroll
+        for (int t = 0; t < NV; ++t) red[warp * NV + t] = v[t];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int t = 0; t < NV; ++t) {
+            double s = 0.0;
+            for (int w = 0; w < THREADS / 32; ++w) s += red[w * NV + t];
+            v[t] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// y = A x (complex128), or y = b - A x with per-CTA partial ||y||^2 when b != null.
+// ---------------------------------------------------------------------------------------------
+template <int ROWS, int THREADS, int UNROLL>
+__global__ void __launch_bounds__(THREADS) k_gemv_n_c128(const double2* __restrict__ A, int64_t n,
+                                                         const double2* __restrict__ x,
+                                                         double2* __restrict__ y,
+                                                         const double2* __restrict__ b,
+                                                         double* __restrict__ part) {
+    __shared__ double red[(THREADS / 32) * 2 * ROWS];
+    const int64_t row0 = blockIdx.x * (int64_t)ROWS;
+    const int nr = static_cast<int>((n - row0) < ROWS ? (n - row0) : ROWS);
+    double acc[2 * ROWS];
+#pragma unroll
+    for (int r = 0; r < 2 * ROWS; ++r) acc[r] = 0.0;
+    const double2* Ar = A + row0 * n;
+    int64_t c = threadIdx.x;
+    for (; c + (UNROLL - 1) * THREADS < n; c += UNROLL * THREADS) {
+        double2 xv[UNROLL];
+        double2 av[UNROLL][ROWS];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            xv[u] = __ldg(x + c + u * THREADS);
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r)
+                av[u][r] = (r < nr) ? ld_stream(Ar + r * n + c + u * THREADS) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u)
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+                acc[2 * r] = fma(av[u][r].x, xv[u].x, fma(-av[u][r].y, xv[u].y, acc[2 * r]));
+                acc[2 * r + 1] = fma(av[u][r].x, xv[u].y, fma(av[u][r].y, xv[u].x, acc[2 * r + 1]));
+            }
+    }
+    for (; c < n; c += THREADS) {
+        const double2 xv = __ldg(x + c);
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            if (r < nr) {
+                const double2 a = ld_stream(Ar + r * n + c);
+                acc[2 * r] = fma(a.x, xv.x, fma(-a.y, xv.y, acc[2 * r]));
+                acc[2 * r + 1] = fma(a.x, xv.y, fma(a.y, xv.x, acc[2 * r + 1]));
+            }
+        }
+    }
+    block_sum<2 * ROWS, THREADS>(acc, red);
+    if (threadIdx.x == 0) {
+        double nrm = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            double2 v = make_double2(acc[2 * r], acc[2 * r + 1]);
+            if (b) {
+                const double2 bb = b[row0 + r];
+                v = make_double2(bb.x - v.x, bb.y - v.y);
+                nrm += v.x * v.x + v.y * v.y;
+            }
+            y[row0 + r] = v;
+        }
+        if (part) part[blockIdx.x] = nrm;
+    }
+}
+
+// y = A^T x or A^H x (complex128): column-per-thread over row chunks, then a chunk reduction.
+constexpr int kTRows = 256;
+template <bool CONJ>
+__global__ void __launch_bounds__(256) k_gemv_t_c128(const double2* __restrict__ A, int64_t n,
+                                                     const double2* __restrict__ x,
+                                                     double2* __restrict__ part) {
+    const int64_t j = blockIdx.x * 256LL + threadIdx.x;
+    const int64_t r0 = blockIdx.y * (int64_t)kTRows;
+    const int64_t r1 = (r0 + kTRows < n) ? r0 + kTRows : n;
+    if (j >= n) return;
+    double ar = 0.0, ai = 0.0;
+    for (int64_t i = r0; i < r1; ++i) {
+        const double2 a = ld_stream(A + i * n + j);
+        const double2 xv = __ldg(x + i);
+        const double ay = CONJ ? -a.y : a.y;
+        ar = fma(a.x, xv.x, fma(-ay, xv.y, ar));
+        ai = fma(a.x, xv.y, fma(ay, xv.x, ai));
+    }
+    part[blockIdx.y * n + j] = make_double2(ar, ai);
+}
+
+__global__ void k_sum_chunks(const double2* __restrict__ part, int64_t n, int64_t chunks,
+                             double2* __restrict__ y) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double2 s = make_double2(0.0, 0.0);
+    for (int64_t c = 0; c < chunks; ++c) s = cadd(s, part[c * n + j]);
+    y[j] = s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Complex64 matrix: FP32 vectors with FP32 accumulation, or FP64 vectors with FP64 accumulation.
+// ---------------------------------------------------------------------------------------------
+template <int ROWS, int THREADS, int UNROLL, bool X64>
+__global__ void __launch_bounds__(THREADS) k_gemv_n_c64(const float2* __restrict__ A, int64_t n,
+                                                        int64_t lda,
+                                                        const void* __restrict__ xv_,
+                                                        void* __restrict__ yv_,
+                                                        const void* __restrict__ bv_,
+                                                        double* __restrict__ part) {
+    using Acc = typename std::conditional<X64, double, float>::type;
+    __shared__ double red[(THREADS / 32) * 2 * ROWS];
+    const int64_t row0 = blockIdx.x * (int64_t)ROWS;
+    const int nr = static_cast<int>((n - row0) < ROWS ? (n - row0) : ROWS);
+    Acc acc[2 * ROWS];
+#pragma unroll
+    for (int r = 0; r < 2 * ROWS; ++r) acc[r] = 0;
+    const int64_t n2 = n >> 1;    // float4 = two complex64 entries
+    const int64_t ld2 = lda >> 1;  // lda is even, so every row starts 16-byte aligned
+    const float4* A4 = reinterpret_cast<const float4*>(A + row0 * lda);
+    int64_t c = threadIdx.x;
+    for (; c + (UNROLL - 1) * THREADS < n2; c += UNROLL * THREADS) {
+        Acc xr[UNROLL][4];
+        float4 av[UNROLL][ROWS];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            const int64_t cc = c + u * THREADS;
+            if (X64) {
+                const double2* x = static_cast<const double2*>(xv_);
+                const double2 p = __ldg(x + 2 * cc), q = __ldg(x + 2 * cc + 1);
+                xr[u][0] = p.x; xr[u][1] = p.y; xr[u][2] = q.x; xr[u][3] = q.y;
+            } else {
+                const float4 p = __ldg(static_cast<const float4*>(xv_) + cc);
+                xr[u][0] = p.x; xr[u][1] = p.y; xr[u][2] = p.z; xr[u][3] = p.w;
+            }
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r)
+                av[u][r] = (r < nr) ? ld_stream(A4 + r * ld2 + cc) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u)
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+                const Acc a0 = av[u][r].x, a1 = av[u][r].y, a2 = av[u][r].z, a3 = av[u][r].w;
+                acc[2 * r] = fma(a0, xr[u][0], fma(-a1, xr[u][1], acc[2 * r]));
+                acc[2 * r + 1] = fma(a0, xr[u][1], fma(a1, xr[u][0], acc[2 * r + 1]));
+                acc[2 * r] = fma(a2, xr[u][2], fma(-a3, xr[u][3], acc[2 * r]));
+                acc[2 * r + 1] = fma(a2, xr[u][3], fma(a3, xr[u][2], acc[2 * r + 1]));
+            }
+    }
+    for (; c < n2; c += THREADS) {
+        Acc x0r, x0i, x1r, x1i;
+        if (X64) {
+            const double2* x = static_cast<const double2*>(xv_);
+            const double2 p = x[2 * c], q = x[2 * c + 1];
+            x0r = p.x; x0i = p.y; x1r = q.x; x1i = q.y;
+        } else {
+            const float4 p = static_cast<const float4*>(xv_)[c];
+            x0r = p.x; x0i = p.y; x1r = p.z; x1i = p.w;
+        }
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            if (r < nr) {
+                const float4 a = ld_stream(A4 + r * ld2 + c);
+                acc[2 * r] = fma((Acc)a.x, x0r, fma(-(Acc)a.y, x0i, acc[2 * r]));
+                acc[2 * r + 1] = fma((Acc)a.x, x0i, fma((Acc)a.y, x0r, acc[2 * r + 1]));
+                acc[2 * r] = fma((Acc)a.z, x1r, fma(-(Acc)a.w, x1i, acc[2 * r]));
+                acc[2 * r + 1] = fma((Acc)a.z, x1i, fma((Acc)a.w, x1r, acc[2 * r + 1]));
+            }
+        }
+    }
+    // Odd n: the last column.
+    if ((n & 1) && threadIdx.x == 0) {
+        const int64_t cl = n - 1;
+        Acc xr0, xi0;
+        if (X64) {
+            const double2 p = static_cast<const double2*>(xv_)[cl];
+            xr0 = p.x; xi0 = p.y;
+        } else {
+            const float2 p = static_cast<const float2*>(xv_)[cl];
+            xr0 = p.x; xi0 = p.y;
+        }
+        for (int r = 0; r < nr; ++r) {
+            const float2 a = A[(row0 + r) * lda + cl];
+            acc[2 * r] = fma((Acc)a.x, xr0, fma(-(Acc)a.y, xi0, acc[2 * r]));
+            acc[2 * r + 1] = fma((Acc)a.x, xi0, fma((Acc)a.y, xr0, acc[2 * r + 1]));
+        }
+    }
+    // Per-thread partial sums (FP32 for the FP32 product) are combined across the block in FP64.
+    double accd[2 * ROWS];
+#pragma unroll
+    for (int r = 0; r < 2 * ROWS; ++r) accd[r] = acc[r];
+    block_sum<2 * ROWS, THREADS>(accd, red);
+    if (threadIdx.x == 0) {
+        double nrm = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            double vr = accd[2 * r], vi = accd[2 * r + 1];
+            if (bv_) {
+                if (X64) {
+                    const double2 bb = static_cast<const double2*>(bv_)[row0 + r];
+                    vr = bb.x - vr;
+                    vi = bb.y - vi;
+                } else {
+                    const float2 bb = static_cast<const float2*>(bv_)[row0 + r];
+                    vr = static_cast<double>(bb.x - static_cast<float>(vr));
+                    vi = static_cast<double>(bb.y - static_cast<float>(vi));
+                }
+                nrm += vr * vr + vi * vi;
+            }
+            if (X64) static_cast<double2*>(yv_)[row0 + r] = make_double2(vr, vi);
+            else static_cast<float2*>(yv_)[row0 + r] = make_float2((float)vr, (float)vi);
+        }
+        if (part) part[blockIdx.x] = nrm;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Arnoldi helpers, templated on the vector element (double2 / float2); reductions in FP64.
+// ---------------------------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ double2 to_d(T v) {
+    return make_double2(static_cast<double>(v.x), static_cast<double>(v.y));
+}
+
+constexpr int kDotRows = 256;
+constexpr int kDotVecs = 8;
+
+// part[(chunk * (k + 1)) + i] = sum over the chunk of conj(V_i) w  (i < k), and |w|^2 at i = k.
+template <class T>
+__global__ void __launch_bounds__(kDotRows) k_dots(const T* __restrict__ V, int64_t ldv, int k,
+                                                   const T* __restrict__ w, int64_t n,
+                                                   double2* __restrict__ part) {
+    __shared__ double red[(kDotRows / 32) * 2 * kDotVecs];
+    const int64_t r = blockIdx.x * (int64_t)kDotRows + threadIdx.x;
+    const int i0 = blockIdx.y * kDotVecs;
+    double acc[2 * kDotVecs];
+#pragma unroll
+    for (int t = 0; t < 2 * kDotVecs; ++t) acc[t] = 0.0;
+    if (r < n) {
+        const double2 wv = to_d(w[r]);
+#pragma unroll
+        for (int t = 0; t < kDotVecs; ++t) {
+            const int i = i0 + t;
+            if (i < k) {
+                const double2 v = to_d(V[i * ldv + r]);
+                acc[2 * t] = v.x * wv.x + v.y * wv.y;
+                acc[2 * t + 1] = v.x * wv.y - v.y * wv.x;
+            } else if (i == k) {
+                acc[2 * t] = wv.x * wv.x + wv.y * wv.y;
+            }
+        }
+    }
+    block_sum<2 * kDotVecs, kDotRows>(acc, red);
+    if (threadIdx.x == 0) {
+        for (int t = 0; t < kDotVecs; ++t) {
+            const int i = i0 + t;
+            if (i <= k) part[blockIdx.x * (int64_t)(k + 1) + i] = make_double2(acc[2 * t], acc[2 * t + 1]);
+        }
+    }
+}
+
+// out[i] = sum over chunks of part[c][i], i <= k (one warp per output).
+__global__ void k_reduce_part(const double2* __restrict__ part, int64_t chunks, int kp1,
+                              double2* __restrict__ out) {
+    const int i = blockIdx.x;
+    double sr = 0.0, si = 0.0;
+    for (int64_t c = threadIdx.x; c < chunks; c += 32) {
+        const double2 v = part[c * kp1 + i];
+        sr += v.x;
+        si += v.y;
+    }
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    if (threadIdx.x == 0) out[i] = make_double2(sr, si);
+}
+
+// w -= sum_i coeff[i] V_i, and a per-CTA partial of |w|^2.
+template <class T>
+__global__ void __launch_bounds__(256) k_project(const T* __restrict__ V, int64_t ldv, int k,
+                                                 const double2* __restrict__ coeff,
+                                                 T* __restrict__ w, int64_t n,
+                                                 double* __restrict__ part) {
+    __shared__ double2 sc[128];
+    __shared__ double red[8];
+    for (int t = threadIdx.x; t < k; t += blockDim.x) sc[t] = coeff[t];
+    __syncthreads();
+    const int64_t r = blockIdx.x * 256LL + threadIdx.x;
+    double nr2[1] = {0.0};
+    if (r < n) {
+        double2 acc = to_d(w[r]);
+        int i = 0;
+        for (; i + 4 <= k; i += 4) {
+            double2 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = to_d(V[(i + u) * ldv + r]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                acc.x -= sc[i + u].x * v[u].x - sc[i + u].y * v[u].y;
+                acc.y -= sc[i + u].x * v[u].y + sc[i + u].y * v[u].x;
+            }
+        }
+        for (; i < k; ++i) {
+            const double2 v = to_d(V[i * ldv + r]);
+            acc.x -= sc[i].x * v.x - sc[i].y * v.y;
+            acc.y -= sc[i].x * v.y + sc[i].y * v.x;
+        }
+        T o;
+        o.x = acc.x;
+        o.y = acc.y;
+        w[r] = o;
+        const double2 ad = to_d(o);
+        nr2[0] = ad.x * ad.x + ad.y * ad.y;
+    }
+    block_sum<1, 256>(nr2, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = nr2[0];
+}
+
+__global__ void k_sum_real(const double* __restrict__ part, int64_t m, double* __restrict__ out) {
+    double s = 0.0;
+    for (int64_t c = threadIdx.x; c < m; c += 32) s += part[c];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// y = alpha * x (alpha real), with type conversion.
+template <class TI, class TO>
+__global__ void k_scale(const TI* __restrict__ x, double alpha, TO* __restrict__ y, int64_t n) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    TO o;
+    o.x = static_cast<double>(x[r].x) * alpha;
+    o.y = static_cast<double>(x[r].y) * alpha;
+    y[r] = o;
+}
+
+// x += sum_i y_i V_i (y on device), x of type TX, V of type T; optional scale of the update.
+template <class T, class TX>
+__global__ void k_update(const T* __restrict__ V, int64_t ldv, int k, const double2* __restrict__ yc,
+                         double alpha, TX* __restrict__ x, int64_t n) {
+    __shared__ double2 sc[128];
+    for (int t = threadIdx.x; t < k; t += blockDim.x) sc[t] = yc[t];
+    __syncthreads();
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double sr = 0.0, si = 0.0;
+    for (int i = 0; i < k; ++i) {
+        const double2 v = to_d(V[i * ldv + r]);
+        sr += sc[i].x * v.x - sc[i].y * v.y;
+        si += sc[i].x * v.y + sc[i].y * v.x;
+    }
+    TX o = x[r];
+    o.x = static_cast<double>(o.x) + alpha * sr;
+    o.y = static_cast<double>(o.y) + alpha * si;
+    x[r] = o;
+}
+
+// y = diag^-1 x (Jacobi), complex division with the FP64 diagonal.
+template <class T>
+__global__ void k_jacobi(const double2* __restrict__ d, const T* __restrict__ x, T* __restrict__ y,
+                         int64_t n) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const double2 a = d[r];
+    const double2 v = to_d(x[r]);
+    const double den = a.x * a.x + a.y * a.y;
+    T o;
+    o.x = (v.x * a.x + v.y * a.y) / den;
+    o.y = (v.y * a.x - v.x * a.y) / den;
+    y[r] = o;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------------------------
+constexpr int kGemvRows = 4;
+constexpr int kGemvThreads = 256;
+constexpr int kGemvUnroll = 2;
+
+void gemv_c128(const double2* A, int64_t n, const double2* x, double2* y, Trans t,
+               cudaStream_t s, DevBuf& scratch) {
+    ProfScope prof(SB_PROF_GEMV64, s);
+    if (t == Trans::N) {
+        k_gemv_n_c128<kGemvRows, kGemvThreads, kGemvUnroll>
+            <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, y, nullptr, nullptr); count_launch();
+        SB_CUDA(cudaGetLastError());
+        return;
+    }
+    const int64_t chunks = cdiv(n, kTRows);
+    const size_t need = sizeof(double2) * chunks * n;
+    if (scratch.bytes < need) {
+        scratch.release();
+        scratch.alloc(need);
+    }
+    dim3 grid(static_cast<unsigned>(cdiv(n, 256)), static_cast<unsigned>(chunks));
+    if (t == Trans::T)
+        k_gemv_t_c128<false><<<grid, 256, 0, s>>>(A, n, x, scratch.as<double2>());
+    else
+        k_gemv_t_c128<true><<<grid, 256, 0, s>>>(A, n, x, scratch.as<double2>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    k_sum_chunks<<<cdiv(n, 256), 256, 0, s>>>(scratch.as<double2>(), n, chunks, y); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+void gemv_residual_c128(const double2* A, int64_t n, const double2* x, const double2* b,
+                        double2* r, double* part, cudaStream_t s) {
+    ProfScope prof(SB_PROF_GEMV64, s);
+    k_gemv_n_c128<kGemvRows, kGemvThreads, kGemvUnroll>
+        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, r, b, part); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+int64_t gemv_partials(int64_t n) { return cdiv(n, kGemvRows); }
+
+void gemv_c64(const float2* A, int64_t n, int64_t lda, const float2* x, float2* y,
+              const float2* b, double* part, cudaStream_t s) {
+    ProfScope prof(SB_PROF_GEMV32, s);
+    k_gemv_n_c64<kGemvRows, kGemvThreads, kGemvUnroll, false>
+        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+void gemv_c64_x64(const float2* A, int64_t n, int64_t lda, const double2* x, double2* y,
+                  const double2* b, double* part, cudaStream_t s) {
+    ProfScope prof(SB_PROF_GEMV32, s);
+    k_gemv_n_c64<kGemvRows, kGemvThreads, kGemvUnroll, true>
+        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+template <class T>
+void arnoldi_dots(const T* V, int64_t ldv, int k, const T* w, int64_t n, double2* part,
+                  double2* out, cudaStream_t s) {
+    ProfScope prof(SB_PROF_ARNOLDI, s);
+    const int64_t chunks = cdiv(n, kDotRows);
+    dim3 grid(static_cast<unsigned>(chunks), static_cast<unsigned>(cdiv(k + 1, kDotVecs)));
+    k_dots<T><<<grid, kDotRows, 0, s>>>(V, ldv, k, w, n, part); count_launch();
+    SB_CUDA(cudaGetLastError());
+    k_reduce_part<<<k + 1, 32, 0, s>>>(part, chunks, k + 1, out); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+int64_t arnoldi_dot_chunks(int64_t n) { return cdiv(n, kDotRows); }
+
+template <class T>
+void arnoldi_project(const T* V, int64_t ldv, int k, const double2* coeff, T* w, int64_t n,
+                     double* part, double* out_norm2, cudaStream_t s) {
+    ProfScope prof(SB_PROF_ARNOLDI, s);
+    const int64_t nb = cdiv(n, 256);
+    k_project<T><<<nb, 256, 0, s>>>(V, ldv, k, coeff, w, n, part); count_launch();
+    SB_CUDA(cudaGetLastError());
+    k_sum_real<<<1, 32, 0, s>>>(part, nb, out_norm2); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+void sum_real(const double* part, int64_t m, double* out, cudaStream_t s) {
+    k_sum_real<<<1, 32, 0, s>>>(part, m, out); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+template <class TI, class TO>
+void scale_vec(const TI* x, double alpha, TO* y, int64_t n, cudaStream_t s) {
+    k_scale<TI, TO><<<cdiv(n, 256), 256, 0, s>>>(x, alpha, y, n); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+template <class T, class TX>
+void basis_update(const T* V, int64_t ldv, int k, const double2* y, double alpha, TX* x, int64_t n,
+                  cudaStream_t s) {
+    ProfScope prof(SB_PROF_ARNOLDI, s);
+    k_update<T, TX><<<cdiv(n, 256), 256, 0, s>>>(V, ldv, k, y, alpha, x, n); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+template <class T>
+void jacobi_apply(const double2* d, const T* x, T* y, int64_t n, cudaStream_t s) {
+    k_jacobi<T><<<cdiv(n, 256), 256, 0, s>>>(d, x, y, n); count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+// Explicit instantiations.
+template void arnoldi_dots<double2>(const double2*, int64_t, int, const double2*, int64_t, double2*, double2*, cudaStream_t);
+template void arnoldi_dots<float2>(const float2*, int64_t, int, const float2*, int64_t, double2*, double2*, cudaStream_t);
+template void arnoldi_project<double2>(const double2*, int64_t, int, const double2*, double2*, int64_t, double*, double*, cudaStream_t);
+template void arnoldi_project<float2>(const float2*, int64_t, int, const double2*, float2*, int64_t, double*, double*, cudaStream_t);
+template void scale_vec<double2, double2>(const double2*, double, double2*, int64_t, cudaStream_t);
+template void scale_vec<float2, float2>(const float2*, double, float2*, int64_t, cudaStream_t);
+template void scale_vec<double2, float2>(const double2*, double, float2*, int64_t, cudaStream_t);
+template void scale_vec<float2, double2>(const float2*, double, double2*, int64_t, cudaStream_t);
+template void basis_update<double2, double2>(const double2*, int64_t, int, const double2*, double, double2*, int64_t, cudaStream_t);
+template void basis_update<float2, float2>(const float2*, int64_t, int, const double2*, double, float2*, int64_t, cudaStream_t);
+template void basis_update<float2, double2>(const float2*, int64_t, int, const double2*, double, double2*, int64_t, cudaStream_t);
+template void jacobi_apply<double2>(const double2*, const double2*, double2*, int64_t, cudaStream_t);
+template void jacobi_apply<float2>(const double2*, const float2*, float2*, int64_t, cudaStream_t);
+
+}  // namespace sb

@@ -1,0 +1,155 @@
+// Internal declarations shared by the sonium-b200 CUDA sources (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/sonium_b200.h"
+
+namespace sb {
+
+// ---------------------------------------------------------------------------------------------
+// Error handling: every entry point converts failures into an sb status plus a message that
+// sb_last_error() returns. Nothing throws across the C ABI.
+// ---------------------------------------------------------------------------------------------
+struct Error {
+    int status;
+    std::string msg;
+};
+
+void set_error(int status, const std::string& msg);
+void clear_error();
+
+#define SB_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            throw ::sb::Error{SB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+        }                                                                                    \
+    } while (0)
+
+#define SB_REQUIRE(cond, status, msg)                        \
+    do {                                                     \
+        if (!(cond)) throw ::sb::Error{(status), (msg)};     \
+    } while (0)
+
+// Number of kernels this library has launched (reported by sb_profile_read).
+void count_launch();
+
+// Host fault injection (points from the header's SB_INJECT_* values).
+extern int g_inject_point;
+void maybe_inject(int point);
+
+// Device memory with ownership; allocation failures surface as SB_ERR_OUT_OF_MEMORY.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void alloc(size_t n);
+    void release();
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Quadrature tables in constant memory (uploaded once per device by ensure_tables()).
+// ---------------------------------------------------------------------------------------------
+constexpr int kMaxGL = 8;              // Gauss-Legendre orders 1..8
+constexpr int kGLTotal = kMaxGL * (kMaxGL + 1) / 2;
+constexpr int kTriOrders = 4;          // regular leaf orders 4..7
+constexpr int kTriTotal = 13 + 25 + 36 + 49;
+constexpr int kFarPoints = 13;         // order-4 rule: the far-field single leaf
+
+void ensure_tables(int device);
+void host_gauss_legendre(int n, double* x, double* w);
+// Triangle rule of leaf order `order` (4..7) as (xi, eta, w) with weights summing to 0.5.
+int host_triangle_rule(int order, double* xi, double* eta, double* w);
+
+// ---------------------------------------------------------------------------------------------
+// Device-resident mesh
+// ---------------------------------------------------------------------------------------------
+// Element record fields in the SoA `elem` array: elem[f * ld + e].
+enum ElemField {
+    EV0X = 0, EV0Y, EV0Z, EV1X, EV1Y, EV1Z, EV2X, EV2Y, EV2Z,  // vertices
+    ECX, ECY, ECZ,                                          // centroid (collocation point)
+    ENX, ENY, ENZ,                                          // unit normal
+    EAREA, EJAC,                                            // area, |dx/ds x dx/dt|
+    EGX, EGY, EGZ,                                          // level-0 subdivision centre
+    ESQA,                                                   // sqrt(area)
+    EFIELDS
+};
+
+constexpr int kFarTile = 128;  // field elements per far-kernel column tile
+
+struct Mesh {
+    int device = 0;
+    int64_t n = 0, n_nodes = 0, ld = 0, n_tiles = 0;
+    std::vector<double> h_nodes;
+    std::vector<uint32_t> h_tris;
+    std::vector<double> h_elem;  // host copy of the element SoA (ld stride)
+    DevBuf nodes, tris, elem, qp;
+    // near-pair CSR (superset of the reference's subdivision criterion; excludes the diagonal)
+    int64_t nnz = 0;
+    DevBuf near_ptr, near_col;
+    // boundary conditions
+    std::vector<int32_t> h_bc_kind;
+    std::vector<double> h_bc_value, h_adm;  // interleaved complex
+    std::vector<uint8_t> h_has_adm;
+    bool any_bc_value = false, any_adm = false;
+    DevBuf bc_kind, bc_value, has_adm, adm;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Device-resident operator (assembled TBEM system)
+// ---------------------------------------------------------------------------------------------
+struct Operator {
+    Mesh* mesh = nullptr;
+    int device = 0;
+    int precision = SB_PRECISION_FP64;
+    int64_t n = 0;
+    sb_physics phys{};
+    double beta_re = 0, beta_im = 0;
+    int64_t lda32 = 0;           // even leading dimension of the complex64 copy
+    DevBuf A64, A32, rhs, diag;  // rhs: BC-induced RHS (N complex); diag: A_ii for Jacobi
+    DevBuf coef, far_part, near_rhs, self_rhs, scratch;
+    cudaStream_t stream = nullptr;
+    double last_assembly_ms = 0.0;
+};
+
+// Assembly (assembly.cu)
+void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im);
+void incident_plane_wave(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im,
+                         const double* dirs_host, const double* amps_host, int64_t r,
+                         double2* rhs_dev, cudaStream_t s, bool accumulate);
+
+void device_sincos(int device, const double* x, int64_t n, double* s, double* c);
+
+// Mesh (assembly.cu)
+Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, int64_t n_tris,
+                  int device);
+void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const uint8_t* has_adm,
+                 const sb_complex* adm);
+void host_element_geometry(const double* nodes, const uint32_t* tris, int64_t n, double* c,
+                           double* nrm, double* area);
+
+enum class Trans { N = 0, T = 1, C = 2 };
+
+// GMRES (gmres.cu)
+void gmres_fp64(const Operator& op, const double2* b_dev, double2* x_dev, bool x0_given,
+                const sb_gmres_config& cfg, int precond, sb_gmres_stats& st);
+void gmres_mixed_ir(const Operator& op, const double2* b_dev, double2* x_dev, bool x0_given,
+                    const sb_ir_config& cfg, sb_gmres_stats& st);
+
+int device_sm_count(int device);
+
+}  // namespace sb

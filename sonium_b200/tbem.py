@@ -1,0 +1,377 @@
+"""Python mirror of the reference's dense TBEM interface over the sonium-b200 C ABI.
+
+Names follow the reference (sonium-bem / sonium-solvers): ``PhysicsParams``,
+``build_tbem_system_with_beta`` (crates/sonium-bem/src/core/assembly/tbem.rs:1196),
+``LinearOperator.apply_into`` / ``apply_block`` (crates/sonium-solvers/crates/sonium-solvers-core/
+src/traits.rs:2949-3120), ``GmresConfig`` / ``gmres`` / ``GmresSolution``
+(crates/sonium-solvers/crates/sonium-solvers-iterative/src/gmres.rs:26-47, 93-118, 286) and
+``IncidentField.compute_rhs_with_beta`` for plane waves (crates/sonium-bem/src/core/incident.rs:
+807-833). Every call goes to the CUDA library; failures raise ``SoniumError``.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import SoniumError, check
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ct.c_void_p)
+
+
+def _c128(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def device_count() -> int:
+    n = ct.c_int(0)
+    check(L.load().sb_device_count(ct.byref(n)))
+    return n.value
+
+
+@dataclass
+class PhysicsParams:
+    """PhysicsParams (crates/sonium-bem/src/core/types.rs:34-53)."""
+
+    frequency: float
+    speed_of_sound: float
+    density: float
+    wave_number: float
+    omega: float
+    wave_length: float
+    harmonic_factor: float
+    pressure_factor: float
+    tau: float
+
+    @classmethod
+    def new(cls, frequency: float, speed_of_sound: float = 343.0, density: float = 1.21,
+            is_internal: bool = False) -> "PhysicsParams":
+        s = L.SbPhysics()
+        check(L.load().sb_physics_new(frequency, speed_of_sound, density, int(is_internal), ct.byref(s)))
+        return cls(*(getattr(s, f) for f, _ in L.SbPhysics._fields_))
+
+    @classmethod
+    def for_wavenumber(cls, k: float, speed_of_sound: float = 343.0, density: float = 1.21,
+                       is_internal: bool = False) -> "PhysicsParams":
+        return cls.new(k * speed_of_sound / (2.0 * np.pi), speed_of_sound, density, is_internal)
+
+    def _struct(self) -> L.SbPhysics:
+        return L.SbPhysics(*(getattr(self, f) for f, _ in L.SbPhysics._fields_))
+
+    def burton_miller_beta(self, scale: float = 1.0) -> complex:
+        out = L.SbComplex()
+        check(L.load().sb_burton_miller_beta(ct.byref(self._struct()), scale, ct.byref(out)))
+        return complex(out.re, out.im)
+
+
+def icosphere(radius: float, level: int, scale=None):
+    """generate_icosphere_mesh (crates/sonium-bem/src/core/mesh/generators.rs:309-397) nodes/tris."""
+    lib = L.load()
+    nn, nt = ct.c_int64(), ct.c_int64()
+    check(lib.sb_icosphere_counts(level, ct.byref(nn), ct.byref(nt)))
+    nodes = np.zeros((nn.value, 3))
+    tris = np.zeros((nt.value, 3), np.uint32)
+    sc = None if scale is None else np.ascontiguousarray(scale, np.float64)
+    check(lib.sb_icosphere(radius, level, None if sc is None else _p(sc), _p(nodes), _p(tris)))
+    return nodes, tris
+
+
+class Mesh:
+    """A device-resident Tri3 constant-panel mesh (element e owns DOF e)."""
+
+    def __init__(self, nodes, tris, device: int = 0):
+        self.nodes = np.ascontiguousarray(nodes, np.float64)
+        self.tris = np.ascontiguousarray(tris, np.uint32)
+        if self.nodes.ndim != 2 or self.nodes.shape[1] != 3 or self.tris.ndim != 2 or self.tris.shape[1] != 3:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "nodes must be (n, 3) and tris (m, 3)")
+        h = ct.c_void_p()
+        check(L.load().sb_mesh_create(_p(self.nodes), self.nodes.shape[0], _p(self.tris),
+                                      self.tris.shape[0], device, ct.byref(h)))
+        self._h = h
+
+    @classmethod
+    def icosphere(cls, radius: float, level: int, scale=None, device: int = 0) -> "Mesh":
+        nodes, tris = icosphere(radius, level, scale)
+        return cls(nodes, tris, device)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "mesh has been closed")
+        return self._h
+
+    @property
+    def num_elements(self) -> int:
+        return self.tris.shape[0]
+
+    def info(self) -> L.SbMeshInfo:
+        i = L.SbMeshInfo()
+        check(L.load().sb_mesh_info_get(self.handle, ct.byref(i)))
+        return i
+
+    def element_geometry(self):
+        m = self.num_elements
+        c, n, a = np.zeros((m, 3)), np.zeros((m, 3)), np.zeros(m)
+        check(L.load().sb_mesh_element_geometry(self.handle, _p(c), _p(n), _p(a)))
+        return c, n, a
+
+    def set_boundary_conditions(self, kind=None, value=None, admittance=None):
+        """Per-element BoundaryCondition; ``admittance`` uses NaN for 'no admittance'."""
+        m = self.num_elements
+        k = None if kind is None else np.ascontiguousarray(np.broadcast_to(kind, (m,)), np.int32)
+        v = None if value is None else _c128(np.broadcast_to(value, (m,)))
+        has = adm = None
+        if admittance is not None:
+            a = np.asarray(np.broadcast_to(admittance, (m,)), np.complex128)
+            has = np.ascontiguousarray(~np.isnan(a.real), np.uint8)
+            adm = _c128(np.nan_to_num(a))
+        check(L.load().sb_mesh_set_bc(self.handle, None if k is None else _p(k), None if v is None else _p(v),
+                                      None if has is None else _p(has), None if adm is None else _p(adm)))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.load().sb_mesh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LinearOperator:
+    """LinearOperator<Complex64> (traits.rs:2949-3120)."""
+
+    def num_rows(self) -> int:
+        raise NotImplementedError
+
+    def num_cols(self) -> int:
+        raise NotImplementedError
+
+    def apply_into(self, x, y) -> None:
+        raise NotImplementedError
+
+    def apply(self, x):
+        y = np.zeros(self.num_rows(), np.complex128)
+        self.apply_into(x, y)
+        return y
+
+
+class TbemOperator(LinearOperator):
+    """The assembled TbemSystem kept on the device, as a dense LinearOperator."""
+
+    def __init__(self, mesh: Mesh, handle, physics: PhysicsParams, beta: complex, precision: int):
+        self.mesh = mesh
+        self._h = handle
+        self.physics = physics
+        self.beta = beta
+        self.precision = precision
+        self.n = mesh.num_elements
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "operator has been closed")
+        return self._h
+
+    def num_rows(self) -> int:
+        return self.n
+
+    def num_cols(self) -> int:
+        return self.n
+
+    def info(self) -> L.SbOperatorInfo:
+        i = L.SbOperatorInfo()
+        check(L.load().sb_operator_info_get(self.handle, ct.byref(i)))
+        return i
+
+    def reassemble(self, physics: PhysicsParams, beta: complex) -> None:
+        check(L.load().sb_assemble_into(self.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag)))
+        self.physics, self.beta = physics, beta
+
+    @property
+    def matrix(self) -> np.ndarray:
+        A = np.zeros((self.n, self.n), np.complex128)
+        check(L.load().sb_operator_copy_to_host(self.handle, _p(A), None))
+        return A
+
+    @property
+    def rhs(self) -> np.ndarray:
+        r = np.zeros(self.n, np.complex128)
+        check(L.load().sb_operator_copy_to_host(self.handle, None, _p(r)))
+        return r
+
+    def rows(self, r0: int, r1: int) -> np.ndarray:
+        A = np.zeros((r1 - r0, self.n), np.complex128)
+        check(L.load().sb_operator_copy_rows_to_host(self.handle, r0, r1, _p(A)))
+        return A
+
+    def matrix_c64(self) -> np.ndarray:
+        A = np.zeros((self.n, self.n), np.complex64)
+        check(L.load().sb_operator_copy_to_host_c64(self.handle, _p(A)))
+        return A
+
+    def _apply(self, trans: int, x, y) -> None:
+        x = _c128(x)
+        if x.shape != (self.n,) or y.shape != (self.n,) or y.dtype != np.complex128 or not y.flags.c_contiguous:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "apply: vectors must be length-n complex128")
+        check(L.load().sb_operator_apply(self.handle, trans, _p(x), _p(y)))
+
+    def apply_into(self, x, y) -> None:
+        self._apply(L.SB_OP_N, x, y)
+
+    def apply_transpose_into(self, x, y) -> None:
+        self._apply(L.SB_OP_T, x, y)
+
+    def apply_hermitian_into(self, x, y) -> None:
+        self._apply(L.SB_OP_C, x, y)
+
+    def apply_block(self, X) -> np.ndarray:
+        X = _c128(X)
+        if X.ndim != 2 or X.shape[0] != self.n:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "apply_block: X must be n x r")
+        Y = np.zeros_like(X)
+        check(L.load().sb_operator_apply_block(self.handle, _p(X), _p(Y), X.shape[1]))
+        return Y
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.load().sb_operator_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class JacobiPreconditioner:
+    """Preconditioner<Complex64> (traits.rs:3645-3720): y = diag(A)^-1 x."""
+
+    kind = L.SB_PRECOND_JACOBI
+
+    def __init__(self, op: TbemOperator):
+        self.op = op
+
+    def apply_into(self, x, y) -> None:
+        x = _c128(x)
+        check(L.load().sb_preconditioner_apply(self.op.handle, self.kind, _p(x), _p(y)))
+
+
+def build_tbem_system_with_beta(mesh: Mesh, physics: PhysicsParams, beta: complex,
+                                precision: int = L.SB_PRECISION_FP64) -> TbemOperator:
+    """build_tbem_system_with_beta (tbem.rs:1196-1203): assemble on the device."""
+    h = ct.c_void_p()
+    check(L.load().sb_assemble(mesh.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag),
+                               precision, ct.byref(h)))
+    return TbemOperator(mesh, h, physics, beta, precision)
+
+
+def build_tbem_system(mesh: Mesh, physics: PhysicsParams, precision: int = L.SB_PRECISION_FP64) -> TbemOperator:
+    """build_tbem_system (tbem.rs:877-883): beta = i/k."""
+    return build_tbem_system_with_beta(mesh, physics, physics.burton_miller_beta(), precision)
+
+
+def rhs_plane_wave(mesh: Mesh, physics: PhysicsParams, beta: complex, directions, amplitudes=None) -> np.ndarray:
+    """IncidentField::compute_rhs_with_beta for plane waves: (n, r) complex128."""
+    d = np.ascontiguousarray(np.atleast_2d(directions), np.float64)
+    r = d.shape[0]
+    a = None if amplitudes is None else _c128(np.broadcast_to(amplitudes, (r,)))
+    out = np.zeros((mesh.num_elements, r), np.complex128)
+    check(L.load().sb_rhs_plane_wave(mesh.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag),
+                                     _p(d), None if a is None else _p(a), r, _p(out)))
+    return out
+
+
+@dataclass
+class GmresConfig:
+    """GmresConfig (gmres.rs:26-47): max_iterations = restart cycles."""
+
+    max_iterations: int = 100
+    restart: int = 30
+    tolerance: float = 1e-6
+    convergence_check_interval: int = 1
+
+    def _struct(self):
+        return L.SbGmresConfig(self.max_iterations, self.restart, self.tolerance, self.convergence_check_interval)
+
+
+@dataclass
+class IrConfig:
+    """Mixed-precision refinement: FP64 outer residual, FP32 inner GMRES."""
+
+    max_refinements: int = 20
+    tolerance: float = 1e-8
+    inner_restart: int = 50
+    inner_max_iterations: int = 20
+    inner_tolerance: float = 1e-5
+
+    def _struct(self):
+        return L.SbIrConfig(self.max_refinements, self.tolerance, self.inner_restart, self.inner_max_iterations,
+                            self.inner_tolerance)
+
+
+STATUS_NAMES = {0: "Converged", 1: "MaxIterationsReached", 2: "Breakdown", 3: "NumericalError"}
+
+
+@dataclass
+class GmresSolution:
+    """GmresSolution (gmres.rs:93-118)."""
+
+    x: np.ndarray
+    iterations: int
+    restarts: int
+    residual: float
+    estimated_residual: float
+    backward_error: float
+    converged: bool
+    status: str
+    matvecs: int = 0
+    matvecs_fp32: int = 0
+    refinements: int = 0
+    device_ms: float = 0.0
+    extra: dict = field(default_factory=dict)
+
+    @classmethod
+    def _from(cls, x, st: L.SbGmresStats) -> "GmresSolution":
+        return cls(x=x, iterations=st.iterations, restarts=st.restarts, residual=st.residual,
+                   estimated_residual=st.estimated_residual, backward_error=st.backward_error,
+                   converged=bool(st.converged), status=STATUS_NAMES.get(st.status, str(st.status)),
+                   matvecs=st.matvecs, matvecs_fp32=st.matvecs_fp32, refinements=st.refinements,
+                   device_ms=st.device_ms)
+
+
+def gmres(operator: TbemOperator, b, config: GmresConfig = GmresConfig(), x0=None,
+          preconditioner: JacobiPreconditioner | None = None) -> GmresSolution:
+    """gmres / gmres_preconditioned (gmres.rs:286-305) on the device-resident operator."""
+    b = _c128(b)
+    if b.shape != (operator.n,):
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "gmres: b must have length n")
+    x = np.zeros(operator.n, np.complex128)
+    x0a = None if x0 is None else _c128(x0)
+    st = L.SbGmresStats()
+    pk = L.SB_PRECOND_IDENTITY if preconditioner is None else preconditioner.kind
+    check(L.load().sb_gmres(operator.handle, _p(b), None if x0a is None else _p(x0a), ct.byref(config._struct()),
+                            pk, _p(x), ct.byref(st)))
+    return GmresSolution._from(x, st)
+
+
+def gmres_mixed(operator: TbemOperator, b, config: IrConfig = IrConfig(), x0=None) -> GmresSolution:
+    """FP32-inner / FP64-refined GMRES (needs a SB_PRECISION_FP64_FP32 operator)."""
+    b = _c128(b)
+    x = np.zeros(operator.n, np.complex128)
+    x0a = None if x0 is None else _c128(x0)
+    st = L.SbGmresStats()
+    check(L.load().sb_gmres_mixed(operator.handle, _p(b), None if x0a is None else _p(x0a),
+                                  ct.byref(config._struct()), _p(x), ct.byref(st)))
+    return GmresSolution._from(x, st)
+
+
+def inject_failure(point: int) -> None:
+    check(L.load().sb_inject_failure(point))
