@@ -118,6 +118,9 @@ SB_API int sb_mesh_set_bc(sb_mesh* mesh, const int32_t* kind, const sb_complex* 
 /* ---- assembly ---- */
 #define SB_PRECISION_FP64 0      /* complex128 matrix only */
 #define SB_PRECISION_FP64_FP32 1 /* complex128 matrix plus a complex64 copy from one epilogue */
+#define SB_PRECISION_FP32 2      /* complex64 matrix only: far pairs in FP32 with the phase
+                                  * argument k r in FP64, near and self pairs in FP64; products
+                                  * with FP64 vectors accumulate in FP64 */
 
 typedef struct sb_operator sb_operator;
 

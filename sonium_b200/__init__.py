@@ -4,7 +4,7 @@ The compute path is the CUDA shared library built from ``sonium_b200/csrc`` (C A
 ``include/sonium_b200.h``); this package is its Python binding. There is no CPU fallback.
 """
 from ._lib import (SB_BC_PRESSURE, SB_BC_VELOCITY, SB_INJECT_ALLOC, SB_INJECT_LAUNCH, SB_INJECT_NONE,
-                   SB_OP_C, SB_OP_N, SB_OP_T, SB_PRECISION_FP64, SB_PRECISION_FP64_FP32,
+                   SB_OP_C, SB_OP_N, SB_OP_T, SB_PRECISION_FP32, SB_PRECISION_FP64, SB_PRECISION_FP64_FP32,
                    SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI, SoniumError)
 from .tbem import (GmresConfig, GmresSolution, IrConfig, JacobiPreconditioner, LinearOperator, Mesh,
                    PhysicsParams, TbemOperator, build_tbem_system, build_tbem_system_with_beta,
@@ -15,6 +15,6 @@ __all__ = [
     "PhysicsParams", "TbemOperator", "build_tbem_system", "build_tbem_system_with_beta", "device_count",
     "gmres", "gmres_mixed", "icosphere", "inject_failure", "rhs_plane_wave", "SoniumError",
     "SB_BC_PRESSURE", "SB_BC_VELOCITY", "SB_INJECT_ALLOC", "SB_INJECT_LAUNCH", "SB_INJECT_NONE",
-    "SB_OP_C", "SB_OP_N", "SB_OP_T", "SB_PRECISION_FP64", "SB_PRECISION_FP64_FP32",
+    "SB_OP_C", "SB_OP_N", "SB_OP_T", "SB_PRECISION_FP32", "SB_PRECISION_FP64", "SB_PRECISION_FP64_FP32",
     "SB_PRECOND_IDENTITY", "SB_PRECOND_JACOBI",
 ]

@@ -23,6 +23,7 @@ SB_ERR_NOT_FINITE = 7
 
 SB_PRECISION_FP64 = 0
 SB_PRECISION_FP64_FP32 = 1
+SB_PRECISION_FP32 = 2
 SB_OP_N, SB_OP_T, SB_OP_C = 0, 1, 2
 SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI = 0, 1
 SB_BC_VELOCITY, SB_BC_PRESSURE = 0, 1

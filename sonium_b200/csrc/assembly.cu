@@ -521,7 +521,7 @@ __global__ void __launch_bounds__(kFarTile) k_far(const double* __restrict__ qp,
                 const double dx = p[0] - xx, dy = p[kFarTile] - xy, dz = p[2 * kFarTile] - xz;
                 const double w = p[3 * kFarTile];
                 const double d2 = dx * dx + dy * dy + dz * dz;
-                const double rinv = sb_rsqrt(d2);
+                const double rinv = sb_rsqrt2(d2);
                 point_channels(a, dx, dy, dz, d2 * rinv, rinv, w, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
             }
             const double2 v = combine(a, coef, ld, j, CF_CG);
@@ -534,6 +534,219 @@ __global__ void __launch_bounds__(kFarTile) k_far(const double* __restrict__ qp,
             if ((tid & 31) == 0) {
                 sred[tid >> 5][0] = sx;
                 sred[tid >> 5][1] = sy;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                double tx = 0, ty = 0;
+                for (int w = 0; w < kFarTile / 32; ++w) {
+                    tx += sred[w][0];
+                    ty += sred[w][1];
+                }
+                far_part[i * n_tiles + tile] = make_double2(tx, ty);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed-precision far kernel (SB_PRECISION_FP32): the phase argument k r stays in FP64, the rest
+// of the 13-point leaf in FP32.
+//
+// Per pair the centroid offset d_c = c_j - x_i, r_c = |d_c| and exp(i k r_c) come from FP64
+// (k r_c reduced modulo 2 pi in FP64, the reduced angle's sin / cos in FP32). Per point, with
+// delta_q = y_q - c_j precomputed per element, the distance change is formed without
+// cancellation as r_q - r_c = (2 d_c . delta_q + |delta_q|^2) / (r_q + r_c) and its small phase
+// k (r_q - r_c) rotates exp(i k r_c). Everything else (G, H, H^T, E factors and the sums) is
+// FP32; the near and self pairs keep the FP64 kernels.
+// ---------------------------------------------------------------------------------------------
+constexpr int kQ32 = 5;  // per point: delta x, y, z, |delta|^2, w * J / (4 pi)
+
+// Element point data for the FP32 far kernel: qp32[(q * 5 + c) * ld + e].
+__global__ void k_far_points32(const double* __restrict__ elem, int64_t n, int64_t ld,
+                               float* __restrict__ qp32) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ld) return;
+    const int o = c_tri_off[0];
+    for (int q = 0; q < kFarPoints; ++q) {
+        float* dst = qp32 + (int64_t)(q * kQ32) * ld + e;
+        if (e >= n) {
+            for (int c = 0; c < kQ32; ++c) dst[c * ld] = 0.f;
+            continue;
+        }
+        const double s = c_tri_xi[o + q], t = c_tri_eta[o + q];
+        const double sf0 = 1.0 - s - t;
+        double dl[3];
+        for (int j = 0; j < 3; ++j)
+            dl[j] = sf0 * E(EV0X + j, e) + s * E(EV1X + j, e) + t * E(EV2X + j, e) - E(ECX + j, e);
+        for (int j = 0; j < 3; ++j) dst[j * ld] = static_cast<float>(dl[j]);
+        dst[3 * ld] = static_cast<float>(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
+        dst[4 * ld] = static_cast<float>(c_tri_w[o + q] * E(EJAC, e) * kInv4Pi);
+    }
+}
+
+// sin / cos in FP32 for |x| <= pi: quadrant reduction by pi/2 and Taylor series to x^9 / x^10
+// on |r| <= pi/4 (truncation below 2e-9).
+__device__ __forceinline__ void sincos_f32(float x, float* so, float* co) {
+    const float q = rintf(x * 0.636619772f);
+    float r = fmaf(-q, 1.57079637f, x);
+    r = fmaf(-q, -4.37113883e-8f, r);
+    const float r2 = r * r;
+    float ps = 2.75573192e-6f;
+    ps = fmaf(ps, r2, -1.98412698e-4f);
+    ps = fmaf(ps, r2, 8.33333333e-3f);
+    ps = fmaf(ps, r2, -1.66666667e-1f);
+    const float sn = fmaf(ps * r2, r, r);
+    float pc = -2.75573192e-7f;
+    pc = fmaf(pc, r2, 2.48015873e-5f);
+    pc = fmaf(pc, r2, -1.38888889e-3f);
+    pc = fmaf(pc, r2, 4.16666667e-2f);
+    pc = fmaf(pc, r2, -0.5f);
+    const float cs = fmaf(pc, r2, 1.0f);
+    const int quad = static_cast<int>(q) & 3;
+    float sv = sn, cv = cs;
+    if (quad & 1) {
+        sv = cs;
+        cv = -sn;
+    }
+    if (quad & 2) {
+        sv = -sv;
+        cv = -cv;
+    }
+    *so = sv;
+    *co = cv;
+}
+
+constexpr int kFar32Rows = 64;
+
+template <bool kWithRhs>
+__global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp32,
+                                                    const double* __restrict__ elem, int64_t n,
+                                                    int64_t ld, const double* __restrict__ coef,
+                                                    double k, float2* __restrict__ A32, int64_t lda32,
+                                                    double2* __restrict__ far_part, int64_t n_tiles) {
+    __shared__ double sx[kFar32Rows][3];
+    __shared__ float snx[kFar32Rows][3];
+    __shared__ double sred[kFarTile / 32][2];
+    const int tid = threadIdx.x;
+    const int64_t tile = blockIdx.x;
+    const int64_t j = tile * kFarTile + tid;
+    const int64_t row0 = blockIdx.y * (int64_t)kFar32Rows;
+    for (int t = tid; t < kFar32Rows * 3; t += kFarTile) {
+        const int r = t / 3, c = t % 3;
+        const int64_t i = row0 + r;
+        sx[r][c] = (i < n) ? E(ECX + c, i) : 0.0;
+        snx[r][c] = (i < n) ? static_cast<float>(E(ENX + c, i)) : 0.f;
+    }
+    // The column's 13 points in registers.
+    float px[kFarPoints], py[kFarPoints], pz[kFarPoints], pd[kFarPoints], pw[kFarPoints];
+    double cx = 0, cy = 0, cz = 0, gx = 0, gy = 0, gz = 0, thr = -1;
+    float nyx = 0, nyy = 0, nyz = 0;
+    float cgr = 0, cgi = 0, chr = 0, chi = 0, ctr = 0, cti = 0, cer = 0, cei = 0;
+    const int64_t jj = j < n ? j : 0;
+#pragma unroll
+    for (int q = 0; q < kFarPoints; ++q) {
+        const float* src = qp32 + (int64_t)(q * kQ32) * ld + jj;
+        px[q] = src[0];
+        py[q] = src[ld];
+        pz[q] = src[2 * ld];
+        pd[q] = src[3 * ld];
+        pw[q] = src[4 * ld];
+    }
+    if (j < n) {
+        cx = E(ECX, j); cy = E(ECY, j); cz = E(ECZ, j);
+        gx = E(EGX, j); gy = E(EGY, j); gz = E(EGZ, j);
+        thr = near_threshold(E(EAREA, j));
+        nyx = static_cast<float>(E(ENX, j));
+        nyy = static_cast<float>(E(ENY, j));
+        nyz = static_cast<float>(E(ENZ, j));
+        cgr = static_cast<float>(coef[(int64_t)(CF_CG) * ld + j]);
+        cgi = static_cast<float>(coef[(int64_t)(CF_CG + 1) * ld + j]);
+        chr = static_cast<float>(coef[(int64_t)(CF_CH) * ld + j]);
+        chi = static_cast<float>(coef[(int64_t)(CF_CH + 1) * ld + j]);
+        ctr = static_cast<float>(coef[(int64_t)(CF_CHT) * ld + j]);
+        cti = static_cast<float>(coef[(int64_t)(CF_CHT + 1) * ld + j]);
+        cer = static_cast<float>(coef[(int64_t)(CF_CE) * ld + j]);
+        cei = static_cast<float>(coef[(int64_t)(CF_CE + 1) * ld + j]);
+    }
+    __syncthreads();
+    const float kf = static_cast<float>(k), k2f = kf * kf;
+    const int64_t rows_here = (n - row0 < kFar32Rows) ? (n - row0) : kFar32Rows;
+    for (int r = 0; r < rows_here; ++r) {
+        const int64_t i = row0 + r;
+        const double x0 = sx[r][0], x1 = sx[r][1], x2 = sx[r][2];
+        const bool active = (j < n) && (j != i) && !near_superset(gx, gy, gz, thr, x0, x1, x2);
+        double2 rhs_c = make_double2(0.0, 0.0);
+        if (active) {
+            // FP64: centroid offset, distance and the reduced phase k r_c mod 2 pi.
+            const double dcx = cx - x0, dcy = cy - x1, dcz = cz - x2;
+            const double rc2 = dcx * dcx + dcy * dcy + dcz * dcz;
+            const double rc = rc2 * sb_rsqrt2(rc2);
+            const double ph = k * rc;
+            const double nq = rint(ph * 0x1.45f306dc9c883p-3);  // 1 / (2 pi)
+            double red = fma(-nq, 0x1.921fb54442d18p+2, ph);    // 2 pi split in two doubles
+            red = fma(-nq, 0x1.1a62633145c07p-52, red);
+            float sc, cc;
+            sincos_f32(static_cast<float>(red), &sc, &cc);
+            const float fx = static_cast<float>(dcx), fy = static_cast<float>(dcy), fz = static_cast<float>(dcz);
+            const float rcf = static_cast<float>(rc), rc2f = static_cast<float>(rc2);
+            const float nxx = snx[r][0], nxy = snx[r][1], nxz = snx[r][2];
+            const float nxny = nxx * nyx + nxy * nyy + nxz * nyz;
+            float ag_r = 0.f, ag_i = 0.f, ah_r = 0.f, ah_i = 0.f, at_r = 0.f, at_i = 0.f, ae_r = 0.f, ae_i = 0.f;
+#pragma unroll
+            for (int q = 0; q < kFarPoints; ++q) {
+                const float num = fmaf(2.f, fx * px[q] + fy * py[q] + fz * pz[q], pd[q]);
+                const float rq2 = rc2f + num;
+                const float rinv = rsqrtf(rq2);
+                const float rq = rq2 * rinv;
+                const float t = kf * __fdividef(num, rq + rcf);
+                float st, ct;
+                if (fabsf(t) <= 0.8f) {
+                    const float t2 = t * t;
+                    float ps = fmaf(fmaf(fmaf(2.75573192e-6f, t2, -1.98412698e-4f), t2, 8.33333333e-3f), t2, -1.66666667e-1f);
+                    st = fmaf(ps * t2, t, t);
+                    float pc = fmaf(fmaf(fmaf(fmaf(-2.75573192e-7f, t2, 2.48015873e-5f), t2, -1.38888889e-3f), t2,
+                                         4.16666667e-2f), t2, -0.5f);
+                    ct = fmaf(pc, t2, 1.0f);
+                } else {
+                    sincos_f32(t, &st, &ct);
+                }
+                const float er = cc * ct - sc * st, ei = sc * ct + cc * st;
+                const float gs = pw[q] * rinv;
+                const float g_r = er * gs, g_i = ei * gs;
+                const float ux = (fx + px[q]) * rinv, uy = (fy + py[q]) * rinv, uz = (fz + pz[q]) * rinv;
+                const float rny = ux * nyx + uy * nyy + uz * nyz;
+                const float rnx = -(ux * nxx + uy * nxy + uz * nxz);
+                const float b_r = -g_r * rinv - g_i * kf;
+                const float b_i = g_r * kf - g_i * rinv;
+                ag_r += g_r;
+                ag_i += g_i;
+                ah_r = fmaf(b_r, rny, ah_r);
+                ah_i = fmaf(b_i, rny, ah_i);
+                at_r = fmaf(b_r, rnx, at_r);
+                at_i = fmaf(b_i, rnx, at_i);
+                const float rqq = rny * rnx;
+                const float ri2 = rinv * rinv;
+                const float f_r = (3.f * ri2 - k2f) * rqq + nxny * ri2;
+                const float f_i = -kf * rinv * (3.f * rqq + nxny);
+                ae_r += g_r * f_r - g_i * f_i;
+                ae_i += g_r * f_i + g_i * f_r;
+            }
+            const float vr = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
+            const float vi = ag_r * cgi + ag_i * cgr + ah_r * chi + ah_i * chr + at_r * cti + at_i * ctr + ae_r * cei + ae_i * cer;
+            A32[i * lda32 + j] = make_float2(vr, vi);
+            if (kWithRhs) {
+                Acc a;
+                a.gr = ag_r; a.gi = ag_i; a.hr = ah_r; a.hi = ah_i;
+                a.tr = at_r; a.ti = at_i; a.er = ae_r; a.ei = ae_i;
+                rhs_c = combine(a, coef, ld, j, CF_DG);
+            }
+        }
+        if (kWithRhs) {
+            double sxr = warp_sum(rhs_c.x), syr = warp_sum(rhs_c.y);
+            if ((tid & 31) == 0) {
+                sred[tid >> 5][0] = sxr;
+                sred[tid >> 5][1] = syr;
             }
             __syncthreads();
             if (tid == 0) {
@@ -759,7 +972,6 @@ __device__ __forceinline__ Acc warp_reduce(const Acc& a) {
     return r;
 }
 
-template <bool kWithF32>
 __global__ void __launch_bounds__(32 * kNearWarps) k_near(const double* __restrict__ elem,
                                                           int64_t n, int64_t ld,
                                                           const int64_t* __restrict__ row_ptr,
@@ -785,8 +997,8 @@ __global__ void __launch_bounds__(32 * kNearWarps) k_near(const double* __restri
     const Acc t = warp_reduce(a);
     if (lane == 0) {
         const double2 v = combine(t, coef, ld, j, CF_CG);
-        A64[i * n + j] = v;
-        if (kWithF32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+        if (A64) A64[i * n + j] = v;
+        if (A32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
         if (near_rhs) near_rhs[p] = combine(t, coef, ld, j, CF_DG);
     }
 }
@@ -794,7 +1006,6 @@ __global__ void __launch_bounds__(32 * kNearWarps) k_near(const double* __restri
 // ---------------------------------------------------------------------------------------------
 // Self kernel: one warp per element (singular_integration_with_params_mode, singular.rs:297-614).
 // ---------------------------------------------------------------------------------------------
-template <bool kWithF32>
 __global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, int64_t n,
                                               int64_t ld, const double* __restrict__ coef,
                                               double k, double2* __restrict__ A64,
@@ -909,8 +1120,8 @@ __global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, i
         double2 v = combine(t, coef, ld, i, CF_CG);
         v.x += coef[(int64_t)(CF_DIAG) * ld + i];
         v.y += coef[(int64_t)(CF_DIAG + 1) * ld + i];
-        A64[i * n + i] = v;
-        if (kWithF32) A32[i * lda32 + i] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+        if (A64) A64[i * n + i] = v;
+        if (A32) A32[i * lda32 + i] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
         diag[i] = v;
         double2 r = make_double2(coef[(int64_t)(CF_RHS) * ld + i], coef[(int64_t)(CF_RHS + 1) * ld + i]);
         if (self_rhs) {
@@ -1015,12 +1226,15 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
         m->tris.alloc(sizeof(uint32_t) * 3 * n_tris);
         m->elem.alloc(sizeof(double) * EFIELDS * m->ld);
         m->qp.alloc(sizeof(double) * kQpTileDoubles * m->n_tiles);
+        m->qp32.alloc(sizeof(float) * kFarPoints * kQ32 * m->ld);
         SB_CUDA(cudaMemcpy(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes, cudaMemcpyHostToDevice));
         SB_CUDA(cudaMemcpy(m->tris.p, tris, sizeof(uint32_t) * 3 * n_tris, cudaMemcpyHostToDevice));
         const int64_t nb = cdiv(m->ld, 256);
         k_element_geometry<<<nb, 256>>>(m->nodes.as<double>(), m->tris.as<uint32_t>(), m->n, m->ld, m->elem.as<double>()); count_launch();
         SB_CUDA(cudaGetLastError());
         k_far_points<<<nb, 256>>>(m->elem.as<double>(), m->n, m->ld, m->qp.as<double>()); count_launch();
+        SB_CUDA(cudaGetLastError());
+        k_far_points32<<<nb, 256>>>(m->elem.as<double>(), m->n, m->ld, m->qp32.as<float>()); count_launch();
         SB_CUDA(cudaGetLastError());
         // Near-pair CSR.
         DevBuf counts;
@@ -1103,8 +1317,8 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     }
     if (!op.rhs.p) op.rhs.alloc(sizeof(double2) * n);
     if (!op.diag.p) op.diag.alloc(sizeof(double2) * n);
-    DevBuf status;
-    status.alloc(sizeof(int));
+    if (!op.status.p) op.status.alloc(sizeof(int));
+    DevBuf& status = op.status;
     SB_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int), op.stream));
     cudaEvent_t e0, e1;
     SB_CUDA(cudaEventCreate(&e0));
@@ -1116,10 +1330,24 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
         m.adm.as<double2>(), ph.tau, ph.pressure_factor, beta, op.coef.as<double>()); count_launch();
     SB_CUDA(cudaGetLastError());
     const double k = ph.harmonic_factor * ph.wave_number;
+    const bool mixed = op.precision == SB_PRECISION_FP32;
     const bool f32 = op.precision == SB_PRECISION_FP64_FP32;
-    double2* A64 = op.A64.as<double2>();
-    float2* A32 = f32 ? op.A32.as<float2>() : nullptr;
-    {
+    double2* A64 = mixed ? nullptr : op.A64.as<double2>();
+    float2* A32 = (f32 || mixed) ? op.A32.as<float2>() : nullptr;
+    if (mixed) {
+        ProfScope prof(SB_PROF_FAR, op.stream);
+        dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFar32Rows)));
+        if (with_rhs)
+            k_far32<true><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
+                                                             op.coef.as<double>(), k, A32, op.lda32,
+                                                             op.far_part.as<double2>(), m.n_tiles);
+        else
+            k_far32<false><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
+                                                              op.coef.as<double>(), k, A32, op.lda32, nullptr,
+                                                              m.n_tiles);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    } else {
         ProfScope prof(SB_PROF_FAR, op.stream);
         dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFarRows)));
         const size_t sm = sizeof(double) * (kQpTileDoubles + kFarRows * 6);
@@ -1140,16 +1368,14 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     if (m.nnz > 0) {
         ProfScope prof(SB_PROF_NEAR, op.stream);
         const int64_t nb = cdiv(m.nnz, kNearWarps);
-        auto kern = f32 ? k_near<true> : k_near<false>;
-        kern<<<nb, 32 * kNearWarps, 0, op.stream>>>(m.elem.as<double>(), n, ld, m.near_ptr.as<int64_t>(),
+        k_near<<<nb, 32 * kNearWarps, 0, op.stream>>>(m.elem.as<double>(), n, ld, m.near_ptr.as<int64_t>(),
                                                      m.near_col.as<int32_t>(), m.nnz, op.coef.as<double>(), k,
                                                      A64, A32, op.lda32, with_rhs ? op.near_rhs.as<double2>() : nullptr); count_launch();
         SB_CUDA(cudaGetLastError());
     }
     {
         ProfScope prof(SB_PROF_SELF, op.stream);
-        auto kern = f32 ? k_self<true> : k_self<false>;
-        kern<<<cdiv(n, 4), 128, 0, op.stream>>>(m.elem.as<double>(), n, ld, op.coef.as<double>(), k, A64, A32, op.lda32,
+        k_self<<<cdiv(n, 4), 128, 0, op.stream>>>(m.elem.as<double>(), n, ld, op.coef.as<double>(), k, A64, A32, op.lda32,
                                                  with_rhs ? op.self_rhs.as<double2>() : nullptr,
                                                  op.diag.as<double2>()); count_launch();
         SB_CUDA(cudaGetLastError());
@@ -1169,7 +1395,8 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     cudaEventDestroy(e1);
     op.last_assembly_ms = ms;
     int st = 0;
-    SB_CUDA(cudaMemcpy(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    SB_CUDA(cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, op.stream));
+    SB_CUDA(cudaStreamSynchronize(op.stream));
     SB_REQUIRE(st == 0, SB_ERR_DEVICE_CHECK, "assembly: shared-memory staging did not complete");
     op.phys = ph;
     op.beta_re = beta_re;

@@ -44,6 +44,13 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
     }
 }
 
+
+// Gates: a kernel launched inside a captured Krylov cycle returns at once when its gate is
+// closed (the instance converged or the step needs no second Gram-Schmidt pass).
+__device__ __forceinline__ bool closed(Gate g) {
+    return (g.a && *g.a == 0) || (g.b && *g.b == 0);
+}
+
 // ---------------------------------------------------------------------------------------------
 // y = A x (complex128), or y = b - A x with per-CTA partial ||y||^2 when b != null.
 // ---------------------------------------------------------------------------------------------
@@ -52,7 +59,8 @@ __global__ void __launch_bounds__(THREADS) k_gemv_n_c128(const double2* __restri
                                                          const double2* __restrict__ x,
                                                          double2* __restrict__ y,
                                                          const double2* __restrict__ b,
-                                                         double* __restrict__ part) {
+                                                         double* __restrict__ part, Gate gate) {
+    if (closed(gate)) return;
     __shared__ double red[(THREADS / 32) * 2 * ROWS];
     const int64_t row0 = blockIdx.x * (int64_t)ROWS;
     const int nr = static_cast<int>((n - row0) < ROWS ? (n - row0) : ROWS);
@@ -145,7 +153,8 @@ __global__ void __launch_bounds__(THREADS) k_gemv_n_c64(const float2* __restrict
                                                         const void* __restrict__ xv_,
                                                         void* __restrict__ yv_,
                                                         const void* __restrict__ bv_,
-                                                        double* __restrict__ part) {
+                                                        double* __restrict__ part, Gate gate) {
+    if (closed(gate)) return;
     using Acc = typename std::conditional<X64, double, float>::type;
     __shared__ double red[(THREADS / 32) * 2 * ROWS];
     const int64_t row0 = blockIdx.x * (int64_t)ROWS;
@@ -153,7 +162,7 @@ __global__ void __launch_bounds__(THREADS) k_gemv_n_c64(const float2* __restrict
     Acc acc[2 * ROWS];
 #pragma unroll
     for (int r = 0; r < 2 * ROWS; ++r) acc[r] = 0;
-    const int64_t n2 = n >> 1;    // float4 = two complex64 entries
+    const int64_t n2 = n >> 1;     // float4 = two complex64 entries
     const int64_t ld2 = lda >> 1;  // lda is even, so every row starts 16-byte aligned
     const float4* A4 = reinterpret_cast<const float4*>(A + row0 * lda);
     int64_t c = threadIdx.x;
@@ -267,7 +276,8 @@ constexpr int kDotVecs = 8;
 template <class T>
 __global__ void __launch_bounds__(kDotRows) k_dots(const T* __restrict__ V, int64_t ldv, int k,
                                                    const T* __restrict__ w, int64_t n,
-                                                   double2* __restrict__ part) {
+                                                   double2* __restrict__ part, Gate gate) {
+    if (closed(gate)) return;
     __shared__ double red[(kDotRows / 32) * 2 * kDotVecs];
     const int64_t r = blockIdx.x * (int64_t)kDotRows + threadIdx.x;
     const int i0 = blockIdx.y * kDotVecs;
@@ -299,7 +309,8 @@ __global__ void __launch_bounds__(kDotRows) k_dots(const T* __restrict__ V, int6
 
 // out[i] = sum over chunks of part[c][i], i <= k (one warp per output).
 __global__ void k_reduce_part(const double2* __restrict__ part, int64_t chunks, int kp1,
-                              double2* __restrict__ out) {
+                              double2* __restrict__ out, Gate gate) {
+    if (closed(gate)) return;
     const int i = blockIdx.x;
     double sr = 0.0, si = 0.0;
     for (int64_t c = threadIdx.x; c < chunks; c += 32) {
@@ -317,8 +328,9 @@ template <class T>
 __global__ void __launch_bounds__(256) k_project(const T* __restrict__ V, int64_t ldv, int k,
                                                  const double2* __restrict__ coeff,
                                                  T* __restrict__ w, int64_t n,
-                                                 double* __restrict__ part) {
-    __shared__ double2 sc[128];
+                                                 double* __restrict__ part, Gate gate) {
+    if (closed(gate)) return;
+    __shared__ double2 sc[kMaxKrylov + 1];
     __shared__ double red[8];
     for (int t = threadIdx.x; t < k; t += blockDim.x) sc[t] = coeff[t];
     __syncthreads();
@@ -353,35 +365,41 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ V, int64_
     if (threadIdx.x == 0) part[blockIdx.x] = nr2[0];
 }
 
-__global__ void k_sum_real(const double* __restrict__ part, int64_t m, double* __restrict__ out) {
+__global__ void k_sum_real(const double* __restrict__ part, int64_t m, double* __restrict__ out,
+                           Gate gate) {
+    if (closed(gate)) return;
     double s = 0.0;
     for (int64_t c = threadIdx.x; c < m; c += 32) s += part[c];
     s = warp_sum(s);
     if (threadIdx.x == 0) *out = s;
 }
 
-// y = alpha * x (alpha real), with type conversion.
+// y = alpha * x with type conversion; alpha from the host, or *alpha_dev when given.
 template <class TI, class TO>
-__global__ void k_scale(const TI* __restrict__ x, double alpha, TO* __restrict__ y, int64_t n) {
+__global__ void k_scale(const TI* __restrict__ x, double alpha, const double* __restrict__ alpha_dev,
+                        TO* __restrict__ y, int64_t n, Gate gate) {
+    if (closed(gate)) return;
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r >= n) return;
+    const double a = alpha_dev ? *alpha_dev : alpha;
     TO o;
-    o.x = static_cast<double>(x[r].x) * alpha;
-    o.y = static_cast<double>(x[r].y) * alpha;
+    o.x = static_cast<double>(x[r].x) * a;
+    o.y = static_cast<double>(x[r].y) * a;
     y[r] = o;
 }
 
-// x += sum_i y_i V_i (y on device), x of type TX, V of type T; optional scale of the update.
+// x += alpha * sum_i y_i V_i (y on device), x of type TX, V of type T.
 template <class T, class TX>
-__global__ void k_update(const T* __restrict__ V, int64_t ldv, int k, const double2* __restrict__ yc,
-                         double alpha, TX* __restrict__ x, int64_t n) {
-    __shared__ double2 sc[128];
-    for (int t = threadIdx.x; t < k; t += blockDim.x) sc[t] = yc[t];
+__global__ void k_update(const T* __restrict__ V, int64_t ldv, int k, const int* __restrict__ k_dev,
+                         const double2* __restrict__ yc, double alpha, TX* __restrict__ x, int64_t n) {
+    __shared__ double2 sc[kMaxKrylov + 1];
+    const int kk = k_dev ? *k_dev : k;
+    for (int t = threadIdx.x; t < kk; t += blockDim.x) sc[t] = yc[t];
     __syncthreads();
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r >= n) return;
     double sr = 0.0, si = 0.0;
-    for (int i = 0; i < k; ++i) {
+    for (int i = 0; i < kk; ++i) {
         const double2 v = to_d(V[i * ldv + r]);
         sr += sc[i].x * v.x - sc[i].y * v.y;
         si += sc[i].x * v.y + sc[i].y * v.x;
@@ -395,7 +413,8 @@ __global__ void k_update(const T* __restrict__ V, int64_t ldv, int k, const doub
 // y = diag^-1 x (Jacobi), complex division with the FP64 diagonal.
 template <class T>
 __global__ void k_jacobi(const double2* __restrict__ d, const T* __restrict__ x, T* __restrict__ y,
-                         int64_t n) {
+                         int64_t n, Gate gate) {
+    if (closed(gate)) return;
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r >= n) return;
     const double2 a = d[r];
@@ -415,11 +434,12 @@ constexpr int kGemvThreads = 256;
 constexpr int kGemvUnroll = 2;
 
 void gemv_c128(const double2* A, int64_t n, const double2* x, double2* y, Trans t,
-               cudaStream_t s, DevBuf& scratch) {
+               cudaStream_t s, DevBuf& scratch, Gate gate) {
     ProfScope prof(SB_PROF_GEMV64, s);
     if (t == Trans::N) {
         k_gemv_n_c128<kGemvRows, kGemvThreads, kGemvUnroll>
-            <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, y, nullptr, nullptr); count_launch();
+            <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, y, nullptr, nullptr, gate);
+        count_launch();
         SB_CUDA(cudaGetLastError());
         return;
     }
@@ -436,97 +456,110 @@ void gemv_c128(const double2* A, int64_t n, const double2* x, double2* y, Trans 
         k_gemv_t_c128<true><<<grid, 256, 0, s>>>(A, n, x, scratch.as<double2>());
     count_launch();
     SB_CUDA(cudaGetLastError());
-    k_sum_chunks<<<cdiv(n, 256), 256, 0, s>>>(scratch.as<double2>(), n, chunks, y); count_launch();
+    k_sum_chunks<<<cdiv(n, 256), 256, 0, s>>>(scratch.as<double2>(), n, chunks, y);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 void gemv_residual_c128(const double2* A, int64_t n, const double2* x, const double2* b,
-                        double2* r, double* part, cudaStream_t s) {
+                        double2* r, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV64, s);
     k_gemv_n_c128<kGemvRows, kGemvThreads, kGemvUnroll>
-        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, r, b, part); count_launch();
+        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, r, b, part, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 int64_t gemv_partials(int64_t n) { return cdiv(n, kGemvRows); }
 
 void gemv_c64(const float2* A, int64_t n, int64_t lda, const float2* x, float2* y,
-              const float2* b, double* part, cudaStream_t s) {
+              const float2* b, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV32, s);
     k_gemv_n_c64<kGemvRows, kGemvThreads, kGemvUnroll, false>
-        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part); count_launch();
+        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 void gemv_c64_x64(const float2* A, int64_t n, int64_t lda, const double2* x, double2* y,
-                  const double2* b, double* part, cudaStream_t s) {
+                  const double2* b, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV32, s);
     k_gemv_n_c64<kGemvRows, kGemvThreads, kGemvUnroll, true>
-        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part); count_launch();
+        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 template <class T>
 void arnoldi_dots(const T* V, int64_t ldv, int k, const T* w, int64_t n, double2* part,
-                  double2* out, cudaStream_t s) {
+                  double2* out, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_ARNOLDI, s);
     const int64_t chunks = cdiv(n, kDotRows);
     dim3 grid(static_cast<unsigned>(chunks), static_cast<unsigned>(cdiv(k + 1, kDotVecs)));
-    k_dots<T><<<grid, kDotRows, 0, s>>>(V, ldv, k, w, n, part); count_launch();
+    k_dots<T><<<grid, kDotRows, 0, s>>>(V, ldv, k, w, n, part, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
-    k_reduce_part<<<k + 1, 32, 0, s>>>(part, chunks, k + 1, out); count_launch();
+    k_reduce_part<<<k + 1, 32, 0, s>>>(part, chunks, k + 1, out, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 int64_t arnoldi_dot_chunks(int64_t n) { return cdiv(n, kDotRows); }
 
 template <class T>
 void arnoldi_project(const T* V, int64_t ldv, int k, const double2* coeff, T* w, int64_t n,
-                     double* part, double* out_norm2, cudaStream_t s) {
+                     double* part, double* out_norm2, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_ARNOLDI, s);
     const int64_t nb = cdiv(n, 256);
-    k_project<T><<<nb, 256, 0, s>>>(V, ldv, k, coeff, w, n, part); count_launch();
+    k_project<T><<<nb, 256, 0, s>>>(V, ldv, k, coeff, w, n, part, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
-    k_sum_real<<<1, 32, 0, s>>>(part, nb, out_norm2); count_launch();
+    k_sum_real<<<1, 32, 0, s>>>(part, nb, out_norm2, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
-void sum_real(const double* part, int64_t m, double* out, cudaStream_t s) {
-    k_sum_real<<<1, 32, 0, s>>>(part, m, out); count_launch();
+void sum_real(const double* part, int64_t m, double* out, cudaStream_t s, Gate gate) {
+    k_sum_real<<<1, 32, 0, s>>>(part, m, out, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 template <class TI, class TO>
-void scale_vec(const TI* x, double alpha, TO* y, int64_t n, cudaStream_t s) {
-    k_scale<TI, TO><<<cdiv(n, 256), 256, 0, s>>>(x, alpha, y, n); count_launch();
+void scale_vec(const TI* x, double alpha, const double* alpha_dev, TO* y, int64_t n, cudaStream_t s,
+               Gate gate) {
+    k_scale<TI, TO><<<cdiv(n, 256), 256, 0, s>>>(x, alpha, alpha_dev, y, n, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 template <class T, class TX>
-void basis_update(const T* V, int64_t ldv, int k, const double2* y, double alpha, TX* x, int64_t n,
-                  cudaStream_t s) {
+void basis_update(const T* V, int64_t ldv, int k, const int* k_dev, const double2* y, double alpha,
+                  TX* x, int64_t n, cudaStream_t s) {
     ProfScope prof(SB_PROF_ARNOLDI, s);
-    k_update<T, TX><<<cdiv(n, 256), 256, 0, s>>>(V, ldv, k, y, alpha, x, n); count_launch();
+    k_update<T, TX><<<cdiv(n, 256), 256, 0, s>>>(V, ldv, k, k_dev, y, alpha, x, n);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 template <class T>
-void jacobi_apply(const double2* d, const T* x, T* y, int64_t n, cudaStream_t s) {
-    k_jacobi<T><<<cdiv(n, 256), 256, 0, s>>>(d, x, y, n); count_launch();
+void jacobi_apply(const double2* d, const T* x, T* y, int64_t n, cudaStream_t s, Gate gate) {
+    k_jacobi<T><<<cdiv(n, 256), 256, 0, s>>>(d, x, y, n, gate);
+    count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 // Explicit instantiations.
-template void arnoldi_dots<double2>(const double2*, int64_t, int, const double2*, int64_t, double2*, double2*, cudaStream_t);
-template void arnoldi_dots<float2>(const float2*, int64_t, int, const float2*, int64_t, double2*, double2*, cudaStream_t);
-template void arnoldi_project<double2>(const double2*, int64_t, int, const double2*, double2*, int64_t, double*, double*, cudaStream_t);
-template void arnoldi_project<float2>(const float2*, int64_t, int, const double2*, float2*, int64_t, double*, double*, cudaStream_t);
-template void scale_vec<double2, double2>(const double2*, double, double2*, int64_t, cudaStream_t);
-template void scale_vec<float2, float2>(const float2*, double, float2*, int64_t, cudaStream_t);
-template void scale_vec<double2, float2>(const double2*, double, float2*, int64_t, cudaStream_t);
-template void scale_vec<float2, double2>(const float2*, double, double2*, int64_t, cudaStream_t);
-template void basis_update<double2, double2>(const double2*, int64_t, int, const double2*, double, double2*, int64_t, cudaStream_t);
-template void basis_update<float2, float2>(const float2*, int64_t, int, const double2*, double, float2*, int64_t, cudaStream_t);
-template void basis_update<float2, double2>(const float2*, int64_t, int, const double2*, double, double2*, int64_t, cudaStream_t);
-template void jacobi_apply<double2>(const double2*, const double2*, double2*, int64_t, cudaStream_t);
-template void jacobi_apply<float2>(const double2*, const float2*, float2*, int64_t, cudaStream_t);
+template void arnoldi_dots<double2>(const double2*, int64_t, int, const double2*, int64_t, double2*, double2*, cudaStream_t, Gate);
+template void arnoldi_dots<float2>(const float2*, int64_t, int, const float2*, int64_t, double2*, double2*, cudaStream_t, Gate);
+template void arnoldi_project<double2>(const double2*, int64_t, int, const double2*, double2*, int64_t, double*, double*, cudaStream_t, Gate);
+template void arnoldi_project<float2>(const float2*, int64_t, int, const double2*, float2*, int64_t, double*, double*, cudaStream_t, Gate);
+template void scale_vec<double2, double2>(const double2*, double, const double*, double2*, int64_t, cudaStream_t, Gate);
+template void scale_vec<float2, float2>(const float2*, double, const double*, float2*, int64_t, cudaStream_t, Gate);
+template void scale_vec<double2, float2>(const double2*, double, const double*, float2*, int64_t, cudaStream_t, Gate);
+template void scale_vec<float2, double2>(const float2*, double, const double*, double2*, int64_t, cudaStream_t, Gate);
+template void basis_update<double2, double2>(const double2*, int64_t, int, const int*, const double2*, double, double2*, int64_t, cudaStream_t);
+template void basis_update<float2, float2>(const float2*, int64_t, int, const int*, const double2*, double, float2*, int64_t, cudaStream_t);
+template void basis_update<float2, double2>(const float2*, int64_t, int, const int*, const double2*, double, double2*, int64_t, cudaStream_t);
+template void jacobi_apply<double2>(const double2*, const double2*, double2*, int64_t, cudaStream_t, Gate);
+template void jacobi_apply<float2>(const double2*, const float2*, float2*, int64_t, cudaStream_t, Gate);
 
 }  // namespace sb

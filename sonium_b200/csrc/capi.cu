@@ -305,8 +305,9 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
     return guarded([&] {
         SB_REQUIRE(mesh && mesh->m && physics && out, SB_ERR_INVALID_ARGUMENT, "null argument");
         *out = nullptr;
-        SB_REQUIRE(precision == SB_PRECISION_FP64 || precision == SB_PRECISION_FP64_FP32, SB_ERR_INVALID_ARGUMENT,
-                   "unknown precision");
+        SB_REQUIRE(precision == SB_PRECISION_FP64 || precision == SB_PRECISION_FP64_FP32 ||
+                       precision == SB_PRECISION_FP32,
+                   SB_ERR_INVALID_ARGUMENT, "unknown precision");
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
         Mesh& m = *mesh->m;
@@ -320,8 +321,8 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
             op->n = m.n;
             op->lda32 = (m.n + 1) / 2 * 2;
             SB_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
-            op->A64.alloc(sizeof(double2) * m.n * m.n);
-            if (precision == SB_PRECISION_FP64_FP32) op->A32.alloc(sizeof(float2) * m.n * op->lda32);
+            if (precision != SB_PRECISION_FP32) op->A64.alloc(sizeof(double2) * m.n * m.n);
+            if (precision != SB_PRECISION_FP64) op->A32.alloc(sizeof(float2) * m.n * op->lda32);
             assemble(*op, *physics, beta.re, beta.im);
         } catch (...) {
             if (op->stream) cudaStreamDestroy(op->stream);
@@ -346,6 +347,7 @@ SB_API int sb_operator_destroy(sb_operator* op) {
         if (!op) return;
         if (op->op) {
             cudaSetDevice(op->op->device);
+            destroy_solve_work(*op->op);
             if (op->op->stream) cudaStreamDestroy(op->op->stream);
             delete op->op;
         }
@@ -371,7 +373,17 @@ SB_API int sb_operator_copy_to_host(const sb_operator* op, sb_complex* matrix, s
         const Operator& o = *op->op;
         SB_CUDA(cudaSetDevice(o.device));
         SB_CUDA(cudaStreamSynchronize(o.stream));
-        if (matrix) SB_CUDA(cudaMemcpy(matrix, o.A64.p, sizeof(double2) * o.n * o.n, cudaMemcpyDeviceToHost));
+        if (matrix && o.A64.p) {
+            SB_CUDA(cudaMemcpy(matrix, o.A64.p, sizeof(double2) * o.n * o.n, cudaMemcpyDeviceToHost));
+        } else if (matrix) {
+            // complex64-only operator: widen its entries
+            std::vector<float2> row(o.n);
+            for (int64_t i = 0; i < o.n; ++i) {
+                SB_CUDA(cudaMemcpy(row.data(), o.A32.as<float2>() + i * o.lda32, sizeof(float2) * o.n,
+                                   cudaMemcpyDeviceToHost));
+                for (int64_t j = 0; j < o.n; ++j) matrix[i * o.n + j] = sb_complex{row[j].x, row[j].y};
+            }
+        }
         if (rhs) SB_CUDA(cudaMemcpy(rhs, o.rhs.p, sizeof(double2) * o.n, cudaMemcpyDeviceToHost));
     });
 }
@@ -383,8 +395,17 @@ SB_API int sb_operator_copy_rows_to_host(const sb_operator* op, int64_t row0, in
         SB_REQUIRE(row0 >= 0 && row1 <= o.n && row0 <= row1, SB_ERR_INVALID_ARGUMENT, "row range out of bounds");
         SB_CUDA(cudaSetDevice(o.device));
         SB_CUDA(cudaStreamSynchronize(o.stream));
-        SB_CUDA(cudaMemcpy(rows, o.A64.as<double2>() + row0 * o.n, sizeof(double2) * (row1 - row0) * o.n,
-                           cudaMemcpyDeviceToHost));
+        if (o.A64.p) {
+            SB_CUDA(cudaMemcpy(rows, o.A64.as<double2>() + row0 * o.n, sizeof(double2) * (row1 - row0) * o.n,
+                               cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float2> row(o.n);
+            for (int64_t i = row0; i < row1; ++i) {
+                SB_CUDA(cudaMemcpy(row.data(), o.A32.as<float2>() + i * o.lda32, sizeof(float2) * o.n,
+                                   cudaMemcpyDeviceToHost));
+                for (int64_t j = 0; j < o.n; ++j) rows[(i - row0) * o.n + j] = sb_complex{row[j].x, row[j].y};
+            }
+        }
     });
 }
 
@@ -400,6 +421,17 @@ SB_API int sb_operator_copy_to_host_c64(const sb_operator* op, sb_complex32* mat
     });
 }
 
+// op(A) x with FP64 vectors; transposed products need the complex128 matrix.
+static void apply_any(Operator& o, Trans t, const double2* x, double2* y) {
+    if (t == Trans::N) {
+        op_gemv64(o, x, y, Gate{});
+        return;
+    }
+    SB_REQUIRE(o.A64.p, SB_ERR_INVALID_ARGUMENT,
+               "transposed products need the complex128 matrix (SB_PRECISION_FP64 or SB_PRECISION_FP64_FP32)");
+    gemv_c128(o.A64.as<double2>(), o.n, x, y, t, o.stream, o.scratch);
+}
+
 static Trans to_trans(int t) {
     SB_REQUIRE(t == SB_OP_N || t == SB_OP_T || t == SB_OP_C, SB_ERR_INVALID_ARGUMENT, "trans must be N, T or C");
     return static_cast<Trans>(t);
@@ -411,8 +443,7 @@ SB_API int sb_operator_apply_device(const sb_operator* op, int trans, const sb_c
         Operator& o = *op->op;
         SB_CUDA(cudaSetDevice(o.device));
         maybe_inject(SB_INJECT_LAUNCH);
-        gemv_c128(o.A64.as<double2>(), o.n, reinterpret_cast<const double2*>(x_dev), reinterpret_cast<double2*>(y_dev),
-                  to_trans(trans), o.stream, o.scratch);
+        apply_any(o, to_trans(trans), reinterpret_cast<const double2*>(x_dev), reinterpret_cast<double2*>(y_dev));
         SB_CUDA(cudaStreamSynchronize(o.stream));
     });
 }
@@ -429,7 +460,7 @@ SB_API int sb_operator_apply(const sb_operator* op, int trans, const sb_complex*
         dx.alloc(sizeof(double2) * o.n);
         dy.alloc(sizeof(double2) * o.n);
         SB_CUDA(cudaMemcpyAsync(dx.p, x, sizeof(double2) * o.n, cudaMemcpyHostToDevice, o.stream));
-        gemv_c128(o.A64.as<double2>(), o.n, dx.as<double2>(), dy.as<double2>(), t, o.stream, o.scratch);
+        apply_any(o, t, dx.as<double2>(), dy.as<double2>());
         SB_CUDA(cudaMemcpyAsync(y, dy.p, sizeof(double2) * o.n, cudaMemcpyDeviceToHost, o.stream));
         SB_CUDA(cudaStreamSynchronize(o.stream));
         SB_REQUIRE(all_finite(y, o.n), SB_ERR_NOT_FINITE, "apply: non-finite output vector");
@@ -452,7 +483,7 @@ SB_API int sb_operator_apply_block(const sb_operator* op, const sb_complex* X, s
         for (int64_t q = 0; q < r; ++q) {
             for (int64_t i = 0; i < n; ++i) col[i] = X[i * r + q];
             SB_CUDA(cudaMemcpyAsync(dx.p, col.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, o.stream));
-            gemv_c128(o.A64.as<double2>(), n, dx.as<double2>(), dy.as<double2>(), Trans::N, o.stream, o.scratch);
+            apply_any(o, Trans::N, dx.as<double2>(), dy.as<double2>());
             SB_CUDA(cudaMemcpyAsync(col.data(), dy.p, sizeof(double2) * n, cudaMemcpyDeviceToHost, o.stream));
             SB_CUDA(cudaStreamSynchronize(o.stream));
             for (int64_t i = 0; i < n; ++i) Y[i * r + q] = col[i];

@@ -1,69 +1,306 @@
-// Restarted GMRES and mixed-precision iterative refinement drivers (host side, device vectors).
+// Restarted GMRES and mixed-precision iterative refinement with device-resident Arnoldi cycles.
 //
 // Reference: gmres_core (crates/sonium-solvers/crates/sonium-solvers-iterative/src/gmres.rs:631-1047)
 // with finalize_gmres_solution (gmres.rs:159-247), givens_rotation / solve_upper_triangular
 // (gmres_common.rs:91-127) and the CGS + DGKS (0.707) orthogonalisation of cgs_orth.rs:180-300.
-// The Krylov basis, the matvec and the Gram-Schmidt passes stay on the device; the (m+1) x m
-// Hessenberg matrix, the Givens rotations and the triangular solve stay on the host in FP64, fed
-// by one small device-to-host copy per Arnoldi step.
+//
+// One restart cycle is a fixed sequence of kernels per Arnoldi step: matvec, Gram-Schmidt dots
+// and projection, a single-thread FP64 kernel that fills the Hessenberg column, applies the
+// Givens rotations and tests convergence, the optional DGKS second pass, and the normalisation of
+// the next basis vector. Every kernel of the cycle is gated by the instance's `active` flag, so
+// the whole cycle is captured once as a CUDA graph and replayed: after convergence the rest of
+// the cycle costs only empty launches, and the host synchronises twice per cycle (initial
+// residual, then true residual after the update) instead of once per step. The arithmetic and the
+// decisions (DGKS threshold, convergence tests, restart / breakdown logic) are the reference's.
 
 #include <complex>
 #include <functional>
 
 #include "sb_blas.cuh"
 #include "sb_internal.cuh"
+#include "sb_profile.cuh"
 
 namespace sb {
 
 using cd = std::complex<double>;
 
+// Device state of one Arnoldi cycle.
+struct KState {
+    int active;     // the cycle is still running
+    int reorth;     // the current step needs the DGKS second pass
+    int jdone;      // Arnoldi steps taken in this cycle
+    int reason;     // 0 = m steps completed, 1 = estimated convergence, 2 = inner breakdown
+    int m, interval;
+    double pbnorm, tol;
+    double wnb, wn, inv_wn;
+    double absres, relres;
+};
+
 namespace {
+
+__device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
+__device__ __forceinline__ double2 cconj_mul(double2 a, double2 b) {  // conj(a) * b
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double2 cmul_(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 csub_(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cadd_(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+__global__ void k_cycle_init(KState* __restrict__ st, double2* __restrict__ H, double2* __restrict__ g,
+                             int m, int interval, double beta, double pbnorm, double tol) {
+    const int64_t tot = (int64_t)(m + 1) * m;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x)
+        H[t] = make_double2(0.0, 0.0);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= m; t += gridDim.x * blockDim.x)
+        g[t] = make_double2(t == 0 ? beta : 0.0, 0.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->active = 1;
+        st->reorth = 0;
+        st->jdone = 0;
+        st->reason = 0;
+        st->m = m;
+        st->interval = interval < 1 ? 1 : interval;
+        st->pbnorm = pbnorm;
+        st->tol = tol;
+        st->wn = st->wnb = st->inv_wn = 0.0;
+        st->absres = st->relres = 0.0;
+    }
+}
+
+// After the first Gram-Schmidt pass: Hessenberg column j and the DGKS decision.
+__global__ void k_after_first(KState* __restrict__ st, const double2* __restrict__ red,
+                              const double* __restrict__ nrm, double2* __restrict__ H, int j) {
+    if (!st->active) return;
+    const int m = st->m;
+    for (int i = 0; i <= j; ++i) H[i * m + j] = red[i];
+    const double wnb = sqrt(red[j + 1].x);
+    const double wn = sqrt(*nrm);
+    st->wnb = wnb;
+    st->wn = wn;
+    st->reorth = wn < 0.707 * wnb ? 1 : 0;
+}
+
+// givens_rotation (gmres_common.rs:91-106).
+__device__ void givens_(double2 a, double2 b, double2& c, double2& s) {
+    const double tol = 1e-30;
+    if (cabs_(b) < tol) {
+        c = make_double2(1.0, 0.0);
+        s = make_double2(0.0, 0.0);
+        return;
+    }
+    if (cabs_(a) < tol) {
+        c = make_double2(0.0, 0.0);
+        s = make_double2(1.0, 0.0);
+        return;
+    }
+    const double r = sqrt((a.x * a.x + a.y * a.y) + (b.x * b.x + b.y * b.y));
+    const double ir = 1.0 / r;
+    c = make_double2(a.x * ir, a.y * ir);
+    s = make_double2(b.x * ir, b.y * ir);
+}
+
+// Second-pass update, Hessenberg subdiagonal, rotations and the convergence test of step j
+// (gmres.rs:818-900).
+__global__ void k_givens(KState* __restrict__ st, const double2* __restrict__ red2,
+                         const double* __restrict__ nrm2, double2* __restrict__ H,
+                         double2* __restrict__ cs, double2* __restrict__ sn, double2* __restrict__ g,
+                         int j) {
+    if (!st->active) return;
+    const int m = st->m;
+    if (st->reorth) {
+        for (int i = 0; i <= j; ++i) H[i * m + j] = cadd_(H[i * m + j], red2[i]);
+        st->wn = sqrt(*nrm2);
+    }
+    const double wn = st->wn;
+    H[(j + 1) * m + j] = make_double2(wn, 0.0);
+    const bool inner = wn < 1e-20;
+    st->inv_wn = inner ? 0.0 : 1.0 / wn;
+    for (int i = 0; i < j; ++i) {
+        const double2 hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
+        const double2 t = cadd_(cconj_mul(cs[i], hij), cconj_mul(sn[i], hi1));
+        H[(i + 1) * m + j] = csub_(cmul_(cs[i], hi1), cmul_(sn[i], hij));
+        H[i * m + j] = t;
+    }
+    double2 c, s;
+    givens_(H[j * m + j], H[(j + 1) * m + j], c, s);
+    cs[j] = c;
+    sn[j] = s;
+    H[j * m + j] = cadd_(cconj_mul(c, H[j * m + j]), cconj_mul(s, H[(j + 1) * m + j]));
+    H[(j + 1) * m + j] = make_double2(0.0, 0.0);
+    const double2 t = cadd_(cconj_mul(c, g[j]), cconj_mul(s, g[j + 1]));
+    g[j + 1] = csub_(cmul_(c, g[j + 1]), cmul_(s, g[j]));
+    g[j] = t;
+    const double absr = cabs_(g[j + 1]);
+    const double relr = absr / st->pbnorm;
+    const bool should_check = (j % st->interval) == 0 || j == m - 1 || inner;
+    const bool conv = relr < st->tol || (!inner && absr < 1e-20);
+    st->jdone = j + 1;
+    st->absres = absr;
+    st->relres = relr;
+    if (should_check && conv) {
+        st->active = 0;
+        st->reason = 1;
+    } else if (inner) {
+        st->active = 0;
+        st->reason = 2;
+    } else if (j == m - 1) {
+        st->active = 0;
+        st->reason = 0;
+    }
+}
+
+// solve_upper_triangular (gmres_common.rs:109-127) for the jdone x jdone leading block.
+__global__ void k_upper_solve(const KState* __restrict__ st, const double2* __restrict__ H,
+                              const double2* __restrict__ g, double2* __restrict__ y) {
+    const int m = st->m, k = st->jdone;
+    for (int i = k - 1; i >= 0; --i) {
+        double2 s = g[i];
+        for (int j = i + 1; j < k; ++j) s = csub_(s, cmul_(H[i * m + j], y[j]));
+        const double2 h = H[i * m + i];
+        if (cabs_(h) > 1e-30) {
+            const double d = h.x * h.x + h.y * h.y;
+            const double2 inv = make_double2(h.x / d, -h.y / d);
+            y[i] = cmul_(s, inv);
+        } else {
+            y[i] = make_double2(0.0, 0.0);
+        }
+    }
+}
 
 struct PinnedBuf {
     void* p = nullptr;
-    explicit PinnedBuf(size_t bytes) { SB_CUDA(cudaMallocHost(&p, bytes)); }
+    void alloc(size_t bytes) {
+        if (p) return;
+        SB_CUDA(cudaMallocHost(&p, bytes));
+    }
     ~PinnedBuf() {
         if (p) cudaFreeHost(p);
     }
-    template <class T>
-    T* as() const {
-        return static_cast<T*>(p);
+};
+
+}  // namespace
+
+// Persistent per-operator workspace of one vector type.
+template <class T>
+struct KrylovWork {
+    int64_t n = 0, m = 0, ldv = 0;
+    DevBuf V, w, opb, r, part, red, red2, nrm, ydev, H, cs, sn, g, st;
+    PinnedBuf host;  // KState + two doubles
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void* key_A = nullptr;
+    int key_jacobi = -1;
+    bool key_prof = false;
+    std::vector<ProfPair> prof_pairs;
+    int64_t graph_kernels = 0;
+
+    void reset_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        profile_release(prof_pairs);
+    }
+    ~KrylovWork() { reset_graph(); }
+
+    void ensure(int64_t n_, int64_t m_) {
+        if (n_ == n && m_ == m) return;
+        reset_graph();
+        n = n_;
+        m = m_;
+        ldv = (n + 1) / 2 * 2;  // even: every basis vector 16-byte aligned for vector loads
+        V.alloc(sizeof(T) * (m + 1) * ldv);
+        w.alloc(sizeof(T) * ldv);
+        opb.alloc(sizeof(T) * ldv);
+        r.alloc(sizeof(T) * ldv);
+        const int64_t dchunks = arnoldi_dot_chunks(n);
+        part.alloc(sizeof(double2) * std::max<int64_t>(dchunks * (m + 2), (n + 255) / 256 + gemv_partials(n)));
+        red.alloc(sizeof(double2) * (m + 2));
+        red2.alloc(sizeof(double2) * (m + 2));
+        nrm.alloc(sizeof(double) * 4);
+        ydev.alloc(sizeof(double2) * (m + 1));
+        H.alloc(sizeof(double2) * (m + 1) * m);
+        cs.alloc(sizeof(double2) * m);
+        sn.alloc(sizeof(double2) * m);
+        g.alloc(sizeof(double2) * (m + 1));
+        st.alloc(sizeof(KState));
+        host.alloc(sizeof(KState) + 64);
+    }
+    KState* hstate() { return static_cast<KState*>(host.p); }
+    double* hscalar() { return reinterpret_cast<double*>(static_cast<char*>(host.p) + sizeof(KState)); }
+};
+
+struct SolveWork {
+    KrylovWork<double2> k64;
+    KrylovWork<float2> k32;
+    DevBuf r64, r32, d32, partg, nrmg, one, ax;
+    PinnedBuf pin;
+    DevBuf npart, nred;  // scratch of the ||b|| reduction
+    int64_t n = 0;
+    double2* k64_part(int64_t) { return npart.as<double2>(); }
+    double2* k64_red() { return nred.as<double2>(); }
+    void ensure(int64_t n_) {
+        if (n_ == n) return;
+        n = n_;
+        pin.alloc(64);
+        npart.alloc(sizeof(double2) * arnoldi_dot_chunks(n));
+        nred.alloc(sizeof(double2) * 2);
+        r64.alloc(sizeof(double2) * n);
+        r32.alloc(sizeof(float2) * n);
+        d32.alloc(sizeof(float2) * n);
+        partg.alloc(sizeof(double) * gemv_partials(n));
+        nrmg.alloc(sizeof(double) * 2);
+        one.alloc(sizeof(double2));
+        const double2 h_one = make_double2(1.0, 0.0);
+        SB_CUDA(cudaMemcpy(one.p, &h_one, sizeof(double2), cudaMemcpyHostToDevice));
+        ax.alloc(sizeof(double2) * n);
     }
 };
 
-void givens(cd a, cd b, cd& c, cd& s) {
-    const double tol = 1e-30;
-    if (std::abs(b) < tol) {
-        c = 1.0;
-        s = 0.0;
-        return;
+void destroy_solve_work(Operator& op) {
+    if (op.work) {
+        cudaSetDevice(op.device);
+        delete static_cast<SolveWork*>(op.work);
+        op.work = nullptr;
     }
-    if (std::abs(a) < tol) {
-        c = 0.0;
-        s = 1.0;
-        return;
-    }
-    const double r = std::sqrt(std::norm(a) + std::norm(b));
-    c = a * (1.0 / r);
-    s = b * (1.0 / r);
 }
 
-std::vector<cd> upper_solve(const std::vector<cd>& h, int64_t ld, const std::vector<cd>& g, int64_t k) {
-    std::vector<cd> y(k, cd(0, 0));
-    for (int64_t i = k - 1; i >= 0; --i) {
-        cd s = g[i];
-        for (int64_t j = i + 1; j < k; ++j) s -= h[i * ld + j] * y[j];
-        if (std::abs(h[i * ld + i]) > 1e-30) y[i] = s * (1.0 / h[i * ld + i]);
-    }
-    return y;
+static SolveWork& solve_work(const Operator& op) {
+    Operator& o = const_cast<Operator&>(op);
+    if (!o.work) o.work = new SolveWork();
+    SolveWork& w = *static_cast<SolveWork*>(o.work);
+    w.ensure(op.n);
+    return w;
 }
 
-// Device operator callbacks of one GMRES instance.
+// y = A x with FP64 vectors: the complex128 matrix when present, else the complex64 one with
+// FP64 accumulation.
+void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g) {
+    if (op.A64.p)
+        gemv_c128(op.A64.as<double2>(), op.n, x, y, Trans::N, op.stream, const_cast<Operator&>(op).scratch, g);
+    else
+        gemv_c64_x64(op.A32.as<float2>(), op.n, op.lda32, x, y, nullptr, nullptr, op.stream, g);
+}
+
+// r = b - A x with FP64 vectors and per-CTA partial norms (gemv_partials(n) entries).
+void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part) {
+    if (op.A64.p)
+        gemv_residual_c128(op.A64.as<double2>(), op.n, x, b, r, part, op.stream);
+    else
+        gemv_c64_x64(op.A32.as<float2>(), op.n, op.lda32, x, r, b, part, op.stream);
+}
+
+namespace {
+
+// Device operator callbacks of one GMRES problem.
 template <class T>
 struct Problem {
     int64_t n = 0;
-    std::function<void(const T*, T*)> apply;                    // y = A x
-    std::function<double(const T*, const T*, T*)> residual;     // r = b - A x, returns ||r||
+    const void* key_A = nullptr;                                // identifies the captured graph
+    std::function<void(const T*, T*, Gate)> apply;              // y = A x (gated)
+    std::function<void(const T*, const T*, T*, double*)> residual;  // r = b - A x, partials
     const double2* jacobi = nullptr;                            // diagonal for Jacobi, or null
     cudaStream_t stream = nullptr;
 };
@@ -75,77 +312,122 @@ struct CoreResult {
     int status = SB_SOLVER_MAX_ITERATIONS;
 };
 
-// gmres_core (gmres.rs:631-1047) with an identity or Jacobi left preconditioner.
+// All Arnoldi steps of one cycle, every launch gated by st->active.
 template <class T>
-CoreResult gmres_core(const Problem<T>& P, const T* b, T* x, int64_t max_it, int64_t m,
-                      double tol, int64_t check_interval) {
+void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
     const int64_t n = P.n;
     const cudaStream_t s = P.stream;
+    KState* st = W.st.template as<KState>();
+    const Gate ga{&st->active, nullptr};
+    const Gate gb{&st->active, &st->reorth};
+    T* Vp = W.V.template as<T>();
+    T* w = W.w.template as<T>();
+    double* nrm = W.nrm.template as<double>();
+    for (int64_t j = 0; j < m; ++j) {
+        capture_step(static_cast<int>(j));
+        const int k = static_cast<int>(j + 1);
+        if (P.jacobi) {
+            P.apply(Vp + j * W.ldv, W.opb.template as<T>(), ga);
+            jacobi_apply<T>(P.jacobi, W.opb.template as<T>(), w, n, s, ga);
+        } else {
+            P.apply(Vp + j * W.ldv, w, ga);
+        }
+        arnoldi_dots<T>(Vp, W.ldv, k, w, n, W.part.template as<double2>(), W.red.template as<double2>(), s, ga);
+        arnoldi_project<T>(Vp, W.ldv, k, W.red.template as<double2>(), w, n, W.part.template as<double>(), nrm, s, ga);
+        k_after_first<<<1, 1, 0, s>>>(st, W.red.template as<double2>(), nrm, W.H.template as<double2>(), static_cast<int>(j));
+        count_launch();
+        arnoldi_dots<T>(Vp, W.ldv, k, w, n, W.part.template as<double2>(), W.red2.template as<double2>(), s, gb);
+        arnoldi_project<T>(Vp, W.ldv, k, W.red2.template as<double2>(), w, n, W.part.template as<double>(), nrm + 1,
+                           s, gb);
+        k_givens<<<1, 1, 0, s>>>(st, W.red2.template as<double2>(), nrm + 1, W.H.template as<double2>(),
+                                 W.cs.template as<double2>(), W.sn.template as<double2>(), W.g.template as<double2>(),
+                                 static_cast<int>(j));
+        count_launch();
+        scale_vec<T, T>(w, 0.0, &st->inv_wn, Vp + (j + 1) * W.ldv, n, s, ga);
+    }
+    SB_CUDA(cudaGetLastError());
+}
+
+// Replays the captured cycle (capturing it first when buffers, matrix or profiling changed).
+template <class T>
+void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
+    const int jac = P.jacobi ? 1 : 0;
+    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_prof != g_prof_on) {
+        W.reset_graph();
+        const int64_t before = kernel_count();
+        capture_begin(&W.prof_pairs);
+        SB_CUDA(cudaStreamBeginCapture(P.stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            launch_cycle<T>(W, P, m);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(P.stream, &g);
+            if (g) cudaGraphDestroy(g);
+            capture_end();
+            throw;
+        }
+        SB_CUDA(cudaStreamEndCapture(P.stream, &W.graph));
+        capture_end();
+        SB_CUDA(cudaGraphInstantiate(&W.exec, W.graph, 0));
+        W.graph_kernels = kernel_count() - before;
+        add_kernel_count(-W.graph_kernels);
+        W.key_A = P.key_A;
+        W.key_jacobi = jac;
+        W.key_prof = g_prof_on;
+    }
+    SB_CUDA(cudaGraphLaunch(W.exec, P.stream));
+    add_kernel_count(W.graph_kernels);
+}
+
+// gmres_core (gmres.rs:631-1047) with an identity or Jacobi left preconditioner.
+template <class T>
+CoreResult gmres_core(KrylovWork<T>& W, const Problem<T>& P, const T* b, T* x, int64_t max_it,
+                      int64_t m, double tol, int64_t check_interval) {
+    const int64_t n = P.n;
+    const cudaStream_t s = P.stream;
+    W.ensure(n, m);
     CoreResult R;
-    DevBuf V, w, opb, r, part, red, red2, nrm, ydev;
-    // Even leading dimension: every basis vector starts 16-byte aligned, which the vectorised
-    // complex64 matvec needs for its two-entry loads of x.
-    const int64_t ldv = (n + 1) / 2 * 2;
-    V.alloc(sizeof(T) * (m + 1) * ldv);
-    w.alloc(sizeof(T) * n);
-    opb.alloc(sizeof(T) * n);
-    r.alloc(sizeof(T) * n);
-    const int64_t dchunks = arnoldi_dot_chunks(n);
-    part.alloc(sizeof(double2) * std::max<int64_t>(dchunks * (m + 2), (n + 255) / 256 + gemv_partials(n)));
-    red.alloc(sizeof(double2) * (m + 2));
-    red2.alloc(sizeof(double2) * (m + 2));
-    nrm.alloc(sizeof(double) * 2);
-    ydev.alloc(sizeof(double2) * (m + 1));
-    PinnedBuf host(sizeof(double2) * (m + 4));
-    double2* hbuf = host.as<double2>();
-    T* Vp = V.as<T>();
-    auto Vj = [&](int64_t j) { return Vp + j * ldv; };
-
+    KState* hst = W.hstate();
+    double* hsc = W.hscalar();
+    double* nrm = W.nrm.template as<double>();
+    double* partd = W.part.template as<double>();
     auto norm_of = [&](const T* v) -> double {
-        arnoldi_dots<T>(v, n, 0, v, n, part.as<double2>(), red2.as<double2>(), s);
-        SB_CUDA(cudaMemcpyAsync(hbuf, red2.p, sizeof(double2), cudaMemcpyDeviceToHost, s));
+        arnoldi_dots<T>(v, n, 0, v, n, W.part.template as<double2>(), W.red2.template as<double2>(), s);
+        SB_CUDA(cudaMemcpyAsync(hsc, W.red2.p, sizeof(double), cudaMemcpyDeviceToHost, s));
         SB_CUDA(cudaStreamSynchronize(s));
-        return std::sqrt(hbuf[0].x);
+        return std::sqrt(hsc[0]);
     };
-    auto precond = [&](const T* in, T* out) {
-        if (P.jacobi) jacobi_apply<T>(P.jacobi, in, out, n, s);
-        else if (in != out) SB_CUDA(cudaMemcpyAsync(out, in, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
-    };
-    auto true_rel = [&](double bnorm) {
+    auto residual = [&](T* out, bool with_state) -> double {
+        P.residual(x, b, out, partd);
+        sum_real(partd, gemv_partials(n), nrm + 2, s);
+        SB_CUDA(cudaMemcpyAsync(hsc, nrm + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (with_state) SB_CUDA(cudaMemcpyAsync(hst, W.st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
         ++R.matvecs;
-        return P.residual(x, b, r.as<T>()) / bnorm;
+        return std::sqrt(hsc[0]);
     };
-    auto update_x = [&](const std::vector<cd>& y) {
-        for (size_t i = 0; i < y.size(); ++i) hbuf[i] = make_double2(y[i].real(), y[i].imag());
-        SB_CUDA(cudaMemcpyAsync(ydev.p, hbuf, sizeof(double2) * y.size(), cudaMemcpyHostToDevice, s));
-        basis_update<T, T>(Vp, ldv, static_cast<int>(y.size()), ydev.as<double2>(), 1.0, x, n, s);
-        SB_CUDA(cudaStreamSynchronize(s));
-    };
-
     const double raw_bn = norm_of(b);
     const bool rhs_zero = raw_bn < 1e-15;
     const double bnorm = rhs_zero ? 1.0 : raw_bn;
     double pbnorm = bnorm;
     if (P.jacobi) {
-        precond(b, w.as<T>());
-        const double raw_pb = norm_of(w.as<T>());
+        jacobi_apply<T>(P.jacobi, b, W.w.template as<T>(), n, s);
+        const double raw_pb = norm_of(W.w.template as<T>());
         if (!rhs_zero && raw_pb < 1e-15) {
             R.status = SB_SOLVER_BREAKDOWN;
             return R;
         }
         pbnorm = rhs_zero ? 1.0 : raw_pb;
     }
-    std::vector<cd> H((m + 1) * m), cs, sn, g(m + 1);
     for (int64_t outer = 0; outer < max_it; ++outer) {
-        ++R.matvecs;
-        const double rn = P.residual(x, b, opb.as<T>());
+        const double rn = residual(W.opb.template as<T>(), false);
         const double trel = rn / bnorm;
         double beta = rn;
+        const T* src = W.opb.template as<T>();
         if (P.jacobi) {
-            precond(opb.as<T>(), w.as<T>());
-            beta = norm_of(w.as<T>());
-        } else {
-            SB_CUDA(cudaMemcpyAsync(w.p, opb.p, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+            jacobi_apply<T>(P.jacobi, W.opb.template as<T>(), W.w.template as<T>(), n, s);
+            beta = norm_of(W.w.template as<T>());
+            src = W.w.template as<T>();
         }
         const double rel = beta / pbnorm;
         if (rel < tol && trel < tol) {
@@ -161,91 +443,41 @@ CoreResult gmres_core(const Problem<T>& P, const T* b, T* x, int64_t max_it, int
             R.residual = trel;
             return R;
         }
-        scale_vec<T, T>(w.as<T>(), 1.0 / beta, Vj(0), n, s);
-        std::fill(H.begin(), H.end(), cd(0, 0));
-        cs.clear();
-        sn.clear();
-        std::fill(g.begin(), g.end(), cd(0, 0));
-        g[0] = beta;
-        bool restart_now = false;
-        for (int64_t j = 0; j < m; ++j) {
-            ++R.iterations;
-            ++R.matvecs;
-            if (P.jacobi) {
-                P.apply(Vj(j), opb.as<T>());
-                precond(opb.as<T>(), w.as<T>());
-            } else {
-                P.apply(Vj(j), w.as<T>());
+        scale_vec<T, T>(src, 1.0 / beta, nullptr, W.V.template as<T>(), n, s);
+        k_cycle_init<<<8, 256, 0, s>>>(W.st.template as<KState>(), W.H.template as<double2>(),
+                                       W.g.template as<double2>(), static_cast<int>(m),
+                                       static_cast<int>(check_interval), beta, pbnorm, tol);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        run_cycle<T>(W, P, m);
+        k_upper_solve<<<1, 1, 0, s>>>(W.st.template as<KState>(), W.H.template as<double2>(),
+                                      W.g.template as<double2>(), W.ydev.template as<double2>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        basis_update<T, T>(W.V.template as<T>(), W.ldv, 0, &W.st.template as<KState>()->jdone,
+                           W.ydev.template as<double2>(), 1.0, x, n, s);
+        const double tr = residual(W.r.template as<T>(), true) / bnorm;
+        profile_account(W.prof_pairs, hst->jdone);
+        R.iterations += hst->jdone;
+        R.matvecs += hst->jdone;
+        if (hst->reason == 1) {
+            if (tr >= tol && tr >= 1e-20) {
+                ++R.restarts;
+                continue;
             }
-            const int k = static_cast<int>(j + 1);
-            arnoldi_dots<T>(Vp, ldv, k, w.as<T>(), n, part.as<double2>(), red.as<double2>(), s);
-            arnoldi_project<T>(Vp, ldv, k, red.as<double2>(), w.as<T>(), n, reinterpret_cast<double*>(part.p),
-                               nrm.as<double>(), s);
-            SB_CUDA(cudaMemcpyAsync(hbuf, red.p, sizeof(double2) * (k + 1), cudaMemcpyDeviceToHost, s));
-            SB_CUDA(cudaMemcpyAsync(hbuf + m + 2, nrm.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-            SB_CUDA(cudaStreamSynchronize(s));
-            const double wnb = std::sqrt(hbuf[k].x);
-            double wn = std::sqrt(hbuf[m + 2].x);
-            for (int i = 0; i < k; ++i) H[i * m + j] = cd(hbuf[i].x, hbuf[i].y);
-            if (wn < 0.707 * wnb) {
-                arnoldi_dots<T>(Vp, ldv, k, w.as<T>(), n, part.as<double2>(), red2.as<double2>(), s);
-                arnoldi_project<T>(Vp, ldv, k, red2.as<double2>(), w.as<T>(), n,
-                                   reinterpret_cast<double*>(part.p), nrm.as<double>(), s);
-                SB_CUDA(cudaMemcpyAsync(hbuf, red2.p, sizeof(double2) * k, cudaMemcpyDeviceToHost, s));
-                SB_CUDA(cudaMemcpyAsync(hbuf + m + 2, nrm.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-                SB_CUDA(cudaStreamSynchronize(s));
-                for (int i = 0; i < k; ++i) H[i * m + j] += cd(hbuf[i].x, hbuf[i].y);
-                wn = std::sqrt(hbuf[m + 2].x);
-            }
-            H[(j + 1) * m + j] = wn;
-            bool inner_conv = false;
-            if (wn < 1e-20) inner_conv = true;
-            else scale_vec<T, T>(w.as<T>(), 1.0 / wn, Vj(j + 1), n, s);
-            for (int64_t i = 0; i < j; ++i) {
-                const cd t = std::conj(cs[i]) * H[i * m + j] + std::conj(sn[i]) * H[(i + 1) * m + j];
-                H[(i + 1) * m + j] = cd(0, 0) - sn[i] * H[i * m + j] + cs[i] * H[(i + 1) * m + j];
-                H[i * m + j] = t;
-            }
-            cd c, sg;
-            givens(H[j * m + j], H[(j + 1) * m + j], c, sg);
-            cs.push_back(c);
-            sn.push_back(sg);
-            H[j * m + j] = std::conj(c) * H[j * m + j] + std::conj(sg) * H[(j + 1) * m + j];
-            H[(j + 1) * m + j] = 0.0;
-            const cd t = std::conj(c) * g[j] + std::conj(sg) * g[j + 1];
-            g[j + 1] = cd(0, 0) - sg * g[j] + c * g[j + 1];
-            g[j] = t;
-            const double absr = std::abs(g[j + 1]);
-            const double relr = absr / pbnorm;
-            const bool should_check = (j % std::max<int64_t>(check_interval, 1)) == 0 || j == m - 1 || inner_conv;
-            const bool conv = relr < tol || (!inner_conv && absr < 1e-20);
-            if (should_check && conv) {
-                update_x(upper_solve(H, m, g, j + 1));
-                const double tr = true_rel(bnorm);
-                if (tr >= tol && tr >= 1e-20) {
-                    ++R.restarts;
-                    restart_now = true;
-                    break;
-                }
-                R.converged = true;
-                R.status = SB_SOLVER_CONVERGED;
-                R.estimated = relr;
-                R.residual = tr;
-                return R;
-            }
-            if (inner_conv) {
-                update_x(upper_solve(H, m, g, j + 1));
-                const double ar = true_rel(bnorm);
-                R.estimated = relr;
-                R.residual = ar;
-                R.converged = ar < tol;
-                R.status = R.converged ? SB_SOLVER_CONVERGED : SB_SOLVER_BREAKDOWN;
-                return R;
-            }
+            R.converged = true;
+            R.status = SB_SOLVER_CONVERGED;
+            R.estimated = hst->relres;
+            R.residual = tr;
+            return R;
         }
-        if (restart_now) continue;
-        update_x(upper_solve(H, m, g, m));
-        const double tr = true_rel(bnorm);
+        if (hst->reason == 2) {
+            R.estimated = hst->relres;
+            R.residual = tr;
+            R.converged = tr < tol;
+            R.status = R.converged ? SB_SOLVER_CONVERGED : SB_SOLVER_BREAKDOWN;
+            return R;
+        }
         if (tr < tol) {
             R.converged = true;
             R.status = SB_SOLVER_CONVERGED;
@@ -255,26 +487,20 @@ CoreResult gmres_core(const Problem<T>& P, const T* b, T* x, int64_t max_it, int
         }
         ++R.restarts;
     }
-    R.residual = true_rel(bnorm);
+    R.residual = residual(W.r.template as<T>(), false) / bnorm;
     R.estimated = R.residual;
     R.status = SB_SOLVER_MAX_ITERATIONS;
     return R;
 }
 
 // finalize_gmres_solution (gmres.rs:159-247): residual and backward error from one more product.
-void finalize(const Operator& op, const double2* b, const double2* x, sb_gmres_stats& st,
-              double tol) {
+void finalize(const Operator& op, SolveWork& sw, const double2* b, const double2* x, sb_gmres_stats& st) {
     const int64_t n = op.n;
-    DevBuf ax, part, sums;
-    ax.alloc(sizeof(double2) * n);
-    part.alloc(sizeof(double2) * (n + 255) / 256 * 4 + 64);
-    gemv_c128(op.A64.as<double2>(), n, x, ax.as<double2>(), Trans::N, op.stream,
-              const_cast<Operator&>(op).scratch);
+    op_gemv64(op, x, sw.ax.as<double2>(), Gate{});
     ++st.matvecs;
-    // |b - Ax|^2, |Ax|^2, |b|^2 on the host (n complex copies: cheap next to the solve).
     std::vector<double2> hb(n), hax(n), hx(n);
     SB_CUDA(cudaMemcpyAsync(hb.data(), b, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
-    SB_CUDA(cudaMemcpyAsync(hax.data(), ax.p, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
+    SB_CUDA(cudaMemcpyAsync(hax.data(), sw.ax.p, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
     SB_CUDA(cudaMemcpyAsync(hx.data(), x, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
     SB_CUDA(cudaStreamSynchronize(op.stream));
     double rs = 0, as = 0, bs = 0;
@@ -298,7 +524,53 @@ void finalize(const Operator& op, const double2* b, const double2* x, sb_gmres_s
     const double rn = std::sqrt(rs), bn = std::sqrt(bs);
     st.residual = bn > 0 ? rn / bn : rn;
     st.backward_error = rn / std::max(std::sqrt(as) + bn, 2.2250738585072014e-308);
-    (void)tol;
+}
+
+struct DeviceTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s;
+    explicit DeviceTimer(cudaStream_t s_) : s(s_) {
+        SB_CUDA(cudaEventCreate(&a));
+        SB_CUDA(cudaEventCreate(&b));
+        SB_CUDA(cudaEventRecord(a, s));
+    }
+    double stop() {
+        SB_CUDA(cudaEventRecord(b, s));
+        SB_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        SB_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return ms;
+    }
+    ~DeviceTimer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+Problem<double2> problem64(const Operator& op) {
+    Problem<double2> P;
+    P.n = op.n;
+    P.stream = op.stream;
+    P.key_A = op.A64.p ? op.A64.p : op.A32.p;
+    P.apply = [&op](const double2* xi, double2* yo, Gate g) { op_gemv64(op, xi, yo, g); };
+    P.residual = [&op](const double2* xi, const double2* bi, double2* ro, double* part) {
+        op_residual64(op, xi, bi, ro, part);
+    };
+    return P;
+}
+
+Problem<float2> problem32(const Operator& op) {
+    Problem<float2> P;
+    P.n = op.n;
+    P.stream = op.stream;
+    P.key_A = op.A32.p;
+    P.apply = [&op](const float2* xi, float2* yo, Gate g) {
+        gemv_c64(op.A32.as<float2>(), op.n, op.lda32, xi, yo, nullptr, nullptr, op.stream, g);
+    };
+    P.residual = [&op](const float2* xi, const float2* bi, float2* ro, double* part) {
+        gemv_c64(op.A32.as<float2>(), op.n, op.lda32, xi, ro, bi, part, op.stream);
+    };
+    return P;
 }
 
 }  // namespace
@@ -306,33 +578,13 @@ void finalize(const Operator& op, const double2* b, const double2* x, sb_gmres_s
 void gmres_fp64(const Operator& op, const double2* b, double2* x, bool x0_given,
                 const sb_gmres_config& cfg, int precond, sb_gmres_stats& st) {
     SB_CUDA(cudaSetDevice(op.device));
-    const int64_t n = op.n;
-    cudaEvent_t e0, e1;
-    SB_CUDA(cudaEventCreate(&e0));
-    SB_CUDA(cudaEventCreate(&e1));
-    SB_CUDA(cudaEventRecord(e0, op.stream));
-    if (!x0_given) SB_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, op.stream));
-    DevBuf part;
-    part.alloc(sizeof(double) * gemv_partials(n));
-    DevBuf nrm;
-    nrm.alloc(sizeof(double));
-    Operator& mop = const_cast<Operator&>(op);
-    Problem<double2> P;
-    P.n = n;
-    P.stream = op.stream;
+    SB_REQUIRE(cfg.restart <= kMaxKrylov, SB_ERR_INVALID_ARGUMENT, "restart exceeds the supported Krylov dimension");
+    SolveWork& sw = solve_work(op);
+    DeviceTimer timer(op.stream);
+    if (!x0_given) SB_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * op.n, op.stream));
+    Problem<double2> P = problem64(op);
     P.jacobi = precond == SB_PRECOND_JACOBI ? op.diag.as<double2>() : nullptr;
-    P.apply = [&](const double2* xi, double2* yo) {
-        gemv_c128(op.A64.as<double2>(), n, xi, yo, Trans::N, op.stream, mop.scratch);
-    };
-    P.residual = [&](const double2* xi, const double2* bi, double2* ro) {
-        gemv_residual_c128(op.A64.as<double2>(), n, xi, bi, ro, part.as<double>(), op.stream);
-        sum_real(part.as<double>(), gemv_partials(n), nrm.as<double>(), op.stream);
-        double h = 0;
-        SB_CUDA(cudaMemcpyAsync(&h, nrm.p, sizeof(double), cudaMemcpyDeviceToHost, op.stream));
-        SB_CUDA(cudaStreamSynchronize(op.stream));
-        return std::sqrt(h);
-    };
-    CoreResult R = gmres_core<double2>(P, b, x, cfg.max_iterations, cfg.restart, cfg.tolerance,
+    CoreResult R = gmres_core<double2>(sw.k64, P, b, x, cfg.max_iterations, cfg.restart, cfg.tolerance,
                                        cfg.convergence_check_interval);
     st = sb_gmres_stats{};
     st.iterations = R.iterations;
@@ -341,80 +593,50 @@ void gmres_fp64(const Operator& op, const double2* b, double2* x, bool x0_given,
     st.estimated_residual = R.estimated;
     st.converged = R.converged ? 1 : 0;
     st.status = R.status;
-    finalize(op, b, x, st, cfg.tolerance);
-    SB_CUDA(cudaEventRecord(e1, op.stream));
-    SB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    st.device_ms = ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    finalize(op, sw, b, x, st);
+    st.device_ms = timer.stop();
 }
 
 void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_given,
                     const sb_ir_config& cfg, sb_gmres_stats& st) {
-    SB_REQUIRE(op.precision == SB_PRECISION_FP64_FP32 && op.A32.p, SB_ERR_INVALID_ARGUMENT,
-               "mixed solve: the operator has no complex64 copy (assemble with SB_PRECISION_FP64_FP32)");
+    SB_REQUIRE(op.A32.p, SB_ERR_INVALID_ARGUMENT,
+               "mixed solve: the operator has no complex64 matrix (assemble with SB_PRECISION_FP64_FP32 or "
+               "SB_PRECISION_FP32)");
+    SB_REQUIRE(cfg.inner_restart <= kMaxKrylov, SB_ERR_INVALID_ARGUMENT,
+               "inner_restart exceeds the supported Krylov dimension");
     SB_CUDA(cudaSetDevice(op.device));
     const int64_t n = op.n;
-    cudaEvent_t e0, e1;
-    SB_CUDA(cudaEventCreate(&e0));
-    SB_CUDA(cudaEventCreate(&e1));
-    SB_CUDA(cudaEventRecord(e0, op.stream));
+    SolveWork& sw = solve_work(op);
+    DeviceTimer timer(op.stream);
     if (!x0_given) SB_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, op.stream));
-    DevBuf r64, r32, d32, part, nrm, one;
-    r64.alloc(sizeof(double2) * n);
-    r32.alloc(sizeof(float2) * n);
-    d32.alloc(sizeof(float2) * n);
-    part.alloc(sizeof(double) * gemv_partials(n));
-    nrm.alloc(sizeof(double));
-    one.alloc(sizeof(double2));
-    const double2 h_one = make_double2(1.0, 0.0);
-    SB_CUDA(cudaMemcpy(one.p, &h_one, sizeof(double2), cudaMemcpyHostToDevice));
-    auto residual64 = [&]() {
-        gemv_residual_c128(op.A64.as<double2>(), n, x, b, r64.as<double2>(), part.as<double>(), op.stream);
-        sum_real(part.as<double>(), gemv_partials(n), nrm.as<double>(), op.stream);
-        double h = 0;
-        SB_CUDA(cudaMemcpyAsync(&h, nrm.p, sizeof(double), cudaMemcpyDeviceToHost, op.stream));
+    double* hsc = static_cast<double*>(sw.pin.p);
+    auto residual64 = [&](const double2* xv) {
+        op_residual64(op, xv, b, sw.r64.as<double2>(), sw.partg.as<double>());
+        sum_real(sw.partg.as<double>(), gemv_partials(n), sw.nrmg.as<double>(), op.stream);
+        SB_CUDA(cudaMemcpyAsync(hsc, sw.nrmg.p, sizeof(double), cudaMemcpyDeviceToHost, op.stream));
         SB_CUDA(cudaStreamSynchronize(op.stream));
-        return std::sqrt(h);
+        return std::sqrt(hsc[0]);
     };
-    Problem<float2> P;
-    P.n = n;
-    P.stream = op.stream;
-    P.apply = [&](const float2* xi, float2* yo) {
-        gemv_c64(op.A32.as<float2>(), n, op.lda32, xi, yo, nullptr, nullptr, op.stream);
-    };
-    P.residual = [&](const float2* xi, const float2* bi, float2* ro) {
-        gemv_c64(op.A32.as<float2>(), n, op.lda32, xi, ro, bi, part.as<double>(), op.stream);
-        sum_real(part.as<double>(), gemv_partials(n), nrm.as<double>(), op.stream);
-        double h = 0;
-        SB_CUDA(cudaMemcpyAsync(&h, nrm.p, sizeof(double), cudaMemcpyDeviceToHost, op.stream));
-        SB_CUDA(cudaStreamSynchronize(op.stream));
-        return std::sqrt(h);
-    };
+    Problem<float2> P = problem32(op);
     st = sb_gmres_stats{};
-    // ||b|| from the residual of x = 0 when no guess is given, else separately.
-    double bnorm;
-    {
-        DevBuf zero;
-        zero.alloc(sizeof(double2) * n);
-        SB_CUDA(cudaMemsetAsync(zero.p, 0, sizeof(double2) * n, op.stream));
-        gemv_residual_c128(op.A64.as<double2>(), n, zero.as<double2>(), b, r64.as<double2>(), part.as<double>(), op.stream);
-        sum_real(part.as<double>(), gemv_partials(n), nrm.as<double>(), op.stream);
-        double h = 0;
-        SB_CUDA(cudaMemcpyAsync(&h, nrm.p, sizeof(double), cudaMemcpyDeviceToHost, op.stream));
-        SB_CUDA(cudaStreamSynchronize(op.stream));
-        bnorm = std::sqrt(h);
-        ++st.matvecs;
-    }
+    // ||b|| by a norm kernel; with a zero initial guess the first residual is b itself.
+    arnoldi_dots<double2>(b, n, 0, b, n, sw.k64_part(n), sw.k64_red(), op.stream);
+    SB_CUDA(cudaMemcpyAsync(hsc, sw.k64_red(), sizeof(double), cudaMemcpyDeviceToHost, op.stream));
+    SB_CUDA(cudaStreamSynchronize(op.stream));
+    const double bnorm = std::sqrt(hsc[0]);
     const double bref = bnorm < 1e-15 ? 1.0 : bnorm;
     int status = SB_SOLVER_MAX_ITERATIONS;
     bool converged = false;
     double rel = 1.0;
     for (int64_t it = 0; it <= cfg.max_refinements; ++it) {
-        const double rn = residual64();
-        ++st.matvecs;
+        double rn;
+        if (it == 0 && !x0_given) {
+            SB_CUDA(cudaMemcpyAsync(sw.r64.p, b, sizeof(double2) * n, cudaMemcpyDeviceToDevice, op.stream));
+            rn = bnorm;
+        } else {
+            rn = residual64(x);
+            ++st.matvecs;
+        }
         rel = rn / bref;
         if (rel < cfg.tolerance) {
             converged = true;
@@ -427,15 +649,18 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
         }
         if (it == cfg.max_refinements) break;
         // Inner correction: A32 d = r / ||r|| in FP32, then x += ||r|| d in FP64.
-        scale_vec<double2, float2>(r64.as<double2>(), 1.0 / rn, r32.as<float2>(), n, op.stream);
-        SB_CUDA(cudaMemsetAsync(d32.p, 0, sizeof(float2) * n, op.stream));
-        CoreResult R = gmres_core<float2>(P, r32.as<float2>(), d32.as<float2>(), cfg.inner_max_iterations,
-                                          cfg.inner_restart, cfg.inner_tolerance, 1);
+        scale_vec<double2, float2>(sw.r64.as<double2>(), 1.0 / rn, nullptr, sw.r32.as<float2>(), n, op.stream);
+        SB_CUDA(cudaMemsetAsync(sw.d32.p, 0, sizeof(float2) * n, op.stream));
+        // The inner solve need not reduce the residual further than the outer target asks:
+        // relax its tolerance (never below inner_tolerance) on the last refinements.
+        const double inner_tol = std::max(cfg.inner_tolerance, 0.5 * cfg.tolerance / rel);
+        CoreResult R = gmres_core<float2>(sw.k32, P, sw.r32.as<float2>(), sw.d32.as<float2>(),
+                                          cfg.inner_max_iterations, cfg.inner_restart, inner_tol, 1);
         st.iterations += R.iterations;
         st.restarts += R.restarts;
         st.matvecs += R.matvecs;
         st.matvecs_fp32 += R.matvecs;
-        basis_update<float2, double2>(d32.as<float2>(), n, 1, one.as<double2>(), rn, x, n, op.stream);
+        basis_update<float2, double2>(sw.d32.as<float2>(), n, 1, nullptr, sw.one.as<double2>(), rn, x, n, op.stream);
         ++st.refinements;
         if (R.status == SB_SOLVER_BREAKDOWN && R.iterations == 0) {
             status = SB_SOLVER_BREAKDOWN;
@@ -445,14 +670,8 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
     st.estimated_residual = rel;
     st.converged = converged ? 1 : 0;
     st.status = status;
-    finalize(op, b, x, st, cfg.tolerance);
-    SB_CUDA(cudaEventRecord(e1, op.stream));
-    SB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    st.device_ms = ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    finalize(op, sw, b, x, st);
+    st.device_ms = timer.stop();
 }
 
 }  // namespace sb

@@ -97,7 +97,7 @@ struct Mesh {
     std::vector<double> h_nodes;
     std::vector<uint32_t> h_tris;
     std::vector<double> h_elem;  // host copy of the element SoA (ld stride)
-    DevBuf nodes, tris, elem, qp;
+    DevBuf nodes, tris, elem, qp, qp32;
     // near-pair CSR (superset of the reference's subdivision criterion; excludes the diagonal)
     int64_t nnz = 0;
     DevBuf near_ptr, near_col;
@@ -121,7 +121,8 @@ struct Operator {
     double beta_re = 0, beta_im = 0;
     int64_t lda32 = 0;           // even leading dimension of the complex64 copy
     DevBuf A64, A32, rhs, diag;  // rhs: BC-induced RHS (N complex); diag: A_ii for Jacobi
-    DevBuf coef, far_part, near_rhs, self_rhs, scratch;
+    DevBuf coef, far_part, near_rhs, self_rhs, scratch, status;
+    void* work = nullptr;        // solver workspace (gmres.cu), released by destroy_solve_work
     cudaStream_t stream = nullptr;
     double last_assembly_ms = 0.0;
 };
@@ -149,6 +150,12 @@ void gmres_fp64(const Operator& op, const double2* b_dev, double2* x_dev, bool x
                 const sb_gmres_config& cfg, int precond, sb_gmres_stats& st);
 void gmres_mixed_ir(const Operator& op, const double2* b_dev, double2* x_dev, bool x0_given,
                     const sb_ir_config& cfg, sb_gmres_stats& st);
+
+void destroy_solve_work(Operator& op);
+struct Gate;
+// Products with FP64 vectors on whichever matrix the operator holds (gmres.cu).
+void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g);
+void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part);
 
 int device_sm_count(int device);
 

@@ -73,6 +73,7 @@ def test_device_sincos_matches_golden(gpu):
 
 
 def assemble_both(sb, oracle, nodes, tris, k, beta_scale=1.0, bc=None, precision=0, rows=None):
+    nodes = np.ascontiguousarray(nodes)
     ph_o = oracle.physics_for_k(k)
     beta = oracle.bm_beta(ph_o, beta_scale)
     kw = {} if bc is None else bc
@@ -280,3 +281,40 @@ def test_reassemble_in_place(gpu, oracle):
     op.reassemble(ph2, ph2.burton_miller_beta())
     A_o, _ = oracle.assemble(nodes, tris, oracle.physics_for_k(3.0), ph2.burton_miller_beta())
     assert entry_error(op.matrix, A_o) < 1e-10
+
+
+@pytest.mark.parametrize("level,k,scale", [(3, 2.0, None), (3, 6.0, (1.0, 0.6, 0.4)), (3, 12.0, None)])
+def test_mixed_assembly_entries_within_fp32_tolerance(gpu, oracle, level, k, scale):
+    """SB_PRECISION_FP32: far pairs in FP32 with the FP64 phase argument; near/self pairs FP64.
+
+    Bar: every entry within 1e-5 relative of the FP64 oracle (floor 1e-6 of the matrix maximum;
+    FP32 sums of the 13 leaf points with cancellation next to the near threshold reach a few
+    1e-6), the median entry within 1e-6; near and self entries are the FP64 values rounded to
+    complex64."""
+    nodes, tris = oracle.icosphere(1.0, level, scale or (1.0, 1.0, 1.0))
+    op, A_o, *_ = assemble_both(gpu, oracle, nodes, tris, k, precision=gpu.SB_PRECISION_FP32)
+    A = op.matrix
+    floor = 1e-6 * np.abs(A_o).max()
+    err = np.abs(A - A_o) / np.maximum(np.abs(A_o), floor)
+    assert err.max() < 1e-5, err.max()
+    assert np.median(err) < 1e-6, np.median(err)
+    d = np.diag_indices(A.shape[0])
+    assert np.array_equal(A[d], A_o[d].astype(np.complex64).astype(np.complex128))
+
+
+def test_mixed_assembly_solution_within_1e5(gpu, oracle):
+    nodes, tris = oracle.icosphere(1.0, 4)
+    mesh = gpu.Mesh(nodes, tris)
+    ph = gpu.PhysicsParams.for_wavenumber(6.0)
+    beta = ph.burton_miller_beta()
+    b = gpu.rhs_plane_wave(mesh, ph, beta, [0, 0, 1])[:, 0]
+    op64 = gpu.build_tbem_system(mesh, ph)
+    x64 = gpu.gmres(op64, b, gpu.GmresConfig(max_iterations=100, restart=50, tolerance=1e-10)).x
+    op32 = gpu.build_tbem_system(mesh, ph, precision=gpu.SB_PRECISION_FP32)
+    mix = gpu.gmres_mixed(op32, b, gpu.IrConfig(tolerance=1e-8))
+    assert mix.converged
+    assert np.linalg.norm(mix.x - x64) / np.linalg.norm(x64) < 1e-5
+    c, nrm, a = mesh.element_geometry()
+    e64 = oracle.rigid_sphere_surface_error(x64, c, a, ph.wave_number, 1.0)
+    e32 = oracle.rigid_sphere_surface_error(mix.x, c, a, ph.wave_number, 1.0)
+    assert abs(e32 - e64) < 1e-5
