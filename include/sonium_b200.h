@@ -164,6 +164,17 @@ SB_API int sb_operator_apply_block(const sb_operator* op, const sb_complex* X, s
 SB_API int sb_operator_apply_device(const sb_operator* op, int trans, const sb_complex* x_dev,
                                     sb_complex* y_dev);
 
+/* Same product without any device allocation. This entry point has no counterpart in the
+ * reference: it serves callers that must not call cudaMalloc / cudaFree, such as a host that has
+ * already given the GPU's memory to its own pool (a driver allocation would fail or fragment it)
+ * or one that keeps other streams busy and cannot take the device-wide wait of cudaFree. The
+ * partial sums of op(A) x live in one fixed 8 MiB device array per GPU, held until the process
+ * exits, so n is limited to 524288 (larger operators: SB_ERR_INVALID_ARGUMENT). The first call on
+ * a device looks that array's address up once; make it before any stream capture. All calls on a
+ * device share the array: calls whose kernels overlap on the GPU race. */
+SB_API int sb_operator_apply_device_noalloc(const sb_operator* op, int trans,
+                                            const sb_complex* x_dev, sb_complex* y_dev);
+
 /* Preconditioner<Complex64>::apply_into (traits.rs:3645-3720): identity or Jacobi (A_ii^-1). */
 #define SB_PRECOND_IDENTITY 0
 #define SB_PRECOND_JACOBI 1

@@ -125,6 +125,7 @@ _SIGNATURES = {
     "sb_operator_apply": ([P, ct.c_int, P, P], ct.c_int),
     "sb_operator_apply_block": ([P, P, P, ct.c_int64], ct.c_int),
     "sb_operator_apply_device": ([P, ct.c_int, P, P], ct.c_int),
+    "sb_operator_apply_device_noalloc": ([P, ct.c_int, P, P], ct.c_int),
     "sb_preconditioner_apply": ([P, ct.c_int, P, P], ct.c_int),
     "sb_rhs_plane_wave": ([P, ct.POINTER(SbPhysics), SbComplex, P, P, ct.c_int64, P], ct.c_int),
     "sb_gmres": ([P, P, P, ct.POINTER(SbGmresConfig), ct.c_int, P, ct.POINTER(SbGmresStats)], ct.c_int),
