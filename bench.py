@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 timing")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--single", action="store_true",
+                    help="one untimed solve per precision mode at --level (profiling driver), no JSON line")
     return ap.parse_args()
 
 
@@ -234,6 +236,9 @@ def main():
     sb_build.build()
     lib = L.load()
     dev = dist.local
+    if a.single:
+        single_solves(sb, a.level, a.k, dev)
+        return
     assert sb.device_count() > dev, "no CUDA device for this rank"
 
     nodes, tris = sb.icosphere(RADIUS, a.level)
@@ -350,10 +355,14 @@ def main():
     hbm_kind = max(("gemv32", "gemv64"), key=lambda kk: ms[kk])
     avg = ms[hbm_kind] / max(launches[hbm_kind], 1) / 1e3
     achieved = bytes_mv[hbm_kind] / avg / 1e9
+    # DRAM traffic per launch from one ncu capture of the same kernel at N = 5120
+    # (dram__bytes_read.sum + dram__bytes_write.sum = 221.9 MB = 8.47 bytes per complex64 matrix
+    # entry), scaled by the entries of this launch; the complex128 kernel was not captured.
+    traffic = 8.47 * n * n if hbm_kind == "gemv32" else None
     roof = {"kernel": ("k_gemv_n_c64 (complex64 matrix; FP32 or FP64 vectors)" if hbm_kind == "gemv32"
                        else "k_gemv_n_c128 (complex128 matvec)"),
             "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk_kind,
+            "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_source": pk_kind,
             "bytes_per_launch": bytes_mv[hbm_kind], "avg_launch_ms": avg * 1e3,
             "launches": launches[hbm_kind], "share_of_kernel_time": ms[hbm_kind] / max(total_ms, 1e-9),
             "dominant_kernel_class": dominant}
@@ -397,6 +406,24 @@ def main():
     rt.cudaFree(b_d)
     rt.cudaFree(x_d)
     dist.close()
+
+
+def single_solves(sb, level, k, dev):
+    """One solve per precision mode, untimed: the small case the ncu captures profile."""
+    nodes, tris = sb.icosphere(RADIUS, level)
+    ph = sb.PhysicsParams.for_wavenumber(k)
+    beta = ph.burton_miller_beta()
+    mesh = sb.Mesh(nodes, tris, device=dev)
+    b = sb.rhs_plane_wave(mesh, ph, beta, [0.0, 0.0, 1.0])[:, 0]
+    for name in ("mixed", "plain_fp64"):
+        prec, solver = MODES[name]
+        op = sb.build_tbem_system_with_beta(mesh, ph, beta, getattr(sb, prec))
+        if solver == "ir":
+            s = sb.gmres_mixed(op, b, sb.IrConfig(20, TOL, RESTART, 20, 1e-5))
+        else:
+            s = sb.gmres(op, b, sb.GmresConfig(100, RESTART, TOL))
+        print(f"{name}: N={tris.shape[0]} iterations {s.iterations} matvecs {s.matvecs} residual {s.residual:.2e}")
+        op.close()
 
 
 def _cudart():

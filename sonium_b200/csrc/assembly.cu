@@ -560,9 +560,9 @@ __global__ void __launch_bounds__(kFarTile) k_far(const double* __restrict__ qp,
 // k (r_q - r_c) rotates exp(i k r_c). Everything else (G, H, H^T, E factors and the sums) is
 // FP32; the near and self pairs keep the FP64 kernels.
 // ---------------------------------------------------------------------------------------------
-constexpr int kQ32 = 5;  // per point: delta x, y, z, |delta|^2, w * J / (4 pi)
+constexpr int kQ32 = 6;  // per point: delta x, y, z, |delta|^2, w * J / (4 pi), delta . n_y
 
-// Element point data for the FP32 far kernel: qp32[(q * 5 + c) * ld + e].
+// Element point data for the FP32 far kernel: qp32[(q * 6 + c) * ld + e].
 __global__ void k_far_points32(const double* __restrict__ elem, int64_t n, int64_t ld,
                                float* __restrict__ qp32) {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -582,6 +582,7 @@ __global__ void k_far_points32(const double* __restrict__ elem, int64_t n, int64
         for (int j = 0; j < 3; ++j) dst[j * ld] = static_cast<float>(dl[j]);
         dst[3 * ld] = static_cast<float>(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
         dst[4 * ld] = static_cast<float>(c_tri_w[o + q] * E(EJAC, e) * kInv4Pi);
+        dst[5 * ld] = static_cast<float>(dl[0] * E(ENX, e) + dl[1] * E(ENY, e) + dl[2] * E(ENZ, e));
     }
 }
 
@@ -627,6 +628,8 @@ __global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp
                                                     double2* __restrict__ far_part, int64_t n_tiles) {
     __shared__ double sx[kFar32Rows][3];
     __shared__ float snx[kFar32Rows][3];
+    __shared__ double sg[4][kFarTile];    // column: level-0 centre and near threshold
+    __shared__ float scf[8][kFarTile];    // column: matrix weights (cG, cH, cHt, cE)
     __shared__ double sred[kFarTile / 32][2];
     const int tid = threadIdx.x;
     const int64_t tile = blockIdx.x;
@@ -639,10 +642,9 @@ __global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp
         snx[r][c] = (i < n) ? static_cast<float>(E(ENX + c, i)) : 0.f;
     }
     // The column's 13 points in registers.
-    float px[kFarPoints], py[kFarPoints], pz[kFarPoints], pd[kFarPoints], pw[kFarPoints];
-    double cx = 0, cy = 0, cz = 0, gx = 0, gy = 0, gz = 0, thr = -1;
+    float px[kFarPoints], py[kFarPoints], pz[kFarPoints], pd[kFarPoints], pw[kFarPoints], pn[kFarPoints];
+    double cx = 0, cy = 0, cz = 0;
     float nyx = 0, nyy = 0, nyz = 0;
-    float cgr = 0, cgi = 0, chr = 0, chi = 0, ctr = 0, cti = 0, cer = 0, cei = 0;
     const int64_t jj = j < n ? j : 0;
 #pragma unroll
     for (int q = 0; q < kFarPoints; ++q) {
@@ -652,22 +654,22 @@ __global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp
         pz[q] = src[2 * ld];
         pd[q] = src[3 * ld];
         pw[q] = src[4 * ld];
+        pn[q] = src[5 * ld];
     }
     if (j < n) {
         cx = E(ECX, j); cy = E(ECY, j); cz = E(ECZ, j);
-        gx = E(EGX, j); gy = E(EGY, j); gz = E(EGZ, j);
-        thr = near_threshold(E(EAREA, j));
         nyx = static_cast<float>(E(ENX, j));
         nyy = static_cast<float>(E(ENY, j));
         nyz = static_cast<float>(E(ENZ, j));
-        cgr = static_cast<float>(coef[(int64_t)(CF_CG) * ld + j]);
-        cgi = static_cast<float>(coef[(int64_t)(CF_CG + 1) * ld + j]);
-        chr = static_cast<float>(coef[(int64_t)(CF_CH) * ld + j]);
-        chi = static_cast<float>(coef[(int64_t)(CF_CH + 1) * ld + j]);
-        ctr = static_cast<float>(coef[(int64_t)(CF_CHT) * ld + j]);
-        cti = static_cast<float>(coef[(int64_t)(CF_CHT + 1) * ld + j]);
-        cer = static_cast<float>(coef[(int64_t)(CF_CE) * ld + j]);
-        cei = static_cast<float>(coef[(int64_t)(CF_CE + 1) * ld + j]);
+        sg[0][tid] = E(EGX, j);
+        sg[1][tid] = E(EGY, j);
+        sg[2][tid] = E(EGZ, j);
+        sg[3][tid] = near_threshold(E(EAREA, j));
+        for (int f = 0; f < 8; ++f) scf[f][tid] = static_cast<float>(coef[(int64_t)(CF_CG + f) * ld + j]);
+    } else {
+        sg[0][tid] = sg[1][tid] = sg[2][tid] = 0.0;
+        sg[3][tid] = -1.0;
+        for (int f = 0; f < 8; ++f) scf[f][tid] = 0.f;
     }
     __syncthreads();
     const float kf = static_cast<float>(k), k2f = kf * kf;
@@ -675,7 +677,7 @@ __global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp
     for (int r = 0; r < rows_here; ++r) {
         const int64_t i = row0 + r;
         const double x0 = sx[r][0], x1 = sx[r][1], x2 = sx[r][2];
-        const bool active = (j < n) && (j != i) && !near_superset(gx, gy, gz, thr, x0, x1, x2);
+        const bool active = (j < n) && (j != i) && !near_superset(sg[0][tid], sg[1][tid], sg[2][tid], sg[3][tid], x0, x1, x2);
         double2 rhs_c = make_double2(0.0, 0.0);
         if (active) {
             // FP64: centroid offset, distance and the reduced phase k r_c mod 2 pi.
@@ -692,15 +694,18 @@ __global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp
             const float rcf = static_cast<float>(rc), rc2f = static_cast<float>(rc2);
             const float nxx = snx[r][0], nxy = snx[r][1], nxz = snx[r][2];
             const float nxny = nxx * nyx + nxy * nyy + nxz * nyz;
+            const float fny = fx * nyx + fy * nyy + fz * nyz;       // d_c . n_y
+            const float fnx = -(fx * nxx + fy * nxy + fz * nxz);    // -d_c . n_x
             float ag_r = 0.f, ag_i = 0.f, ah_r = 0.f, ah_i = 0.f, at_r = 0.f, at_i = 0.f, ae_r = 0.f, ae_i = 0.f;
 #pragma unroll
             for (int q = 0; q < kFarPoints; ++q) {
                 const float num = fmaf(2.f, fx * px[q] + fy * py[q] + fz * pz[q], pd[q]);
                 const float rq2 = rc2f + num;
                 const float rinv = rsqrtf(rq2);
-                const float rq = rq2 * rinv;
-                const float t = kf * __fdividef(num, rq + rcf);
+                const float t = kf * __fdividef(num, fmaf(rq2, rinv, rcf));
                 float st, ct;
+                // The short series serves every resolved mesh (|t| <= k h); larger phase offsets
+                // take the quadrant-reduced version.
                 if (fabsf(t) <= 0.8f) {
                     const float t2 = t * t;
                     float ps = fmaf(fmaf(fmaf(2.75573192e-6f, t2, -1.98412698e-4f), t2, 8.33333333e-3f), t2, -1.66666667e-1f);
@@ -711,27 +716,29 @@ __global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp
                 } else {
                     sincos_f32(t, &st, &ct);
                 }
-                const float er = cc * ct - sc * st, ei = sc * ct + cc * st;
                 const float gs = pw[q] * rinv;
-                const float g_r = er * gs, g_i = ei * gs;
-                const float ux = (fx + px[q]) * rinv, uy = (fy + py[q]) * rinv, uz = (fz + pz[q]) * rinv;
-                const float rny = ux * nyx + uy * nyy + uz * nyz;
-                const float rnx = -(ux * nxx + uy * nxy + uz * nxz);
-                const float b_r = -g_r * rinv - g_i * kf;
-                const float b_i = g_r * kf - g_i * rinv;
+                const float g_r = (cc * ct - sc * st) * gs, g_i = (sc * ct + cc * st) * gs;
+                // r_hat . n_y and -r_hat . n_x from per-pair and per-point dot products
+                const float rny = (fny + pn[q]) * rinv;
+                const float rnx = (fnx - (px[q] * nxx + py[q] * nxy + pz[q] * nxz)) * rinv;
+                const float b_r = -fmaf(g_r, rinv, g_i * kf);
+                const float b_i = fmaf(g_r, kf, -g_i * rinv);
                 ag_r += g_r;
                 ag_i += g_i;
                 ah_r = fmaf(b_r, rny, ah_r);
                 ah_i = fmaf(b_i, rny, ah_i);
                 at_r = fmaf(b_r, rnx, at_r);
                 at_i = fmaf(b_i, rnx, at_i);
+                // E factor: ((3/r^2 - k^2) rq + nx.ny / r^2, -(k / r) (3 rq + nx.ny))
                 const float rqq = rny * rnx;
-                const float ri2 = rinv * rinv;
-                const float f_r = (3.f * ri2 - k2f) * rqq + nxny * ri2;
-                const float f_i = -kf * rinv * (3.f * rqq + nxny);
-                ae_r += g_r * f_r - g_i * f_i;
-                ae_i += g_r * f_i + g_i * f_r;
+                const float s3 = fmaf(3.f, rqq, nxny);
+                const float f_r = fmaf(rinv * rinv, s3, -k2f * rqq);
+                const float f_i = -kf * rinv * s3;
+                ae_r = fmaf(g_r, f_r, fmaf(-g_i, f_i, ae_r));
+                ae_i = fmaf(g_r, f_i, fmaf(g_i, f_r, ae_i));
             }
+            const float cgr = scf[0][tid], cgi = scf[1][tid], chr = scf[2][tid], chi = scf[3][tid];
+            const float ctr = scf[4][tid], cti = scf[5][tid], cer = scf[6][tid], cei = scf[7][tid];
             const float vr = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
             const float vi = ag_r * cgi + ag_i * cgr + ah_r * chi + ah_i * chr + at_r * cti + at_i * ctr + ae_r * cei + ae_i * cer;
             A32[i * lda32 + j] = make_float2(vr, vi);

@@ -310,6 +310,7 @@ struct CoreResult {
     double residual = 1.0, estimated = 1.0;
     bool converged = false;
     int status = SB_SOLVER_MAX_ITERATIONS;
+    const void* r_last = nullptr;  // device b - A x for the returned x, when one was formed
 };
 
 // All Arnoldi steps of one cycle, every launch gated by st->active.
@@ -380,9 +381,13 @@ void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
 }
 
 // gmres_core (gmres.rs:631-1047) with an identity or Jacobi left preconditioner.
+// x_zero: x enters as zero, so the first residual is b itself (no product needed).
+// trust_estimate: an inner solve of iterative refinement, whose caller forms the FP64 residual
+// itself: an estimated convergence ends the solve without the exact residual product.
 template <class T>
 CoreResult gmres_core(KrylovWork<T>& W, const Problem<T>& P, const T* b, T* x, int64_t max_it,
-                      int64_t m, double tol, int64_t check_interval) {
+                      int64_t m, double tol, int64_t check_interval, bool x_zero = false,
+                      bool trust_estimate = false) {
     const int64_t n = P.n;
     const cudaStream_t s = P.stream;
     W.ensure(n, m);
@@ -420,7 +425,14 @@ CoreResult gmres_core(KrylovWork<T>& W, const Problem<T>& P, const T* b, T* x, i
         pbnorm = rhs_zero ? 1.0 : raw_pb;
     }
     for (int64_t outer = 0; outer < max_it; ++outer) {
-        const double rn = residual(W.opb.template as<T>(), false);
+        double rn;
+        if (outer == 0 && x_zero) {
+            SB_CUDA(cudaMemcpyAsync(W.opb.p, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, s));
+            rn = raw_bn;
+        } else {
+            rn = residual(W.opb.template as<T>(), false);
+        }
+        R.r_last = W.opb.p;
         const double trel = rn / bnorm;
         double beta = rn;
         const T* src = W.opb.template as<T>();
@@ -456,7 +468,24 @@ CoreResult gmres_core(KrylovWork<T>& W, const Problem<T>& P, const T* b, T* x, i
         SB_CUDA(cudaGetLastError());
         basis_update<T, T>(W.V.template as<T>(), W.ldv, 0, &W.st.template as<KState>()->jdone,
                            W.ydev.template as<double2>(), 1.0, x, n, s);
+        R.r_last = nullptr;
+        if (trust_estimate) {
+            SB_CUDA(cudaMemcpyAsync(hst, W.st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
+            SB_CUDA(cudaStreamSynchronize(s));
+            profile_account(W.prof_pairs, hst->jdone);
+            R.iterations += hst->jdone;
+            R.matvecs += hst->jdone;
+            if (hst->reason != 0) {
+                R.estimated = R.residual = hst->relres;
+                R.converged = hst->relres < tol;
+                R.status = R.converged ? SB_SOLVER_CONVERGED : SB_SOLVER_BREAKDOWN;
+                return R;
+            }
+            ++R.restarts;
+            continue;
+        }
         const double tr = residual(W.r.template as<T>(), true) / bnorm;
+        R.r_last = W.r.p;
         profile_account(W.prof_pairs, hst->jdone);
         R.iterations += hst->jdone;
         R.matvecs += hst->jdone;
@@ -488,21 +517,30 @@ CoreResult gmres_core(KrylovWork<T>& W, const Problem<T>& P, const T* b, T* x, i
         ++R.restarts;
     }
     R.residual = residual(W.r.template as<T>(), false) / bnorm;
+    R.r_last = W.r.p;
     R.estimated = R.residual;
     R.status = SB_SOLVER_MAX_ITERATIONS;
     return R;
 }
 
-// finalize_gmres_solution (gmres.rs:159-247): residual and backward error from one more product.
-void finalize(const Operator& op, SolveWork& sw, const double2* b, const double2* x, sb_gmres_stats& st) {
+// finalize_gmres_solution (gmres.rs:159-247): residual and backward error of the returned x.
+// `r`, when given, is b - A x already formed for this x (A x = b - r then needs no product).
+void finalize(const Operator& op, SolveWork& sw, const double2* b, const double2* x, sb_gmres_stats& st,
+              const double2* r = nullptr) {
     const int64_t n = op.n;
-    op_gemv64(op, x, sw.ax.as<double2>(), Gate{});
-    ++st.matvecs;
     std::vector<double2> hb(n), hax(n), hx(n);
+    if (r) {
+        SB_CUDA(cudaMemcpyAsync(hax.data(), r, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
+    } else {
+        op_gemv64(op, x, sw.ax.as<double2>(), Gate{});
+        ++st.matvecs;
+        SB_CUDA(cudaMemcpyAsync(hax.data(), sw.ax.p, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
+    }
     SB_CUDA(cudaMemcpyAsync(hb.data(), b, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
-    SB_CUDA(cudaMemcpyAsync(hax.data(), sw.ax.p, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
     SB_CUDA(cudaMemcpyAsync(hx.data(), x, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
     SB_CUDA(cudaStreamSynchronize(op.stream));
+    if (r)
+        for (int64_t i = 0; i < n; ++i) hax[i] = make_double2(hb[i].x - hax[i].x, hb[i].y - hax[i].y);
     double rs = 0, as = 0, bs = 0;
     bool finite = true;
     for (int64_t i = 0; i < n; ++i) {
@@ -585,7 +623,7 @@ void gmres_fp64(const Operator& op, const double2* b, double2* x, bool x0_given,
     Problem<double2> P = problem64(op);
     P.jacobi = precond == SB_PRECOND_JACOBI ? op.diag.as<double2>() : nullptr;
     CoreResult R = gmres_core<double2>(sw.k64, P, b, x, cfg.max_iterations, cfg.restart, cfg.tolerance,
-                                       cfg.convergence_check_interval);
+                                       cfg.convergence_check_interval, !x0_given, false);
     st = sb_gmres_stats{};
     st.iterations = R.iterations;
     st.restarts = R.restarts;
@@ -593,7 +631,7 @@ void gmres_fp64(const Operator& op, const double2* b, double2* x, bool x0_given,
     st.estimated_residual = R.estimated;
     st.converged = R.converged ? 1 : 0;
     st.status = R.status;
-    finalize(op, sw, b, x, st);
+    finalize(op, sw, b, x, st, static_cast<const double2*>(R.r_last));
     st.device_ms = timer.stop();
 }
 
@@ -628,6 +666,7 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
     int status = SB_SOLVER_MAX_ITERATIONS;
     bool converged = false;
     double rel = 1.0;
+    bool r_valid = false;  // r64 holds b - A x for the current x
     for (int64_t it = 0; it <= cfg.max_refinements; ++it) {
         double rn;
         if (it == 0 && !x0_given) {
@@ -637,6 +676,7 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
             rn = residual64(x);
             ++st.matvecs;
         }
+        r_valid = true;
         rel = rn / bref;
         if (rel < cfg.tolerance) {
             converged = true;
@@ -655,12 +695,14 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
         // relax its tolerance (never below inner_tolerance) on the last refinements.
         const double inner_tol = std::max(cfg.inner_tolerance, 0.5 * cfg.tolerance / rel);
         CoreResult R = gmres_core<float2>(sw.k32, P, sw.r32.as<float2>(), sw.d32.as<float2>(),
-                                          cfg.inner_max_iterations, cfg.inner_restart, inner_tol, 1);
+                                          cfg.inner_max_iterations, cfg.inner_restart, inner_tol, 1,
+                                          /*x_zero=*/true, /*trust_estimate=*/true);
         st.iterations += R.iterations;
         st.restarts += R.restarts;
         st.matvecs += R.matvecs;
         st.matvecs_fp32 += R.matvecs;
         basis_update<float2, double2>(sw.d32.as<float2>(), n, 1, nullptr, sw.one.as<double2>(), rn, x, n, op.stream);
+        r_valid = false;
         ++st.refinements;
         if (R.status == SB_SOLVER_BREAKDOWN && R.iterations == 0) {
             status = SB_SOLVER_BREAKDOWN;
@@ -670,7 +712,7 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
     st.estimated_residual = rel;
     st.converged = converged ? 1 : 0;
     st.status = status;
-    finalize(op, sw, b, x, st);
+    finalize(op, sw, b, x, st, r_valid ? sw.r64.as<double2>() : nullptr);
     st.device_ms = timer.stop();
 }
 
