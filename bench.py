@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 timing")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the batched frequency-sweep leg")
+    ap.add_argument("--sweep-count", type=int, default=64, help="instances of the frequency sweep")
+    ap.add_argument("--sweep-only", action="store_true", help="run only the sweep leg and print its JSON")
     ap.add_argument("--single", action="store_true",
                     help="one untimed solve per precision mode at --level (profiling driver), no JSON line")
     return ap.parse_args()
@@ -240,6 +243,12 @@ def main():
         single_solves(sb, a.level, a.k, dev)
         return
     assert sb.device_count() > dev, "no CUDA device for this rank"
+    if a.sweep_only:
+        out = sweep_leg(sb, a, dist, dev, _cudart())
+        if dist.rank == 0:
+            print(json.dumps({"sweep": out}), flush=True)
+        dist.close()
+        return
 
     nodes, tris = sb.icosphere(RADIUS, a.level)
     n = tris.shape[0]
@@ -342,6 +351,9 @@ def main():
                "path": "sb_mesh_create + sb_assemble(SB_PRECISION_FP32) + sb_rhs_plane_wave + sb_gmres_mixed "
                        "(host buffers), wall clock"}
 
+    # ---- batched frequency sweep ----
+    sweep = None if a.no_sweep else sweep_leg(sb, a, dist, dev, rt)
+
     # ---- roofline of the dominant kernel of the headline step ----
     pk, pk_kind = peaks()
     names = L.PROF_NAMES
@@ -399,6 +411,7 @@ def main():
         "gpu_launches": int(prof.kernels),
         "clocks": clk,
         "e2e": e2e,
+        "sweep": sweep,
         "cpu_baseline": None if cpu is None else {kk: cpu[kk] for kk in ("value", "unit", "cores", "kind", "sample")},
     }
     if dist.rank == 0:
@@ -406,6 +419,91 @@ def main():
     rt.cudaFree(b_d)
     rt.cudaFree(x_d)
     dist.close()
+
+
+def sweep_leg(sb, a, dist, dev, rt):
+    """Batched frequency sweep: 64 instances, ka log-spaced 1 -> 32 on the (1, 0.6, 0.4) ellipsoid,
+    icosphere level per instance for >= 8 elements per wavelength (levels 2-5), plane wave +z.
+
+    One step = batched assembly of all 64 complex64 matrices (one persistent launch), the incident
+    right-hand sides, and the batched FP32-inner / FP64-refined GMRES to rtol 1e-8. Baseline: the
+    same 64 instances solved one after another in plain FP64 (complex128 assembly re-done into one
+    operator per mesh level, FP64 GMRES(50) to 1e-8), timed once. Wall clock around device-synchronised
+    work on both sides; the per-instance error of the batched solution against the FP64 one is
+    reported as its maximum."""
+    from sonium_b200.sweep import SweepBatch, build_ellipsoid_sweep, ellipsoid_sweep_plan
+
+    plan = ellipsoid_sweep_plan(count=a.sweep_count)
+    meshes, physics, betas = build_ellipsoid_sweep(plan, device=dev)
+    sizes = [m.num_elements for m in meshes]
+    cfg = sb.IrConfig(20, TOL, RESTART, 20, 1e-5)
+    batch = SweepBatch(meshes, physics, betas)
+
+    def step():
+        batch.assemble()
+        batch.set_rhs_plane_wave([0.0, 0.0, 1.0])
+        return batch.solve(cfg)
+
+    def wall(fn):
+        rt.cudaDeviceSynchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        out = fn()
+        rt.cudaDeviceSynchronize()
+        dt = time.perf_counter() - t0
+        dist.barrier()
+        return dist.max(dt), out
+
+    st0 = step()
+    xb = [batch.solution(i) for i in range(len(batch))]
+    asm_ms, solve_ms = batch.timings()
+    for _ in range(a.warmup):
+        step()
+    t_batch, _ = wall(lambda: [step() for _ in range(a.steps)])
+    batched = dist.world * len(batch) * a.steps / t_batch
+    batch.close()
+    # plain FP64 baseline, one instance after another
+    ops = {}
+    errs, fp64_iters = [], []
+
+    def fp64_sweep():
+        out = []
+        for m, ph, be in zip(meshes, physics, betas):
+            key = id(m)
+            if key not in ops:
+                ops[key] = sb.build_tbem_system_with_beta(m, ph, be)
+            else:
+                ops[key].reassemble(ph, be)
+            b = sb.rhs_plane_wave(m, ph, be, [[0.0, 0.0, 1.0]])[:, 0]
+            out.append(sb.gmres(ops[key], b, sb.GmresConfig(100, RESTART, TOL)))
+        return out
+
+    fp64_sweep()  # warm-up: allocations, graphs
+    t_fp64, sols = wall(fp64_sweep)
+    for i, s in enumerate(sols):
+        errs.append(float(np.linalg.norm(xb[i] - s.x) / np.linalg.norm(s.x)))
+        fp64_iters.append(int(s.iterations))
+    for o in ops.values():
+        o.close()
+    plain = dist.world * len(sols) / t_fp64
+    levels = [p[2] for p in plan]
+    return {
+        "workload": (f"{len(plan)} instances, ka log-spaced {plan[0][0]:g} -> {plan[-1][0]:g} on the ellipsoid "
+                     "(1, 0.6, 0.4), icosphere level per instance for >= 8 elements per wavelength "
+                     f"(levels {min(levels)}-{max(levels)}: " +
+                     ", ".join(f"L{lv} x{levels.count(lv)}" for lv in sorted(set(levels))) +
+                     f"), plane wave +z, rtol {TOL}"),
+        "value": batched, "unit": "solves/s", "ms_per_step": 1e3 * t_batch / a.steps,
+        "plain_fp64": plain, "plain_fp64_ms_per_sweep": 1e3 * t_fp64,
+        "speedup_vs_plain_fp64": batched / plain,
+        "max_error_vs_fp64": max(errs), "median_error_vs_fp64": float(np.median(errs)),
+        "all_converged": bool(all(s.converged for s in st0)),
+        "max_residual": float(max(s.residual for s in st0)),
+        "matrix_gb_c64": float(sum(8.0 * n * n for n in sizes) / 1e9),
+        "assembly_ms": asm_ms, "solve_ms": solve_ms,
+        "iterations_batched": [int(s.iterations) for s in st0], "iterations_fp64": fp64_iters,
+        "timing": "wall clock around device-synchronised steps, max over ranks",
+    }
 
 
 def single_solves(sb, level, k, dev):

@@ -247,6 +247,33 @@ SB_API int sb_gmres_mixed_device(const sb_operator* op, const sb_complex* b_dev,
 SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs,
                                     const sb_complex* amps, int64_t r, sb_complex* rhs_dev);
 
+/* ---- batched frequency sweep ----
+ * Replaces the reference's per-frequency loop (crates/sonium-bem/src/core/solver/
+ * frequency_sweep.rs:541-600: build_tbem_system_stabilized at :20, then one GMRES solve per
+ * frequency) for many independent instances (mesh, physics, beta) on one device: one persistent
+ * assembly launch writes every instance's complex64 matrix (the SB_PRECISION_FP32 arithmetic of
+ * sb_assemble), and one batched mixed-precision solve (the sb_gmres_mixed algorithm and
+ * statistics per instance, zero initial guess) advances all instances in lockstep, each with its
+ * own convergence state. Meshes must carry no prescribed boundary values (rigid or admittance
+ * surfaces; the right-hand side is an incident field): SB_ERR_INVALID_ARGUMENT otherwise. The
+ * meshes must outlive the batch. */
+typedef struct sb_batch sb_batch;
+SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physics* physics,
+                           const sb_complex* betas, sb_batch** out);
+SB_API int sb_batch_destroy(sb_batch* batch);
+SB_API int sb_batch_assemble(sb_batch* batch);
+/* Incident plane wave of unit amplitude along `direction` (3 doubles) for every instance. */
+SB_API int sb_batch_set_rhs_plane_wave(sb_batch* batch, const double* direction);
+/* Right-hand side of one instance from host memory (n complex128). */
+SB_API int sb_batch_set_rhs(sb_batch* batch, int64_t index, const sb_complex* b);
+/* stats: count entries, one per instance (device_ms is the whole batch's time). */
+SB_API int sb_batch_solve(sb_batch* batch, const sb_ir_config* cfg, sb_gmres_stats* stats);
+SB_API int sb_batch_solution(const sb_batch* batch, int64_t index, sb_complex* x);
+/* The assembled complex64 matrix of one instance, row-major n x n. */
+SB_API int sb_batch_matrix_c64(const sb_batch* batch, int64_t index, sb_complex32* matrix);
+/* Device time of the last sb_batch_assemble and sb_batch_solve, milliseconds. */
+SB_API int sb_batch_timings(const sb_batch* batch, double* assembly_ms, double* solve_ms);
+
 /* ---- timing (no reference counterpart: instrumentation, the PerfModel / runtime-stats role of
  * crates/sonium-compute/src/perf.rs:1-30) ---- */
 /* Kernel classes timed by CUDA events recorded on their launching stream when profiling is on. */

@@ -133,6 +133,15 @@ _SIGNATURES = {
     "sb_gmres_mixed": ([P, P, P, ct.POINTER(SbIrConfig), P, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_mixed_device": ([P, P, P, ct.c_int, ct.POINTER(SbIrConfig), ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_rhs_plane_wave_device": ([P, P, P, ct.c_int64, P], ct.c_int),
+    "sb_batch_create": ([ct.c_int64, P, P, P, ct.POINTER(P)], ct.c_int),
+    "sb_batch_destroy": ([P], ct.c_int),
+    "sb_batch_assemble": ([P], ct.c_int),
+    "sb_batch_set_rhs_plane_wave": ([P, P], ct.c_int),
+    "sb_batch_set_rhs": ([P, ct.c_int64, P], ct.c_int),
+    "sb_batch_solve": ([P, ct.POINTER(SbIrConfig), P], ct.c_int),
+    "sb_batch_solution": ([P, ct.c_int64, P], ct.c_int),
+    "sb_batch_matrix_c64": ([P, ct.c_int64, P], ct.c_int),
+    "sb_batch_timings": ([P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
     "sb_profile_enable": ([ct.c_int], ct.c_int),
     "sb_profile_read": ([ct.POINTER(SbProfile), ct.c_int], ct.c_int),
     "sb_event_create": ([ct.POINTER(P)], ct.c_int),

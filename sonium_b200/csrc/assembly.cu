@@ -620,21 +620,20 @@ __device__ __forceinline__ void sincos_f32(float x, float* so, float* co) {
 
 constexpr int kFar32Rows = 64;
 
+// One (128-column tile, 64-row block) of the FP32 far field; all 128 threads of the CTA call it.
 template <bool kWithRhs>
-__global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp32,
-                                                    const double* __restrict__ elem, int64_t n,
-                                                    int64_t ld, const double* __restrict__ coef,
-                                                    double k, float2* __restrict__ A32, int64_t lda32,
-                                                    double2* __restrict__ far_part, int64_t n_tiles) {
+__device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const double* __restrict__ elem,
+                                           int64_t n, int64_t ld, const double* __restrict__ coef, double k,
+                                           float2* __restrict__ A32, int64_t lda32, double2* __restrict__ far_part,
+                                           int64_t n_tiles, int64_t tile, int64_t row0) {
     __shared__ double sx[kFar32Rows][3];
     __shared__ float snx[kFar32Rows][3];
     __shared__ double sg[4][kFarTile];    // column: level-0 centre and near threshold
     __shared__ float scf[8][kFarTile];    // column: matrix weights (cG, cH, cHt, cE)
     __shared__ double sred[kFarTile / 32][2];
     const int tid = threadIdx.x;
-    const int64_t tile = blockIdx.x;
     const int64_t j = tile * kFarTile + tid;
-    const int64_t row0 = blockIdx.y * (int64_t)kFar32Rows;
+    __syncthreads();  // a previous tile of a persistent CTA may still read the shared arrays
     for (int t = tid; t < kFar32Rows * 3; t += kFarTile) {
         const int r = t / 3, c = t % 3;
         const int64_t i = row0 + r;
@@ -767,6 +766,16 @@ __global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp
             __syncthreads();
         }
     }
+}
+
+template <bool kWithRhs>
+__global__ void __launch_bounds__(kFarTile) k_far32(const float* __restrict__ qp32,
+                                                    const double* __restrict__ elem, int64_t n,
+                                                    int64_t ld, const double* __restrict__ coef,
+                                                    double k, float2* __restrict__ A32, int64_t lda32,
+                                                    double2* __restrict__ far_part, int64_t n_tiles) {
+    far32_tile<kWithRhs>(qp32, elem, n, ld, coef, k, A32, lda32, far_part, n_tiles, blockIdx.x,
+                         blockIdx.y * (int64_t)kFar32Rows);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1013,15 +1022,9 @@ __global__ void __launch_bounds__(32 * kNearWarps) k_near(const double* __restri
 // ---------------------------------------------------------------------------------------------
 // Self kernel: one warp per element (singular_integration_with_params_mode, singular.rs:297-614).
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, int64_t n,
-                                              int64_t ld, const double* __restrict__ coef,
-                                              double k, double2* __restrict__ A64,
-                                              float2* __restrict__ A32, int64_t lda32,
-                                              double2* __restrict__ self_rhs,
-                                              double2* __restrict__ diag) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp;
-    if (i >= n) return;
+// Channel sums of the self pair of element i, partial per lane (reduce with warp_reduce).
+__device__ __forceinline__ void self_channels(Acc& a, const double* __restrict__ elem, int64_t ld, int64_t i,
+                                              double k, int lane) {
     const double k2 = k * k;
     const double x0 = E(ECX, i), x1 = E(ECY, i), x2 = E(ECZ, i);
     const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
@@ -1042,7 +1045,6 @@ __global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, i
     const int per_edge = n_edge + n_bulk;
     const double csi6[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
     const double eta6[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
-    Acc a;
     double edge_r = 0.0, edge_i = 0.0;
     for (int f = lane; f < 3 * per_edge; f += 32) {
         const int ieg = f / per_edge, rem = f % per_edge;
@@ -1122,21 +1124,105 @@ __global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, i
     }
     a.er += edge_r;
     a.ei += edge_i;
+}
+
+__device__ __forceinline__ void self_store(const Acc& t, const double* __restrict__ coef, int64_t ld, int64_t n,
+                                           int64_t i, double2* __restrict__ A64, float2* __restrict__ A32,
+                                           int64_t lda32, double2* __restrict__ self_rhs,
+                                           double2* __restrict__ diag) {
+    double2 v = combine(t, coef, ld, i, CF_CG);
+    v.x += coef[(int64_t)(CF_DIAG) * ld + i];
+    v.y += coef[(int64_t)(CF_DIAG + 1) * ld + i];
+    if (A64) A64[i * n + i] = v;
+    if (A32) A32[i * lda32 + i] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+    diag[i] = v;
+    double2 r = make_double2(coef[(int64_t)(CF_RHS) * ld + i], coef[(int64_t)(CF_RHS + 1) * ld + i]);
+    if (self_rhs) {
+        const double2 c = combine(t, coef, ld, i, CF_DG);
+        r.x += c.x;
+        r.y += c.y;
+        self_rhs[i] = r;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, int64_t n,
+                                              int64_t ld, const double* __restrict__ coef,
+                                              double k, double2* __restrict__ A64,
+                                              float2* __restrict__ A32, int64_t lda32,
+                                              double2* __restrict__ self_rhs,
+                                              double2* __restrict__ diag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp;
+    if (i >= n) return;
+    Acc a;
+    self_channels(a, elem, ld, i, k, lane);
     const Acc t = warp_reduce(a);
-    if (lane == 0) {
-        double2 v = combine(t, coef, ld, i, CF_CG);
-        v.x += coef[(int64_t)(CF_DIAG) * ld + i];
-        v.y += coef[(int64_t)(CF_DIAG + 1) * ld + i];
-        if (A64) A64[i * n + i] = v;
-        if (A32) A32[i * lda32 + i] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
-        diag[i] = v;
-        double2 r = make_double2(coef[(int64_t)(CF_RHS) * ld + i], coef[(int64_t)(CF_RHS + 1) * ld + i]);
-        if (self_rhs) {
-            const double2 c = combine(t, coef, ld, i, CF_DG);
-            r.x += c.x;
-            r.y += c.y;
+    if (lane == 0) self_store(t, coef, ld, n, i, A64, A32, lda32, self_rhs, diag);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Persistent batched assembly: every instance of a frequency sweep in one launch. The work list
+// is [far tiles of all instances | near pairs (4 per item) | self elements (4 per item)]; each CTA
+// walks it with a grid stride, so instances of any size share the SMs. Complex64 output
+// (SB_PRECISION_FP32 numerics); instances have no prescribed boundary values.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ int find_instance(const int64_t* __restrict__ pre, int ninst, int64_t item) {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kFarTile) k_assemble_batch(const BatchAsmInst* __restrict__ inst, int ninst,
+                                                             const int64_t* __restrict__ pre) {
+    __shared__ NearWarpSmem nsm[kNearWarps];
+    const int64_t* fpre = pre;
+    const int64_t* npre = pre + (ninst + 1);
+    const int64_t* spre = pre + 2 * (ninst + 1);
+    const int64_t nf = fpre[ninst], nn = npre[ninst], ns = spre[ninst];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int64_t item = blockIdx.x; item < nf + nn + ns; item += gridDim.x) {
+        if (item < nf) {
+            const int b = find_instance(fpre, ninst, item);
+            const BatchAsmInst I = inst[b];
+            const int64_t local = item - fpre[b];
+            const int64_t nrb = (I.n + kFar32Rows - 1) / kFar32Rows;
+            far32_tile<false>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr, I.n_tiles,
+                              local / nrb, (local % nrb) * kFar32Rows);
+        } else if (item < nf + nn) {
+            const int64_t it = item - nf;
+            const int b = find_instance(npre, ninst, it);
+            const BatchAsmInst I = inst[b];
+            const int64_t p = (it - npre[b]) * kNearWarps + warp;
+            if (p < I.nnz) {
+                int64_t lo = 0, hi = I.n - 1;
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi + 1) >> 1;
+                    if (I.near_ptr[mid] <= p) lo = mid; else hi = mid - 1;
+                }
+                const int64_t i = lo, j = I.near_col[p];
+                Acc a;
+                near_pair_channels(a, nsm[warp], I.elem, I.ld, i, j, I.k, I.k * I.k, lane);
+                const Acc t = warp_reduce(a);
+                if (lane == 0) {
+                    const double2 v = combine(t, I.coef, I.ld, j, CF_CG);
+                    I.A32[i * I.lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+                }
+            }
+        } else {
+            const int64_t it = item - nf - nn;
+            const int b = find_instance(spre, ninst, it);
+            const BatchAsmInst I = inst[b];
+            const int64_t e = (it - spre[b]) * kNearWarps + warp;
+            if (e < I.n) {
+                Acc a;
+                self_channels(a, I.elem, I.ld, e, I.k, lane);
+                const Acc t = warp_reduce(a);
+                if (lane == 0) self_store(t, I.coef, I.ld, I.n, e, nullptr, I.A32, I.lda32, nullptr, I.diag);
+            }
         }
-        self_rhs ? (void)(self_rhs[i] = r) : (void)0;
     }
 }
 
@@ -1409,6 +1495,40 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     op.beta_re = beta_re;
     op.beta_im = beta_im;
 }
+
+void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst* d_inst, DevBuf& pre_buf,
+                    cudaStream_t s, int device) {
+    const int ninst = static_cast<int>(h_inst.size());
+    std::vector<int64_t> pre(3 * (ninst + 1), 0);
+    for (int b = 0; b < ninst; ++b) {
+        const BatchAsmInst& I = h_inst[b];
+        pre[b + 1] = pre[b] + I.n_tiles * cdiv(I.n, kFar32Rows);
+        pre[(ninst + 1) + b + 1] = pre[(ninst + 1) + b] + cdiv(I.nnz, kNearWarps);
+        pre[2 * (ninst + 1) + b + 1] = pre[2 * (ninst + 1) + b] + cdiv(I.n, kNearWarps);
+    }
+    if (pre_buf.bytes < sizeof(int64_t) * pre.size()) pre_buf.alloc(sizeof(int64_t) * pre.size());
+    SB_CUDA(cudaMemcpyAsync(pre_buf.p, pre.data(), sizeof(int64_t) * pre.size(), cudaMemcpyHostToDevice, s));
+    int per_sm = 0;
+    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_batch, kFarTile, 0));
+    const int64_t items = pre[ninst] + pre[2 * (ninst + 1) - 1] + pre[3 * (ninst + 1) - 1];
+    const int64_t grid = std::min<int64_t>(items, static_cast<int64_t>(std::max(per_sm, 1)) * device_sm_count(device));
+    ProfScope prof(SB_PROF_FAR, s);
+    k_assemble_batch<<<static_cast<unsigned>(std::max<int64_t>(grid, 1)), kFarTile, 0, s>>>(d_inst, ninst,
+                                                                                           pre_buf.as<int64_t>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+void coefficients_for(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im, double* coef,
+                      cudaStream_t s) {
+    k_coefficients<<<cdiv(m.ld, 256), 256, 0, s>>>(m.n, m.ld, m.bc_kind.as<int32_t>(), m.bc_value.as<double2>(),
+                                                   m.has_adm.as<uint8_t>(), m.adm.as<double2>(), ph.tau,
+                                                   ph.pressure_factor, make_double2(beta_re, beta_im), coef);
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+int coefficient_fields() { return CF_FIELDS; }
 
 void incident_plane_wave(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im,
                          const double* dirs_host, const double* amps_host, int64_t r,

@@ -1,0 +1,1019 @@
+// Batched frequency sweep: many independent TBEM instances (mesh, wavenumber) assembled in one
+// persistent launch and solved together by a batched mixed-precision GMRES.
+//
+// Reference: the frequency sweep re-assembles and solves one frequency after another
+// (crates/sonium-bem/src/core/solver/frequency_sweep.rs:541-600, build_tbem_system_stabilized at
+// :20); each solve is gmres_core (crates/sonium-solvers/crates/sonium-solvers-iterative/src/
+// gmres.rs:631-1047). Here all instances advance in lockstep: every kernel of an Arnoldi step
+// covers all instances through a flattened list of row blocks (an instance's blocks are
+// contiguous; a block finds its instance by binary search over a prefix array), every instance
+// carries its own convergence state, and kernels of an instance whose flag says "done" return at
+// once (the per-instance mask). One restart cycle of the whole batch is one CUDA graph. The
+// arithmetic per instance is the single-instance mixed solver's (gmres.cu, gmres_mixed_ir): FP32
+// inner GMRES on the complex64 matrix, FP64 Hessenberg / Givens, FP64 refinement residual with
+// FP64 accumulation, the same stopping rules and statistics.
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "sb_blas.cuh"
+#include "sb_device.cuh"
+#include "sb_gemv.cuh"
+#include "sb_internal.cuh"
+#include "sb_krylov.cuh"
+#include "sb_profile.cuh"
+
+struct sb_mesh {
+    sb::Mesh* m;
+};
+
+namespace sb {
+
+// Per-instance device descriptor of the batched solver.
+struct BInst {
+    const float2* A;  // complex64 matrix, row-major, even leading dimension lda
+    int64_t lda, n, ldv;
+    float2* V;        // Krylov basis, (m + 1) x ldv
+    float2* w;
+    float2* rb;       // inner right-hand side r / ||r||
+    float2* d;        // inner solution
+    float2* rq;       // inner residual at restarts
+    double2* x;       // FP64 solution
+    const double2* b; // FP64 right-hand side
+    double2* r;       // FP64 residual b - A x
+    KState* st;
+    double2 *H, *cs, *sn, *g, *y, *red, *red2, *part;
+    double* pnorm;    // per-block / per-chunk squared-norm partials
+    double* nrm;      // [0] first Gram-Schmidt |w|^2, [1] second pass, [2] reduced norm^2
+    double* scal;     // [0] 1 / ||r||, [1] ||r||, [2] inner beta, [3] inner tolerance, [4] inner ||b||
+    int* outer;       // 1 while the instance refines
+    int* live;        // 1 while its inner solve runs
+    int* brk;         // inner breakdown before the first step
+};
+
+namespace {
+
+constexpr int kChunk = 256;  // vector rows per CTA of the vector kernels
+constexpr int kBDotVecs = 8;
+constexpr int kScal = 5;
+
+__device__ __forceinline__ int find_inst(const int64_t* __restrict__ pre, int ninst, int64_t unit) {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= unit) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Which per-instance flag gates a launch.
+enum GateKind { G_NONE = 0, G_OUTER = 1, G_LIVE = 2, G_ACTIVE = 3, G_REORTH = 4, G_RESTART = 5 };
+__device__ __forceinline__ bool open_gate(const BInst& I, int gk) {
+    switch (gk) {
+        case G_OUTER: return *I.outer != 0;
+        case G_LIVE: return *I.live != 0;
+        case G_ACTIVE: return I.st->active != 0;
+        case G_REORTH: return I.st->active != 0 && I.st->reorth != 0;
+        case G_RESTART: return *I.live != 0 && I.st->reason == 0;
+        default: return true;
+    }
+}
+
+// Matrix-vector products over the flattened row blocks (kGemvRows rows per CTA).
+// mode 0: w = A V_j; mode 1: rq = rb - A d (partial norms).
+__global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restrict__ inst,
+                                                          const int64_t* __restrict__ pre, int ninst, int mode,
+                                                          int j, int gk) {
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const int64_t blk = blockIdx.x - pre[b];
+    if (mode == 0)
+        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.V + (int64_t)j * I.ldv, I.w,
+                                                                    nullptr, nullptr, blk);
+    else
+        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.d, I.rq, I.rb, I.pnorm, blk);
+}
+
+// r = b - A x with FP64 vectors and FP64 accumulation on the complex64 matrix, partial norms.
+__global__ void __launch_bounds__(kGemvThreads) k_bres64(const BInst* __restrict__ inst,
+                                                         const int64_t* __restrict__ pre, int ninst, int gk) {
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, true>(I.A, I.n, I.lda, I.x, I.r, I.b, I.pnorm,
+                                                               blockIdx.x - pre[b]);
+}
+
+// Per-chunk squared norms: sel 0 = rb, 1 = b, 2 = b - r (= A x).
+__global__ void __launch_bounds__(kChunk) k_bvnorm(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+                                                   int ninst, int sel, int gk) {
+    __shared__ double red[kChunk / 32];
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const int64_t chunk = blockIdx.x - pre[b];
+    const int64_t r = chunk * kChunk + threadIdx.x;
+    double v[1] = {0.0};
+    if (r < I.n) {
+        if (sel == 0) {
+            const float2 a = I.rb[r];
+            v[0] = (double)a.x * a.x + (double)a.y * a.y;
+        } else if (sel == 1) {
+            const double2 a = I.b[r];
+            v[0] = a.x * a.x + a.y * a.y;
+        } else {
+            const double2 a = I.b[r], q = I.r[r];
+            const double ar = a.x - q.x, ai = a.y - q.y;
+            v[0] = ar * ar + ai * ai;
+        }
+    }
+    block_sum<1, kChunk>(v, red);
+    if (threadIdx.x == 0) I.pnorm[chunk] = v[0];
+}
+
+// nrm[slot] = sum of the instance's partials (their count is the instance's span of `pre`).
+__global__ void k_bsum_partials(const BInst* __restrict__ inst, const int64_t* __restrict__ pre, int slot, int gk) {
+    const BInst& I = inst[blockIdx.x];
+    if (!open_gate(I, gk)) return;
+    const int64_t cnt = pre[blockIdx.x + 1] - pre[blockIdx.x];
+    double s = 0.0;
+    for (int64_t c = threadIdx.x; c < cnt; c += 32) s += I.pnorm[c];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) I.nrm[slot] = s;
+}
+
+// Gram-Schmidt dots over the flattened chunks: part[chunk * (k + 1) + i] = V_i^H w (i < k),
+// |w|^2 at i = k.
+__global__ void __launch_bounds__(kChunk) k_bdots(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+                                                  int ninst, int k, int gk) {
+    __shared__ double red[(kChunk / 32) * 2 * kBDotVecs];
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const int64_t chunk = blockIdx.x - pre[b];
+    const int64_t r = chunk * kChunk + threadIdx.x;
+    const int i0 = blockIdx.y * kBDotVecs;
+    double acc[2 * kBDotVecs];
+#pragma unroll
+    for (int t = 0; t < 2 * kBDotVecs; ++t) acc[t] = 0.0;
+    if (r < I.n) {
+        const float2 wv = I.w[r];
+#pragma unroll
+        for (int t = 0; t < kBDotVecs; ++t) {
+            const int i = i0 + t;
+            if (i < k) {
+                const float2 v = I.V[i * I.ldv + r];
+                acc[2 * t] = (double)v.x * wv.x + (double)v.y * wv.y;
+                acc[2 * t + 1] = (double)v.x * wv.y - (double)v.y * wv.x;
+            } else if (i == k) {
+                acc[2 * t] = (double)wv.x * wv.x + (double)wv.y * wv.y;
+            }
+        }
+    }
+    block_sum<2 * kBDotVecs, kChunk>(acc, red);
+    if (threadIdx.x == 0)
+        for (int t = 0; t < kBDotVecs; ++t) {
+            const int i = i0 + t;
+            if (i <= k) I.part[chunk * (k + 1) + i] = make_double2(acc[2 * t], acc[2 * t + 1]);
+        }
+}
+
+// red (second = 0) or red2 (second = 1) [i] = sum over the instance's chunks, i <= k.
+__global__ void k_breduce(const BInst* __restrict__ inst, const int64_t* __restrict__ pre, int k, int second, int gk) {
+    const BInst& I = inst[blockIdx.y];
+    if (!open_gate(I, gk)) return;
+    const int i = blockIdx.x;
+    const int64_t chunks = pre[blockIdx.y + 1] - pre[blockIdx.y];
+    double sr = 0.0, si = 0.0;
+    for (int64_t c = threadIdx.x; c < chunks; c += 32) {
+        const double2 v = I.part[c * (k + 1) + i];
+        sr += v.x;
+        si += v.y;
+    }
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    if (threadIdx.x == 0) (second ? I.red2 : I.red)[i] = make_double2(sr, si);
+}
+
+// w -= sum_{i<k} coeff[i] V_i (coeff = red or red2), partial |w|^2 per chunk.
+__global__ void __launch_bounds__(kChunk) k_bproject(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+                                                     int ninst, int k, int second, int gk) {
+    __shared__ double2 sc[kMaxKrylov + 1];
+    __shared__ double red[kChunk / 32];
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const double2* coeff = second ? I.red2 : I.red;
+    for (int t = threadIdx.x; t < k; t += kChunk) sc[t] = coeff[t];
+    __syncthreads();
+    const int64_t chunk = blockIdx.x - pre[b];
+    const int64_t r = chunk * kChunk + threadIdx.x;
+    double nr2[1] = {0.0};
+    if (r < I.n) {
+        const float2 w0 = I.w[r];
+        double ar = w0.x, ai = w0.y;
+        for (int i = 0; i < k; ++i) {
+            const float2 v = I.V[i * I.ldv + r];
+            ar -= sc[i].x * v.x - sc[i].y * v.y;
+            ai -= sc[i].x * v.y + sc[i].y * v.x;
+        }
+        const float2 o = make_float2(static_cast<float>(ar), static_cast<float>(ai));
+        I.w[r] = o;
+        nr2[0] = (double)o.x * o.x + (double)o.y * o.y;
+    }
+    block_sum<1, kChunk>(nr2, red);
+    if (threadIdx.x == 0) I.pnorm[chunk] = nr2[0];
+}
+
+__global__ void k_bafter_first(const BInst* __restrict__ inst, int ninst, int j) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ninst) return;
+    const BInst& I = inst[b];
+    after_first_dev(I.st, I.red, I.nrm + 0, I.H, j);
+}
+
+__global__ void k_bgivens(const BInst* __restrict__ inst, int ninst, int j) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ninst) return;
+    const BInst& I = inst[b];
+    givens_step_dev(I.st, I.red2, I.nrm + 1, I.H, I.cs, I.sn, I.g, j);
+}
+
+// V_{j+1} = w / ||w|| for the instances still running.
+__global__ void __launch_bounds__(kChunk) k_bnext(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+                                                  int ninst, int j) {
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!I.st->active) return;
+    const int64_t r = (blockIdx.x - pre[b]) * kChunk + threadIdx.x;
+    if (r >= I.n) return;
+    const double s = I.st->inv_wn;
+    const float2 v = I.w[r];
+    I.V[(int64_t)(j + 1) * I.ldv + r] = make_float2(static_cast<float>(v.x * s), static_cast<float>(v.y * s));
+}
+
+// Vector updates over the flattened chunks.
+enum VecOp {
+    OP_B_TO_R = 0,    // r = b, x = 0
+    OP_R_TO_RB = 1,   // rb = r / ||r|| (complex64), d = 0
+    OP_RB_TO_V0 = 2,  // V_0 = rb / beta (first inner cycle)
+    OP_RQ_TO_V0 = 3,  // V_0 = rq / beta (restarts)
+    OP_D_UPDATE = 4,  // d += V y (k = jdone)
+    OP_X_UPDATE = 5,  // x += ||r|| d
+};
+__global__ void __launch_bounds__(kChunk) k_bvec(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+                                                 int ninst, int op, int gk) {
+    __shared__ double2 sy[kMaxKrylov + 1];
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const int64_t r = (blockIdx.x - pre[b]) * kChunk + threadIdx.x;
+    if (op == OP_D_UPDATE) {
+        const int k = I.st->jdone;
+        for (int t = threadIdx.x; t < k; t += kChunk) sy[t] = I.y[t];
+        __syncthreads();
+        if (r >= I.n) return;
+        double sr = 0.0, si = 0.0;
+        for (int i = 0; i < k; ++i) {
+            const float2 v = I.V[i * I.ldv + r];
+            sr += sy[i].x * v.x - sy[i].y * v.y;
+            si += sy[i].x * v.y + sy[i].y * v.x;
+        }
+        const float2 d = I.d[r];
+        I.d[r] = make_float2(static_cast<float>(d.x + sr), static_cast<float>(d.y + si));
+        return;
+    }
+    if (r >= I.n) return;
+    switch (op) {
+        case OP_B_TO_R:
+            I.r[r] = I.b[r];
+            I.x[r] = make_double2(0.0, 0.0);
+            break;
+        case OP_R_TO_RB: {
+            const double s = I.scal[0];
+            I.rb[r] = make_float2(static_cast<float>(I.r[r].x * s), static_cast<float>(I.r[r].y * s));
+            I.d[r] = make_float2(0.f, 0.f);
+            break;
+        }
+        case OP_RB_TO_V0:
+        case OP_RQ_TO_V0: {
+            const float2 v = op == OP_RB_TO_V0 ? I.rb[r] : I.rq[r];
+            const double s = 1.0 / I.scal[2];
+            I.V[r] = make_float2(static_cast<float>(v.x * s), static_cast<float>(v.y * s));
+            break;
+        }
+        case OP_X_UPDATE: {
+            const double s = I.scal[1];
+            const float2 d = I.d[r];
+            I.x[r] = make_double2(I.x[r].x + s * d.x, I.x[r].y + s * d.y);
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// Cycle start: live instances get H = 0, g = (beta, 0, ...) and an active state; the others an
+// inactive state, so every gated kernel of the cycle skips them.
+__global__ void k_bcycle_init(const BInst* __restrict__ inst, int m) {
+    const BInst& I = inst[blockIdx.x];
+    cycle_init_dev(I.st, I.H, I.g, m, 1, I.scal[2], I.scal[4], I.scal[3], threadIdx.x, blockDim.x, *I.live != 0);
+}
+
+__global__ void k_bupper(const BInst* __restrict__ inst, int ninst) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ninst) return;
+    const BInst& I = inst[b];
+    if (!*I.live) return;
+    upper_solve_dev(I.st, I.H, I.g, I.y);
+}
+
+// Inner-solve control per instance (thread per instance), the decisions gmres_core takes between
+// cycles (gmres.rs:790-1047 with the refinement caller's trusted estimate):
+// mode 0, inner start: live = outer; beta = ||rb|| (nrm[2]) becomes the inner ||b||; a zero or
+//   non-finite beta is a breakdown before the first step.
+// mode 1, after a cycle: an estimated convergence or an inner breakdown (reason != 0), or the last
+//   allowed cycle, ends the inner solve; otherwise the restart residual norm (nrm[2]) is the next
+//   beta, and the solve ends when it meets the inner tolerance or is not finite.
+__global__ void k_bcontrol(const BInst* __restrict__ inst, int ninst, int mode, int last) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ninst) return;
+    const BInst& I = inst[b];
+    if (mode == 0) {
+        *I.brk = 0;
+        *I.live = *I.outer;
+        if (!*I.live) return;
+        const double beta = sqrt(I.nrm[2]);
+        I.scal[4] = beta < 1e-15 ? 1.0 : beta;
+        I.scal[2] = beta;
+        if (!isfinite(beta) || beta == 0.0) {
+            *I.live = 0;
+            *I.brk = 1;
+        }
+        return;
+    }
+    if (!*I.live) return;
+    if (I.st->reason != 0 || last) {
+        *I.live = 0;
+        return;
+    }
+    const double beta = sqrt(I.nrm[2]);
+    I.scal[2] = beta;
+    if (beta / I.scal[4] < I.scal[3] || !isfinite(beta) || beta == 0.0) *I.live = 0;
+}
+
+int64_t cdiv64(int64_t a, int64_t b) { return (a + b - 1) / b; }
+size_t round256(size_t v) { return (v + 255) / 256 * 256; }
+
+struct Pinned {
+    void* p = nullptr;
+    void alloc(size_t n) {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        SB_CUDA(cudaMallocHost(&p, n));
+    }
+    ~Pinned() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Batch object
+// ---------------------------------------------------------------------------------------------
+struct Batch {
+    int device = 0;
+    int ninst = 0;
+    int64_t m = 0;  // Krylov dimension the workspace was sized for
+    std::vector<Mesh*> meshes;
+    std::vector<sb_physics> phys;
+    std::vector<double2> beta;
+    std::vector<BatchAsmInst> asm_h;
+    std::vector<double2*> rhs;  // per-instance right-hand side (pool_rhs)
+    std::vector<BInst> h;
+    std::vector<int64_t> pre4, pre256;
+    DevBuf asm_d, inst_d, pre4_d, pre256_d, pre_asm;
+    DevBuf pool_mat, pool_rhs, pool_f32, pool_f64, pool_small, pool_state;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t graph_kernels = 0;
+    bool graph_prof = false;
+    std::vector<ProfPair> prof_pairs;
+    Pinned pin;  // host mirror of the per-instance states, norms, scalars and flags
+    bool assembled = false, solved = false;
+    double last_assembly_ms = 0.0, last_solve_ms = 0.0;
+    void reset_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        profile_release(prof_pairs);
+    }
+    ~Batch() {
+        reset_graph();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// The device block pool_state and its pinned host mirror share one layout, so one copy moves a
+// group of fields for all instances.
+struct StateView {
+    KState* st;
+    double* nrm;   // 3 per instance
+    double* scal;  // kScal per instance
+    int* outer;
+    int* live;
+    int* brk;
+};
+StateView state_view(void* base, int ni) {
+    char* p = static_cast<char*>(base);
+    StateView v;
+    v.st = reinterpret_cast<KState*>(p);
+    p += round256(sizeof(KState) * ni);
+    v.nrm = reinterpret_cast<double*>(p);
+    p += round256(sizeof(double) * 3 * ni);
+    v.scal = reinterpret_cast<double*>(p);
+    p += round256(sizeof(double) * kScal * ni);
+    v.outer = reinterpret_cast<int*>(p);
+    p += round256(sizeof(int) * ni);
+    v.live = reinterpret_cast<int*>(p);
+    p += round256(sizeof(int) * ni);
+    v.brk = reinterpret_cast<int*>(p);
+    return v;
+}
+size_t state_bytes(int ni) {
+    return round256(sizeof(KState) * ni) + round256(sizeof(double) * 3 * ni) +
+           round256(sizeof(double) * kScal * ni) + 3 * round256(sizeof(int) * ni);
+}
+
+}  // namespace
+
+// Sizes the solver workspace of every instance for restart m and builds the descriptors.
+static void batch_workspace(Batch& B, int64_t m) {
+    if (B.m == m) return;
+    B.reset_graph();
+    B.m = 0;
+    B.solved = false;
+    const int ni = B.ninst;
+    size_t f32 = 0, f64 = 0, small = 0;
+    for (int b = 0; b < ni; ++b) {
+        const int64_t n = B.meshes[b]->n, ldv = (n + 1) / 2 * 2;
+        const int64_t chunks = cdiv64(n, kChunk);
+        f32 += round256(sizeof(float2) * (m + 1) * ldv) + 4 * round256(sizeof(float2) * ldv);
+        f64 += 2 * round256(sizeof(double2) * ldv);
+        small += round256(sizeof(double2) * (m + 1) * m) + 2 * round256(sizeof(double2) * m) +
+                 2 * round256(sizeof(double2) * (m + 1)) + 2 * round256(sizeof(double2) * (m + 2)) +
+                 round256(sizeof(double2) * chunks * (m + 2)) +
+                 round256(sizeof(double) * std::max(cdiv64(n, kGemvRows), chunks));
+    }
+    B.pool_f32.alloc(f32);
+    B.pool_f64.alloc(f64);
+    B.pool_small.alloc(small);
+    B.pool_state.alloc(state_bytes(ni));
+    B.pin.alloc(state_bytes(ni));
+    SB_CUDA(cudaMemset(B.pool_state.p, 0, state_bytes(ni)));
+    std::memset(B.pin.p, 0, state_bytes(ni));
+    const StateView dv = state_view(B.pool_state.p, ni);
+    char* pf32 = B.pool_f32.as<char>();
+    char* pf64 = B.pool_f64.as<char>();
+    char* ps = B.pool_small.as<char>();
+    auto take = [](char*& pool, size_t bytes) {
+        char* p = pool;
+        pool += round256(bytes);
+        return p;
+    };
+    B.h.assign(ni, BInst{});
+    B.pre4.assign(ni + 1, 0);
+    B.pre256.assign(ni + 1, 0);
+    for (int b = 0; b < ni; ++b) {
+        const int64_t n = B.meshes[b]->n, ldv = (n + 1) / 2 * 2;
+        const int64_t chunks = cdiv64(n, kChunk);
+        BInst& I = B.h[b];
+        I.A = B.asm_h[b].A32;
+        I.lda = B.asm_h[b].lda32;
+        I.n = n;
+        I.ldv = ldv;
+        I.V = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * (m + 1) * ldv));
+        I.w = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+        I.rb = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+        I.d = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+        I.rq = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+        I.x = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
+        I.r = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
+        I.b = B.rhs[b];
+        I.H = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 1) * m));
+        I.cs = reinterpret_cast<double2*>(take(ps, sizeof(double2) * m));
+        I.sn = reinterpret_cast<double2*>(take(ps, sizeof(double2) * m));
+        I.g = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 1)));
+        I.y = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 1)));
+        I.red = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 2)));
+        I.red2 = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 2)));
+        I.part = reinterpret_cast<double2*>(take(ps, sizeof(double2) * chunks * (m + 2)));
+        I.pnorm = reinterpret_cast<double*>(take(ps, sizeof(double) * std::max(cdiv64(n, kGemvRows), chunks)));
+        I.st = dv.st + b;
+        I.nrm = dv.nrm + 3 * b;
+        I.scal = dv.scal + kScal * b;
+        I.outer = dv.outer + b;
+        I.live = dv.live + b;
+        I.brk = dv.brk + b;
+        B.pre4[b + 1] = B.pre4[b] + cdiv64(n, kGemvRows);
+        B.pre256[b + 1] = B.pre256[b] + chunks;
+    }
+    B.inst_d.alloc(sizeof(BInst) * ni);
+    B.pre4_d.alloc(sizeof(int64_t) * (ni + 1));
+    B.pre256_d.alloc(sizeof(int64_t) * (ni + 1));
+    SB_CUDA(cudaMemcpy(B.inst_d.p, B.h.data(), sizeof(BInst) * ni, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemcpy(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
+    SB_CUDA(cudaMemcpy(B.pre256_d.p, B.pre256.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
+    B.m = m;
+}
+
+// One Arnoldi step of every running instance (every launch gated per instance).
+static void batch_step(Batch& B, int j) {
+    const BInst* I = B.inst_d.as<BInst>();
+    const int ni = B.ninst;
+    const unsigned g4 = static_cast<unsigned>(B.pre4.back()), g256 = static_cast<unsigned>(B.pre256.back());
+    const int64_t* p4 = B.pre4_d.as<int64_t>();
+    const int64_t* p256 = B.pre256_d.as<int64_t>();
+    const int k = j + 1;
+    const cudaStream_t s = B.stream;
+    const unsigned gi = static_cast<unsigned>(cdiv64(ni, 64));
+    capture_step(j);
+    {
+        ProfScope prof(SB_PROF_GEMV32, s);
+        k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 0, j, G_ACTIVE);
+        count_launch();
+    }
+    ProfScope prof(SB_PROF_ARNOLDI, s);
+    const dim3 gd(g256, static_cast<unsigned>(cdiv64(k + 1, kBDotVecs)));
+    const dim3 gr(static_cast<unsigned>(k + 1), static_cast<unsigned>(ni));
+    k_bdots<<<gd, kChunk, 0, s>>>(I, p256, ni, k, G_ACTIVE);
+    k_breduce<<<gr, 32, 0, s>>>(I, p256, k, 0, G_ACTIVE);
+    k_bproject<<<g256, kChunk, 0, s>>>(I, p256, ni, k, 0, G_ACTIVE);
+    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 0, G_ACTIVE);
+    k_bafter_first<<<gi, 64, 0, s>>>(I, ni, j);
+    k_bdots<<<gd, kChunk, 0, s>>>(I, p256, ni, k, G_REORTH);
+    k_breduce<<<gr, 32, 0, s>>>(I, p256, k, 1, G_REORTH);
+    k_bproject<<<g256, kChunk, 0, s>>>(I, p256, ni, k, 1, G_REORTH);
+    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 1, G_REORTH);
+    k_bgivens<<<gi, 64, 0, s>>>(I, ni, j);
+    k_bnext<<<g256, kChunk, 0, s>>>(I, p256, ni, j);
+    for (int t = 0; t < 11; ++t) count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+// One restart cycle of the whole batch: m Arnoldi steps captured once into a CUDA graph.
+static void batch_cycle(Batch& B) {
+    if (!B.exec || B.graph_prof != g_prof_on) {
+        B.reset_graph();
+        const int64_t before = kernel_count();
+        capture_begin(&B.prof_pairs);
+        SB_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (int j = 0; j < B.m; ++j) batch_step(B, j);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(B.stream, &g);
+            if (g) cudaGraphDestroy(g);
+            capture_end();
+            throw;
+        }
+        SB_CUDA(cudaStreamEndCapture(B.stream, &B.graph));
+        capture_end();
+        SB_CUDA(cudaGraphInstantiate(&B.exec, B.graph, 0));
+        B.graph_kernels = kernel_count() - before;
+        add_kernel_count(-B.graph_kernels);
+        B.graph_prof = g_prof_on;
+    }
+    SB_CUDA(cudaGraphLaunch(B.exec, B.stream));
+    add_kernel_count(B.graph_kernels);
+}
+
+// Mixed-precision iterative refinement of every instance in lockstep (gmres_mixed_ir semantics
+// per instance, zero initial guess).
+static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats) {
+    SB_CUDA(cudaSetDevice(B.device));
+    batch_workspace(B, cfg.inner_restart);
+    const int ni = B.ninst;
+    const BInst* I = B.inst_d.as<BInst>();
+    const unsigned g4 = static_cast<unsigned>(B.pre4.back()), g256 = static_cast<unsigned>(B.pre256.back());
+    const unsigned gi = static_cast<unsigned>(cdiv64(ni, 64));
+    const int64_t* p4 = B.pre4_d.as<int64_t>();
+    const int64_t* p256 = B.pre256_d.as<int64_t>();
+    const cudaStream_t s = B.stream;
+    const StateView hv = state_view(B.pin.p, ni);
+    const StateView dv = state_view(B.pool_state.p, ni);
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        SB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    };
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        SB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    };
+    auto launched = [&](int count) {
+        for (int t = 0; t < count; ++t) count_launch();
+        SB_CUDA(cudaGetLastError());
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    struct EvGuard {
+        cudaEvent_t& a;
+        cudaEvent_t& b;
+        ~EvGuard() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } evg{e0, e1};
+    SB_CUDA(cudaEventRecord(e0, s));
+    for (int b = 0; b < ni; ++b) stats[b] = sb_gmres_stats{};
+    // x = 0, r = b and ||b|| (with a zero initial guess the first residual needs no product).
+    k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_B_TO_R, G_NONE);
+    k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 1, G_NONE);
+    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_NONE);
+    launched(3);
+    d2h(hv.nrm, dv.nrm, sizeof(double) * 3 * ni);
+    SB_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> bnorm(ni), bref(ni), rn(ni), rel(ni, 1.0);
+    std::vector<int> status(ni, SB_SOLVER_MAX_ITERATIONS), outer(ni, 1), was_live(ni, 0);
+    for (int b = 0; b < ni; ++b) {
+        bnorm[b] = std::sqrt(hv.nrm[3 * b + 2]);
+        bref[b] = bnorm[b] < 1e-15 ? 1.0 : bnorm[b];
+        rn[b] = bnorm[b];
+    }
+    for (int64_t it = 0; it <= cfg.max_refinements; ++it) {
+        if (it > 0) {
+            // FP64 residual of the refining instances.
+            {
+                ProfScope prof(SB_PROF_GEMV32, s);
+                k_bres64<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, G_OUTER);
+            }
+            k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_OUTER);
+            launched(2);
+            d2h(hv.nrm, dv.nrm, sizeof(double) * 3 * ni);
+            SB_CUDA(cudaStreamSynchronize(s));
+            for (int b = 0; b < ni; ++b)
+                if (outer[b]) {
+                    rn[b] = std::sqrt(hv.nrm[3 * b + 2]);
+                    ++stats[b].matvecs;
+                }
+        }
+        int refining = 0;
+        for (int b = 0; b < ni; ++b) {
+            if (outer[b]) {
+                rel[b] = rn[b] / bref[b];
+                if (rel[b] < cfg.tolerance) {
+                    outer[b] = 0;
+                    status[b] = SB_SOLVER_CONVERGED;
+                } else if (!std::isfinite(rn[b])) {
+                    outer[b] = 0;
+                    status[b] = SB_SOLVER_NUMERICAL_ERROR;
+                } else if (it == cfg.max_refinements) {
+                    outer[b] = 0;
+                } else {
+                    ++refining;
+                    hv.scal[kScal * b + 0] = 1.0 / rn[b];
+                    hv.scal[kScal * b + 1] = rn[b];
+                    // The inner solve need not go further than the outer target asks.
+                    hv.scal[kScal * b + 3] = std::max(cfg.inner_tolerance, 0.5 * cfg.tolerance / rel[b]);
+                }
+            }
+            hv.outer[b] = outer[b];
+        }
+        if (!refining) break;
+        // The pinned mirror is modified only after a synchronisation that follows its last copy.
+        h2d(dv.outer, hv.outer, sizeof(int) * ni);
+        h2d(dv.scal, hv.scal, sizeof(double) * kScal * ni);
+        // Inner FP32 solves of A d = r / ||r||, in lockstep.
+        k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_R_TO_RB, G_OUTER);
+        k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 0, G_OUTER);
+        k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_OUTER);
+        k_bcontrol<<<gi, 64, 0, s>>>(I, ni, 0, 0);
+        launched(4);
+        for (int b = 0; b < ni; ++b) was_live[b] = outer[b];
+        for (int64_t cyc = 0; cyc < cfg.inner_max_iterations; ++cyc) {
+            const bool last = cyc + 1 == cfg.inner_max_iterations;
+            k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, cyc == 0 ? OP_RB_TO_V0 : OP_RQ_TO_V0, G_LIVE);
+            k_bcycle_init<<<ni, 256, 0, s>>>(I, static_cast<int>(B.m));
+            launched(2);
+            batch_cycle(B);
+            k_bupper<<<gi, 64, 0, s>>>(I, ni);
+            k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_D_UPDATE, G_LIVE);
+            launched(2);
+            if (!last) {
+                // restart residual rq = rb - A d of the instances that completed m steps
+                {
+                    ProfScope prof(SB_PROF_GEMV32, s);
+                    k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 1, 0, G_RESTART);
+                }
+                k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_RESTART);
+                launched(2);
+            }
+            d2h(hv.st, dv.st, sizeof(KState) * ni);
+            k_bcontrol<<<gi, 64, 0, s>>>(I, ni, 1, last ? 1 : 0);
+            launched(1);
+            d2h(hv.live, dv.live, sizeof(int) * ni);
+            d2h(hv.brk, dv.brk, sizeof(int) * ni);
+            SB_CUDA(cudaStreamSynchronize(s));
+            int steps_max = 0, running = 0;
+            for (int b = 0; b < ni; ++b) {
+                if (!was_live[b]) continue;
+                const KState& st = hv.st[b];
+                steps_max = std::max(steps_max, st.jdone);
+                stats[b].iterations += st.jdone;
+                stats[b].matvecs += st.jdone;
+                stats[b].matvecs_fp32 += st.jdone;
+                if (st.reason == 0) {
+                    ++stats[b].restarts;
+                    if (!last) {
+                        ++stats[b].matvecs;
+                        ++stats[b].matvecs_fp32;
+                    }
+                }
+                was_live[b] = hv.live[b];
+                running += hv.live[b];
+            }
+            profile_account(B.prof_pairs, steps_max);
+            if (!running) break;
+        }
+        // x += ||r|| d
+        k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_X_UPDATE, G_OUTER);
+        launched(1);
+        for (int b = 0; b < ni; ++b) {
+            if (!outer[b]) continue;
+            ++stats[b].refinements;
+            if (hv.brk[b]) {  // breakdown before the first inner step: x is unchanged, r stays valid
+                outer[b] = 0;
+                status[b] = SB_SOLVER_BREAKDOWN;
+            }
+        }
+    }
+    // Every instance stopped right after its residual was formed, so r = b - A x is current:
+    // ||A x|| = ||b - r|| gives the backward error without another product.
+    k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 2, G_NONE);
+    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 0, G_NONE);
+    launched(2);
+    d2h(hv.nrm, dv.nrm, sizeof(double) * 3 * ni);
+    SB_CUDA(cudaEventRecord(e1, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    B.last_solve_ms = ms;
+    B.solved = true;
+    for (int b = 0; b < ni; ++b) {
+        sb_gmres_stats& st = stats[b];
+        const double axn = std::sqrt(hv.nrm[3 * b + 0]);
+        st.estimated_residual = rel[b];
+        st.device_ms = ms;
+        if (!std::isfinite(rn[b]) || !std::isfinite(axn)) {
+            st.status = SB_SOLVER_NUMERICAL_ERROR;
+            st.converged = 0;
+            st.residual = INFINITY;
+            st.backward_error = INFINITY;
+            continue;
+        }
+        st.converged = status[b] == SB_SOLVER_CONVERGED ? 1 : 0;
+        st.status = status[b];
+        st.residual = bnorm[b] > 0 ? rn[b] / bnorm[b] : rn[b];
+        st.backward_error = rn[b] / std::max(axn + bnorm[b], 2.2250738585072014e-308);
+    }
+}
+
+}  // namespace sb
+
+using namespace sb;
+
+struct sb_batch {
+    sb::Batch* b;
+};
+
+namespace {
+
+template <class F>
+int guarded_batch(F&& f) {
+    try {
+        clear_error();
+        f();
+        return SB_OK;
+    } catch (const Error& e) {
+        set_error(e.status, e.msg);
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_error(SB_ERR_OUT_OF_MEMORY, "host allocation failed");
+        return SB_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        set_error(SB_ERR_CUDA, "unknown failure");
+        return SB_ERR_CUDA;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physics* physics,
+                           const sb_complex* betas, sb_batch** out) {
+    return guarded_batch([&] {
+        SB_REQUIRE(out, SB_ERR_INVALID_ARGUMENT, "batch: null output handle");
+        *out = nullptr;
+        SB_REQUIRE(meshes && physics && betas && count >= 1, SB_ERR_INVALID_ARGUMENT,
+                   "batch: need at least one instance with mesh, physics and beta");
+        SB_REQUIRE(count <= 4096, SB_ERR_INVALID_ARGUMENT, "batch: at most 4096 instances");
+        Batch* B = new Batch();
+        try {
+            B->ninst = static_cast<int>(count);
+            for (int64_t i = 0; i < count; ++i) {
+                SB_REQUIRE(meshes[i] && meshes[i]->m, SB_ERR_INVALID_ARGUMENT, "batch: null mesh");
+                SB_REQUIRE(sb_physics_validate(&physics[i]) == SB_OK, SB_ERR_INVALID_ARGUMENT,
+                           "batch: invalid physics parameters");
+                SB_REQUIRE(std::isfinite(betas[i].re) && std::isfinite(betas[i].im), SB_ERR_INVALID_ARGUMENT,
+                           "batch: beta must be finite");
+                Mesh* m = meshes[i]->m;
+                if (i == 0) B->device = m->device;
+                SB_REQUIRE(m->device == B->device, SB_ERR_INVALID_ARGUMENT, "batch: all meshes on one device");
+                SB_CUDA(cudaSetDevice(B->device));
+                if (!m->bc_kind.p) mesh_set_bc(*m, nullptr, nullptr, nullptr, nullptr);
+                SB_REQUIRE(!m->any_bc_value, SB_ERR_INVALID_ARGUMENT,
+                           "batch: meshes with prescribed boundary values are not batched (rigid or "
+                           "admittance surfaces only)");
+                B->meshes.push_back(m);
+                B->phys.push_back(physics[i]);
+                B->beta.push_back(make_double2(betas[i].re, betas[i].im));
+            }
+            SB_CUDA(cudaSetDevice(B->device));
+            ensure_tables(B->device);
+            SB_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+            // complex64 matrices, coefficient arrays and diagonals in one pool, right-hand sides
+            // in another (they survive workspace re-sizing).
+            size_t mat = 0, cof = 0, dg = 0, rhs = 0;
+            for (Mesh* m : B->meshes) {
+                const int64_t lda = (m->n + 1) / 2 * 2;
+                mat += round256(sizeof(float2) * m->n * lda);
+                cof += round256(sizeof(double) * coefficient_fields() * m->ld);
+                dg += round256(sizeof(double2) * m->n);
+                rhs += round256(sizeof(double2) * ((m->n + 1) / 2 * 2));
+            }
+            B->pool_mat.alloc(mat + cof + dg);
+            B->pool_rhs.alloc(rhs);
+            SB_CUDA(cudaMemset(B->pool_rhs.p, 0, rhs));
+            char* pm = B->pool_mat.as<char>();
+            char* pc = pm + mat;
+            char* pd = pc + cof;
+            char* pr = B->pool_rhs.as<char>();
+            for (int i = 0; i < B->ninst; ++i) {
+                Mesh* m = B->meshes[i];
+                BatchAsmInst A;
+                A.elem = m->elem.as<double>();
+                A.qp32 = m->qp32.as<float>();
+                A.n = m->n;
+                A.ld = m->ld;
+                A.n_tiles = m->n_tiles;
+                A.lda32 = (m->n + 1) / 2 * 2;
+                A.A32 = reinterpret_cast<float2*>(pm);
+                pm += round256(sizeof(float2) * m->n * A.lda32);
+                A.coef = reinterpret_cast<double*>(pc);
+                pc += round256(sizeof(double) * coefficient_fields() * m->ld);
+                A.diag = reinterpret_cast<double2*>(pd);
+                pd += round256(sizeof(double2) * m->n);
+                A.k = B->phys[i].harmonic_factor * B->phys[i].wave_number;
+                A.near_ptr = m->near_ptr.as<int64_t>();
+                A.near_col = m->near_col.as<int32_t>();
+                A.nnz = m->nnz;
+                B->asm_h.push_back(A);
+                B->rhs.push_back(reinterpret_cast<double2*>(pr));
+                pr += round256(sizeof(double2) * ((m->n + 1) / 2 * 2));
+            }
+            B->asm_d.alloc(sizeof(BatchAsmInst) * B->ninst);
+            SB_CUDA(cudaMemcpy(B->asm_d.p, B->asm_h.data(), sizeof(BatchAsmInst) * B->ninst,
+                               cudaMemcpyHostToDevice));
+        } catch (...) {
+            delete B;
+            throw;
+        }
+        *out = new sb_batch{B};
+    });
+}
+
+SB_API int sb_batch_destroy(sb_batch* batch) {
+    if (!batch) return SB_OK;
+    if (batch->b) {
+        cudaSetDevice(batch->b->device);
+        delete batch->b;
+    }
+    delete batch;
+    return SB_OK;
+}
+
+SB_API int sb_batch_assemble(sb_batch* batch) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null handle");
+        Batch& B = *batch->b;
+        SB_CUDA(cudaSetDevice(B.device));
+        maybe_inject(SB_INJECT_LAUNCH);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        SB_CUDA(cudaEventCreate(&e0));
+        SB_CUDA(cudaEventCreate(&e1));
+        struct EvGuard {
+            cudaEvent_t a, b;
+            ~EvGuard() {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } evg{e0, e1};
+        SB_CUDA(cudaEventRecord(e0, B.stream));
+        for (int i = 0; i < B.ninst; ++i)
+            coefficients_for(*B.meshes[i], B.phys[i], B.beta[i].x, B.beta[i].y,
+                             const_cast<double*>(B.asm_h[i].coef), B.stream);
+        assemble_batch(B.asm_h, B.asm_d.as<BatchAsmInst>(), B.pre_asm, B.stream, B.device);
+        SB_CUDA(cudaEventRecord(e1, B.stream));
+        SB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        B.last_assembly_ms = ms;
+        B.assembled = true;
+    });
+}
+
+SB_API int sb_batch_set_rhs_plane_wave(sb_batch* batch, const double* direction) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b && direction, SB_ERR_INVALID_ARGUMENT, "batch: null argument");
+        Batch& B = *batch->b;
+        const double dn = std::sqrt(direction[0] * direction[0] + direction[1] * direction[1] +
+                                    direction[2] * direction[2]);
+        SB_REQUIRE(std::isfinite(dn) && dn > 0, SB_ERR_INVALID_ARGUMENT, "batch: direction must be nonzero");
+        SB_CUDA(cudaSetDevice(B.device));
+        for (int i = 0; i < B.ninst; ++i)
+            incident_plane_wave(*B.meshes[i], B.phys[i], B.beta[i].x, B.beta[i].y, direction, nullptr, 1, B.rhs[i],
+                                B.stream, false);
+        SB_CUDA(cudaStreamSynchronize(B.stream));
+    });
+}
+
+SB_API int sb_batch_set_rhs(sb_batch* batch, int64_t index, const sb_complex* b) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b && b, SB_ERR_INVALID_ARGUMENT, "batch: null argument");
+        Batch& B = *batch->b;
+        SB_REQUIRE(index >= 0 && index < B.ninst, SB_ERR_INVALID_ARGUMENT, "batch: index out of range");
+        const int64_t n = B.meshes[index]->n;
+        for (int64_t i = 0; i < n; ++i)
+            SB_REQUIRE(std::isfinite(b[i].re) && std::isfinite(b[i].im), SB_ERR_NOT_FINITE,
+                       "batch: non-finite right-hand side");
+        SB_CUDA(cudaSetDevice(B.device));
+        SB_CUDA(cudaStreamSynchronize(B.stream));
+        SB_CUDA(cudaMemcpy(B.rhs[index], b, sizeof(double2) * n, cudaMemcpyHostToDevice));
+    });
+}
+
+SB_API int sb_batch_solve(sb_batch* batch, const sb_ir_config* cfg, sb_gmres_stats* stats) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b && cfg && stats, SB_ERR_INVALID_ARGUMENT, "batch: null argument");
+        SB_REQUIRE(cfg->max_refinements >= 0 && cfg->inner_restart > 0 && cfg->inner_restart <= kMaxKrylov &&
+                       cfg->inner_max_iterations > 0 && cfg->tolerance > 0 && cfg->inner_tolerance > 0,
+                   SB_ERR_INVALID_ARGUMENT, "batch: invalid refinement configuration");
+        Batch& B = *batch->b;
+        SB_REQUIRE(B.assembled, SB_ERR_INVALID_ARGUMENT, "batch: assemble before solving");
+        maybe_inject(SB_INJECT_LAUNCH);
+        batch_solve(B, *cfg, stats);
+    });
+}
+
+SB_API int sb_batch_solution(const sb_batch* batch, int64_t index, sb_complex* x) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b && x, SB_ERR_INVALID_ARGUMENT, "batch: null argument");
+        Batch& B = *batch->b;
+        SB_REQUIRE(index >= 0 && index < B.ninst, SB_ERR_INVALID_ARGUMENT, "batch: index out of range");
+        SB_REQUIRE(B.solved, SB_ERR_INVALID_ARGUMENT, "batch: no solution yet");
+        SB_CUDA(cudaSetDevice(B.device));
+        SB_CUDA(cudaStreamSynchronize(B.stream));
+        SB_CUDA(cudaMemcpy(x, B.h[index].x, sizeof(double2) * B.h[index].n, cudaMemcpyDeviceToHost));
+    });
+}
+
+SB_API int sb_batch_matrix_c64(const sb_batch* batch, int64_t index, sb_complex32* matrix) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b && matrix, SB_ERR_INVALID_ARGUMENT, "batch: null argument");
+        Batch& B = *batch->b;
+        SB_REQUIRE(index >= 0 && index < B.ninst, SB_ERR_INVALID_ARGUMENT, "batch: index out of range");
+        SB_REQUIRE(B.assembled, SB_ERR_INVALID_ARGUMENT, "batch: not assembled");
+        const BatchAsmInst& A = B.asm_h[index];
+        SB_CUDA(cudaSetDevice(B.device));
+        SB_CUDA(cudaStreamSynchronize(B.stream));
+        SB_CUDA(cudaMemcpy2D(matrix, sizeof(float2) * A.n, A.A32, sizeof(float2) * A.lda32, sizeof(float2) * A.n,
+                             A.n, cudaMemcpyDeviceToHost));
+    });
+}
+
+SB_API int sb_batch_timings(const sb_batch* batch, double* assembly_ms, double* solve_ms) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null handle");
+        if (assembly_ms) *assembly_ms = batch->b->last_assembly_ms;
+        if (solve_ms) *solve_ms = batch->b->last_solve_ms;
+    });
+}
+
+}  // extern "C"

@@ -13,37 +13,13 @@
 
 #include "sb_blas.cuh"
 #include "sb_device.cuh"
+#include "sb_gemv.cuh"
 #include "sb_internal.cuh"
 #include "sb_profile.cuh"
 
 namespace sb {
 
 static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
-
-__device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
-__device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
-
-// Block-wide sum of NV doubles held per thread; result valid in thread 0.
-template <int NV, int THREADS>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int t = 0; t < NV; ++t) v[t] = warp_sum(v[t]);
-    if (lane == 0) {
-#pragma unroll
-        for (int t = 0; t < NV; ++t) red[warp * NV + t] = v[t];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int t = 0; t < NV; ++t) {
-            double s = 0.0;
-            for (int w = 0; w < THREADS / 32; ++w) s += red[w * NV + t];
-            v[t] = s;
-        }
-    }
-}
-
 
 // Gates: a kernel launched inside a captured Krylov cycle returns at once when its gate is
 // closed (the instance converged or the step needs no second Gram-Schmidt pass).
@@ -155,110 +131,7 @@ __global__ void __launch_bounds__(THREADS) k_gemv_n_c64(const float2* __restrict
                                                         const void* __restrict__ bv_,
                                                         double* __restrict__ part, Gate gate) {
     if (closed(gate)) return;
-    using Acc = typename std::conditional<X64, double, float>::type;
-    __shared__ double red[(THREADS / 32) * 2 * ROWS];
-    const int64_t row0 = blockIdx.x * (int64_t)ROWS;
-    const int nr = static_cast<int>((n - row0) < ROWS ? (n - row0) : ROWS);
-    Acc acc[2 * ROWS];
-#pragma unroll
-    for (int r = 0; r < 2 * ROWS; ++r) acc[r] = 0;
-    const int64_t n2 = n >> 1;     // float4 = two complex64 entries
-    const int64_t ld2 = lda >> 1;  // lda is even, so every row starts 16-byte aligned
-    const float4* A4 = reinterpret_cast<const float4*>(A + row0 * lda);
-    int64_t c = threadIdx.x;
-    for (; c + (UNROLL - 1) * THREADS < n2; c += UNROLL * THREADS) {
-        Acc xr[UNROLL][4];
-        float4 av[UNROLL][ROWS];
-#pragma unroll
-        for (int u = 0; u < UNROLL; ++u) {
-            const int64_t cc = c + u * THREADS;
-            if (X64) {
-                const double2* x = static_cast<const double2*>(xv_);
-                const double2 p = __ldg(x + 2 * cc), q = __ldg(x + 2 * cc + 1);
-                xr[u][0] = p.x; xr[u][1] = p.y; xr[u][2] = q.x; xr[u][3] = q.y;
-            } else {
-                const float4 p = __ldg(static_cast<const float4*>(xv_) + cc);
-                xr[u][0] = p.x; xr[u][1] = p.y; xr[u][2] = p.z; xr[u][3] = p.w;
-            }
-#pragma unroll
-            for (int r = 0; r < ROWS; ++r)
-                av[u][r] = (r < nr) ? ld_stream(A4 + r * ld2 + cc) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < UNROLL; ++u)
-#pragma unroll
-            for (int r = 0; r < ROWS; ++r) {
-                const Acc a0 = av[u][r].x, a1 = av[u][r].y, a2 = av[u][r].z, a3 = av[u][r].w;
-                acc[2 * r] = fma(a0, xr[u][0], fma(-a1, xr[u][1], acc[2 * r]));
-                acc[2 * r + 1] = fma(a0, xr[u][1], fma(a1, xr[u][0], acc[2 * r + 1]));
-                acc[2 * r] = fma(a2, xr[u][2], fma(-a3, xr[u][3], acc[2 * r]));
-                acc[2 * r + 1] = fma(a2, xr[u][3], fma(a3, xr[u][2], acc[2 * r + 1]));
-            }
-    }
-    for (; c < n2; c += THREADS) {
-        Acc x0r, x0i, x1r, x1i;
-        if (X64) {
-            const double2* x = static_cast<const double2*>(xv_);
-            const double2 p = x[2 * c], q = x[2 * c + 1];
-            x0r = p.x; x0i = p.y; x1r = q.x; x1i = q.y;
-        } else {
-            const float4 p = static_cast<const float4*>(xv_)[c];
-            x0r = p.x; x0i = p.y; x1r = p.z; x1i = p.w;
-        }
-#pragma unroll
-        for (int r = 0; r < ROWS; ++r) {
-            if (r < nr) {
-                const float4 a = ld_stream(A4 + r * ld2 + c);
-                acc[2 * r] = fma((Acc)a.x, x0r, fma(-(Acc)a.y, x0i, acc[2 * r]));
-                acc[2 * r + 1] = fma((Acc)a.x, x0i, fma((Acc)a.y, x0r, acc[2 * r + 1]));
-                acc[2 * r] = fma((Acc)a.z, x1r, fma(-(Acc)a.w, x1i, acc[2 * r]));
-                acc[2 * r + 1] = fma((Acc)a.z, x1i, fma((Acc)a.w, x1r, acc[2 * r + 1]));
-            }
-        }
-    }
-    // Odd n: the last column.
-    if ((n & 1) && threadIdx.x == 0) {
-        const int64_t cl = n - 1;
-        Acc xr0, xi0;
-        if (X64) {
-            const double2 p = static_cast<const double2*>(xv_)[cl];
-            xr0 = p.x; xi0 = p.y;
-        } else {
-            const float2 p = static_cast<const float2*>(xv_)[cl];
-            xr0 = p.x; xi0 = p.y;
-        }
-        for (int r = 0; r < nr; ++r) {
-            const float2 a = A[(row0 + r) * lda + cl];
-            acc[2 * r] = fma((Acc)a.x, xr0, fma(-(Acc)a.y, xi0, acc[2 * r]));
-            acc[2 * r + 1] = fma((Acc)a.x, xi0, fma((Acc)a.y, xr0, acc[2 * r + 1]));
-        }
-    }
-    // Per-thread partial sums (FP32 for the FP32 product) are combined across the block in FP64.
-    double accd[2 * ROWS];
-#pragma unroll
-    for (int r = 0; r < 2 * ROWS; ++r) accd[r] = acc[r];
-    block_sum<2 * ROWS, THREADS>(accd, red);
-    if (threadIdx.x == 0) {
-        double nrm = 0.0;
-        for (int r = 0; r < nr; ++r) {
-            double vr = accd[2 * r], vi = accd[2 * r + 1];
-            if (bv_) {
-                if (X64) {
-                    const double2 bb = static_cast<const double2*>(bv_)[row0 + r];
-                    vr = bb.x - vr;
-                    vi = bb.y - vi;
-                } else {
-                    const float2 bb = static_cast<const float2*>(bv_)[row0 + r];
-                    vr = static_cast<double>(bb.x - static_cast<float>(vr));
-                    vi = static_cast<double>(bb.y - static_cast<float>(vi));
-                }
-                nrm += vr * vr + vi * vi;
-            }
-            if (X64) static_cast<double2*>(yv_)[row0 + r] = make_double2(vr, vi);
-            else static_cast<float2*>(yv_)[row0 + r] = make_float2((float)vr, (float)vi);
-        }
-        if (part) part[blockIdx.x] = nrm;
-    }
+    gemv_c64_block<ROWS, THREADS, UNROLL, X64>(A, n, lda, xv_, yv_, bv_, part, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -429,9 +302,6 @@ __global__ void k_jacobi(const double2* __restrict__ d, const T* __restrict__ x,
 // ---------------------------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------------------------
-constexpr int kGemvRows = 4;
-constexpr int kGemvThreads = 256;
-constexpr int kGemvUnroll = 2;
 
 void gemv_c128(const double2* A, int64_t n, const double2* x, double2* y, Trans t,
                cudaStream_t s, DevBuf& scratch, Gate gate) {

@@ -127,6 +127,25 @@ struct Operator {
     double last_assembly_ms = 0.0;
 };
 
+// Batched assembly (assembly.cu): one persistent launch over all instances of a batch.
+struct BatchAsmInst {
+    const double* elem;
+    const float* qp32;
+    const double* coef;
+    double2* diag;
+    float2* A32;
+    int64_t n, ld, n_tiles, lda32;
+    double k;
+    const int64_t* near_ptr;
+    const int32_t* near_col;
+    int64_t nnz;
+};
+void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst* d_inst, DevBuf& pre_buf,
+                    cudaStream_t s, int device);
+void coefficients_for(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im, double* coef,
+                      cudaStream_t s);
+int coefficient_fields();
+
 // Assembly (assembly.cu)
 void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im);
 void incident_plane_wave(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im,

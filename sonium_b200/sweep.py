@@ -1,0 +1,195 @@
+"""Batched frequency sweep over the sonium-b200 C ABI.
+
+Mirrors the reference's sweep lifecycle (crates/sonium-bem/src/core/solver/frequency_sweep.rs:
+``FrequencySweepConfig`` at :43-170, ``FrequencySweepResult`` at :175-230, the per-frequency loop of
+``frequency_sweep_with_physics_and_admittances`` at :592-700), but instead of assembling and solving
+one frequency after another, every instance (mesh, physics, Burton-Miller beta) is assembled in one
+persistent launch and all are solved together by the batched mixed-precision GMRES
+(``sb_batch_*`` in ``include/sonium_b200.h``). Instances may use different meshes, so a sweep can
+refine the mesh with frequency.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import SoniumError, check
+from .tbem import GmresSolution, IrConfig, Mesh, PhysicsParams, _c128, _p
+
+
+class SweepBatch:
+    """Device-resident batch of TBEM instances (complex64 matrices, FP64-refined solves)."""
+
+    def __init__(self, meshes, physics, betas):
+        meshes = list(meshes)
+        physics = list(physics)
+        betas = [complex(b) for b in betas]
+        if not (len(meshes) == len(physics) == len(betas)) or not meshes:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "batch: meshes, physics and betas must have one "
+                                                         "entry per instance")
+        self.meshes = meshes  # the batch refers to the meshes' device data: keep them alive
+        self.physics = physics
+        self.betas = betas
+        n = len(meshes)
+        handles = (ct.c_void_p * n)(*[m.handle.value for m in meshes])
+        phys = (L.SbPhysics * n)(*[p._struct() for p in physics])
+        bet = (L.SbComplex * n)(*[L.SbComplex(b.real, b.imag) for b in betas])
+        h = ct.c_void_p()
+        check(L.load().sb_batch_create(n, ct.cast(handles, ct.c_void_p), ct.cast(phys, ct.c_void_p),
+                                       ct.cast(bet, ct.c_void_p), ct.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "batch has been closed")
+        return self._h
+
+    def __len__(self) -> int:
+        return len(self.meshes)
+
+    def sizes(self):
+        return [m.num_elements for m in self.meshes]
+
+    def assemble(self) -> float:
+        """Assemble every instance; returns the device time in ms."""
+        check(L.load().sb_batch_assemble(self.handle))
+        return self.timings()[0]
+
+    def set_rhs_plane_wave(self, direction=(0.0, 0.0, 1.0)) -> None:
+        d = np.ascontiguousarray(direction, np.float64)
+        check(L.load().sb_batch_set_rhs_plane_wave(self.handle, _p(d)))
+
+    def set_rhs(self, index: int, b) -> None:
+        b = _c128(b)
+        if b.shape != (self.meshes[index].num_elements,):
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "batch: right-hand side length must be n")
+        check(L.load().sb_batch_set_rhs(self.handle, index, _p(b)))
+
+    def solve(self, config: IrConfig = IrConfig()) -> list:
+        """Batched FP32-inner / FP64-refined GMRES; one GmresSolution (without x) per instance."""
+        n = len(self)
+        stats = (L.SbGmresStats * n)()
+        check(L.load().sb_batch_solve(self.handle, ct.byref(config._struct()), ct.cast(stats, ct.c_void_p)))
+        return [GmresSolution._from(None, stats[i]) for i in range(n)]
+
+    def solution(self, index: int) -> np.ndarray:
+        x = np.zeros(self.meshes[index].num_elements, np.complex128)
+        check(L.load().sb_batch_solution(self.handle, index, _p(x)))
+        return x
+
+    def matrix_c64(self, index: int) -> np.ndarray:
+        m = self.meshes[index].num_elements
+        a = np.zeros((m, m), np.complex64)
+        check(L.load().sb_batch_matrix_c64(self.handle, index, _p(a)))
+        return a
+
+    def timings(self):
+        """(assembly_ms, solve_ms) of the last assemble / solve."""
+        a, s = ct.c_double(), ct.c_double()
+        check(L.load().sb_batch_timings(self.handle, ct.byref(a), ct.byref(s)))
+        return a.value, s.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.load().sb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class FrequencySweepResult:
+    """FrequencySweepResult (frequency_sweep.rs:175-230) of a batched sweep."""
+
+    solutions: list
+    frequencies: list
+    iteration_counts: list
+    converged: list
+    exact_relative_residuals: list
+    assembly_ms: float
+    solve_ms: float
+    stats: list = field(default_factory=list)
+
+    def total_iterations(self) -> int:
+        return int(sum(self.iteration_counts))
+
+    def average_iterations(self) -> float:
+        return self.total_iterations() / len(self.iteration_counts) if self.iteration_counts else 0.0
+
+    def num_converged(self) -> int:
+        return int(sum(bool(c) for c in self.converged))
+
+
+def frequency_sweep_batched(meshes, physics, betas, direction=(0.0, 0.0, 1.0),
+                            config: IrConfig = IrConfig()) -> FrequencySweepResult:
+    """Assemble and solve every instance of a plane-wave scattering sweep in one batch."""
+    batch = SweepBatch(meshes, physics, betas)
+    try:
+        batch.assemble()
+        batch.set_rhs_plane_wave(direction)
+        stats = batch.solve(config)
+        sols = [batch.solution(i) for i in range(len(batch))]
+        a_ms, s_ms = batch.timings()
+    finally:
+        batch.close()
+    return FrequencySweepResult(
+        solutions=sols, frequencies=[p.frequency for p in physics],
+        iteration_counts=[s.iterations for s in stats], converged=[s.converged for s in stats],
+        exact_relative_residuals=[s.residual for s in stats], assembly_ms=a_ms, solve_ms=s_ms, stats=stats)
+
+
+# Sweep workload: ka log-spaced on a triaxial ellipsoid, mesh refined with frequency.
+ELLIPSOID_AXES = (1.0, 0.6, 0.4)
+
+
+def max_edge_length(nodes: np.ndarray, tris: np.ndarray) -> float:
+    e = [np.linalg.norm(nodes[tris[:, i]] - nodes[tris[:, (i + 1) % 3]], axis=1).max() for i in range(3)]
+    return float(max(e))
+
+
+def level_for_wavenumber(k: float, edge_by_level: dict, elements_per_wavelength: float = 8.0) -> int:
+    """Smallest icosphere level whose longest edge gives `elements_per_wavelength` per wavelength
+    (the finest level offered when none does)."""
+    lam = 2.0 * np.pi / k
+    for level in sorted(edge_by_level):
+        if lam / edge_by_level[level] >= elements_per_wavelength:
+            return level
+    return max(edge_by_level)
+
+
+def ellipsoid_sweep_plan(count: int = 64, ka_min: float = 1.0, ka_max: float = 32.0,
+                         axes=ELLIPSOID_AXES, levels=(2, 3, 4, 5), elements_per_wavelength: float = 8.0):
+    """[(ka, k, level)] for `count` instances with ka = k * axes[0] log-spaced in [ka_min, ka_max]."""
+    from .tbem import icosphere
+    edges = {}
+    for lv in levels:
+        nodes, tris = icosphere(1.0, lv, axes)
+        edges[lv] = max_edge_length(nodes, tris)
+    plan = []
+    for ka in np.geomspace(ka_min, ka_max, count):
+        k = float(ka) / axes[0]
+        plan.append((float(ka), k, level_for_wavenumber(k, edges, elements_per_wavelength)))
+    return plan
+
+
+def build_ellipsoid_sweep(plan, axes=ELLIPSOID_AXES, device: int = 0, speed_of_sound: float = 343.0,
+                          density: float = 1.21):
+    """Meshes (one per level, shared by the instances of that level), physics and betas of a plan."""
+    meshes_by_level = {}
+    meshes, physics, betas = [], [], []
+    for _, k, level in plan:
+        if level not in meshes_by_level:
+            meshes_by_level[level] = Mesh.icosphere(1.0, level, axes, device=device)
+        ph = PhysicsParams.for_wavenumber(k, speed_of_sound, density)
+        meshes.append(meshes_by_level[level])
+        physics.append(ph)
+        betas.append(ph.burton_miller_beta())
+    return meshes, physics, betas

@@ -1,0 +1,181 @@
+"""Batched frequency sweep (sb_batch_*): one persistent assembly launch for many instances and
+the batched mixed-precision GMRES with per-instance convergence masks.
+
+Bars (written into each test):
+  * each instance's complex64 matrix matches the single-instance SB_PRECISION_FP32 assembly of the
+    same mesh and wavenumber to 4 units in the last place per entry, most entries bit-identical
+    (the same device functions compiled into another kernel may contract or order FP32
+    operations differently), and the FP64 oracle within the mixed-assembly bar (3e-5 per entry,
+    median 1e-6),
+  * each batched solution is within 1e-6 (relative) of the single-instance sb_gmres_mixed
+    solution and within 1e-5 of the FP64 solve (the metric's tolerance); every instance
+    converges to its own tolerance with its own iteration count,
+  * per-instance masks: a converged or already-solved instance stops costing iterations.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu(sb):
+    if sb.device_count() < 1:
+        pytest.fail("no CUDA device visible: the GPU tests need a B200")
+    return sb
+
+
+def ulp_distance(a, b):
+    """Largest distance in complex64 units in the last place between matching real / imaginary
+    parts (0 where both are equal)."""
+    x = np.stack([a.real, a.imag]).astype(np.float32).view(np.int32).astype(np.int64)
+    y = np.stack([b.real, b.imag]).astype(np.float32).view(np.int32).astype(np.int64)
+    # map the sign-magnitude bit patterns onto a monotone integer line
+    x = np.where(x < 0, -(x & 0x7FFFFFFF), x)
+    y = np.where(y < 0, -(y & 0x7FFFFFFF), y)
+    return int(np.abs(x - y).max())
+
+
+def _instances(gpu, oracle, spec):
+    """spec: [(level, k, scale)] -> meshes (one per (level, scale)), physics, betas."""
+    cache, meshes, phys, betas = {}, [], [], []
+    for level, k, scale in spec:
+        key = (level, scale)
+        if key not in cache:
+            nodes, tris = oracle.icosphere(1.0, level, scale)
+            cache[key] = gpu.Mesh(nodes, tris)
+        ph = gpu.PhysicsParams.for_wavenumber(k)
+        meshes.append(cache[key])
+        phys.append(ph)
+        betas.append(ph.burton_miller_beta())
+    return meshes, phys, betas
+
+
+SPEC = [(1, 0.7, (1.0, 1.0, 1.0)), (2, 2.0, (1.0, 0.6, 0.4)), (2, 3.5, (1.0, 0.6, 0.4)),
+        (3, 2.0, (1.0, 1.0, 1.0)), (3, 6.0, (1.0, 0.6, 0.4)), (1, 1.3, (1.0, 0.6, 0.4))]
+
+
+def test_batch_matrices_match_single_instance_assembly(gpu, oracle):
+    from sonium_b200.sweep import SweepBatch
+
+    meshes, phys, betas = _instances(gpu, oracle, SPEC)
+    oracle_nodes = [oracle.icosphere(1.0, lv, sc)[0] for lv, _, sc in SPEC]
+    oracle_tris = [oracle.icosphere(1.0, lv, sc)[1] for lv, _, sc in SPEC]
+    batch = SweepBatch(meshes, phys, betas)
+    batch.assemble()
+    for i, (m, ph, be) in enumerate(zip(meshes, phys, betas)):
+        op = gpu.build_tbem_system_with_beta(m, ph, be, precision=gpu.SB_PRECISION_FP32)
+        A1 = op.matrix_c64()
+        Ab = batch.matrix_c64(i)
+        assert ulp_distance(Ab, A1) <= 4, (i, ulp_distance(Ab, A1))
+        assert np.mean(Ab == A1) > 0.9, i
+        # and the FP32 bar of the single-instance mixed assembly against the FP64 oracle
+        A_o, _ = oracle.assemble(oracle_nodes[i], oracle_tris[i], oracle.physics_for_k(SPEC[i][1]), be)
+        floor = 1e-6 * np.abs(A_o).max()
+        err = np.abs(Ab - A_o) / np.maximum(np.abs(A_o), floor)
+        assert err.max() < 3e-5 and np.median(err) < 1e-6, (i, err.max(), np.median(err))
+        op.close()
+    batch.close()
+
+
+def test_batch_odd_size_mesh(gpu, oracle):
+    """n odd (open surface): padded leading dimensions, the odd last column of the products."""
+    from sonium_b200.sweep import SweepBatch
+
+    nodes, tris = oracle.icosphere(1.0, 2, (1.0, 0.6, 0.4))
+    mesh_odd = gpu.Mesh(nodes, tris[:-1])
+    nodes3, tris3 = oracle.icosphere(1.0, 1)
+    mesh_even = gpu.Mesh(nodes3, tris3)
+    ph1, ph2 = gpu.PhysicsParams.for_wavenumber(1.5), gpu.PhysicsParams.for_wavenumber(0.9)
+    batch = SweepBatch([mesh_even, mesh_odd], [ph1, ph2], [ph1.burton_miller_beta(), ph2.burton_miller_beta()])
+    batch.assemble()
+    op = gpu.build_tbem_system_with_beta(mesh_odd, ph2, ph2.burton_miller_beta(), precision=gpu.SB_PRECISION_FP32)
+    assert ulp_distance(batch.matrix_c64(1), op.matrix_c64()) <= 4
+    b = gpu.rhs_plane_wave(mesh_odd, ph2, ph2.burton_miller_beta(), [0, 0, 1])[:, 0]
+    batch.set_rhs_plane_wave([0, 0, 1])
+    st = batch.solve(gpu.IrConfig(tolerance=1e-9))
+    assert all(s.converged for s in st)
+    ref = gpu.gmres_mixed(op, b, gpu.IrConfig(tolerance=1e-9))
+    x = batch.solution(1)
+    assert np.linalg.norm(x - ref.x) / np.linalg.norm(ref.x) < 1e-6
+
+
+def test_batch_solutions_match_single_instance_and_fp64(gpu, oracle):
+    from sonium_b200.sweep import SweepBatch
+
+    meshes, phys, betas = _instances(gpu, oracle, SPEC)
+    cfg = gpu.IrConfig(tolerance=1e-8)
+    batch = SweepBatch(meshes, phys, betas)
+    batch.assemble()
+    batch.set_rhs_plane_wave([0.0, 0.0, 1.0])
+    stats = batch.solve(cfg)
+    for i, (m, ph, be) in enumerate(zip(meshes, phys, betas)):
+        b = gpu.rhs_plane_wave(m, ph, be, [0, 0, 1])[:, 0]
+        op32 = gpu.build_tbem_system_with_beta(m, ph, be, precision=gpu.SB_PRECISION_FP32)
+        single = gpu.gmres_mixed(op32, b, cfg)
+        op64 = gpu.build_tbem_system_with_beta(m, ph, be)
+        x64 = gpu.gmres(op64, b, gpu.GmresConfig(max_iterations=100, restart=50, tolerance=1e-10)).x
+        x = batch.solution(i)
+        st = stats[i]
+        assert st.converged and st.residual < cfg.tolerance, (i, st)
+        assert np.linalg.norm(x - single.x) / np.linalg.norm(single.x) < 1e-6, i
+        assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-5, i
+        # same algorithm per instance: the Krylov work matches the single-instance solve closely
+        assert abs(st.iterations - single.iterations) <= max(2, single.iterations // 10), (i, st, single)
+        assert abs(st.refinements - single.refinements) <= 1, (i, st.refinements, single.refinements)
+        # the residual reported is the exact FP64 one
+        r = b - op64.apply(x)
+        assert abs(np.linalg.norm(r) / np.linalg.norm(b) - st.residual) < 1e-3 * st.residual + 1e-14
+        op32.close()
+        op64.close()
+    batch.close()
+
+
+def test_batch_instances_converge_independently(gpu, oracle):
+    """Masks: an instance with a zero right-hand side is done at once (no Krylov steps), the
+    others proceed; solving twice gives identical results (state fully reset per solve)."""
+    from sonium_b200.sweep import SweepBatch
+
+    meshes, phys, betas = _instances(gpu, oracle, SPEC[:3])
+    batch = SweepBatch(meshes, phys, betas)
+    batch.assemble()
+    batch.set_rhs_plane_wave([1.0, 0.0, 0.0])
+    batch.set_rhs(1, np.zeros(meshes[1].num_elements, np.complex128))
+    cfg = gpu.IrConfig(tolerance=1e-9)
+    st = batch.solve(cfg)
+    assert st[1].iterations == 0 and st[1].converged and np.all(batch.solution(1) == 0)
+    assert st[0].iterations > 0 and st[2].iterations > 0
+    x0, x2 = batch.solution(0), batch.solution(2)
+    st2 = batch.solve(cfg)
+    assert np.array_equal(batch.solution(0), x0) and np.array_equal(batch.solution(2), x2)
+    assert [s.iterations for s in st2] == [s.iterations for s in st]
+    # a different restart re-sizes the workspace and still converges
+    st3 = batch.solve(gpu.IrConfig(tolerance=1e-9, inner_restart=20))
+    assert all(s.converged for s in st3)
+    assert np.linalg.norm(batch.solution(2) - x2) / np.linalg.norm(x2) < 1e-7
+    batch.close()
+
+
+def test_batch_rejects_bc_values_and_bad_config(gpu, oracle):
+    from sonium_b200.sweep import SweepBatch
+
+    nodes, tris = oracle.icosphere(1.0, 1)
+    mesh = gpu.Mesh(nodes, tris)
+    ph = gpu.PhysicsParams.for_wavenumber(1.0)
+    mesh_bc = gpu.Mesh(nodes, tris)
+    mesh_bc.set_boundary_conditions(kind=gpu.SB_BC_VELOCITY, value=1.0)
+    with pytest.raises(gpu.SoniumError) as e:
+        SweepBatch([mesh, mesh_bc], [ph, ph], [ph.burton_miller_beta()] * 2)
+    assert "boundary values" in str(e.value)
+    batch = SweepBatch([mesh], [ph], [ph.burton_miller_beta()])
+    with pytest.raises(gpu.SoniumError):
+        batch.solve(gpu.IrConfig())  # not assembled
+    with pytest.raises(gpu.SoniumError):
+        batch.solution(0)
+    batch.assemble()
+    with pytest.raises(gpu.SoniumError):
+        batch.solve(gpu.IrConfig(inner_restart=500))
+    with pytest.raises(gpu.SoniumError):
+        batch.set_rhs(0, np.full(mesh.num_elements, np.nan, np.complex128))
+    batch.close()
+

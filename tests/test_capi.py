@@ -105,3 +105,15 @@ def test_null_and_bad_arguments(sb):
     assert lib.sb_mesh_destroy(None) == L.SB_OK
     assert lib.sb_operator_destroy(None) == L.SB_OK
     assert lib.sb_icosphere_counts(12, None, None) == L.SB_ERR_INVALID_ARGUMENT
+
+
+def test_ellipsoid_sweep_plan_levels(sb):
+    """The sweep plan: 64 instances, ka 1 -> 32, level refined with frequency, N 320 -> 20480."""
+    from sonium_b200.sweep import ellipsoid_sweep_plan
+
+    plan = ellipsoid_sweep_plan()
+    assert len(plan) == 64
+    ka = np.array([p[0] for p in plan])
+    assert ka[0] == pytest.approx(1.0) and ka[-1] == pytest.approx(32.0)
+    levels = [p[2] for p in plan]
+    assert levels == sorted(levels) and levels[0] == 2 and levels[-1] == 5
