@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true", help="skip the batched frequency-sweep leg")
     ap.add_argument("--sweep-count", type=int, default=64, help="instances of the frequency sweep")
     ap.add_argument("--sweep-only", action="store_true", help="run only the sweep leg and print its JSON")
+    ap.add_argument("--precision-form", action="store_true",
+                    help="run only the N = 81920, k = 40 precision-form leg (~165 GB) and print its JSON")
     ap.add_argument("--single", action="store_true",
                     help="one untimed solve per precision mode at --level (profiling driver), no JSON line")
     return ap.parse_args()
@@ -243,10 +245,10 @@ def main():
         single_solves(sb, a.level, a.k, dev)
         return
     assert sb.device_count() > dev, "no CUDA device for this rank"
-    if a.sweep_only:
-        out = sweep_leg(sb, a, dist, dev, _cudart())
+    if a.sweep_only or a.precision_form:
+        out = (sweep_leg if a.sweep_only else precision_leg)(sb, a, dist, dev, _cudart())
         if dist.rank == 0:
-            print(json.dumps({"sweep": out}), flush=True)
+            print(json.dumps({"sweep" if a.sweep_only else "precision_form": out}), flush=True)
         dist.close()
         return
 
@@ -503,6 +505,48 @@ def sweep_leg(sb, a, dist, dev, rt):
         "assembly_ms": asm_ms, "solve_ms": solve_ms,
         "iterations_batched": [int(s.iterations) for s in st0], "iterations_fp64": fp64_iters,
         "timing": "wall clock around device-synchronised steps, max over ranks",
+    }
+
+
+def precision_leg(sb, a, dist, dev, rt):
+    """Precision form: rigid sphere, icosphere level 6 (N = 81920), k = 40, plane wave +z.
+
+    The complex128 matrix (107 GB) and its complex64 copy (54 GB) come from one assembly; a step
+    solves to rtol 1e-10 once in plain FP64 GMRES(50) and once with FP32-inner GMRES(50) to 1e-5 and
+    FP64 refinement on the complex128 matrix. Device times from the solver statistics (CUDA events
+    on the operator's stream); error of the mixed solution against the FP64 one."""
+    level, k = 6, 40.0
+    nodes, tris = sb.icosphere(RADIUS, level)
+    n = tris.shape[0]
+    mesh = sb.Mesh(nodes, tris, device=dev)
+    ph = sb.PhysicsParams.for_wavenumber(k)
+    beta = ph.burton_miller_beta()
+    op = sb.build_tbem_system_with_beta(mesh, ph, beta, sb.SB_PRECISION_FP64_FP32)
+    asm_ms = op.info().assembly_ms
+    b = sb.rhs_plane_wave(mesh, ph, beta, [0.0, 0.0, 1.0])[:, 0]
+    gc = sb.GmresConfig(max_iterations=400, restart=RESTART, tolerance=1e-10)
+    ir = sb.IrConfig(max_refinements=20, tolerance=1e-10, inner_restart=RESTART, inner_max_iterations=40,
+                     inner_tolerance=1e-5)
+    t64, tmix = [], []
+    s64 = mix = None
+    for i in range(max(1, a.steps)):
+        s64 = sb.gmres(op, b, gc)
+        mix = sb.gmres_mixed(op, b, ir)
+        t64.append(s64.device_ms)
+        tmix.append(mix.device_ms)
+    op.close()
+    mesh.close()
+    err = float(np.linalg.norm(mix.x - s64.x) / np.linalg.norm(s64.x))
+    return {
+        "workload": f"rigid sphere icosphere L{level} (N={n}), k={k}, complex128 + complex64 matrices "
+                    f"({16 * n * n / 1e9:.0f} + {8 * n * n / 1e9:.0f} GB), rtol 1e-10",
+        "assembly_ms": asm_ms,
+        "fp64_solve_ms": float(np.median(t64)), "mixed_solve_ms": float(np.median(tmix)),
+        "solve_speedup": float(np.median(t64) / np.median(tmix)),
+        "fp64": {"iterations": s64.iterations, "matvecs": s64.matvecs, "residual": s64.residual},
+        "mixed": {"iterations": mix.iterations, "matvecs": mix.matvecs, "matvecs_fp32": mix.matvecs_fp32,
+                  "refinements": mix.refinements, "residual": mix.residual},
+        "mixed_error_vs_fp64": err,
     }
 
 
