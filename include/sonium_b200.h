@@ -247,6 +247,19 @@ SB_API int sb_gmres_mixed_device(const sb_operator* op, const sb_complex* b_dev,
 SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs,
                                     const sb_complex* amps, int64_t r, sb_complex* rhs_dev);
 
+/* ---- tensor-core block product ----
+ * The block product of LinearOperator::apply_block (crates/sonium-solvers/crates/
+ * sonium-solvers-core/src/traits.rs:2949-3120 -> DenseMatrix::matmul_into, dense.rs:450-490) as
+ * used by block GMRES (crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:
+ * 163), on the tensor cores: every real operand is split into two BF16 terms (hi + lo, 16
+ * significant bits) and the three leading cross products are accumulated in FP32, so each entry
+ * of Y = A X carries a relative error of order 1e-5 of the row's magnitude (not an FP64
+ * product: sb_operator_apply_block is the exact one). prepare builds the split planes of the
+ * operator's matrix (4 N^2 * 2 bytes); re-assembly drops them. apply: x and y hold r complex64
+ * vectors of length n, vector c at x + c * n (host memory). */
+SB_API int sb_operator_prepare_block_tensor(sb_operator* op);
+SB_API int sb_operator_apply_block_tensor(const sb_operator* op, const sb_complex32* x, sb_complex32* y, int64_t r);
+
 /* ---- batched frequency sweep ----
  * Replaces the reference's per-frequency loop (crates/sonium-bem/src/core/solver/
  * frequency_sweep.rs:541-600: build_tbem_system_stabilized at :20, then one GMRES solve per
@@ -284,6 +297,7 @@ SB_API int sb_batch_timings(const sb_batch* batch, double* assembly_ms, double* 
 #define SB_PROF_GEMV32 4     /* complex64 matvec (FP32 or FP64 vectors) */
 #define SB_PROF_ARNOLDI 5    /* Gram-Schmidt dots / projections / basis updates */
 #define SB_PROF_OTHER 6      /* geometry, coefficients, RHS reductions, plane waves */
+#define SB_PROF_TENSOR 7     /* tensor-core block product (BF16 split, tcgen05) */
 #define SB_PROF_KINDS 8
 typedef struct sb_profile {
     double ms[SB_PROF_KINDS];

@@ -84,9 +84,10 @@ class SbGmresStats(ct.Structure):
                 ("converged", ct.c_int32), ("status", ct.c_int32)]
 
 
-SB_PROF_FAR, SB_PROF_NEAR, SB_PROF_SELF, SB_PROF_GEMV64, SB_PROF_GEMV32, SB_PROF_ARNOLDI, SB_PROF_OTHER = range(7)
+(SB_PROF_FAR, SB_PROF_NEAR, SB_PROF_SELF, SB_PROF_GEMV64, SB_PROF_GEMV32, SB_PROF_ARNOLDI, SB_PROF_OTHER,
+ SB_PROF_TENSOR) = range(8)
 SB_PROF_KINDS = 8
-PROF_NAMES = ["far", "near", "self", "gemv64", "gemv32", "arnoldi", "other", "reserved"]
+PROF_NAMES = ["far", "near", "self", "gemv64", "gemv32", "arnoldi", "other", "tensor"]
 
 
 class SbProfile(ct.Structure):
@@ -133,6 +134,8 @@ _SIGNATURES = {
     "sb_gmres_mixed": ([P, P, P, ct.POINTER(SbIrConfig), P, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_mixed_device": ([P, P, P, ct.c_int, ct.POINTER(SbIrConfig), ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_rhs_plane_wave_device": ([P, P, P, ct.c_int64, P], ct.c_int),
+    "sb_operator_prepare_block_tensor": ([P], ct.c_int),
+    "sb_operator_apply_block_tensor": ([P, P, P, ct.c_int64], ct.c_int),
     "sb_batch_create": ([ct.c_int64, P, P, P, ct.POINTER(P)], ct.c_int),
     "sb_batch_destroy": ([P], ct.c_int),
     "sb_batch_assemble": ([P], ct.c_int),

@@ -338,6 +338,7 @@ SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_compl
         SB_REQUIRE(op && op->op && physics, SB_ERR_INVALID_ARGUMENT, "null argument");
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
+        tensor_release(*op->op);
         assemble(*op->op, *physics, beta.re, beta.im);
     });
 }
@@ -348,6 +349,7 @@ SB_API int sb_operator_destroy(sb_operator* op) {
         if (op->op) {
             cudaSetDevice(op->op->device);
             destroy_solve_work(*op->op);
+            tensor_release(*op->op);
             if (op->op->stream) cudaStreamDestroy(op->op->stream);
             delete op->op;
         }
@@ -489,6 +491,37 @@ SB_API int sb_operator_apply_block(const sb_operator* op, const sb_complex* X, s
             for (int64_t i = 0; i < n; ++i) Y[i * r + q] = col[i];
         }
         SB_REQUIRE(all_finite(Y, n * r), SB_ERR_NOT_FINITE, "apply_block: non-finite output block");
+    });
+}
+
+SB_API int sb_operator_prepare_block_tensor(sb_operator* op) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op, SB_ERR_INVALID_ARGUMENT, "null operator");
+        maybe_inject(SB_INJECT_LAUNCH);
+        tensor_prepare(*op->op);
+    });
+}
+
+SB_API int sb_operator_apply_block_tensor(const sb_operator* op, const sb_complex32* x, sb_complex32* y, int64_t r) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && x && y && r >= 1, SB_ERR_INVALID_ARGUMENT, "bad argument");
+        SB_REQUIRE(r <= (int64_t)1 << 20, SB_ERR_INVALID_ARGUMENT, "apply_block_tensor: too many vectors");
+        Operator& o = *op->op;
+        const int64_t n = o.n;
+        for (int64_t t = 0; t < n * r; ++t)
+            SB_REQUIRE(std::isfinite(x[t].re) && std::isfinite(x[t].im), SB_ERR_NOT_FINITE,
+                       "apply_block_tensor: non-finite input block");
+        SB_CUDA(cudaSetDevice(o.device));
+        maybe_inject(SB_INJECT_LAUNCH);
+        DevBuf dx, dy;
+        dx.alloc(sizeof(float2) * n * r);
+        dy.alloc(sizeof(float2) * n * r);
+        SB_CUDA(cudaMemcpyAsync(dx.p, x, sizeof(float2) * n * r, cudaMemcpyHostToDevice, o.stream));
+        tensor_block_product(o, dx.as<float2>(), n, static_cast<int>(r), dy.as<float2>(), n, o.stream);
+        SB_CUDA(cudaMemcpyAsync(y, dy.p, sizeof(float2) * n * r, cudaMemcpyDeviceToHost, o.stream));
+        SB_CUDA(cudaStreamSynchronize(o.stream));
+        SB_REQUIRE(tensor_status(o, true) == 0, SB_ERR_DEVICE_CHECK,
+                   "apply_block_tensor: a pipeline wait of the tensor-core kernel timed out");
     });
 }
 

@@ -123,6 +123,7 @@ struct Operator {
     DevBuf A64, A32, rhs, diag;  // rhs: BC-induced RHS (N complex); diag: A_ii for Jacobi
     DevBuf coef, far_part, near_rhs, self_rhs, scratch, status;
     void* work = nullptr;        // solver workspace (gmres.cu), released by destroy_solve_work
+    void* tensor = nullptr;      // BF16 split planes for the tensor-core block product (tensor.cu)
     cudaStream_t stream = nullptr;
     double last_assembly_ms = 0.0;
 };
@@ -177,5 +178,14 @@ void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g);
 void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part);
 
 int device_sm_count(int device);
+
+// Tensor-core block product (tensor.cu): BF16 hi/lo split planes of the operator's matrix, then
+// Y = A X for r complex64 vectors (vector c at x + c * ldx, result at y + c * ldy).
+void tensor_prepare(Operator& op);
+void tensor_release(Operator& op);
+bool tensor_ready(const Operator& op);
+void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int r, float2* y, int64_t ldy,
+                          cudaStream_t s);
+int tensor_status(const Operator& op, bool reset);
 
 }  // namespace sb

@@ -5,6 +5,8 @@ inputs before touching a device (validate_cuda_tbem_inputs, crates/sonium-bem/sr
 tbem.rs:4659-4798) and fail loudly -- never fall back to the CPU -- when no device exists.
 """
 import ctypes as ct
+import os
+import sys
 
 import numpy as np
 import pytest
@@ -117,3 +119,31 @@ def test_ellipsoid_sweep_plan_levels(sb):
     assert ka[0] == pytest.approx(1.0) and ka[-1] == pytest.approx(32.0)
     levels = [p[2] for p in plan]
     assert levels == sorted(levels) and levels[0] == 2 and levels[-1] == 5
+
+
+def test_umma_descriptors_match_cutlass(tmp_path):
+    """The tcgen05 instruction / shared-memory descriptor encoders agree bit for bit with CUTLASS's
+    cute::UMMA descriptor types (compiled host-side; skipped when nvcc or the headers are absent)."""
+    import glob
+    import shutil
+    import subprocess
+
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    cands = [p for p in glob.glob(os.path.join(sys.prefix, "lib", "python3*", "site-packages", "*", "data",
+                                               "cutlass", "include"))
+             + glob.glob(os.path.join(sys.prefix, "lib", "python3*", "site-packages", "*", "3rdparty",
+                                      "cutlass", "include"))
+             if os.path.exists(os.path.join(p, "cute", "arch", "mma_sm100_desc.hpp"))]
+    if not cands:
+        pytest.skip("no CUTLASS headers with sm100 descriptors in this environment")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "umma_desc_check")
+    cmd = [nvcc, "-std=c++17", "-Wno-deprecated-gpu-targets", "-I" + cands[0],
+           "-I" + os.path.join(root, "sonium_b200", "csrc"), os.path.join(root, "tests", "native", "umma_desc_check.cu"),
+           "-o", exe]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr[-2000:]
+    out = subprocess.run([exe], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip().endswith("OK"), out.stdout
