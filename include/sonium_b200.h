@@ -260,6 +260,23 @@ SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs,
 SB_API int sb_operator_prepare_block_tensor(sb_operator* op);
 SB_API int sb_operator_apply_block_tensor(const sb_operator* op, const sb_complex32* x, sb_complex32* y, int64_t r);
 
+/* Many right-hand sides of one operator (the role of block_gmres_preconditioned,
+ * crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:163, called via
+ * solve_compressed_many, bem_solver.rs:4072-4110): r systems A x_c = b_c solved in lockstep by
+ * FP32-inner GMRES with FP64 refinement, every right-hand side with its own Krylov basis and
+ * convergence state (the reference's block method shares one basis across right-hand sides; this
+ * one shares the products instead). Each step's products for all right-hand sides are one
+ * tensor-core block product (the BF16 split of sb_operator_apply_block_tensor); the refinement
+ * residual of all of them is one complex128 GEMM on the FP64 matrix, so the operator must hold it
+ * (SB_PRECISION_FP64 or SB_PRECISION_FP64_FP32). The split planes are built on first use. b and
+ * x: n x r row-major (b[i * r + c], the reference's DenseMatrix block layout); stats: r entries,
+ * the sb_gmres_mixed statistics per right-hand side (device_ms = the whole block's time). */
+SB_API int sb_gmres_multi(const sb_operator* op, const sb_complex* b, int64_t r, const sb_ir_config* cfg,
+                          sb_complex* x, sb_gmres_stats* stats);
+/* Device-resident variant: b_dev and x_dev hold right-hand side c at + c * n (complex128). */
+SB_API int sb_gmres_multi_device(const sb_operator* op, const sb_complex* b_dev, int64_t r,
+                                 const sb_ir_config* cfg, sb_complex* x_dev, sb_gmres_stats* stats);
+
 /* ---- batched frequency sweep ----
  * Replaces the reference's per-frequency loop (crates/sonium-bem/src/core/solver/
  * frequency_sweep.rs:541-600: build_tbem_system_stabilized at :20, then one GMRES solve per

@@ -136,6 +136,8 @@ _SIGNATURES = {
     "sb_rhs_plane_wave_device": ([P, P, P, ct.c_int64, P], ct.c_int),
     "sb_operator_prepare_block_tensor": ([P], ct.c_int),
     "sb_operator_apply_block_tensor": ([P, P, P, ct.c_int64], ct.c_int),
+    "sb_gmres_multi": ([P, P, ct.c_int64, ct.POINTER(SbIrConfig), P, P], ct.c_int),
+    "sb_gmres_multi_device": ([P, P, ct.c_int64, ct.POINTER(SbIrConfig), P, P], ct.c_int),
     "sb_batch_create": ([ct.c_int64, P, P, P, ct.POINTER(P)], ct.c_int),
     "sb_batch_destroy": ([P], ct.c_int),
     "sb_batch_assemble": ([P], ct.c_int),

@@ -12,6 +12,15 @@
 // arithmetic per instance is the single-instance mixed solver's (gmres.cu, gmres_mixed_ir): FP32
 // inner GMRES on the complex64 matrix, FP64 Hessenberg / Givens, FP64 refinement residual with
 // FP64 accumulation, the same stopping rules and statistics.
+//
+// The same machinery solves many right-hand sides of ONE operator (sb_gmres_multi): the
+// instances are the right-hand sides, every vector family is stored right-hand-side-major so a
+// step's products for all of them are one block product on the tensor cores (tensor.cu: BF16
+// hi/lo split, FP32 accumulation), and the FP64 refinement residual of all of them is one complex128
+// GEMM (cuBLAS ZGEMM) on the FP64 matrix. Each right-hand side keeps its own Krylov basis and
+// convergence state (the reference's block_gmres, block_gmres.rs:163, shares one basis instead).
+
+#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cstring>
@@ -34,7 +43,8 @@ namespace sb {
 struct BInst {
     const float2* A;  // complex64 matrix, row-major, even leading dimension lda
     int64_t lda, n, ldv;
-    float2* V;        // Krylov basis, (m + 1) x ldv
+    int64_t vs;       // distance between consecutive basis vectors
+    float2* V;        // Krylov basis: vector i at V + i * vs
     float2* w;
     float2* rb;       // inner right-hand side r / ||r||
     float2* d;        // inner solution
@@ -90,7 +100,7 @@ __global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restric
     if (!open_gate(I, gk)) return;
     const int64_t blk = blockIdx.x - pre[b];
     if (mode == 0)
-        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.V + (int64_t)j * I.ldv, I.w,
+        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.V + (int64_t)j * I.vs, I.w,
                                                                     nullptr, nullptr, blk);
     else
         gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.d, I.rq, I.rb, I.pnorm, blk);
@@ -106,7 +116,7 @@ __global__ void __launch_bounds__(kGemvThreads) k_bres64(const BInst* __restrict
                                                                blockIdx.x - pre[b]);
 }
 
-// Per-chunk squared norms: sel 0 = rb, 1 = b, 2 = b - r (= A x).
+// Per-chunk squared norms: sel 0 = rb, 1 = b, 2 = b - r (= A x), 3 = r.
 __global__ void __launch_bounds__(kChunk) k_bvnorm(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
                                                    int ninst, int sel, int gk) {
     __shared__ double red[kChunk / 32];
@@ -123,11 +133,34 @@ __global__ void __launch_bounds__(kChunk) k_bvnorm(const BInst* __restrict__ ins
         } else if (sel == 1) {
             const double2 a = I.b[r];
             v[0] = a.x * a.x + a.y * a.y;
-        } else {
+        } else if (sel == 2) {
             const double2 a = I.b[r], q = I.r[r];
             const double ar = a.x - q.x, ai = a.y - q.y;
             v[0] = ar * ar + ai * ai;
+        } else {
+            const double2 q = I.r[r];
+            v[0] = q.x * q.x + q.y * q.y;
         }
+    }
+    block_sum<1, kChunk>(v, red);
+    if (threadIdx.x == 0) I.pnorm[chunk] = v[0];
+}
+
+// rq = rb - w (w = A d from a block product), per-chunk squared norms of rq.
+__global__ void __launch_bounds__(kChunk) k_bresid_w(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+                                                     int ninst, int gk) {
+    __shared__ double red[kChunk / 32];
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const int64_t chunk = blockIdx.x - pre[b];
+    const int64_t r = chunk * kChunk + threadIdx.x;
+    double v[1] = {0.0};
+    if (r < I.n) {
+        const float2 a = I.rb[r], q = I.w[r];
+        const float2 o = make_float2(a.x - q.x, a.y - q.y);
+        I.rq[r] = o;
+        v[0] = (double)o.x * o.x + (double)o.y * o.y;
     }
     block_sum<1, kChunk>(v, red);
     if (threadIdx.x == 0) I.pnorm[chunk] = v[0];
@@ -164,7 +197,7 @@ __global__ void __launch_bounds__(kChunk) k_bdots(const BInst* __restrict__ inst
         for (int t = 0; t < kBDotVecs; ++t) {
             const int i = i0 + t;
             if (i < k) {
-                const float2 v = I.V[i * I.ldv + r];
+                const float2 v = I.V[i * I.vs + r];
                 acc[2 * t] = (double)v.x * wv.x + (double)v.y * wv.y;
                 acc[2 * t + 1] = (double)v.x * wv.y - (double)v.y * wv.x;
             } else if (i == k) {
@@ -215,7 +248,7 @@ __global__ void __launch_bounds__(kChunk) k_bproject(const BInst* __restrict__ i
         const float2 w0 = I.w[r];
         double ar = w0.x, ai = w0.y;
         for (int i = 0; i < k; ++i) {
-            const float2 v = I.V[i * I.ldv + r];
+            const float2 v = I.V[i * I.vs + r];
             ar -= sc[i].x * v.x - sc[i].y * v.y;
             ai -= sc[i].x * v.y + sc[i].y * v.x;
         }
@@ -251,7 +284,7 @@ __global__ void __launch_bounds__(kChunk) k_bnext(const BInst* __restrict__ inst
     if (r >= I.n) return;
     const double s = I.st->inv_wn;
     const float2 v = I.w[r];
-    I.V[(int64_t)(j + 1) * I.ldv + r] = make_float2(static_cast<float>(v.x * s), static_cast<float>(v.y * s));
+    I.V[(int64_t)(j + 1) * I.vs + r] = make_float2(static_cast<float>(v.x * s), static_cast<float>(v.y * s));
 }
 
 // Vector updates over the flattened chunks.
@@ -277,7 +310,7 @@ __global__ void __launch_bounds__(kChunk) k_bvec(const BInst* __restrict__ inst,
         if (r >= I.n) return;
         double sr = 0.0, si = 0.0;
         for (int i = 0; i < k; ++i) {
-            const float2 v = I.V[i * I.ldv + r];
+            const float2 v = I.V[i * I.vs + r];
             sr += sy[i].x * v.x - sy[i].y * v.y;
             si += sy[i].x * v.y + sy[i].y * v.x;
         }
@@ -388,6 +421,14 @@ struct Batch {
     int device = 0;
     int ninst = 0;
     int64_t m = 0;  // Krylov dimension the workspace was sized for
+    std::vector<int64_t> nvec;  // unknowns per instance
+    // Many right-hand sides of one operator: products through `shared` (tensor-core block product
+    // for the inner solves, ZGEMM for the FP64 residual); vectors stored right-hand-side-major.
+    Operator* shared = nullptr;
+    cublasHandle_t blas = nullptr;
+    float2 *w_all = nullptr, *d_all = nullptr, *v_all = nullptr;
+    double2 *x_all = nullptr, *r_all = nullptr, *b_all = nullptr;
+    int64_t ld_all = 0;
     std::vector<Mesh*> meshes;
     std::vector<sb_physics> phys;
     std::vector<double2> beta;
@@ -402,6 +443,7 @@ struct Batch {
     cudaGraphExec_t exec = nullptr;
     int64_t graph_kernels = 0;
     bool graph_prof = false;
+    uint64_t graph_gen = 0;  // tensor-plane generation the captured cycle refers to
     std::vector<ProfPair> prof_pairs;
     Pinned pin;  // host mirror of the per-instance states, norms, scalars and flags
     bool assembled = false, solved = false;
@@ -415,6 +457,7 @@ struct Batch {
     }
     ~Batch() {
         reset_graph();
+        if (blas) cublasDestroy(blas);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -461,9 +504,10 @@ static void batch_workspace(Batch& B, int64_t m) {
     B.m = 0;
     B.solved = false;
     const int ni = B.ninst;
+    const bool shared = B.shared != nullptr;
     size_t f32 = 0, f64 = 0, small = 0;
     for (int b = 0; b < ni; ++b) {
-        const int64_t n = B.meshes[b]->n, ldv = (n + 1) / 2 * 2;
+        const int64_t n = B.nvec[b], ldv = (n + 1) / 2 * 2;
         const int64_t chunks = cdiv64(n, kChunk);
         f32 += round256(sizeof(float2) * (m + 1) * ldv) + 4 * round256(sizeof(float2) * ldv);
         f64 += 2 * round256(sizeof(double2) * ldv);
@@ -489,23 +533,52 @@ static void batch_workspace(Batch& B, int64_t m) {
         return p;
     };
     B.h.assign(ni, BInst{});
+    if (shared) {
+        // Right-hand-side-major families, each one block: vector c of a family at base + c * ld_all,
+        // basis vector i of right-hand side c at v_all + (i * ninst + c) * ld_all. Zero-filled so the
+        // block products never read stale values.
+        SB_CUDA(cudaMemset(B.pool_f32.p, 0, f32));
+        SB_CUDA(cudaMemset(B.pool_f64.p, 0, f64));
+        const int64_t ld = B.ld_all;
+        B.v_all = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * (m + 1) * ni * ld));
+        B.w_all = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ni * ld));
+        float2* rb_all = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ni * ld));
+        B.d_all = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ni * ld));
+        float2* rq_all = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ni * ld));
+        B.x_all = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ni * ld));
+        B.r_all = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ni * ld));
+        for (int b = 0; b < ni; ++b) {
+            BInst& I = B.h[b];
+            I.V = B.v_all + b * ld;
+            I.vs = ni * ld;
+            I.w = B.w_all + b * ld;
+            I.rb = rb_all + b * ld;
+            I.d = B.d_all + b * ld;
+            I.rq = rq_all + b * ld;
+            I.x = B.x_all + b * ld;
+            I.r = B.r_all + b * ld;
+        }
+    }
     B.pre4.assign(ni + 1, 0);
     B.pre256.assign(ni + 1, 0);
     for (int b = 0; b < ni; ++b) {
-        const int64_t n = B.meshes[b]->n, ldv = (n + 1) / 2 * 2;
+        const int64_t n = B.nvec[b], ldv = (n + 1) / 2 * 2;
         const int64_t chunks = cdiv64(n, kChunk);
         BInst& I = B.h[b];
-        I.A = B.asm_h[b].A32;
-        I.lda = B.asm_h[b].lda32;
         I.n = n;
         I.ldv = ldv;
-        I.V = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * (m + 1) * ldv));
-        I.w = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
-        I.rb = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
-        I.d = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
-        I.rq = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
-        I.x = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
-        I.r = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
+        if (!shared) {
+            I.A = B.asm_h[b].A32;
+            I.lda = B.asm_h[b].lda32;
+            I.V = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * (m + 1) * ldv));
+            I.vs = ldv;
+            I.w = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+            I.rb = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+            I.d = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+            I.rq = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+            I.x = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
+            I.r = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
+        }
         I.b = B.rhs[b];
         I.H = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 1) * m));
         I.cs = reinterpret_cast<double2*>(take(ps, sizeof(double2) * m));
@@ -545,7 +618,10 @@ static void batch_step(Batch& B, int j) {
     const cudaStream_t s = B.stream;
     const unsigned gi = static_cast<unsigned>(cdiv64(ni, 64));
     capture_step(j);
-    {
+    if (B.shared) {
+        // all right-hand sides at once: W = A V_j on the tensor cores
+        tensor_block_product(*B.shared, B.v_all + (int64_t)j * ni * B.ld_all, B.ld_all, ni, B.w_all, B.ld_all, s);
+    } else {
         ProfScope prof(SB_PROF_GEMV32, s);
         k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 0, j, G_ACTIVE);
         count_launch();
@@ -565,12 +641,14 @@ static void batch_step(Batch& B, int j) {
     k_bgivens<<<gi, 64, 0, s>>>(I, ni, j);
     k_bnext<<<g256, kChunk, 0, s>>>(I, p256, ni, j);
     for (int t = 0; t < 11; ++t) count_launch();
+    (void)g4;
     SB_CUDA(cudaGetLastError());
 }
 
 // One restart cycle of the whole batch: m Arnoldi steps captured once into a CUDA graph.
 static void batch_cycle(Batch& B) {
-    if (!B.exec || B.graph_prof != g_prof_on) {
+    const uint64_t gen = B.shared ? tensor_generation(*B.shared) : 0;
+    if (!B.exec || B.graph_prof != g_prof_on || B.graph_gen != gen) {
         B.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&B.prof_pairs);
@@ -590,9 +668,26 @@ static void batch_cycle(Batch& B) {
         B.graph_kernels = kernel_count() - before;
         add_kernel_count(-B.graph_kernels);
         B.graph_prof = g_prof_on;
+        B.graph_gen = gen;
     }
     SB_CUDA(cudaGraphLaunch(B.exec, B.stream));
     add_kernel_count(B.graph_kernels);
+}
+
+// r = b - A x for every right-hand side of a shared operator: one complex128 GEMM on the FP64
+// matrix (row-major A is the transpose of the column-major view cuBLAS takes).
+static void shared_residual64(Batch& B) {
+    const Operator& op = *B.shared;
+    const int64_t n = op.n, ld = B.ld_all;
+    SB_CUDA(cudaMemcpyAsync(B.r_all, B.b_all, sizeof(double2) * B.ninst * ld, cudaMemcpyDeviceToDevice, B.stream));
+    ProfScope prof(SB_PROF_GEMV64, B.stream);
+    const cuDoubleComplex alpha = make_cuDoubleComplex(-1.0, 0.0), beta = make_cuDoubleComplex(1.0, 0.0);
+    const cublasStatus_t st = cublasZgemm(B.blas, CUBLAS_OP_T, CUBLAS_OP_N, static_cast<int>(n), B.ninst,
+                                          static_cast<int>(n), &alpha,
+                                          reinterpret_cast<const cuDoubleComplex*>(op.A64.p), static_cast<int>(n),
+                                          reinterpret_cast<const cuDoubleComplex*>(B.x_all), static_cast<int>(ld),
+                                          &beta, reinterpret_cast<cuDoubleComplex*>(B.r_all), static_cast<int>(ld));
+    SB_REQUIRE(st == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasZgemm failed (FP64 residual of the block)");
 }
 
 // Mixed-precision iterative refinement of every instance in lockstep (gmres_mixed_ir semantics
@@ -649,12 +744,19 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
     for (int64_t it = 0; it <= cfg.max_refinements; ++it) {
         if (it > 0) {
             // FP64 residual of the refining instances.
-            {
-                ProfScope prof(SB_PROF_GEMV32, s);
-                k_bres64<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, G_OUTER);
+            if (B.shared) {
+                shared_residual64(B);
+                k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 3, G_OUTER);
+                k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_OUTER);
+                launched(2);
+            } else {
+                {
+                    ProfScope prof(SB_PROF_GEMV32, s);
+                    k_bres64<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, G_OUTER);
+                }
+                k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_OUTER);
+                launched(2);
             }
-            k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_OUTER);
-            launched(2);
             d2h(hv.nrm, dv.nrm, sizeof(double) * 3 * ni);
             SB_CUDA(cudaStreamSynchronize(s));
             for (int b = 0; b < ni; ++b)
@@ -707,12 +809,19 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
             launched(2);
             if (!last) {
                 // restart residual rq = rb - A d of the instances that completed m steps
-                {
-                    ProfScope prof(SB_PROF_GEMV32, s);
-                    k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 1, 0, G_RESTART);
+                if (B.shared) {
+                    tensor_block_product(*B.shared, B.d_all, B.ld_all, ni, B.w_all, B.ld_all, s);
+                    k_bresid_w<<<g256, kChunk, 0, s>>>(I, p256, ni, G_RESTART);
+                    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_RESTART);
+                    launched(2);
+                } else {
+                    {
+                        ProfScope prof(SB_PROF_GEMV32, s);
+                        k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 1, 0, G_RESTART);
+                    }
+                    k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_RESTART);
+                    launched(2);
                 }
-                k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_RESTART);
-                launched(2);
             }
             d2h(hv.st, dv.st, sizeof(KState) * ni);
             k_bcontrol<<<gi, 64, 0, s>>>(I, ni, 1, last ? 1 : 0);
@@ -784,6 +893,60 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Many right-hand sides of one operator
+// ---------------------------------------------------------------------------------------------
+static Batch& multi_batch(Operator& op, int r) {
+    Batch* B = static_cast<Batch*>(op.multi);
+    if (B && B->ninst == r) return *B;
+    delete B;
+    op.multi = nullptr;
+    B = new Batch();
+    op.multi = B;
+    B->device = op.device;
+    B->ninst = r;
+    B->shared = &op;
+    B->nvec.assign(r, op.n);
+    B->ld_all = (op.n + 1) / 2 * 2;
+    SB_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    SB_REQUIRE(cublasCreate(&B->blas) == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasCreate failed");
+    SB_REQUIRE(cublasSetStream(B->blas, B->stream) == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasSetStream failed");
+    B->pool_rhs.alloc(sizeof(double2) * r * B->ld_all);
+    SB_CUDA(cudaMemset(B->pool_rhs.p, 0, sizeof(double2) * r * B->ld_all));
+    B->b_all = B->pool_rhs.as<double2>();
+    for (int c = 0; c < r; ++c) B->rhs.push_back(B->b_all + (int64_t)c * B->ld_all);
+    B->assembled = true;
+    return *B;
+}
+
+void multi_release(Operator& op) {
+    delete static_cast<Batch*>(op.multi);
+    op.multi = nullptr;
+}
+
+// Solve A x_c = b_c for r right-hand sides given right-hand-side-major on the device (b_c at
+// b + c * ldb, x_c at x + c * ldx, complex128).
+void multi_solve_device(Operator& op, const double2* b, int64_t ldb, int r, double2* x, int64_t ldx,
+                        const sb_ir_config& cfg, sb_gmres_stats* stats) {
+    SB_REQUIRE(op.A64.p, SB_ERR_INVALID_ARGUMENT,
+               "multi-RHS solve: the FP64 refinement needs the complex128 matrix (SB_PRECISION_FP64 or "
+               "SB_PRECISION_FP64_FP32)");
+    SB_CUDA(cudaSetDevice(op.device));
+    if (!tensor_ready(op)) tensor_prepare(op);
+    tensor_reserve(op, r);
+    Batch& B = multi_batch(op, r);
+    batch_workspace(B, cfg.inner_restart);
+    SB_CUDA(cudaStreamSynchronize(op.stream));
+    SB_CUDA(cudaMemcpy2DAsync(B.b_all, sizeof(double2) * B.ld_all, b, sizeof(double2) * ldb, sizeof(double2) * op.n,
+                              r, cudaMemcpyDeviceToDevice, B.stream));
+    batch_solve(B, cfg, stats);
+    SB_REQUIRE(tensor_status(op, true) == 0, SB_ERR_DEVICE_CHECK,
+               "multi-RHS solve: a pipeline wait of the tensor-core kernel timed out");
+    SB_CUDA(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, B.x_all, sizeof(double2) * B.ld_all, sizeof(double2) * op.n,
+                              r, cudaMemcpyDeviceToDevice, B.stream));
+    SB_CUDA(cudaStreamSynchronize(B.stream));
+}
+
 }  // namespace sb
 
 using namespace sb;
@@ -842,6 +1005,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
                            "batch: meshes with prescribed boundary values are not batched (rigid or "
                            "admittance surfaces only)");
                 B->meshes.push_back(m);
+                B->nvec.push_back(m->n);
                 B->phys.push_back(physics[i]);
                 B->beta.push_back(make_double2(betas[i].re, betas[i].im));
             }

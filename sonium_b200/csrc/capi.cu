@@ -349,6 +349,7 @@ SB_API int sb_operator_destroy(sb_operator* op) {
         if (op->op) {
             cudaSetDevice(op->op->device);
             destroy_solve_work(*op->op);
+            multi_release(*op->op);
             tensor_release(*op->op);
             if (op->op->stream) cudaStreamDestroy(op->op->stream);
             delete op->op;
@@ -522,6 +523,47 @@ SB_API int sb_operator_apply_block_tensor(const sb_operator* op, const sb_comple
         SB_CUDA(cudaStreamSynchronize(o.stream));
         SB_REQUIRE(tensor_status(o, true) == 0, SB_ERR_DEVICE_CHECK,
                    "apply_block_tensor: a pipeline wait of the tensor-core kernel timed out");
+    });
+}
+
+static void check_ir(const sb_ir_config* cfg);
+
+SB_API int sb_gmres_multi(const sb_operator* op, const sb_complex* b, int64_t r, const sb_ir_config* cfg,
+                          sb_complex* x, sb_gmres_stats* stats) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && b && x && cfg && stats && r >= 1, SB_ERR_INVALID_ARGUMENT, "bad argument");
+        SB_REQUIRE(r <= 65536, SB_ERR_INVALID_ARGUMENT, "gmres_multi: at most 65536 right-hand sides");
+        check_ir(cfg);
+        Operator& o = *op->op;
+        const int64_t n = o.n;
+        SB_REQUIRE(all_finite(b, n * r), SB_ERR_NOT_FINITE, "gmres_multi: non-finite right-hand side block");
+        SB_CUDA(cudaSetDevice(o.device));
+        maybe_inject(SB_INJECT_LAUNCH);
+        // n x r row-major block (the reference's DenseMatrix layout) <-> right-hand-side-major device
+        std::vector<sb_complex> t(n * r);
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t c = 0; c < r; ++c) t[c * n + i] = b[i * r + c];
+        DevBuf db, dx;
+        db.alloc(sizeof(double2) * n * r);
+        dx.alloc(sizeof(double2) * n * r);
+        SB_CUDA(cudaMemcpy(db.p, t.data(), sizeof(double2) * n * r, cudaMemcpyHostToDevice));
+        multi_solve_device(o, db.as<double2>(), n, static_cast<int>(r), dx.as<double2>(), n, *cfg, stats);
+        SB_CUDA(cudaMemcpy(t.data(), dx.p, sizeof(double2) * n * r, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t c = 0; c < r; ++c) x[i * r + c] = t[c * n + i];
+    });
+}
+
+SB_API int sb_gmres_multi_device(const sb_operator* op, const sb_complex* b_dev, int64_t r, const sb_ir_config* cfg,
+                                 sb_complex* x_dev, sb_gmres_stats* stats) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && b_dev && x_dev && cfg && stats && r >= 1, SB_ERR_INVALID_ARGUMENT, "bad argument");
+        SB_REQUIRE(r <= 65536, SB_ERR_INVALID_ARGUMENT, "gmres_multi: at most 65536 right-hand sides");
+        check_ir(cfg);
+        Operator& o = *op->op;
+        maybe_inject(SB_INJECT_LAUNCH);
+        multi_solve_device(o, reinterpret_cast<const double2*>(b_dev), o.n, static_cast<int>(r),
+                           reinterpret_cast<double2*>(x_dev), o.n, *cfg, stats);
     });
 }
 

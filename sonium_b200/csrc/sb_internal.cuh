@@ -124,6 +124,7 @@ struct Operator {
     DevBuf coef, far_part, near_rhs, self_rhs, scratch, status;
     void* work = nullptr;        // solver workspace (gmres.cu), released by destroy_solve_work
     void* tensor = nullptr;      // BF16 split planes for the tensor-core block product (tensor.cu)
+    void* multi = nullptr;       // many-right-hand-side solver workspace (batch.cu)
     cudaStream_t stream = nullptr;
     double last_assembly_ms = 0.0;
 };
@@ -187,5 +188,15 @@ bool tensor_ready(const Operator& op);
 void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int r, float2* y, int64_t ldy,
                           cudaStream_t s);
 int tensor_status(const Operator& op, bool reset);
+// Split planes for up to r vectors, allocated ahead of any stream capture.
+void tensor_reserve(const Operator& op, int r);
+// Changes whenever the planes (and so the tensor maps baked into captured graphs) change.
+uint64_t tensor_generation(const Operator& op);
+
+// Many right-hand sides of one operator (batch.cu): r systems solved in lockstep, products for all
+// of them on the tensor cores, FP64 refinement residual by one complex128 GEMM.
+void multi_solve_device(Operator& op, const double2* b, int64_t ldb, int r, double2* x, int64_t ldx,
+                        const sb_ir_config& cfg, sb_gmres_stats* stats);
+void multi_release(Operator& op);
 
 }  // namespace sb

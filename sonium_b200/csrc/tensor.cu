@@ -258,6 +258,7 @@ CUtensorMap make_map(void* base, int64_t rows, int64_t ldk, int box_rows) {
 
 // Split planes of an operator's matrix and of the right-hand-side blocks (internal).
 struct TensorWork {
+    uint64_t gen = 0;  // changes whenever a plane (and so a tensor map) is re-allocated
     int64_t n = 0, ldk = 0, rows = 0;
     DevBuf a_hi, a_lo;
     CUtensorMap tm_a_hi, tm_a_lo;
@@ -265,6 +266,13 @@ struct TensorWork {
     DevBuf x_hi, x_lo, status;
     CUtensorMap tm_x_hi, tm_x_lo;
 };
+
+static uint64_t g_tensor_gen = 0;
+
+uint64_t tensor_generation(const Operator& op) {
+    const TensorWork* w = static_cast<const TensorWork*>(op.tensor);
+    return w ? w->gen : 0;
+}
 
 void tensor_release(Operator& op) {
     delete static_cast<TensorWork*>(op.tensor);
@@ -279,6 +287,7 @@ void tensor_prepare(Operator& op) {
     tensor_release(op);
     TensorWork* w = new TensorWork();
     op.tensor = w;
+    w->gen = ++g_tensor_gen;
     w->n = op.n;
     w->ldk = cdiv(op.n, kTileK) * kTileK;
     w->rows = cdiv(2 * op.n, kTileM) * kTileM;
@@ -306,6 +315,22 @@ void tensor_prepare(Operator& op) {
     SB_CUDA(cudaStreamSynchronize(op.stream));
 }
 
+void tensor_reserve(const Operator& op, int r) {
+    TensorWork* w = static_cast<TensorWork*>(op.tensor);
+    SB_REQUIRE(w, SB_ERR_INVALID_ARGUMENT, "tensor-core block product: call sb_operator_prepare_block_tensor first");
+    const int rblocks = static_cast<int>(cdiv(r, kTileRhs));
+    if (rblocks <= w->rblocks) return;
+    const size_t bytes = sizeof(__nv_bfloat16) * (size_t)rblocks * 2 * kTileRhs * w->ldk;
+    w->x_hi.alloc(bytes);
+    w->x_lo.alloc(bytes);
+    SB_CUDA(cudaMemset(w->x_hi.p, 0, bytes));
+    SB_CUDA(cudaMemset(w->x_lo.p, 0, bytes));
+    w->rblocks = rblocks;
+    w->gen = ++g_tensor_gen;
+    w->tm_x_hi = make_map(w->x_hi.p, (int64_t)rblocks * 2 * kTileRhs, w->ldk, 2 * kTileRhs);
+    w->tm_x_lo = make_map(w->x_lo.p, (int64_t)rblocks * 2 * kTileRhs, w->ldk, 2 * kTileRhs);
+}
+
 // Y (r vectors, vector c at y + c * ldy, complex64) = A X (vector c at x + c * ldx).
 void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int r, float2* y, int64_t ldy,
                           cudaStream_t s) {
@@ -313,16 +338,7 @@ void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int 
     SB_REQUIRE(w, SB_ERR_INVALID_ARGUMENT, "tensor-core block product: call sb_operator_prepare_block_tensor first");
     SB_REQUIRE(r >= 1, SB_ERR_INVALID_ARGUMENT, "tensor-core block product: r must be positive");
     const int rblocks = static_cast<int>(cdiv(r, kTileRhs));
-    if (rblocks > w->rblocks) {
-        const size_t bytes = sizeof(__nv_bfloat16) * (size_t)rblocks * 2 * kTileRhs * w->ldk;
-        w->x_hi.alloc(bytes);
-        w->x_lo.alloc(bytes);
-        SB_CUDA(cudaMemset(w->x_hi.p, 0, bytes));
-        SB_CUDA(cudaMemset(w->x_lo.p, 0, bytes));
-        w->rblocks = rblocks;
-        w->tm_x_hi = make_map(w->x_hi.p, (int64_t)rblocks * 2 * kTileRhs, w->ldk, 2 * kTileRhs);
-        w->tm_x_lo = make_map(w->x_lo.p, (int64_t)rblocks * 2 * kTileRhs, w->ldk, 2 * kTileRhs);
-    }
+    if (rblocks > w->rblocks) tensor_reserve(op, r);
     const int64_t tot = (int64_t)rblocks * kTileRhs * w->n;
     {
         ProfScope prof(SB_PROF_OTHER, s);

@@ -373,5 +373,31 @@ def gmres_mixed(operator: TbemOperator, b, config: IrConfig = IrConfig(), x0=Non
     return GmresSolution._from(x, st)
 
 
+def gmres_multi(operator: TbemOperator, B, config: IrConfig = IrConfig()):
+    """Many right-hand sides of one operator (the block_gmres_preconditioned role,
+    crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:163): B is n x r, returns
+    (X n x r, [GmresSolution without x per right-hand side]). Inner products on the tensor cores,
+    FP64 refinement; the operator must hold the complex128 matrix."""
+    B = _c128(B)
+    if B.ndim != 2 or B.shape[0] != operator.n:
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "gmres_multi: B must be n x r")
+    r = B.shape[1]
+    X = np.zeros_like(B)
+    stats = (L.SbGmresStats * r)()
+    check(L.load().sb_gmres_multi(operator.handle, _p(B), r, ct.byref(config._struct()), _p(X),
+                                  ct.cast(stats, ct.c_void_p)))
+    return X, [GmresSolution._from(None, stats[i]) for i in range(r)]
+
+
+def fibonacci_sphere_directions(n: int) -> np.ndarray:
+    """Unit vectors on a Fibonacci sphere (the reference's fibonacci_sphere_directions,
+    crates/sonium-bem/src/core/assembly/mlfmm.rs:8012-8024)."""
+    golden = (1.0 + np.sqrt(5.0)) / 2.0
+    i = np.arange(n, dtype=np.float64)
+    theta = np.arccos(1.0 - 2.0 * (i + 0.5) / n)
+    phi = 2.0 * np.pi * i / golden
+    return np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)], axis=1)
+
+
 def inject_failure(point: int) -> None:
     check(L.load().sb_inject_failure(point))

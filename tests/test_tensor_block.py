@@ -82,3 +82,53 @@ def test_block_product_plane_wave_rhs_block(gpu, oracle):
     with pytest.raises(gpu.SoniumError):
         _apply_tensor(op, X)
     op.close()
+
+
+def test_multi_rhs_solve_matches_fp64_solves(gpu, oracle):
+    """sb_gmres_multi: 64 plane-wave right-hand sides (Fibonacci directions) on an ellipsoid, each
+    within 1e-6 of its own FP64 GMRES solve, every one converged to its FP64 residual target."""
+    nodes, tris = oracle.icosphere(1.0, 3, (1.0, 0.6, 0.4))
+    mesh = gpu.Mesh(nodes, tris)
+    ph = gpu.PhysicsParams.for_wavenumber(4.0)
+    beta = ph.burton_miller_beta()
+    op = gpu.build_tbem_system_with_beta(mesh, ph, beta)
+    dirs = gpu.fibonacci_sphere_directions(64)
+    B = gpu.rhs_plane_wave(mesh, ph, beta, dirs)
+    cfg = gpu.IrConfig(tolerance=1e-9)
+    X, st = gpu.gmres_multi(op, B, cfg)
+    A = op.matrix
+    for c in (0, 17, 40, 63):
+        ref = gpu.gmres(op, B[:, c], gpu.GmresConfig(max_iterations=100, restart=50, tolerance=1e-11)).x
+        assert np.linalg.norm(X[:, c] - ref) / np.linalg.norm(ref) < 1e-6, c
+    assert all(s.converged and s.residual < 1e-9 for s in st)
+    res = np.linalg.norm(B - A @ X, axis=0) / np.linalg.norm(B, axis=0)
+    assert res.max() < 1e-9
+    assert np.allclose([s.residual for s in st], res, rtol=1e-3, atol=1e-14)
+    assert all(s.matvecs_fp32 > 0 and s.refinements >= 1 for s in st)
+    op.close()
+
+
+def test_multi_rhs_partial_block_zero_rhs_and_rejections(gpu, oracle):
+    """Fewer right-hand sides than a tile, one of them zero (done at once, x = 0), a second solve
+    reusing the workspace, and an operator without the complex128 matrix rejected."""
+    nodes, tris = oracle.icosphere(1.0, 2)
+    mesh = gpu.Mesh(nodes, tris[:-1])  # odd n
+    ph = gpu.PhysicsParams.for_wavenumber(2.0)
+    beta = ph.burton_miller_beta()
+    op = gpu.build_tbem_system_with_beta(mesh, ph, beta, gpu.SB_PRECISION_FP64_FP32)
+    B = gpu.rhs_plane_wave(mesh, ph, beta, gpu.fibonacci_sphere_directions(5))
+    B[:, 2] = 0
+    X, st = gpu.gmres_multi(op, B, gpu.IrConfig(tolerance=1e-10))
+    assert st[2].iterations == 0 and st[2].converged and np.all(X[:, 2] == 0)
+    A = op.matrix
+    for c in (0, 1, 3, 4):
+        assert st[c].converged
+        assert np.linalg.norm(B[:, c] - A @ X[:, c]) / np.linalg.norm(B[:, c]) < 1e-10
+    X2, _ = gpu.gmres_multi(op, B, gpu.IrConfig(tolerance=1e-10))
+    assert np.array_equal(X2, X)
+    op32 = gpu.build_tbem_system_with_beta(mesh, ph, beta, gpu.SB_PRECISION_FP32)
+    with pytest.raises(gpu.SoniumError) as e:
+        gpu.gmres_multi(op32, B, gpu.IrConfig())
+    assert "complex128" in str(e.value)
+    op.close()
+    op32.close()
