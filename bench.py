@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true", help="skip the batched frequency-sweep leg")
     ap.add_argument("--sweep-count", type=int, default=64, help="instances of the frequency sweep")
     ap.add_argument("--sweep-only", action="store_true", help="run only the sweep leg and print its JSON")
+    ap.add_argument("--multi-rhs", action="store_true",
+                    help="run only the 256-right-hand-side tensor-core leg and print its JSON")
+    ap.add_argument("--rhs", type=int, default=256, help="right-hand sides of the multi-RHS leg")
     ap.add_argument("--precision-form", action="store_true",
                     help="run only the N = 81920, k = 40 precision-form leg (~165 GB) and print its JSON")
     ap.add_argument("--single", action="store_true",
@@ -245,10 +248,12 @@ def main():
         single_solves(sb, a.level, a.k, dev)
         return
     assert sb.device_count() > dev, "no CUDA device for this rank"
-    if a.sweep_only or a.precision_form:
-        out = (sweep_leg if a.sweep_only else precision_leg)(sb, a, dist, dev, _cudart())
+    if a.sweep_only or a.precision_form or a.multi_rhs:
+        name, leg = (("sweep", sweep_leg) if a.sweep_only else ("precision_form", precision_leg)
+                     if a.precision_form else ("multi_rhs", multi_rhs_leg))
+        out = leg(sb, a, dist, dev, _cudart())
         if dist.rank == 0:
-            print(json.dumps({"sweep" if a.sweep_only else "precision_form": out}), flush=True)
+            print(json.dumps({name: out}), flush=True)
         dist.close()
         return
 
@@ -505,6 +510,105 @@ def sweep_leg(sb, a, dist, dev, rt):
         "assembly_ms": asm_ms, "solve_ms": solve_ms,
         "iterations_batched": [int(s.iterations) for s in st0], "iterations_fp64": fp64_iters,
         "timing": "wall clock around device-synchronised steps, max over ranks",
+    }
+
+
+def multi_rhs_leg(sb, a, dist, dev, rt):
+    """Multi-RHS tensor-core form: ellipsoid (1, 0.6, 0.4) icosphere level 5 (N = 20480), k = 16,
+    256 plane waves along Fibonacci-sphere directions, complex128 assembly.
+
+    A step = one sb_gmres_multi_device solve of all 256 right-hand sides (device-resident b and x):
+    FP32-inner GMRES(50) with every step's 256 products as one tensor-core block product (BF16
+    hi/lo split, FP32 accumulation) and FP64 refinement to rtol 1e-8 by one complex128 GEMM per
+    refinement. Device time from the solver (CUDA events on its stream). Baseline: plain FP64
+    GMRES(50) to 1e-8, one right-hand side after another, timed on a sample of 16 directions and
+    reported per right-hand side; the error of the multi-RHS solutions against those FP64 solutions."""
+    from sonium_b200 import _lib as L
+
+    level, k, r = 5, 16.0, a.rhs
+    nodes, tris = sb.icosphere(RADIUS, level, (1.0, 0.6, 0.4))
+    n = tris.shape[0]
+    mesh = sb.Mesh(nodes, tris, device=dev)
+    ph = sb.PhysicsParams.for_wavenumber(k)
+    beta = ph.burton_miller_beta()
+    op = sb.build_tbem_system_with_beta(mesh, ph, beta, sb.SB_PRECISION_FP64)
+    B = sb.rhs_plane_wave(mesh, ph, beta, sb.fibonacci_sphere_directions(r))  # n x r
+    lib = L.load()
+    bt = np.ascontiguousarray(B.T)  # right-hand-side-major
+    b_d = _dev_alloc(rt, bt.nbytes)
+    x_d = _dev_alloc(rt, bt.nbytes)
+    if rt.cudaMemcpy(b_d, bt.ctypes.data, bt.nbytes, 1) != 0:
+        raise RuntimeError("cudaMemcpy failed")
+    ir = L.SbIrConfig(20, TOL, RESTART, 20, 1e-5)
+    stats = (L.SbGmresStats * r)()
+
+    def solve():
+        L.check(lib.sb_gmres_multi_device(op.handle, b_d, r, ct.byref(ir), x_d, ct.cast(stats, ct.c_void_p)))
+        return stats[0].device_ms
+
+    solve()
+    X = np.zeros((r, n), np.complex128)
+    rt.cudaDeviceSynchronize()
+    rt.cudaMemcpy(X.ctypes.data, x_d, X.nbytes, 2)
+    first = [L.SbGmresStats.from_buffer_copy(stats[i]) for i in range(r)]
+    for _ in range(a.warmup):
+        solve()
+    prof = L.SbProfile()
+    L.check(lib.sb_profile_read(ct.byref(prof), 1))
+    L.check(lib.sb_profile_enable(1))
+    times = [solve() for _ in range(a.steps)]
+    L.check(lib.sb_profile_enable(0))
+    L.check(lib.sb_profile_read(ct.byref(prof), 1))
+    t_block = float(np.median(times)) / 1e3
+    return multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, t_block, rt, b_d, x_d, n, r, level, k)
+
+
+def multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, t_block, rt, b_d, x_d, n, r, level, k):
+    """FP64 baseline on a sample of right-hand sides and the tensor-kernel roofline of the leg."""
+    sample = list(range(0, r, max(1, r // 16)))[:16]
+    gc = sb.GmresConfig(100, RESTART, TOL)
+    rt.cudaDeviceSynchronize()
+    t0 = time.perf_counter()
+    errs, it64 = [], []
+    for c in sample:
+        s = sb.gmres(op, B[:, c], gc)
+        errs.append(float(np.linalg.norm(X[c] - s.x) / np.linalg.norm(s.x)))
+        it64.append(int(s.iterations))
+    rt.cudaDeviceSynchronize()
+    t64 = (time.perf_counter() - t0) / len(sample)
+    rt.cudaFree(b_d)
+    rt.cudaFree(x_d)
+    op.close()
+    mesh.close()
+    pk, pk_kind = peaks()
+    names = L.PROF_NAMES
+    ms = {names[i]: prof.ms[i] for i in range(L.SB_PROF_KINDS)}
+    launches = {names[i]: prof.launches[i] for i in range(L.SB_PROF_KINDS)}
+    tl = launches["tensor"]
+    avg = ms["tensor"] / max(tl, 1) / 1e3
+    executed = 24.0 * n * n * 128 * ((r + 127) // 128)  # 3 BF16 terms x real GEMM (2N x 2R x N)
+    algorithmic = 8.0 * n * n * r                         # complex flops of A X
+    achieved = executed / max(avg, 1e-12) / 1e12
+    return {
+        "workload": f"ellipsoid (1, 0.6, 0.4) icosphere L{level} (N={n}), k={k}, {r} plane waves on "
+                    f"Fibonacci-sphere directions, complex128 assembly, rtol {TOL}",
+        "rhs_solves_per_s": r / t_block, "block_solve_ms": 1e3 * t_block,
+        "plain_fp64_rhs_solves_per_s": 1.0 / t64, "plain_fp64_ms_per_rhs": 1e3 * t64,
+        "speedup_vs_plain_fp64": (r / t_block) * t64,
+        "max_error_vs_fp64": max(errs), "error_sample": len(sample),
+        "all_converged": bool(all(s.converged for s in first)),
+        "max_residual": float(max(s.residual for s in first)),
+        "iterations_median": float(np.median([s.iterations for s in first])),
+        "refinements_median": float(np.median([s.refinements for s in first])),
+        "fp64_iterations_median": float(np.median(it64)),
+        "tensor_kernel": {"kernel": "k_block_bf16x3 (tcgen05 BF16 hi/lo split, TMA, TMEM)",
+                          "launches_per_solve": tl / max(a.steps, 1), "avg_launch_ms": avg * 1e3,
+                          "bound": "tensor", "achieved": achieved, "unit": "TFLOP/s",
+                          "peak": pk["bf16_tflops"], "frac": achieved / pk["bf16_tflops"],
+                          "peak_source": pk_kind, "executed_flop_per_launch": executed,
+                          "algorithmic_complex_flop_per_launch": algorithmic,
+                          "share_of_kernel_time": ms["tensor"] / max(sum(ms.values()), 1e-9)},
+        "kernel_ms_per_solve": {kk: v / max(a.steps, 1) for kk, v in ms.items() if v > 0},
     }
 
 
