@@ -514,8 +514,8 @@ def sweep_leg(sb, a, dist, dev, rt):
 
 
 def multi_rhs_leg(sb, a, dist, dev, rt):
-    """Multi-RHS tensor-core form: ellipsoid (1, 0.6, 0.4) icosphere level 5 (N = 20480), k = 16,
-    256 plane waves along Fibonacci-sphere directions, complex128 assembly.
+    """Multi-RHS tensor-core form: ellipsoid (1, 0.6, 0.4) icosphere level 5 (N = 20480; --level
+    changes it), k = 16, 256 plane waves along Fibonacci-sphere directions, complex128 assembly.
 
     A step = one sb_gmres_multi_device solve of all 256 right-hand sides (device-resident b and x):
     FP32-inner GMRES(50) with every step's 256 products as one tensor-core block product (BF16
@@ -525,7 +525,7 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
     reported per right-hand side; the error of the multi-RHS solutions against those FP64 solutions."""
     from sonium_b200 import _lib as L
 
-    level, k, r = 5, 16.0, a.rhs
+    level, k, r = a.level, 16.0, a.rhs
     nodes, tris = sb.icosphere(RADIUS, level, (1.0, 0.6, 0.4))
     n = tris.shape[0]
     mesh = sb.Mesh(nodes, tris, device=dev)
