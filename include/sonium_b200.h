@@ -247,6 +247,17 @@ SB_API int sb_gmres_mixed_device(const sb_operator* op, const sb_complex* b_dev,
 SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs,
                                     const sb_complex* amps, int64_t r, sb_complex* rhs_dev);
 
+/* ---- exterior field ----
+ * compute_scattered_field_checked (crates/sonium-bem/src/core/postprocess/pressure.rs:250-289 ->
+ * compute_scattered_field_with_incident :1388-1448, integrate_element_field :1566-1606 with the
+ * 7-point triangle rule, integrate_quad_point :1987-2042): the scattered pressure at m points
+ * (points: m x 3) from the constant surface pressure (n values, e.g. the solution of a rigid or
+ * admittance problem) and the surface normal velocity (n values, NULL = rigid). FP64. Add the
+ * incident field for the total field (compute_total_field_checked, :501). Points on the surface
+ * give a non-finite result (SB_ERR_NOT_FINITE), as the reference's checked form. */
+SB_API int sb_field_eval(const sb_mesh* mesh, const sb_physics* physics, const sb_complex* surface_pressure,
+                         const sb_complex* surface_velocity, const double* points, int64_t m, sb_complex* field);
+
 /* ---- tensor-core block product ----
  * The block product of LinearOperator::apply_block (crates/sonium-solvers/crates/
  * sonium-solvers-core/src/traits.rs:2949-3120 -> DenseMatrix::matmul_into, dense.rs:450-490) as

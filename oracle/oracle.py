@@ -80,6 +80,8 @@ def _declare(L):
     L.or_mie_rigid_coefficients.argtypes = [ct.c_double, ct.c_int, P]
     L.or_mie_rigid_field.argtypes = [ct.c_double, ct.c_double, ct.c_int, ct.c_double,
                                      ct.c_int64, P, P]
+    L.or_field_eval.argtypes = [P, P, ct.c_int64, P, P, ct.c_double, ct.c_double, ct.c_double, P,
+                                ct.c_int64, ct.c_int, P]
 
 
 def _p(a: np.ndarray):
@@ -236,6 +238,21 @@ def mie_field(k, radius, num_terms, r, theta):
     theta = np.ascontiguousarray(theta, np.float64)
     out = np.zeros(theta.shape[0], np.complex128)
     lib().or_mie_rigid_field(k, radius, num_terms, r, theta.shape[0], _p(theta), _p(out))
+    return out
+
+
+def field_eval(nodes, tris, pressure, ph: OrPhysics, points, velocity=None, threads: int = 0):
+    """Scattered field at exterior points (compute_scattered_field with explicit surface velocity,
+    crates/sonium-bem/src/core/postprocess/pressure.rs:1388-1448; 7-point rule per element)."""
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    tris = np.ascontiguousarray(tris, np.uint32)
+    p = np.ascontiguousarray(pressure, np.complex128)
+    v = None if velocity is None else np.ascontiguousarray(velocity, np.complex128)
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    out = np.zeros(pts.shape[0], np.complex128)
+    lib().or_field_eval(_p(nodes), _p(tris), tris.shape[0], _p(p), None if v is None else _p(v),
+                        ph.wave_number, ph.harmonic_factor, ph.pressure_factor, _p(pts), pts.shape[0],
+                        threads, _p(out))
     return out
 
 

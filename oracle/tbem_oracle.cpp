@@ -1099,3 +1099,50 @@ extern "C" void or_mie_rigid_field(double k, double radius, int nt, double r, in
         out[t] = O(tot);
     }
 }
+
+// ---------------------------------------------------------------------------------------------
+// Exterior field evaluation, constant Tri3 surface data
+// ---------------------------------------------------------------------------------------------
+// compute_scattered_field_with_incident (crates/sonium-bem/src/core/postprocess/pressure.rs:
+// 1388-1448) with explicit surface velocity (constant_cauchy_data, :1489-1491) ->
+// integrate_element_field (:1566-1606, Tri3: the 7-point rule of triangle_quadrature(3)) ->
+// integrate_quad_point (:1987-2042), geometry by quadrature_geometry (element.rs:420-464).
+// p_scat(x) = sum_e sum_q [ p_e dG/dn_y - v_e (i pressure_factor) G ] J w_q.
+extern "C" void or_field_eval(const double* nodes, const uint32_t* tris, int64_t n_tris,
+                              const or_c128* pressure, const or_c128* velocity, double k,
+                              double harmonic_factor, double pressure_factor, const double* points,
+                              int64_t m, int threads, or_c128* out) {
+    const std::vector<TriPoint> rule = triangle_quadrature(3);
+    const double wavruim = k * harmonic_factor;
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = 0; i < m; ++i) {
+        const double* x = points + 3 * i;
+        cd acc(0.0, 0.0);
+        for (int64_t e = 0; e < n_tris; ++e) {
+            Coords c;
+            for (int a = 0; a < 3; ++a)
+                for (int d = 0; d < 3; ++d) c.v[a][d] = nodes[3 * (int64_t)tris[3 * e + a] + d];
+            const cd p_surf = C(pressure[e]);
+            const cd v_surf = velocity ? C(velocity[e]) : cd(0.0, 0.0);
+            cd contrib_e(0.0, 0.0);
+            for (const TriPoint& q : rule) {
+                double pos[3], jac, nrm[3];
+                tri_parameters(c, q.xi, q.eta, pos, jac, nrm);
+                if (jac < 1e-15) continue;
+                const double rv[3] = {pos[0] - x[0], pos[1] - x[1], pos[2] - x[2]};
+                const double r = std::sqrt(rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2]);
+                if (r < 1e-15) continue;
+                const double vjacwe = jac * q.w;
+                const cd zgrfu = exp_i(wavruim * r) / (4.0 * kPi * r);
+                const cd zgikr = zgrfu * cd(-1.0 / r, wavruim);
+                const double drdn = (rv[0] * nrm[0] + rv[1] * nrm[1] + rv[2] * nrm[2]) / r;
+                cd contrib = p_surf * (zgikr * drdn) * vjacwe;
+                if (std::abs(v_surf) > 1e-15) contrib -= v_surf * cd(0.0, pressure_factor) * zgrfu * vjacwe;
+                contrib_e += contrib;
+            }
+            acc += contrib_e;
+        }
+        out[i] = O(acc);
+    }
+}

@@ -107,6 +107,11 @@ double or_sph_y(int n, double x);
 void or_mie_rigid_coefficients(double ka, int num_terms, or_c128* out);
 void or_mie_rigid_field(double k, double radius, int num_terms, double r, int64_t n_theta,
                         const double* theta, or_c128* out);
+/* Scattered field at m exterior points from constant Tri3 surface pressure / velocity
+ * (velocity may be NULL = rigid); compute_scattered_field, postprocess/pressure.rs:1388-1448. */
+void or_field_eval(const double* nodes, const uint32_t* tris, int64_t n_tris, const or_c128* pressure,
+                   const or_c128* velocity, double k, double harmonic_factor, double pressure_factor,
+                   const double* points, int64_t m, int threads, or_c128* out);
 
 #ifdef __cplusplus
 }

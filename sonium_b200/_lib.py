@@ -134,6 +134,7 @@ _SIGNATURES = {
     "sb_gmres_mixed": ([P, P, P, ct.POINTER(SbIrConfig), P, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_mixed_device": ([P, P, P, ct.c_int, ct.POINTER(SbIrConfig), ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_rhs_plane_wave_device": ([P, P, P, ct.c_int64, P], ct.c_int),
+    "sb_field_eval": ([P, ct.POINTER(SbPhysics), P, P, P, ct.c_int64, P], ct.c_int),
     "sb_operator_prepare_block_tensor": ([P], ct.c_int),
     "sb_operator_apply_block_tensor": ([P, P, P, ct.c_int64], ct.c_int),
     "sb_gmres_multi": ([P, P, ct.c_int64, ct.POINTER(SbIrConfig), P, P], ct.c_int),

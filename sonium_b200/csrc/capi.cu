@@ -605,6 +605,40 @@ SB_API int sb_rhs_plane_wave(const sb_mesh* mesh, const sb_physics* physics, sb_
     });
 }
 
+SB_API int sb_field_eval(const sb_mesh* mesh, const sb_physics* physics, const sb_complex* surface_pressure,
+                         const sb_complex* surface_velocity, const double* points, int64_t m, sb_complex* field) {
+    return guarded([&] {
+        SB_REQUIRE(mesh && mesh->m && physics && surface_pressure && m >= 0, SB_ERR_INVALID_ARGUMENT,
+                   "bad argument");
+        SB_REQUIRE(m == 0 || (points && field), SB_ERR_INVALID_ARGUMENT, "null points or output");
+        SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
+        const Mesh& me = *mesh->m;
+        SB_REQUIRE(all_finite(surface_pressure, me.n), SB_ERR_NOT_FINITE, "field_eval: non-finite surface pressure");
+        if (surface_velocity)
+            SB_REQUIRE(all_finite(surface_velocity, me.n), SB_ERR_NOT_FINITE,
+                       "field_eval: non-finite surface velocity");
+        for (int64_t q = 0; q < 3 * m; ++q)
+            SB_REQUIRE(std::isfinite(points[q]), SB_ERR_INVALID_ARGUMENT, "field_eval: non-finite point");
+        if (m == 0) return;
+        SB_CUDA(cudaSetDevice(me.device));
+        maybe_inject(SB_INJECT_LAUNCH);
+        DevBuf dp, dv, dx, dout;
+        dp.alloc(sizeof(double2) * me.n);
+        SB_CUDA(cudaMemcpy(dp.p, surface_pressure, sizeof(double2) * me.n, cudaMemcpyHostToDevice));
+        if (surface_velocity) {
+            dv.alloc(sizeof(double2) * me.n);
+            SB_CUDA(cudaMemcpy(dv.p, surface_velocity, sizeof(double2) * me.n, cudaMemcpyHostToDevice));
+        }
+        dx.alloc(sizeof(double) * 3 * m);
+        dout.alloc(sizeof(double2) * m);
+        SB_CUDA(cudaMemcpy(dx.p, points, sizeof(double) * 3 * m, cudaMemcpyHostToDevice));
+        field_eval(me, *physics, dp.as<double2>(), surface_velocity ? dv.as<double2>() : nullptr, dx.as<double>(), m,
+                   dout.as<double2>(), 0);
+        SB_CUDA(cudaMemcpy(field, dout.p, sizeof(double2) * m, cudaMemcpyDeviceToHost));
+        SB_REQUIRE(all_finite(field, m), SB_ERR_NOT_FINITE, "field_eval: non-finite result (point on the surface?)");
+    });
+}
+
 static void check_cfg(const sb_gmres_config* cfg) {
     SB_REQUIRE(cfg, SB_ERR_INVALID_ARGUMENT, "null config");
     SB_REQUIRE(cfg->max_iterations > 0 && cfg->restart > 0, SB_ERR_INVALID_ARGUMENT,

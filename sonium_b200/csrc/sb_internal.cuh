@@ -180,6 +180,11 @@ void op_residual64(const Operator& op, const double2* x, const double2* b, doubl
 
 int device_sm_count(int device);
 
+// Scattered field at m points from constant surface pressure / velocity (field.cu); device
+// pointers, velocity may be null (rigid surface).
+void field_eval(const Mesh& mesh, const sb_physics& ph, const double2* pressure, const double2* velocity,
+                const double* points, int64_t m, double2* out, cudaStream_t s);
+
 // Tensor-core block product (tensor.cu): BF16 hi/lo split planes of the operator's matrix, then
 // Y = A X for r complex64 vectors (vector c at x + c * ldx, result at y + c * ldy).
 void tensor_prepare(Operator& op);

@@ -389,6 +389,32 @@ def gmres_multi(operator: TbemOperator, B, config: IrConfig = IrConfig()):
     return X, [GmresSolution._from(None, stats[i]) for i in range(r)]
 
 
+def compute_scattered_field(mesh: Mesh, physics: PhysicsParams, surface_pressure, points,
+                            surface_velocity=None) -> np.ndarray:
+    """compute_scattered_field_checked (crates/sonium-bem/src/core/postprocess/pressure.rs:250):
+    scattered pressure at points (m x 3) from constant surface pressure / velocity."""
+    p = _c128(surface_pressure)
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    if p.shape != (mesh.num_elements,):
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "surface_pressure must have one value per element")
+    v = None if surface_velocity is None else _c128(np.broadcast_to(surface_velocity, p.shape))
+    out = np.zeros(pts.shape[0], np.complex128)
+    check(L.load().sb_field_eval(mesh.handle, ct.byref(physics._struct()), _p(p), None if v is None else _p(v),
+                                 _p(pts), pts.shape[0], _p(out)))
+    return out
+
+
+def compute_total_field(mesh: Mesh, physics: PhysicsParams, surface_pressure, points, direction=(0.0, 0.0, 1.0),
+                        amplitude: complex = 1.0, surface_velocity=None) -> np.ndarray:
+    """compute_total_field_checked (pressure.rs:501): scattered field plus the incident plane wave
+    A exp(i k d.x) (IncidentField::evaluate_pressure, incident.rs:216-245)."""
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    d = np.asarray(direction, np.float64)
+    d = d / np.linalg.norm(d)
+    inc = amplitude * np.exp(1j * physics.harmonic_factor * physics.wave_number * (pts @ d))
+    return compute_scattered_field(mesh, physics, surface_pressure, pts, surface_velocity) + inc
+
+
 def fibonacci_sphere_directions(n: int) -> np.ndarray:
     """Unit vectors on a Fibonacci sphere (the reference's fibonacci_sphere_directions,
     crates/sonium-bem/src/core/assembly/mlfmm.rs:8012-8024)."""
