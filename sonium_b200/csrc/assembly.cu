@@ -1172,7 +1172,7 @@ __device__ __forceinline__ int find_instance(const int64_t* __restrict__ pre, in
     return lo;
 }
 
-__global__ void __launch_bounds__(kFarTile) k_assemble_batch(const BatchAsmInst* __restrict__ inst, int ninst,
+__global__ void __launch_bounds__(kFarTile, 4) k_assemble_batch(const BatchAsmInst* __restrict__ inst, int ninst,
                                                              const int64_t* __restrict__ pre) {
     __shared__ NearWarpSmem nsm[kNearWarps];
     const int64_t* fpre = pre;
