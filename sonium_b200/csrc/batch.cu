@@ -66,6 +66,7 @@ namespace {
 
 constexpr int kChunk = 256;  // vector rows per CTA of the vector kernels
 constexpr int kBDotVecs = 8;
+constexpr int kDotSpan = 8;  // kChunk row slices per CTA of the Gram-Schmidt dots
 constexpr int kScal = 5;
 
 __device__ __forceinline__ int find_inst(const int64_t* __restrict__ pre, int ninst, int64_t unit) {
@@ -146,6 +147,16 @@ __global__ void __launch_bounds__(kChunk) k_bvnorm(const BInst* __restrict__ ins
     if (threadIdx.x == 0) I.pnorm[chunk] = v[0];
 }
 
+// gate[g] = 1 when any instance of group g (kTensorRhsTile instances) still runs its Arnoldi
+// cycle: groups that are all done skip the step's block product.
+__global__ void __launch_bounds__(kTensorRhsTile) k_bany_active(const BInst* __restrict__ inst, int ninst,
+                                                                int* __restrict__ gate) {
+    const int b = blockIdx.x * kTensorRhsTile + threadIdx.x;
+    const int on = (b < ninst && inst[b].st->active) ? 1 : 0;
+    const int any = __syncthreads_or(on);
+    if (threadIdx.x == 0) gate[blockIdx.x] = any;
+}
+
 // rq = rb - w (w = A d from a block product), per-chunk squared norms of rq.
 __global__ void __launch_bounds__(kChunk) k_bresid_w(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
                                                      int ninst, int gk) {
@@ -177,8 +188,8 @@ __global__ void k_bsum_partials(const BInst* __restrict__ inst, const int64_t* _
     if (threadIdx.x == 0) I.nrm[slot] = s;
 }
 
-// Gram-Schmidt dots over the flattened chunks: part[chunk * (k + 1) + i] = V_i^H w (i < k),
-// |w|^2 at i = k.
+// Gram-Schmidt dots over the flattened chunks of kDotSpan * kChunk rows:
+// part[chunk * (k + 1) + i] = V_i^H w (i < k), |w|^2 at i = k.
 __global__ void __launch_bounds__(kChunk) k_bdots(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
                                                   int ninst, int k, int gk) {
     __shared__ double red[(kChunk / 32) * 2 * kBDotVecs];
@@ -186,22 +197,24 @@ __global__ void __launch_bounds__(kChunk) k_bdots(const BInst* __restrict__ inst
     const BInst& I = inst[b];
     if (!open_gate(I, gk)) return;
     const int64_t chunk = blockIdx.x - pre[b];
-    const int64_t r = chunk * kChunk + threadIdx.x;
     const int i0 = blockIdx.y * kBDotVecs;
     double acc[2 * kBDotVecs];
 #pragma unroll
     for (int t = 0; t < 2 * kBDotVecs; ++t) acc[t] = 0.0;
-    if (r < I.n) {
+    // kDotSpan row slices of kChunk per CTA: one block reduction per kDotSpan * kChunk rows
+    for (int sl = 0; sl < kDotSpan; ++sl) {
+        const int64_t r = (chunk * kDotSpan + sl) * kChunk + threadIdx.x;
+        if (r >= I.n) break;
         const float2 wv = I.w[r];
 #pragma unroll
         for (int t = 0; t < kBDotVecs; ++t) {
             const int i = i0 + t;
             if (i < k) {
                 const float2 v = I.V[i * I.vs + r];
-                acc[2 * t] = (double)v.x * wv.x + (double)v.y * wv.y;
-                acc[2 * t + 1] = (double)v.x * wv.y - (double)v.y * wv.x;
+                acc[2 * t] = fma((double)v.x, wv.x, fma((double)v.y, wv.y, acc[2 * t]));
+                acc[2 * t + 1] = fma((double)v.x, wv.y, fma(-(double)v.y, wv.x, acc[2 * t + 1]));
             } else if (i == k) {
-                acc[2 * t] = (double)wv.x * wv.x + (double)wv.y * wv.y;
+                acc[2 * t] = fma((double)wv.x, wv.x, fma((double)wv.y, wv.y, acc[2 * t]));
             }
         }
     }
@@ -435,9 +448,10 @@ struct Batch {
     std::vector<BatchAsmInst> asm_h;
     std::vector<double2*> rhs;  // per-instance right-hand side (pool_rhs)
     std::vector<BInst> h;
-    std::vector<int64_t> pre4, pre256;
-    DevBuf asm_d, inst_d, pre4_d, pre256_d, pre_asm;
+    std::vector<int64_t> pre4, pre256, predot;
+    DevBuf asm_d, inst_d, pre4_d, pre256_d, predot_d, pre_asm;
     DevBuf pool_mat, pool_rhs, pool_f32, pool_f64, pool_small, pool_state;
+    DevBuf gate;  // per group of kTensorRhsTile instances: any still in the Arnoldi cycle
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -561,6 +575,7 @@ static void batch_workspace(Batch& B, int64_t m) {
     }
     B.pre4.assign(ni + 1, 0);
     B.pre256.assign(ni + 1, 0);
+    B.predot.assign(ni + 1, 0);
     for (int b = 0; b < ni; ++b) {
         const int64_t n = B.nvec[b], ldv = (n + 1) / 2 * 2;
         const int64_t chunks = cdiv64(n, kChunk);
@@ -597,10 +612,13 @@ static void batch_workspace(Batch& B, int64_t m) {
         I.brk = dv.brk + b;
         B.pre4[b + 1] = B.pre4[b] + cdiv64(n, kGemvRows);
         B.pre256[b + 1] = B.pre256[b] + chunks;
+        B.predot[b + 1] = B.predot[b] + cdiv64(n, (int64_t)kChunk * kDotSpan);
     }
     B.inst_d.alloc(sizeof(BInst) * ni);
     B.pre4_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre256_d.alloc(sizeof(int64_t) * (ni + 1));
+    B.predot_d.alloc(sizeof(int64_t) * (ni + 1));
+    SB_CUDA(cudaMemcpy(B.predot_d.p, B.predot.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
     SB_CUDA(cudaMemcpy(B.inst_d.p, B.h.data(), sizeof(BInst) * ni, cudaMemcpyHostToDevice));
     SB_CUDA(cudaMemcpy(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
     SB_CUDA(cudaMemcpy(B.pre256_d.p, B.pre256.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
@@ -619,23 +637,29 @@ static void batch_step(Batch& B, int j) {
     const unsigned gi = static_cast<unsigned>(cdiv64(ni, 64));
     capture_step(j);
     if (B.shared) {
-        // all right-hand sides at once: W = A V_j on the tensor cores
-        tensor_block_product(*B.shared, B.v_all + (int64_t)j * ni * B.ld_all, B.ld_all, ni, B.w_all, B.ld_all, s);
+        // all right-hand sides at once: W = A V_j on the tensor cores, skipping groups whose
+        // instances have all left the cycle
+        const unsigned groups = static_cast<unsigned>(cdiv64(ni, kTensorRhsTile));
+        k_bany_active<<<groups, kTensorRhsTile, 0, s>>>(I, ni, B.gate.as<int>());
+        count_launch();
+        tensor_block_product(*B.shared, B.v_all + (int64_t)j * ni * B.ld_all, B.ld_all, ni, B.w_all, B.ld_all, s,
+                             B.gate.as<int>());
     } else {
         ProfScope prof(SB_PROF_GEMV32, s);
         k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 0, j, G_ACTIVE);
         count_launch();
     }
     ProfScope prof(SB_PROF_ARNOLDI, s);
-    const dim3 gd(g256, static_cast<unsigned>(cdiv64(k + 1, kBDotVecs)));
+    const int64_t* pdot = B.predot_d.as<int64_t>();
+    const dim3 gd(static_cast<unsigned>(B.predot.back()), static_cast<unsigned>(cdiv64(k + 1, kBDotVecs)));
     const dim3 gr(static_cast<unsigned>(k + 1), static_cast<unsigned>(ni));
-    k_bdots<<<gd, kChunk, 0, s>>>(I, p256, ni, k, G_ACTIVE);
-    k_breduce<<<gr, 32, 0, s>>>(I, p256, k, 0, G_ACTIVE);
+    k_bdots<<<gd, kChunk, 0, s>>>(I, pdot, ni, k, G_ACTIVE);
+    k_breduce<<<gr, 32, 0, s>>>(I, pdot, k, 0, G_ACTIVE);
     k_bproject<<<g256, kChunk, 0, s>>>(I, p256, ni, k, 0, G_ACTIVE);
     k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 0, G_ACTIVE);
     k_bafter_first<<<gi, 64, 0, s>>>(I, ni, j);
-    k_bdots<<<gd, kChunk, 0, s>>>(I, p256, ni, k, G_REORTH);
-    k_breduce<<<gr, 32, 0, s>>>(I, p256, k, 1, G_REORTH);
+    k_bdots<<<gd, kChunk, 0, s>>>(I, pdot, ni, k, G_REORTH);
+    k_breduce<<<gr, 32, 0, s>>>(I, pdot, k, 1, G_REORTH);
     k_bproject<<<g256, kChunk, 0, s>>>(I, p256, ni, k, 1, G_REORTH);
     k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 1, G_REORTH);
     k_bgivens<<<gi, 64, 0, s>>>(I, ni, j);
@@ -911,6 +935,7 @@ static Batch& multi_batch(Operator& op, int r) {
     SB_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
     SB_REQUIRE(cublasCreate(&B->blas) == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasCreate failed");
     SB_REQUIRE(cublasSetStream(B->blas, B->stream) == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasSetStream failed");
+    B->gate.alloc(sizeof(int) * cdiv64(r, kTensorRhsTile));
     B->pool_rhs.alloc(sizeof(double2) * r * B->ld_all);
     SB_CUDA(cudaMemset(B->pool_rhs.p, 0, sizeof(double2) * r * B->ld_all));
     B->b_all = B->pool_rhs.as<double2>();

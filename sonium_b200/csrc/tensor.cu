@@ -40,7 +40,7 @@ namespace sb {
 namespace {
 
 constexpr int kTileM = 128;       // Ahat rows per CTA (64 complex rows)
-constexpr int kTileRhs = 128;     // right-hand sides per CTA (256 Xhat rows)
+constexpr int kTileRhs = kTensorRhsTile;  // right-hand sides per CTA (256 Xhat rows)
 constexpr int kTileK = 64;        // K per stage: one 128-byte swizzle row of BF16
 constexpr int kStages = 2;
 constexpr uint32_t kABytes = kTileM * kTileK * 2;           // 16 KB per term
@@ -59,8 +59,12 @@ constexpr int kErrTimeoutEpilogue = 4;
 __global__ void __launch_bounds__(128, 1)
     k_block_bf16x3(const __grid_constant__ CUtensorMap tm_a_hi, const __grid_constant__ CUtensorMap tm_a_lo,
                    const __grid_constant__ CUtensorMap tm_x_hi, const __grid_constant__ CUtensorMap tm_x_lo,
-                   int ldk, int64_t n, int r, float* __restrict__ y, int64_t ldy, int* __restrict__ status) {
+                   int ldk, int64_t n, int r, float* __restrict__ y, int64_t ldy, int* __restrict__ status,
+                   const int* __restrict__ block_gate) {
 #if defined(__CUDA_ARCH__)
+    // A group of right-hand sides with nothing left to compute: the whole CTA returns before it
+    // allocates or initialises anything.
+    if (block_gate && block_gate[blockIdx.x] == 0) return;
     using namespace umma;
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], acc_bar;
@@ -333,7 +337,7 @@ void tensor_reserve(const Operator& op, int r) {
 
 // Y (r vectors, vector c at y + c * ldy, complex64) = A X (vector c at x + c * ldx).
 void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int r, float2* y, int64_t ldy,
-                          cudaStream_t s) {
+                          cudaStream_t s, const int* block_gate) {
     TensorWork* w = static_cast<TensorWork*>(op.tensor);
     SB_REQUIRE(w, SB_ERR_INVALID_ARGUMENT, "tensor-core block product: call sb_operator_prepare_block_tensor first");
     SB_REQUIRE(r >= 1, SB_ERR_INVALID_ARGUMENT, "tensor-core block product: r must be positive");
@@ -351,7 +355,7 @@ void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int 
     const dim3 grid(static_cast<unsigned>(rblocks), static_cast<unsigned>(w->rows / kTileM));
     k_block_bf16x3<<<grid, 128, kSmemBytes, s>>>(w->tm_a_hi, w->tm_a_lo, w->tm_x_hi, w->tm_x_lo,
                                                   static_cast<int>(w->ldk), w->n, r, reinterpret_cast<float*>(y), ldy,
-                                                  w->status.as<int>());
+                                                  w->status.as<int>(), block_gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }
