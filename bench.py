@@ -14,6 +14,14 @@ solve: re-assembly of the dense system on the device, the incident right-hand si
   * `cpu_baseline` / `--impl reference` -- the CPU restatement of the reference path (oracle),
                 timed on a bounded sample (assembly rows + a CPU matvec) and scaled to one solve.
 
+  * `sweep`  -- the batched frequency sweep: 64 instances (ka 1 -> 32 on the (1, 0.6, 0.4) ellipsoid,
+                levels 2-5) assembled in one launch and solved by the batched mixed GMRES,
+                against the same instances solved one after another in plain FP64.
+  * `multi_rhs` -- 256 plane-wave right-hand sides of one operator (ellipsoid level 5, k = 16)
+                solved together with tensor-core block products, against plain FP64 GMRES per
+                right-hand side; carries the tensor kernel's roofline.
+  Opt-in legs: `--precision-form` (N = 81920, k = 40, ~165 GB), `--sweep-only`, `--multi-rhs`.
+
 With torchrun (N > 1 ranks) every rank solves its own copy of the workload (replicas: the path
 has no exchange step); value = all ranks' solves / max-over-ranks time.
 """
@@ -58,6 +66,7 @@ def parse():
     ap.add_argument("--multi-rhs", action="store_true",
                     help="run only the 256-right-hand-side tensor-core leg and print its JSON")
     ap.add_argument("--rhs", type=int, default=256, help="right-hand sides of the multi-RHS leg")
+    ap.add_argument("--no-multi", action="store_true", help="skip the multi-RHS leg in the default run")
     ap.add_argument("--precision-form", action="store_true",
                     help="run only the N = 81920, k = 40 precision-form leg (~165 GB) and print its JSON")
     ap.add_argument("--single", action="store_true",
@@ -360,6 +369,12 @@ def main():
 
     # ---- batched frequency sweep ----
     sweep = None if a.no_sweep else sweep_leg(sb, a, dist, dev, rt)
+    multi = None
+    if not a.no_multi:
+        lvl = a.level
+        a.level = LEVEL
+        multi = multi_rhs_leg(sb, a, dist, dev, rt)
+        a.level = lvl
 
     # ---- roofline of the dominant kernel of the headline step ----
     pk, pk_kind = peaks()
@@ -419,6 +434,7 @@ def main():
         "clocks": clk,
         "e2e": e2e,
         "sweep": sweep,
+        "multi_rhs": multi,
         "cpu_baseline": None if cpu is None else {kk: cpu[kk] for kk in ("value", "unit", "cores", "kind", "sample")},
     }
     if dist.rank == 0:

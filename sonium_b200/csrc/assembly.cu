@@ -695,11 +695,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             const float nxny = nxx * nyx + nxy * nyy + nxz * nyz;
             const float fny = fx * nyx + fy * nyy + fz * nyz;       // d_c . n_y
             const float fnx = -(fx * nxx + fy * nxy + fz * nxz);    // -d_c . n_x
-            // Complex channel sums as float2 pairs: the paired FP32 instructions of sm_100
-            // (__ffma2_rn / __fmul2_rn / __fadd2_rn, one issue slot for both halves) carry the
-            // complex arithmetic; each lane rounds exactly as the scalar fmaf / mul / add would.
-            float2 ag = make_float2(0.f, 0.f), ah = ag, at = ag, ae = ag;
-            const float2 csn = make_float2(cc, sc), csr = make_float2(-sc, cc);
+            float ag_r = 0.f, ag_i = 0.f, ah_r = 0.f, ah_i = 0.f, at_r = 0.f, at_i = 0.f, ae_r = 0.f, ae_i = 0.f;
 #pragma unroll
             for (int q = 0; q < kFarPoints; ++q) {
                 const float num = fmaf(2.f, fx * px[q] + fy * py[q] + fz * pz[q], pd[q]);
@@ -717,29 +713,26 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                     sincos_f32(t, &st, &ct);
                 }
                 const float gs = pw[q] * rinv;
-                // g = exp(i k r_c) exp(i t) w / (4 pi r): (cc ct - sc st, sc ct + cc st) gs
-                const float2 g = __fmul2_rn(__ffma2_rn(csn, make_float2(ct, ct), __fmul2_rn(csr, make_float2(st, st))),
-                                            make_float2(gs, gs));
+                const float g_r = (cc * ct - sc * st) * gs, g_i = (sc * ct + cc * st) * gs;
                 // r_hat . n_y and -r_hat . n_x from per-pair and per-point dot products
                 const float rny = (fny + pn[q]) * rinv;
                 const float rnx = (fnx - (px[q] * nxx + py[q] * nxy + pz[q] * nxz)) * rinv;
-                // b = g (-1/r + i k) = (-(g_r / r + g_i k), g_r k - g_i / r)
-                const float2 bvec = __ffma2_rn(make_float2(g.x, g.x), make_float2(-rinv, kf),
-                                               __fmul2_rn(make_float2(g.y, g.y), make_float2(-kf, -rinv)));
-                ag = __fadd2_rn(ag, g);
-                ah = __ffma2_rn(bvec, make_float2(rny, rny), ah);
-                at = __ffma2_rn(bvec, make_float2(rnx, rnx), at);
+                const float b_r = -fmaf(g_r, rinv, g_i * kf);
+                const float b_i = fmaf(g_r, kf, -g_i * rinv);
+                ag_r += g_r;
+                ag_i += g_i;
+                ah_r = fmaf(b_r, rny, ah_r);
+                ah_i = fmaf(b_i, rny, ah_i);
+                at_r = fmaf(b_r, rnx, at_r);
+                at_i = fmaf(b_i, rnx, at_i);
                 // E factor: ((3/r^2 - k^2) rq + nx.ny / r^2, -(k / r) (3 rq + nx.ny))
                 const float rqq = rny * rnx;
                 const float s3 = fmaf(3.f, rqq, nxny);
                 const float f_r = fmaf(rinv * rinv, s3, -k2f * rqq);
                 const float f_i = -kf * rinv * s3;
-                // ae += g f
-                ae = __ffma2_rn(make_float2(g.x, g.x), make_float2(f_r, f_i),
-                                __ffma2_rn(make_float2(g.y, g.y), make_float2(-f_i, f_r), ae));
+                ae_r = fmaf(g_r, f_r, fmaf(-g_i, f_i, ae_r));
+                ae_i = fmaf(g_r, f_i, fmaf(g_i, f_r, ae_i));
             }
-            const float ag_r = ag.x, ag_i = ag.y, ah_r = ah.x, ah_i = ah.y;
-            const float at_r = at.x, at_i = at.y, ae_r = ae.x, ae_i = ae.y;
             const float cgr = scf[0][tid], cgi = scf[1][tid], chr = scf[2][tid], chi = scf[3][tid];
             const float ctr = scf[4][tid], cti = scf[5][tid], cer = scf[6][tid], cei = scf[7][tid];
             const float vr = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
