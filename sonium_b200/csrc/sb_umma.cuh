@@ -28,6 +28,16 @@ __host__ __device__ constexpr uint64_t smem_desc_k_sw128(uint32_t smem_addr) {
            | ((uint64_t)2u << 61);                      // layout type SWIZZLE_128B, [61,64)
 }
 
+// The same for a TMA SWIZZLE_64B box: rows of 32 bf16 (64 B), 8-row groups 512 B apart; layout
+// type 4 = SWIZZLE_64B.
+__host__ __device__ constexpr uint64_t smem_desc_k_sw64(uint32_t smem_addr) {
+    return (uint64_t)((smem_addr >> 4) & 0x3FFFu)      // start address, bits [0,14)
+           | ((uint64_t)1u << 16)                       // leading byte offset (unused with swizzle), [16,30)
+           | ((uint64_t)(512u >> 4) << 32)              // stride byte offset: 8-row group pitch, [32,46)
+           | ((uint64_t)1u << 46)                       // descriptor version, [46,48)
+           | ((uint64_t)4u << 61);                      // layout type SWIZZLE_64B, [61,64)
+}
+
 // Instruction descriptor of kind::f16 with BF16 A and B, FP32 accumulator, both K-major, M x N.
 __host__ __device__ constexpr uint32_t instr_desc_bf16_f32(int m, int n) {
     return (1u << 4)                    // D format F32, bits [4,6)

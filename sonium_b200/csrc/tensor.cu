@@ -18,8 +18,8 @@
 //
 // Kernel structure: one CTA per (128 Ahat rows, 128 right-hand sides); 4 warps. Warp 0 allocates
 // 256 TMEM columns (the 128 x 256 FP32 accumulator), lane 0 of warp 0 issues the TMA loads of a
-// two-stage ring (per stage: Ahat hi/lo 128 x 64 and Xhat hi/lo 256 x 64 BF16 tiles, 128-byte
-// swizzle, 96 KB), lane 0 of warp 1 issues 12 MMAs (128 x 256 x 16) per stage and commits them to
+// four-stage ring (per stage: Ahat hi/lo 128 x 32 and Xhat hi/lo 256 x 32 BF16 tiles, 64-byte
+// swizzle, 48 KB), lane 0 of warp 1 issues 6 MMAs (128 x 256 x 16) per stage and commits them to
 // the stage's "empty" barrier; after the last stage all four warps read the accumulator
 // (tcgen05.ld) and write Y. Consecutive CTAs take the right-hand-side blocks of one row tile, so
 // the second read of an Ahat tile comes from L2. All waits are bounded; a timeout records an
@@ -41,11 +41,11 @@ namespace {
 
 constexpr int kTileM = 128;       // Ahat rows per CTA (64 complex rows)
 constexpr int kTileRhs = kTensorRhsTile;  // right-hand sides per CTA (256 Xhat rows)
-constexpr int kTileK = 64;        // K per stage: one 128-byte swizzle row of BF16
-constexpr int kStages = 2;
-constexpr uint32_t kABytes = kTileM * kTileK * 2;           // 16 KB per term
-constexpr uint32_t kXBytes = 2 * kTileRhs * kTileK * 2;     // 32 KB per term
-constexpr uint32_t kStageBytes = 2 * kABytes + 2 * kXBytes; // 96 KB
+constexpr int kTileK = 32;        // K per stage: one 64-byte swizzle row of BF16
+constexpr int kStages = 4;        // stages in flight: three stage times to hide a TMA load
+constexpr uint32_t kABytes = kTileM * kTileK * 2;           // 8 KB per term
+constexpr uint32_t kXBytes = 2 * kTileRhs * kTileK * 2;     // 16 KB per term
+constexpr uint32_t kStageBytes = 2 * kABytes + 2 * kXBytes; // 48 KB
 constexpr uint32_t kSmemBytes = kStages * kStageBytes + 1024;
 constexpr uint32_t kTmemCols = 2 * kTileRhs;                // 256 FP32 columns
 
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(128, 1)
         // TMA producer
         int issued = 0;
         for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb & 1, use = kb >> 1;
+            const int s = kb % kStages, use = kb / kStages;
             if (kb >= kStages && !mbar_wait(smem_u32(&empty_bar[s]), (use - 1) & 1)) {
                 err |= kErrTimeoutProducer;
                 abort_flag = 1;
@@ -119,13 +119,13 @@ __global__ void __launch_bounds__(128, 1)
         if (abort_flag) {
             __threadfence_block();
             for (int kb = consumed; kb < issued; ++kb)
-                if (!mbar_wait(smem_u32(&full_bar[kb & 1]), (kb >> 1) & 1)) err |= kErrTimeoutProducer;
+                if (!mbar_wait(smem_u32(&full_bar[kb % kStages]), (kb / kStages) & 1)) err |= kErrTimeoutProducer;
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
         const uint32_t idesc = instr_desc_bf16_f32(kTileM, 2 * kTileRhs);
         for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb & 1, use = kb >> 1;
+            const int s = kb % kStages, use = kb / kStages;
             if (abort_flag || !mbar_wait(smem_u32(&full_bar[s]), use & 1)) {
                 if (!abort_flag) err |= kErrTimeoutMma;
                 abort_flag = 1;
@@ -136,10 +136,10 @@ __global__ void __launch_bounds__(128, 1)
             const uint32_t st = base + s * kStageBytes;
 #pragma unroll
             for (int kk = 0; kk < kTileK / 16; ++kk) {
-                const uint64_t a_hi = smem_desc_k_sw128(st + kk * 32);
-                const uint64_t a_lo = smem_desc_k_sw128(st + kABytes + kk * 32);
-                const uint64_t x_hi = smem_desc_k_sw128(st + 2 * kABytes + kk * 32);
-                const uint64_t x_lo = smem_desc_k_sw128(st + 2 * kABytes + kXBytes + kk * 32);
+                const uint64_t a_hi = smem_desc_k_sw64(st + kk * 32);
+                const uint64_t a_lo = smem_desc_k_sw64(st + kABytes + kk * 32);
+                const uint64_t x_hi = smem_desc_k_sw64(st + 2 * kABytes + kk * 32);
+                const uint64_t x_lo = smem_desc_k_sw64(st + 2 * kABytes + kXBytes + kk * 32);
                 mma_bf16(tacc, a_hi, x_hi, idesc, (kb | kk) != 0 ? 1u : 0u);
                 mma_bf16(tacc, a_hi, x_lo, idesc, 1u);
                 mma_bf16(tacc, a_lo, x_hi, idesc, 1u);
@@ -243,7 +243,7 @@ EncodeTiled encode_fn() {
     return fn;
 }
 
-// 2-D BF16 tensor map over rows x ldk (row pitch ldk elements), box of box_rows x 64, 128B swizzle.
+// 2-D BF16 tensor map over rows x ldk (row pitch ldk elements), box of box_rows x 32, 64B swizzle.
 CUtensorMap make_map(void* base, int64_t rows, int64_t ldk, int box_rows) {
     CUtensorMap m;
     std::memset(&m, 0, sizeof(m));
@@ -252,7 +252,7 @@ CUtensorMap make_map(void* base, int64_t rows, int64_t ldk, int box_rows) {
     const cuuint32_t box[2] = {(cuuint32_t)kTileK, (cuuint32_t)box_rows};
     const cuuint32_t elem[2] = {1, 1};
     const CUresult rc = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, elem,
-                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     SB_REQUIRE(rc == CUDA_SUCCESS, SB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     return m;

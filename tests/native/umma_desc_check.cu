@@ -45,6 +45,22 @@ int main() {
             bad = 1;
         }
     }
+    for (uint32_t addr : {0x0u, 0x200u, 0x12340u, 0x3FFF0u}) {
+        cute::UMMA::SmemDescriptor d;
+        d.start_address_ = static_cast<uint16_t>(addr >> 4);
+        d.leading_byte_offset_ = 1;
+        d.stride_byte_offset_ = 512 >> 4;
+        d.version_ = 1;
+        d.base_offset_ = 0;
+        d.lbo_mode_ = 0;
+        d.layout_type_ = uint8_t(cute::UMMA::LayoutType::SWIZZLE_64B);
+        const uint64_t ours = sb::umma::smem_desc_k_sw64(addr);
+        if (ours != d.desc_) {
+            std::printf("smem64 %x: ours %016llx cutlass %016llx\n", addr, (unsigned long long)ours,
+                        (unsigned long long)d.desc_);
+            bad = 1;
+        }
+    }
     std::printf(bad ? "MISMATCH\n" : "OK\n");
     return bad;
 }
