@@ -191,7 +191,7 @@ void tensor_prepare(Operator& op);
 void tensor_release(Operator& op);
 bool tensor_ready(const Operator& op);
 // block_gate (optional, one int per group of kTensorRhsTile vectors): a group whose entry is 0
-// is skipped and its results are left as they were.
+// is skipped; its results are unspecified (zero or left as they were).
 constexpr int kTensorRhsTile = 128;
 void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int r, float2* y, int64_t ldy,
                           cudaStream_t s, const int* block_gate = nullptr);

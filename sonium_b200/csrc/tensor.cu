@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(128, 1)
     k_block_bf16x3(const __grid_constant__ CUtensorMap tm_a_hi, const __grid_constant__ CUtensorMap tm_a_lo,
                    const __grid_constant__ CUtensorMap tm_x_hi, const __grid_constant__ CUtensorMap tm_x_lo,
                    int ldk, int64_t n, int r, float* __restrict__ y, int64_t ldy, int* __restrict__ status,
-                   const int* __restrict__ block_gate) {
+                   const int* __restrict__ block_gate, int ksplit) {
 #if defined(__CUDA_ARCH__)
     // A group of right-hand sides with nothing left to compute: the whole CTA returns before it
     // allocates or initialises anything.
@@ -93,7 +93,12 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tacc = tmem_base;
-    const int nkb = ldk / kTileK;
+    // K blocks of this CTA: split blockIdx.z of ksplit; partial sums are added into y (zeroed by the
+    // host), two of them exactly (fl(a + b) either order), so the result does not depend on timing.
+    const int nkb_all = ldk / kTileK;
+    const int per = (nkb_all + ksplit - 1) / ksplit;
+    const int kb0 = blockIdx.z * per;
+    const int nkb = (nkb_all - kb0) < per ? (nkb_all - kb0) : per;
     int err = 0;
     if (warp == 0 && lane == 0) {
         // TMA producer
@@ -109,10 +114,11 @@ __global__ void __launch_bounds__(128, 1)
             const uint32_t st = base + s * kStageBytes;
             const uint32_t fb = smem_u32(&full_bar[s]);
             mbar_expect_tx(fb, kStageBytes);
-            tma_load_2d(st, &tm_a_hi, fb, kb * kTileK, mtile * kTileM);
-            tma_load_2d(st + kABytes, &tm_a_lo, fb, kb * kTileK, mtile * kTileM);
-            tma_load_2d(st + 2 * kABytes, &tm_x_hi, fb, kb * kTileK, rblock * 2 * kTileRhs);
-            tma_load_2d(st + 2 * kABytes + kXBytes, &tm_x_lo, fb, kb * kTileK, rblock * 2 * kTileRhs);
+            const int kx = (kb0 + kb) * kTileK;
+            tma_load_2d(st, &tm_a_hi, fb, kx, mtile * kTileM);
+            tma_load_2d(st + kABytes, &tm_a_lo, fb, kx, mtile * kTileM);
+            tma_load_2d(st + 2 * kABytes, &tm_x_hi, fb, kx, rblock * 2 * kTileRhs);
+            tma_load_2d(st + 2 * kABytes + kXBytes, &tm_x_lo, fb, kx, rblock * 2 * kTileRhs);
             ++issued;
         }
         // Loads still in flight land before the CTA may exit.
@@ -171,7 +177,11 @@ __global__ void __launch_bounds__(128, 1)
                 const float v = __shfl_xor_sync(0xffffffffu, b[c], 1);
                 const float out = parity ? a[c] + v : a[c] - v;
                 const int rhs = rblock * kTileRhs + g * 32 + c;
-                if (i < n && rhs < r) y[((int64_t)rhs * ldy + i) * 2 + parity] = out;
+                if (i < n && rhs < r) {
+                    float* dst = y + ((int64_t)rhs * ldy + i) * 2 + parity;
+                    if (ksplit > 1) atomicAdd(dst, out);
+                    else *dst = out;
+                }
             }
         }
     }
@@ -351,11 +361,19 @@ void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int 
         count_launch();
     }
     SB_CUDA(cudaGetLastError());
+    // Two K halves per tile when one pass over the tiles would leave the last wave of SMs mostly
+    // idle (fewer than 6 waves of CTAs); every half keeps at least one K block.
+    const int64_t ctas = (int64_t)rblocks * (w->rows / kTileM);
+    const int nkb = static_cast<int>(w->ldk / kTileK);
+    const int ksplit = (ctas < 6 * (int64_t)device_sm_count(op.device) && nkb >= 2) ? 2 : 1;
+    if (ksplit > 1)
+        SB_CUDA(cudaMemset2DAsync(y, sizeof(float2) * ldy, 0, sizeof(float2) * w->n, r, s));
     ProfScope prof(SB_PROF_TENSOR, s);
-    const dim3 grid(static_cast<unsigned>(rblocks), static_cast<unsigned>(w->rows / kTileM));
+    const dim3 grid(static_cast<unsigned>(rblocks), static_cast<unsigned>(w->rows / kTileM),
+                    static_cast<unsigned>(ksplit));
     k_block_bf16x3<<<grid, 128, kSmemBytes, s>>>(w->tm_a_hi, w->tm_a_lo, w->tm_x_hi, w->tm_x_lo,
                                                   static_cast<int>(w->ldk), w->n, r, reinterpret_cast<float*>(y), ldy,
-                                                  w->status.as<int>(), block_gate);
+                                                  w->status.as<int>(), block_gate, ksplit);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }
