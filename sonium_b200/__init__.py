@@ -11,13 +11,14 @@ from .tbem import (GmresConfig, GmresSolution, IrConfig, JacobiPreconditioner, L
                    compute_scattered_field, compute_total_field, device_count,
                    fibonacci_sphere_directions, gmres, gmres_mixed, gmres_multi, icosphere,
                    inject_failure, rhs_plane_wave)
-from .sweep import FrequencySweepResult, SweepBatch, frequency_sweep_batched
+from .sweep import (FrequencySweepConfig, FrequencySweepResult, SweepBatch, frequency_sweep,
+                    frequency_sweep_batched)
 
 __all__ = [
     "GmresConfig", "GmresSolution", "IrConfig", "JacobiPreconditioner", "LinearOperator", "Mesh",
     "PhysicsParams", "TbemOperator", "build_tbem_system", "build_tbem_system_with_beta", "device_count",
     "gmres", "gmres_mixed", "icosphere", "inject_failure", "rhs_plane_wave", "SoniumError",
-    "FrequencySweepResult", "SweepBatch", "frequency_sweep_batched", "gmres_multi", "fibonacci_sphere_directions",
+    "FrequencySweepConfig", "FrequencySweepResult", "SweepBatch", "frequency_sweep", "frequency_sweep_batched", "gmres_multi", "fibonacci_sphere_directions",
     "compute_scattered_field", "compute_total_field",
     "SB_BC_PRESSURE", "SB_BC_VELOCITY", "SB_INJECT_ALLOC", "SB_INJECT_LAUNCH", "SB_INJECT_NONE",
     "SB_OP_C", "SB_OP_N", "SB_OP_T", "SB_PRECISION_FP32", "SB_PRECISION_FP64", "SB_PRECISION_FP64_FP32",

@@ -17,7 +17,8 @@ import numpy as np
 
 from . import _lib as L
 from ._lib import SoniumError, check
-from .tbem import GmresSolution, IrConfig, Mesh, PhysicsParams, _c128, _p
+from .tbem import (GmresConfig, GmresSolution, IrConfig, Mesh, PhysicsParams, _c128, _p,
+                   build_tbem_system_with_beta, gmres, gmres_mixed, rhs_plane_wave)
 
 
 class SweepBatch:
@@ -117,6 +118,8 @@ class FrequencySweepResult:
     assembly_ms: float
     solve_ms: float
     stats: list = field(default_factory=list)
+    assembly_times: list = field(default_factory=list)  # seconds per frequency (sequential sweep)
+    solve_times: list = field(default_factory=list)
 
     def total_iterations(self) -> int:
         return int(sum(self.iteration_counts))
@@ -144,6 +147,103 @@ def frequency_sweep_batched(meshes, physics, betas, direction=(0.0, 0.0, 1.0),
         solutions=sols, frequencies=[p.frequency for p in physics],
         iteration_counts=[s.iterations for s in stats], converged=[s.converged for s in stats],
         exact_relative_residuals=[s.residual for s in stats], assembly_ms=a_ms, solve_ms=s_ms, stats=stats)
+
+
+@dataclass
+class FrequencySweepConfig:
+    """FrequencySweepConfig (frequency_sweep.rs:43-170): frequencies (Hz, strictly increasing),
+    GMRES tolerance / restarts / restart length, warm start from the previous frequency's solution
+    (recycle_solution), Burton-Miller beta scale."""
+
+    frequencies: list = field(default_factory=list)
+    tolerance: float = 1e-6
+    max_iterations: int = 200
+    recycle_solution: bool = True
+    gmres_restart: int = 30
+    beta_scale: float = 4.0
+
+    def validate(self) -> None:
+        """FrequencySweepConfig::validate (frequency_sweep.rs:88-114) and validate_frequency_grid
+        (:306-320)."""
+        if not (np.isfinite(self.tolerance) and self.tolerance > 0):
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "frequency-sweep tolerance must be finite and positive")
+        if self.max_iterations <= 0 or self.gmres_restart <= 0:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT,
+                              "frequency-sweep iteration and restart limits must be non-zero")
+        if not (np.isfinite(self.beta_scale) and self.beta_scale > 0):
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "Burton-Miller beta scale must be finite and positive")
+        f = np.asarray(self.frequencies, np.float64)
+        if f.size == 0 or not np.all(np.isfinite(f)) or np.any(f <= 0) or np.any(np.diff(f) <= 0):
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT,
+                              "frequency sweep frequencies must be finite, positive, and strictly increasing")
+
+    @classmethod
+    def linear(cls, start_hz: float, end_hz: float, num_points: int) -> "FrequencySweepConfig":
+        step = (end_hz - start_hz) / (num_points - 1) if num_points > 1 else 0.0
+        return cls(frequencies=[start_hz + i * step for i in range(num_points)])
+
+    @classmethod
+    def logarithmic(cls, start_hz: float, end_hz: float, num_points: int) -> "FrequencySweepConfig":
+        a, b = np.log(start_hz), np.log(end_hz)
+        step = (b - a) / (num_points - 1) if num_points > 1 else 0.0
+        return cls(frequencies=[float(np.exp(a + i * step)) for i in range(num_points)])
+
+
+def frequency_sweep(mesh: Mesh, config: FrequencySweepConfig, direction=(0.0, 0.0, 1.0),
+                    speed_of_sound: float = 343.0, density: float = 1.21, mixed: bool = False,
+                    ir: IrConfig | None = None) -> FrequencySweepResult:
+    """The reference's sequential sweep (frequency_sweep_with_physics_and_admittances,
+    frequency_sweep.rs:592-850, dense branch): per frequency, re-assemble the dense system into one
+    device operator (the CudaTbemAssemblyWorkspace pattern), add the incident plane wave to the
+    boundary-condition right-hand side, solve with the previous frequency's solution as the
+    initial guess when recycle_solution is set, and accept the point only if the exact relative
+    residual is within max(20 tol, 1e-10) (:790-799). `mixed` solves with the FP32-inner /
+    FP64-refined GMRES instead of FP64 GMRES."""
+    import time
+
+    config.validate()
+    op = None
+    prev = None
+    res = FrequencySweepResult([], [], [], [], [], 0.0, 0.0)
+    try:
+        for f in config.frequencies:
+            ph = PhysicsParams.new(f, speed_of_sound, density)
+            beta = ph.burton_miller_beta(config.beta_scale)
+            t0 = time.perf_counter()
+            if op is None:
+                op = build_tbem_system_with_beta(mesh, ph, beta,
+                                                 L.SB_PRECISION_FP64_FP32 if mixed else L.SB_PRECISION_FP64)
+            else:
+                op.reassemble(ph, beta)
+            b = op.rhs + rhs_plane_wave(mesh, ph, beta, [direction])[:, 0]
+            t1 = time.perf_counter()
+            x0 = prev if (config.recycle_solution and prev is not None) else None
+            if mixed:
+                cfg = ir or IrConfig(tolerance=config.tolerance, inner_restart=config.gmres_restart)
+                sol = gmres_mixed(op, b, cfg, x0=x0)
+            else:
+                sol = gmres(op, b, GmresConfig(max_iterations=config.max_iterations, restart=config.gmres_restart,
+                                               tolerance=config.tolerance), x0=x0)
+            t2 = time.perf_counter()
+            tol = max(20.0 * config.tolerance, 1e-10)
+            if not np.isfinite(sol.residual) or sol.residual > tol:
+                raise SoniumError(L.SB_ERR_NOT_FINITE,
+                                  f"frequency sweep at {f:.3f} Hz: residual {sol.residual:.3e} above {tol:.3e}")
+            prev = sol.x
+            res.solutions.append(sol.x)
+            res.frequencies.append(f)
+            res.iteration_counts.append(sol.iterations)
+            res.converged.append(sol.converged)
+            res.exact_relative_residuals.append(sol.residual)
+            res.assembly_times.append(t1 - t0)
+            res.solve_times.append(t2 - t1)
+            res.stats.append(sol)
+    finally:
+        if op is not None:
+            op.close()
+    res.assembly_ms = 1e3 * sum(res.assembly_times)
+    res.solve_ms = 1e3 * sum(res.solve_times)
+    return res
 
 
 # Sweep workload: ka log-spaced on a triaxial ellipsoid, mesh refined with frequency.

@@ -169,3 +169,36 @@ def test_batch_rejects_bc_values_and_bad_config(gpu, oracle):
         batch.set_rhs(0, np.full(mesh.num_elements, np.nan, np.complex128))
     batch.close()
 
+
+
+def test_sequential_sweep_warm_start(gpu, oracle):
+    """frequency_sweep (frequency_sweep.rs:592-850, dense branch): re-assembly into one operator
+    per frequency, warm start from the previous solution. Recycling gives the same solutions (to
+    the tolerance) with fewer GMRES iterations on a closely spaced grid; every point passes the
+    exact-residual acceptance check; the mixed solver gives the FP64 solutions within 1e-5."""
+    from sonium_b200.sweep import FrequencySweepConfig, frequency_sweep
+
+    nodes, tris = oracle.icosphere(1.0, 2)
+    mesh = gpu.Mesh(nodes, tris)
+    c = 343.0
+    freqs = list(np.linspace(2.0, 2.4, 6) * c / (2 * np.pi))  # k = 2.0 .. 2.4
+    warm = frequency_sweep(mesh, FrequencySweepConfig(frequencies=freqs, tolerance=1e-9), speed_of_sound=c)
+    cold = frequency_sweep(mesh, FrequencySweepConfig(frequencies=freqs, tolerance=1e-9, recycle_solution=False),
+                           speed_of_sound=c)
+    assert warm.num_converged() == len(freqs) == cold.num_converged()
+    assert warm.total_iterations() < cold.total_iterations()
+    for xw, xc in zip(warm.solutions, cold.solutions):
+        assert np.linalg.norm(xw - xc) / np.linalg.norm(xc) < 1e-7
+    assert max(warm.exact_relative_residuals) < 1e-9
+    mixed = frequency_sweep(mesh, FrequencySweepConfig(frequencies=freqs, tolerance=1e-9), speed_of_sound=c,
+                            mixed=True)
+    for xm, xc in zip(mixed.solutions, cold.solutions):
+        assert np.linalg.norm(xm - xc) / np.linalg.norm(xc) < 1e-5
+    # each frequency's solution is that frequency's own system's (single solve, same beta)
+    ph = gpu.PhysicsParams.new(freqs[3], c)
+    beta = ph.burton_miller_beta(4.0)
+    op = gpu.build_tbem_system_with_beta(mesh, ph, beta)
+    b = gpu.rhs_plane_wave(mesh, ph, beta, [0, 0, 1])[:, 0]
+    x = gpu.gmres(op, b, gpu.GmresConfig(max_iterations=200, restart=30, tolerance=1e-10)).x
+    assert np.linalg.norm(warm.solutions[3] - x) / np.linalg.norm(x) < 1e-7
+    op.close()

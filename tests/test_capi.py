@@ -147,3 +147,19 @@ def test_umma_descriptors_match_cutlass(tmp_path):
     assert res.returncode == 0, res.stderr[-2000:]
     out = subprocess.run([exe], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.strip().endswith("OK"), out.stdout
+
+
+def test_frequency_sweep_config_validation(sb):
+    """FrequencySweepConfig::validate / validate_frequency_grid (frequency_sweep.rs:88-114, 306-320)."""
+    ok = sb.FrequencySweepConfig.linear(100.0, 200.0, 3)
+    ok.validate()
+    assert ok.frequencies == [100.0, 150.0, 200.0]
+    lg = sb.FrequencySweepConfig.logarithmic(10.0, 1000.0, 3)
+    assert np.allclose(lg.frequencies, [10.0, 100.0, 1000.0])
+    for bad in (sb.FrequencySweepConfig(frequencies=[]), sb.FrequencySweepConfig(frequencies=[200.0, 100.0]),
+                sb.FrequencySweepConfig(frequencies=[100.0, 100.0]), sb.FrequencySweepConfig(frequencies=[-1.0]),
+                sb.FrequencySweepConfig(frequencies=[100.0], tolerance=0.0),
+                sb.FrequencySweepConfig(frequencies=[100.0], gmres_restart=0),
+                sb.FrequencySweepConfig(frequencies=[100.0], beta_scale=float("nan"))):
+        with pytest.raises(sb.SoniumError):
+            bad.validate()
