@@ -270,6 +270,10 @@ SB_API int sb_field_eval(const sb_mesh* mesh, const sb_physics* physics, const s
  * vectors of length n, vector c at x + c * n (host memory). */
 SB_API int sb_operator_prepare_block_tensor(sb_operator* op);
 SB_API int sb_operator_apply_block_tensor(const sb_operator* op, const sb_complex32* x, sb_complex32* y, int64_t r);
+/* Device-resident variant: x_dev and y_dev hold vector c at + c * n (complex64), on the operator's
+ * device; the product runs on the operator's stream and is complete on return. */
+SB_API int sb_operator_apply_block_tensor_device(const sb_operator* op, const sb_complex32* x_dev,
+                                                 sb_complex32* y_dev, int64_t r);
 
 /* Many right-hand sides of one operator (the role of block_gmres_preconditioned,
  * crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:163, called via
@@ -333,6 +337,9 @@ typedef struct sb_profile {
     int64_t kernels; /* all kernels launched by the library (counted whether profiling is on or not) */
 } sb_profile;
 SB_API int sb_profile_enable(int on);
+/* Profile only the kernel classes whose bit (1 << SB_PROF_*) is set in mask (0 = off): timing one
+ * class adds fewer event records to the work it measures. */
+SB_API int sb_profile_enable_classes(unsigned mask);
 /* Totals since the last reset (synchronises the recorded events); reset != 0 clears them. */
 SB_API int sb_profile_read(sb_profile* out, int reset);
 /* CUDA event helpers on an operator's stream, for timing whole solves on the device. */

@@ -137,6 +137,7 @@ _SIGNATURES = {
     "sb_field_eval": ([P, ct.POINTER(SbPhysics), P, P, P, ct.c_int64, P], ct.c_int),
     "sb_operator_prepare_block_tensor": ([P], ct.c_int),
     "sb_operator_apply_block_tensor": ([P, P, P, ct.c_int64], ct.c_int),
+    "sb_operator_apply_block_tensor_device": ([P, P, P, ct.c_int64], ct.c_int),
     "sb_gmres_multi": ([P, P, ct.c_int64, ct.POINTER(SbIrConfig), P, P], ct.c_int),
     "sb_gmres_multi_device": ([P, P, ct.c_int64, ct.POINTER(SbIrConfig), P, P], ct.c_int),
     "sb_batch_create": ([ct.c_int64, P, P, P, ct.POINTER(P)], ct.c_int),
@@ -149,6 +150,7 @@ _SIGNATURES = {
     "sb_batch_matrix_c64": ([P, ct.c_int64, P], ct.c_int),
     "sb_batch_timings": ([P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
     "sb_profile_enable": ([ct.c_int], ct.c_int),
+    "sb_profile_enable_classes": ([ct.c_uint], ct.c_int),
     "sb_profile_read": ([ct.POINTER(SbProfile), ct.c_int], ct.c_int),
     "sb_event_create": ([ct.POINTER(P)], ct.c_int),
     "sb_event_destroy": ([P], ct.c_int),

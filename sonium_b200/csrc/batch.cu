@@ -456,7 +456,7 @@ struct Batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t graph_kernels = 0;
-    bool graph_prof = false;
+    unsigned graph_prof = 0;
     uint64_t graph_gen = 0;  // tensor-plane generation the captured cycle refers to
     std::vector<ProfPair> prof_pairs;
     Pinned pin;  // host mirror of the per-instance states, norms, scalars and flags
@@ -672,7 +672,7 @@ static void batch_step(Batch& B, int j) {
 // One restart cycle of the whole batch: m Arnoldi steps captured once into a CUDA graph.
 static void batch_cycle(Batch& B) {
     const uint64_t gen = B.shared ? tensor_generation(*B.shared) : 0;
-    if (!B.exec || B.graph_prof != g_prof_on || B.graph_gen != gen) {
+    if (!B.exec || B.graph_prof != prof_key() || B.graph_gen != gen) {
         B.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&B.prof_pairs);
@@ -691,7 +691,7 @@ static void batch_cycle(Batch& B) {
         SB_CUDA(cudaGraphInstantiate(&B.exec, B.graph, 0));
         B.graph_kernels = kernel_count() - before;
         add_kernel_count(-B.graph_kernels);
-        B.graph_prof = g_prof_on;
+        B.graph_prof = prof_key();
         B.graph_gen = gen;
     }
     SB_CUDA(cudaGraphLaunch(B.exec, B.stream));

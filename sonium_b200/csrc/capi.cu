@@ -528,6 +528,22 @@ SB_API int sb_operator_apply_block_tensor(const sb_operator* op, const sb_comple
 
 static void check_ir(const sb_ir_config* cfg);
 
+SB_API int sb_operator_apply_block_tensor_device(const sb_operator* op, const sb_complex32* x_dev,
+                                                 sb_complex32* y_dev, int64_t r) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && x_dev && y_dev && r >= 1, SB_ERR_INVALID_ARGUMENT, "bad argument");
+        SB_REQUIRE(r <= (int64_t)1 << 20, SB_ERR_INVALID_ARGUMENT, "apply_block_tensor: too many vectors");
+        Operator& o = *op->op;
+        SB_CUDA(cudaSetDevice(o.device));
+        maybe_inject(SB_INJECT_LAUNCH);
+        tensor_block_product(o, reinterpret_cast<const float2*>(x_dev), o.n, static_cast<int>(r),
+                             reinterpret_cast<float2*>(y_dev), o.n, o.stream);
+        SB_CUDA(cudaStreamSynchronize(o.stream));
+        SB_REQUIRE(tensor_status(o, true) == 0, SB_ERR_DEVICE_CHECK,
+                   "apply_block_tensor: a pipeline wait of the tensor-core kernel timed out");
+    });
+}
+
 SB_API int sb_gmres_multi(const sb_operator* op, const sb_complex* b, int64_t r, const sb_ir_config* cfg,
                           sb_complex* x, sb_gmres_stats* stats) {
     return guarded([&] {
@@ -739,7 +755,17 @@ SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs, c
 }
 
 SB_API int sb_profile_enable(int on) {
-    return guarded([&] { g_prof_on = on != 0; });
+    return guarded([&] {
+        g_prof_on = on != 0;
+        g_prof_mask = ~0u;
+    });
+}
+
+SB_API int sb_profile_enable_classes(unsigned mask) {
+    return guarded([&] {
+        g_prof_on = mask != 0;
+        g_prof_mask = mask;
+    });
 }
 
 SB_API int sb_profile_read(sb_profile* out, int reset) {

@@ -73,7 +73,7 @@ struct KrylovWork {
     cudaGraphExec_t exec = nullptr;
     const void* key_A = nullptr;
     int key_jacobi = -1;
-    bool key_prof = false;
+    unsigned key_prof = 0;
     std::vector<ProfPair> prof_pairs;
     int64_t graph_kernels = 0;
 
@@ -234,7 +234,7 @@ void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
 template <class T>
 void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
     const int jac = P.jacobi ? 1 : 0;
-    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_prof != g_prof_on) {
+    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_prof != prof_key()) {
         W.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&W.prof_pairs);
@@ -255,7 +255,7 @@ void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
         add_kernel_count(-W.graph_kernels);
         W.key_A = P.key_A;
         W.key_jacobi = jac;
-        W.key_prof = g_prof_on;
+        W.key_prof = prof_key();
     }
     SB_CUDA(cudaGraphLaunch(W.exec, P.stream));
     add_kernel_count(W.graph_kernels);

@@ -8,6 +8,7 @@
 namespace sb {
 
 bool g_prof_on = false;
+unsigned g_prof_mask = ~0u;
 static std::atomic<int64_t> g_kernels{0};
 static std::mutex g_prof_mu;
 static std::vector<ProfPair> g_pending;
@@ -28,7 +29,7 @@ void capture_step(int step) { t_step = step; }
 void capture_end() { t_capture = nullptr; }
 
 ProfScope::ProfScope(int kind, cudaStream_t s) : kind_(kind), s_(s) {
-    if (!g_prof_on) return;
+    if (!g_prof_on || !(g_prof_mask & (1u << kind_))) return;
     if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) {
         cudaGetLastError();
         a_ = b_ = nullptr;

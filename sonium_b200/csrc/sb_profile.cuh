@@ -13,6 +13,9 @@
 namespace sb {
 
 extern bool g_prof_on;
+extern unsigned g_prof_mask;  // kernel classes timed while profiling is on (bit = SB_PROF_*)
+// Identifies the profiling configuration a captured graph was recorded under.
+inline unsigned prof_key() { return g_prof_on ? g_prof_mask : 0u; }
 
 struct ProfPair {
     int kind;
