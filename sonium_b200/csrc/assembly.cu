@@ -712,8 +712,10 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                 } else {
                     sincos_f32(t, &st, &ct);
                 }
+                // The pair phase exp(i k r_c) is common to all points: the channel sums are
+                // accumulated in its frame and rotated once after the loop.
                 const float gs = pw[q] * rinv;
-                const float g_r = (cc * ct - sc * st) * gs, g_i = (sc * ct + cc * st) * gs;
+                const float g_r = ct * gs, g_i = st * gs;
                 // r_hat . n_y and -r_hat . n_x from per-pair and per-point dot products
                 const float rny = (fny + pn[q]) * rinv;
                 const float rnx = (fnx - (px[q] * nxx + py[q] * nxy + pz[q] * nxz)) * rinv;
@@ -735,13 +737,16 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             }
             const float cgr = scf[0][tid], cgi = scf[1][tid], chr = scf[2][tid], chi = scf[3][tid];
             const float ctr = scf[4][tid], cti = scf[5][tid], cer = scf[6][tid], cei = scf[7][tid];
-            const float vr = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
-            const float vi = ag_r * cgi + ag_i * cgr + ah_r * chi + ah_i * chr + at_r * cti + at_i * ctr + ae_r * cei + ae_i * cer;
-            A32[i * lda32 + j] = make_float2(vr, vi);
+            const float ur = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
+            const float ui = ag_r * cgi + ag_i * cgr + ah_r * chi + ah_i * chr + at_r * cti + at_i * ctr + ae_r * cei + ae_i * cer;
+            // rotate by the pair phase exp(i k r_c) = (cc, sc)
+            A32[i * lda32 + j] = make_float2(ur * cc - ui * sc, ur * sc + ui * cc);
             if (kWithRhs) {
                 Acc a;
-                a.gr = ag_r; a.gi = ag_i; a.hr = ah_r; a.hi = ah_i;
-                a.tr = at_r; a.ti = at_i; a.er = ae_r; a.ei = ae_i;
+                a.gr = ag_r * cc - ag_i * sc; a.gi = ag_r * sc + ag_i * cc;
+                a.hr = ah_r * cc - ah_i * sc; a.hi = ah_r * sc + ah_i * cc;
+                a.tr = at_r * cc - at_i * sc; a.ti = at_r * sc + at_i * cc;
+                a.er = ae_r * cc - ae_i * sc; a.ei = ae_r * sc + ae_i * cc;
                 rhs_c = combine(a, coef, ld, j, CF_DG);
             }
         }
