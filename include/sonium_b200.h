@@ -141,6 +141,15 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
 /* Re-assemble an existing operator for a new frequency / beta in place
  * (CudaTbemAssemblyWorkspace::assemble, tbem.rs:4230-4389). */
 SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_complex beta);
+/* DenseMatrixOperator over a caller's matrix (crates/sonium-bem/src/core/bem_solver.rs:6548-6590:
+ * the LinearOperator<Complex64> of any dense row-major matrix): matrix is n x n complex128,
+ * row-major, copied to the device. SB_PRECISION_FP64 keeps it in complex128, SB_PRECISION_FP64_FP32
+ * adds the complex64 copy of the mixed solver, SB_PRECISION_FP32 keeps only the complex64 copy.
+ * The operator has no mesh: sb_assemble_into and sb_rhs_plane_wave_device return
+ * SB_ERR_INVALID_ARGUMENT for it, its boundary-condition right-hand side is zero; the products,
+ * the preconditioner and every solver accept it. Non-finite entries: SB_ERR_NOT_FINITE. */
+SB_API int sb_operator_from_dense(int device, int64_t n, const sb_complex* matrix, int precision,
+                                  sb_operator** out);
 SB_API int sb_operator_destroy(sb_operator* op);
 SB_API int sb_operator_info_get(const sb_operator* op, sb_operator_info* info);
 /* TbemSystem { matrix, rhs } (tbem.rs:134-150) copied to host; either pointer may be NULL. */
@@ -242,6 +251,45 @@ SB_API int sb_gmres_mixed(const sb_operator* op, const sb_complex* b, const sb_c
 SB_API int sb_gmres_mixed_device(const sb_operator* op, const sb_complex* b_dev,
                                  sb_complex* x_dev, int x0_given, const sb_ir_config* cfg,
                                  sb_gmres_stats* stats);
+
+/* GCRO-DR: Krylov subspace recycling across a sequence of related systems (consecutive
+ * frequencies of a sweep). gcro_dr / gcro_dr_preconditioned (crates/sonium-solvers/crates/
+ * sonium-solvers-iterative/src/gcro_dr.rs:164-260, core :339-760) with the recycled subspace of
+ * GcroDrSubspace (:65-110): a subspace keeps up to k orthonormal vectors U (k = its target size,
+ * 0..100) on one device. Each solve rebuilds C = orth(M^-1 A U) for the operator it is given
+ * (k extra products; columns whose projected norm falls below 1e-12 are dropped, as build_c_r
+ * :769-850), runs restarted Arnoldi cycles of the restart length whose vectors are projected
+ * against C twice before CGS + DGKS against the cycle basis, tests convergence every step and
+ * the exact residual when a cycle claims convergence, and on an accepted solution (or after the
+ * last cycle without one) replaces U by the harmonic Ritz vectors of smallest magnitude of the
+ * augmented (k + m) problem (update_recycled_subspace :922-1050). An empty subspace gives plain
+ * GMRES with a convergence check every step. cfg as sb_gmres (max_iterations = restart cycles;
+ * convergence_check_interval is not used). stats: iterations, restarts, matvecs (incl. the
+ * rebuild of C and residual checks), residual = backward_error = exact relative residual.
+ * A subspace holding vectors of another length than the operator's n gives
+ * status SB_SOLVER_NUMERICAL_ERROR (x = x0) without touching it. Host entry: b, x0 (NULL = 0), x
+ * host buffers; non-finite b or x0 return SB_ERR_NOT_FINITE before any device work. */
+typedef struct sb_gcro_subspace sb_gcro_subspace;
+SB_API int sb_gcro_subspace_create(int device, int64_t k, sb_gcro_subspace** out);
+SB_API int sb_gcro_subspace_destroy(sb_gcro_subspace* s);
+/* GcroDrSubspace::reset: drop every vector (the next solve seeds a fresh subspace). */
+SB_API int sb_gcro_subspace_reset(sb_gcro_subspace* s);
+/* num_vectors held now, target size, vector length (0 while empty); any pointer may be NULL. */
+SB_API int sb_gcro_subspace_info(const sb_gcro_subspace* s, int64_t* num_vectors, int64_t* target,
+                                 int64_t* n);
+/* The held vectors to host memory (num_vectors x n, vector i at u + i * n) and back (the
+ * validated checkpoint round trip of GcroDrSubspace::vectors / replace_vectors, :98-110; count <=
+ * target, finite entries; the vectors are taken as given, orthonormal ones expected). */
+SB_API int sb_gcro_subspace_get_vectors(const sb_gcro_subspace* s, sb_complex* u);
+SB_API int sb_gcro_subspace_set_vectors(sb_gcro_subspace* s, int64_t count, int64_t n,
+                                        const sb_complex* u);
+SB_API int sb_gcro_dr(const sb_operator* op, const sb_complex* b, const sb_complex* x0,
+                      sb_gcro_subspace* s, const sb_gmres_config* cfg, int precond, sb_complex* x,
+                      sb_gmres_stats* stats);
+/* Same with device-resident b / x (x holds x0 on entry when x0_given != 0). */
+SB_API int sb_gcro_dr_device(const sb_operator* op, const sb_complex* b_dev, sb_complex* x_dev,
+                             int x0_given, sb_gcro_subspace* s, const sb_gmres_config* cfg,
+                             int precond, sb_gmres_stats* stats);
 
 /* Plane-wave RHS written to device memory (n x r complex128) on the operator's stream. */
 SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs,

@@ -118,6 +118,7 @@ _SIGNATURES = {
     "sb_mesh_set_bc": ([P, P, P, P, P], ct.c_int),
     "sb_assemble": ([P, ct.POINTER(SbPhysics), SbComplex, ct.c_int, ct.POINTER(P)], ct.c_int),
     "sb_assemble_into": ([P, ct.POINTER(SbPhysics), SbComplex], ct.c_int),
+    "sb_operator_from_dense": ([ct.c_int, ct.c_int64, P, ct.c_int, ct.POINTER(P)], ct.c_int),
     "sb_operator_destroy": ([P], ct.c_int),
     "sb_operator_info_get": ([P, ct.POINTER(SbOperatorInfo)], ct.c_int),
     "sb_operator_copy_to_host": ([P, P, P], ct.c_int),
@@ -134,6 +135,15 @@ _SIGNATURES = {
     "sb_gmres_mixed": ([P, P, P, ct.POINTER(SbIrConfig), P, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_mixed_device": ([P, P, P, ct.c_int, ct.POINTER(SbIrConfig), ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_rhs_plane_wave_device": ([P, P, P, ct.c_int64, P], ct.c_int),
+    "sb_gcro_subspace_create": ([ct.c_int, ct.c_int64, ct.POINTER(P)], ct.c_int),
+    "sb_gcro_subspace_destroy": ([P], ct.c_int),
+    "sb_gcro_subspace_reset": ([P], ct.c_int),
+    "sb_gcro_subspace_info": ([P, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)], ct.c_int),
+    "sb_gcro_subspace_get_vectors": ([P, P], ct.c_int),
+    "sb_gcro_subspace_set_vectors": ([P, ct.c_int64, ct.c_int64, P], ct.c_int),
+    "sb_gcro_dr": ([P, P, P, P, ct.POINTER(SbGmresConfig), ct.c_int, P, ct.POINTER(SbGmresStats)], ct.c_int),
+    "sb_gcro_dr_device": ([P, P, P, ct.c_int, P, ct.POINTER(SbGmresConfig), ct.c_int, ct.POINTER(SbGmresStats)],
+                          ct.c_int),
     "sb_field_eval": ([P, ct.POINTER(SbPhysics), P, P, P, ct.c_int64, P], ct.c_int),
     "sb_operator_prepare_block_tensor": ([P], ct.c_int),
     "sb_operator_apply_block_tensor": ([P, P, P, ct.c_int64], ct.c_int),

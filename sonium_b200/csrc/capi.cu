@@ -15,6 +15,9 @@ struct sb_mesh {
 struct sb_operator {
     sb::Operator* op;
 };
+struct sb_gcro_subspace {
+    sb::RecycleSpace* s;
+};
 
 namespace sb {
 
@@ -333,9 +336,60 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
     });
 }
 
+SB_API int sb_operator_from_dense(int device, int64_t n, const sb_complex* matrix, int precision, sb_operator** out) {
+    return guarded([&] {
+        SB_REQUIRE(matrix && out, SB_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        SB_REQUIRE(n > 0, SB_ERR_INVALID_ARGUMENT, "dense operator: n must be positive");
+        SB_REQUIRE(precision == SB_PRECISION_FP64 || precision == SB_PRECISION_FP64_FP32 ||
+                       precision == SB_PRECISION_FP32,
+                   SB_ERR_INVALID_ARGUMENT, "unknown precision");
+        int count = 0;
+        SB_CUDA(cudaGetDeviceCount(&count));
+        SB_REQUIRE(device >= 0 && device < count, SB_ERR_INVALID_ARGUMENT, "no such device");
+        SB_REQUIRE(all_finite(matrix, n * n), SB_ERR_NOT_FINITE, "dense operator: non-finite matrix entry");
+        SB_CUDA(cudaSetDevice(device));
+        Operator* op = new Operator();
+        try {
+            op->device = device;
+            op->precision = precision;
+            op->n = n;
+            op->lda32 = (n + 1) / 2 * 2;
+            SB_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
+            if (precision != SB_PRECISION_FP32) {
+                op->A64.alloc(sizeof(double2) * n * n);
+                SB_CUDA(cudaMemcpy(op->A64.p, matrix, sizeof(double2) * n * n, cudaMemcpyHostToDevice));
+            }
+            if (precision != SB_PRECISION_FP64) {
+                op->A32.alloc(sizeof(float2) * n * op->lda32);
+                std::vector<float2> row(op->lda32, make_float2(0.f, 0.f));
+                for (int64_t i = 0; i < n; ++i) {
+                    for (int64_t j = 0; j < n; ++j)
+                        row[j] = make_float2(static_cast<float>(matrix[i * n + j].re),
+                                             static_cast<float>(matrix[i * n + j].im));
+                    SB_CUDA(cudaMemcpy(op->A32.as<float2>() + i * op->lda32, row.data(), sizeof(float2) * op->lda32,
+                                       cudaMemcpyHostToDevice));
+                }
+            }
+            std::vector<sb_complex> d(n);
+            for (int64_t i = 0; i < n; ++i) d[i] = matrix[i * n + i];
+            op->diag.alloc(sizeof(double2) * n);
+            SB_CUDA(cudaMemcpy(op->diag.p, d.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+            op->rhs.alloc(sizeof(double2) * n);
+            SB_CUDA(cudaMemset(op->rhs.p, 0, sizeof(double2) * n));
+        } catch (...) {
+            if (op->stream) cudaStreamDestroy(op->stream);
+            delete op;
+            throw;
+        }
+        *out = new sb_operator{op};
+    });
+}
+
 SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_complex beta) {
     return guarded([&] {
         SB_REQUIRE(op && op->op && physics, SB_ERR_INVALID_ARGUMENT, "null argument");
+        SB_REQUIRE(op->op->mesh, SB_ERR_INVALID_ARGUMENT, "operator was not assembled from a mesh");
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
         tensor_release(*op->op);
@@ -749,8 +803,98 @@ SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs, c
         for (int64_t q = 0; q < 3 * r; ++q)
             SB_REQUIRE(std::isfinite(dirs[q]), SB_ERR_INVALID_ARGUMENT, "non-finite direction");
         const Operator& o = *op->op;
+        SB_REQUIRE(o.mesh, SB_ERR_INVALID_ARGUMENT, "operator was not assembled from a mesh");
         incident_plane_wave(*o.mesh, o.phys, o.beta_re, o.beta_im, dirs, reinterpret_cast<const double*>(amps), r,
                             reinterpret_cast<double2*>(rhs_dev), o.stream, false);
+    });
+}
+
+// ---- GCRO-DR ----
+SB_API int sb_gcro_subspace_create(int device, int64_t k, sb_gcro_subspace** out) {
+    return guarded([&] {
+        SB_REQUIRE(out, SB_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        SB_REQUIRE(k >= 0 && k <= 100, SB_ERR_INVALID_ARGUMENT, "recycled subspace size must be in 0..100");
+        int count = 0;
+        SB_CUDA(cudaGetDeviceCount(&count));
+        SB_REQUIRE(device >= 0 && device < count, SB_ERR_INVALID_ARGUMENT, "no such device");
+        *out = new sb_gcro_subspace{recycle_create(device, k)};
+    });
+}
+
+SB_API int sb_gcro_subspace_destroy(sb_gcro_subspace* s) {
+    return guarded([&] {
+        if (!s) return;
+        recycle_destroy(s->s);
+        delete s;
+    });
+}
+
+SB_API int sb_gcro_subspace_reset(sb_gcro_subspace* s) {
+    return guarded([&] {
+        SB_REQUIRE(s && s->s, SB_ERR_INVALID_ARGUMENT, "null subspace");
+        recycle_reset(*s->s);
+    });
+}
+
+SB_API int sb_gcro_subspace_info(const sb_gcro_subspace* s, int64_t* num_vectors, int64_t* target, int64_t* n) {
+    return guarded([&] {
+        SB_REQUIRE(s && s->s, SB_ERR_INVALID_ARGUMENT, "null subspace");
+        recycle_info(*s->s, num_vectors, target, n);
+    });
+}
+
+SB_API int sb_gcro_subspace_get_vectors(const sb_gcro_subspace* s, sb_complex* u) {
+    return guarded([&] {
+        SB_REQUIRE(s && s->s && u, SB_ERR_INVALID_ARGUMENT, "null argument");
+        recycle_get(*s->s, reinterpret_cast<double2*>(u));
+    });
+}
+
+SB_API int sb_gcro_subspace_set_vectors(sb_gcro_subspace* s, int64_t count, int64_t n, const sb_complex* u) {
+    return guarded([&] {
+        SB_REQUIRE(s && s->s && (u || count == 0), SB_ERR_INVALID_ARGUMENT, "null argument");
+        if (count > 0) {
+            SB_REQUIRE(n > 0, SB_ERR_INVALID_ARGUMENT, "vector length must be positive");
+            SB_REQUIRE(all_finite(u, count * n), SB_ERR_NOT_FINITE, "recycled subspace: non-finite vector entry");
+        }
+        recycle_set(*s->s, count, n, reinterpret_cast<const double2*>(u));
+    });
+}
+
+SB_API int sb_gcro_dr_device(const sb_operator* op, const sb_complex* b_dev, sb_complex* x_dev, int x0_given,
+                             sb_gcro_subspace* s, const sb_gmres_config* cfg, int precond, sb_gmres_stats* stats) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && s && s->s && b_dev && x_dev && stats, SB_ERR_INVALID_ARGUMENT, "null argument");
+        check_cfg(cfg);
+        SB_REQUIRE(precond == SB_PRECOND_IDENTITY || precond == SB_PRECOND_JACOBI, SB_ERR_INVALID_ARGUMENT,
+                   "unknown preconditioner");
+        maybe_inject(SB_INJECT_LAUNCH);
+        gcro_dr(*op->op, reinterpret_cast<const double2*>(b_dev), reinterpret_cast<double2*>(x_dev), x0_given != 0,
+                *s->s, *cfg, precond, *stats);
+    });
+}
+
+SB_API int sb_gcro_dr(const sb_operator* op, const sb_complex* b, const sb_complex* x0, sb_gcro_subspace* s,
+                      const sb_gmres_config* cfg, int precond, sb_complex* x, sb_gmres_stats* stats) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && s && s->s && b && x && stats, SB_ERR_INVALID_ARGUMENT, "null argument");
+        check_cfg(cfg);
+        SB_REQUIRE(precond == SB_PRECOND_IDENTITY || precond == SB_PRECOND_JACOBI, SB_ERR_INVALID_ARGUMENT,
+                   "unknown preconditioner");
+        const Operator& o = *op->op;
+        SB_REQUIRE(all_finite(b, o.n), SB_ERR_NOT_FINITE, "gcro_dr: non-finite right-hand side");
+        if (x0) SB_REQUIRE(all_finite(x0, o.n), SB_ERR_NOT_FINITE, "gcro_dr: non-finite initial guess");
+        SB_CUDA(cudaSetDevice(o.device));
+        DevBuf db, dx;
+        db.alloc(sizeof(double2) * o.n);
+        dx.alloc(sizeof(double2) * o.n);
+        SB_CUDA(cudaMemcpyAsync(db.p, b, sizeof(double2) * o.n, cudaMemcpyHostToDevice, o.stream));
+        if (x0) SB_CUDA(cudaMemcpyAsync(dx.p, x0, sizeof(double2) * o.n, cudaMemcpyHostToDevice, o.stream));
+        maybe_inject(SB_INJECT_LAUNCH);
+        gcro_dr(o, db.as<double2>(), dx.as<double2>(), x0 != nullptr, *s->s, *cfg, precond, *stats);
+        SB_CUDA(cudaMemcpyAsync(x, dx.p, sizeof(double2) * o.n, cudaMemcpyDeviceToHost, o.stream));
+        SB_CUDA(cudaStreamSynchronize(o.stream));
     });
 }
 

@@ -207,4 +207,15 @@ void multi_solve_device(Operator& op, const double2* b, int64_t ldb, int r, doub
                         const sb_ir_config& cfg, sb_gmres_stats* stats);
 void multi_release(Operator& op);
 
+// GCRO-DR with a recycled subspace kept across solves (gcro.cu).
+struct RecycleSpace;
+RecycleSpace* recycle_create(int device, int64_t k);
+void recycle_destroy(RecycleSpace* s);
+void recycle_reset(RecycleSpace& s);
+void recycle_info(const RecycleSpace& s, int64_t* count, int64_t* target, int64_t* n);
+void recycle_get(const RecycleSpace& s, double2* host);  // count x n, vector i at host + i * n
+void recycle_set(RecycleSpace& s, int64_t count, int64_t n, const double2* host);
+void gcro_dr(const Operator& op, const double2* b_dev, double2* x_dev, bool x0_given, RecycleSpace& sp,
+             const sb_gmres_config& cfg, int precond, sb_gmres_stats& st);
+
 }  // namespace sb

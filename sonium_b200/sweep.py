@@ -120,6 +120,7 @@ class FrequencySweepResult:
     stats: list = field(default_factory=list)
     assembly_times: list = field(default_factory=list)  # seconds per frequency (sequential sweep)
     solve_times: list = field(default_factory=list)
+    recycled_subspace_eligible: list = field(default_factory=list)  # sequential sweep (:196)
 
     def total_iterations(self) -> int:
         return int(sum(self.iteration_counts))
@@ -161,6 +162,10 @@ class FrequencySweepConfig:
     recycle_solution: bool = True
     gmres_restart: int = 30
     beta_scale: float = 4.0
+    # GCRO-DR vectors recycled between adjacent frequencies (0 = warm start only), and the largest
+    # relative frequency step |f_new - f_old| / max(f_new, f_old) that keeps the subspace (:60-68).
+    recycle_subspace_size: int = 0
+    max_recycle_relative_frequency_delta: float = 0.1
 
     def validate(self) -> None:
         """FrequencySweepConfig::validate (frequency_sweep.rs:88-114) and validate_frequency_grid
@@ -172,6 +177,12 @@ class FrequencySweepConfig:
                               "frequency-sweep iteration and restart limits must be non-zero")
         if not (np.isfinite(self.beta_scale) and self.beta_scale > 0):
             raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "Burton-Miller beta scale must be finite and positive")
+        d = self.max_recycle_relative_frequency_delta
+        if not (np.isfinite(d) and d >= 0):
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT,
+                              "frequency-sweep recycle frequency bound must be finite and non-negative")
+        if self.recycle_subspace_size < 0:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "recycle_subspace_size must be non-negative")
         f = np.asarray(self.frequencies, np.float64)
         if f.size == 0 or not np.all(np.isfinite(f)) or np.any(f <= 0) or np.any(np.diff(f) <= 0):
             raise SoniumError(L.SB_ERR_INVALID_ARGUMENT,
@@ -197,16 +208,31 @@ def frequency_sweep(mesh: Mesh, config: FrequencySweepConfig, direction=(0.0, 0.
     device operator (the CudaTbemAssemblyWorkspace pattern), add the incident plane wave to the
     boundary-condition right-hand side, solve with the previous frequency's solution as the
     initial guess when recycle_solution is set, and accept the point only if the exact relative
-    residual is within max(20 tol, 1e-10) (:790-799). `mixed` solves with the FP32-inner /
-    FP64-refined GMRES instead of FP64 GMRES."""
+    residual is within max(20 tol, 1e-10) (:790-799). With recycle_subspace_size > 0 every solve is
+    GCRO-DR (solve_sweep_operator, :495-508) on one recycled subspace, started afresh whenever the
+    relative step from the previous frequency exceeds max_recycle_relative_frequency_delta
+    (:636-647, relative_frequency_delta of crates/sonium-bem/src/core/mesh/lineage.rs:548).
+    `mixed` solves with the FP32-inner / FP64-refined GMRES instead of FP64 GMRES (no recycling)."""
     import time
 
+    from .tbem import GcroDrConfig, GcroDrSubspace, gcro_dr
+
     config.validate()
+    if mixed and config.recycle_subspace_size > 0:
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "subspace recycling runs the FP64 solver: mixed must be False")
     op = None
     prev = None
+    prev_f = None
+    sub = None
     res = FrequencySweepResult([], [], [], [], [], 0.0, 0.0)
     try:
         for f in config.frequencies:
+            eligible = prev_f is not None and abs(f - prev_f) / max(abs(prev_f), abs(f)) <= \
+                config.max_recycle_relative_frequency_delta
+            if config.recycle_subspace_size > 0 and (sub is None or not eligible):
+                if sub is not None:
+                    sub.close()
+                sub = GcroDrSubspace(config.recycle_subspace_size, mesh.device)
             ph = PhysicsParams.new(f, speed_of_sound, density)
             beta = ph.burton_miller_beta(config.beta_scale)
             t0 = time.perf_counter()
@@ -221,6 +247,9 @@ def frequency_sweep(mesh: Mesh, config: FrequencySweepConfig, direction=(0.0, 0.
             if mixed:
                 cfg = ir or IrConfig(tolerance=config.tolerance, inner_restart=config.gmres_restart)
                 sol = gmres_mixed(op, b, cfg, x0=x0)
+            elif sub is not None:
+                sol = gcro_dr(op, b, sub, GcroDrConfig(config.max_iterations, config.gmres_restart, config.tolerance),
+                              x0=x0)
             else:
                 sol = gmres(op, b, GmresConfig(max_iterations=config.max_iterations, restart=config.gmres_restart,
                                                tolerance=config.tolerance), x0=x0)
@@ -238,9 +267,13 @@ def frequency_sweep(mesh: Mesh, config: FrequencySweepConfig, direction=(0.0, 0.
             res.assembly_times.append(t1 - t0)
             res.solve_times.append(t2 - t1)
             res.stats.append(sol)
+            res.recycled_subspace_eligible.append(bool(eligible))
+            prev_f = f
     finally:
         if op is not None:
             op.close()
+        if sub is not None:
+            sub.close()
     res.assembly_ms = 1e3 * sum(res.assembly_times)
     res.solve_ms = 1e3 * sum(res.solve_times)
     return res

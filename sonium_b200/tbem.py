@@ -92,6 +92,7 @@ class Mesh:
         check(L.load().sb_mesh_create(_p(self.nodes), self.nodes.shape[0], _p(self.tris),
                                       self.tris.shape[0], device, ct.byref(h)))
         self._h = h
+        self.device = device
 
     @classmethod
     def icosphere(cls, radius: float, level: int, scale=None, device: int = 0) -> "Mesh":
@@ -251,6 +252,28 @@ class TbemOperator(LinearOperator):
             pass
 
 
+class DenseMatrixOperator(TbemOperator):
+    """DenseMatrixOperator (crates/sonium-bem/src/core/bem_solver.rs:6548-6590) over a caller's
+    n x n matrix, copied to the device: the LinearOperator of any dense system, with the same
+    products and solvers as an assembled operator (no mesh: no re-assembly, zero BC right-hand side)."""
+
+    def __init__(self, matrix, precision: int = L.SB_PRECISION_FP64, device: int = 0):
+        A = np.ascontiguousarray(matrix, np.complex128)
+        if A.ndim != 2 or A.shape[0] != A.shape[1] or A.shape[0] == 0:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "dense operator: matrix must be square and non-empty")
+        h = ct.c_void_p()
+        check(L.load().sb_operator_from_dense(device, A.shape[0], _p(A), precision, ct.byref(h)))
+        self.mesh = None
+        self._h = h
+        self.physics = None
+        self.beta = None
+        self.precision = precision
+        self.n = A.shape[0]
+
+    def reassemble(self, physics: PhysicsParams, beta: complex) -> None:
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "a dense operator has no mesh to re-assemble")
+
+
 class JacobiPreconditioner:
     """Preconditioner<Complex64> (traits.rs:3645-3720): y = diag(A)^-1 x."""
 
@@ -387,6 +410,96 @@ def gmres_multi(operator: TbemOperator, B, config: IrConfig = IrConfig()):
     check(L.load().sb_gmres_multi(operator.handle, _p(B), r, ct.byref(config._struct()), _p(X),
                                   ct.cast(stats, ct.c_void_p)))
     return X, [GmresSolution._from(None, stats[i]) for i in range(r)]
+
+
+class GcroDrSubspace:
+    """GcroDrSubspace (crates/sonium-solvers/crates/sonium-solvers-iterative/src/gcro_dr.rs:65-110):
+    up to k orthonormal recycled vectors kept on one device across GCRO-DR solves."""
+
+    def __init__(self, k: int, device: int = 0):
+        h = ct.c_void_p()
+        check(L.load().sb_gcro_subspace_create(device, int(k), ct.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "subspace has been closed")
+        return self._h
+
+    def _info(self):
+        c, t, n = ct.c_int64(), ct.c_int64(), ct.c_int64()
+        check(L.load().sb_gcro_subspace_info(self.handle, ct.byref(c), ct.byref(t), ct.byref(n)))
+        return c.value, t.value, n.value
+
+    def num_vectors(self) -> int:
+        return self._info()[0]
+
+    def target_size(self) -> int:
+        return self._info()[1]
+
+    def is_populated(self) -> bool:
+        return self.num_vectors() > 0
+
+    def reset(self) -> None:
+        check(L.load().sb_gcro_subspace_reset(self.handle))
+
+    def vectors(self) -> np.ndarray:
+        """The held vectors, (num_vectors, n) complex128."""
+        c, _, n = self._info()
+        u = np.zeros((c, n), np.complex128)
+        if c:
+            check(L.load().sb_gcro_subspace_get_vectors(self.handle, _p(u)))
+        return u
+
+    def replace_vectors(self, u) -> None:
+        u = np.ascontiguousarray(np.atleast_2d(u), np.complex128)
+        check(L.load().sb_gcro_subspace_set_vectors(self.handle, u.shape[0], u.shape[1] if u.shape[0] else 0,
+                                                    _p(u) if u.size else None))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            L.load().sb_gcro_subspace_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class GcroDrConfig:
+    """GcroDrConfig (gcro_dr.rs:114-160): restart cycles, Krylov dimension per cycle, relative
+    tolerance."""
+
+    max_iterations: int = 100
+    restart: int = 50
+    tolerance: float = 1e-6
+
+    @classmethod
+    def from_gmres(cls, g: GmresConfig) -> "GcroDrConfig":
+        return cls(g.max_iterations, g.restart, g.tolerance)
+
+    def _struct(self):
+        return L.SbGmresConfig(self.max_iterations, self.restart, self.tolerance, 1)
+
+
+def gcro_dr(operator: TbemOperator, b, subspace: GcroDrSubspace, config: GcroDrConfig = GcroDrConfig(),
+            x0=None, preconditioner: JacobiPreconditioner | None = None) -> GmresSolution:
+    """gcro_dr / gcro_dr_preconditioned (gcro_dr.rs:164-260) on the device: consumes the recycled
+    subspace and leaves the updated one in it."""
+    b = _c128(b)
+    if b.shape != (operator.n,):
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "gcro_dr: b must have length n")
+    x = np.zeros(operator.n, np.complex128)
+    x0a = None if x0 is None else _c128(x0)
+    st = L.SbGmresStats()
+    pk = L.SB_PRECOND_IDENTITY if preconditioner is None else preconditioner.kind
+    check(L.load().sb_gcro_dr(operator.handle, _p(b), None if x0a is None else _p(x0a), subspace.handle,
+                              ct.byref(config._struct()), pk, _p(x), ct.byref(st)))
+    return GmresSolution._from(x, st)
 
 
 def compute_scattered_field(mesh: Mesh, physics: PhysicsParams, surface_pressure, points,
