@@ -15,7 +15,8 @@ solve: re-assembly of the dense system on the device, the incident right-hand si
                 timed on a bounded sample (assembly rows + a CPU matvec) and scaled to one solve.
 
   * `sweep`  -- the batched frequency sweep: 64 instances (ka 1 -> 32 on the (1, 0.6, 0.4) ellipsoid,
-                levels 2-5) assembled in one launch and solved by the batched mixed GMRES,
+                levels 2-5) assembled together (the autotuned form: one persistent launch or
+                per-instance kernels on two streams) and solved by the batched mixed GMRES,
                 against the same instances solved one after another in plain FP64.
   * `multi_rhs` -- 256 plane-wave right-hand sides of one operator (ellipsoid level 5, k = 16)
                 solved together with tensor-core block products, against plain FP64 GMRES per
@@ -465,7 +466,8 @@ def sweep_leg(sb, a, dist, dev, rt):
     """Batched frequency sweep: 64 instances, ka log-spaced 1 -> 32 on the (1, 0.6, 0.4) ellipsoid,
     icosphere level per instance for >= 8 elements per wavelength (levels 2-5), plane wave +z.
 
-    One step = batched assembly of all 64 complex64 matrices (one persistent launch), the incident
+    One step = batched assembly of all 64 complex64 matrices (the form the autotuner chose on the
+    first, untimed step), the incident
     right-hand sides, and the batched FP32-inner / FP64-refined GMRES to rtol 1e-8. Baseline: the
     same 64 instances solved one after another in plain FP64 (complex128 assembly re-done into one
     operator per mesh level, FP64 GMRES(50) to 1e-8), timed once. Wall clock around device-synchronised
@@ -501,6 +503,8 @@ def sweep_leg(sb, a, dist, dev, rt):
         step()
     t_batch, _ = wall(lambda: [step() for _ in range(a.steps)])
     batched = dist.world * len(batch) * a.steps / t_batch
+    asm_ms, solve_ms = batch.timings()  # the last timed step
+    form, tune_p, tune_s = batch.assembly_tuning()
     batch.close()
     # plain FP64 baseline, one instance after another
     ops = {}
@@ -541,6 +545,8 @@ def sweep_leg(sb, a, dist, dev, rt):
         "max_residual": float(max(s.residual for s in st0)),
         "matrix_gb_c64": float(sum(8.0 * n * n for n in sizes) / 1e9),
         "assembly_ms": asm_ms, "solve_ms": solve_ms,
+        "assembly_form": {1: "persistent", 2: "streams"}.get(form, str(form)),
+        "assembly_autotune_ms": {"persistent": tune_p, "streams": tune_s},
         "iterations_batched": [int(s.iterations) for s in st0], "iterations_fp64": fp64_iters,
         "timing": "wall clock around device-synchronised steps, max over ranks",
     }

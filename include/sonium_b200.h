@@ -364,6 +364,22 @@ SB_API int sb_batch_solve(sb_batch* batch, const sb_ir_config* cfg, sb_gmres_sta
 SB_API int sb_batch_solution(const sb_batch* batch, int64_t index, sb_complex* x);
 /* The assembled complex64 matrix of one instance, row-major n x n. */
 SB_API int sb_batch_matrix_c64(const sb_batch* batch, int64_t index, sb_complex32* matrix);
+/* Assembly form of sb_batch_assemble (no reference counterpart: the execution choice of this
+ * implementation). SB_BATCH_ASM_PERSISTENT: one persistent launch walks a flattened work list of
+ * every instance's far tiles, near pairs and self terms. SB_BATCH_ASM_STREAMS: per-instance far
+ * kernels on the batch's stream with the near and self kernels on a second, higher-priority
+ * stream beside them. Both run the same device functions and write the same entries.
+ * SB_BATCH_ASM_AUTO (default): the first assembly of a batch shape (device, unknowns and near
+ * pairs per instance) runs both forms, keeps the faster one for every later batch of that shape
+ * in the process, and reports both times through sb_batch_assembly_tuning. */
+#define SB_BATCH_ASM_AUTO 0
+#define SB_BATCH_ASM_PERSISTENT 1
+#define SB_BATCH_ASM_STREAMS 2
+SB_API int sb_batch_set_assembly_mode(sb_batch* batch, int mode);
+/* The form the last sb_batch_assemble used, and the autotuner's measurements of the two forms in
+ * milliseconds (0 when this batch did not run the autotuner). Any pointer may be NULL. */
+SB_API int sb_batch_assembly_tuning(const sb_batch* batch, int* chosen, double* persistent_ms,
+                                    double* streams_ms);
 /* Device time of the last sb_batch_assemble and sb_batch_solve, milliseconds. */
 SB_API int sb_batch_timings(const sb_batch* batch, double* assembly_ms, double* solve_ms);
 

@@ -29,6 +29,7 @@ SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI = 0, 1
 SB_BC_VELOCITY, SB_BC_PRESSURE = 0, 1
 SB_INJECT_NONE, SB_INJECT_ALLOC, SB_INJECT_LAUNCH = 0, 1, 2
 SB_SOLVER_CONVERGED, SB_SOLVER_MAX_ITERATIONS, SB_SOLVER_BREAKDOWN, SB_SOLVER_NUMERICAL_ERROR = 0, 1, 2, 3
+SB_BATCH_ASM_AUTO, SB_BATCH_ASM_PERSISTENT, SB_BATCH_ASM_STREAMS = 0, 1, 2
 
 _ERROR_NAMES = {
     SB_ERR_INVALID_ARGUMENT: "InvalidInput",
@@ -159,6 +160,9 @@ _SIGNATURES = {
     "sb_batch_solution": ([P, ct.c_int64, P], ct.c_int),
     "sb_batch_matrix_c64": ([P, ct.c_int64, P], ct.c_int),
     "sb_batch_timings": ([P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
+    "sb_batch_set_assembly_mode": ([P, ct.c_int], ct.c_int),
+    "sb_batch_assembly_tuning": ([P, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)],
+                                 ct.c_int),
     "sb_profile_enable": ([ct.c_int], ct.c_int),
     "sb_profile_enable_classes": ([ct.c_uint], ct.c_int),
     "sb_profile_read": ([ct.POINTER(SbProfile), ct.c_int], ct.c_int),

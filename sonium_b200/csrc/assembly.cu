@@ -1521,6 +1521,61 @@ void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst*
     SB_CUDA(cudaGetLastError());
 }
 
+void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_t s, SideStream& side) {
+    side.ensure();
+    side.begin(s);
+    for (const BatchAsmInst& I : h_inst) {
+        if (I.nnz > 0) {
+            ProfScope prof(SB_PROF_NEAR, side.s);
+            k_near<<<cdiv(I.nnz, kNearWarps), 32 * kNearWarps, 0, side.s>>>(I.elem, I.n, I.ld, I.near_ptr, I.near_col,
+                                                                          I.nnz, I.coef, I.k, nullptr, I.A32, I.lda32,
+                                                                          nullptr);
+            count_launch();
+        }
+        ProfScope prof(SB_PROF_SELF, side.s);
+        k_self<<<cdiv(I.n, 4), 128, 0, side.s>>>(I.elem, I.n, I.ld, I.coef, I.k, nullptr, I.A32, I.lda32, nullptr,
+                                                I.diag);
+        count_launch();
+    }
+    SB_CUDA(cudaGetLastError());
+    for (const BatchAsmInst& I : h_inst) {
+        ProfScope prof(SB_PROF_FAR, s);
+        dim3 grid(static_cast<unsigned>(I.n_tiles), static_cast<unsigned>(cdiv(I.n, kFar32Rows)));
+        k_far32<false><<<grid, kFarTile, 0, s>>>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr,
+                                                 I.n_tiles);
+        count_launch();
+    }
+    SB_CUDA(cudaGetLastError());
+    side.end(s);
+}
+
+void SideStream::ensure() {
+    if (s) return;
+    int least = 0, greatest = 0;
+    SB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    SB_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest));
+    SB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    SB_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+}
+
+void SideStream::release() {
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (s) cudaStreamDestroy(s);
+    s = nullptr;
+    fork = join = nullptr;
+}
+
+void SideStream::begin(cudaStream_t main) {
+    SB_CUDA(cudaEventRecord(fork, main));
+    SB_CUDA(cudaStreamWaitEvent(s, fork, 0));
+}
+
+void SideStream::end(cudaStream_t main) {
+    SB_CUDA(cudaEventRecord(join, s));
+    SB_CUDA(cudaStreamWaitEvent(main, join, 0));
+}
+
 void coefficients_for(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im, double* coef,
                       cudaStream_t s) {
     k_coefficients<<<cdiv(m.ld, 256), 256, 0, s>>>(m.n, m.ld, m.bc_kind.as<int32_t>(), m.bc_value.as<double2>(),

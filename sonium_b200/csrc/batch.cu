@@ -24,6 +24,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 
 #include "sb_blas.cuh"
@@ -462,6 +464,11 @@ struct Batch {
     Pinned pin;  // host mirror of the per-instance states, norms, scalars and flags
     bool assembled = false, solved = false;
     double last_assembly_ms = 0.0, last_solve_ms = 0.0;
+    // Assembly form: SB_BATCH_ASM_AUTO (the autotuner's choice for this batch shape), _PERSISTENT
+    // or _STREAMS; the autotuner's two measurements when it ran for this batch.
+    int asm_mode = SB_BATCH_ASM_AUTO, asm_chosen = 0;
+    double tune_persistent_ms = 0.0, tune_streams_ms = 0.0;
+    SideStream side;
     void reset_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -471,6 +478,7 @@ struct Batch {
     }
     ~Batch() {
         reset_graph();
+        side.release();
         if (blas) cublasDestroy(blas);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -1098,6 +1106,49 @@ SB_API int sb_batch_destroy(sb_batch* batch) {
     return SB_OK;
 }
 
+// Autotuner memory: batch shape (device, per-instance unknowns and near pairs) -> assembly form.
+static std::mutex g_tune_mu;
+static std::map<std::vector<int64_t>, int> g_tune;
+
+static std::vector<int64_t> batch_shape_key(const Batch& B) {
+    std::vector<int64_t> key{B.device};
+    for (const BatchAsmInst& I : B.asm_h) {
+        key.push_back(I.n);
+        key.push_back(I.nnz);
+    }
+    return key;
+}
+
+static int tuned_assembly_form(const Batch& B) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(batch_shape_key(B));
+    return it == g_tune.end() ? SB_BATCH_ASM_AUTO : it->second;
+}
+
+static void remember_assembly_form(const Batch& B, int form) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[batch_shape_key(B)] = form;
+}
+
+SB_API int sb_batch_set_assembly_mode(sb_batch* batch, int mode) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null handle");
+        SB_REQUIRE(mode == SB_BATCH_ASM_AUTO || mode == SB_BATCH_ASM_PERSISTENT || mode == SB_BATCH_ASM_STREAMS,
+                   SB_ERR_INVALID_ARGUMENT, "batch: unknown assembly mode");
+        batch->b->asm_mode = mode;
+    });
+}
+
+SB_API int sb_batch_assembly_tuning(const sb_batch* batch, int* chosen, double* persistent_ms, double* streams_ms) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null handle");
+        const Batch& B = *batch->b;
+        if (chosen) *chosen = B.asm_chosen;
+        if (persistent_ms) *persistent_ms = B.tune_persistent_ms;
+        if (streams_ms) *streams_ms = B.tune_streams_ms;
+    });
+}
+
 SB_API int sb_batch_assemble(sb_batch* batch) {
     return guarded_batch([&] {
         SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null handle");
@@ -1114,16 +1165,35 @@ SB_API int sb_batch_assemble(sb_batch* batch) {
                 cudaEventDestroy(b);
             }
         } evg{e0, e1};
-        SB_CUDA(cudaEventRecord(e0, B.stream));
-        for (int i = 0; i < B.ninst; ++i)
-            coefficients_for(*B.meshes[i], B.phys[i], B.beta[i].x, B.beta[i].y,
-                             const_cast<double*>(B.asm_h[i].coef), B.stream);
-        assemble_batch(B.asm_h, B.asm_d.as<BatchAsmInst>(), B.pre_asm, B.stream, B.device);
-        SB_CUDA(cudaEventRecord(e1, B.stream));
-        SB_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        B.last_assembly_ms = ms;
+        auto run = [&](int form) -> double {
+            SB_CUDA(cudaEventRecord(e0, B.stream));
+            for (int i = 0; i < B.ninst; ++i)
+                coefficients_for(*B.meshes[i], B.phys[i], B.beta[i].x, B.beta[i].y,
+                                 const_cast<double*>(B.asm_h[i].coef), B.stream);
+            if (form == SB_BATCH_ASM_PERSISTENT)
+                assemble_batch(B.asm_h, B.asm_d.as<BatchAsmInst>(), B.pre_asm, B.stream, B.device);
+            else
+                assemble_batch_streams(B.asm_h, B.stream, B.side);
+            SB_CUDA(cudaEventRecord(e1, B.stream));
+            SB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            return ms;
+        };
+        int form = B.asm_mode;
+        if (form == SB_BATCH_ASM_AUTO) form = tuned_assembly_form(B);
+        if (form == SB_BATCH_ASM_AUTO) {
+            // Autotune: both forms once (each writes the complete matrices), keep the faster one
+            // for every batch of this shape on this device.
+            B.tune_persistent_ms = run(SB_BATCH_ASM_PERSISTENT);
+            B.tune_streams_ms = run(SB_BATCH_ASM_STREAMS);
+            form = B.tune_streams_ms < B.tune_persistent_ms ? SB_BATCH_ASM_STREAMS : SB_BATCH_ASM_PERSISTENT;
+            remember_assembly_form(B, form);
+            B.last_assembly_ms = std::min(B.tune_persistent_ms, B.tune_streams_ms);
+        } else {
+            B.last_assembly_ms = run(form);
+        }
+        B.asm_chosen = form;
         B.assembled = true;
     });
 }

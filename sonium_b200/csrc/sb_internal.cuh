@@ -109,6 +109,19 @@ struct Mesh {
     DevBuf bc_kind, bc_value, has_adm, adm;
 };
 
+// A second stream, of the device's highest priority, for work independent of the main stream's
+// (the batched near-pair and self kernels beside the far-field tiles: they write disjoint matrix
+// entries).
+// begin() makes it wait for the main stream's work so far; end() makes the main stream wait for it.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    void ensure();
+    void release();
+    void begin(cudaStream_t main);
+    void end(cudaStream_t main);
+};
+
 // ---------------------------------------------------------------------------------------------
 // Device-resident operator (assembled TBEM system)
 // ---------------------------------------------------------------------------------------------
@@ -144,6 +157,9 @@ struct BatchAsmInst {
 };
 void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst* d_inst, DevBuf& pre_buf,
                     cudaStream_t s, int device);
+// The same batch as per-instance launches: far tiles on s, near pairs and self terms on the side
+// stream (same device functions, so the same entries).
+void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_t s, SideStream& side);
 void coefficients_for(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im, double* coef,
                       cudaStream_t s);
 int coefficient_fields();

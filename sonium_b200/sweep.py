@@ -60,6 +60,16 @@ class SweepBatch:
         check(L.load().sb_batch_assemble(self.handle))
         return self.timings()[0]
 
+    def set_assembly_mode(self, mode: int) -> None:
+        """SB_BATCH_ASM_AUTO (autotuned), SB_BATCH_ASM_PERSISTENT or SB_BATCH_ASM_STREAMS."""
+        check(L.load().sb_batch_set_assembly_mode(self.handle, int(mode)))
+
+    def assembly_tuning(self):
+        """(form used by the last assembly, autotuner's persistent ms, autotuner's streams ms)."""
+        c, a, b = ct.c_int(), ct.c_double(), ct.c_double()
+        check(L.load().sb_batch_assembly_tuning(self.handle, ct.byref(c), ct.byref(a), ct.byref(b)))
+        return c.value, a.value, b.value
+
     def set_rhs_plane_wave(self, direction=(0.0, 0.0, 1.0)) -> None:
         d = np.ascontiguousarray(direction, np.float64)
         check(L.load().sb_batch_set_rhs_plane_wave(self.handle, _p(d)))

@@ -1,5 +1,6 @@
-"""Batched frequency sweep (sb_batch_*): one persistent assembly launch for many instances and
-the batched mixed-precision GMRES with per-instance convergence masks.
+"""Batched frequency sweep (sb_batch_*): the batched assembly of many instances (one persistent
+launch, or per-instance kernels on two streams, chosen by the autotuner) and the batched
+mixed-precision GMRES with per-instance convergence masks.
 
 Bars (written into each test):
   * each instance's complex64 matrix meets the mixed-assembly bar against the FP64 oracle (3e-5
@@ -63,6 +64,37 @@ def test_batch_matrices_match_single_instance_assembly(gpu, oracle):
         # and the two kernels agree to FP32 rounding of the largest entries
         assert np.abs(Ab - A1).max() <= 1e-6 * np.abs(A1).max(), (i, float(np.abs(Ab - A1).max()))
         op.close()
+    batch.close()
+
+
+def test_batch_assembly_forms_agree_and_autotune(gpu, oracle):
+    """The persistent single launch and the per-instance two-stream form write the same matrices;
+    the autotuner measures both on the first assembly of a new batch shape and keeps the faster."""
+    from sonium_b200._lib import SB_BATCH_ASM_AUTO, SB_BATCH_ASM_PERSISTENT, SB_BATCH_ASM_STREAMS
+    from sonium_b200.sweep import SweepBatch
+
+    spec = [(2, 1.7, (1.0, 0.6, 0.4)), (3, 3.1, (1.0, 0.6, 0.4)), (1, 0.9, (1.0, 1.0, 1.0))]  # a shape no other test uses
+    meshes, phys, betas = _instances(gpu, oracle, spec)
+    batch = SweepBatch(meshes, phys, betas)
+    batch.set_assembly_mode(SB_BATCH_ASM_PERSISTENT)
+    batch.assemble()
+    assert batch.assembly_tuning()[0] == SB_BATCH_ASM_PERSISTENT
+    Ap = [batch.matrix_c64(i) for i in range(len(batch))]
+    batch.set_assembly_mode(SB_BATCH_ASM_STREAMS)
+    batch.assemble()
+    assert batch.assembly_tuning()[0] == SB_BATCH_ASM_STREAMS
+    for i in range(len(batch)):
+        As = batch.matrix_c64(i)
+        assert np.abs(As - Ap[i]).max() <= 1e-6 * np.abs(Ap[i]).max(), i
+    batch.set_assembly_mode(SB_BATCH_ASM_AUTO)
+    batch.assemble()
+    chosen, t_p, t_s = batch.assembly_tuning()
+    assert t_p > 0 and t_s > 0
+    assert chosen == (SB_BATCH_ASM_STREAMS if t_s < t_p else SB_BATCH_ASM_PERSISTENT)
+    batch.assemble()  # remembered: no second tuning run
+    assert batch.assembly_tuning()[0] == chosen
+    with pytest.raises(gpu.SoniumError):
+        batch.set_assembly_mode(7)
     batch.close()
 
 
