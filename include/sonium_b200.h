@@ -141,6 +141,28 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
 /* Re-assemble an existing operator for a new frequency / beta in place
  * (CudaTbemAssemblyWorkspace::assemble, tbem.rs:4230-4389). */
 SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_complex beta);
+/* Discontinuous linear Tri3 basis: build_tbem_system_linear (crates/sonium-bem/src/core/assembly/
+ * tbem.rs:1490-1620) with regular_integration_linear (integration/regular.rs:337-470) and
+ * singular_integration_linear (integration/singular.rs:719-1170). Every element carries three
+ * DOFs, DOF 3e + c collocated at local point c of (1/6, 1/6), (2/3, 1/6), (1/6, 2/3)
+ * (mesh/element.rs:91-99) with the element normal, basis 2 lambda_c - 1/3 (element.rs:229-236);
+ * the operator is 3m x 3m complex128 (SB_PRECISION_FP64). Boundary conditions as sb_mesh_set_bc,
+ * without prescribed values (rigid, zero-pressure and admittance surfaces): a mesh with nonzero
+ * prescribed values gives SB_ERR_INVALID_ARGUMENT. sb_assemble_into re-assembles it at another
+ * frequency; sb_rhs_plane_wave_device evaluates the incident field at its collocation points. */
+#define SB_BASIS_CONSTANT 0
+#define SB_BASIS_LINEAR 1
+SB_API int sb_assemble_linear(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta,
+                              sb_operator** out);
+/* Collocation points and normals of a basis (host arrays, DOF-major x 3): m of them for
+ * SB_BASIS_CONSTANT (the centroids), 3m for SB_BASIS_LINEAR. */
+SB_API int sb_mesh_collocation(const sb_mesh* mesh, int basis, double* points, double* normals);
+/* IncidentField::compute_rhs_with_beta (incident.rs:807-833) for plane waves at np arbitrary
+ * collocation points with normals (host arrays np x 3), on the device: rhs[i * r + q]. */
+SB_API int sb_rhs_plane_wave_points(int device, int64_t np, const double* points, const double* normals,
+                                    const sb_physics* physics, sb_complex beta, const double* dirs,
+                                    const sb_complex* amps, int64_t r, sb_complex* rhs);
+
 /* DenseMatrixOperator over a caller's matrix (crates/sonium-bem/src/core/bem_solver.rs:6548-6590:
  * the LinearOperator<Complex64> of any dense row-major matrix): matrix is n x n complex128,
  * row-major, copied to the device. SB_PRECISION_FP64 keeps it in complex128, SB_PRECISION_FP64_FP32

@@ -1146,3 +1146,349 @@ extern "C" void or_field_eval(const double* nodes, const uint32_t* tris, int64_t
         out[i] = O(acc);
     }
 }
+
+// =============================================================================================
+// Discontinuous linear Tri3 basis: build_tbem_system_linear (crates/sonium-bem/src/core/
+// assembly/tbem.rs:1490-1620) with regular_integration_linear_with_normals (integration/
+// regular.rs:359-470) and singular_integration_linear_with_params_mode (integration/
+// singular.rs:868-1170). Three DOFs per element, collocated at the interior points
+// (1/6, 1/6), (2/3, 1/6), (1/6, 2/3) (mesh/element.rs:91-99), basis 2 lambda_b - 1/3
+// (element.rs:229-236), element e owns DOFs 3e, 3e + 1, 3e + 2.
+// =============================================================================================
+namespace {
+
+const double kLinColl[3][2] = {{1.0 / 6.0, 1.0 / 6.0}, {2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}};
+
+inline void lin_basis(double s, double t, double nb[3]) {
+    const double l[3] = {1.0 - s - t, s, t};
+    for (int b = 0; b < 3; ++b) nb[b] = 2.0 * l[b] - 1.0 / 3.0;
+}
+
+// local_to_global (element.rs:65-76), Tri3 shape functions.
+void lin_point(const Coords& c, double s, double t, double x[3]) {
+    const double sf[3] = {1.0 - s - t, s, t};
+    x[0] = x[1] = x[2] = 0.0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) x[j] += sf[i] * c.v[i][j];
+}
+
+struct Channels3 {
+    Channels b[3];
+};
+
+// regular_integration_linear_with_normals (regular.rs:359-470), flat normals.
+Channels3 regular_pair_linear(const double x[3], const double nx[3], const Coords& c, double area,
+                              const or_physics& ph) {
+    const double wavruim = ph.harmonic_factor * ph.wave_number;
+    const double k2 = ph.wave_number * ph.wave_number;
+    Channels3 r;
+    std::vector<Leaf> leaves = generate_subelements(x, c, area);
+    for (const Leaf& lf : leaves) {
+        const bool iforie = std::fabs(std::fabs(lf.factor) - 1.0) < 1e-10;
+        std::vector<TriPoint> pts = triangle_quadrature(lf.order);
+        for (const TriPoint& p : pts) {
+            double xio, eto, weih2;
+            if (iforie) {
+                xio = p.xi;
+                eto = p.eta;
+                weih2 = p.w;
+            } else {
+                double l0 = 1.0 - p.xi - p.eta;
+                xio = lf.tv[0][0] * l0 + lf.tv[1][0] * p.xi + lf.tv[2][0] * p.eta;
+                eto = lf.tv[0][1] * l0 + lf.tv[1][1] * p.xi + lf.tv[2][1] * p.eta;
+                double dx1 = lf.tv[1][0] - lf.tv[0][0];
+                double dy1 = lf.tv[1][1] - lf.tv[0][1];
+                double dx2 = lf.tv[2][0] - lf.tv[0][0];
+                double dy2 = lf.tv[2][1] - lf.tv[0][1];
+                weih2 = p.w * std::fabs(dx1 * dy2 - dx2 * dy1);
+            }
+            double pos[3], jac, ny[3];
+            tri_parameters(c, xio, eto, pos, jac, ny);
+            double wga = weih2 * jac;
+            double d[3] = {pos[0] - x[0], pos[1] - x[1], pos[2] - x[2]};
+            double u[3];
+            double dis = normalize3(d, u);
+            if (dis < 1e-15) continue;
+            cd zg = exp_i(wavruim * dis) * (wga / (4.0 * kPi * dis));
+            cd zb = zg * cd(-1.0 / dis, wavruim);
+            double rny = u[0] * ny[0] + u[1] * ny[1] + u[2] * ny[2];
+            double rnx = -(u[0] * nx[0] + u[1] * nx[1] + u[2] * nx[2]);
+            double rq = rny * rnx;
+            double nxny = nx[0] * ny[0] + nx[1] * ny[1] + nx[2] * ny[2];
+            double dq = dis * dis;
+            cd ef((3.0 / dq - k2) * rq + nxny / dq, -wavruim / dis * (3.0 * rq + nxny));
+            cd zh = zb * rny, zt = zb * rnx, ze = zg * ef;
+            double nb[3];
+            lin_basis(xio, eto, nb);
+            for (int b = 0; b < 3; ++b) {
+                r.b[b].g += zg * nb[b];
+                r.b[b].h += zh * nb[b];
+                r.b[b].ht += zt * nb[b];
+                r.b[b].e += ze * nb[b];
+            }
+        }
+    }
+    return r;
+}
+
+// panel_basis_gradients (singular.rs:1173-1258), Tri3 linear: surface gradients of the three
+// basis functions (constant over a flat panel).
+void lin_gradients(const Coords& c, double grad[3][3]) {
+    const double der[3][2] = {{-2.0, -2.0}, {2.0, 0.0}, {0.0, 2.0}};
+    const double sds[3] = {-1.0, 1.0, 0.0}, sdt[3] = {-1.0, 0.0, 1.0};
+    double ts[3] = {0, 0, 0}, tt[3] = {0, 0, 0};
+    for (int node = 0; node < 3; ++node)
+        for (int a = 0; a < 3; ++a) {
+            ts[a] += sds[node] * c.v[node][a];
+            tt[a] += sdt[node] * c.v[node][a];
+        }
+    double ss = 0, tq = 0, st = 0;
+    for (int a = 0; a < 3; ++a) {
+        ss += ts[a] * ts[a];
+        tq += tt[a] * tt[a];
+        st += ts[a] * tt[a];
+    }
+    const double det = ss * tq - st * st;
+    for (int b = 0; b < 3; ++b) {
+        const double ga = (tq * der[b][0] - st * der[b][1]) / det;
+        const double gb = (ss * der[b][1] - st * der[b][0]) / det;
+        for (int a = 0; a < 3; ++a) grad[b][a] = ga * ts[a] + gb * tt[a];
+    }
+}
+
+// singular_integration_linear_with_params_mode (singular.rs:868-1170), Tri3, flat normals, no
+// derivative: the edge line integral of the regularised E weighted by the basis at the edge
+// point, the centroid-centred Duffy sub-triangles for G, H, H^T and the area part of E
+// (k^2 n_x.n_y G N_b plus the basis-gradient term of the weighted Stokes identity).
+Channels3 singular_pair_linear(const double x[3], const double nx[3], const Coords& c,
+                               const or_physics& ph) {
+    static const double csi6[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+    static const double eta6[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
+    const double wavruim = ph.harmonic_factor * ph.wave_number;
+    const double k2 = ph.wave_number * ph.wave_number;
+    const SingularParams q = singular_params(c, ph.wave_number);
+    std::vector<double> ecx, ecw, scx, scw;
+    gauss_legendre(q.edge_order, ecx, ecw);
+    gauss_legendre(q.sub_order, scx, scw);
+    const int nsec1 = q.sections, nsec2 = q.subtri;
+    double grad[3][3];
+    lin_gradients(c, grad);
+    Channels3 r;
+    for (int ieg = 0; ieg < 3; ++ieg) {
+        const int ig1 = (ieg + 1) % 3, ig2 = ieg + 3;
+        double dp[3];
+        double leneg = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            dp[i] = c.v[ig1][i] - c.v[ieg][i];
+            leneg += dp[i] * dp[i];
+        }
+        leneg = std::sqrt(leneg);
+        const double dpo[3] = {dp[0] / leneg, dp[1] / leneg, dp[2] / leneg};
+        const double leneg_scaled = leneg / (2.0 * nsec1);
+        const double delsec = 2.0 / nsec1;
+        double secmid = -1.0 - delsec / 2.0;
+        for (int is = 0; is < nsec1; ++is) {
+            secmid += delsec;
+            for (int ig = 0; ig < q.edge_order; ++ig) {
+                double sga = secmid + ecx[ig] / nsec1;
+                double wga = ecw[ig] * leneg_scaled;
+                double d[3];
+                for (int i = 0; i < 3; ++i) {
+                    double gp = c.v[ieg][i] + dp[i] * (sga + 1.0) / 2.0;
+                    d[i] = gp - x[i];
+                }
+                double u[3];
+                double dis = normalize3(d, u);
+                if (dis < 1e-15) continue;
+                cd zg = exp_i(wavruim * dis) / (4.0 * kPi * dis);
+                cd zf = zg * cd(-1.0 / dis, wavruim);
+                cd zd[3] = {zf * u[0], zf * u[1], zf * u[2]};
+                cd w0 = zd[1] * dpo[2] - zd[2] * dpo[1];
+                cd w1 = zd[2] * dpo[0] - zd[0] * dpo[2];
+                cd w2 = zd[0] * dpo[1] - zd[1] * dpo[0];
+                cd contrib = (w0 * nx[0] + w1 * nx[1] + w2 * nx[2]) * wga;
+                const double te = (sga + 1.0) / 2.0;
+                const double sl = csi6[ieg] * (1.0 - te) + csi6[ig1] * te;
+                const double tl = eta6[ieg] * (1.0 - te) + eta6[ig1] * te;
+                double nb[3];
+                lin_basis(sl, tl, nb);
+                for (int b = 0; b < 3; ++b) r.b[b].e += contrib * nb[b];
+            }
+        }
+        for (int isec = 0; isec < nsec2; ++isec) {
+            const double aresub = 1.0 / 24.0 / nsec2;
+            double ss[3], ts[3];
+            ss[0] = 1.0 / 3.0;
+            ts[0] = 1.0 / 3.0;
+            if (isec == 0) {
+                ss[1] = csi6[ieg];
+                ss[2] = csi6[ig2];
+                ts[1] = eta6[ieg];
+                ts[2] = eta6[ig2];
+            } else {
+                ss[1] = csi6[ig2];
+                ss[2] = csi6[ig1];
+                ts[1] = eta6[ig2];
+                ts[2] = eta6[ig1];
+            }
+            for (int a = 0; a < q.sub_order; ++a) {
+                const double sga = scx[a];
+                for (int b2 = 0; b2 < q.sub_order; ++b2) {
+                    const double tga = scx[b2];
+                    const double wei = scw[a] * scw[b2];
+                    double sgg = 0.5 * (1.0 - sga) * ss[0] +
+                                 0.25 * (1.0 + sga) * ((1.0 - tga) * ss[1] + (1.0 + tga) * ss[2]);
+                    double tgg = 0.5 * (1.0 - sga) * ts[0] +
+                                 0.25 * (1.0 + sga) * ((1.0 - tga) * ts[1] + (1.0 + tga) * ts[2]);
+                    double pos[3], jac, ny[3];
+                    tri_parameters(c, sgg, tgg, pos, jac, ny);
+                    double wga = wei * (1.0 + sga) * aresub * jac;
+                    double d[3] = {pos[0] - x[0], pos[1] - x[1], pos[2] - x[2]};
+                    double u[3];
+                    double dis = normalize3(d, u);
+                    if (dis < 1e-15) continue;
+                    cd zg = exp_i(wavruim * dis) * (wga / (4.0 * kPi * dis));
+                    cd zb = zg * cd(-1.0 / dis, wavruim);
+                    double rny = u[0] * ny[0] + u[1] * ny[1] + u[2] * ny[2];
+                    double rnx = -(u[0] * nx[0] + u[1] * nx[1] + u[2] * nx[2]);
+                    cd zh = zb * rny, zt = zb * rnx;
+                    double nd = nx[0] * ny[0] + nx[1] * ny[1] + nx[2] * ny[2];
+                    cd earea = zg * k2 * nd;
+                    double nb[3];
+                    lin_basis(sgg, tgg, nb);
+                    for (int b = 0; b < 3; ++b) {
+                        r.b[b].g += zg * nb[b];
+                        r.b[b].h += zh * nb[b];
+                        r.b[b].ht += zt * nb[b];
+                        const double gr = grad[b][0] * u[0] + grad[b][1] * u[1] + grad[b][2] * u[2];
+                        const double gs = grad[b][0] * nx[0] + grad[b][1] * nx[1] + grad[b][2] * nx[2];
+                        r.b[b].e += earea * nb[b] + zb * (-nd * gr + rny * gs);
+                    }
+                }
+            }
+        }
+    }
+    return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Collocation points and normals of the linear basis: 3 per element (element.rs:91-99 through
+// local_to_global; flat normals, tbem.rs:1516-1527).
+void or_linear_collocation(int64_t n_tris, const double* nodes, const uint32_t* tris, double* points,
+                           double* normals) {
+    std::vector<double> centers(3 * n_tris), nrm(3 * n_tris), areas(n_tris);
+    element_geometry(n_tris, nodes, tris, centers.data(), nrm.data(), areas.data());
+    for (int64_t e = 0; e < n_tris; ++e) {
+        Coords c;
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 3; ++j) c.v[a][j] = nodes[3 * tris[3 * e + a] + j];
+        for (int q = 0; q < 3; ++q) {
+            lin_point(c, kLinColl[q][0], kLinColl[q][1], points + 3 * (3 * e + q));
+            for (int j = 0; j < 3; ++j) normals[3 * (3 * e + q) + j] = nrm[3 * e + j];
+        }
+    }
+}
+
+// build_tbem_system_linear (tbem.rs:1490-1620): A is 3m x 3m row-major, rhs 3m. Prescribed
+// boundary values are read per element (one value; the DOFs of an element share it through
+// add_free_terms' average, tbem.rs:1248-1281, and the field BC's first basis slot).
+int or_assemble_linear(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris,
+                       const or_bc* bc, const or_physics* ph, or_c128 beta_in, int threads, or_c128* A,
+                       or_c128* rhs) {
+    if (m <= 0) return 1;
+    for (int64_t i = 0; i < 3 * m; ++i)
+        if (tris[i] >= static_cast<uint64_t>(n_nodes)) return 1;
+    std::vector<double> centers(3 * m), normals(3 * m), areas(m);
+    element_geometry(m, nodes, tris, centers.data(), normals.data(), areas.data());
+    std::vector<Coords> coords(m);
+    for (int64_t e = 0; e < m; ++e)
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 3; ++j) coords[e].v[a][j] = nodes[3 * tris[3 * e + a] + j];
+    const cd gamma(1.0, 0.0), tau(ph->tau, 0.0), iwr(0.0, ph->pressure_factor);
+    const cd beta = C(beta_in);
+    std::vector<BcView> bcs(m);
+    for (int64_t e = 0; e < m; ++e) bcs[e] = bc_at(bc, e);
+    const int64_t n = 3 * m;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t r = 0; r < n; ++r) {
+        const int64_t i = r / 3;
+        const int cq = static_cast<int>(r % 3);
+        std::vector<cd> local(n, cd(0, 0));
+        cd lrhs(0, 0);
+        const BcView& sb = bcs[i];
+        if (sb.kind == 0) {  // add_free_terms (tbem.rs:1248-1281)
+            local[r] -= gamma * 0.5;
+            if (sb.has_adm) local[r] -= sb.adm * iwr * beta * tau * 0.5;
+            lrhs += sb.value * iwr * beta * tau * 0.5;
+        } else if (sb.kind == 1) {
+            local[r] += beta * tau * 0.5;
+            lrhs -= sb.value * gamma * 0.5;
+        }
+        double x[3];
+        lin_point(coords[i], kLinColl[cq][0], kLinColl[cq][1], x);
+        const double* nx = &normals[3 * i];
+        for (int64_t j = 0; j < m; ++j) {
+            const BcView& fb = bcs[j];
+            const bool compute_rhs = std::abs(fb.value) > 1e-15;
+            Channels3 rr = (j == i) ? singular_pair_linear(x, nx, coords[j], *ph)
+                                    : regular_pair_linear(x, nx, coords[j], areas[j], *ph);
+            for (int b = 0; b < 3; ++b) {
+                const Channels& q = rr.b[b];
+                cd coeff(0, 0);
+                if (fb.kind == 0) {
+                    coeff = q.h * gamma * tau + q.e * beta;
+                    if (fb.has_adm) coeff -= (q.g * gamma * tau + q.ht * beta) * fb.adm * iwr;
+                } else if (fb.kind == 1) {
+                    coeff = -(q.g * gamma * tau + q.ht * beta);
+                }
+                local[3 * j + b] += coeff;
+                if (compute_rhs && b == 0) {  // values.get(b): one prescribed value per element
+                    if (fb.kind == 0)
+                        lrhs += (q.g * gamma * tau + q.ht * beta) * fb.value * iwr;
+                    else if (fb.kind == 1)
+                        lrhs += -(q.h * gamma * tau + q.e * beta) * fb.value;
+                }
+            }
+        }
+        for (int64_t j = 0; j < n; ++j) A[r * n + j] = O(local[j]);
+        if (rhs) rhs[r] = O(lrhs);
+    }
+    return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Pair-level access to the linear-basis channels (tests): out12 = (g, h, ht, e) for b = 0, 1, 2.
+void or_regular_pair_linear(const double* x, const double* nx, const double* c9, double area,
+                            const or_physics* ph, or_c128* out12) {
+    Coords c;
+    std::memcpy(c.v, c9, sizeof(c.v));
+    Channels3 r = regular_pair_linear(x, nx, c, area, *ph);
+    for (int b = 0; b < 3; ++b) {
+        out12[4 * b + 0] = O(r.b[b].g);
+        out12[4 * b + 1] = O(r.b[b].h);
+        out12[4 * b + 2] = O(r.b[b].ht);
+        out12[4 * b + 3] = O(r.b[b].e);
+    }
+}
+
+void or_singular_pair_linear(const double* x, const double* nx, const double* c9, const or_physics* ph,
+                             or_c128* out12) {
+    Coords c;
+    std::memcpy(c.v, c9, sizeof(c.v));
+    Channels3 r = singular_pair_linear(x, nx, c, *ph);
+    for (int b = 0; b < 3; ++b) {
+        out12[4 * b + 0] = O(r.b[b].g);
+        out12[4 * b + 1] = O(r.b[b].h);
+        out12[4 * b + 2] = O(r.b[b].ht);
+        out12[4 * b + 3] = O(r.b[b].e);
+    }
+}
+
+}  // extern "C"

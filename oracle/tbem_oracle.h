@@ -109,6 +109,20 @@ void or_mie_rigid_field(double k, double radius, int num_terms, double r, int64_
                         const double* theta, or_c128* out);
 /* Scattered field at m exterior points from constant Tri3 surface pressure / velocity
  * (velocity may be NULL = rigid); compute_scattered_field, postprocess/pressure.rs:1388-1448. */
+/* Discontinuous linear Tri3 basis: collocation points / normals (3 per element, DOF 3e + c) and
+ * build_tbem_system_linear (A: 3m x 3m row-major, rhs: 3m). */
+void or_linear_collocation(int64_t n_tris, const double* nodes, const uint32_t* tris, double* points,
+                           double* normals);
+int or_assemble_linear(int64_t n_nodes, const double* nodes, int64_t n_tris, const uint32_t* tris,
+                       const or_bc* bc, const or_physics* phys, or_c128 beta, int threads, or_c128* A,
+                       or_c128* rhs);
+
+/* Linear-basis channels of one pair: out12 = (g, h, ht, e) for basis 0, 1, 2. */
+void or_regular_pair_linear(const double* x, const double* nx, const double* coords9, double area,
+                            const or_physics* phys, or_c128* out12);
+void or_singular_pair_linear(const double* x, const double* nx, const double* coords9,
+                             const or_physics* phys, or_c128* out12);
+
 void or_field_eval(const double* nodes, const uint32_t* tris, int64_t n_tris, const or_c128* pressure,
                    const or_c128* velocity, double k, double harmonic_factor, double pressure_factor,
                    const double* points, int64_t m, int threads, or_c128* out);

@@ -807,12 +807,55 @@ __device__ __forceinline__ int gauss_order(double disfac) {
     return 7;
 }
 
-// Evaluates the regular-integration channels of pair (i, j) into lane-partial sums.
-__device__ void near_pair_channels(Acc& a, NearWarpSmem& S, const double* __restrict__ elem,
-                                   int64_t ld, int64_t i, int64_t j, double k, double k2,
-                                   int lane) {
-    const double x0 = E(ECX, i), x1 = E(ECY, i), x2 = E(ECZ, i);
-    const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
+// Adds one quadrature point's (G, H, H^T, E) to NB basis-weighted channel sums (weights nb[b]).
+template <int NB>
+__device__ __forceinline__ void point_channels_w(Acc* a, const double* nb, double dx, double dy, double dz,
+                                                 double r, double rinv, double wga, double nyx, double nyy,
+                                                 double nyz, double nxx, double nxy, double nxz, double k,
+                                                 double k2) {
+    double s, c;
+    sb_sincos(k * r, &s, &c);
+    const double gs = wga * kInv4Pi * rinv;
+    const double g_r = c * gs, g_i = s * gs;
+    const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+    const double rny = ux * nyx + uy * nyy + uz * nyz;
+    const double rnx = -(ux * nxx + uy * nxy + uz * nxz);
+    const double b_r = -g_r * rinv - g_i * k;
+    const double b_i = g_r * k - g_i * rinv;
+    const double rq = rny * rnx;
+    const double nxny = nxx * nyx + nxy * nyy + nxz * nyz;
+    const double ri2 = rinv * rinv;
+    const double f_r = (3.0 * ri2 - k2) * rq + nxny * ri2;
+    const double f_i = -k * rinv * (3.0 * rq + nxny);
+    const double e_r = g_r * f_r - g_i * f_i, e_i = g_r * f_i + g_i * f_r;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const double w = nb[b];
+        a[b].gr = fma(g_r, w, a[b].gr);
+        a[b].gi = fma(g_i, w, a[b].gi);
+        a[b].hr = fma(b_r * rny, w, a[b].hr);
+        a[b].hi = fma(b_i * rny, w, a[b].hi);
+        a[b].tr = fma(b_r * rnx, w, a[b].tr);
+        a[b].ti = fma(b_i * rnx, w, a[b].ti);
+        a[b].er = fma(e_r, w, a[b].er);
+        a[b].ei = fma(e_i, w, a[b].ei);
+    }
+}
+
+// Discontinuous linear Tri3 basis N_b = 2 lambda_b - 1/3 (crates/sonium-bem/src/core/mesh/
+// element.rs:229-236).
+__device__ __forceinline__ void lin_basis(double s, double t, double nb[3]) {
+    nb[0] = 2.0 * (1.0 - s - t) - 1.0 / 3.0;
+    nb[1] = 2.0 * s - 1.0 / 3.0;
+    nb[2] = 2.0 * t - 1.0 / 3.0;
+}
+
+// Evaluates the regular-integration channels of field element j seen from the point x with
+// normal nx into lane-partial sums: NB = 1 the constant basis, NB = 3 the linear basis weights.
+template <int NB>
+__device__ void near_channels_at(Acc* a, NearWarpSmem& S, const double* __restrict__ elem, int64_t ld,
+                                 double x0, double x1, double x2, double nxx, double nxy, double nxz,
+                                 int64_t j, double k, double k2, int lane) {
     double V[3][3];
     for (int t = 0; t < 3; ++t)
         for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, j);
@@ -971,7 +1014,14 @@ __device__ void near_pair_channels(Acc& a, NearWarpSmem& S, const double* __rest
             const double dis = sqrt(dx * dx + dy * dy + dz * dz);
             if (!(dis >= 1e-15)) continue;
             const double rinv = 1.0 / dis;
-            point_channels(a, dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
+            if constexpr (NB == 1) {
+                point_channels(a[0], dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
+            } else {
+                double nb[3];
+                lin_basis(xio, eto, nb);
+                point_channels_w<NB>(a, nb, dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k,
+                                     k2);
+            }
         }
         total += keep;
         __syncwarp();
@@ -979,6 +1029,14 @@ __device__ void near_pair_channels(Acc& a, NearWarpSmem& S, const double* __rest
         nsel = min(nsub, 15) * 4;
         cur = nxt;
     }
+}
+
+// The constant basis: pair (i, j) seen from the centroid of element i.
+__device__ __forceinline__ void near_pair_channels(Acc& a, NearWarpSmem& S, const double* __restrict__ elem,
+                                                   int64_t ld, int64_t i, int64_t j, double k, double k2,
+                                                   int lane) {
+    near_channels_at<1>(&a, S, elem, ld, E(ECX, i), E(ECY, i), E(ECZ, i), E(ENX, i), E(ENY, i), E(ENZ, i), j, k,
+                        k2, lane);
 }
 
 __device__ __forceinline__ Acc warp_reduce(const Acc& a) {
@@ -1160,6 +1218,363 @@ __global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, i
     self_channels(a, elem, ld, i, k, lane);
     const Acc t = warp_reduce(a);
     if (lane == 0) self_store(t, coef, ld, n, i, A64, A32, lda32, self_rhs, diag);
+}
+
+// =============================================================================================
+// Discontinuous linear Tri3 basis (build_tbem_system_linear, crates/sonium-bem/src/core/assembly/
+// tbem.rs:1490-1620): DOF 3e + c of element e is collocated at local point c of (1/6, 1/6),
+// (2/3, 1/6), (1/6, 2/3) (mesh/element.rs:91-99) with the element's flat normal; the row of
+// that DOF holds, for every field element j, the three basis-weighted integrals in columns
+// 3j + b. FP64 throughout (complex128 matrix).
+// =============================================================================================
+__constant__ double c_lin_coll[3][2] = {{1.0 / 6.0, 1.0 / 6.0}, {2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}};
+constexpr int kLinRows = 32;
+
+// Collocation points of the 3n rows (local_to_global, element.rs:65-76) and their (flat element)
+// normals, SoA: cp[c * n3 + r], cn[c * n3 + r].
+__global__ void k_lin_points(const double* __restrict__ elem, int64_t n, int64_t ld, double* __restrict__ cp,
+                             double* __restrict__ cn) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t n3 = 3 * n;
+    if (r >= n3) return;
+    const int64_t e = r / 3;
+    const int q = static_cast<int>(r % 3);
+    const double s = c_lin_coll[q][0], t = c_lin_coll[q][1];
+    const double sf[3] = {1.0 - s - t, s, t};
+    for (int c = 0; c < 3; ++c) {
+        double v = 0.0;
+        for (int a = 0; a < 3; ++a) v += sf[a] * E(EV0X + 3 * a + c, e);
+        cp[c * n3 + r] = v;
+        cn[c * n3 + r] = E(ENX + c, e);
+    }
+}
+
+// Incident plane-wave right-hand side at arbitrary collocation points (IncidentField::
+// compute_rhs_with_beta, incident.rs:807-833): points / normals SoA with stride `st`.
+__global__ void k_plane_wave_at(const double* __restrict__ pts, const double* __restrict__ nrm, int64_t np,
+                                int64_t st, const double* __restrict__ dirs, const double2* __restrict__ amps,
+                                int64_t r, double k, double hf, double tau, double2 beta,
+                                double2* __restrict__ rhs) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= np * r) return;
+    const int64_t i = t / r, q = t % r;
+    const double d0 = dirs[3 * q], d1 = dirs[3 * q + 1], d2 = dirs[3 * q + 2];
+    const double2 A = amps ? amps[q] : make_double2(1.0, 0.0);
+    const double kdx = hf * k * (d0 * pts[i] + d1 * pts[st + i] + d2 * pts[2 * st + i]);
+    const double kdn = hf * k * (d0 * nrm[i] + d1 * nrm[st + i] + d2 * nrm[2 * st + i]);
+    double s, c;
+    sb_sincos(kdx, &s, &c);
+    const double2 p = cmul(A, make_double2(c, s));
+    const double2 dpdn = make_double2(-kdn * p.y, kdn * p.x);  // i kdn p
+    const double2 bt = cscale(beta, tau);
+    rhs[t] = make_double2(-(p.x + bt.x * dpdn.x - bt.y * dpdn.y), -(p.y + bt.x * dpdn.y + bt.y * dpdn.x));
+}
+
+// Near-pair classification of the 3n collocation rows against the n elements (the element's
+// own row block excluded): pass 0 counts, pass 1 writes the columns in increasing order.
+__global__ void __launch_bounds__(256) k_lin_near_pass(const double* __restrict__ elem, int64_t n, int64_t ld,
+                                                       const double* __restrict__ cp, int pass,
+                                                       int64_t* __restrict__ counts,
+                                                       const int64_t* __restrict__ row_ptr,
+                                                       int32_t* __restrict__ cols) {
+    __shared__ double sx[kNearRows][3];
+    __shared__ unsigned sball[8][kNearRows];
+    __shared__ int64_t sbase[kNearRows];
+    __shared__ int scount[kNearRows];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t n3 = 3 * n;
+    const int64_t row0 = blockIdx.x * (int64_t)kNearRows;
+    if (tid < kNearRows) {
+        const int64_t r = row0 + tid;
+        for (int c = 0; c < 3; ++c) sx[tid][c] = (r < n3) ? cp[c * n3 + r] : 1e300;
+        scount[tid] = 0;
+        sbase[tid] = (pass == 1 && r < n3) ? row_ptr[r] : 0;
+    }
+    __syncthreads();
+    for (int64_t c0 = 0; c0 < n; c0 += 256) {
+        const int64_t j = c0 + tid;
+        double gx = 0, gy = 0, gz = 0, thr = -1.0;
+        if (j < n) {
+            gx = E(EGX, j);
+            gy = E(EGY, j);
+            gz = E(EGZ, j);
+            thr = near_threshold(E(EAREA, j));
+        }
+        for (int rr = 0; rr < kNearRows; ++rr) {
+            const int64_t r = row0 + rr;
+            const bool p = (j < n) && (r < n3) && (j != r / 3) &&
+                           near_superset(gx, gy, gz, thr, sx[rr][0], sx[rr][1], sx[rr][2]);
+            const unsigned b = __ballot_sync(0xffffffffu, p);
+            if (pass == 0) {
+                if (lane == 0 && b) atomicAdd(&scount[rr], __popc(b));
+            } else {
+                if (lane == 0) sball[warp][rr] = b;
+            }
+        }
+        if (pass == 1) {
+            __syncthreads();
+            for (int rr = 0; rr < kNearRows; ++rr) {
+                const unsigned b = sball[warp][rr];
+                if (b & (1u << lane)) {
+                    int before = __popc(b & ((1u << lane) - 1u));
+                    for (int w = 0; w < warp; ++w) before += __popc(sball[w][rr]);
+                    cols[sbase[rr] + scount[rr] + before] = static_cast<int32_t>(j);
+                }
+            }
+            __syncthreads();
+            if (tid < kNearRows) {
+                int add = 0;
+                for (int w = 0; w < 8; ++w) add += __popc(sball[w][tid]);
+                scount[tid] += add;
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    if (pass == 0 && tid < kNearRows && row0 + tid < n3) counts[row0 + tid] = scount[tid];
+}
+
+// Far field of the linear basis: one thread per field element (128-column tiles), 32 rows per
+// CTA; the element's 13-point leaf (the reference's single far leaf) staged in shared memory,
+// the three basis values of each point from the rule's reference coordinates.
+__global__ void __launch_bounds__(kFarTile) k_lin_far(const double* __restrict__ qp, const double* __restrict__ elem,
+                                                      int64_t n, int64_t ld, const double* __restrict__ cp,
+                                                      const double* __restrict__ coef, double k,
+                                                      double2* __restrict__ A) {
+    extern __shared__ __align__(128) double smem[];
+    double* sq = smem;                   // [13][4][kFarTile]
+    double* sr = smem + kQpTileDoubles;  // [kLinRows][6]
+    const int tid = threadIdx.x;
+    const int64_t tile = blockIdx.x;
+    const int64_t j = tile * kFarTile + tid;
+    const int64_t n3 = 3 * n;
+    const int64_t row0 = blockIdx.y * (int64_t)kLinRows;
+    const double k2 = k * k;
+    const double* src = qp + tile * (int64_t)kQpTileDoubles;
+    for (int t = tid; t < kQpTileDoubles; t += kFarTile) sq[t] = src[t];
+    for (int t = tid; t < kLinRows * 6; t += kFarTile) {
+        const int rr = t / 6, f = t % 6;
+        const int64_t r = row0 + rr;
+        double v = 0.0;
+        if (r < n3) v = f < 3 ? cp[f * n3 + r] : E(ENX + (f - 3), r / 3);
+        sr[t] = v;
+    }
+    double nyx = 0, nyy = 0, nyz = 0, gx = 0, gy = 0, gz = 0, thr = -1;
+    if (j < n) {
+        nyx = E(ENX, j);
+        nyy = E(ENY, j);
+        nyz = E(ENZ, j);
+        gx = E(EGX, j);
+        gy = E(EGY, j);
+        gz = E(EGZ, j);
+        thr = near_threshold(E(EAREA, j));
+    }
+    __syncthreads();
+    const int64_t rows_here = (n3 - row0 < kLinRows) ? (n3 - row0) : kLinRows;
+    for (int rr = 0; rr < rows_here; ++rr) {
+        const int64_t r = row0 + rr;
+        const double xx = sr[rr * 6 + 0], xy = sr[rr * 6 + 1], xz = sr[rr * 6 + 2];
+        const double nxx = sr[rr * 6 + 3], nxy = sr[rr * 6 + 4], nxz = sr[rr * 6 + 5];
+        const bool active = (j < n) && (j != r / 3) && !near_superset(gx, gy, gz, thr, xx, xy, xz);
+        if (!active) continue;
+        Acc a[3];
+        for (int q = 0; q < kFarPoints; ++q) {
+            const double* p = sq + q * 4 * kFarTile + tid;
+            const double dx = p[0] - xx, dy = p[kFarTile] - xy, dz = p[2 * kFarTile] - xz;
+            const double w = p[3 * kFarTile];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            const double rinv = sb_rsqrt2(d2);
+            double nb[3];
+            lin_basis(c_tri_xi[c_tri_off[0] + q], c_tri_eta[c_tri_off[0] + q], nb);  // the 13-point leaf
+            point_channels_w<3>(a, nb, dx, dy, dz, d2 * rinv, rinv, w, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
+        }
+        for (int b = 0; b < 3; ++b) A[r * n3 + 3 * j + b] = combine(a[b], coef, ld, j, CF_CG);
+    }
+}
+
+__device__ __forceinline__ Acc lin_reduce(const Acc& a) { return warp_reduce(a); }
+
+// Near pairs of the linear basis: one warp per (collocation row, field element) pair.
+__global__ void __launch_bounds__(32 * kNearWarps) k_lin_near(const double* __restrict__ elem, int64_t n, int64_t ld,
+                                                              const double* __restrict__ cp,
+                                                              const int64_t* __restrict__ row_ptr,
+                                                              const int32_t* __restrict__ cols, int64_t nnz,
+                                                              const double* __restrict__ coef, double k,
+                                                              double2* __restrict__ A) {
+    __shared__ NearWarpSmem sm[kNearWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t p = blockIdx.x * (int64_t)kNearWarps + warp;
+    if (p >= nnz) return;
+    const int64_t n3 = 3 * n;
+    int64_t lo = 0, hi = n3 - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (row_ptr[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    const int64_t r = lo, j = cols[p], e = r / 3;
+    Acc a[3];
+    near_channels_at<3>(a, sm[warp], elem, ld, cp[r], cp[n3 + r], cp[2 * n3 + r], E(ENX, e), E(ENY, e), E(ENZ, e),
+                        j, k, k * k, lane);
+    Acc t[3];
+    for (int b = 0; b < 3; ++b) t[b] = lin_reduce(a[b]);
+    if (lane == 0)
+        for (int b = 0; b < 3; ++b) A[r * n3 + 3 * j + b] = combine(t[b], coef, ld, j, CF_CG);
+}
+// Self element of the linear basis (singular_integration_linear_with_params_mode, integration/
+// singular.rs:868-1170): one warp per collocation row. The regularised edge integral of E is
+// weighted by the basis at the edge point; the centroid-centred Duffy sub-triangles give G, H,
+// H^T and the area part of E, k^2 (n_x . n_y) G N_b plus the basis-gradient term
+// (-(n_x . n_y)(grad N_b . r_hat) + (r_hat . n_y)(grad N_b . n_x)) times G (-1/r + i k). The
+// free term of the row's element goes on the diagonal.
+__global__ void __launch_bounds__(128) k_lin_self(const double* __restrict__ elem, int64_t n, int64_t ld,
+                                                  const double* __restrict__ cp, const double* __restrict__ coef,
+                                                  double k, double2* __restrict__ A, double2* __restrict__ diag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t n3 = 3 * n;
+    const int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp;
+    if (r >= n3) return;
+    const int64_t i = r / 3;
+    const double k2 = k * k;
+    const double x0 = cp[r], x1 = cp[n3 + r], x2 = cp[2 * n3 + r];
+    const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
+    const double nyx = nxx, nyy = nxy, nyz = nxz;
+    const double jac = E(EJAC, i);
+    double V[3][3];
+    for (int t = 0; t < 3; ++t)
+        for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, i);
+    // panel_basis_gradients (singular.rs:1173-1258): constant surface gradients of N_b.
+    double grad[3][3];
+    {
+        const double der[3][2] = {{-2.0, -2.0}, {2.0, 0.0}, {0.0, 2.0}};
+        double ts[3], tt[3];
+        for (int c = 0; c < 3; ++c) {
+            ts[c] = -V[0][c] + V[1][c] + 0.0 * V[2][c];
+            tt[c] = -V[0][c] + 0.0 * V[1][c] + V[2][c];
+        }
+        double ss = 0, tq = 0, st = 0;
+        for (int c = 0; c < 3; ++c) {
+            ss += ts[c] * ts[c];
+            tq += tt[c] * tt[c];
+            st += ts[c] * tt[c];
+        }
+        const double det = ss * tq - st * st;
+        for (int b = 0; b < 3; ++b) {
+            const double ga = (tq * der[b][0] - st * der[b][1]) / det;
+            const double gb = (ss * der[b][1] - st * der[b][0]) / det;
+            for (int c = 0; c < 3; ++c) grad[b][c] = ga * ts[c] + gb * tt[c];
+        }
+    }
+    const double ka = k * fmax(sqrt(E(EAREA, i)), 1e-10);
+    int ngpo1, nsub, nsec1, nsec2;
+    if (ka < 0.3) { ngpo1 = 3; nsub = 4; nsec1 = 4; nsec2 = 2; }
+    else if (ka < 1.0) { ngpo1 = 4; nsub = 5; nsec1 = 6; nsec2 = 2; }
+    else if (ka < 2.0) { ngpo1 = 5; nsub = 6; nsec1 = 8; nsec2 = 3; }
+    else { ngpo1 = 6; nsub = 7; nsec1 = 10; nsec2 = 4; }
+    const int ego = ngpo1 * (ngpo1 - 1) / 2, sgo = nsub * (nsub - 1) / 2;
+    const int n_edge = nsec1 * ngpo1, n_bulk = nsec2 * nsub * nsub;
+    const int per_edge = n_edge + n_bulk;
+    const double csi6[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+    const double eta6[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
+    Acc a[3];
+    for (int f = lane; f < 3 * per_edge; f += 32) {
+        const int ieg = f / per_edge, rem = f % per_edge;
+        const int ig1 = (ieg + 1) % 3, ig2 = ieg + 3;
+        if (rem < n_edge) {
+            const int isec = rem / ngpo1, ig = rem % ngpo1;
+            double dp[3], leneg = 0.0;
+            for (int c = 0; c < 3; ++c) {
+                dp[c] = V[ig1][c] - V[ieg][c];
+                leneg += dp[c] * dp[c];
+            }
+            leneg = sqrt(leneg);
+            const double to0 = dp[0] / leneg, to1 = dp[1] / leneg, to2 = dp[2] / leneg;
+            const double leneg_scaled = leneg / (2.0 * nsec1);
+            const double delsec = 2.0 / nsec1;
+            double secmid = -1.0 - delsec / 2.0;
+            for (int sct = 0; sct <= isec; ++sct) secmid += delsec;
+            const double sga = secmid + c_gl_x[ego + ig] / nsec1;
+            const double wga = c_gl_w[ego + ig] * leneg_scaled;
+            const double dx = V[ieg][0] + dp[0] * (sga + 1.0) / 2.0 - x0;
+            const double dy = V[ieg][1] + dp[1] * (sga + 1.0) / 2.0 - x1;
+            const double dz = V[ieg][2] + dp[2] * (sga + 1.0) / 2.0 - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            double sn, cs;
+            sb_sincos(k * dis, &sn, &cs);
+            const double g_r = cs * kInv4Pi * rinv, g_i = sn * kInv4Pi * rinv;
+            const double f_r = -g_r * rinv - g_i * k, f_i = g_r * k - g_i * rinv;
+            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+            const double cr = (uy * to2 - uz * to1) * nxx + (uz * to0 - ux * to2) * nxy + (ux * to1 - uy * to0) * nxz;
+            const double te = (sga + 1.0) / 2.0;
+            double nb[3];
+            lin_basis(csi6[ieg] * (1.0 - te) + csi6[ig1] * te, eta6[ieg] * (1.0 - te) + eta6[ig1] * te, nb);
+            for (int b = 0; b < 3; ++b) {
+                a[b].er += f_r * cr * wga * nb[b];
+                a[b].ei += f_i * cr * wga * nb[b];
+            }
+        } else {
+            const int r2 = rem - n_edge;
+            const int isec = r2 / (nsub * nsub), ab = r2 % (nsub * nsub);
+            const int ia = ab / nsub, ib = ab % nsub;
+            const double aresub = 1.0 / 24.0 / nsec2;
+            double ss[3], ts[3];
+            ss[0] = ts[0] = 1.0 / 3.0;
+            if (isec == 0) {
+                ss[1] = csi6[ieg]; ss[2] = csi6[ig2]; ts[1] = eta6[ieg]; ts[2] = eta6[ig2];
+            } else {
+                ss[1] = csi6[ig2]; ss[2] = csi6[ig1]; ts[1] = eta6[ig2]; ts[2] = eta6[ig1];
+            }
+            const double sga = c_gl_x[sgo + ia], tga = c_gl_x[sgo + ib];
+            const double wei = c_gl_w[sgo + ia] * c_gl_w[sgo + ib];
+            const double sgg = 0.5 * (1.0 - sga) * ss[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ss[1] + (1.0 + tga) * ss[2]);
+            const double tgg = 0.5 * (1.0 - sga) * ts[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ts[1] + (1.0 + tga) * ts[2]);
+            const double sf0 = 1.0 - sgg - tgg;
+            const double dx = sf0 * V[0][0] + sgg * V[1][0] + tgg * V[2][0] - x0;
+            const double dy = sf0 * V[0][1] + sgg * V[1][1] + tgg * V[2][1] - x1;
+            const double dz = sf0 * V[0][2] + sgg * V[1][2] + tgg * V[2][2] - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            const double wga = wei * (1.0 + sga) * aresub * jac;
+            double sn, cs;
+            sb_sincos(k * dis, &sn, &cs);
+            const double gs = wga * kInv4Pi * rinv;
+            const double g_r = cs * gs, g_i = sn * gs;
+            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+            const double rny = ux * nyx + uy * nyy + uz * nyz;
+            const double rnx = -(ux * nxx + uy * nxy + uz * nxz);
+            const double b_r = -g_r * rinv - g_i * k, b_i = g_r * k - g_i * rinv;
+            const double nd = nxx * nyx + nxy * nyy + nxz * nyz;
+            double nb[3];
+            lin_basis(sgg, tgg, nb);
+            for (int b = 0; b < 3; ++b) {
+                const double w = nb[b];
+                a[b].gr += g_r * w; a[b].gi += g_i * w;
+                a[b].hr += b_r * rny * w; a[b].hi += b_i * rny * w;
+                a[b].tr += b_r * rnx * w; a[b].ti += b_i * rnx * w;
+                const double gr = grad[b][0] * ux + grad[b][1] * uy + grad[b][2] * uz;
+                const double gsn = grad[b][0] * nxx + grad[b][1] * nxy + grad[b][2] * nxz;
+                const double gf = -nd * gr + rny * gsn;
+                a[b].er += g_r * k2 * nd * w + b_r * gf;
+                a[b].ei += g_i * k2 * nd * w + b_i * gf;
+            }
+        }
+    }
+    Acc t[3];
+    for (int b = 0; b < 3; ++b) t[b] = warp_reduce(a[b]);
+    if (lane == 0) {
+        const int c = static_cast<int>(r % 3);
+        for (int b = 0; b < 3; ++b) {
+            double2 v = combine(t[b], coef, ld, i, CF_CG);
+            if (b == c) {
+                v.x += coef[(int64_t)(CF_DIAG) * ld + i];
+                v.y += coef[(int64_t)(CF_DIAG + 1) * ld + i];
+                diag[r] = v;
+            }
+            A[r * n3 + 3 * i + b] = v;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1496,6 +1911,128 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     op.phys = ph;
     op.beta_re = beta_re;
     op.beta_im = beta_im;
+}
+
+// build_tbem_system_linear on the device: collocation points and the near-pair CSR of the 3n
+// rows once per operator, then coefficients, far tiles, near pairs and self rows per assembly.
+void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
+    Mesh& m = *op.mesh;
+    SB_CUDA(cudaSetDevice(m.device));
+    SB_REQUIRE(!m.any_bc_value, SB_ERR_INVALID_ARGUMENT,
+               "linear basis: prescribed boundary values are not supported (rigid, pressure-release with zero "
+               "value, or admittance surfaces)");
+    maybe_inject(SB_INJECT_LAUNCH);
+    const int64_t n = m.n, ld = m.ld, n3 = 3 * n;
+    const cudaStream_t s = op.stream;
+    if (!op.coef.p) op.coef.alloc(sizeof(double) * CF_FIELDS * ld);
+    if (!op.diag.p) op.diag.alloc(sizeof(double2) * n3);
+    if (!op.rhs.p) {
+        op.rhs.alloc(sizeof(double2) * n3);
+        SB_CUDA(cudaMemsetAsync(op.rhs.p, 0, sizeof(double2) * n3, s));
+    }
+    if (!op.lin_cp.p) {
+        op.lin_cp.alloc(sizeof(double) * 3 * n3);
+        op.lin_cn.alloc(sizeof(double) * 3 * n3);
+        k_lin_points<<<cdiv(n3, 256), 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
+                                                   op.lin_cn.as<double>());
+        count_launch();
+        DevBuf counts;
+        counts.alloc(sizeof(int64_t) * (n3 + 1));
+        const int64_t nblk = cdiv(n3, kNearRows);
+        k_lin_near_pass<<<nblk, 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), 0,
+                                             counts.as<int64_t>(), nullptr, nullptr);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        std::vector<int64_t> cnt(n3), ptr(n3 + 1);
+        SB_CUDA(cudaMemcpyAsync(cnt.data(), counts.p, sizeof(int64_t) * n3, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        ptr[0] = 0;
+        for (int64_t r = 0; r < n3; ++r) ptr[r + 1] = ptr[r] + cnt[r];
+        op.lin_nnz = ptr[n3];
+        op.lin_ptr.alloc(sizeof(int64_t) * (n3 + 1));
+        SB_CUDA(cudaMemcpyAsync(op.lin_ptr.p, ptr.data(), sizeof(int64_t) * (n3 + 1), cudaMemcpyHostToDevice, s));
+        op.lin_col.alloc(sizeof(int32_t) * std::max<int64_t>(op.lin_nnz, 1));
+        k_lin_near_pass<<<nblk, 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), 1, nullptr,
+                                             op.lin_ptr.as<int64_t>(), op.lin_col.as<int32_t>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        SB_CUDA(cudaStreamSynchronize(s));
+    }
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    k_coefficients<<<cdiv(ld, 256), 256, 0, s>>>(n, ld, m.bc_kind.as<int32_t>(), m.bc_value.as<double2>(),
+                                                 m.has_adm.as<uint8_t>(), m.adm.as<double2>(), ph.tau,
+                                                 ph.pressure_factor, make_double2(beta_re, beta_im),
+                                                 op.coef.as<double>());
+    count_launch();
+    const double k = ph.harmonic_factor * ph.wave_number;
+    double2* A = op.A64.as<double2>();
+    {
+        ProfScope prof(SB_PROF_FAR, s);
+        const size_t sm = sizeof(double) * (kQpTileDoubles + kLinRows * 6);
+        SB_CUDA(cudaFuncSetAttribute(k_lin_far, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n3, kLinRows)));
+        k_lin_far<<<grid, kFarTile, sm, s>>>(m.qp.as<double>(), m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
+                                             op.coef.as<double>(), k, A);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    if (op.lin_nnz > 0) {
+        ProfScope prof(SB_PROF_NEAR, s);
+        k_lin_near<<<cdiv(op.lin_nnz, kNearWarps), 32 * kNearWarps, 0, s>>>(
+            m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), op.lin_ptr.as<int64_t>(), op.lin_col.as<int32_t>(),
+            op.lin_nnz, op.coef.as<double>(), k, A);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    {
+        ProfScope prof(SB_PROF_SELF, s);
+        k_lin_self<<<cdiv(n3, 4), 128, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
+                                              op.coef.as<double>(), k, A, op.diag.as<double2>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    SB_CUDA(cudaEventRecord(e1, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    op.last_assembly_ms = ms;
+    op.phys = ph;
+    op.beta_re = beta_re;
+    op.beta_im = beta_im;
+}
+
+void lin_collocation(const Mesh& m, double* cp_dev, double* cn_dev) {
+    SB_CUDA(cudaSetDevice(m.device));
+    k_lin_points<<<cdiv(3 * m.n, 256), 256>>>(m.elem.as<double>(), m.n, m.ld, cp_dev, cn_dev);
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaDeviceSynchronize());
+}
+
+void incident_plane_wave_at(int device, const double* pts_dev, const double* nrm_dev, int64_t np, int64_t stride,
+                            const sb_physics& ph, double beta_re, double beta_im, const double* dirs_host,
+                            const double* amps_host, int64_t r, double2* rhs_dev, cudaStream_t s) {
+    SB_CUDA(cudaSetDevice(device));
+    DevBuf dd, da;
+    dd.alloc(sizeof(double) * 3 * r);
+    SB_CUDA(cudaMemcpyAsync(dd.p, dirs_host, sizeof(double) * 3 * r, cudaMemcpyHostToDevice, s));
+    if (amps_host) {
+        da.alloc(sizeof(double2) * r);
+        SB_CUDA(cudaMemcpyAsync(da.p, amps_host, sizeof(double2) * r, cudaMemcpyHostToDevice, s));
+    }
+    ProfScope prof(SB_PROF_OTHER, s);
+    k_plane_wave_at<<<cdiv(np * r, 256), 256, 0, s>>>(pts_dev, nrm_dev, np, stride, dd.as<double>(),
+                                                      amps_host ? da.as<double2>() : nullptr, r, ph.wave_number,
+                                                      ph.harmonic_factor, ph.tau, make_double2(beta_re, beta_im),
+                                                      rhs_dev);
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(s));
 }
 
 void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst* d_inst, DevBuf& pre_buf,

@@ -393,7 +393,108 @@ SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_compl
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
         tensor_release(*op->op);
-        assemble(*op->op, *physics, beta.re, beta.im);
+        if (op->op->basis == SB_BASIS_LINEAR)
+            assemble_linear(*op->op, *physics, beta.re, beta.im);
+        else
+            assemble(*op->op, *physics, beta.re, beta.im);
+    });
+}
+
+SB_API int sb_assemble_linear(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta, sb_operator** out) {
+    return guarded([&] {
+        SB_REQUIRE(mesh && mesh->m && physics && out, SB_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
+        check_beta(beta);
+        Mesh& m = *mesh->m;
+        if (!m.bc_kind.p) mesh_set_bc(m, nullptr, nullptr, nullptr, nullptr);
+        SB_REQUIRE(!m.any_bc_value, SB_ERR_INVALID_ARGUMENT,
+                   "linear basis: prescribed boundary values are not supported (rigid, zero-pressure or "
+                   "admittance surfaces)");
+        SB_CUDA(cudaSetDevice(m.device));
+        Operator* op = new Operator();
+        try {
+            op->mesh = &m;
+            op->device = m.device;
+            op->precision = SB_PRECISION_FP64;
+            op->basis = SB_BASIS_LINEAR;
+            op->n = 3 * m.n;
+            op->lda32 = (op->n + 1) / 2 * 2;
+            SB_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
+            op->A64.alloc(sizeof(double2) * op->n * op->n);
+            assemble_linear(*op, *physics, beta.re, beta.im);
+        } catch (...) {
+            if (op->stream) cudaStreamDestroy(op->stream);
+            delete op;
+            throw;
+        }
+        *out = new sb_operator{op};
+    });
+}
+
+SB_API int sb_mesh_collocation(const sb_mesh* mesh, int basis, double* points, double* normals) {
+    return guarded([&] {
+        SB_REQUIRE(mesh && mesh->m && points && normals, SB_ERR_INVALID_ARGUMENT, "null argument");
+        SB_REQUIRE(basis == SB_BASIS_CONSTANT || basis == SB_BASIS_LINEAR, SB_ERR_INVALID_ARGUMENT, "unknown basis");
+        const Mesh& m = *mesh->m;
+        if (basis == SB_BASIS_CONSTANT) {
+            for (int64_t e = 0; e < m.n; ++e)
+                for (int c = 0; c < 3; ++c) {
+                    points[3 * e + c] = m.h_elem[(ECX + c) * m.ld + e];
+                    normals[3 * e + c] = m.h_elem[(ENX + c) * m.ld + e];
+                }
+            return;
+        }
+        // The linear rows' points from a temporary linear operator shell (same kernel as assembly).
+        SB_CUDA(cudaSetDevice(m.device));
+        Operator tmp;
+        tmp.mesh = const_cast<Mesh*>(&m);
+        tmp.device = m.device;
+        const int64_t n3 = 3 * m.n;
+        tmp.lin_cp.alloc(sizeof(double) * 3 * n3);
+        tmp.lin_cn.alloc(sizeof(double) * 3 * n3);
+        lin_collocation(m, tmp.lin_cp.as<double>(), tmp.lin_cn.as<double>());
+        std::vector<double> cp(3 * n3), cn(3 * n3);
+        SB_CUDA(cudaMemcpy(cp.data(), tmp.lin_cp.p, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost));
+        SB_CUDA(cudaMemcpy(cn.data(), tmp.lin_cn.p, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost));
+        for (int64_t r = 0; r < n3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                points[3 * r + c] = cp[c * n3 + r];
+                normals[3 * r + c] = cn[c * n3 + r];
+            }
+    });
+}
+
+SB_API int sb_rhs_plane_wave_points(int device, int64_t np, const double* points, const double* normals,
+                                    const sb_physics* physics, sb_complex beta, const double* dirs,
+                                    const sb_complex* amps, int64_t r, sb_complex* rhs) {
+    return guarded([&] {
+        SB_REQUIRE(points && normals && physics && dirs && rhs && np >= 1 && r >= 1, SB_ERR_INVALID_ARGUMENT,
+                   "bad argument");
+        SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
+        check_beta(beta);
+        for (int64_t q = 0; q < 3 * r; ++q)
+            SB_REQUIRE(std::isfinite(dirs[q]), SB_ERR_INVALID_ARGUMENT, "non-finite direction");
+        for (int64_t i = 0; i < 3 * np; ++i)
+            SB_REQUIRE(std::isfinite(points[i]) && std::isfinite(normals[i]), SB_ERR_NOT_FINITE,
+                       "non-finite collocation point or normal");
+        int count = 0;
+        SB_CUDA(cudaGetDeviceCount(&count));
+        SB_REQUIRE(device >= 0 && device < count, SB_ERR_INVALID_ARGUMENT, "no such device");
+        SB_CUDA(cudaSetDevice(device));
+        std::vector<double> soa(6 * np);
+        for (int64_t i = 0; i < np; ++i)
+            for (int c = 0; c < 3; ++c) {
+                soa[c * np + i] = points[3 * i + c];
+                soa[(3 + c) * np + i] = normals[3 * i + c];
+            }
+        DevBuf dp, dr;
+        dp.alloc(sizeof(double) * 6 * np);
+        dr.alloc(sizeof(double2) * np * r);
+        SB_CUDA(cudaMemcpy(dp.p, soa.data(), sizeof(double) * 6 * np, cudaMemcpyHostToDevice));
+        incident_plane_wave_at(device, dp.as<double>(), dp.as<double>() + 3 * np, np, np, *physics, beta.re, beta.im,
+                               dirs, reinterpret_cast<const double*>(amps), r, dr.as<double2>(), 0);
+        SB_CUDA(cudaMemcpy(rhs, dr.p, sizeof(double2) * np * r, cudaMemcpyDeviceToHost));
     });
 }
 
@@ -804,6 +905,12 @@ SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs, c
             SB_REQUIRE(std::isfinite(dirs[q]), SB_ERR_INVALID_ARGUMENT, "non-finite direction");
         const Operator& o = *op->op;
         SB_REQUIRE(o.mesh, SB_ERR_INVALID_ARGUMENT, "operator was not assembled from a mesh");
+        if (o.basis == SB_BASIS_LINEAR) {
+            incident_plane_wave_at(o.device, o.lin_cp.as<double>(), o.lin_cn.as<double>(), o.n, o.n, o.phys, o.beta_re,
+                                   o.beta_im, dirs, reinterpret_cast<const double*>(amps), r,
+                                   reinterpret_cast<double2*>(rhs_dev), o.stream);
+            return;
+        }
         incident_plane_wave(*o.mesh, o.phys, o.beta_re, o.beta_im, dirs, reinterpret_cast<const double*>(amps), r,
                             reinterpret_cast<double2*>(rhs_dev), o.stream, false);
     });

@@ -120,6 +120,15 @@ class Mesh:
         check(L.load().sb_mesh_element_geometry(self.handle, _p(c), _p(n), _p(a)))
         return c, n, a
 
+    def collocation(self, basis: int = L.SB_BASIS_CONSTANT):
+        """Collocation points and normals of a basis: (m, 3) each for the constant basis (centroids),
+        (3m, 3) for the linear basis (DOF 3e + c)."""
+        rows = self.num_elements * (3 if basis == L.SB_BASIS_LINEAR else 1)
+        pts = np.zeros((rows, 3))
+        nrm = np.zeros((rows, 3))
+        check(L.load().sb_mesh_collocation(self.handle, basis, _p(pts), _p(nrm)))
+        return pts, nrm
+
     def set_boundary_conditions(self, kind=None, value=None, admittance=None):
         """Per-element BoundaryCondition; ``admittance`` uses NaN for 'no admittance'."""
         m = self.num_elements
@@ -173,6 +182,7 @@ class TbemOperator(LinearOperator):
         self.beta = beta
         self.precision = precision
         self.n = mesh.num_elements
+        self.basis = L.SB_BASIS_CONSTANT
 
     @property
     def handle(self):
@@ -294,6 +304,36 @@ def build_tbem_system_with_beta(mesh: Mesh, physics: PhysicsParams, beta: comple
     check(L.load().sb_assemble(mesh.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag),
                                precision, ct.byref(h)))
     return TbemOperator(mesh, h, physics, beta, precision)
+
+
+def build_tbem_system_linear(mesh: Mesh, physics: PhysicsParams, beta: complex) -> TbemOperator:
+    """build_tbem_system_linear (tbem.rs:1490-1620): the discontinuous linear Tri3 basis, three DOFs
+    per element (DOF 3e + c), a 3m x 3m complex128 operator on the device."""
+    h = ct.c_void_p()
+    check(L.load().sb_assemble_linear(mesh.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag),
+                                      ct.byref(h)))
+    op = TbemOperator(mesh, h, physics, beta, L.SB_PRECISION_FP64)
+    op.n = 3 * mesh.num_elements
+    op.basis = L.SB_BASIS_LINEAR
+    return op
+
+
+def rhs_plane_wave_at(points, normals, physics: PhysicsParams, beta: complex, directions, amplitudes=None,
+                      device: int = 0) -> np.ndarray:
+    """IncidentField::compute_rhs_with_beta (incident.rs:807-833) at arbitrary collocation points
+    and normals (np x 3 each), computed on the device: (np, r) complex128."""
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    nrm = np.ascontiguousarray(normals, np.float64).reshape(-1, 3)
+    if pts.shape != nrm.shape:
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "points and normals must have the same shape")
+    d = np.ascontiguousarray(np.atleast_2d(directions), np.float64)
+    r = d.shape[0]
+    a = None if amplitudes is None else _c128(np.broadcast_to(amplitudes, (r,)))
+    out = np.zeros((pts.shape[0], r), np.complex128)
+    check(L.load().sb_rhs_plane_wave_points(device, pts.shape[0], _p(pts), _p(nrm), ct.byref(physics._struct()),
+                                            L.SbComplex(beta.real, beta.imag), _p(d), None if a is None else _p(a),
+                                            r, _p(out)))
+    return out
 
 
 def build_tbem_system(mesh: Mesh, physics: PhysicsParams, precision: int = L.SB_PRECISION_FP64) -> TbemOperator:
