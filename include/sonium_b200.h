@@ -152,10 +152,18 @@ SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_compl
  * frequency; sb_rhs_plane_wave_device evaluates the incident field at its collocation points. */
 #define SB_BASIS_CONSTANT 0
 #define SB_BASIS_LINEAR 1
+#define SB_BASIS_QUADRATIC 2
 SB_API int sb_assemble_linear(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta,
                               sb_operator** out);
+/* build_tbem_system_linear_stabilized / build_tbem_system_quadratic_stabilized (tbem.rs:2993-3030
+ * -> build_tbem_system_discontinuous_stabilized :2810-2990): the same assembly for
+ * SB_BASIS_LINEAR or SB_BASIS_QUADRATIC (six DOFs per element, DOF 6e + c collocated at the
+ * six interior points of element.rs:108-115, quadratic Lagrange basis), every matrix entry
+ * multiplied by sign (+1 or -1); pass beta = burton_miller_beta_scaled(beta_scale). */
+SB_API int sb_assemble_discontinuous(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta,
+                                     int basis, double sign, sb_operator** out);
 /* Collocation points and normals of a basis (host arrays, DOF-major x 3): m of them for
- * SB_BASIS_CONSTANT (the centroids), 3m for SB_BASIS_LINEAR. */
+ * SB_BASIS_CONSTANT (the centroids), 3m for SB_BASIS_LINEAR, 6m for SB_BASIS_QUADRATIC. */
 SB_API int sb_mesh_collocation(const sb_mesh* mesh, int basis, double* points, double* normals);
 /* IncidentField::compute_rhs_with_beta (incident.rs:807-833) for plane waves at np arbitrary
  * collocation points with normals (host arrays np x 3), on the device: rhs[i * r + q]. */

@@ -83,8 +83,11 @@ def _declare(L):
     L.or_field_eval.argtypes = [P, P, ct.c_int64, P, P, ct.c_double, ct.c_double, ct.c_double, P,
                                 ct.c_int64, ct.c_int, P]
     L.or_linear_collocation.argtypes = [ct.c_int64, P, P, P, P]
-    L.or_regular_pair_linear.argtypes = [P, P, P, ct.c_double, ct.POINTER(OrPhysics), P]
-    L.or_singular_pair_linear.argtypes = [P, P, P, ct.POINTER(OrPhysics), P]
+    L.or_regular_pair_disc.argtypes = [P, P, P, ct.c_double, ct.POINTER(OrPhysics), ct.c_int, P]
+    L.or_singular_pair_disc.argtypes = [P, P, P, ct.POINTER(OrPhysics), ct.c_int, P]
+    L.or_disc_collocation.argtypes = [ct.c_int64, P, P, ct.c_int, P, P]
+    L.or_assemble_discontinuous.argtypes = [ct.c_int64, P, ct.c_int64, P, ct.POINTER(OrBc), ct.POINTER(OrPhysics),
+                                            OrC128, ct.c_int, ct.c_double, ct.c_int, P, P]
     L.or_assemble_linear.argtypes = [ct.c_int64, P, ct.c_int64, P, ct.POINTER(OrBc), ct.POINTER(OrPhysics),
                                      OrC128, ct.c_int, P, P]
 
@@ -168,48 +171,68 @@ def assemble(nodes, tris, ph: OrPhysics, beta: complex, rows=None, bc_kind=None,
     return A, rhs
 
 
-def linear_collocation(nodes, tris):
-    """Collocation points and normals of the discontinuous linear basis: (3m, 3) each, DOF 3e + c."""
+def disc_collocation(nodes, tris, nbas: int = 3):
+    """Collocation points and normals of a discontinuous basis (nbas 3 or 6): (nbas m, 3) each."""
     nodes = np.ascontiguousarray(nodes, np.float64)
     tris = np.ascontiguousarray(tris, np.uint32)
     m = tris.shape[0]
-    pts = np.zeros((3 * m, 3))
-    nrm = np.zeros((3 * m, 3))
-    lib().or_linear_collocation(m, _p(nodes), _p(tris), _p(pts), _p(nrm))
+    pts = np.zeros((nbas * m, 3))
+    nrm = np.zeros((nbas * m, 3))
+    lib().or_disc_collocation(m, _p(nodes), _p(tris), nbas, _p(pts), _p(nrm))
     return pts, nrm
 
 
-def assemble_linear(nodes, tris, ph: OrPhysics, beta: complex, bc_kind=None, bc_value=None, admittance=None,
-                    threads: int = 0):
-    """build_tbem_system_linear (tbem.rs:1490-1620): (3m x 3m matrix, 3m rhs)."""
+def linear_collocation(nodes, tris):
+    """Collocation points and normals of the discontinuous linear basis: (3m, 3) each, DOF 3e + c."""
+    return disc_collocation(nodes, tris, 3)
+
+
+def assemble_discontinuous(nodes, tris, ph: OrPhysics, beta: complex, nbas: int = 3, sign: float = 1.0,
+                           bc_kind=None, bc_value=None, admittance=None, threads: int = 0):
+    """build_tbem_system_discontinuous_stabilized (tbem.rs:2810-2990): ((nbas m)^2 matrix, rhs)."""
     nodes = np.ascontiguousarray(nodes, np.float64)
     tris = np.ascontiguousarray(tris, np.uint32)
     m = tris.shape[0]
-    A = np.zeros((3 * m, 3 * m), np.complex128)
-    rhs = np.zeros(3 * m, np.complex128)
+    n = nbas * m
+    A = np.zeros((n, n), np.complex128)
+    rhs = np.zeros(n, np.complex128)
     keep = []
     b = _bc_struct(m, bc_kind, bc_value, admittance, keep)
-    rc = lib().or_assemble_linear(nodes.shape[0], _p(nodes), m, _p(tris), ct.byref(b), ct.byref(ph),
-                                  OrC128(beta.real, beta.imag), threads, _p(A), _p(rhs))
+    rc = lib().or_assemble_discontinuous(nodes.shape[0], _p(nodes), m, _p(tris), ct.byref(b), ct.byref(ph),
+                                         OrC128(beta.real, beta.imag), nbas, float(sign), threads, _p(A), _p(rhs))
     if rc:
         raise ValueError("oracle assembly rejected its input")
     return A, rhs
 
 
-def regular_pair_linear(x, nx, coords, area, ph):
-    """(3, 4) channels (g, h, ht, e) per linear basis function, regular integration."""
-    out = np.zeros(12, np.complex128)
+def assemble_linear(nodes, tris, ph: OrPhysics, beta: complex, bc_kind=None, bc_value=None, admittance=None,
+                    threads: int = 0):
+    """build_tbem_system_linear (tbem.rs:1490-1620): (3m x 3m matrix, 3m rhs)."""
+    return assemble_discontinuous(nodes, tris, ph, beta, 3, 1.0, bc_kind, bc_value, admittance, threads)
+
+
+def regular_pair_disc(x, nx, coords, area, ph, nbas: int = 3):
+    """(nbas, 4) channels (g, h, ht, e) per basis function, regular integration."""
+    out = np.zeros(4 * nbas, np.complex128)
     x, nx, c = (np.ascontiguousarray(v, np.float64) for v in (x, nx, coords))
-    lib().or_regular_pair_linear(_p(x), _p(nx), _p(c), float(area), ct.byref(ph), _p(out))
-    return out.reshape(3, 4)
+    lib().or_regular_pair_disc(_p(x), _p(nx), _p(c), float(area), ct.byref(ph), nbas, _p(out))
+    return out.reshape(nbas, 4)
+
+
+def singular_pair_disc(x, nx, coords, ph, nbas: int = 3):
+    """(nbas, 4) channels (g, h, ht, e) per basis function, self element."""
+    out = np.zeros(4 * nbas, np.complex128)
+    x, nx, c = (np.ascontiguousarray(v, np.float64) for v in (x, nx, coords))
+    lib().or_singular_pair_disc(_p(x), _p(nx), _p(c), ct.byref(ph), nbas, _p(out))
+    return out.reshape(nbas, 4)
+
+
+def regular_pair_linear(x, nx, coords, area, ph):
+    return regular_pair_disc(x, nx, coords, area, ph, 3)
 
 
 def singular_pair_linear(x, nx, coords, ph):
-    """(3, 4) channels (g, h, ht, e) per linear basis function, self element."""
-    out = np.zeros(12, np.complex128)
-    x, nx, c = (np.ascontiguousarray(v, np.float64) for v in (x, nx, coords))
-    lib().or_singular_pair_linear(_p(x), _p(nx), _p(c), ct.byref(ph), _p(out))
-    return out.reshape(3, 4)
+    return singular_pair_disc(x, nx, coords, ph, 3)
 
 
 def regular_pair(x, nx, coords, area, ph):

@@ -1148,20 +1148,51 @@ extern "C" void or_field_eval(const double* nodes, const uint32_t* tris, int64_t
 }
 
 // =============================================================================================
-// Discontinuous linear Tri3 basis: build_tbem_system_linear (crates/sonium-bem/src/core/
-// assembly/tbem.rs:1490-1620) with regular_integration_linear_with_normals (integration/
-// regular.rs:359-470) and singular_integration_linear_with_params_mode (integration/
-// singular.rs:868-1170). Three DOFs per element, collocated at the interior points
-// (1/6, 1/6), (2/3, 1/6), (1/6, 2/3) (mesh/element.rs:91-99), basis 2 lambda_b - 1/3
-// (element.rs:229-236), element e owns DOFs 3e, 3e + 1, 3e + 2.
+// Discontinuous Tri3 bases: build_tbem_system_linear (crates/sonium-bem/src/core/assembly/
+// tbem.rs:1490-1620) and build_tbem_system_discontinuous_stabilized (:2810-2990) with
+// regular_integration_linear_with_normals (integration/regular.rs:359-470) and
+// singular_integration_linear_with_params_mode (integration/singular.rs:868-1170). NB = 3
+// (linear) or 6 (quadratic) DOFs per element, collocated at the interior points of
+// mesh/element.rs:91-115, basis_values of element.rs:229-262; element e owns DOFs NB e + c.
 // =============================================================================================
 namespace {
 
 const double kLinColl[3][2] = {{1.0 / 6.0, 1.0 / 6.0}, {2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}};
+const double kQuadColl[6][2] = {{0.0915762135097715, 0.0915762135097715}, {0.8168475729804585, 0.0915762135097715},
+                                {0.0915762135097715, 0.8168475729804585}, {0.445948490915965, 0.445948490915965},
+                                {0.445948490915965, 0.108103018168070},   {0.108103018168070, 0.445948490915965}};
 
-inline void lin_basis(double s, double t, double nb[3]) {
+inline void coll_local(int nb, int q, double& s, double& t) {
+    s = nb == 6 ? kQuadColl[q][0] : kLinColl[q][0];
+    t = nb == 6 ? kQuadColl[q][1] : kLinColl[q][1];
+}
+
+// basis_values (element.rs:229-262), Tri3: linear 2 lambda - 1/3, quadratic Lagrange.
+inline void panel_basis(int nbas, double s, double t, double nb[6]) {
     const double l[3] = {1.0 - s - t, s, t};
-    for (int b = 0; b < 3; ++b) nb[b] = 2.0 * l[b] - 1.0 / 3.0;
+    if (nbas == 3) {
+        for (int b = 0; b < 3; ++b) nb[b] = 2.0 * l[b] - 1.0 / 3.0;
+        return;
+    }
+    nb[0] = l[0] * (2.0 * l[0] - 1.0);
+    nb[1] = l[1] * (2.0 * l[1] - 1.0);
+    nb[2] = l[2] * (2.0 * l[2] - 1.0);
+    nb[3] = 4.0 * l[0] * l[1];
+    nb[4] = 4.0 * l[1] * l[2];
+    nb[5] = 4.0 * l[2] * l[0];
+}
+
+// Reference derivatives of the basis (panel_basis_gradients, singular.rs:1180-1195).
+inline void panel_deriv(int nbas, double s, double t, double d[6][2]) {
+    if (nbas == 3) {
+        const double dd[3][2] = {{-2.0, -2.0}, {2.0, 0.0}, {0.0, 2.0}};
+        std::memcpy(d, dd, sizeof(dd));
+        return;
+    }
+    const double l = 1.0 - s - t;
+    const double dd[6][2] = {{1.0 - 4.0 * l, 1.0 - 4.0 * l}, {4.0 * s - 1.0, 0.0}, {0.0, 4.0 * t - 1.0},
+                             {4.0 * (l - s), -4.0 * s},      {4.0 * t, 4.0 * s},   {-4.0 * t, 4.0 * (l - t)}};
+    std::memcpy(d, dd, sizeof(dd));
 }
 
 // local_to_global (element.rs:65-76), Tri3 shape functions.
@@ -1173,12 +1204,12 @@ void lin_point(const Coords& c, double s, double t, double x[3]) {
 }
 
 struct Channels3 {
-    Channels b[3];
+    Channels b[6];
 };
 
 // regular_integration_linear_with_normals (regular.rs:359-470), flat normals.
 Channels3 regular_pair_linear(const double x[3], const double nx[3], const Coords& c, double area,
-                              const or_physics& ph) {
+                              const or_physics& ph, int nbas = 3) {
     const double wavruim = ph.harmonic_factor * ph.wave_number;
     const double k2 = ph.wave_number * ph.wave_number;
     Channels3 r;
@@ -1218,9 +1249,9 @@ Channels3 regular_pair_linear(const double x[3], const double nx[3], const Coord
             double dq = dis * dis;
             cd ef((3.0 / dq - k2) * rq + nxny / dq, -wavruim / dis * (3.0 * rq + nxny));
             cd zh = zb * rny, zt = zb * rnx, ze = zg * ef;
-            double nb[3];
-            lin_basis(xio, eto, nb);
-            for (int b = 0; b < 3; ++b) {
+            double nb[6];
+            panel_basis(nbas, xio, eto, nb);
+            for (int b = 0; b < nbas; ++b) {
                 r.b[b].g += zg * nb[b];
                 r.b[b].h += zh * nb[b];
                 r.b[b].ht += zt * nb[b];
@@ -1231,10 +1262,11 @@ Channels3 regular_pair_linear(const double x[3], const double nx[3], const Coord
     return r;
 }
 
-// panel_basis_gradients (singular.rs:1173-1258), Tri3 linear: surface gradients of the three
-// basis functions (constant over a flat panel).
-void lin_gradients(const Coords& c, double grad[3][3]) {
-    const double der[3][2] = {{-2.0, -2.0}, {2.0, 0.0}, {0.0, 2.0}};
+// panel_basis_gradients (singular.rs:1173-1258), Tri3: surface gradients of the basis functions
+// at (s, t) from the panel's tangents and metric.
+void lin_gradients(const Coords& c, int nbas, double s, double t, double grad[6][3]) {
+    double der[6][2];
+    panel_deriv(nbas, s, t, der);
     const double sds[3] = {-1.0, 1.0, 0.0}, sdt[3] = {-1.0, 0.0, 1.0};
     double ts[3] = {0, 0, 0}, tt[3] = {0, 0, 0};
     for (int node = 0; node < 3; ++node)
@@ -1249,7 +1281,7 @@ void lin_gradients(const Coords& c, double grad[3][3]) {
         st += ts[a] * tt[a];
     }
     const double det = ss * tq - st * st;
-    for (int b = 0; b < 3; ++b) {
+    for (int b = 0; b < nbas; ++b) {
         const double ga = (tq * der[b][0] - st * der[b][1]) / det;
         const double gb = (ss * der[b][1] - st * der[b][0]) / det;
         for (int a = 0; a < 3; ++a) grad[b][a] = ga * ts[a] + gb * tt[a];
@@ -1261,7 +1293,7 @@ void lin_gradients(const Coords& c, double grad[3][3]) {
 // point, the centroid-centred Duffy sub-triangles for G, H, H^T and the area part of E
 // (k^2 n_x.n_y G N_b plus the basis-gradient term of the weighted Stokes identity).
 Channels3 singular_pair_linear(const double x[3], const double nx[3], const Coords& c,
-                               const or_physics& ph) {
+                               const or_physics& ph, int nbas = 3) {
     static const double csi6[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
     static const double eta6[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
     const double wavruim = ph.harmonic_factor * ph.wave_number;
@@ -1271,8 +1303,6 @@ Channels3 singular_pair_linear(const double x[3], const double nx[3], const Coor
     gauss_legendre(q.edge_order, ecx, ecw);
     gauss_legendre(q.sub_order, scx, scw);
     const int nsec1 = q.sections, nsec2 = q.subtri;
-    double grad[3][3];
-    lin_gradients(c, grad);
     Channels3 r;
     for (int ieg = 0; ieg < 3; ++ieg) {
         const int ig1 = (ieg + 1) % 3, ig2 = ieg + 3;
@@ -1310,9 +1340,9 @@ Channels3 singular_pair_linear(const double x[3], const double nx[3], const Coor
                 const double te = (sga + 1.0) / 2.0;
                 const double sl = csi6[ieg] * (1.0 - te) + csi6[ig1] * te;
                 const double tl = eta6[ieg] * (1.0 - te) + eta6[ig1] * te;
-                double nb[3];
-                lin_basis(sl, tl, nb);
-                for (int b = 0; b < 3; ++b) r.b[b].e += contrib * nb[b];
+                double nb[6];
+                panel_basis(nbas, sl, tl, nb);
+                for (int b = 0; b < nbas; ++b) r.b[b].e += contrib * nb[b];
             }
         }
         for (int isec = 0; isec < nsec2; ++isec) {
@@ -1354,9 +1384,10 @@ Channels3 singular_pair_linear(const double x[3], const double nx[3], const Coor
                     cd zh = zb * rny, zt = zb * rnx;
                     double nd = nx[0] * ny[0] + nx[1] * ny[1] + nx[2] * ny[2];
                     cd earea = zg * k2 * nd;
-                    double nb[3];
-                    lin_basis(sgg, tgg, nb);
-                    for (int b = 0; b < 3; ++b) {
+                    double nb[6], grad[6][3];
+                    panel_basis(nbas, sgg, tgg, nb);
+                    lin_gradients(c, nbas, sgg, tgg, grad);
+                    for (int b = 0; b < nbas; ++b) {
                         r.b[b].g += zg * nb[b];
                         r.b[b].h += zh * nb[b];
                         r.b[b].ht += zt * nb[b];
@@ -1375,30 +1406,38 @@ Channels3 singular_pair_linear(const double x[3], const double nx[3], const Coor
 
 extern "C" {
 
-// Collocation points and normals of the linear basis: 3 per element (element.rs:91-99 through
-// local_to_global; flat normals, tbem.rs:1516-1527).
-void or_linear_collocation(int64_t n_tris, const double* nodes, const uint32_t* tris, double* points,
-                           double* normals) {
+// Collocation points and normals of a discontinuous basis: nbas per element (element.rs:91-115
+// through local_to_global; flat normals, tbem.rs:1516-1527).
+void or_disc_collocation(int64_t n_tris, const double* nodes, const uint32_t* tris, int nbas, double* points,
+                         double* normals) {
     std::vector<double> centers(3 * n_tris), nrm(3 * n_tris), areas(n_tris);
     element_geometry(n_tris, nodes, tris, centers.data(), nrm.data(), areas.data());
     for (int64_t e = 0; e < n_tris; ++e) {
         Coords c;
         for (int a = 0; a < 3; ++a)
             for (int j = 0; j < 3; ++j) c.v[a][j] = nodes[3 * tris[3 * e + a] + j];
-        for (int q = 0; q < 3; ++q) {
-            lin_point(c, kLinColl[q][0], kLinColl[q][1], points + 3 * (3 * e + q));
-            for (int j = 0; j < 3; ++j) normals[3 * (3 * e + q) + j] = nrm[3 * e + j];
+        for (int q = 0; q < nbas; ++q) {
+            double sq, tq;
+            coll_local(nbas, q, sq, tq);
+            lin_point(c, sq, tq, points + 3 * (nbas * e + q));
+            for (int j = 0; j < 3; ++j) normals[3 * (nbas * e + q) + j] = nrm[3 * e + j];
         }
     }
 }
 
-// build_tbem_system_linear (tbem.rs:1490-1620): A is 3m x 3m row-major, rhs 3m. Prescribed
-// boundary values are read per element (one value; the DOFs of an element share it through
-// add_free_terms' average, tbem.rs:1248-1281, and the field BC's first basis slot).
-int or_assemble_linear(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris,
-                       const or_bc* bc, const or_physics* ph, or_c128 beta_in, int threads, or_c128* A,
-                       or_c128* rhs) {
-    if (m <= 0) return 1;
+void or_linear_collocation(int64_t n_tris, const double* nodes, const uint32_t* tris, double* points,
+                           double* normals) {
+    or_disc_collocation(n_tris, nodes, tris, 3, points, normals);
+}
+
+// build_tbem_system_linear (tbem.rs:1490-1620) and, with nbas 3 or 6 and sign +-1,
+// build_tbem_system_discontinuous_stabilized (:2810-2990): A is (nbas m) x (nbas m) row-major.
+// Prescribed boundary values are read per element (one value; the DOFs of an element share it
+// through the free terms' average, tbem.rs:1248-1281, and the field BC's first basis slot).
+int or_assemble_discontinuous(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris,
+                              const or_bc* bc, const or_physics* ph, or_c128 beta_in, int nbas, double sign,
+                              int threads, or_c128* A, or_c128* rhs) {
+    if (m <= 0 || (nbas != 3 && nbas != 6)) return 1;
     for (int64_t i = 0; i < 3 * m; ++i)
         if (tris[i] >= static_cast<uint64_t>(n_nodes)) return 1;
     std::vector<double> centers(3 * m), normals(3 * m), areas(m);
@@ -1411,41 +1450,42 @@ int or_assemble_linear(int64_t n_nodes, const double* nodes, int64_t m, const ui
     const cd beta = C(beta_in);
     std::vector<BcView> bcs(m);
     for (int64_t e = 0; e < m; ++e) bcs[e] = bc_at(bc, e);
-    const int64_t n = 3 * m;
+    const int64_t n = nbas * m;
     set_threads(threads);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t r = 0; r < n; ++r) {
-        const int64_t i = r / 3;
-        const int cq = static_cast<int>(r % 3);
+        const int64_t i = r / nbas;
+        const int cq = static_cast<int>(r % nbas);
         std::vector<cd> local(n, cd(0, 0));
         cd lrhs(0, 0);
         const BcView& sb = bcs[i];
         if (sb.kind == 0) {  // add_free_terms (tbem.rs:1248-1281)
-            local[r] -= gamma * 0.5;
-            if (sb.has_adm) local[r] -= sb.adm * iwr * beta * tau * 0.5;
-            lrhs += sb.value * iwr * beta * tau * 0.5;
+            local[r] -= sign * (gamma * 0.5);
+            if (sb.has_adm) local[r] -= sign * sb.adm * iwr * beta * tau * 0.5;
+            lrhs += sb.value * iwr * beta * tau * 0.5 * sign;
         } else if (sb.kind == 1) {
-            local[r] += beta * tau * 0.5;
-            lrhs -= sb.value * gamma * 0.5;
+            local[r] += sign * (beta * tau * 0.5);
+            lrhs -= sb.value * gamma * 0.5 * sign;
         }
-        double x[3];
-        lin_point(coords[i], kLinColl[cq][0], kLinColl[cq][1], x);
+        double x[3], sq, tq;
+        coll_local(nbas, cq, sq, tq);
+        lin_point(coords[i], sq, tq, x);
         const double* nx = &normals[3 * i];
         for (int64_t j = 0; j < m; ++j) {
             const BcView& fb = bcs[j];
             const bool compute_rhs = std::abs(fb.value) > 1e-15;
-            Channels3 rr = (j == i) ? singular_pair_linear(x, nx, coords[j], *ph)
-                                    : regular_pair_linear(x, nx, coords[j], areas[j], *ph);
-            for (int b = 0; b < 3; ++b) {
+            Channels3 rr = (j == i) ? singular_pair_linear(x, nx, coords[j], *ph, nbas)
+                                    : regular_pair_linear(x, nx, coords[j], areas[j], *ph, nbas);
+            for (int b = 0; b < nbas; ++b) {
                 const Channels& q = rr.b[b];
                 cd coeff(0, 0);
                 if (fb.kind == 0) {
-                    coeff = q.h * gamma * tau + q.e * beta;
-                    if (fb.has_adm) coeff -= (q.g * gamma * tau + q.ht * beta) * fb.adm * iwr;
+                    coeff = sign * (q.h * gamma * tau + q.e * beta);
+                    if (fb.has_adm) coeff -= sign * (q.g * gamma * tau + q.ht * beta) * fb.adm * iwr;
                 } else if (fb.kind == 1) {
-                    coeff = -(q.g * gamma * tau + q.ht * beta);
+                    coeff = -sign * (q.g * gamma * tau + q.ht * beta);
                 }
-                local[3 * j + b] += coeff;
+                local[nbas * j + b] += coeff;
                 if (compute_rhs && b == 0) {  // values.get(b): one prescribed value per element
                     if (fb.kind == 0)
                         lrhs += (q.g * gamma * tau + q.ht * beta) * fb.value * iwr;
@@ -1460,34 +1500,40 @@ int or_assemble_linear(int64_t n_nodes, const double* nodes, int64_t m, const ui
     return 0;
 }
 
+int or_assemble_linear(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris,
+                       const or_bc* bc, const or_physics* ph, or_c128 beta_in, int threads, or_c128* A,
+                       or_c128* rhs) {
+    return or_assemble_discontinuous(n_nodes, nodes, m, tris, bc, ph, beta_in, 3, 1.0, threads, A, rhs);
+}
+
 }  // extern "C"
 
 extern "C" {
 
-// Pair-level access to the linear-basis channels (tests): out12 = (g, h, ht, e) for b = 0, 1, 2.
-void or_regular_pair_linear(const double* x, const double* nx, const double* c9, double area,
-                            const or_physics* ph, or_c128* out12) {
+// Pair-level access to the discontinuous-basis channels (tests): out = (g, h, ht, e) per basis.
+void or_regular_pair_disc(const double* x, const double* nx, const double* c9, double area,
+                          const or_physics* ph, int nbas, or_c128* out) {
     Coords c;
     std::memcpy(c.v, c9, sizeof(c.v));
-    Channels3 r = regular_pair_linear(x, nx, c, area, *ph);
-    for (int b = 0; b < 3; ++b) {
-        out12[4 * b + 0] = O(r.b[b].g);
-        out12[4 * b + 1] = O(r.b[b].h);
-        out12[4 * b + 2] = O(r.b[b].ht);
-        out12[4 * b + 3] = O(r.b[b].e);
+    Channels3 r = regular_pair_linear(x, nx, c, area, *ph, nbas);
+    for (int b = 0; b < nbas; ++b) {
+        out[4 * b + 0] = O(r.b[b].g);
+        out[4 * b + 1] = O(r.b[b].h);
+        out[4 * b + 2] = O(r.b[b].ht);
+        out[4 * b + 3] = O(r.b[b].e);
     }
 }
 
-void or_singular_pair_linear(const double* x, const double* nx, const double* c9, const or_physics* ph,
-                             or_c128* out12) {
+void or_singular_pair_disc(const double* x, const double* nx, const double* c9, const or_physics* ph, int nbas,
+                           or_c128* out) {
     Coords c;
     std::memcpy(c.v, c9, sizeof(c.v));
-    Channels3 r = singular_pair_linear(x, nx, c, *ph);
-    for (int b = 0; b < 3; ++b) {
-        out12[4 * b + 0] = O(r.b[b].g);
-        out12[4 * b + 1] = O(r.b[b].h);
-        out12[4 * b + 2] = O(r.b[b].ht);
-        out12[4 * b + 3] = O(r.b[b].e);
+    Channels3 r = singular_pair_linear(x, nx, c, *ph, nbas);
+    for (int b = 0; b < nbas; ++b) {
+        out[4 * b + 0] = O(r.b[b].g);
+        out[4 * b + 1] = O(r.b[b].h);
+        out[4 * b + 2] = O(r.b[b].ht);
+        out[4 * b + 3] = O(r.b[b].e);
     }
 }
 

@@ -117,11 +117,18 @@ int or_assemble_linear(int64_t n_nodes, const double* nodes, int64_t n_tris, con
                        const or_bc* bc, const or_physics* phys, or_c128 beta, int threads, or_c128* A,
                        or_c128* rhs);
 
-/* Linear-basis channels of one pair: out12 = (g, h, ht, e) for basis 0, 1, 2. */
-void or_regular_pair_linear(const double* x, const double* nx, const double* coords9, double area,
-                            const or_physics* phys, or_c128* out12);
-void or_singular_pair_linear(const double* x, const double* nx, const double* coords9,
-                             const or_physics* phys, or_c128* out12);
+/* Discontinuous-basis channels of one pair: out = (g, h, ht, e) for each of nbas (3 or 6) basis
+ * functions. */
+void or_regular_pair_disc(const double* x, const double* nx, const double* coords9, double area,
+                          const or_physics* phys, int nbas, or_c128* out);
+void or_singular_pair_disc(const double* x, const double* nx, const double* coords9,
+                           const or_physics* phys, int nbas, or_c128* out);
+/* Any discontinuous basis (nbas 3 or 6) and sign +-1: collocation and assembly. */
+void or_disc_collocation(int64_t n_tris, const double* nodes, const uint32_t* tris, int nbas, double* points,
+                         double* normals);
+int or_assemble_discontinuous(int64_t n_nodes, const double* nodes, int64_t n_tris, const uint32_t* tris,
+                              const or_bc* bc, const or_physics* phys, or_c128 beta, int nbas, double sign,
+                              int threads, or_c128* A, or_c128* rhs);
 
 void or_field_eval(const double* nodes, const uint32_t* tris, int64_t n_tris, const or_c128* pressure,
                    const or_c128* velocity, double k, double harmonic_factor, double pressure_factor,

@@ -30,7 +30,7 @@ SB_BC_VELOCITY, SB_BC_PRESSURE = 0, 1
 SB_INJECT_NONE, SB_INJECT_ALLOC, SB_INJECT_LAUNCH = 0, 1, 2
 SB_SOLVER_CONVERGED, SB_SOLVER_MAX_ITERATIONS, SB_SOLVER_BREAKDOWN, SB_SOLVER_NUMERICAL_ERROR = 0, 1, 2, 3
 SB_BATCH_ASM_AUTO, SB_BATCH_ASM_PERSISTENT, SB_BATCH_ASM_STREAMS = 0, 1, 2
-SB_BASIS_CONSTANT, SB_BASIS_LINEAR = 0, 1
+SB_BASIS_CONSTANT, SB_BASIS_LINEAR, SB_BASIS_QUADRATIC = 0, 1, 2
 
 _ERROR_NAMES = {
     SB_ERR_INVALID_ARGUMENT: "InvalidInput",
@@ -123,6 +123,8 @@ _SIGNATURES = {
     "sb_operator_from_dense": ([ct.c_int, ct.c_int64, P, ct.c_int, ct.POINTER(P)], ct.c_int),
     "sb_assemble_linear": ([P, ct.POINTER(SbPhysics), SbComplex, ct.POINTER(P)], ct.c_int),
     "sb_mesh_collocation": ([P, ct.c_int, P, P], ct.c_int),
+    "sb_assemble_discontinuous": ([P, ct.POINTER(SbPhysics), SbComplex, ct.c_int, ct.c_double, ct.POINTER(P)],
+                                  ct.c_int),
     "sb_rhs_plane_wave_points": ([ct.c_int, ct.c_int64, P, P, ct.POINTER(SbPhysics), SbComplex, P, P, ct.c_int64, P],
                                  ct.c_int),
     "sb_operator_destroy": ([P], ct.c_int),

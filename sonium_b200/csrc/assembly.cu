@@ -842,16 +842,48 @@ __device__ __forceinline__ void point_channels_w(Acc* a, const double* nb, doubl
     }
 }
 
-// Discontinuous linear Tri3 basis N_b = 2 lambda_b - 1/3 (crates/sonium-bem/src/core/mesh/
-// element.rs:229-236).
-__device__ __forceinline__ void lin_basis(double s, double t, double nb[3]) {
-    nb[0] = 2.0 * (1.0 - s - t) - 1.0 / 3.0;
-    nb[1] = 2.0 * s - 1.0 / 3.0;
-    nb[2] = 2.0 * t - 1.0 / 3.0;
+// Discontinuous Tri3 panel bases (basis_values, crates/sonium-bem/src/core/mesh/element.rs:
+// 229-262): NB = 3 the linear basis 2 lambda_b - 1/3, NB = 6 the quadratic one (vertex functions
+// lambda (2 lambda - 1), then 4 lambda0 lambda1, 4 lambda1 lambda2, 4 lambda2 lambda0).
+template <int NB>
+__device__ __forceinline__ void panel_basis(double s, double t, double* nb) {
+    const double l0 = 1.0 - s - t;
+    if constexpr (NB == 3) {
+        nb[0] = 2.0 * l0 - 1.0 / 3.0;
+        nb[1] = 2.0 * s - 1.0 / 3.0;
+        nb[2] = 2.0 * t - 1.0 / 3.0;
+    } else {
+        nb[0] = l0 * (2.0 * l0 - 1.0);
+        nb[1] = s * (2.0 * s - 1.0);
+        nb[2] = t * (2.0 * t - 1.0);
+        nb[3] = 4.0 * l0 * s;
+        nb[4] = 4.0 * s * t;
+        nb[5] = 4.0 * t * l0;
+    }
+}
+
+// Reference-coordinate derivatives (d/ds, d/dt) of the panel basis (panel_basis_gradients,
+// integration/singular.rs:1180-1195).
+template <int NB>
+__device__ __forceinline__ void panel_basis_deriv(double s, double t, double (*d)[2]) {
+    if constexpr (NB == 3) {
+        d[0][0] = -2.0; d[0][1] = -2.0;
+        d[1][0] = 2.0; d[1][1] = 0.0;
+        d[2][0] = 0.0; d[2][1] = 2.0;
+    } else {
+        const double l = 1.0 - s - t;
+        d[0][0] = 1.0 - 4.0 * l; d[0][1] = 1.0 - 4.0 * l;
+        d[1][0] = 4.0 * s - 1.0; d[1][1] = 0.0;
+        d[2][0] = 0.0; d[2][1] = 4.0 * t - 1.0;
+        d[3][0] = 4.0 * (l - s); d[3][1] = -4.0 * s;
+        d[4][0] = 4.0 * t; d[4][1] = 4.0 * s;
+        d[5][0] = -4.0 * t; d[5][1] = 4.0 * (l - t);
+    }
 }
 
 // Evaluates the regular-integration channels of field element j seen from the point x with
-// normal nx into lane-partial sums: NB = 1 the constant basis, NB = 3 the linear basis weights.
+// normal nx into lane-partial sums: NB = 1 the constant basis, NB = 3 / 6 the discontinuous
+// linear / quadratic basis weights.
 template <int NB>
 __device__ void near_channels_at(Acc* a, NearWarpSmem& S, const double* __restrict__ elem, int64_t ld,
                                  double x0, double x1, double x2, double nxx, double nxy, double nxz,
@@ -1017,8 +1049,8 @@ __device__ void near_channels_at(Acc* a, NearWarpSmem& S, const double* __restri
             if constexpr (NB == 1) {
                 point_channels(a[0], dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
             } else {
-                double nb[3];
-                lin_basis(xio, eto, nb);
+                double nb[NB];
+                panel_basis<NB>(xio, eto, nb);
                 point_channels_w<NB>(a, nb, dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k,
                                      k2);
             }
@@ -1221,25 +1253,45 @@ __global__ void __launch_bounds__(128) k_self(const double* __restrict__ elem, i
 }
 
 // =============================================================================================
-// Discontinuous linear Tri3 basis (build_tbem_system_linear, crates/sonium-bem/src/core/assembly/
-// tbem.rs:1490-1620): DOF 3e + c of element e is collocated at local point c of (1/6, 1/6),
-// (2/3, 1/6), (1/6, 2/3) (mesh/element.rs:91-99) with the element's flat normal; the row of
-// that DOF holds, for every field element j, the three basis-weighted integrals in columns
-// 3j + b. FP64 throughout (complex128 matrix).
+// Discontinuous Tri3 bases (build_tbem_system_linear, crates/sonium-bem/src/core/assembly/
+// tbem.rs:1490-1620; build_tbem_system_discontinuous_stabilized, :2810-2990): element e carries
+// NB DOFs (3 linear, 6 quadratic), DOF NB e + c collocated at local point c of the basis's
+// interior points (mesh/element.rs:91-123) with the element's flat normal; the row of that DOF
+// holds, for every field element j, the NB basis-weighted integrals in columns NB j + b. FP64
+// throughout (complex128 matrix).
 // =============================================================================================
 __constant__ double c_lin_coll[3][2] = {{1.0 / 6.0, 1.0 / 6.0}, {2.0 / 3.0, 1.0 / 6.0}, {1.0 / 6.0, 2.0 / 3.0}};
+__constant__ double c_quad_coll[6][2] = {{0.0915762135097715, 0.0915762135097715},
+                                         {0.8168475729804585, 0.0915762135097715},
+                                         {0.0915762135097715, 0.8168475729804585},
+                                         {0.445948490915965, 0.445948490915965},
+                                         {0.445948490915965, 0.108103018168070},
+                                         {0.108103018168070, 0.445948490915965}};
 constexpr int kLinRows = 32;
 
-// Collocation points of the 3n rows (local_to_global, element.rs:65-76) and their (flat element)
-// normals, SoA: cp[c * n3 + r], cn[c * n3 + r].
+template <int NB>
+__device__ __forceinline__ void coll_local(int q, double& s, double& t) {
+    if constexpr (NB == 3) {
+        s = c_lin_coll[q][0];
+        t = c_lin_coll[q][1];
+    } else {
+        s = c_quad_coll[q][0];
+        t = c_quad_coll[q][1];
+    }
+}
+
+// Collocation points of the NB n rows (local_to_global, element.rs:65-76) and their (flat
+// element) normals, SoA: cp[c * n3 + r], cn[c * n3 + r].
+template <int NB>
 __global__ void k_lin_points(const double* __restrict__ elem, int64_t n, int64_t ld, double* __restrict__ cp,
                              double* __restrict__ cn) {
     const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t n3 = 3 * n;
+    const int64_t n3 = NB * n;
     if (r >= n3) return;
-    const int64_t e = r / 3;
-    const int q = static_cast<int>(r % 3);
-    const double s = c_lin_coll[q][0], t = c_lin_coll[q][1];
+    const int64_t e = r / NB;
+    const int q = static_cast<int>(r % NB);
+    double s, t;
+    coll_local<NB>(q, s, t);
     const double sf[3] = {1.0 - s - t, s, t};
     for (int c = 0; c < 3; ++c) {
         double v = 0.0;
@@ -1270,8 +1322,9 @@ __global__ void k_plane_wave_at(const double* __restrict__ pts, const double* __
     rhs[t] = make_double2(-(p.x + bt.x * dpdn.x - bt.y * dpdn.y), -(p.y + bt.x * dpdn.y + bt.y * dpdn.x));
 }
 
-// Near-pair classification of the 3n collocation rows against the n elements (the element's
+// Near-pair classification of the NB n collocation rows against the n elements (the element's
 // own row block excluded): pass 0 counts, pass 1 writes the columns in increasing order.
+template <int NB>
 __global__ void __launch_bounds__(256) k_lin_near_pass(const double* __restrict__ elem, int64_t n, int64_t ld,
                                                        const double* __restrict__ cp, int pass,
                                                        int64_t* __restrict__ counts,
@@ -1282,7 +1335,7 @@ __global__ void __launch_bounds__(256) k_lin_near_pass(const double* __restrict_
     __shared__ int64_t sbase[kNearRows];
     __shared__ int scount[kNearRows];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int64_t n3 = 3 * n;
+    const int64_t n3 = NB * n;
     const int64_t row0 = blockIdx.x * (int64_t)kNearRows;
     if (tid < kNearRows) {
         const int64_t r = row0 + tid;
@@ -1302,7 +1355,7 @@ __global__ void __launch_bounds__(256) k_lin_near_pass(const double* __restrict_
         }
         for (int rr = 0; rr < kNearRows; ++rr) {
             const int64_t r = row0 + rr;
-            const bool p = (j < n) && (r < n3) && (j != r / 3) &&
+            const bool p = (j < n) && (r < n3) && (j != r / NB) &&
                            near_superset(gx, gy, gz, thr, sx[rr][0], sx[rr][1], sx[rr][2]);
             const unsigned b = __ballot_sync(0xffffffffu, p);
             if (pass == 0) {
@@ -1334,9 +1387,10 @@ __global__ void __launch_bounds__(256) k_lin_near_pass(const double* __restrict_
     if (pass == 0 && tid < kNearRows && row0 + tid < n3) counts[row0 + tid] = scount[tid];
 }
 
-// Far field of the linear basis: one thread per field element (128-column tiles), 32 rows per
-// CTA; the element's 13-point leaf (the reference's single far leaf) staged in shared memory,
-// the three basis values of each point from the rule's reference coordinates.
+// Far field of the discontinuous bases: one thread per field element (128-column tiles), 32 rows
+// per CTA; the element's 13-point leaf (the reference's single far leaf) staged in shared memory,
+// the NB basis values of each point from the rule's reference coordinates.
+template <int NB>
 __global__ void __launch_bounds__(kFarTile) k_lin_far(const double* __restrict__ qp, const double* __restrict__ elem,
                                                       int64_t n, int64_t ld, const double* __restrict__ cp,
                                                       const double* __restrict__ coef, double k,
@@ -1347,7 +1401,7 @@ __global__ void __launch_bounds__(kFarTile) k_lin_far(const double* __restrict__
     const int tid = threadIdx.x;
     const int64_t tile = blockIdx.x;
     const int64_t j = tile * kFarTile + tid;
-    const int64_t n3 = 3 * n;
+    const int64_t n3 = NB * n;
     const int64_t row0 = blockIdx.y * (int64_t)kLinRows;
     const double k2 = k * k;
     const double* src = qp + tile * (int64_t)kQpTileDoubles;
@@ -1356,7 +1410,7 @@ __global__ void __launch_bounds__(kFarTile) k_lin_far(const double* __restrict__
         const int rr = t / 6, f = t % 6;
         const int64_t r = row0 + rr;
         double v = 0.0;
-        if (r < n3) v = f < 3 ? cp[f * n3 + r] : E(ENX + (f - 3), r / 3);
+        if (r < n3) v = f < 3 ? cp[f * n3 + r] : E(ENX + (f - 3), r / NB);
         sr[t] = v;
     }
     double nyx = 0, nyy = 0, nyz = 0, gx = 0, gy = 0, gz = 0, thr = -1;
@@ -1375,26 +1429,27 @@ __global__ void __launch_bounds__(kFarTile) k_lin_far(const double* __restrict__
         const int64_t r = row0 + rr;
         const double xx = sr[rr * 6 + 0], xy = sr[rr * 6 + 1], xz = sr[rr * 6 + 2];
         const double nxx = sr[rr * 6 + 3], nxy = sr[rr * 6 + 4], nxz = sr[rr * 6 + 5];
-        const bool active = (j < n) && (j != r / 3) && !near_superset(gx, gy, gz, thr, xx, xy, xz);
+        const bool active = (j < n) && (j != r / NB) && !near_superset(gx, gy, gz, thr, xx, xy, xz);
         if (!active) continue;
-        Acc a[3];
+        Acc a[NB];
         for (int q = 0; q < kFarPoints; ++q) {
             const double* p = sq + q * 4 * kFarTile + tid;
             const double dx = p[0] - xx, dy = p[kFarTile] - xy, dz = p[2 * kFarTile] - xz;
             const double w = p[3 * kFarTile];
             const double d2 = dx * dx + dy * dy + dz * dz;
             const double rinv = sb_rsqrt2(d2);
-            double nb[3];
-            lin_basis(c_tri_xi[c_tri_off[0] + q], c_tri_eta[c_tri_off[0] + q], nb);  // the 13-point leaf
-            point_channels_w<3>(a, nb, dx, dy, dz, d2 * rinv, rinv, w, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
+            double nb[NB];
+            panel_basis<NB>(c_tri_xi[c_tri_off[0] + q], c_tri_eta[c_tri_off[0] + q], nb);  // the 13-point leaf
+            point_channels_w<NB>(a, nb, dx, dy, dz, d2 * rinv, rinv, w, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
         }
-        for (int b = 0; b < 3; ++b) A[r * n3 + 3 * j + b] = combine(a[b], coef, ld, j, CF_CG);
+        for (int b = 0; b < NB; ++b) A[r * n3 + NB * j + b] = combine(a[b], coef, ld, j, CF_CG);
     }
 }
 
 __device__ __forceinline__ Acc lin_reduce(const Acc& a) { return warp_reduce(a); }
 
-// Near pairs of the linear basis: one warp per (collocation row, field element) pair.
+// Near pairs of the discontinuous bases: one warp per (collocation row, field element) pair.
+template <int NB>
 __global__ void __launch_bounds__(32 * kNearWarps) k_lin_near(const double* __restrict__ elem, int64_t n, int64_t ld,
                                                               const double* __restrict__ cp,
                                                               const int64_t* __restrict__ row_ptr,
@@ -1405,35 +1460,36 @@ __global__ void __launch_bounds__(32 * kNearWarps) k_lin_near(const double* __re
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t p = blockIdx.x * (int64_t)kNearWarps + warp;
     if (p >= nnz) return;
-    const int64_t n3 = 3 * n;
+    const int64_t n3 = NB * n;
     int64_t lo = 0, hi = n3 - 1;
     while (lo < hi) {
         const int64_t mid = (lo + hi + 1) >> 1;
         if (row_ptr[mid] <= p) lo = mid; else hi = mid - 1;
     }
-    const int64_t r = lo, j = cols[p], e = r / 3;
-    Acc a[3];
-    near_channels_at<3>(a, sm[warp], elem, ld, cp[r], cp[n3 + r], cp[2 * n3 + r], E(ENX, e), E(ENY, e), E(ENZ, e),
+    const int64_t r = lo, j = cols[p], e = r / NB;
+    Acc a[NB];
+    near_channels_at<NB>(a, sm[warp], elem, ld, cp[r], cp[n3 + r], cp[2 * n3 + r], E(ENX, e), E(ENY, e), E(ENZ, e),
                         j, k, k * k, lane);
-    Acc t[3];
-    for (int b = 0; b < 3; ++b) t[b] = lin_reduce(a[b]);
+    Acc t[NB];
+    for (int b = 0; b < NB; ++b) t[b] = lin_reduce(a[b]);
     if (lane == 0)
-        for (int b = 0; b < 3; ++b) A[r * n3 + 3 * j + b] = combine(t[b], coef, ld, j, CF_CG);
+        for (int b = 0; b < NB; ++b) A[r * n3 + NB * j + b] = combine(t[b], coef, ld, j, CF_CG);
 }
-// Self element of the linear basis (singular_integration_linear_with_params_mode, integration/
+// Self element of the discontinuous bases (singular_integration_linear_with_params_mode, integration/
 // singular.rs:868-1170): one warp per collocation row. The regularised edge integral of E is
 // weighted by the basis at the edge point; the centroid-centred Duffy sub-triangles give G, H,
 // H^T and the area part of E, k^2 (n_x . n_y) G N_b plus the basis-gradient term
 // (-(n_x . n_y)(grad N_b . r_hat) + (r_hat . n_y)(grad N_b . n_x)) times G (-1/r + i k). The
 // free term of the row's element goes on the diagonal.
+template <int NB>
 __global__ void __launch_bounds__(128) k_lin_self(const double* __restrict__ elem, int64_t n, int64_t ld,
                                                   const double* __restrict__ cp, const double* __restrict__ coef,
                                                   double k, double2* __restrict__ A, double2* __restrict__ diag) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t n3 = 3 * n;
+    const int64_t n3 = NB * n;
     const int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp;
     if (r >= n3) return;
-    const int64_t i = r / 3;
+    const int64_t i = r / NB;
     const double k2 = k * k;
     const double x0 = cp[r], x1 = cp[n3 + r], x2 = cp[2 * n3 + r];
     const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
@@ -1442,28 +1498,20 @@ __global__ void __launch_bounds__(128) k_lin_self(const double* __restrict__ ele
     double V[3][3];
     for (int t = 0; t < 3; ++t)
         for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, i);
-    // panel_basis_gradients (singular.rs:1173-1258): constant surface gradients of N_b.
-    double grad[3][3];
-    {
-        const double der[3][2] = {{-2.0, -2.0}, {2.0, 0.0}, {0.0, 2.0}};
-        double ts[3], tt[3];
-        for (int c = 0; c < 3; ++c) {
-            ts[c] = -V[0][c] + V[1][c] + 0.0 * V[2][c];
-            tt[c] = -V[0][c] + 0.0 * V[1][c] + V[2][c];
-        }
-        double ss = 0, tq = 0, st = 0;
-        for (int c = 0; c < 3; ++c) {
-            ss += ts[c] * ts[c];
-            tq += tt[c] * tt[c];
-            st += ts[c] * tt[c];
-        }
-        const double det = ss * tq - st * st;
-        for (int b = 0; b < 3; ++b) {
-            const double ga = (tq * der[b][0] - st * der[b][1]) / det;
-            const double gb = (ss * der[b][1] - st * der[b][0]) / det;
-            for (int c = 0; c < 3; ++c) grad[b][c] = ga * ts[c] + gb * tt[c];
-        }
+    // panel_basis_gradients (singular.rs:1173-1258): the surface gradient of N_b is
+    // a ts + b tt with the panel's tangents and metric (constant over a flat panel).
+    double tan_s[3], tan_t[3];
+    for (int c = 0; c < 3; ++c) {
+        tan_s[c] = -V[0][c] + V[1][c] + 0.0 * V[2][c];
+        tan_t[c] = -V[0][c] + 0.0 * V[1][c] + V[2][c];
     }
+    double gss = 0, gtt = 0, gst = 0;
+    for (int c = 0; c < 3; ++c) {
+        gss += tan_s[c] * tan_s[c];
+        gtt += tan_t[c] * tan_t[c];
+        gst += tan_s[c] * tan_t[c];
+    }
+    const double gdet = gss * gtt - gst * gst;
     const double ka = k * fmax(sqrt(E(EAREA, i)), 1e-10);
     int ngpo1, nsub, nsec1, nsec2;
     if (ka < 0.3) { ngpo1 = 3; nsub = 4; nsec1 = 4; nsec2 = 2; }
@@ -1475,7 +1523,7 @@ __global__ void __launch_bounds__(128) k_lin_self(const double* __restrict__ ele
     const int per_edge = n_edge + n_bulk;
     const double csi6[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
     const double eta6[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
-    Acc a[3];
+    Acc a[NB];
     for (int f = lane; f < 3 * per_edge; f += 32) {
         const int ieg = f / per_edge, rem = f % per_edge;
         const int ig1 = (ieg + 1) % 3, ig2 = ieg + 3;
@@ -1507,9 +1555,9 @@ __global__ void __launch_bounds__(128) k_lin_self(const double* __restrict__ ele
             const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
             const double cr = (uy * to2 - uz * to1) * nxx + (uz * to0 - ux * to2) * nxy + (ux * to1 - uy * to0) * nxz;
             const double te = (sga + 1.0) / 2.0;
-            double nb[3];
-            lin_basis(csi6[ieg] * (1.0 - te) + csi6[ig1] * te, eta6[ieg] * (1.0 - te) + eta6[ig1] * te, nb);
-            for (int b = 0; b < 3; ++b) {
+            double nb[NB];
+            panel_basis<NB>(csi6[ieg] * (1.0 - te) + csi6[ig1] * te, eta6[ieg] * (1.0 - te) + eta6[ig1] * te, nb);
+            for (int b = 0; b < NB; ++b) {
                 a[b].er += f_r * cr * wga * nb[b];
                 a[b].ei += f_i * cr * wga * nb[b];
             }
@@ -1546,33 +1594,38 @@ __global__ void __launch_bounds__(128) k_lin_self(const double* __restrict__ ele
             const double rnx = -(ux * nxx + uy * nxy + uz * nxz);
             const double b_r = -g_r * rinv - g_i * k, b_i = g_r * k - g_i * rinv;
             const double nd = nxx * nyx + nxy * nyy + nxz * nyz;
-            double nb[3];
-            lin_basis(sgg, tgg, nb);
-            for (int b = 0; b < 3; ++b) {
+            double nb[NB], der[NB][2];
+            panel_basis<NB>(sgg, tgg, nb);
+            panel_basis_deriv<NB>(sgg, tgg, der);
+            for (int b = 0; b < NB; ++b) {
                 const double w = nb[b];
                 a[b].gr += g_r * w; a[b].gi += g_i * w;
                 a[b].hr += b_r * rny * w; a[b].hi += b_i * rny * w;
                 a[b].tr += b_r * rnx * w; a[b].ti += b_i * rnx * w;
-                const double gr = grad[b][0] * ux + grad[b][1] * uy + grad[b][2] * uz;
-                const double gsn = grad[b][0] * nxx + grad[b][1] * nxy + grad[b][2] * nxz;
+                const double ga = (gtt * der[b][0] - gst * der[b][1]) / gdet;
+                const double gb = (gss * der[b][1] - gst * der[b][0]) / gdet;
+                const double grad0 = ga * tan_s[0] + gb * tan_t[0], grad1 = ga * tan_s[1] + gb * tan_t[1];
+                const double grad2 = ga * tan_s[2] + gb * tan_t[2];
+                const double gr = grad0 * ux + grad1 * uy + grad2 * uz;
+                const double gsn = grad0 * nxx + grad1 * nxy + grad2 * nxz;
                 const double gf = -nd * gr + rny * gsn;
                 a[b].er += g_r * k2 * nd * w + b_r * gf;
                 a[b].ei += g_i * k2 * nd * w + b_i * gf;
             }
         }
     }
-    Acc t[3];
-    for (int b = 0; b < 3; ++b) t[b] = warp_reduce(a[b]);
+    Acc t[NB];
+    for (int b = 0; b < NB; ++b) t[b] = warp_reduce(a[b]);
     if (lane == 0) {
-        const int c = static_cast<int>(r % 3);
-        for (int b = 0; b < 3; ++b) {
+        const int c = static_cast<int>(r % NB);
+        for (int b = 0; b < NB; ++b) {
             double2 v = combine(t[b], coef, ld, i, CF_CG);
             if (b == c) {
                 v.x += coef[(int64_t)(CF_DIAG) * ld + i];
                 v.y += coef[(int64_t)(CF_DIAG + 1) * ld + i];
                 diag[r] = v;
             }
-            A[r * n3 + 3 * i + b] = v;
+            A[r * n3 + NB * i + b] = v;
         }
     }
 }
@@ -1913,16 +1966,18 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     op.beta_im = beta_im;
 }
 
-// build_tbem_system_linear on the device: collocation points and the near-pair CSR of the 3n
-// rows once per operator, then coefficients, far tiles, near pairs and self rows per assembly.
-void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
+// Scales the per-element coefficients (matrix weights, RHS weights, free terms) by `sign`: every
+// entry of the stabilised discontinuous systems is sign times the unsigned one
+// (build_tbem_system_discontinuous_stabilized, tbem.rs:2810-2990).
+__global__ void k_scale_coef(double* __restrict__ coef, int64_t count, double sign) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < count) coef[t] *= sign;
+}
+
+template <int NB>
+static void assemble_disc_nb(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
     Mesh& m = *op.mesh;
-    SB_CUDA(cudaSetDevice(m.device));
-    SB_REQUIRE(!m.any_bc_value, SB_ERR_INVALID_ARGUMENT,
-               "linear basis: prescribed boundary values are not supported (rigid, pressure-release with zero "
-               "value, or admittance surfaces)");
-    maybe_inject(SB_INJECT_LAUNCH);
-    const int64_t n = m.n, ld = m.ld, n3 = 3 * n;
+    const int64_t n = m.n, ld = m.ld, n3 = NB * n;
     const cudaStream_t s = op.stream;
     if (!op.coef.p) op.coef.alloc(sizeof(double) * CF_FIELDS * ld);
     if (!op.diag.p) op.diag.alloc(sizeof(double2) * n3);
@@ -1933,14 +1988,14 @@ void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double 
     if (!op.lin_cp.p) {
         op.lin_cp.alloc(sizeof(double) * 3 * n3);
         op.lin_cn.alloc(sizeof(double) * 3 * n3);
-        k_lin_points<<<cdiv(n3, 256), 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
-                                                   op.lin_cn.as<double>());
+        k_lin_points<NB><<<cdiv(n3, 256), 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
+                                                       op.lin_cn.as<double>());
         count_launch();
         DevBuf counts;
         counts.alloc(sizeof(int64_t) * (n3 + 1));
         const int64_t nblk = cdiv(n3, kNearRows);
-        k_lin_near_pass<<<nblk, 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), 0,
-                                             counts.as<int64_t>(), nullptr, nullptr);
+        k_lin_near_pass<NB><<<nblk, 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), 0,
+                                                 counts.as<int64_t>(), nullptr, nullptr);
         count_launch();
         SB_CUDA(cudaGetLastError());
         std::vector<int64_t> cnt(n3), ptr(n3 + 1);
@@ -1952,8 +2007,8 @@ void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double 
         op.lin_ptr.alloc(sizeof(int64_t) * (n3 + 1));
         SB_CUDA(cudaMemcpyAsync(op.lin_ptr.p, ptr.data(), sizeof(int64_t) * (n3 + 1), cudaMemcpyHostToDevice, s));
         op.lin_col.alloc(sizeof(int32_t) * std::max<int64_t>(op.lin_nnz, 1));
-        k_lin_near_pass<<<nblk, 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), 1, nullptr,
-                                             op.lin_ptr.as<int64_t>(), op.lin_col.as<int32_t>());
+        k_lin_near_pass<NB><<<nblk, 256, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), 1, nullptr,
+                                                 op.lin_ptr.as<int64_t>(), op.lin_col.as<int32_t>());
         count_launch();
         SB_CUDA(cudaGetLastError());
         SB_CUDA(cudaStreamSynchronize(s));
@@ -1967,21 +2022,26 @@ void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double 
                                                  ph.pressure_factor, make_double2(beta_re, beta_im),
                                                  op.coef.as<double>());
     count_launch();
+    if (op.sign != 1.0) {
+        k_scale_coef<<<cdiv(CF_FIELDS * ld, 256), 256, 0, s>>>(op.coef.as<double>(), CF_FIELDS * ld, op.sign);
+        count_launch();
+    }
     const double k = ph.harmonic_factor * ph.wave_number;
     double2* A = op.A64.as<double2>();
     {
         ProfScope prof(SB_PROF_FAR, s);
         const size_t sm = sizeof(double) * (kQpTileDoubles + kLinRows * 6);
-        SB_CUDA(cudaFuncSetAttribute(k_lin_far, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        SB_CUDA(cudaFuncSetAttribute(k_lin_far<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(sm)));
         dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n3, kLinRows)));
-        k_lin_far<<<grid, kFarTile, sm, s>>>(m.qp.as<double>(), m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
-                                             op.coef.as<double>(), k, A);
+        k_lin_far<NB><<<grid, kFarTile, sm, s>>>(m.qp.as<double>(), m.elem.as<double>(), n, ld,
+                                                 op.lin_cp.as<double>(), op.coef.as<double>(), k, A);
         count_launch();
         SB_CUDA(cudaGetLastError());
     }
     if (op.lin_nnz > 0) {
         ProfScope prof(SB_PROF_NEAR, s);
-        k_lin_near<<<cdiv(op.lin_nnz, kNearWarps), 32 * kNearWarps, 0, s>>>(
+        k_lin_near<NB><<<cdiv(op.lin_nnz, kNearWarps), 32 * kNearWarps, 0, s>>>(
             m.elem.as<double>(), n, ld, op.lin_cp.as<double>(), op.lin_ptr.as<int64_t>(), op.lin_col.as<int32_t>(),
             op.lin_nnz, op.coef.as<double>(), k, A);
         count_launch();
@@ -1989,8 +2049,8 @@ void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double 
     }
     {
         ProfScope prof(SB_PROF_SELF, s);
-        k_lin_self<<<cdiv(n3, 4), 128, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
-                                              op.coef.as<double>(), k, A, op.diag.as<double2>());
+        k_lin_self<NB><<<cdiv(n3, 4), 128, 0, s>>>(m.elem.as<double>(), n, ld, op.lin_cp.as<double>(),
+                                                  op.coef.as<double>(), k, A, op.diag.as<double2>());
         count_launch();
         SB_CUDA(cudaGetLastError());
     }
@@ -2001,14 +2061,33 @@ void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     op.last_assembly_ms = ms;
+}
+
+// build_tbem_system_linear / build_tbem_system_discontinuous_stabilized on the device: collocation
+// points and the near-pair CSR of the NB n rows once per operator, then coefficients (times the
+// operator's sign), far tiles, near pairs and self rows per assembly.
+void assemble_discontinuous(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
+    Mesh& m = *op.mesh;
+    SB_CUDA(cudaSetDevice(m.device));
+    SB_REQUIRE(!m.any_bc_value, SB_ERR_INVALID_ARGUMENT,
+               "discontinuous bases: prescribed boundary values are not supported (rigid, pressure-release "
+               "with zero value, or admittance surfaces)");
+    maybe_inject(SB_INJECT_LAUNCH);
+    if (op.basis == SB_BASIS_QUADRATIC)
+        assemble_disc_nb<6>(op, ph, beta_re, beta_im);
+    else
+        assemble_disc_nb<3>(op, ph, beta_re, beta_im);
     op.phys = ph;
     op.beta_re = beta_re;
     op.beta_im = beta_im;
 }
 
-void lin_collocation(const Mesh& m, double* cp_dev, double* cn_dev) {
+void lin_collocation(const Mesh& m, int basis, double* cp_dev, double* cn_dev) {
     SB_CUDA(cudaSetDevice(m.device));
-    k_lin_points<<<cdiv(3 * m.n, 256), 256>>>(m.elem.as<double>(), m.n, m.ld, cp_dev, cn_dev);
+    if (basis == SB_BASIS_QUADRATIC)
+        k_lin_points<6><<<cdiv(6 * m.n, 256), 256>>>(m.elem.as<double>(), m.n, m.ld, cp_dev, cn_dev);
+    else
+        k_lin_points<3><<<cdiv(3 * m.n, 256), 256>>>(m.elem.as<double>(), m.n, m.ld, cp_dev, cn_dev);
     count_launch();
     SB_CUDA(cudaGetLastError());
     SB_CUDA(cudaDeviceSynchronize());

@@ -393,17 +393,20 @@ SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_compl
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
         tensor_release(*op->op);
-        if (op->op->basis == SB_BASIS_LINEAR)
-            assemble_linear(*op->op, *physics, beta.re, beta.im);
+        if (op->op->basis != SB_BASIS_CONSTANT)
+            assemble_discontinuous(*op->op, *physics, beta.re, beta.im);
         else
             assemble(*op->op, *physics, beta.re, beta.im);
     });
 }
 
-SB_API int sb_assemble_linear(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta, sb_operator** out) {
-    return guarded([&] {
+static void create_discontinuous(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta, int basis,
+                                 double sign, sb_operator** out) {
         SB_REQUIRE(mesh && mesh->m && physics && out, SB_ERR_INVALID_ARGUMENT, "null argument");
         *out = nullptr;
+        SB_REQUIRE(basis == SB_BASIS_LINEAR || basis == SB_BASIS_QUADRATIC, SB_ERR_INVALID_ARGUMENT,
+                   "discontinuous basis must be SB_BASIS_LINEAR or SB_BASIS_QUADRATIC");
+        SB_REQUIRE(sign == 1.0 || sign == -1.0, SB_ERR_INVALID_ARGUMENT, "sign must be +1 or -1");
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
         Mesh& m = *mesh->m;
@@ -417,25 +420,35 @@ SB_API int sb_assemble_linear(const sb_mesh* mesh, const sb_physics* physics, sb
             op->mesh = &m;
             op->device = m.device;
             op->precision = SB_PRECISION_FP64;
-            op->basis = SB_BASIS_LINEAR;
-            op->n = 3 * m.n;
+            op->basis = basis;
+            op->sign = sign;
+            op->n = (basis == SB_BASIS_QUADRATIC ? 6 : 3) * m.n;
             op->lda32 = (op->n + 1) / 2 * 2;
             SB_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
             op->A64.alloc(sizeof(double2) * op->n * op->n);
-            assemble_linear(*op, *physics, beta.re, beta.im);
+            assemble_discontinuous(*op, *physics, beta.re, beta.im);
         } catch (...) {
             if (op->stream) cudaStreamDestroy(op->stream);
             delete op;
             throw;
         }
         *out = new sb_operator{op};
-    });
+}
+
+SB_API int sb_assemble_linear(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta, sb_operator** out) {
+    return guarded([&] { create_discontinuous(mesh, physics, beta, SB_BASIS_LINEAR, 1.0, out); });
+}
+
+SB_API int sb_assemble_discontinuous(const sb_mesh* mesh, const sb_physics* physics, sb_complex beta, int basis,
+                                     double sign, sb_operator** out) {
+    return guarded([&] { create_discontinuous(mesh, physics, beta, basis, sign, out); });
 }
 
 SB_API int sb_mesh_collocation(const sb_mesh* mesh, int basis, double* points, double* normals) {
     return guarded([&] {
         SB_REQUIRE(mesh && mesh->m && points && normals, SB_ERR_INVALID_ARGUMENT, "null argument");
-        SB_REQUIRE(basis == SB_BASIS_CONSTANT || basis == SB_BASIS_LINEAR, SB_ERR_INVALID_ARGUMENT, "unknown basis");
+        SB_REQUIRE(basis == SB_BASIS_CONSTANT || basis == SB_BASIS_LINEAR || basis == SB_BASIS_QUADRATIC,
+                   SB_ERR_INVALID_ARGUMENT, "unknown basis");
         const Mesh& m = *mesh->m;
         if (basis == SB_BASIS_CONSTANT) {
             for (int64_t e = 0; e < m.n; ++e)
@@ -445,18 +458,16 @@ SB_API int sb_mesh_collocation(const sb_mesh* mesh, int basis, double* points, d
                 }
             return;
         }
-        // The linear rows' points from a temporary linear operator shell (same kernel as assembly).
+        // The discontinuous rows' points from the assembly's kernel.
         SB_CUDA(cudaSetDevice(m.device));
-        Operator tmp;
-        tmp.mesh = const_cast<Mesh*>(&m);
-        tmp.device = m.device;
-        const int64_t n3 = 3 * m.n;
-        tmp.lin_cp.alloc(sizeof(double) * 3 * n3);
-        tmp.lin_cn.alloc(sizeof(double) * 3 * n3);
-        lin_collocation(m, tmp.lin_cp.as<double>(), tmp.lin_cn.as<double>());
+        const int64_t n3 = (basis == SB_BASIS_QUADRATIC ? 6 : 3) * m.n;
+        DevBuf dcp, dcn;
+        dcp.alloc(sizeof(double) * 3 * n3);
+        dcn.alloc(sizeof(double) * 3 * n3);
+        lin_collocation(m, basis, dcp.as<double>(), dcn.as<double>());
         std::vector<double> cp(3 * n3), cn(3 * n3);
-        SB_CUDA(cudaMemcpy(cp.data(), tmp.lin_cp.p, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost));
-        SB_CUDA(cudaMemcpy(cn.data(), tmp.lin_cn.p, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost));
+        SB_CUDA(cudaMemcpy(cp.data(), dcp.p, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost));
+        SB_CUDA(cudaMemcpy(cn.data(), dcn.p, sizeof(double) * 3 * n3, cudaMemcpyDeviceToHost));
         for (int64_t r = 0; r < n3; ++r)
             for (int c = 0; c < 3; ++c) {
                 points[3 * r + c] = cp[c * n3 + r];
@@ -905,7 +916,7 @@ SB_API int sb_rhs_plane_wave_device(const sb_operator* op, const double* dirs, c
             SB_REQUIRE(std::isfinite(dirs[q]), SB_ERR_INVALID_ARGUMENT, "non-finite direction");
         const Operator& o = *op->op;
         SB_REQUIRE(o.mesh, SB_ERR_INVALID_ARGUMENT, "operator was not assembled from a mesh");
-        if (o.basis == SB_BASIS_LINEAR) {
+        if (o.basis != SB_BASIS_CONSTANT) {
             incident_plane_wave_at(o.device, o.lin_cp.as<double>(), o.lin_cn.as<double>(), o.n, o.n, o.phys, o.beta_re,
                                    o.beta_im, dirs, reinterpret_cast<const double*>(amps), r,
                                    reinterpret_cast<double2*>(rhs_dev), o.stream);

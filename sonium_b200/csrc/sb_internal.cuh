@@ -138,9 +138,10 @@ struct Operator {
     void* work = nullptr;        // solver workspace (gmres.cu), released by destroy_solve_work
     void* tensor = nullptr;      // BF16 split planes for the tensor-core block product (tensor.cu)
     void* multi = nullptr;       // many-right-hand-side solver workspace (batch.cu)
-    // Discontinuous linear basis (n = 3 x elements): collocation points / normals (SoA) and the
+    // Discontinuous bases (n = 3 or 6 x elements): collocation points / normals (SoA) and the
     // near-pair CSR of the collocation rows.
     int basis = SB_BASIS_CONSTANT;
+    double sign = 1.0;  // the stabilised discontinuous systems' sign (every entry times sign)
     DevBuf lin_cp, lin_cn, lin_ptr, lin_col;
     int64_t lin_nnz = 0;
     cudaStream_t stream = nullptr;
@@ -171,9 +172,10 @@ int coefficient_fields();
 
 // Assembly (assembly.cu)
 void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im);
-void assemble_linear(Operator& op, const sb_physics& ph, double beta_re, double beta_im);
-// Collocation points / normals of the linear basis (SoA, 3 x 3n device arrays).
-void lin_collocation(const Mesh& m, double* cp_dev, double* cn_dev);
+// The discontinuous linear / quadratic bases (op.basis, op.sign).
+void assemble_discontinuous(Operator& op, const sb_physics& ph, double beta_re, double beta_im);
+// Collocation points / normals of a discontinuous basis (SoA, 3 x (NB n) device arrays).
+void lin_collocation(const Mesh& m, int basis, double* cp_dev, double* cn_dev);
 // Plane-wave right-hand side at np points with normals (SoA, component c of point i at c * stride
 // + i), on the device.
 void incident_plane_wave_at(int device, const double* pts_dev, const double* nrm_dev, int64_t np, int64_t stride,

@@ -123,7 +123,7 @@ class Mesh:
     def collocation(self, basis: int = L.SB_BASIS_CONSTANT):
         """Collocation points and normals of a basis: (m, 3) each for the constant basis (centroids),
         (3m, 3) for the linear basis (DOF 3e + c)."""
-        rows = self.num_elements * (3 if basis == L.SB_BASIS_LINEAR else 1)
+        rows = self.num_elements * {L.SB_BASIS_LINEAR: 3, L.SB_BASIS_QUADRATIC: 6}.get(basis, 1)
         pts = np.zeros((rows, 3))
         nrm = np.zeros((rows, 3))
         check(L.load().sb_mesh_collocation(self.handle, basis, _p(pts), _p(nrm)))
@@ -316,6 +316,28 @@ def build_tbem_system_linear(mesh: Mesh, physics: PhysicsParams, beta: complex) 
     op.n = 3 * mesh.num_elements
     op.basis = L.SB_BASIS_LINEAR
     return op
+
+
+def build_tbem_system_discontinuous_stabilized(mesh: Mesh, physics: PhysicsParams, sign: float = 1.0,
+                                               beta_scale: float = 1.0,
+                                               basis: int = L.SB_BASIS_QUADRATIC) -> TbemOperator:
+    """build_tbem_system_{linear,quadratic}_stabilized (tbem.rs:2993-3030): the discontinuous
+    linear (3 DOFs per element) or quadratic (6) basis, every entry times sign, beta =
+    burton_miller_beta_scaled(beta_scale)."""
+    beta = physics.burton_miller_beta(beta_scale)
+    h = ct.c_void_p()
+    check(L.load().sb_assemble_discontinuous(mesh.handle, ct.byref(physics._struct()),
+                                             L.SbComplex(beta.real, beta.imag), basis, float(sign), ct.byref(h)))
+    op = TbemOperator(mesh, h, physics, beta, L.SB_PRECISION_FP64)
+    op.n = (6 if basis == L.SB_BASIS_QUADRATIC else 3) * mesh.num_elements
+    op.basis = basis
+    return op
+
+
+def build_tbem_system_quadratic_stabilized(mesh: Mesh, physics: PhysicsParams, sign: float = 1.0,
+                                           beta_scale: float = 1.0) -> TbemOperator:
+    """build_tbem_system_quadratic_stabilized (tbem.rs:3010-3030)."""
+    return build_tbem_system_discontinuous_stabilized(mesh, physics, sign, beta_scale, L.SB_BASIS_QUADRATIC)
 
 
 def rhs_plane_wave_at(points, normals, physics: PhysicsParams, beta: complex, directions, amplitudes=None,

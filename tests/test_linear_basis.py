@@ -1,10 +1,12 @@
-"""Discontinuous linear Tri3 basis (sb_assemble_linear; build_tbem_system_linear,
-crates/sonium-bem/src/core/assembly/tbem.rs:1490-1620).
+"""Discontinuous linear and quadratic Tri3 bases (sb_assemble_linear, sb_assemble_discontinuous;
+build_tbem_system_linear and build_tbem_system_discontinuous_stabilized,
+crates/sonium-bem/src/core/assembly/tbem.rs:1490-1620, 2810-2990).
 
-CPU: the oracle's restatement pinned by identities the reference's formulas imply (the three
-basis functions sum to one and their gradients to zero, so the summed linear channels equal the
+CPU: the oracle's restatement pinned by identities the reference's formulas imply (the basis
+functions sum to one and their gradients to zero, so the summed basis channels equal the
 constant-basis channels of the same source point, the self term when that point is the
-centroid), and by convergence of the solved rigid sphere to the Mie series. GPU: the device
+centroid), by convergence of the solved linear-basis rigid sphere to the Mie series, and for the
+quadratic basis by the reference's own Mie bound. GPU: the device
 matrix against the oracle's entry by entry (1e-10 relative to the entry, floor 1e-8 of the
 largest), the collocation points and incident right-hand side, re-assembly at another
 frequency, the GMRES solution against the oracle's dense solve.
@@ -19,25 +21,58 @@ def _coords(nodes, tris, e):
 
 # ---- CPU: the oracle ----
 
+@pytest.mark.parametrize("nbas", [3, 6])
 @pytest.mark.parametrize("k", [0.5, 2.0, 9.0])
-def test_oracle_linear_channels_sum_to_constant(oracle, k):
+def test_oracle_basis_channels_sum_to_constant(oracle, k, nbas):
     nodes, tris = oracle.icosphere(1.0, 2, (1.0, 0.6, 0.4))
     c, nrm, ar = oracle.element_geometry(nodes, tris)
-    pts, pn = oracle.linear_collocation(nodes, tris)
+    pts, pn = oracle.disc_collocation(nodes, tris, nbas)
     ph = oracle.physics_for_k(k)
     rng = np.random.default_rng(3)
     for r in rng.choice(pts.shape[0], 12, replace=False):
-        i = r // 3
+        i = r // nbas
         for j in (i + 1, (i + 7) % tris.shape[0], int(rng.integers(tris.shape[0]))):
-            if j == i:
+            if j == i or j >= tris.shape[0]:
                 continue
-            lin = oracle.regular_pair_linear(pts[r], pn[r], _coords(nodes, tris, j), ar[j], ph).sum(axis=0)
+            lin = oracle.regular_pair_disc(pts[r], pn[r], _coords(nodes, tris, j), ar[j], ph, nbas).sum(axis=0)
             con = oracle.regular_pair(pts[r], pn[r], _coords(nodes, tris, j), ar[j], ph)
             assert np.max(np.abs(lin - con)) <= 1e-12 * np.max(np.abs(con)), (r, j)
     for e in (0, 5, 77):
-        lin = oracle.singular_pair_linear(c[e], nrm[e], _coords(nodes, tris, e), ph).sum(axis=0)
+        lin = oracle.singular_pair_disc(c[e], nrm[e], _coords(nodes, tris, e), ph, nbas).sum(axis=0)
         con = oracle.singular_pair(c[e], nrm[e], _coords(nodes, tris, e), ph)
         assert np.max(np.abs(lin - con)) <= 1e-11 * np.max(np.abs(con)), e
+
+
+def test_oracle_quadratic_sign_and_sphere(oracle):
+    nodes, tris = oracle.icosphere(1.0, 1)
+    ph = oracle.physics_for_k(2.0)
+    beta = oracle.bm_beta(ph)
+    Ap, _ = oracle.assemble_discontinuous(nodes, tris, ph, beta, 6, 1.0)
+    Am, _ = oracle.assemble_discontinuous(nodes, tris, ph, beta, 6, -1.0)
+    assert np.array_equal(Am, -Ap)
+    # The unknowns are the quadratic Lagrange coefficients (vertex and edge-midpoint values), so
+    # the surface pressure at collocation point c is sum_b x_b N_b(point c). The reference bounds
+    # its own quadratic-panel Mie error at 0.80 (tests/higher_order_formulation_reference.rs:
+    # 264-283): the free term sits on the diagonal as if the basis were cardinal at the
+    # collocation points, which the quadratic one is not.
+    a, b_, c, d = 0.8168475729804585, 0.0915762135097715, 0.108103018168070, 0.445948490915965
+    coll = [(b_, b_), (a, b_), (b_, a), (d, d), (d, c), (c, d)]
+
+    def p2(s, t):
+        l0 = 1 - s - t
+        return [l0 * (2 * l0 - 1), s * (2 * s - 1), t * (2 * t - 1), 4 * l0 * s, 4 * s * t, 4 * t * l0]
+
+    N = np.array([p2(s, t) for s, t in coll])
+    for level in (1, 2):
+        nodes, tris = oracle.icosphere(1.0, level)
+        A, _ = oracle.assemble_discontinuous(nodes, tris, ph, beta, 6)
+        pts, pn = oracle.disc_collocation(nodes, tris, 6)
+        b = oracle.rhs_plane_wave(pts, pn, ph, beta, [[0.0, 0.0, 1.0]])[:, 0]
+        x = np.linalg.solve(A, b)
+        p = (N @ x.reshape(-1, 6).T).T.reshape(-1)
+        _, _, ar = oracle.element_geometry(nodes, tris)
+        err = oracle.rigid_sphere_surface_error(p, pts, np.repeat(ar / 6, 6), 2.0, 1.0)
+        assert np.isfinite(err) and err < 0.8, (level, err)
 
 
 def test_oracle_linear_collocation_points(oracle):
@@ -95,6 +130,26 @@ def test_linear_matrix_matches_oracle(gpu, oracle, level, k, scale):
     assert A.shape == (3 * tris.shape[0],) * 2
     assert _entry_err(A, R) < 1e-10
     assert np.all(op.rhs == 0)
+    op.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level,k,sign", [(1, 2.0, 1.0), (2, 7.0, -1.0)])
+def test_quadratic_matrix_matches_oracle(gpu, oracle, level, k, sign):
+    nodes, tris = oracle.icosphere(1.0, level, (1.0, 0.6, 0.4))
+    mesh = gpu.Mesh(nodes, tris)
+    ph = gpu.PhysicsParams.for_wavenumber(k)
+    op = gpu.build_tbem_system_quadratic_stabilized(mesh, ph, sign=sign, beta_scale=4.0)
+    R, _ = oracle.assemble_discontinuous(nodes, tris, oracle.physics_for_k(k), ph.burton_miller_beta(4.0), 6, sign)
+    assert op.n == 6 * tris.shape[0]
+    assert _entry_err(op.matrix, R) < 1e-10
+    pts, pn = mesh.collocation(gpu.SB_BASIS_QUADRATIC)
+    opts, _ = oracle.disc_collocation(nodes, tris, 6)
+    assert np.max(np.abs(pts - opts)) <= 1e-15
+    # (the quadratic system is poorly conditioned for restarted GMRES: its free term treats the
+    # non-cardinal basis as cardinal; the product is what a solver sees)
+    x = gpu.rhs_plane_wave_at(pts, pn, ph, op.beta, [0.0, 0.0, 1.0])[:, 0]
+    assert np.linalg.norm(op.apply(x) - R @ x) <= 1e-13 * np.linalg.norm(R @ x)
     op.close()
 
 
