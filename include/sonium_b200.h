@@ -100,6 +100,16 @@ typedef struct sb_mesh_info {
  * points and the near-pair list. The default boundary condition is rigid (velocity 0). */
 SB_API int sb_mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris,
                           int64_t n_tris, int device, sb_mesh** out);
+/* A Quad4 mesh (constant panels, element e owns DOF e): quads[e * 4 + v], vertices ordered
+ * around the element so that the bilinear map of (1, 1), (-1, 1), (-1, -1), (1, -1) runs through
+ * them; the element normal is that of the diagonals, (p2 - p0) x (p3 - p1) (compute_element_geometry,
+ * crates/sonium-bem/src/core/mesh/generators.rs:771-850). sb_assemble builds its constant-panel
+ * system with the Quad4 branches of the regular and singular integration (bilinear geometry,
+ * tensor Gauss-Legendre rules, four-quad subdivision; SB_PRECISION_FP64 only, no prescribed
+ * boundary values); the batched, tensor-core, field and discontinuous-basis entry points take
+ * Tri3 meshes only (SB_ERR_UNSUPPORTED_ELEMENT). */
+SB_API int sb_mesh_create_quad4(const double* nodes, int64_t n_nodes, const uint32_t* quads, int64_t n_quads,
+                                int device, sb_mesh** out);
 SB_API int sb_mesh_destroy(sb_mesh* mesh);
 SB_API int sb_mesh_info_get(const sb_mesh* mesh, sb_mesh_info* info);
 /* Element centroid (collocation point), unit normal and area, each n_elements long. */

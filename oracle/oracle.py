@@ -83,6 +83,9 @@ def _declare(L):
     L.or_field_eval.argtypes = [P, P, ct.c_int64, P, P, ct.c_double, ct.c_double, ct.c_double, P,
                                 ct.c_int64, ct.c_int, P]
     L.or_linear_collocation.argtypes = [ct.c_int64, P, P, P, P]
+    L.or_quad_geometry.argtypes = [ct.c_int64, P, P, P, P, P]
+    L.or_assemble_quad.argtypes = [ct.c_int64, P, ct.c_int64, P, ct.POINTER(OrBc), ct.POINTER(OrPhysics), OrC128,
+                                   ct.c_int, P, P]
     L.or_regular_pair_disc.argtypes = [P, P, P, ct.c_double, ct.POINTER(OrPhysics), ct.c_int, P]
     L.or_singular_pair_disc.argtypes = [P, P, P, ct.POINTER(OrPhysics), ct.c_int, P]
     L.or_disc_collocation.argtypes = [ct.c_int64, P, P, ct.c_int, P, P]
@@ -169,6 +172,68 @@ def assemble(nodes, tris, ph: OrPhysics, beta: complex, rows=None, bc_kind=None,
     if rc:
         raise ValueError("oracle assembly rejected its input")
     return A, rhs
+
+
+def quad_geometry(nodes, quads):
+    """Quad4 element geometry: centres, normals, areas (generators.rs:771-850)."""
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    quads = np.ascontiguousarray(quads, np.uint32)
+    m = quads.shape[0]
+    c, n, a = np.zeros((m, 3)), np.zeros((m, 3)), np.zeros(m)
+    lib().or_quad_geometry(m, _p(nodes), _p(quads), _p(c), _p(n), _p(a))
+    return c, n, a
+
+
+def assemble_quad(nodes, quads, ph: OrPhysics, beta: complex, bc_kind=None, bc_value=None, admittance=None,
+                  threads: int = 0):
+    """The constant-panel system of a Quad4 mesh: (m x m matrix, rhs)."""
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    quads = np.ascontiguousarray(quads, np.uint32)
+    m = quads.shape[0]
+    A = np.zeros((m, m), np.complex128)
+    rhs = np.zeros(m, np.complex128)
+    keep = []
+    b = _bc_struct(m, bc_kind, bc_value, admittance, keep)
+    rc = lib().or_assemble_quad(nodes.shape[0], _p(nodes), m, _p(quads), ct.byref(b), ct.byref(ph),
+                                OrC128(beta.real, beta.imag), threads, _p(A), _p(rhs))
+    if rc:
+        raise ValueError("oracle assembly rejected its input")
+    return A, rhs
+
+
+def cubed_sphere(radius: float, n: int, scale=(1.0, 1.0, 1.0)):
+    """Quad4 test mesh: the six faces of a cube split into n x n quads, projected onto the sphere
+    (then scaled per axis), shared nodes merged, vertex order such that (p2 - p0) x (p3 - p1)
+    points outward."""
+    faces = []
+    t = np.linspace(-1.0, 1.0, n + 1)
+    for axis in range(3):
+        for sgn in (1.0, -1.0):
+            u, v = np.meshgrid(t, t, indexing="ij")
+            p = np.zeros((n + 1, n + 1, 3))
+            p[..., axis] = sgn
+            p[..., (axis + 1) % 3] = u
+            p[..., (axis + 2) % 3] = v
+            faces.append((p, axis, sgn))
+    pts, quads, index = [], [], {}
+
+    def node(x):
+        key = tuple(np.round(x, 12))
+        if key not in index:
+            index[key] = len(pts)
+            pts.append(x)
+        return index[key]
+
+    for p, axis, sgn in faces:
+        for i in range(n):
+            for j in range(n):
+                q = [p[i, j], p[i + 1, j], p[i + 1, j + 1], p[i, j + 1]]
+                ids = [node(x / np.linalg.norm(x)) for x in q]
+                if sgn < 0:
+                    ids = ids[::-1]
+                quads.append(ids)
+    nodes = np.array(pts) * radius * np.asarray(scale)
+    return nodes, np.array(quads, np.uint32)
 
 
 def disc_collocation(nodes, tris, nbas: int = 3):

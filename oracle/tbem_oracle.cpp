@@ -1538,3 +1538,374 @@ void or_singular_pair_disc(const double* x, const double* nx, const double* c9, 
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Quad4 constant panels (the ElementType::Quad4 branches of the constant path): element
+// geometry (compute_element_geometry, mesh/generators.rs:771-850, with compute_element_area,
+// mesh/element.rs:326-362), compute_parameters (integration/regular.rs:636-714, bilinear on
+// [-1, 1]^2 with vertices (1, 1), (-1, 1), (-1, -1), (1, -1)), generate_subelements
+// (integration/singular.rs:1372-1540, four quads per split about the subelement centre, leaves
+// mapped by centre and edge factor), quad_quadrature (integration/gauss.rs:159-170) and the
+// Quad4 branch of singular_integration_with_params_mode (integration/singular.rs:297-614).
+// =============================================================================================
+namespace {
+
+const double kCsi8[8] = {1.0, -1.0, -1.0, 1.0, 0.0, -1.0, 0.0, 1.0};
+const double kEta8[8] = {1.0, 1.0, -1.0, -1.0, 1.0, 0.0, -1.0, 0.0};
+
+struct Coords4 {
+    double v[4][3];
+};
+
+void quad_parameters(const Coords4& c, double s, double t, double pos[3], double& jac, double nrm[3]) {
+    const double s1 = 0.25 * (s + 1.0), s2 = 0.25 * (s - 1.0), t1 = t + 1.0, t2 = t - 1.0;
+    const double sf[4] = {s1 * t1, -s2 * t1, s2 * t2, -s1 * t2};
+    const double sds[4] = {0.25 * (t + 1.0), -0.25 * (t + 1.0), 0.25 * (t - 1.0), -0.25 * (t - 1.0)};
+    const double sdt[4] = {0.25 * (s + 1.0), 0.25 * (1.0 - s), 0.25 * (s - 1.0), -0.25 * (s + 1.0)};
+    double dxs[3] = {0, 0, 0}, dxt[3] = {0, 0, 0};
+    pos[0] = pos[1] = pos[2] = 0.0;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 3; ++j) {
+            pos[j] += sf[i] * c.v[i][j];
+            dxs[j] += sds[i] * c.v[i][j];
+            dxt[j] += sdt[i] * c.v[i][j];
+        }
+    double n0 = dxs[1] * dxt[2] - dxs[2] * dxt[1];
+    double n1 = dxs[2] * dxt[0] - dxs[0] * dxt[2];
+    double n2 = dxs[0] * dxt[1] - dxs[1] * dxt[0];
+    jac = std::sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+    if (jac > 1e-15) {
+        nrm[0] = n0 / jac;
+        nrm[1] = n1 / jac;
+        nrm[2] = n2 / jac;
+    } else {
+        nrm[0] = nrm[1] = nrm[2] = 0.0;
+    }
+}
+
+struct QuadLeaf {
+    double xc, ec, factor;
+    int order;
+};
+
+std::vector<QuadLeaf> generate_subelements_quad(const double x[3], const Coords4& c, double area) {
+    const int kMaxNse = 60, kNse = 4, kMaxLeaves = 110;
+    std::vector<QuadLeaf> out;
+    double xs[kMaxNse][4], es[kMaxNse][4];
+    for (int j = 0; j < 4; ++j) {
+        xs[0][j] = kCsi8[j];
+        es[0][j] = kEta8[j];
+    }
+    int nsfl = 1;
+    double faclin = 2.0;
+    for (;;) {
+        int ndie = 0;
+        faclin *= 0.5;
+        const double arels = area * faclin * faclin;
+        const int nsel = nsfl;
+        double xp[kMaxNse][4], ep[kMaxNse][4];
+        std::memcpy(xp, xs, sizeof(double) * 4 * nsel);
+        std::memcpy(ep, es, sizeof(double) * 4 * nsel);
+        for (int idi = 0; idi < nsel; ++idi) {
+            const double sc = (((0.0 + xp[idi][0]) + xp[idi][1]) + xp[idi][2] + xp[idi][3]) / 4.0;
+            const double tc = (((0.0 + ep[idi][0]) + ep[idi][1]) + ep[idi][2] + ep[idi][3]) / 4.0;
+            double g[3], jac, nrm[3];
+            quad_parameters(c, sc, tc, g, jac, nrm);
+            double dx = g[0] - x[0], dy = g[1] - x[1], dz = g[2] - x[2];
+            double ratdis = std::sqrt(dx * dx + dy * dy + dz * dz) / std::sqrt(arels);
+            if (ratdis < 3.0) {
+                ++ndie;
+                if (ndie > 15) break;
+                nsfl = ndie * kNse;
+                const int nsf0 = nsfl - kNse;
+                double xsp[8], esp[8];
+                for (int j = 0; j < 4; ++j) {
+                    int j1 = (j + 1) % 4;
+                    xsp[j] = xp[idi][j];
+                    xsp[j + 4] = (xp[idi][j] + xp[idi][j1]) / 2.0;
+                    esp[j] = ep[idi][j];
+                    esp[j + 4] = (ep[idi][j] + ep[idi][j1]) / 2.0;
+                }
+                for (int j = 0; j < 4; ++j) {
+                    const int nsu = nsf0 + j, j1 = j + 4, j2 = (j == 0) ? 7 : j - 1 + 4;
+                    xs[nsu][0] = xsp[j];
+                    xs[nsu][1] = xsp[j1];
+                    xs[nsu][2] = sc;
+                    xs[nsu][3] = xsp[j2];
+                    es[nsu][0] = esp[j];
+                    es[nsu][1] = esp[j1];
+                    es[nsu][2] = tc;
+                    es[nsu][3] = esp[j2];
+                }
+            } else {
+                QuadLeaf lf;
+                lf.xc = (((0.0 + xp[idi][0]) + xp[idi][1]) + xp[idi][2] + xp[idi][3]) / 4.0;
+                lf.ec = (((0.0 + ep[idi][0]) + ep[idi][1]) + ep[idi][2] + ep[idi][3]) / 4.0;
+                lf.factor = faclin;
+                lf.order = compute_gauss_order(0.5 / ratdis);
+                out.push_back(lf);
+                if (static_cast<int>(out.size()) >= kMaxLeaves) return out;
+            }
+        }
+        if (ndie == 0) break;
+    }
+    return out;
+}
+
+Channels regular_pair_quad(const double x[3], const double nx[3], const Coords4& c, double area,
+                           const or_physics& ph) {
+    const double wavruim = ph.harmonic_factor * ph.wave_number;
+    const double k2 = ph.wave_number * ph.wave_number;
+    Channels r;
+    for (const QuadLeaf& lf : generate_subelements_quad(x, c, area)) {
+        const bool iforie = std::fabs(std::fabs(lf.factor) - 1.0) < 1e-10;
+        std::vector<double> gx, gw;
+        gauss_legendre(lf.order, gx, gw);
+        for (int a = 0; a < lf.order; ++a)
+            for (int b = 0; b < lf.order; ++b) {
+                const double csi = gx[a], eta = gx[b], wq = gw[a] * gw[b];
+                double xio, eto, weih2;
+                if (iforie) {
+                    xio = csi;
+                    eto = eta;
+                    weih2 = wq;
+                } else {
+                    xio = lf.xc + csi * lf.factor;
+                    eto = lf.ec + eta * lf.factor;
+                    weih2 = wq * (lf.factor * lf.factor);
+                }
+                double pos[3], jac, ny[3];
+                quad_parameters(c, xio, eto, pos, jac, ny);
+                double wga = weih2 * jac;
+                double d[3] = {pos[0] - x[0], pos[1] - x[1], pos[2] - x[2]};
+                double u[3];
+                double dis = normalize3(d, u);
+                if (dis < 1e-15) continue;
+                cd zg = exp_i(wavruim * dis) * (wga / (4.0 * kPi * dis));
+                cd zb = zg * cd(-1.0 / dis, wavruim);
+                double rny = u[0] * ny[0] + u[1] * ny[1] + u[2] * ny[2];
+                double rnx = -(u[0] * nx[0] + u[1] * nx[1] + u[2] * nx[2]);
+                double rq = rny * rnx;
+                double nxny = nx[0] * ny[0] + nx[1] * ny[1] + nx[2] * ny[2];
+                double dq = dis * dis;
+                cd ef((3.0 / dq - k2) * rq + nxny / dq, -wavruim / dis * (3.0 * rq + nxny));
+                r.g += zg;
+                r.h += zb * rny;
+                r.ht += zb * rnx;
+                r.e += zg * ef;
+            }
+    }
+    return r;
+}
+
+// estimate_element_size (singular.rs:1641-1676), Quad4: sqrt of the two triangles split on the
+// diagonal 0-2.
+double quad_size(const Coords4& c) {
+    double v1[3], v2[3], v3[3];
+    for (int j = 0; j < 3; ++j) {
+        v1[j] = c.v[1][j] - c.v[0][j];
+        v2[j] = c.v[2][j] - c.v[0][j];
+        v3[j] = c.v[3][j] - c.v[0][j];
+    }
+    double c1[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2], v1[0] * v2[1] - v1[1] * v2[0]};
+    double c2[3] = {v2[1] * v3[2] - v2[2] * v3[1], v2[2] * v3[0] - v2[0] * v3[2], v2[0] * v3[1] - v2[1] * v3[0]};
+    double a1 = 0.5 * std::sqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+    double a2 = 0.5 * std::sqrt(c2[0] * c2[0] + c2[1] * c2[1] + c2[2] * c2[2]);
+    return std::max(std::sqrt(a1 + a2), 1e-10);
+}
+
+Channels singular_pair_quad(const double x[3], const double nx[3], const Coords4& c, const or_physics& ph) {
+    const double wavruim = ph.harmonic_factor * ph.wave_number;
+    const double k2 = ph.wave_number * ph.wave_number;
+    const double ka = ph.wave_number * quad_size(c);
+    SingularParams q;
+    if (ka < 0.3) q = {3, 4, 4, 2};
+    else if (ka < 1.0) q = {4, 5, 6, 2};
+    else if (ka < 2.0) q = {5, 6, 8, 3};
+    else q = {6, 7, 10, 4};
+    std::vector<double> ecx, ecw, scx, scw;
+    gauss_legendre(q.edge_order, ecx, ecw);
+    gauss_legendre(q.sub_order, scx, scw);
+    const int nsec1 = q.sections, nsec2 = q.subtri;
+    Channels r;
+    for (int ieg = 0; ieg < 4; ++ieg) {
+        const int ig1 = (ieg + 1) % 4, ig2 = ieg + 4;
+        double dp[3];
+        double leneg = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            dp[i] = c.v[ig1][i] - c.v[ieg][i];
+            leneg += dp[i] * dp[i];
+        }
+        leneg = std::sqrt(leneg);
+        const double dpo[3] = {dp[0] / leneg, dp[1] / leneg, dp[2] / leneg};
+        const double leneg_scaled = leneg / (2.0 * nsec1);
+        cd zre(0, 0);
+        const double delsec = 2.0 / nsec1;
+        double secmid = -1.0 - delsec / 2.0;
+        for (int is = 0; is < nsec1; ++is) {
+            secmid += delsec;
+            for (int ig = 0; ig < q.edge_order; ++ig) {
+                double sga = secmid + ecx[ig] / nsec1;
+                double wga = ecw[ig] * leneg_scaled;
+                double d[3];
+                for (int i = 0; i < 3; ++i) d[i] = c.v[ieg][i] + dp[i] * (sga + 1.0) / 2.0 - x[i];
+                double u[3];
+                double dis = normalize3(d, u);
+                if (dis < 1e-15) continue;
+                cd zg = exp_i(wavruim * dis) / (4.0 * kPi * dis);
+                cd zf = zg * cd(-1.0 / dis, wavruim);
+                cd zd[3] = {zf * u[0], zf * u[1], zf * u[2]};
+                cd w0 = zd[1] * dpo[2] - zd[2] * dpo[1];
+                cd w1 = zd[2] * dpo[0] - zd[0] * dpo[2];
+                cd w2 = zd[0] * dpo[1] - zd[1] * dpo[0];
+                zre += (w0 * nx[0] + w1 * nx[1] + w2 * nx[2]) * wga;
+            }
+        }
+        r.e += zre;
+        for (int isec = 0; isec < nsec2; ++isec) {
+            const double aresub = 0.25 / nsec2;
+            double ss[3] = {0.0, 0.0, 0.0}, ts[3] = {0.0, 0.0, 0.0};
+            if (isec == 0) {
+                ss[1] = kCsi8[ieg];
+                ss[2] = kCsi8[ig2];
+                ts[1] = kEta8[ieg];
+                ts[2] = kEta8[ig2];
+            } else {
+                ss[1] = kCsi8[ig2];
+                ss[2] = kCsi8[ig1];
+                ts[1] = kEta8[ig2];
+                ts[2] = kEta8[ig1];
+            }
+            for (int a = 0; a < q.sub_order; ++a)
+                for (int b = 0; b < q.sub_order; ++b) {
+                    const double sga = scx[a], tga = scx[b], wei = scw[a] * scw[b];
+                    double sgg = 0.5 * (1.0 - sga) * ss[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ss[1] + (1.0 + tga) * ss[2]);
+                    double tgg = 0.5 * (1.0 - sga) * ts[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ts[1] + (1.0 + tga) * ts[2]);
+                    double pos[3], jac, ny[3];
+                    quad_parameters(c, sgg, tgg, pos, jac, ny);
+                    double wga = wei * (1.0 + sga) * aresub * jac;
+                    double d[3] = {pos[0] - x[0], pos[1] - x[1], pos[2] - x[2]};
+                    double u[3];
+                    double dis = normalize3(d, u);
+                    if (dis < 1e-15) continue;
+                    cd zg = exp_i(wavruim * dis) * (wga / (4.0 * kPi * dis));
+                    cd zb = zg * cd(-1.0 / dis, wavruim);
+                    double rny = u[0] * ny[0] + u[1] * ny[1] + u[2] * ny[2];
+                    double rnx = -(u[0] * nx[0] + u[1] * nx[1] + u[2] * nx[2]);
+                    r.g += zg;
+                    r.h += zb * rny;
+                    r.ht += zb * rnx;
+                    double nd = nx[0] * ny[0] + nx[1] * ny[1] + nx[2] * ny[2];
+                    r.e += zg * k2 * nd;
+                }
+        }
+    }
+    return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+// compute_element_geometry (generators.rs:771-850) for Quad4 elements: centre = node average,
+// normal from the diagonal cross product (p2 - p0) x (p3 - p1), area = compute_element_area
+// (element.rs:326-362, the mean of both diagonal splits).
+void or_quad_geometry(int64_t m, const double* nodes, const uint32_t* quads, double* centers, double* normals,
+                      double* areas) {
+    for (int64_t e = 0; e < m; ++e) {
+        const uint32_t* q = quads + 4 * e;
+        double p[4][3];
+        for (int a = 0; a < 4; ++a)
+            for (int j = 0; j < 3; ++j) p[a][j] = nodes[3 * q[a] + j];
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int a = 0; a < 4; ++a) s += p[a][j];
+            centers[3 * e + j] = s / 4.0;
+        }
+        double d1[3], d2[3];
+        for (int j = 0; j < 3; ++j) {
+            d1[j] = p[2][j] - p[0][j];
+            d2[j] = p[3][j] - p[1][j];
+        }
+        double cr[3] = {d1[1] * d2[2] - d1[2] * d2[1], d1[2] * d2[0] - d1[0] * d2[2], d1[0] * d2[1] - d1[1] * d2[0]};
+        double len = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        for (int j = 0; j < 3; ++j) normals[3 * e + j] = len > 1e-15 ? cr[j] / len : 0.0;
+        auto sub = [&](int a, int b, double o[3]) {
+            for (int j = 0; j < 3; ++j) o[j] = p[a][j] - p[b][j];
+        };
+        auto clen = [](const double a[3], const double b[3]) {
+            double c0 = a[1] * b[2] - a[2] * b[1], c1 = a[2] * b[0] - a[0] * b[2], c2 = a[0] * b[1] - a[1] * b[0];
+            return std::sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+        };
+        double v1[3], v2[3], v3[3], v4[3], v5[3], v6[3];
+        sub(1, 0, v1);
+        sub(2, 0, v2);
+        sub(3, 0, v3);
+        sub(2, 1, v4);
+        sub(3, 1, v5);
+        sub(0, 1, v6);
+        const double a1 = 0.5 * clen(v1, v2), a2 = 0.5 * clen(v2, v3), a3 = 0.5 * clen(v4, v5),
+                     a4 = 0.5 * clen(v5, v6);
+        areas[e] = 0.5 * (a1 + a2 + a3 + a4);
+    }
+}
+
+// The constant-panel system of a Quad4 mesh (build_tbem_system_with_beta_parallel, tbem.rs:
+// 1284-1466, Quad4 branches): A is m x m row-major.
+int or_assemble_quad(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* quads, const or_bc* bc,
+                     const or_physics* ph, or_c128 beta_in, int threads, or_c128* A, or_c128* rhs) {
+    if (m <= 0) return 1;
+    for (int64_t i = 0; i < 4 * m; ++i)
+        if (quads[i] >= static_cast<uint64_t>(n_nodes)) return 1;
+    std::vector<double> centers(3 * m), normals(3 * m), areas(m);
+    or_quad_geometry(m, nodes, quads, centers.data(), normals.data(), areas.data());
+    std::vector<Coords4> coords(m);
+    for (int64_t e = 0; e < m; ++e)
+        for (int a = 0; a < 4; ++a)
+            for (int j = 0; j < 3; ++j) coords[e].v[a][j] = nodes[3 * quads[4 * e + a] + j];
+    const cd gamma(1.0, 0.0), tau(ph->tau, 0.0), iwr(0.0, ph->pressure_factor);
+    const cd beta = C(beta_in);
+    std::vector<BcView> bcs(m);
+    for (int64_t e = 0; e < m; ++e) bcs[e] = bc_at(bc, e);
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t i = 0; i < m; ++i) {
+        std::vector<cd> local(m, cd(0, 0));
+        cd lrhs(0, 0);
+        const BcView& sb = bcs[i];
+        if (sb.kind == 0) {
+            local[i] -= gamma * 0.5;
+            if (sb.has_adm) local[i] -= sb.adm * iwr * beta * tau * 0.5;
+            lrhs += sb.value * iwr * beta * tau * 0.5;
+        } else if (sb.kind == 1) {
+            local[i] += beta * tau * 0.5;
+            lrhs -= sb.value * gamma * 0.5;
+        }
+        const double* x = &centers[3 * i];
+        const double* nx = &normals[3 * i];
+        for (int64_t j = 0; j < m; ++j) {
+            const BcView& fb = bcs[j];
+            Channels r = (j == i) ? singular_pair_quad(x, nx, coords[j], *ph)
+                                  : regular_pair_quad(x, nx, coords[j], areas[j], *ph);
+            cd coeff(0, 0);
+            if (fb.kind == 0) {
+                coeff = r.h * gamma * tau + r.e * beta;
+                if (fb.has_adm) coeff -= (r.g * gamma * tau + r.ht * beta) * fb.adm * iwr;
+            } else if (fb.kind == 1) {
+                coeff = -(r.g * gamma * tau + r.ht * beta);
+            }
+            local[j] += coeff;
+            if (std::abs(fb.value) > 1e-15) {
+                if (fb.kind == 0)
+                    lrhs += (r.g * gamma * tau + r.ht * beta) * fb.value * iwr;
+                else if (fb.kind == 1)
+                    lrhs += (r.h * gamma * tau + r.e * beta) * fb.value;
+            }
+        }
+        for (int64_t j = 0; j < m; ++j) A[i * m + j] = O(local[j]);
+        if (rhs) rhs[i] = O(lrhs);
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -130,6 +130,14 @@ int or_assemble_discontinuous(int64_t n_nodes, const double* nodes, int64_t n_tr
                               const or_bc* bc, const or_physics* phys, or_c128 beta, int nbas, double sign,
                               int threads, or_c128* A, or_c128* rhs);
 
+/* Quad4 constant panels: element geometry (centre, diagonal-cross normal, mean-split area) and
+ * the m x m constant-panel system. */
+void or_quad_geometry(int64_t n_quads, const double* nodes, const uint32_t* quads, double* centers,
+                      double* normals, double* areas);
+int or_assemble_quad(int64_t n_nodes, const double* nodes, int64_t n_quads, const uint32_t* quads,
+                     const or_bc* bc, const or_physics* phys, or_c128 beta, int threads, or_c128* A,
+                     or_c128* rhs);
+
 void or_field_eval(const double* nodes, const uint32_t* tris, int64_t n_tris, const or_c128* pressure,
                    const or_c128* velocity, double k, double harmonic_factor, double pressure_factor,
                    const double* points, int64_t m, int threads, or_c128* out);

@@ -114,6 +114,7 @@ _SIGNATURES = {
     "sb_icosphere_counts": ([ct.c_int, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)], ct.c_int),
     "sb_icosphere": ([ct.c_double, ct.c_int, P, P, P], ct.c_int),
     "sb_mesh_create": ([P, ct.c_int64, P, ct.c_int64, ct.c_int, ct.POINTER(P)], ct.c_int),
+    "sb_mesh_create_quad4": ([P, ct.c_int64, P, ct.c_int64, ct.c_int, ct.POINTER(P)], ct.c_int),
     "sb_mesh_destroy": ([P], ct.c_int),
     "sb_mesh_info_get": ([P, ct.POINTER(SbMeshInfo)], ct.c_int),
     "sb_mesh_element_geometry": ([P, P, P, P], ct.c_int),

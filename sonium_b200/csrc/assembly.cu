@@ -1630,6 +1630,504 @@ __global__ void __launch_bounds__(128) k_lin_self(const double* __restrict__ ele
     }
 }
 
+// =============================================================================================
+// Quad4 constant panels (the ElementType::Quad4 branches of the constant path): bilinear geometry
+// on [-1, 1]^2 with vertices (1, 1), (-1, 1), (-1, -1), (1, -1) (compute_parameters,
+// integration/regular.rs:636-714), tensor Gauss-Legendre rules (quad_quadrature,
+// integration/gauss.rs:159-170), four-quad subdivision about the subelement centre
+// (generate_subelements, integration/singular.rs:1372-1540), the Quad4 self term
+// (singular.rs:297-614). FP64, complex128 output.
+// =============================================================================================
+__constant__ double c_csi8[8] = {1.0, -1.0, -1.0, 1.0, 0.0, -1.0, 0.0, 1.0};
+__constant__ double c_eta8[8] = {1.0, 1.0, -1.0, -1.0, 1.0, 0.0, -1.0, 0.0};
+constexpr int kQuadTile = 64;   // columns per far-kernel CTA
+constexpr int kQuadRows = 32;   // rows per far-kernel CTA
+constexpr int kQuadFar = 16;    // far leaf: the 4 x 4 rule
+
+// Position, Jacobian and unit normal of the bilinear map at (s, t), correctly rounded operations
+// in the reference's order (the subdivision decisions depend on the positions).
+__device__ __forceinline__ void quad_params(const double V[4][3], double s, double t, double pos[3], double& jac,
+                                            double nrm[3]) {
+    const double s1 = __dmul_rn(0.25, __dadd_rn(s, 1.0)), s2 = __dmul_rn(0.25, __dsub_rn(s, 1.0));
+    const double t1 = __dadd_rn(t, 1.0), t2 = __dsub_rn(t, 1.0);
+    const double sf[4] = {__dmul_rn(s1, t1), -__dmul_rn(s2, t1), __dmul_rn(s2, t2), -__dmul_rn(s1, t2)};
+    const double a = __dmul_rn(0.25, __dadd_rn(t, 1.0)), b = __dmul_rn(0.25, __dsub_rn(t, 1.0));
+    const double sds[4] = {a, -a, b, -b};
+    const double c = __dmul_rn(0.25, __dadd_rn(s, 1.0)), d = __dmul_rn(0.25, __dsub_rn(1.0, s));
+    const double sdt[4] = {c, d, __dmul_rn(0.25, __dsub_rn(s, 1.0)), -c};
+    double dxs[3] = {0.0, 0.0, 0.0}, dxt[3] = {0.0, 0.0, 0.0};
+    pos[0] = pos[1] = pos[2] = 0.0;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 3; ++j) {
+            pos[j] = __dadd_rn(pos[j], __dmul_rn(sf[i], V[i][j]));
+            dxs[j] = __dadd_rn(dxs[j], __dmul_rn(sds[i], V[i][j]));
+            dxt[j] = __dadd_rn(dxt[j], __dmul_rn(sdt[i], V[i][j]));
+        }
+    const double n0 = __dsub_rn(__dmul_rn(dxs[1], dxt[2]), __dmul_rn(dxs[2], dxt[1]));
+    const double n1 = __dsub_rn(__dmul_rn(dxs[2], dxt[0]), __dmul_rn(dxs[0], dxt[2]));
+    const double n2 = __dsub_rn(__dmul_rn(dxs[0], dxt[1]), __dmul_rn(dxs[1], dxt[0]));
+    jac = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(n0, n0), __dmul_rn(n1, n1)), __dmul_rn(n2, n2)));
+    if (jac > 1e-15) {
+        nrm[0] = __ddiv_rn(n0, jac);
+        nrm[1] = __ddiv_rn(n1, jac);
+        nrm[2] = __ddiv_rn(n2, jac);
+    } else {
+        nrm[0] = nrm[1] = nrm[2] = 0.0;
+    }
+}
+
+__device__ __forceinline__ void quad_vertices(const double* __restrict__ elem, int64_t ld, int64_t e,
+                                              double V[4][3]) {
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) V[a][c] = E(EV0X + 3 * a + c, e);
+    for (int c = 0; c < 3; ++c) V[3][c] = E(EV3X + c, e);
+}
+
+// compute_element_geometry (mesh/generators.rs:771-850) for Quad4: centre = node average,
+// normal from the diagonal cross product (p2 - p0) x (p3 - p1), area = compute_element_area
+// (mesh/element.rs:326-362, mean of both diagonal splits); level-0 subdivision centre =
+// the bilinear map at (0, 0).
+__global__ void k_quad_geometry(const double* __restrict__ nodes, const uint32_t* __restrict__ quads, int64_t n,
+                                int64_t ld, double* __restrict__ elem) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ld) return;
+    if (e >= n) {
+        for (int f = 0; f < EFIELDS; ++f) E(f, e) = 0.0;
+        return;
+    }
+    double V[4][3];
+    for (int a = 0; a < 4; ++a)
+        for (int j = 0; j < 3; ++j) V[a][j] = nodes[3 * (int64_t)quads[4 * e + a] + j];
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 3; ++j) E(EV0X + 3 * a + j, e) = V[a][j];
+    for (int j = 0; j < 3; ++j) E(EV3X + j, e) = V[3][j];
+    for (int j = 0; j < 3; ++j) {
+        const double sm = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(0.0, V[0][j]), V[1][j]), V[2][j]), V[3][j]);
+        E(ECX + j, e) = __ddiv_rn(sm, 4.0);
+    }
+    auto cross_len = [](const double* a, const double* b) {
+        const double c0 = __dsub_rn(__dmul_rn(a[1], b[2]), __dmul_rn(a[2], b[1]));
+        const double c1 = __dsub_rn(__dmul_rn(a[2], b[0]), __dmul_rn(a[0], b[2]));
+        const double c2 = __dsub_rn(__dmul_rn(a[0], b[1]), __dmul_rn(a[1], b[0]));
+        return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(c0, c0), __dmul_rn(c1, c1)), __dmul_rn(c2, c2)));
+    };
+    double d1[3], d2[3];
+    for (int j = 0; j < 3; ++j) {
+        d1[j] = __dsub_rn(V[2][j], V[0][j]);
+        d2[j] = __dsub_rn(V[3][j], V[1][j]);
+    }
+    const double c0 = __dsub_rn(__dmul_rn(d1[1], d2[2]), __dmul_rn(d1[2], d2[1]));
+    const double c1 = __dsub_rn(__dmul_rn(d1[2], d2[0]), __dmul_rn(d1[0], d2[2]));
+    const double c2 = __dsub_rn(__dmul_rn(d1[0], d2[1]), __dmul_rn(d1[1], d2[0]));
+    const double len = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(c0, c0), __dmul_rn(c1, c1)), __dmul_rn(c2, c2)));
+    if (len > 1e-15) {
+        E(ENX, e) = __ddiv_rn(c0, len);
+        E(ENY, e) = __ddiv_rn(c1, len);
+        E(ENZ, e) = __ddiv_rn(c2, len);
+    } else {
+        E(ENX, e) = E(ENY, e) = E(ENZ, e) = 0.0;
+    }
+    double v1[3], v2[3], v3[3], v4[3], v5[3], v6[3];
+    for (int j = 0; j < 3; ++j) {
+        v1[j] = __dsub_rn(V[1][j], V[0][j]);
+        v2[j] = __dsub_rn(V[2][j], V[0][j]);
+        v3[j] = __dsub_rn(V[3][j], V[0][j]);
+        v4[j] = __dsub_rn(V[2][j], V[1][j]);
+        v5[j] = __dsub_rn(V[3][j], V[1][j]);
+        v6[j] = __dsub_rn(V[0][j], V[1][j]);
+    }
+    const double a1 = __dmul_rn(0.5, cross_len(v1, v2)), a2 = __dmul_rn(0.5, cross_len(v2, v3));
+    const double a3 = __dmul_rn(0.5, cross_len(v4, v5)), a4 = __dmul_rn(0.5, cross_len(v5, v6));
+    E(EAREA, e) = __dmul_rn(0.5, __dadd_rn(__dadd_rn(__dadd_rn(a1, a2), a3), a4));
+    E(EJAC, e) = 0.0;
+    double g[3], jac, nrm[3];
+    quad_params(V, 0.0, 0.0, g, jac, nrm);
+    for (int j = 0; j < 3; ++j) E(EGX + j, e) = g[j];
+    E(ESQA, e) = __dsqrt_rn(E(EAREA, e));
+}
+
+// Far points of every element: the 4 x 4 Gauss-Legendre rule (quad_quadrature(4)) mapped by the
+// bilinear map, weight * Jacobian and the local normal: qq[(q * 7 + f) * ld + e].
+__global__ void k_quad_points(const double* __restrict__ elem, int64_t n, int64_t ld, double* __restrict__ qq) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= ld) return;
+    double V[4][3];
+    if (e < n) quad_vertices(elem, ld, e, V);
+    const int o = 4 * 3 / 2;  // Gauss-Legendre order 4 in the triangular GL table
+    for (int q = 0; q < kQuadFar; ++q) {
+        double v[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (e < n) {
+            const int a = q / 4, b = q % 4;
+            double pos[3], jac, nrm[3];
+            quad_params(V, c_gl_x[o + a], c_gl_x[o + b], pos, jac, nrm);
+            v[0] = pos[0];
+            v[1] = pos[1];
+            v[2] = pos[2];
+            v[3] = c_gl_w[o + a] * c_gl_w[o + b] * jac;
+            v[4] = nrm[0];
+            v[5] = nrm[1];
+            v[6] = nrm[2];
+        }
+        for (int f = 0; f < 7; ++f) qq[(int64_t)(q * 7 + f) * ld + e] = v[f];
+    }
+}
+
+// Far pairs of a Quad4 mesh: one thread per field element (64-column tiles), 32 rows per CTA,
+// the column tile's 16 far points (position, weight * Jacobian, normal) in shared memory.
+__global__ void __launch_bounds__(kQuadTile) k_quad_far(const double* __restrict__ qq,
+                                                        const double* __restrict__ elem, int64_t n, int64_t ld,
+                                                        const double* __restrict__ coef, double k,
+                                                        double2* __restrict__ A) {
+    extern __shared__ __align__(16) double smem[];
+    double* sq = smem;                                 // [16 * 7][kQuadTile]
+    double* sr = smem + kQuadFar * 7 * kQuadTile;      // [kQuadRows][6]
+    const int tid = threadIdx.x;
+    const int64_t j0 = blockIdx.x * (int64_t)kQuadTile;
+    const int64_t j = j0 + tid;
+    const int64_t row0 = blockIdx.y * (int64_t)kQuadRows;
+    const double k2 = k * k;
+    for (int f = 0; f < kQuadFar * 7; ++f) sq[f * kQuadTile + tid] = (j < ld) ? qq[(int64_t)f * ld + j] : 0.0;
+    for (int t = tid; t < kQuadRows * 6; t += kQuadTile) {
+        const int rr = t / 6, f = t % 6;
+        const int64_t i = row0 + rr;
+        sr[t] = (i < n) ? E(ECX + f, i) : 0.0;
+    }
+    double gx = 0, gy = 0, gz = 0, thr = -1;
+    if (j < n) {
+        gx = E(EGX, j);
+        gy = E(EGY, j);
+        gz = E(EGZ, j);
+        thr = near_threshold(E(EAREA, j));
+    }
+    __syncthreads();
+    const int64_t rows_here = (n - row0 < kQuadRows) ? (n - row0) : kQuadRows;
+    for (int rr = 0; rr < rows_here; ++rr) {
+        const int64_t i = row0 + rr;
+        const double xx = sr[rr * 6 + 0], xy = sr[rr * 6 + 1], xz = sr[rr * 6 + 2];
+        const double nxx = sr[rr * 6 + 3], nxy = sr[rr * 6 + 4], nxz = sr[rr * 6 + 5];
+        const bool active = (j < n) && (j != i) && !near_superset(gx, gy, gz, thr, xx, xy, xz);
+        if (!active) continue;
+        Acc a;
+        for (int q = 0; q < kQuadFar; ++q) {
+            const double* p = sq + q * 7 * kQuadTile + tid;
+            const double dx = p[0] - xx, dy = p[kQuadTile] - xy, dz = p[2 * kQuadTile] - xz;
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            const double rinv = sb_rsqrt2(d2);
+            point_channels(a, dx, dy, dz, d2 * rinv, rinv, p[3 * kQuadTile], p[4 * kQuadTile], p[5 * kQuadTile],
+                           p[6 * kQuadTile], nxx, nxy, nxz, k, k2);
+        }
+        A[i * n + j] = combine(a, coef, ld, j, CF_CG);
+    }
+}
+
+struct QuadWarpSmem {
+    double xs[2][kMaxNse][4];
+    double es[2][kMaxNse][4];
+    double lc[kMaxNse][3];  // kept leaves of the current level: centre (s, t) and edge factor
+    int lorder[kMaxNse];
+    int loff[kMaxNse + 1];
+};
+
+// Regular-integration channels of Quad4 element j seen from x (normal nx), lane-partial sums:
+// the level-by-level replay of generate_subelements with the subelements of a level spread
+// over the lanes, ballots for the split decisions (the 16th split ends the level), the 110-leaf
+// cap, each kept leaf's order x order Gauss-Legendre points spread over the lanes.
+__device__ void quad_near_channels(Acc& a, QuadWarpSmem& S, const double* __restrict__ elem, int64_t ld,
+                                   double x0, double x1, double x2, double nxx, double nxy, double nxz, int64_t j,
+                                   double k, double k2, int lane) {
+    double V[4][3];
+    quad_vertices(elem, ld, j, V);
+    const double area = E(EAREA, j);
+    if (lane == 0) {
+        for (int v = 0; v < 4; ++v) {
+            S.xs[0][0][v] = c_csi8[v];
+            S.es[0][0][v] = c_eta8[v];
+        }
+    }
+    __syncwarp();
+    int cur = 0, nsel = 1, total = 0;
+    double faclin = 2.0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int level = 0; level < 64; ++level) {
+        faclin *= 0.5;
+        const double arels = __dmul_rn(__dmul_rn(area, faclin), faclin);
+        const double sqa = __dsqrt_rn(arels);
+        bool sub[2] = {false, false};
+        double rat[2] = {0.0, 0.0}, scs[2] = {0.0, 0.0}, tcs[2] = {0.0, 0.0};
+        for (int h = 0; h < 2; ++h) {
+            const int s = lane + 32 * h;
+            if (s < nsel) {
+                const double* xp = S.xs[cur][s];
+                const double* ep = S.es[cur][s];
+                const double sc = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(0.0, xp[0]), xp[1]), xp[2]), xp[3]), 4.0);
+                const double tc = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(0.0, ep[0]), ep[1]), ep[2]), ep[3]), 4.0);
+                double g[3], jac, nrm[3];
+                quad_params(V, sc, tc, g, jac, nrm);
+                const double dx = __dsub_rn(g[0], x0), dy = __dsub_rn(g[1], x1), dz = __dsub_rn(g[2], x2);
+                const double dist = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+                rat[h] = __ddiv_rn(dist, sqa);
+                sub[h] = rat[h] < 3.0;
+                scs[h] = sc;
+                tcs[h] = tc;
+            }
+        }
+        const unsigned m0 = __ballot_sync(0xffffffffu, sub[0]);
+        const unsigned m1 = __ballot_sync(0xffffffffu, sub[1]);
+        const int nsub = __popc(m0) + __popc(m1);
+        int breakpos = nsel;
+        if (nsub >= 16) {
+            if (__popc(m0) >= 16) {
+                unsigned m = m0;
+                for (int t = 0; t < 15; ++t) m &= m - 1;
+                breakpos = __ffs(m) - 1;
+            } else {
+                unsigned m = m1;
+                for (int t = 0; t < 15 - __popc(m0); ++t) m &= m - 1;
+                breakpos = 32 + __ffs(m) - 1;
+            }
+        }
+        const unsigned valid0 = breakpos >= 32 ? 0xffffffffu : ((1u << breakpos) - 1u);
+        const unsigned valid1 = breakpos >= 64 ? 0xffffffffu : (breakpos <= 32 ? 0u : ((1u << (breakpos - 32)) - 1u));
+        const unsigned nsel0 = nsel >= 32 ? 0xffffffffu : ((1u << nsel) - 1u);
+        const unsigned nsel1 = nsel >= 64 ? 0xffffffffu : (nsel <= 32 ? 0u : ((1u << (nsel - 32)) - 1u));
+        const unsigned l0 = ~m0 & valid0 & nsel0;
+        const unsigned l1 = ~m1 & valid1 & nsel1;
+        const int nleaf = __popc(l0) + __popc(l1);
+        const int keep = min(nleaf, kMaxLeaves - total);
+        const int nxt = cur ^ 1;
+        for (int h = 0; h < 2; ++h) {
+            const int s = lane + 32 * h;
+            if (s >= nsel) continue;
+            const unsigned lm = h == 0 ? l0 : l1;
+            if (lm & (1u << lane)) {
+                const int rank = (h == 0) ? __popc(l0 & lt) : __popc(l0) + __popc(l1 & lt);
+                if (rank < keep) {
+                    S.lc[rank][0] = scs[h];
+                    S.lc[rank][1] = tcs[h];
+                    S.lc[rank][2] = faclin;
+                    S.lorder[rank] = gauss_order(0.5 / rat[h]);
+                }
+            }
+            const unsigned sm = h == 0 ? m0 : m1;
+            if (sm & (1u << lane)) {
+                const int rank = (h == 0) ? __popc(m0 & lt) : __popc(m0) + __popc(m1 & lt);
+                if (rank < 15) {
+                    const double* xp = S.xs[cur][s];
+                    const double* ep = S.es[cur][s];
+                    double xm[8], em[8];
+                    for (int t = 0; t < 4; ++t) {
+                        const int t1 = (t + 1) % 4;
+                        xm[t] = xp[t];
+                        xm[t + 4] = (xp[t] + xp[t1]) / 2.0;
+                        em[t] = ep[t];
+                        em[t + 4] = (ep[t] + ep[t1]) / 2.0;
+                    }
+                    const int b = 4 * rank;
+                    for (int t = 0; t < 4; ++t) {
+                        const int t2 = (t == 0) ? 7 : t + 3;
+                        S.xs[nxt][b + t][0] = xm[t];
+                        S.xs[nxt][b + t][1] = xm[t + 4];
+                        S.xs[nxt][b + t][2] = scs[h];
+                        S.xs[nxt][b + t][3] = xm[t2];
+                        S.es[nxt][b + t][0] = em[t];
+                        S.es[nxt][b + t][1] = em[t + 4];
+                        S.es[nxt][b + t][2] = tcs[h];
+                        S.es[nxt][b + t][3] = em[t2];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int o = 0;
+            for (int l = 0; l < keep; ++l) {
+                S.loff[l] = o;
+                o += S.lorder[l] * S.lorder[l];
+            }
+            S.loff[keep] = o;
+        }
+        __syncwarp();
+        const int npts = S.loff[keep];
+        for (int f = lane; f < npts; f += 32) {
+            int lo = 0, hi = keep - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (S.loff[mid] <= f) lo = mid; else hi = mid - 1;
+            }
+            const int l = lo, ord = S.lorder[l];
+            const int q = f - S.loff[l];
+            const int go = ord * (ord - 1) / 2;
+            const double csi = c_gl_x[go + q / ord], eta = c_gl_x[go + q % ord];
+            const double wq = c_gl_w[go + q / ord] * c_gl_w[go + q % ord];
+            const double fac = S.lc[l][2];
+            const bool iforie = fabs(fabs(fac) - 1.0) < 1e-10;
+            double xio, eto, weih2;
+            if (iforie) {
+                xio = csi;
+                eto = eta;
+                weih2 = wq;
+            } else {
+                xio = S.lc[l][0] + csi * fac;
+                eto = S.lc[l][1] + eta * fac;
+                weih2 = wq * (fac * fac);
+            }
+            double pos[3], jac, ny[3];
+            quad_params(V, xio, eto, pos, jac, ny);
+            const double dx = pos[0] - x0, dy = pos[1] - x1, dz = pos[2] - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            point_channels(a, dx, dy, dz, dis, rinv, weih2 * jac, ny[0], ny[1], ny[2], nxx, nxy, nxz, k, k2);
+        }
+        total += keep;
+        __syncwarp();
+        if (total >= kMaxLeaves || nsub == 0) break;
+        nsel = min(nsub, 15) * 4;
+        cur = nxt;
+    }
+}
+
+__global__ void __launch_bounds__(32 * kNearWarps) k_quad_near(const double* __restrict__ elem, int64_t n, int64_t ld,
+                                                               const int64_t* __restrict__ row_ptr,
+                                                               const int32_t* __restrict__ cols, int64_t nnz,
+                                                               const double* __restrict__ coef, double k,
+                                                               double2* __restrict__ A) {
+    __shared__ QuadWarpSmem sm[kNearWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t p = blockIdx.x * (int64_t)kNearWarps + warp;
+    if (p >= nnz) return;
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (row_ptr[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    const int64_t i = lo, j = cols[p];
+    Acc a;
+    quad_near_channels(a, sm[warp], elem, ld, E(ECX, i), E(ECY, i), E(ECZ, i), E(ENX, i), E(ENY, i), E(ENZ, i), j, k,
+                       k * k, lane);
+    const Acc t = warp_reduce(a);
+    if (lane == 0) A[i * n + j] = combine(t, coef, ld, j, CF_CG);
+}
+
+// Self term of a Quad4 element (the Quad4 branch of singular_integration_with_params_mode,
+// singular.rs:297-614): four edges, sub-triangles fanned from the centre (0, 0) over each edge's
+// two halves (area weight 1/4 / nsec2), the bilinear map's Jacobian and normal per point; the
+// quadrature parameters from estimate_element_size (singular.rs:1641-1676: sqrt of the two
+// triangles split along the diagonal 0-2).
+__global__ void __launch_bounds__(128) k_quad_self(const double* __restrict__ elem, int64_t n, int64_t ld,
+                                                   const double* __restrict__ coef, double k,
+                                                   double2* __restrict__ A, double2* __restrict__ diag) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp;
+    if (i >= n) return;
+    const double k2 = k * k;
+    const double x0 = E(ECX, i), x1 = E(ECY, i), x2 = E(ECZ, i);
+    const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
+    double V[4][3];
+    quad_vertices(elem, ld, i, V);
+    double size;
+    {
+        double v1[3], v2[3], v3[3];
+        for (int c = 0; c < 3; ++c) {
+            v1[c] = V[1][c] - V[0][c];
+            v2[c] = V[2][c] - V[0][c];
+            v3[c] = V[3][c] - V[0][c];
+        }
+        const double c10 = v1[1] * v2[2] - v1[2] * v2[1], c11 = v1[2] * v2[0] - v1[0] * v2[2],
+                     c12 = v1[0] * v2[1] - v1[1] * v2[0];
+        const double c20 = v2[1] * v3[2] - v2[2] * v3[1], c21 = v2[2] * v3[0] - v2[0] * v3[2],
+                     c22 = v2[0] * v3[1] - v2[1] * v3[0];
+        const double a1 = 0.5 * sqrt(c10 * c10 + c11 * c11 + c12 * c12);
+        const double a2 = 0.5 * sqrt(c20 * c20 + c21 * c21 + c22 * c22);
+        size = fmax(sqrt(a1 + a2), 1e-10);
+    }
+    const double ka = k * size;
+    int ngpo1, nsub, nsec1, nsec2;
+    if (ka < 0.3) { ngpo1 = 3; nsub = 4; nsec1 = 4; nsec2 = 2; }
+    else if (ka < 1.0) { ngpo1 = 4; nsub = 5; nsec1 = 6; nsec2 = 2; }
+    else if (ka < 2.0) { ngpo1 = 5; nsub = 6; nsec1 = 8; nsec2 = 3; }
+    else { ngpo1 = 6; nsub = 7; nsec1 = 10; nsec2 = 4; }
+    const int ego = ngpo1 * (ngpo1 - 1) / 2, sgo = nsub * (nsub - 1) / 2;
+    const int n_edge = nsec1 * ngpo1, n_bulk = nsec2 * nsub * nsub;
+    const int per_edge = n_edge + n_bulk;
+    Acc a;
+    double edge_r = 0.0, edge_i = 0.0;
+    for (int f = lane; f < 4 * per_edge; f += 32) {
+        const int ieg = f / per_edge, rem = f % per_edge;
+        const int ig1 = (ieg + 1) % 4, ig2 = ieg + 4;
+        if (rem < n_edge) {
+            const int isec = rem / ngpo1, ig = rem % ngpo1;
+            double dp[3], leneg = 0.0;
+            for (int c = 0; c < 3; ++c) {
+                dp[c] = V[ig1][c] - V[ieg][c];
+                leneg += dp[c] * dp[c];
+            }
+            leneg = sqrt(leneg);
+            const double to0 = dp[0] / leneg, to1 = dp[1] / leneg, to2 = dp[2] / leneg;
+            const double leneg_scaled = leneg / (2.0 * nsec1);
+            const double delsec = 2.0 / nsec1;
+            double secmid = -1.0 - delsec / 2.0;
+            for (int sct = 0; sct <= isec; ++sct) secmid += delsec;
+            const double sga = secmid + c_gl_x[ego + ig] / nsec1;
+            const double wga = c_gl_w[ego + ig] * leneg_scaled;
+            const double dx = V[ieg][0] + dp[0] * (sga + 1.0) / 2.0 - x0;
+            const double dy = V[ieg][1] + dp[1] * (sga + 1.0) / 2.0 - x1;
+            const double dz = V[ieg][2] + dp[2] * (sga + 1.0) / 2.0 - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            double sn, cs;
+            sb_sincos(k * dis, &sn, &cs);
+            const double g_r = cs * kInv4Pi * rinv, g_i = sn * kInv4Pi * rinv;
+            const double f_r = -g_r * rinv - g_i * k, f_i = g_r * k - g_i * rinv;
+            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+            const double cr = (uy * to2 - uz * to1) * nxx + (uz * to0 - ux * to2) * nxy + (ux * to1 - uy * to0) * nxz;
+            edge_r += f_r * cr * wga;
+            edge_i += f_i * cr * wga;
+        } else {
+            const int r2 = rem - n_edge;
+            const int isec = r2 / (nsub * nsub), ab = r2 % (nsub * nsub);
+            const int ia = ab / nsub, ib = ab % nsub;
+            const double aresub = 0.25 / nsec2;
+            double ss[3] = {0.0, 0.0, 0.0}, ts[3] = {0.0, 0.0, 0.0};
+            if (isec == 0) {
+                ss[1] = c_csi8[ieg]; ss[2] = c_csi8[ig2]; ts[1] = c_eta8[ieg]; ts[2] = c_eta8[ig2];
+            } else {
+                ss[1] = c_csi8[ig2]; ss[2] = c_csi8[ig1]; ts[1] = c_eta8[ig2]; ts[2] = c_eta8[ig1];
+            }
+            const double sga = c_gl_x[sgo + ia], tga = c_gl_x[sgo + ib];
+            const double wei = c_gl_w[sgo + ia] * c_gl_w[sgo + ib];
+            const double sgg = 0.5 * (1.0 - sga) * ss[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ss[1] + (1.0 + tga) * ss[2]);
+            const double tgg = 0.5 * (1.0 - sga) * ts[0] + 0.25 * (1.0 + sga) * ((1.0 - tga) * ts[1] + (1.0 + tga) * ts[2]);
+            double pos[3], jac, ny[3];
+            quad_params(V, sgg, tgg, pos, jac, ny);
+            const double dx = pos[0] - x0, dy = pos[1] - x1, dz = pos[2] - x2;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(dis >= 1e-15)) continue;
+            const double rinv = 1.0 / dis;
+            const double wga = wei * (1.0 + sga) * aresub * jac;
+            double sn, cs;
+            sb_sincos(k * dis, &sn, &cs);
+            const double gs = wga * kInv4Pi * rinv;
+            const double g_r = cs * gs, g_i = sn * gs;
+            const double ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;
+            const double rny = ux * ny[0] + uy * ny[1] + uz * ny[2];
+            const double rnx = -(ux * nxx + uy * nxy + uz * nxz);
+            const double b_r = -g_r * rinv - g_i * k, b_i = g_r * k - g_i * rinv;
+            a.gr += g_r; a.gi += g_i;
+            a.hr += b_r * rny; a.hi += b_i * rny;
+            a.tr += b_r * rnx; a.ti += b_i * rnx;
+            const double nd = nxx * ny[0] + nxy * ny[1] + nxz * ny[2];
+            a.er += g_r * k2 * nd;
+            a.ei += g_i * k2 * nd;
+        }
+    }
+    a.er += edge_r;
+    a.ei += edge_i;
+    const Acc t = warp_reduce(a);
+    if (lane == 0) self_store(t, coef, ld, n, i, A, nullptr, 0, nullptr, diag);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Persistent batched assembly: every instance of a frequency sweep in one launch. The work list
 // is [far tiles of all instances | near pairs (4 per item) | self elements (4 per item)]; each CTA
@@ -1829,6 +2327,150 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
     return m;
 }
 
+// A Quad4 mesh (constant panels): geometry and far points on the device, the same near-pair
+// classifier as triangle meshes (it needs only the centres, level-0 centres and areas).
+Mesh* mesh_create_quad(const double* nodes, int64_t n_nodes, const uint32_t* quads, int64_t n_quads, int device) {
+    SB_REQUIRE(nodes && quads, SB_ERR_INVALID_ARGUMENT, "mesh: null nodes or connectivity");
+    SB_REQUIRE(n_nodes >= 4 && n_quads >= 1, SB_ERR_INVALID_ARGUMENT, "mesh: empty mesh");
+    SB_REQUIRE(n_quads < (int64_t(1) << 31), SB_ERR_INVALID_ARGUMENT, "mesh: too many elements");
+    for (int64_t a = 0; a < 3 * n_nodes; ++a)
+        SB_REQUIRE(std::isfinite(nodes[a]), SB_ERR_INVALID_ARGUMENT, "mesh: non-finite node coordinate");
+    for (int64_t a = 0; a < 4 * n_quads; ++a)
+        SB_REQUIRE(quads[a] < static_cast<uint64_t>(n_nodes), SB_ERR_INVALID_ARGUMENT,
+                   "mesh: connectivity index out of range");
+    int ndev = 0;
+    SB_CUDA(cudaGetDeviceCount(&ndev));
+    SB_REQUIRE(device >= 0 && device < ndev, SB_ERR_CUDA, "mesh: CUDA device not available");
+    SB_CUDA(cudaSetDevice(device));
+    ensure_tables(device);
+    maybe_inject(SB_INJECT_ALLOC);
+    Mesh* m = new Mesh();
+    try {
+        m->device = device;
+        m->quad = true;
+        m->n = n_quads;
+        m->n_nodes = n_nodes;
+        m->n_tiles = cdiv(n_quads, kFarTile);
+        m->ld = m->n_tiles * kFarTile;
+        m->h_nodes.assign(nodes, nodes + 3 * n_nodes);
+        m->h_tris.assign(quads, quads + 4 * n_quads);
+        m->nodes.alloc(sizeof(double) * 3 * n_nodes);
+        m->tris.alloc(sizeof(uint32_t) * 4 * n_quads);
+        m->elem.alloc(sizeof(double) * EFIELDS * m->ld);
+        m->qq.alloc(sizeof(double) * kQuadFar * 7 * m->ld);
+        SB_CUDA(cudaMemcpy(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes, cudaMemcpyHostToDevice));
+        SB_CUDA(cudaMemcpy(m->tris.p, quads, sizeof(uint32_t) * 4 * n_quads, cudaMemcpyHostToDevice));
+        const int64_t nb = cdiv(m->ld, 256);
+        k_quad_geometry<<<nb, 256>>>(m->nodes.as<double>(), m->tris.as<uint32_t>(), m->n, m->ld, m->elem.as<double>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        k_quad_points<<<nb, 256>>>(m->elem.as<double>(), m->n, m->ld, m->qq.as<double>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        m->h_elem.resize(static_cast<size_t>(EFIELDS) * m->ld);
+        SB_CUDA(cudaMemcpy(m->h_elem.data(), m->elem.p, sizeof(double) * m->h_elem.size(), cudaMemcpyDeviceToHost));
+        for (int64_t e = 0; e < m->n; ++e) {
+            const double ar = m->h_elem[static_cast<size_t>(EAREA) * m->ld + e];
+            SB_REQUIRE(ar > 1e-300 && std::isfinite(ar), SB_ERR_UNSUPPORTED_ELEMENT,
+                       "mesh: degenerate quadrilateral " + std::to_string(e));
+        }
+        DevBuf counts;
+        counts.alloc(sizeof(int64_t) * (m->n + 1));
+        const int64_t nblk = cdiv(m->n, kNearRows);
+        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 0, counts.as<int64_t>(), nullptr, nullptr);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        std::vector<int64_t> cnt(m->n), ptr(m->n + 1);
+        SB_CUDA(cudaMemcpy(cnt.data(), counts.p, sizeof(int64_t) * m->n, cudaMemcpyDeviceToHost));
+        ptr[0] = 0;
+        for (int64_t i = 0; i < m->n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
+        m->nnz = ptr[m->n];
+        m->near_ptr.alloc(sizeof(int64_t) * (m->n + 1));
+        SB_CUDA(cudaMemcpy(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1), cudaMemcpyHostToDevice));
+        m->near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m->nnz, 1));
+        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 1, nullptr, m->near_ptr.as<int64_t>(),
+                                   m->near_col.as<int32_t>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        SB_CUDA(cudaDeviceSynchronize());
+        m->h_bc_kind.assign(m->n, SB_BC_VELOCITY);
+        m->h_bc_value.assign(2 * m->n, 0.0);
+        m->h_adm.assign(2 * m->n, 0.0);
+        m->h_has_adm.assign(m->n, 0);
+    } catch (...) {
+        delete m;
+        throw;
+    }
+    return m;
+}
+
+// The constant-panel system of a Quad4 mesh (complex128): coefficients, far pairs, near pairs,
+// self terms (rigid, zero-pressure or admittance surfaces).
+void assemble_quad(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
+    Mesh& m = *op.mesh;
+    SB_CUDA(cudaSetDevice(m.device));
+    SB_REQUIRE(!m.any_bc_value, SB_ERR_INVALID_ARGUMENT,
+               "Quad4 mesh: prescribed boundary values are not supported (rigid, zero-pressure or admittance "
+               "surfaces)");
+    SB_REQUIRE(op.A64.p && !op.A32.p, SB_ERR_INVALID_ARGUMENT, "Quad4 mesh: only SB_PRECISION_FP64 is supported");
+    maybe_inject(SB_INJECT_LAUNCH);
+    const int64_t n = m.n, ld = m.ld;
+    const cudaStream_t s = op.stream;
+    if (!op.coef.p) op.coef.alloc(sizeof(double) * CF_FIELDS * ld);
+    if (!op.diag.p) op.diag.alloc(sizeof(double2) * n);
+    if (!op.rhs.p) {
+        op.rhs.alloc(sizeof(double2) * n);
+        SB_CUDA(cudaMemsetAsync(op.rhs.p, 0, sizeof(double2) * n, s));
+    }
+    cudaEvent_t e0, e1;
+    SB_CUDA(cudaEventCreate(&e0));
+    SB_CUDA(cudaEventCreate(&e1));
+    SB_CUDA(cudaEventRecord(e0, s));
+    k_coefficients<<<cdiv(ld, 256), 256, 0, s>>>(n, ld, m.bc_kind.as<int32_t>(), m.bc_value.as<double2>(),
+                                                 m.has_adm.as<uint8_t>(), m.adm.as<double2>(), ph.tau,
+                                                 ph.pressure_factor, make_double2(beta_re, beta_im),
+                                                 op.coef.as<double>());
+    count_launch();
+    const double k = ph.harmonic_factor * ph.wave_number;
+    double2* A = op.A64.as<double2>();
+    {
+        ProfScope prof(SB_PROF_FAR, s);
+        const size_t sm = sizeof(double) * (kQuadFar * 7 * kQuadTile + kQuadRows * 6);
+        SB_CUDA(cudaFuncSetAttribute(k_quad_far, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+        dim3 grid(static_cast<unsigned>(cdiv(n, kQuadTile)), static_cast<unsigned>(cdiv(n, kQuadRows)));
+        k_quad_far<<<grid, kQuadTile, sm, s>>>(m.qq.as<double>(), m.elem.as<double>(), n, ld, op.coef.as<double>(), k,
+                                               A);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    if (m.nnz > 0) {
+        ProfScope prof(SB_PROF_NEAR, s);
+        k_quad_near<<<cdiv(m.nnz, kNearWarps), 32 * kNearWarps, 0, s>>>(m.elem.as<double>(), n, ld,
+                                                                       m.near_ptr.as<int64_t>(),
+                                                                       m.near_col.as<int32_t>(), m.nnz,
+                                                                       op.coef.as<double>(), k, A);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    {
+        ProfScope prof(SB_PROF_SELF, s);
+        k_quad_self<<<cdiv(n, 4), 128, 0, s>>>(m.elem.as<double>(), n, ld, op.coef.as<double>(), k, A,
+                                               op.diag.as<double2>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    SB_CUDA(cudaEventRecord(e1, s));
+    SB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    op.last_assembly_ms = ms;
+    op.phys = ph;
+    op.beta_re = beta_re;
+    op.beta_im = beta_im;
+}
+
 void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const uint8_t* has_adm,
                  const sb_complex* adm) {
     for (int64_t e = 0; e < m.n; ++e) {
@@ -1867,6 +2509,10 @@ void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const ui
 }
 
 void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
+    if (op.mesh->quad) {
+        assemble_quad(op, ph, beta_re, beta_im);
+        return;
+    }
     Mesh& m = *op.mesh;
     SB_CUDA(cudaSetDevice(m.device));
     maybe_inject(SB_INJECT_LAUNCH);

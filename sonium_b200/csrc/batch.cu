@@ -1025,6 +1025,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
             B->ninst = static_cast<int>(count);
             for (int64_t i = 0; i < count; ++i) {
                 SB_REQUIRE(meshes[i] && meshes[i]->m, SB_ERR_INVALID_ARGUMENT, "batch: null mesh");
+                SB_REQUIRE(!meshes[i]->m->quad, SB_ERR_UNSUPPORTED_ELEMENT, "batch: Tri3 meshes only");
                 SB_REQUIRE(sb_physics_validate(&physics[i]) == SB_OK, SB_ERR_INVALID_ARGUMENT,
                            "batch: invalid physics parameters");
                 SB_REQUIRE(std::isfinite(betas[i].re) && std::isfinite(betas[i].im), SB_ERR_INVALID_ARGUMENT,

@@ -255,6 +255,16 @@ SB_API int sb_mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* 
     });
 }
 
+SB_API int sb_mesh_create_quad4(const double* nodes, int64_t n_nodes, const uint32_t* quads, int64_t n_quads,
+                                int device, sb_mesh** out) {
+    return guarded([&] {
+        SB_REQUIRE(out, SB_ERR_INVALID_ARGUMENT, "null output handle");
+        *out = nullptr;
+        Mesh* m = mesh_create_quad(nodes, n_nodes, quads, n_quads, device);
+        *out = new sb_mesh{m};
+    });
+}
+
 SB_API int sb_mesh_destroy(sb_mesh* mesh) {
     return guarded([&] {
         if (!mesh) return;
@@ -314,6 +324,8 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
         Mesh& m = *mesh->m;
+        SB_REQUIRE(!m.quad || precision == SB_PRECISION_FP64, SB_ERR_INVALID_ARGUMENT,
+                   "Quad4 mesh: only SB_PRECISION_FP64 is supported");
         if (!m.bc_kind.p) mesh_set_bc(m, nullptr, nullptr, nullptr, nullptr);
         SB_CUDA(cudaSetDevice(m.device));
         Operator* op = new Operator();
@@ -404,6 +416,7 @@ static void create_discontinuous(const sb_mesh* mesh, const sb_physics* physics,
                                  double sign, sb_operator** out) {
         SB_REQUIRE(mesh && mesh->m && physics && out, SB_ERR_INVALID_ARGUMENT, "null argument");
         *out = nullptr;
+        SB_REQUIRE(!mesh->m->quad, SB_ERR_UNSUPPORTED_ELEMENT, "discontinuous bases: Tri3 meshes only");
         SB_REQUIRE(basis == SB_BASIS_LINEAR || basis == SB_BASIS_QUADRATIC, SB_ERR_INVALID_ARGUMENT,
                    "discontinuous basis must be SB_BASIS_LINEAR or SB_BASIS_QUADRATIC");
         SB_REQUIRE(sign == 1.0 || sign == -1.0, SB_ERR_INVALID_ARGUMENT, "sign must be +1 or -1");
@@ -450,6 +463,8 @@ SB_API int sb_mesh_collocation(const sb_mesh* mesh, int basis, double* points, d
         SB_REQUIRE(basis == SB_BASIS_CONSTANT || basis == SB_BASIS_LINEAR || basis == SB_BASIS_QUADRATIC,
                    SB_ERR_INVALID_ARGUMENT, "unknown basis");
         const Mesh& m = *mesh->m;
+        SB_REQUIRE(basis == SB_BASIS_CONSTANT || !m.quad, SB_ERR_UNSUPPORTED_ELEMENT,
+                   "discontinuous bases: Tri3 meshes only");
         if (basis == SB_BASIS_CONSTANT) {
             for (int64_t e = 0; e < m.n; ++e)
                 for (int c = 0; c < 3; ++c) {
@@ -795,6 +810,7 @@ SB_API int sb_field_eval(const sb_mesh* mesh, const sb_physics* physics, const s
         SB_REQUIRE(m == 0 || (points && field), SB_ERR_INVALID_ARGUMENT, "null points or output");
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         const Mesh& me = *mesh->m;
+        SB_REQUIRE(!me.quad, SB_ERR_UNSUPPORTED_ELEMENT, "field_eval: Tri3 meshes only");
         SB_REQUIRE(all_finite(surface_pressure, me.n), SB_ERR_NOT_FINITE, "field_eval: non-finite surface pressure");
         if (surface_velocity)
             SB_REQUIRE(all_finite(surface_velocity, me.n), SB_ERR_NOT_FINITE,

@@ -86,6 +86,7 @@ enum ElemField {
     EAREA, EJAC,                                            // area, |dx/ds x dx/dt|
     EGX, EGY, EGZ,                                          // level-0 subdivision centre
     ESQA,                                                   // sqrt(area)
+    EV3X, EV3Y, EV3Z,                                       // fourth vertex (Quad4 meshes)
     EFIELDS
 };
 
@@ -101,6 +102,10 @@ struct Mesh {
     // near-pair CSR (superset of the reference's subdivision criterion; excludes the diagonal)
     int64_t nnz = 0;
     DevBuf near_ptr, near_col;
+    // Quad4 meshes: four vertices per element (EV0..EV3), far points of the 4 x 4 rule with their
+    // normals, qq[(q * 7 + f) * ld + e] for f = x, y, z, w J, nx, ny, nz.
+    bool quad = false;
+    DevBuf qq;
     // boundary conditions
     std::vector<int32_t> h_bc_kind;
     std::vector<double> h_bc_value, h_adm;  // interleaved complex
@@ -190,6 +195,8 @@ void device_sincos(int device, const double* x, int64_t n, double* s, double* c)
 // Mesh (assembly.cu)
 Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, int64_t n_tris,
                   int device);
+Mesh* mesh_create_quad(const double* nodes, int64_t n_nodes, const uint32_t* quads, int64_t n_quads, int device);
+void assemble_quad(Operator& op, const sb_physics& ph, double beta_re, double beta_im);
 void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const uint8_t* has_adm,
                  const sb_complex* adm);
 void host_element_geometry(const double* nodes, const uint32_t* tris, int64_t n, double* c,

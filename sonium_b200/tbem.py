@@ -95,6 +95,21 @@ class Mesh:
         self.device = device
 
     @classmethod
+    def quad4(cls, nodes, quads, device: int = 0) -> "Mesh":
+        """A Quad4 mesh of constant panels (quads: (m, 4) vertex indices)."""
+        self = cls.__new__(cls)
+        self.nodes = np.ascontiguousarray(nodes, np.float64)
+        self.tris = np.ascontiguousarray(quads, np.uint32)
+        if self.nodes.ndim != 2 or self.nodes.shape[1] != 3 or self.tris.ndim != 2 or self.tris.shape[1] != 4:
+            raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "nodes must be (n, 3) and quads (m, 4)")
+        h = ct.c_void_p()
+        check(L.load().sb_mesh_create_quad4(_p(self.nodes), self.nodes.shape[0], _p(self.tris), self.tris.shape[0],
+                                            device, ct.byref(h)))
+        self._h = h
+        self.device = device
+        return self
+
+    @classmethod
     def icosphere(cls, radius: float, level: int, scale=None, device: int = 0) -> "Mesh":
         nodes, tris = icosphere(radius, level, scale)
         return cls(nodes, tris, device)
