@@ -423,6 +423,16 @@ SB_API int sb_batch_assembly_tuning(const sb_batch* batch, int* chosen, double* 
 /* Device time of the last sb_batch_assemble and sb_batch_solve, milliseconds. */
 SB_API int sb_batch_timings(const sb_batch* batch, double* assembly_ms, double* solve_ms);
 
+/* ---- device memory (no reference counterpart: the allocator of this implementation) ----
+ * Device buffers of meshes, operators, solvers and batches come from a per-device cache of
+ * released blocks of the same size (rounded to 2 MiB, or 512 B below 1 MiB) before cudaMalloc is
+ * asked; a released block enters the cache after a device synchronisation (as cudaFree waits)
+ * while the cache holds at most 96 GiB per device, and an allocation that fails empties the
+ * cache and retries. trim returns every cached block of a device (device < 0: all devices) to
+ * the driver; stats reports the bytes held by live buffers and by the cache. */
+SB_API int sb_memory_trim(int device);
+SB_API int sb_memory_stats(int device, int64_t* in_use_bytes, int64_t* cached_bytes);
+
 /* ---- timing (no reference counterpart: instrumentation, the PerfModel / runtime-stats role of
  * crates/sonium-compute/src/perf.rs:1-30) ---- */
 /* Kernel classes timed by CUDA events recorded on their launching stream when profiling is on. */

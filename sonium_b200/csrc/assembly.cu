@@ -141,6 +141,7 @@ void ensure_tables(int device) {
     SB_CUDA(cudaMemcpyToSymbol(c_tri_w, tw, sizeof(tw)));
     SB_CUDA(cudaMemcpyToSymbol(c_tri_off, off, sizeof(off)));
     SB_CUDA(cudaMemcpyToSymbol(c_tri_cnt, cnt, sizeof(cnt)));
+    SB_CUDA(cudaDeviceSynchronize());  // tables in place before kernels on any stream read them
     done[device] = true;
 }
 
@@ -2288,8 +2289,8 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
         m->elem.alloc(sizeof(double) * EFIELDS * m->ld);
         m->qp.alloc(sizeof(double) * kQpTileDoubles * m->n_tiles);
         m->qp32.alloc(sizeof(float) * kFarPoints * kQ32 * m->ld);
-        SB_CUDA(cudaMemcpy(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes, cudaMemcpyHostToDevice));
-        SB_CUDA(cudaMemcpy(m->tris.p, tris, sizeof(uint32_t) * 3 * n_tris, cudaMemcpyHostToDevice));
+        h2d_sync(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes);
+        h2d_sync(m->tris.p, tris, sizeof(uint32_t) * 3 * n_tris);
         const int64_t nb = cdiv(m->ld, 256);
         k_element_geometry<<<nb, 256>>>(m->nodes.as<double>(), m->tris.as<uint32_t>(), m->n, m->ld, m->elem.as<double>()); count_launch();
         SB_CUDA(cudaGetLastError());
@@ -2309,7 +2310,7 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
         for (int64_t i = 0; i < m->n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
         m->nnz = ptr[m->n];
         m->near_ptr.alloc(sizeof(int64_t) * (m->n + 1));
-        SB_CUDA(cudaMemcpy(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1), cudaMemcpyHostToDevice));
+        h2d_sync(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1));
         m->near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m->nnz, 1));
         k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 1, nullptr, m->near_ptr.as<int64_t>(), m->near_col.as<int32_t>()); count_launch();
         SB_CUDA(cudaGetLastError());
@@ -2358,8 +2359,8 @@ Mesh* mesh_create_quad(const double* nodes, int64_t n_nodes, const uint32_t* qua
         m->tris.alloc(sizeof(uint32_t) * 4 * n_quads);
         m->elem.alloc(sizeof(double) * EFIELDS * m->ld);
         m->qq.alloc(sizeof(double) * kQuadFar * 7 * m->ld);
-        SB_CUDA(cudaMemcpy(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes, cudaMemcpyHostToDevice));
-        SB_CUDA(cudaMemcpy(m->tris.p, quads, sizeof(uint32_t) * 4 * n_quads, cudaMemcpyHostToDevice));
+        h2d_sync(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes);
+        h2d_sync(m->tris.p, quads, sizeof(uint32_t) * 4 * n_quads);
         const int64_t nb = cdiv(m->ld, 256);
         k_quad_geometry<<<nb, 256>>>(m->nodes.as<double>(), m->tris.as<uint32_t>(), m->n, m->ld, m->elem.as<double>());
         count_launch();
@@ -2386,7 +2387,7 @@ Mesh* mesh_create_quad(const double* nodes, int64_t n_nodes, const uint32_t* qua
         for (int64_t i = 0; i < m->n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
         m->nnz = ptr[m->n];
         m->near_ptr.alloc(sizeof(int64_t) * (m->n + 1));
-        SB_CUDA(cudaMemcpy(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1), cudaMemcpyHostToDevice));
+        h2d_sync(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1));
         m->near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m->nnz, 1));
         k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 1, nullptr, m->near_ptr.as<int64_t>(),
                                    m->near_col.as<int32_t>());
@@ -2502,10 +2503,10 @@ void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const ui
         m.has_adm.alloc(m.n);
         m.adm.alloc(sizeof(double2) * m.n);
     }
-    SB_CUDA(cudaMemcpy(m.bc_kind.p, m.h_bc_kind.data(), sizeof(int32_t) * m.n, cudaMemcpyHostToDevice));
-    SB_CUDA(cudaMemcpy(m.bc_value.p, m.h_bc_value.data(), sizeof(double2) * m.n, cudaMemcpyHostToDevice));
-    SB_CUDA(cudaMemcpy(m.has_adm.p, m.h_has_adm.data(), m.n, cudaMemcpyHostToDevice));
-    SB_CUDA(cudaMemcpy(m.adm.p, m.h_adm.data(), sizeof(double2) * m.n, cudaMemcpyHostToDevice));
+    h2d_sync(m.bc_kind.p, m.h_bc_kind.data(), sizeof(int32_t) * m.n);
+    h2d_sync(m.bc_value.p, m.h_bc_value.data(), sizeof(double2) * m.n);
+    h2d_sync(m.has_adm.p, m.h_has_adm.data(), m.n);
+    h2d_sync(m.adm.p, m.h_adm.data(), sizeof(double2) * m.n);
 }
 
 void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
@@ -2876,7 +2877,7 @@ void device_sincos(int device, const double* x, int64_t n, double* s, double* c)
     dx.alloc(sizeof(double) * n);
     ds.alloc(sizeof(double) * n);
     dc.alloc(sizeof(double) * n);
-    SB_CUDA(cudaMemcpy(dx.p, x, sizeof(double) * n, cudaMemcpyHostToDevice));
+    h2d_sync(dx.p, x, sizeof(double) * n);
     k_sincos<<<cdiv(n, 256), 256>>>(dx.as<double>(), n, ds.as<double>(), dc.as<double>()); count_launch();
     SB_CUDA(cudaGetLastError());
     SB_CUDA(cudaMemcpy(s, ds.p, sizeof(double) * n, cudaMemcpyDeviceToHost));

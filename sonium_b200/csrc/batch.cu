@@ -543,7 +543,7 @@ static void batch_workspace(Batch& B, int64_t m) {
     B.pool_small.alloc(small);
     B.pool_state.alloc(state_bytes(ni));
     B.pin.alloc(state_bytes(ni));
-    SB_CUDA(cudaMemset(B.pool_state.p, 0, state_bytes(ni)));
+    memset_sync(B.pool_state.p, 0, state_bytes(ni));
     std::memset(B.pin.p, 0, state_bytes(ni));
     const StateView dv = state_view(B.pool_state.p, ni);
     char* pf32 = B.pool_f32.as<char>();
@@ -559,8 +559,8 @@ static void batch_workspace(Batch& B, int64_t m) {
         // Right-hand-side-major families, each one block: vector c of a family at base + c * ld_all,
         // basis vector i of right-hand side c at v_all + (i * ninst + c) * ld_all. Zero-filled so the
         // block products never read stale values.
-        SB_CUDA(cudaMemset(B.pool_f32.p, 0, f32));
-        SB_CUDA(cudaMemset(B.pool_f64.p, 0, f64));
+        memset_sync(B.pool_f32.p, 0, f32);
+        memset_sync(B.pool_f64.p, 0, f64);
         const int64_t ld = B.ld_all;
         B.v_all = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * (m + 1) * ni * ld));
         B.w_all = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ni * ld));
@@ -626,10 +626,10 @@ static void batch_workspace(Batch& B, int64_t m) {
     B.pre4_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre256_d.alloc(sizeof(int64_t) * (ni + 1));
     B.predot_d.alloc(sizeof(int64_t) * (ni + 1));
-    SB_CUDA(cudaMemcpy(B.predot_d.p, B.predot.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
-    SB_CUDA(cudaMemcpy(B.inst_d.p, B.h.data(), sizeof(BInst) * ni, cudaMemcpyHostToDevice));
-    SB_CUDA(cudaMemcpy(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
-    SB_CUDA(cudaMemcpy(B.pre256_d.p, B.pre256.data(), sizeof(int64_t) * (ni + 1), cudaMemcpyHostToDevice));
+    h2d_sync(B.predot_d.p, B.predot.data(), sizeof(int64_t) * (ni + 1));
+    h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
+    h2d_sync(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1));
+    h2d_sync(B.pre256_d.p, B.pre256.data(), sizeof(int64_t) * (ni + 1));
     B.m = m;
 }
 
@@ -945,7 +945,7 @@ static Batch& multi_batch(Operator& op, int r) {
     SB_REQUIRE(cublasSetStream(B->blas, B->stream) == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasSetStream failed");
     B->gate.alloc(sizeof(int) * cdiv64(r, kTensorRhsTile));
     B->pool_rhs.alloc(sizeof(double2) * r * B->ld_all);
-    SB_CUDA(cudaMemset(B->pool_rhs.p, 0, sizeof(double2) * r * B->ld_all));
+    memset_sync(B->pool_rhs.p, 0, sizeof(double2) * r * B->ld_all);
     B->b_all = B->pool_rhs.as<double2>();
     for (int c = 0; c < r; ++c) B->rhs.push_back(B->b_all + (int64_t)c * B->ld_all);
     B->assembled = true;
@@ -1058,7 +1058,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
             }
             B->pool_mat.alloc(mat + cof + dg);
             B->pool_rhs.alloc(rhs);
-            SB_CUDA(cudaMemset(B->pool_rhs.p, 0, rhs));
+            memset_sync(B->pool_rhs.p, 0, rhs);
             char* pm = B->pool_mat.as<char>();
             char* pc = pm + mat;
             char* pd = pc + cof;
@@ -1088,7 +1088,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
             }
             B->asm_d.alloc(sizeof(BatchAsmInst) * B->ninst);
             SB_CUDA(cudaMemcpy(B->asm_d.p, B->asm_h.data(), sizeof(BatchAsmInst) * B->ninst,
-                               cudaMemcpyHostToDevice));
+                               cudaMemcpyHostToDevice)); SB_CUDA(cudaStreamSynchronize(0));
         } catch (...) {
             delete B;
             throw;
@@ -1225,7 +1225,7 @@ SB_API int sb_batch_set_rhs(sb_batch* batch, int64_t index, const sb_complex* b)
                        "batch: non-finite right-hand side");
         SB_CUDA(cudaSetDevice(B.device));
         SB_CUDA(cudaStreamSynchronize(B.stream));
-        SB_CUDA(cudaMemcpy(B.rhs[index], b, sizeof(double2) * n, cudaMemcpyHostToDevice));
+        h2d_sync(B.rhs[index], b, sizeof(double2) * n);
     });
 }
 

@@ -2,7 +2,9 @@
 // failures and turns them into a status code plus a thread-local message; nothing falls back
 // to a CPU computation.
 
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "sb_blas.cuh"
@@ -37,25 +39,120 @@ void maybe_inject(int point) {
     }
 }
 
+// ---- caching device allocator ----
+namespace {
+std::mutex g_mem_mu;
+// Free blocks per (device, rounded size).
+std::map<std::pair<int, size_t>, std::vector<void*>> g_free;
+std::map<int, int64_t> g_in_use, g_cached;
+constexpr size_t kCacheLimit = size_t(96) << 30;  // per device; larger releases go back to the driver
+
+// SB_DEVICE_CACHE=0 in the environment turns the cache off (every release is a cudaFree).
+bool cache_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("SB_DEVICE_CACHE");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
+size_t round_block(size_t n) {
+    const size_t g = n >= (size_t(1) << 20) ? (size_t(2) << 20) : 512;
+    return (n + g - 1) / g * g;
+}
+
+void trim_locked(int device) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto it = g_free.begin(); it != g_free.end();) {
+        if (device >= 0 && it->first.first != device) {
+            ++it;
+            continue;
+        }
+        cudaSetDevice(it->first.first);
+        for (void* q : it->second) cudaFree(q);
+        g_cached[it->first.first] -= static_cast<int64_t>(it->first.second * it->second.size());
+        it = g_free.erase(it);
+    }
+    cudaSetDevice(cur);
+}
+}  // namespace
+
+void h2d_sync(void* dst, const void* src, size_t bytes) {
+    SB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    SB_CUDA(cudaStreamSynchronize(0));
+}
+
+void memset_sync(void* dst, int value, size_t bytes) {
+    SB_CUDA(cudaMemset(dst, value, bytes));
+    SB_CUDA(cudaStreamSynchronize(0));
+}
+
+void memory_trim(int device) {
+    std::lock_guard<std::mutex> lock(g_mem_mu);
+    trim_locked(device);
+}
+
+void memory_stats(int device, int64_t* in_use, int64_t* cached) {
+    std::lock_guard<std::mutex> lock(g_mem_mu);
+    if (in_use) *in_use = g_in_use[device];
+    if (cached) *cached = g_cached[device];
+}
+
 void DevBuf::alloc(size_t n) {
     release();
     if (n == 0) n = 16;
     maybe_inject(SB_INJECT_ALLOC);
-    cudaError_t e = cudaMalloc(&p, n);
-    if (e != cudaSuccess) {
-        p = nullptr;
-        cudaGetLastError();
-        throw Error{e == cudaErrorMemoryAllocation ? SB_ERR_OUT_OF_MEMORY : SB_ERR_CUDA,
-                    std::string("device allocation of ") + std::to_string(n) + " bytes failed: " +
-                        cudaGetErrorString(e)};
+    int device = 0;
+    SB_CUDA(cudaGetDevice(&device));
+    const size_t c = round_block(n);
+    std::lock_guard<std::mutex> lock(g_mem_mu);
+    auto it = g_free.find({device, c});
+    if (it != g_free.end() && !it->second.empty()) {
+        p = it->second.back();
+        it->second.pop_back();
+        g_cached[device] -= static_cast<int64_t>(c);
+    } else {
+        cudaError_t e = cudaMalloc(&p, c);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            trim_locked(-1);
+            e = cudaMalloc(&p, c);
+        }
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            throw Error{e == cudaErrorMemoryAllocation ? SB_ERR_OUT_OF_MEMORY : SB_ERR_CUDA,
+                        std::string("device allocation of ") + std::to_string(n) + " bytes failed: " +
+                            cudaGetErrorString(e)};
+        }
     }
     bytes = n;
+    cap = c;
+    dev = device;
+    g_in_use[device] += static_cast<int64_t>(c);
 }
 
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_mem_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    g_in_use[dev] -= static_cast<int64_t>(cap);
+    // Work still queued on any stream may use the block: wait for the device, as cudaFree does.
+    if (cache_enabled() && cudaDeviceSynchronize() == cudaSuccess &&
+        g_cached[dev] + static_cast<int64_t>(cap) <= static_cast<int64_t>(kCacheLimit)) {
+        g_free[{dev, cap}].push_back(p);
+        g_cached[dev] += static_cast<int64_t>(cap);
+    } else {
+        cudaGetLastError();
+        cudaFree(p);
+    }
+    if (cur != dev) cudaSetDevice(cur);
     p = nullptr;
-    bytes = 0;
+    bytes = cap = 0;
+    dev = -1;
 }
 
 int device_sm_count(int device) {
@@ -370,7 +467,7 @@ SB_API int sb_operator_from_dense(int device, int64_t n, const sb_complex* matri
             SB_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
             if (precision != SB_PRECISION_FP32) {
                 op->A64.alloc(sizeof(double2) * n * n);
-                SB_CUDA(cudaMemcpy(op->A64.p, matrix, sizeof(double2) * n * n, cudaMemcpyHostToDevice));
+                h2d_sync(op->A64.p, matrix, sizeof(double2) * n * n);
             }
             if (precision != SB_PRECISION_FP64) {
                 op->A32.alloc(sizeof(float2) * n * op->lda32);
@@ -380,15 +477,15 @@ SB_API int sb_operator_from_dense(int device, int64_t n, const sb_complex* matri
                         row[j] = make_float2(static_cast<float>(matrix[i * n + j].re),
                                              static_cast<float>(matrix[i * n + j].im));
                     SB_CUDA(cudaMemcpy(op->A32.as<float2>() + i * op->lda32, row.data(), sizeof(float2) * op->lda32,
-                                       cudaMemcpyHostToDevice));
+                                       cudaMemcpyHostToDevice)); SB_CUDA(cudaStreamSynchronize(0));
                 }
             }
             std::vector<sb_complex> d(n);
             for (int64_t i = 0; i < n; ++i) d[i] = matrix[i * n + i];
             op->diag.alloc(sizeof(double2) * n);
-            SB_CUDA(cudaMemcpy(op->diag.p, d.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+            h2d_sync(op->diag.p, d.data(), sizeof(double2) * n);
             op->rhs.alloc(sizeof(double2) * n);
-            SB_CUDA(cudaMemset(op->rhs.p, 0, sizeof(double2) * n));
+            memset_sync(op->rhs.p, 0, sizeof(double2) * n);
         } catch (...) {
             if (op->stream) cudaStreamDestroy(op->stream);
             delete op;
@@ -517,7 +614,7 @@ SB_API int sb_rhs_plane_wave_points(int device, int64_t np, const double* points
         DevBuf dp, dr;
         dp.alloc(sizeof(double) * 6 * np);
         dr.alloc(sizeof(double2) * np * r);
-        SB_CUDA(cudaMemcpy(dp.p, soa.data(), sizeof(double) * 6 * np, cudaMemcpyHostToDevice));
+        h2d_sync(dp.p, soa.data(), sizeof(double) * 6 * np);
         incident_plane_wave_at(device, dp.as<double>(), dp.as<double>() + 3 * np, np, np, *physics, beta.re, beta.im,
                                dirs, reinterpret_cast<const double*>(amps), r, dr.as<double2>(), 0);
         SB_CUDA(cudaMemcpy(rhs, dr.p, sizeof(double2) * np * r, cudaMemcpyDeviceToHost));
@@ -743,7 +840,7 @@ SB_API int sb_gmres_multi(const sb_operator* op, const sb_complex* b, int64_t r,
         DevBuf db, dx;
         db.alloc(sizeof(double2) * n * r);
         dx.alloc(sizeof(double2) * n * r);
-        SB_CUDA(cudaMemcpy(db.p, t.data(), sizeof(double2) * n * r, cudaMemcpyHostToDevice));
+        h2d_sync(db.p, t.data(), sizeof(double2) * n * r);
         multi_solve_device(o, db.as<double2>(), n, static_cast<int>(r), dx.as<double2>(), n, *cfg, stats);
         SB_CUDA(cudaMemcpy(t.data(), dx.p, sizeof(double2) * n * r, cudaMemcpyDeviceToHost));
         for (int64_t i = 0; i < n; ++i)
@@ -822,14 +919,14 @@ SB_API int sb_field_eval(const sb_mesh* mesh, const sb_physics* physics, const s
         maybe_inject(SB_INJECT_LAUNCH);
         DevBuf dp, dv, dx, dout;
         dp.alloc(sizeof(double2) * me.n);
-        SB_CUDA(cudaMemcpy(dp.p, surface_pressure, sizeof(double2) * me.n, cudaMemcpyHostToDevice));
+        h2d_sync(dp.p, surface_pressure, sizeof(double2) * me.n);
         if (surface_velocity) {
             dv.alloc(sizeof(double2) * me.n);
-            SB_CUDA(cudaMemcpy(dv.p, surface_velocity, sizeof(double2) * me.n, cudaMemcpyHostToDevice));
+            h2d_sync(dv.p, surface_velocity, sizeof(double2) * me.n);
         }
         dx.alloc(sizeof(double) * 3 * m);
         dout.alloc(sizeof(double2) * m);
-        SB_CUDA(cudaMemcpy(dx.p, points, sizeof(double) * 3 * m, cudaMemcpyHostToDevice));
+        h2d_sync(dx.p, points, sizeof(double) * 3 * m);
         field_eval(me, *physics, dp.as<double2>(), surface_velocity ? dv.as<double2>() : nullptr, dx.as<double>(), m,
                    dout.as<double2>(), 0);
         SB_CUDA(cudaMemcpy(field, dout.p, sizeof(double2) * m, cudaMemcpyDeviceToHost));
@@ -1030,6 +1127,14 @@ SB_API int sb_gcro_dr(const sb_operator* op, const sb_complex* b, const sb_compl
         SB_CUDA(cudaMemcpyAsync(x, dx.p, sizeof(double2) * o.n, cudaMemcpyDeviceToHost, o.stream));
         SB_CUDA(cudaStreamSynchronize(o.stream));
     });
+}
+
+SB_API int sb_memory_trim(int device) {
+    return guarded([&] { memory_trim(device); });
+}
+
+SB_API int sb_memory_stats(int device, int64_t* in_use_bytes, int64_t* cached_bytes) {
+    return guarded([&] { memory_stats(device, in_use_bytes, cached_bytes); });
 }
 
 SB_API int sb_profile_enable(int on) {

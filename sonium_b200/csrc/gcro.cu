@@ -293,7 +293,12 @@ struct RecycleSpace {
     DevBuf V, C, w, opb, part, red, red2, redc, redc2, nrm, ydev, zdev, H, cs, sn, g, B, st;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // Everything the captured cycle bakes in besides the subspace's own buffers: the operator's
+    // matrices and Jacobi diagonal (a later operator may reuse the same addresses for other roles).
     const void* key_A = nullptr;
+    const void* key_A32 = nullptr;
+    const void* key_jac = nullptr;
+    int64_t key_lda = -1;
     int key_jacobi = -1, key_k = -1;
     unsigned key_prof = 0;
     std::vector<ProfPair> prof_pairs;
@@ -381,6 +386,7 @@ void recycle_set(RecycleSpace& s, int64_t count, int64_t n, const double2* host)
     s.ensure_vectors(n);
     SB_CUDA(cudaMemcpy2D(s.U.p, sizeof(double2) * s.ld, host, sizeof(double2) * n, sizeof(double2) * n, count,
                          cudaMemcpyHostToDevice));
+    SB_CUDA(cudaStreamSynchronize(0));  // the copy lands before kernels on the solver's stream read it
     s.count = count;
 }
 
@@ -436,9 +442,10 @@ void gcro_launch_cycle(const Operator& op, RecycleSpace& S, const double2* jac, 
 
 // Replays the captured cycle, capturing it first when the operator, k or profiling changed.
 void gcro_run_cycle(const Operator& op, RecycleSpace& S, const double2* jac, int k, int64_t m) {
-    const void* key_A = op.A64.p ? op.A64.p : op.A32.p;
+    const void* key_A = op.A64.p;
     const int kj = jac ? 1 : 0;
-    if (!S.exec || S.key_A != key_A || S.key_jacobi != kj || S.key_k != k || S.key_prof != prof_key()) {
+    if (!S.exec || S.key_A != key_A || S.key_A32 != op.A32.p || S.key_lda != op.lda32 || S.key_jac != jac ||
+        S.key_jacobi != kj || S.key_k != k || S.key_prof != prof_key()) {
         S.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&S.prof_pairs);
@@ -458,6 +465,9 @@ void gcro_run_cycle(const Operator& op, RecycleSpace& S, const double2* jac, int
         S.graph_kernels = kernel_count() - before;
         add_kernel_count(-S.graph_kernels);
         S.key_A = key_A;
+        S.key_A32 = op.A32.p;
+        S.key_lda = op.lda32;
+        S.key_jac = jac;
         S.key_jacobi = kj;
         S.key_k = k;
         S.key_prof = prof_key();
@@ -653,8 +663,7 @@ void update_subspace(Ctx& c, const std::vector<cd>& R, int64_t ldr, const std::v
         }
     }
     if (acc > 0) {
-        std::swap(S.U.p, S.Unew.p);
-        std::swap(S.U.bytes, S.Unew.bytes);
+        S.U.swap(S.Unew);
         S.count = acc;
     }
 }

@@ -72,6 +72,7 @@ struct KrylovWork {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     const void* key_A = nullptr;
+    const void* key_jac = nullptr;  // the Jacobi diagonal the cycle reads, if any
     int key_jacobi = -1;
     unsigned key_prof = 0;
     std::vector<ProfPair> prof_pairs;
@@ -135,7 +136,7 @@ struct SolveWork {
         nrmg.alloc(sizeof(double) * 2);
         one.alloc(sizeof(double2));
         const double2 h_one = make_double2(1.0, 0.0);
-        SB_CUDA(cudaMemcpy(one.p, &h_one, sizeof(double2), cudaMemcpyHostToDevice));
+        SB_CUDA(cudaMemcpy(one.p, &h_one, sizeof(double2), cudaMemcpyHostToDevice)); SB_CUDA(cudaStreamSynchronize(0));
         ax.alloc(sizeof(double2) * n);
     }
 };
@@ -234,7 +235,7 @@ void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
 template <class T>
 void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
     const int jac = P.jacobi ? 1 : 0;
-    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_prof != prof_key()) {
+    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_jac != P.jacobi || W.key_prof != prof_key()) {
         W.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&W.prof_pairs);
@@ -254,6 +255,7 @@ void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
         W.graph_kernels = kernel_count() - before;
         add_kernel_count(-W.graph_kernels);
         W.key_A = P.key_A;
+        W.key_jac = P.jacobi;
         W.key_jacobi = jac;
         W.key_prof = prof_key();
     }

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/sonium_b200.h"
@@ -45,21 +46,42 @@ void count_launch();
 extern int g_inject_point;
 void maybe_inject(int point);
 
-// Device memory with ownership; allocation failures surface as SB_ERR_OUT_OF_MEMORY.
+// Device memory with ownership; allocation failures surface as SB_ERR_OUT_OF_MEMORY. Blocks come
+// from a per-device cache of released blocks of the same rounded size when one is free (a
+// released block enters the cache after a device synchronisation, as cudaFree would wait), and
+// from cudaMalloc otherwise; an allocation that fails empties the cache and retries once.
 struct DevBuf {
     void* p = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0;  // requested size
+    size_t cap = 0;    // rounded size of the block
+    int dev = -1;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void alloc(size_t n);
     void release();
+    void swap(DevBuf& o) {
+        std::swap(p, o.p);
+        std::swap(bytes, o.bytes);
+        std::swap(cap, o.cap);
+        std::swap(dev, o.dev);
+    }
     template <class T>
     T* as() const {
         return static_cast<T*>(p);
     }
 };
+// Host-to-device copy / device memset on the legacy default stream that are complete on return.
+// The legacy stream does not order work on the library's non-blocking streams, and a copy from
+// pageable host memory may return before its DMA has landed, so every upload or fill that a
+// kernel on another stream reads goes through these.
+void h2d_sync(void* dst, const void* src, size_t bytes);
+void memset_sync(void* dst, int value, size_t bytes);
+// Frees every cached block of `device` (all devices when device < 0).
+void memory_trim(int device);
+// Bytes held by live DevBufs and by the cache on `device`.
+void memory_stats(int device, int64_t* in_use, int64_t* cached);
 
 // ---------------------------------------------------------------------------------------------
 // Quadrature tables in constant memory (uploaded once per device by ensure_tables()).

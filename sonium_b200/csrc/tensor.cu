@@ -337,8 +337,8 @@ void tensor_reserve(const Operator& op, int r) {
     const size_t bytes = sizeof(__nv_bfloat16) * (size_t)rblocks * 2 * kTileRhs * w->ldk;
     w->x_hi.alloc(bytes);
     w->x_lo.alloc(bytes);
-    SB_CUDA(cudaMemset(w->x_hi.p, 0, bytes));
-    SB_CUDA(cudaMemset(w->x_lo.p, 0, bytes));
+    memset_sync(w->x_hi.p, 0, bytes);
+    memset_sync(w->x_lo.p, 0, bytes);
     w->rblocks = rblocks;
     w->gen = ++g_tensor_gen;
     w->tm_x_hi = make_map(w->x_hi.p, (int64_t)rblocks * 2 * kTileRhs, w->ldk, 2 * kTileRhs);
@@ -383,7 +383,7 @@ int tensor_status(const Operator& op, bool reset) {
     if (!w) return 0;
     int v = 0;
     SB_CUDA(cudaMemcpy(&v, w->status.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (reset && v) SB_CUDA(cudaMemset(w->status.p, 0, sizeof(int)));
+    if (reset && v) memset_sync(w->status.p, 0, sizeof(int));
     return v;
 }
 
