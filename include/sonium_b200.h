@@ -428,8 +428,11 @@ SB_API int sb_batch_timings(const sb_batch* batch, double* assembly_ms, double* 
  * released blocks of the same size (rounded to 2 MiB, or 512 B below 1 MiB) before cudaMalloc is
  * asked; a released block enters the cache after a device synchronisation (as cudaFree waits)
  * while the cache holds at most 96 GiB per device, and an allocation that fails empties the
- * cache and retries. trim returns every cached block of a device (device < 0: all devices) to
- * the driver; stats reports the bytes held by live buffers and by the cache. */
+ * cache and retries. The solver workspaces of destroyed operators (vectors, pinned host memory,
+ * captured cycle graphs) are likewise kept, four per process, for the next operator of the same
+ * size. trim frees the kept workspaces and returns every cached block of a device (device < 0:
+ * all devices) to the driver; stats reports the bytes held by live buffers (kept workspaces
+ * included) and by the cache. */
 SB_API int sb_memory_trim(int device);
 SB_API int sb_memory_stats(int device, int64_t* in_use_bytes, int64_t* cached_bytes);
 

@@ -1130,7 +1130,10 @@ SB_API int sb_gcro_dr(const sb_operator* op, const sb_complex* b, const sb_compl
 }
 
 SB_API int sb_memory_trim(int device) {
-    return guarded([&] { memory_trim(device); });
+    return guarded([&] {
+        solve_work_pool_trim(device);
+        memory_trim(device);
+    });
 }
 
 SB_API int sb_memory_stats(int device, int64_t* in_use_bytes, int64_t* cached_bytes) {

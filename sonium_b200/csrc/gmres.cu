@@ -15,6 +15,7 @@
 
 #include <complex>
 #include <functional>
+#include <mutex>
 
 #include "sb_blas.cuh"
 #include "sb_internal.cuh"
@@ -141,17 +142,56 @@ struct SolveWork {
     }
 };
 
+// Workspaces of destroyed operators are kept (a few per process) for the next operator of the
+// same size and device: its buffers, pinned host memory and captured cycle graphs are reused (a
+// graph is replayed only when every pointer it bakes in matches; see run_cycle).
+namespace {
+std::mutex g_ws_mu;
+std::vector<std::pair<int, SolveWork*>> g_ws_pool;
+constexpr size_t kWsPool = 4;
+}  // namespace
+
 void destroy_solve_work(Operator& op) {
-    if (op.work) {
-        cudaSetDevice(op.device);
-        delete static_cast<SolveWork*>(op.work);
-        op.work = nullptr;
+    if (!op.work) return;
+    cudaSetDevice(op.device);
+    SolveWork* w = static_cast<SolveWork*>(op.work);
+    op.work = nullptr;
+    std::lock_guard<std::mutex> lock(g_ws_mu);
+    if (g_ws_pool.size() < kWsPool) {
+        g_ws_pool.push_back({op.device, w});
+    } else {
+        delete w;
     }
+}
+
+void solve_work_pool_trim(int device) {
+    std::lock_guard<std::mutex> lock(g_ws_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto it = g_ws_pool.begin(); it != g_ws_pool.end();) {
+        if (device >= 0 && it->first != device) {
+            ++it;
+            continue;
+        }
+        cudaSetDevice(it->first);
+        delete it->second;
+        it = g_ws_pool.erase(it);
+    }
+    cudaSetDevice(cur);
 }
 
 static SolveWork& solve_work(const Operator& op) {
     Operator& o = const_cast<Operator&>(op);
-    if (!o.work) o.work = new SolveWork();
+    if (!o.work) {
+        std::lock_guard<std::mutex> lock(g_ws_mu);
+        for (auto it = g_ws_pool.begin(); it != g_ws_pool.end(); ++it)
+            if (it->first == op.device && it->second->n == op.n) {
+                o.work = it->second;
+                g_ws_pool.erase(it);
+                break;
+            }
+        if (!o.work) o.work = new SolveWork();
+    }
     SolveWork& w = *static_cast<SolveWork*>(o.work);
     w.ensure(op.n);
     return w;

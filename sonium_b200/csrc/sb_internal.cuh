@@ -233,6 +233,8 @@ void gmres_mixed_ir(const Operator& op, const double2* b_dev, double2* x_dev, bo
                     const sb_ir_config& cfg, sb_gmres_stats& st);
 
 void destroy_solve_work(Operator& op);
+// Frees the kept solver workspaces of `device` (all devices when device < 0).
+void solve_work_pool_trim(int device);
 struct Gate;
 // Products with FP64 vectors on whichever matrix the operator holds (gmres.cu).
 void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g);
