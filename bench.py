@@ -114,30 +114,65 @@ class Dist:
 # clocks
 # ---------------------------------------------------------------------------------------------
 class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons around a timed region.
+
+    The sampler runs at 25 ms; start() waits for its first sample so that the timed region is
+    covered from its beginning, and stop() keeps the samples taken between mark() and stop()
+    (plus the one just before mark(), so that a region shorter than the period still has one).
+    """
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 25
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.rows = []
+        self.t_mark = None
+        self.thread = None
+
+    def _reader(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.perf_counter(), line))
 
     def start(self):
+        import threading
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.PERIOD_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return
+        self.thread = threading.Thread(target=self._reader, daemon=True)
+        self.thread.start()
+        t0 = time.perf_counter()
+        while not self.rows and time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.t_mark = time.perf_counter()
+
+    def mark(self):
+        self.t_mark = time.perf_counter()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(self.PERIOD_MS / 1000.0 * 1.5)  # one more sample after the region
+        t_stop = time.perf_counter()
         self.proc.terminate()
-        out, _ = self.proc.communicate(timeout=10)
+        try:
+            self.proc.wait(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=10)
+        rows = list(self.rows)
+        before = [r for r in rows if r[0] < self.t_mark]
+        inside = [r for r in rows if self.t_mark <= r[0] <= t_stop]
+        keep = (before[-1:] if before else []) + inside
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for row in csv.reader(io.StringIO(out)):
+        for row in csv.reader(io.StringIO("".join(line for _, line in keep))):
             if len(row) < 9:
                 continue
             try:
@@ -151,7 +186,7 @@ class Clocks:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "sm_mhz_min": min(sm), "period_ms": self.PERIOD_MS}
 
 
 def peaks():
