@@ -4,12 +4,15 @@ Workload (default): rigid sphere, icosphere level 5 (N = 20480 flat triangles, c
 collocated at centroids), k = 10, incident plane wave exp(i k z), beta = i/k. One step = one
 solve: re-assembly of the dense system on the device, the incident right-hand side, and GMRES.
 
-  * `value`  -- the mixed-precision solver (complex128 matrix + complex64 copy written by one
-                assembly epilogue; FP32 inner GMRES(50) to 1e-5 inside FP64 refinement to 1e-8),
-                inputs resident in HBM, device time by CUDA events on the operator's stream.
-                Its relative error against the plain FP64 solution is measured and reported.
+  * `value`  -- the fastest mixed-precision form whose solution is within 1e-5 of the plain FP64
+                one (`headline_mode`): FP32 assembly (FP64 phase, near and self terms) and FP64
+                refinement to 1e-8 around an inner GMRES(50) with FP32 vectors, on the complex64
+                matrix (`mixed`, inner tolerance 1e-5) or on its power-of-two-scaled complex-half
+                copy (`mixed_half`, inner tolerance 1e-3); `mixed_fp64_matrix` refines on the
+                complex128 matrix. Inputs resident in HBM, device time by CUDA events on the
+                operator's stream; every mode's error against the plain FP64 solution is reported.
   * `plain_fp64` -- the same solve with complex128 only and FP64 GMRES(50) to 1e-8.
-  * `e2e`    -- the mixed solve through the C ABI with host buffers: mesh upload, assembly,
+  * `e2e`    -- the headline form through the C ABI with host buffers: mesh upload, assembly,
                 host RHS, solve with host b / x (all copies inside the timed region).
   * `cpu_baseline` / `--impl reference` -- the CPU restatement of the reference path (oracle),
                 timed on a bounded sample (assembly rows + a CPU matvec) and scaled to one solve.
@@ -72,6 +75,8 @@ def parse():
                     help="run only the N = 81920, k = 40 precision-form leg (~165 GB) and print its JSON")
     ap.add_argument("--single", action="store_true",
                     help="one untimed solve per precision mode at --level (profiling driver), no JSON line")
+    ap.add_argument("--single-mode", choices=sorted(MODES), default=None,
+                    help="with --single: run only this mode")
     return ap.parse_args()
 
 
@@ -269,10 +274,20 @@ def reference_arm(a, dist: Dist):
 # ---------------------------------------------------------------------------------------------
 MODES = {
     # name: (assembly precision, solver)
+    "mixed_half": ("SB_PRECISION_FP32", "ir16"),
     "mixed": ("SB_PRECISION_FP32", "ir"),
     "mixed_fp64_matrix": ("SB_PRECISION_FP64_FP32", "ir"),
     "plain_fp64": ("SB_PRECISION_FP64", "fp64"),
 }
+# Inner tolerance of the refinement with the complex-half inner matrix: the half copy limits each
+# refinement to about three digits, so a tighter inner solve buys nothing.
+HALF_INNER_TOL = 1e-3
+# DRAM bytes per matrix entry of one k_gemv_n_c16 launch: dram__bytes_read.sum +
+# dram__bytes_write.sum = 108.19 MB at N = 5120 (ncu, cold caches).
+GEMV16_TRAFFIC_PER_ENTRY = 4.13
+# Modes that may carry the headline (fastest first when both meet the accuracy bar), with the
+# kernel class of their dominant matrix-vector product.
+HEADLINE_MODES = {"mixed_half": "SB_PROF_GEMV16", "mixed": "SB_PROF_GEMV32"}
 
 
 def main():
@@ -290,7 +305,7 @@ def main():
     lib = L.load()
     dev = dist.local
     if a.single:
-        single_solves(sb, a.level, a.k, dev)
+        single_solves(sb, a.level, a.k, dev, a.single_mode and [a.single_mode])
         return
     assert sb.device_count() > dev, "no CUDA device for this rank"
     if a.sweep_only or a.precision_form or a.multi_rhs:
@@ -314,6 +329,7 @@ def main():
     phys = ph._struct()
     bta = L.SbComplex(beta.real, beta.imag)
     ir = L.SbIrConfig(20, TOL, RESTART, 20, 1e-5)
+    ir16 = L.SbIrConfig(20, TOL, RESTART, 20, HALF_INNER_TOL)
     gc = L.SbGmresConfig(100, RESTART, TOL, 1)
     st = L.SbGmresStats()
     ev0, ev1 = ct.c_void_p(), ct.c_void_p()
@@ -324,8 +340,9 @@ def main():
         def step():
             L.check(lib.sb_assemble_into(op.handle, ct.byref(phys), bta))
             L.check(lib.sb_rhs_plane_wave_device(op.handle, dirs.ctypes.data, None, 1, b_d))
-            if solver == "ir":
-                L.check(lib.sb_gmres_mixed_device(op.handle, b_d, x_d, 0, ct.byref(ir), ct.byref(st)))
+            if solver in ("ir", "ir16"):
+                cfg = ir16 if solver == "ir16" else ir
+                L.check(lib.sb_gmres_mixed_device(op.handle, b_d, x_d, 0, ct.byref(cfg), ct.byref(st)))
             else:
                 L.check(lib.sb_gmres_device(op.handle, b_d, x_d, 0, ct.byref(gc), 0, ct.byref(st)))
             return L.SbGmresStats.from_buffer_copy(st)
@@ -344,10 +361,12 @@ def main():
         return dist.max(ms.value / 1e3), stats
 
     results, x_ref = {}, None
-    prof_main = clk = None
-    for name in ("plain_fp64", "mixed_fp64_matrix", "mixed"):
+    live = {}  # per headline-capable mode: (live profile, class breakdown, clocks, launches)
+    for name in ("plain_fp64", "mixed_fp64_matrix", "mixed", "mixed_half"):
         prec, solver = MODES[name]
         op = sb.build_tbem_system_with_beta(mesh, ph, beta, getattr(sb, prec))
+        if solver == "ir16":
+            op.set_inner_precision(sb.SB_INNER_FP16)
         step = make_step(op, solver)
         s0 = step()  # untimed: solution for the accuracy check
         x = _to_host(rt, x_d, n)
@@ -355,22 +374,20 @@ def main():
             x_ref = x
         for _ in range(a.warmup):
             step()
-        headline = name == "mixed"
-        if headline:
+        cls = HEADLINE_MODES.get(name)
+        if cls:
             count = L.SbProfile()
             L.check(lib.sb_profile_read(ct.byref(count), 1))  # resets the counters
-            # Inside the timed region only the complex64 matvec (the dominant kernel class) is
-            # timed, by CUDA events on its stream, for the roofline.
-            L.check(lib.sb_profile_enable_classes(1 << L.SB_PROF_GEMV32))
+            # Inside the timed region only the dominant matrix-vector product class is timed, by
+            # CUDA events on its stream, for the roofline.
+            L.check(lib.sb_profile_enable_classes(1 << getattr(L, cls)))
             clocks = Clocks(dev)
             clocks.start()
         t, stats = timed(step, op.handle, a.steps)
-        if headline:
+        if cls:
             clk = clocks.stop()
             L.check(lib.sb_profile_enable_classes(0))
             L.check(lib.sb_profile_read(ct.byref(count), 1))
-            launches_timed = int(count.kernels)
-            prof_live = count
             # Kernel-class times from a second pass of the same K steps with the library's event
             # profiling on: its event pairs stay out of the timed region above.
             prof = L.SbProfile()
@@ -380,14 +397,20 @@ def main():
             rt.cudaDeviceSynchronize()
             L.check(lib.sb_profile_enable(0))
             L.check(lib.sb_profile_read(ct.byref(prof), 1))
-            prof_main = prof
+            live[name] = (count, prof, clk, int(count.kernels))
         results[name] = {
             "value": dist.world * a.steps / t, "unit": "solves/s", "ms_per_step": 1e3 * t / a.steps,
             "assembly": prec, "error_vs_fp64": float(np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref)),
             "iterations": int(s0.iterations), "matvecs": int(s0.matvecs), "matvecs_fp32": int(s0.matvecs_fp32),
             "refinements": int(s0.refinements), "residual": s0.residual,
         }
+        if solver == "ir16":
+            results[name]["inner"] = "complex-half matrix, inner tolerance %g" % HALF_INNER_TOL
         op.close()
+    # Headline: the fastest mixed form whose solution is within 1e-5 of the FP64 one.
+    ok = [m for m in HEADLINE_MODES if results[m]["error_vs_fp64"] <= 1e-5]
+    head_mode = max(ok, key=lambda m: results[m]["value"]) if ok else "mixed"
+    prof_live, prof_main, clk, launches_timed = live[head_mode]
 
     # ---- e2e through the C ABI with host buffers ----
     e2e = None
@@ -400,8 +423,11 @@ def main():
             t0 = time.perf_counter()
             m2 = sb.Mesh(nodes, tris, device=dev)
             o2 = sb.build_tbem_system_with_beta(m2, ph, beta, sb.SB_PRECISION_FP32)
+            if head_mode == "mixed_half":
+                o2.set_inner_precision(sb.SB_INNER_FP16)
             bh = sb.rhs_plane_wave(m2, ph, beta, dirs)[:, 0]
-            sb.gmres_mixed(o2, bh, sb.IrConfig(20, TOL, RESTART, 20, 1e-5))
+            sb.gmres_mixed(o2, bh, sb.IrConfig(20, TOL, RESTART, 20,
+                                               HALF_INNER_TOL if head_mode == "mixed_half" else 1e-5))
             o2.close()
             m2.close()
             rt.cudaDeviceSynchronize()
@@ -413,8 +439,9 @@ def main():
         d2h = 16 * n + 16 * n                           # RHS and solution
         e2e = {"value": dist.world * len(ts) / sum(ts), "unit": "solves/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "sb_mesh_create + sb_assemble(SB_PRECISION_FP32) + sb_rhs_plane_wave + sb_gmres_mixed "
-                       "(host buffers), wall clock"}
+               "path": "sb_mesh_create + sb_assemble(SB_PRECISION_FP32) + "
+                       + ("sb_operator_set_inner_precision(SB_INNER_FP16) + " if head_mode == "mixed_half" else "")
+                       + "sb_rhs_plane_wave + sb_gmres_mixed (host buffers), wall clock"}
 
     # ---- batched frequency sweep ----
     sweep = None if a.no_sweep else sweep_leg(sb, a, dist, dev, rt)
@@ -433,20 +460,25 @@ def main():
     launches = {names[i]: prof.launches[i] for i in range(L.SB_PROF_KINDS)}
     total_ms = sum(ms.values())
     dominant = max(ms, key=lambda kk: ms[kk])
-    # complex64 matvec: 8 N^2 bytes of matrix per launch (+ 8 N x, 8 N y); complex128: 16 N^2
-    bytes_mv = {"gemv32": 8.0 * n * n + 16.0 * n, "gemv64": 16.0 * n * n + 32.0 * n}
-    hbm_kind = "gemv32"
+    # complex-half matvec: 4 N^2 bytes of matrix per launch (+ 8 N x, 8 N y); complex64: 8 N^2;
+    # complex128: 16 N^2
+    bytes_mv = {"gemv16": 4.0 * n * n + 16.0 * n, "gemv32": 8.0 * n * n + 16.0 * n,
+                "gemv64": 16.0 * n * n + 32.0 * n}
+    hbm_kind = "gemv16" if head_mode == "mixed_half" else "gemv32"
+    hbm_cls = getattr(L, HEADLINE_MODES[head_mode])
     # average working launch of the matvec, from the events recorded inside the timed region
-    live_ms = prof_live.ms[L.SB_PROF_GEMV32]
-    live_n = prof_live.launches[L.SB_PROF_GEMV32]
+    live_ms = prof_live.ms[hbm_cls]
+    live_n = prof_live.launches[hbm_cls]
     avg = live_ms / max(live_n, 1) / 1e3
     achieved = bytes_mv[hbm_kind] / avg / 1e9
-    # DRAM traffic per launch from one ncu capture of the same kernel at N = 5120
-    # (dram__bytes_read.sum + dram__bytes_write.sum = 221.9 MB = 8.47 bytes per complex64 matrix
-    # entry), scaled by the entries of this launch; the complex128 kernel was not captured.
-    traffic = 8.47 * n * n if hbm_kind == "gemv32" else None
-    roof = {"kernel": ("k_gemv_n_c64 (complex64 matrix; FP32 or FP64 vectors)" if hbm_kind == "gemv32"
-                       else "k_gemv_n_c128 (complex128 matvec)"),
+    # DRAM traffic per launch from one ncu capture of the same kernel at N = 5120, scaled by the
+    # entries of this launch: dram__bytes_read.sum + dram__bytes_write.sum per matrix entry.
+    traffic_per_entry = {"gemv16": GEMV16_TRAFFIC_PER_ENTRY, "gemv32": 8.47}
+    tpe = traffic_per_entry.get(hbm_kind)
+    traffic = None if tpe is None else tpe * n * n
+    kernel_names = {"gemv16": "k_gemv_n_c16 (complex-half matrix, FP32 vectors)",
+                    "gemv32": "k_gemv_n_c64 (complex64 matrix; FP32 or FP64 vectors)"}
+    roof = {"kernel": kernel_names[hbm_kind],
             "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_source": pk_kind,
             "bytes_per_launch": bytes_mv[hbm_kind], "avg_launch_ms": avg * 1e3,
@@ -463,9 +495,7 @@ def main():
     cpu = None
     if not a.no_cpu and dist.rank == 0:
         cpu = cpu_baseline(a.level, a.k, results["plain_fp64"]["matvecs"])
-    head = results["mixed"]
-    if head["error_vs_fp64"] > 1e-5:  # accuracy bar of the metric: fall back to the FP64-matrix IR
-        head = results["mixed_fp64_matrix"]
+    head = results[head_mode]
     line = {
         "metric": "BEM solves/s at <=1e-5 rel err vs FP64 (mixed-precision solve, dense Burton-Miller TBEM)",
         "value": head["value"], "unit": "solves/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
@@ -473,10 +503,12 @@ def main():
         "vs_baseline": None, "dtype": "c64 (FP64 phase, near/self, refinement)",
         "data": "synthetic (icosphere geometry, analytic incident plane wave)",
         "config": {"workload": f"rigid sphere icosphere L{a.level} (N={n}), k={a.k}, beta=i/k, plane wave +z; "
-                               f"one step = assembly + RHS + GMRES({RESTART}) FP32 inner / FP64-refined to "
-                               f"rtol {TOL}",
+                               f"one step = assembly + RHS + GMRES({RESTART}) inner solve on the "
+                               f"{'complex-half' if head_mode == 'mixed_half' else 'complex64'} matrix with FP32 "
+                               f"vectors / FP64-refined on the complex64 matrix to rtol {TOL}",
                    "N": n, "l2": "inputs larger than L2 (complex64 matrix %.1f GB)" % (8 * n * n / 1e9),
                    "parallelism": f"replicas x{dist.world}"},
+        "headline_mode": head_mode,
         "error_vs_fp64": head["error_vs_fp64"],
         "speedup_vs_plain_fp64": head["value"] / results["plain_fp64"]["value"],
         "modes": results,
@@ -755,17 +787,20 @@ def precision_leg(sb, a, dist, dev, rt):
     }
 
 
-def single_solves(sb, level, k, dev):
+def single_solves(sb, level, k, dev, modes=None):
     """One solve per precision mode, untimed: the small case the ncu captures profile."""
     nodes, tris = sb.icosphere(RADIUS, level)
     ph = sb.PhysicsParams.for_wavenumber(k)
     beta = ph.burton_miller_beta()
     mesh = sb.Mesh(nodes, tris, device=dev)
     b = sb.rhs_plane_wave(mesh, ph, beta, [0.0, 0.0, 1.0])[:, 0]
-    for name in ("mixed", "plain_fp64"):
+    for name in (modes or ("mixed", "mixed_half", "plain_fp64")):
         prec, solver = MODES[name]
         op = sb.build_tbem_system_with_beta(mesh, ph, beta, getattr(sb, prec))
-        if solver == "ir":
+        if solver == "ir16":
+            op.set_inner_precision(sb.SB_INNER_FP16)
+            s = sb.gmres_mixed(op, b, sb.IrConfig(20, TOL, RESTART, 20, HALF_INNER_TOL))
+        elif solver == "ir":
             s = sb.gmres_mixed(op, b, sb.IrConfig(20, TOL, RESTART, 20, 1e-5))
         else:
             s = sb.gmres(op, b, sb.GmresConfig(100, RESTART, TOL))

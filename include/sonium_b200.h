@@ -288,6 +288,19 @@ typedef struct sb_ir_config {
 } sb_ir_config;
 SB_API int sb_gmres_mixed(const sb_operator* op, const sb_complex* b, const sb_complex* x0,
                           const sb_ir_config* cfg, sb_complex* x, sb_gmres_stats* stats);
+/* Matrix of the inner GMRES of sb_gmres_mixed (no reference counterpart: a storage choice of this
+ * library). SB_INNER_FP32 (default): the complex64 copy. SB_INNER_FP16: a complex-half copy of the
+ * complex64 matrix (real and imaginary parts times one power-of-two scale s, chosen so that the
+ * largest part maps to [2^13, 2^14), rounded to FP16; products divide by s exactly), built on the
+ * device on the first mixed solve after each assembly. The inner products read 4 bytes per entry
+ * instead of 8; the outer residual stays on the complex64 (or complex128) matrix with FP64
+ * vectors, so the converged solution is that of the complex64 system, as with SB_INNER_FP32. The
+ * copy perturbs the inner operator by about 2^-11 of each entry, so each refinement gains about
+ * three digits: inner_tolerance near 1e-3 avoids inner iterations that cannot pay. Needs an
+ * operator with a complex64 matrix (SB_PRECISION_FP64_FP32 or SB_PRECISION_FP32). */
+#define SB_INNER_FP32 0
+#define SB_INNER_FP16 1
+SB_API int sb_operator_set_inner_precision(sb_operator* op, int inner);
 SB_API int sb_gmres_mixed_device(const sb_operator* op, const sb_complex* b_dev,
                                  sb_complex* x_dev, int x0_given, const sb_ir_config* cfg,
                                  sb_gmres_stats* stats);
@@ -447,7 +460,8 @@ SB_API int sb_memory_stats(int device, int64_t* in_use_bytes, int64_t* cached_by
 #define SB_PROF_ARNOLDI 5    /* Gram-Schmidt dots / projections / basis updates */
 #define SB_PROF_OTHER 6      /* geometry, coefficients, RHS reductions, plane waves */
 #define SB_PROF_TENSOR 7     /* tensor-core block product (BF16 split, tcgen05) */
-#define SB_PROF_KINDS 8
+#define SB_PROF_GEMV16 8     /* complex-half matvec of the FP16 inner solve (incl. its copy) */
+#define SB_PROF_KINDS 9
 typedef struct sb_profile {
     double ms[SB_PROF_KINDS];
     int64_t launches[SB_PROF_KINDS];

@@ -24,6 +24,8 @@ SB_ERR_NOT_FINITE = 7
 SB_PRECISION_FP64 = 0
 SB_PRECISION_FP64_FP32 = 1
 SB_PRECISION_FP32 = 2
+SB_INNER_FP32 = 0
+SB_INNER_FP16 = 1
 SB_OP_N, SB_OP_T, SB_OP_C = 0, 1, 2
 SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI = 0, 1
 SB_BC_VELOCITY, SB_BC_PRESSURE = 0, 1
@@ -87,9 +89,9 @@ class SbGmresStats(ct.Structure):
 
 
 (SB_PROF_FAR, SB_PROF_NEAR, SB_PROF_SELF, SB_PROF_GEMV64, SB_PROF_GEMV32, SB_PROF_ARNOLDI, SB_PROF_OTHER,
- SB_PROF_TENSOR) = range(8)
-SB_PROF_KINDS = 8
-PROF_NAMES = ["far", "near", "self", "gemv64", "gemv32", "arnoldi", "other", "tensor"]
+ SB_PROF_TENSOR, SB_PROF_GEMV16) = range(9)
+SB_PROF_KINDS = 9
+PROF_NAMES = ["far", "near", "self", "gemv64", "gemv32", "arnoldi", "other", "tensor", "gemv16"]
 
 
 class SbProfile(ct.Structure):
@@ -143,6 +145,7 @@ _SIGNATURES = {
     "sb_gmres_device": ([P, P, P, ct.c_int, ct.POINTER(SbGmresConfig), ct.c_int, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_mixed": ([P, P, P, ct.POINTER(SbIrConfig), P, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_mixed_device": ([P, P, P, ct.c_int, ct.POINTER(SbIrConfig), ct.POINTER(SbGmresStats)], ct.c_int),
+    "sb_operator_set_inner_precision": ([P, ct.c_int], ct.c_int),
     "sb_rhs_plane_wave_device": ([P, P, P, ct.c_int64, P], ct.c_int),
     "sb_gcro_subspace_create": ([ct.c_int, ct.c_int64, ct.POINTER(P)], ct.c_int),
     "sb_gcro_subspace_destroy": ([P], ct.c_int),

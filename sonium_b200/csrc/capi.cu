@@ -502,6 +502,7 @@ SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_compl
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
         tensor_release(*op->op);
+        op->op->half_valid = false;
         if (op->op->basis != SB_BASIS_CONSTANT)
             assemble_discontinuous(*op->op, *physics, beta.re, beta.im);
         else
@@ -1018,6 +1019,21 @@ SB_API int sb_gmres_mixed(const sb_operator* op, const sb_complex* b, const sb_c
         gmres_mixed_ir(o, db.as<double2>(), dx.as<double2>(), x0 != nullptr, *cfg, *stats);
         SB_CUDA(cudaMemcpyAsync(x, dx.p, sizeof(double2) * o.n, cudaMemcpyDeviceToHost, o.stream));
         SB_CUDA(cudaStreamSynchronize(o.stream));
+    });
+}
+
+SB_API int sb_operator_set_inner_precision(sb_operator* op, int inner) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op, SB_ERR_INVALID_ARGUMENT, "null argument");
+        SB_REQUIRE(inner == SB_INNER_FP32 || inner == SB_INNER_FP16, SB_ERR_INVALID_ARGUMENT,
+                   "inner precision must be SB_INNER_FP32 or SB_INNER_FP16");
+        SB_REQUIRE(inner == SB_INNER_FP32 || op->op->A32.p, SB_ERR_INVALID_ARGUMENT,
+                   "SB_INNER_FP16 needs a complex64 matrix (SB_PRECISION_FP64_FP32 or SB_PRECISION_FP32)");
+        op->op->inner = inner;
+        if (inner == SB_INNER_FP32) {
+            op->op->A16.release();
+            op->op->half_valid = false;
+        }
     });
 }
 

@@ -223,6 +223,7 @@ struct Problem {
     const void* key_A = nullptr;                                // identifies the captured graph
     std::function<void(const T*, T*, Gate)> apply;              // y = A x (gated)
     std::function<void(const T*, const T*, T*, double*)> residual;  // r = b - A x, partials
+    int64_t partials = 0;                                       // partial norms residual writes
     const double2* jacobi = nullptr;                            // diagonal for Jacobi, or null
     cudaStream_t stream = nullptr;
 };
@@ -327,7 +328,7 @@ CoreResult gmres_core(KrylovWork<T>& W, const Problem<T>& P, const T* b, T* x, i
     };
     auto residual = [&](T* out, bool with_state) -> double {
         P.residual(x, b, out, partd);
-        sum_real(partd, gemv_partials(n), nrm + 2, s);
+        sum_real(partd, P.partials, nrm + 2, s);
         SB_CUDA(cudaMemcpyAsync(hsc, nrm + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
         if (with_state) SB_CUDA(cudaMemcpyAsync(hst, W.st.p, sizeof(KState), cudaMemcpyDeviceToHost, s));
         SB_CUDA(cudaStreamSynchronize(s));
@@ -513,6 +514,7 @@ Problem<double2> problem64(const Operator& op) {
     P.n = op.n;
     P.stream = op.stream;
     P.key_A = op.A64.p ? op.A64.p : op.A32.p;
+    P.partials = gemv_partials(op.n);
     P.apply = [&op](const double2* xi, double2* yo, Gate g) { op_gemv64(op, xi, yo, g); };
     P.residual = [&op](const double2* xi, const double2* bi, double2* ro, double* part) {
         op_residual64(op, xi, bi, ro, part);
@@ -525,11 +527,29 @@ Problem<float2> problem32(const Operator& op) {
     P.n = op.n;
     P.stream = op.stream;
     P.key_A = op.A32.p;
+    P.partials = gemv_partials(op.n);
     P.apply = [&op](const float2* xi, float2* yo, Gate g) {
         gemv_c64(op.A32.as<float2>(), op.n, op.lda32, xi, yo, nullptr, nullptr, op.stream, g);
     };
     P.residual = [&op](const float2* xi, const float2* bi, float2* ro, double* part) {
         gemv_c64(op.A32.as<float2>(), op.n, op.lda32, xi, ro, bi, part, op.stream);
+    };
+    return P;
+}
+
+// The inner problem on the complex-half copy (SB_INNER_FP16).
+Problem<float2> problem16(const Operator& op) {
+    Problem<float2> P;
+    P.n = op.n;
+    P.stream = op.stream;
+    P.key_A = op.A16.p;
+    P.partials = gemv16_partials(op.n);
+    const float* inv = reinterpret_cast<const float*>(op.half_aux.as<unsigned>() + 2);
+    P.apply = [&op, inv](const float2* xi, float2* yo, Gate g) {
+        gemv_c16(op.A16.as<uint32_t>(), op.n, op.lda16, inv, xi, yo, nullptr, nullptr, op.stream, g);
+    };
+    P.residual = [&op, inv](const float2* xi, const float2* bi, float2* ro, double* part) {
+        gemv_c16(op.A16.as<uint32_t>(), op.n, op.lda16, inv, xi, ro, bi, part, op.stream);
     };
     return P;
 }
@@ -578,7 +598,9 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
         SB_CUDA(cudaStreamSynchronize(op.stream));
         return std::sqrt(hsc[0]);
     };
-    Problem<float2> P = problem32(op);
+    const bool half = op.inner == SB_INNER_FP16;
+    if (half) half_prepare(const_cast<Operator&>(op));
+    Problem<float2> P = half ? problem16(op) : problem32(op);
     st = sb_gmres_stats{};
     // ||b|| by a norm kernel; with a zero initial guess the first residual is b itself.
     arnoldi_dots<double2>(b, n, 0, b, n, sw.k64_part(n), sw.k64_red(), op.stream);

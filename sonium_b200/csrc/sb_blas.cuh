@@ -31,6 +31,11 @@ void gemv_c64(const float2* A, int64_t n, int64_t lda, const float2* x, float2* 
               const float2* b, double* part, cudaStream_t s, Gate gate = {});
 void gemv_c64_x64(const float2* A, int64_t n, int64_t lda, const double2* x, double2* y,
                   const double2* b, double* part, cudaStream_t s, Gate gate = {});
+// Complex-half matrix (uint32 = FP16 re | FP16 im << 16; lda a multiple of 4), FP32 vectors and
+// accumulation: y = (A x) * inv_scale[0], or b - (A x) * inv_scale[0] with part = ||.||^2.
+void gemv_c16(const uint32_t* A, int64_t n, int64_t lda, const float* inv_scale, const float2* x, float2* y,
+              const float2* b, double* part, cudaStream_t s, Gate gate = {});
+int64_t gemv16_partials(int64_t n);
 
 // out[i] = V_i^H w (i < k), out[k].x = |w|^2; part holds arnoldi_dot_chunks(n) * (k + 1).
 template <class T>

@@ -171,6 +171,13 @@ struct Operator {
     double sign = 1.0;  // the stabilised discontinuous systems' sign (every entry times sign)
     DevBuf lin_cp, lin_cn, lin_ptr, lin_col;
     int64_t lin_nnz = 0;
+    // Complex-half copy of the complex64 matrix for the inner solve of the mixed solver
+    // (SB_INNER_FP16): FP16 (re, im) pairs of the entries times a power-of-two scale, rows lda16
+    // entries apart; half_aux holds the largest part's bits, the scale and its inverse (device).
+    int inner = SB_INNER_FP32;
+    DevBuf A16, half_aux;
+    int64_t lda16 = 0;
+    bool half_valid = false;
     cudaStream_t stream = nullptr;
     double last_assembly_ms = 0.0;
 };
@@ -236,6 +243,8 @@ void destroy_solve_work(Operator& op);
 // Frees the kept solver workspaces of `device` (all devices when device < 0).
 void solve_work_pool_trim(int device);
 struct Gate;
+// Builds the complex-half copy of the complex64 matrix on the operator's stream (blas.cu).
+void half_prepare(Operator& op);
 // Products with FP64 vectors on whichever matrix the operator holds (gmres.cu).
 void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g);
 void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part);

@@ -216,6 +216,12 @@ class TbemOperator(LinearOperator):
         check(L.load().sb_operator_info_get(self.handle, ct.byref(i)))
         return i
 
+    def set_inner_precision(self, inner: int) -> None:
+        """Matrix of gmres_mixed's inner GMRES: SB_INNER_FP32 (the complex64 copy, default) or
+        SB_INNER_FP16 (a power-of-two-scaled complex-half copy, half the bytes per product; pair it
+        with IrConfig(inner_tolerance=1e-3)). Needs a complex64 matrix."""
+        check(L.load().sb_operator_set_inner_precision(self.handle, int(inner)))
+
     def reassemble(self, physics: PhysicsParams, beta: complex) -> None:
         check(L.load().sb_assemble_into(self.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag)))
         self.physics, self.beta = physics, beta
