@@ -414,6 +414,11 @@ SB_API int sb_batch_set_rhs_plane_wave(sb_batch* batch, const double* direction)
 SB_API int sb_batch_set_rhs(sb_batch* batch, int64_t index, const sb_complex* b);
 /* stats: count entries, one per instance (device_ms is the whole batch's time). */
 SB_API int sb_batch_solve(sb_batch* batch, const sb_ir_config* cfg, sb_gmres_stats* stats);
+/* Matrix of the batched inner products, as sb_operator_set_inner_precision: SB_INNER_FP32 (the
+ * complex64 matrices, default) or SB_INNER_FP16 (complex-half copies of every instance's matrix,
+ * each with its own power-of-two scale, built on the device by the first solve after each
+ * sb_batch_assemble and counted in its time; 4 bytes per entry of extra device memory). */
+SB_API int sb_batch_set_inner_precision(sb_batch* batch, int inner);
 SB_API int sb_batch_solution(const sb_batch* batch, int64_t index, sb_complex* x);
 /* The assembled complex64 matrix of one instance, row-major n x n. */
 SB_API int sb_batch_matrix_c64(const sb_batch* batch, int64_t index, sb_complex32* matrix);

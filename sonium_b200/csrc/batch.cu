@@ -62,6 +62,11 @@ struct BInst {
     int* outer;       // 1 while the instance refines
     int* live;        // 1 while its inner solve runs
     int* brk;         // inner breakdown before the first step
+    // Complex-half copy of A for the inner products (SB_INNER_FP16): entries times a power-of-two
+    // scale, rows lda16 apart; aux16 = [largest part's bits, scale, 1 / scale].
+    const uint32_t* A16;
+    int64_t lda16;
+    unsigned* aux16;
 };
 
 namespace {
@@ -107,6 +112,45 @@ __global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restric
                                                                     nullptr, nullptr, blk);
     else
         gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.d, I.rq, I.rb, I.pnorm, blk);
+}
+
+// The same products on the complex-half copies (kGemv16Rows rows per CTA).
+__global__ void __launch_bounds__(kGemvThreads) k_bgemv16(const BInst* __restrict__ inst,
+                                                          const int64_t* __restrict__ pre, int ninst, int mode,
+                                                          int j, int gk) {
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const int64_t blk = blockIdx.x - pre[b];
+    const float* inv = reinterpret_cast<const float*>(I.aux16 + 2);
+    if (mode == 0)
+        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, I.V + (int64_t)j * I.vs,
+                                                                 I.w, nullptr, nullptr, blk);
+    else
+        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, I.d, I.rq, I.rb,
+                                                                 I.pnorm, blk);
+}
+
+// Complex-half copies of every instance's complex64 matrix: largest part, scale, conversion,
+// over the same kGemv16Rows row blocks.
+__global__ void __launch_bounds__(kHalfThreads) k_bhalf_absmax(const BInst* __restrict__ inst,
+                                                               const int64_t* __restrict__ pre, int ninst) {
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    const int64_t r0 = (blockIdx.x - pre[b]) * kGemv16Rows;
+    half_absmax_rows(I.A, I.n, I.lda, r0, r0 + kGemv16Rows < I.n ? r0 + kGemv16Rows : I.n, 1, I.aux16);
+}
+__global__ void k_bhalf_scale(const BInst* __restrict__ inst, int ninst) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < ninst) half_scale_from_max(inst[b].aux16);
+}
+__global__ void __launch_bounds__(kHalfThreads) k_bhalf_convert(const BInst* __restrict__ inst,
+                                                                const int64_t* __restrict__ pre, int ninst) {
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    const int64_t r0 = (blockIdx.x - pre[b]) * kGemv16Rows;
+    half_convert_rows(I.A, I.n, I.lda, I.aux16, const_cast<uint32_t*>(I.A16), I.lda16, r0,
+                      r0 + kGemv16Rows < I.n ? r0 + kGemv16Rows : I.n, 1);
 }
 
 // r = b - A x with FP64 vectors and FP64 accumulation on the complex64 matrix, partial norms.
@@ -450,8 +494,14 @@ struct Batch {
     std::vector<BatchAsmInst> asm_h;
     std::vector<double2*> rhs;  // per-instance right-hand side (pool_rhs)
     std::vector<BInst> h;
-    std::vector<int64_t> pre4, pre256, predot;
-    DevBuf asm_d, inst_d, pre4_d, pre256_d, predot_d, pre_asm;
+    std::vector<int64_t> pre4, pre16, pre256, predot;
+    DevBuf asm_d, inst_d, pre4_d, pre16_d, pre256_d, predot_d, pre_asm;
+    // Inner products on the complex64 matrices (SB_INNER_FP32) or on complex-half copies built
+    // after each assembly (SB_INNER_FP16; independent instances only).
+    int inner = SB_INNER_FP32;
+    bool half_valid = false;
+    DevBuf pool_half, pool_half_aux;
+    int graph_inner = -1;
     DevBuf pool_mat, pool_rhs, pool_f32, pool_f64, pool_small, pool_state;
     DevBuf gate;  // per group of kTensorRhsTile instances: any still in the Arnoldi cycle
     cudaStream_t stream = nullptr;
@@ -520,6 +570,46 @@ size_t state_bytes(int ni) {
 }  // namespace
 
 // Sizes the solver workspace of every instance for restart m and builds the descriptors.
+// Where instance b's complex-half copy and scale live in the batch's half pools (null before the
+// pools exist).
+static void half_pointers(const Batch& B, int b, BInst& I) {
+    I.lda16 = (B.nvec[b] + 3) / 4 * 4;
+    if (!B.pool_half.p) {
+        I.A16 = nullptr;
+        I.aux16 = nullptr;
+        return;
+    }
+    size_t off = 0;
+    for (int c = 0; c < b; ++c) off += round256(sizeof(uint32_t) * B.nvec[c] * ((B.nvec[c] + 3) / 4 * 4));
+    I.A16 = reinterpret_cast<const uint32_t*>(B.pool_half.as<char>() + off);
+    I.aux16 = B.pool_half_aux.as<unsigned>() + 4 * b;
+}
+
+// Builds the complex-half copies of every instance's complex64 matrix (after each assembly).
+static void batch_half_prepare(Batch& B) {
+    if (B.half_valid) return;
+    const int ni = B.ninst;
+    if (!B.pool_half.p) {
+        size_t bytes = 0;
+        for (int b = 0; b < ni; ++b) bytes += round256(sizeof(uint32_t) * B.nvec[b] * ((B.nvec[b] + 3) / 4 * 4));
+        B.pool_half.alloc(bytes);
+        B.pool_half_aux.alloc(sizeof(unsigned) * 4 * ni);
+        for (int b = 0; b < ni; ++b) half_pointers(B, b, B.h[b]);
+        h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
+    }
+    const cudaStream_t s = B.stream;
+    const BInst* I = B.inst_d.as<BInst>();
+    const unsigned g16 = static_cast<unsigned>(B.pre16.back());
+    ProfScope prof(SB_PROF_OTHER, s);
+    SB_CUDA(cudaMemsetAsync(B.pool_half_aux.p, 0, sizeof(unsigned) * 4 * ni, s));
+    k_bhalf_absmax<<<g16, kHalfThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni);
+    k_bhalf_scale<<<static_cast<unsigned>(cdiv64(ni, 64)), 64, 0, s>>>(I, ni);
+    k_bhalf_convert<<<g16, kHalfThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni);
+    for (int t = 0; t < 3; ++t) count_launch();
+    SB_CUDA(cudaGetLastError());
+    B.half_valid = true;
+}
+
 static void batch_workspace(Batch& B, int64_t m) {
     if (B.m == m) return;
     B.reset_graph();
@@ -582,6 +672,7 @@ static void batch_workspace(Batch& B, int64_t m) {
         }
     }
     B.pre4.assign(ni + 1, 0);
+    B.pre16.assign(ni + 1, 0);
     B.pre256.assign(ni + 1, 0);
     B.predot.assign(ni + 1, 0);
     for (int b = 0; b < ni; ++b) {
@@ -593,6 +684,7 @@ static void batch_workspace(Batch& B, int64_t m) {
         if (!shared) {
             I.A = B.asm_h[b].A32;
             I.lda = B.asm_h[b].lda32;
+            half_pointers(B, b, I);
             I.V = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * (m + 1) * ldv));
             I.vs = ldv;
             I.w = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
@@ -619,16 +711,19 @@ static void batch_workspace(Batch& B, int64_t m) {
         I.live = dv.live + b;
         I.brk = dv.brk + b;
         B.pre4[b + 1] = B.pre4[b] + cdiv64(n, kGemvRows);
+        B.pre16[b + 1] = B.pre16[b] + cdiv64(n, kGemv16Rows);
         B.pre256[b + 1] = B.pre256[b] + chunks;
         B.predot[b + 1] = B.predot[b] + cdiv64(n, (int64_t)kChunk * kDotSpan);
     }
     B.inst_d.alloc(sizeof(BInst) * ni);
     B.pre4_d.alloc(sizeof(int64_t) * (ni + 1));
+    B.pre16_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre256_d.alloc(sizeof(int64_t) * (ni + 1));
     B.predot_d.alloc(sizeof(int64_t) * (ni + 1));
     h2d_sync(B.predot_d.p, B.predot.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
     h2d_sync(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1));
+    h2d_sync(B.pre16_d.p, B.pre16.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.pre256_d.p, B.pre256.data(), sizeof(int64_t) * (ni + 1));
     B.m = m;
 }
@@ -652,6 +747,11 @@ static void batch_step(Batch& B, int j) {
         count_launch();
         tensor_block_product(*B.shared, B.v_all + (int64_t)j * ni * B.ld_all, B.ld_all, ni, B.w_all, B.ld_all, s,
                              B.gate.as<int>());
+    } else if (B.inner == SB_INNER_FP16) {
+        ProfScope prof(SB_PROF_GEMV16, s);
+        k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni, 0,
+                                                                                 j, G_ACTIVE);
+        count_launch();
     } else {
         ProfScope prof(SB_PROF_GEMV32, s);
         k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 0, j, G_ACTIVE);
@@ -680,7 +780,7 @@ static void batch_step(Batch& B, int j) {
 // One restart cycle of the whole batch: m Arnoldi steps captured once into a CUDA graph.
 static void batch_cycle(Batch& B) {
     const uint64_t gen = B.shared ? tensor_generation(*B.shared) : 0;
-    if (!B.exec || B.graph_prof != prof_key() || B.graph_gen != gen) {
+    if (!B.exec || B.graph_prof != prof_key() || B.graph_gen != gen || B.graph_inner != B.inner) {
         B.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&B.prof_pairs);
@@ -701,6 +801,7 @@ static void batch_cycle(Batch& B) {
         add_kernel_count(-B.graph_kernels);
         B.graph_prof = prof_key();
         B.graph_gen = gen;
+        B.graph_inner = B.inner;
     }
     SB_CUDA(cudaGraphLaunch(B.exec, B.stream));
     add_kernel_count(B.graph_kernels);
@@ -758,6 +859,7 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
         }
     } evg{e0, e1};
     SB_CUDA(cudaEventRecord(e0, s));
+    if (B.inner == SB_INNER_FP16) batch_half_prepare(B);
     for (int b = 0; b < ni; ++b) stats[b] = sb_gmres_stats{};
     // x = 0, r = b and ||b|| (with a zero initial guess the first residual needs no product).
     k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_B_TO_R, G_NONE);
@@ -845,6 +947,14 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
                     tensor_block_product(*B.shared, B.d_all, B.ld_all, ni, B.w_all, B.ld_all, s);
                     k_bresid_w<<<g256, kChunk, 0, s>>>(I, p256, ni, G_RESTART);
                     k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_RESTART);
+                    launched(2);
+                } else if (B.inner == SB_INNER_FP16) {
+                    {
+                        ProfScope prof(SB_PROF_GEMV16, s);
+                        k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(
+                            I, B.pre16_d.as<int64_t>(), ni, 1, 0, G_RESTART);
+                    }
+                    k_bsum_partials<<<ni, 32, 0, s>>>(I, B.pre16_d.as<int64_t>(), 2, G_RESTART);
                     launched(2);
                 } else {
                     {
@@ -1196,6 +1306,28 @@ SB_API int sb_batch_assemble(sb_batch* batch) {
         }
         B.asm_chosen = form;
         B.assembled = true;
+        B.half_valid = false;
+    });
+}
+
+SB_API int sb_batch_set_inner_precision(sb_batch* batch, int inner) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null argument");
+        SB_REQUIRE(inner == SB_INNER_FP32 || inner == SB_INNER_FP16, SB_ERR_INVALID_ARGUMENT,
+                   "inner precision must be SB_INNER_FP32 or SB_INNER_FP16");
+        Batch& B = *batch->b;
+        B.inner = inner;
+        if (inner == SB_INNER_FP32 && B.pool_half.p) {
+            // Drop the copies and the instance descriptors' pointers to them.
+            B.pool_half.release();
+            B.pool_half_aux.release();
+            B.half_valid = false;
+            if (!B.h.empty()) {
+                SB_CUDA(cudaSetDevice(B.device));
+                for (int b = 0; b < B.ninst; ++b) half_pointers(B, b, B.h[b]);
+                h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * B.ninst);
+            }
+        }
     });
 }
 

@@ -70,6 +70,11 @@ class SweepBatch:
         check(L.load().sb_batch_assembly_tuning(self.handle, ct.byref(c), ct.byref(a), ct.byref(b)))
         return c.value, a.value, b.value
 
+    def set_inner_precision(self, inner: int) -> None:
+        """SB_INNER_FP32 (the complex64 matrices) or SB_INNER_FP16 (complex-half copies, built by
+        the first solve after each assembly; pair with IrConfig(inner_tolerance=1e-3))."""
+        check(L.load().sb_batch_set_inner_precision(self.handle, int(inner)))
+
     def set_rhs_plane_wave(self, direction=(0.0, 0.0, 1.0)) -> None:
         d = np.ascontiguousarray(direction, np.float64)
         check(L.load().sb_batch_set_rhs_plane_wave(self.handle, _p(d)))

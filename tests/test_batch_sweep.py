@@ -234,3 +234,65 @@ def test_sequential_sweep_warm_start(gpu, oracle):
     x = gpu.gmres(op, b, gpu.GmresConfig(max_iterations=200, restart=30, tolerance=1e-10)).x
     assert np.linalg.norm(warm.solutions[3] - x) / np.linalg.norm(x) < 1e-7
     op.close()
+
+
+def test_batch_half_inner_matches_single_instance(gpu, oracle):
+    """SB_INNER_FP16 on a batch: every instance's solution equals the single-instance FP16-inner
+    solve of the same complex64 matrix (same algorithm per instance) and the batch's own FP32-inner
+    solution to the solver tolerance; the copies are rebuilt after a re-assembly; restarts inside
+    the inner solves (inner_restart 8, inner tolerance 1e-5) take the residual on the half copies; an odd size covers
+    the column tail."""
+    from sonium_b200.sweep import SweepBatch
+
+    meshes, phys, betas = _instances(gpu, oracle, SPEC)
+    nodes, tris = oracle.icosphere(1.0, 2, (1.0, 0.6, 0.4))
+    meshes.append(gpu.Mesh(nodes, tris[:-1]))
+    ph = gpu.PhysicsParams.for_wavenumber(1.7)
+    phys.append(ph)
+    betas.append(ph.burton_miller_beta())
+    batch = SweepBatch(meshes, phys, betas)
+    batch.assemble()
+    batch.set_rhs_plane_wave([0.0, 0.0, 1.0])
+    cfg32 = gpu.IrConfig(tolerance=1e-8)
+    s32 = batch.solve(cfg32)
+    x32 = [batch.solution(i) for i in range(len(batch))]
+    batch.set_inner_precision(gpu.SB_INNER_FP16)
+    for cfg16 in (gpu.IrConfig(tolerance=1e-8, inner_tolerance=1e-3),
+                  gpu.IrConfig(tolerance=1e-8, inner_tolerance=1e-5, inner_restart=8)):
+        s16 = batch.solve(cfg16)
+        for i, (m, ph_i, be) in enumerate(zip(meshes, phys, betas)):
+            x = batch.solution(i)
+            assert s16[i].converged and s16[i].residual < 1e-8, (i, s16[i])
+            assert np.linalg.norm(x - x32[i]) / np.linalg.norm(x32[i]) < 1e-6, i
+        if cfg16.inner_restart == 8:  # inner solves to 1e-5 need more than 8 steps
+            assert sum(st.restarts for st in s16) > 0
+        # single-instance FP16-inner solve of instance 4: the same iterations within rounding noise
+        m, ph_i, be = meshes[4], phys[4], betas[4]
+        b = gpu.rhs_plane_wave(m, ph_i, be, [0, 0, 1])[:, 0]
+        op = gpu.build_tbem_system_with_beta(m, ph_i, be, precision=gpu.SB_PRECISION_FP32)
+        op.set_inner_precision(gpu.SB_INNER_FP16)
+        single = gpu.gmres_mixed(op, b, cfg16)
+        assert abs(s16[4].iterations - single.iterations) <= max(2, single.iterations // 10)
+        assert np.linalg.norm(batch.solution(4) - single.x) / np.linalg.norm(single.x) < 1e-6
+        op.close()
+    # re-assembly at other wavenumbers: the half copies follow the new matrices
+    phys2 = [gpu.PhysicsParams.for_wavenumber(0.9 * p.wave_number) for p in phys]
+    betas2 = [p.burton_miller_beta() for p in phys2]
+    batch.close()
+    batch = SweepBatch(meshes, phys2, betas2)
+    batch.set_inner_precision(gpu.SB_INNER_FP16)
+    batch.assemble()
+    batch.set_rhs_plane_wave([1.0, 0.0, 0.0])
+    a = batch.solve(gpu.IrConfig(tolerance=1e-8, inner_tolerance=1e-3))
+    xa = [batch.solution(i) for i in range(len(batch))]
+    batch.assemble()  # same matrices again: the copies are rebuilt and the answers repeat
+    b2 = batch.solve(gpu.IrConfig(tolerance=1e-8, inner_tolerance=1e-3))
+    assert [s.iterations for s in a] == [s.iterations for s in b2]
+    assert all(np.array_equal(batch.solution(i), xa[i]) for i in range(len(batch)))
+    batch.set_inner_precision(gpu.SB_INNER_FP32)
+    c = batch.solve(gpu.IrConfig(tolerance=1e-8))
+    assert all(s.converged for s in c)
+    assert all(np.linalg.norm(batch.solution(i) - xa[i]) / np.linalg.norm(xa[i]) < 1e-6 for i in range(len(batch)))
+    with pytest.raises(gpu.SoniumError):
+        batch.set_inner_precision(5)
+    batch.close()
