@@ -621,6 +621,64 @@ __device__ __forceinline__ void sincos_f32(float x, float* so, float* co) {
 
 constexpr int kFar32Rows = 64;
 
+// Packed FP32 pairs: sm_100 executes one f32x2 add / multiply / fma for two lanes in one issue
+// slot, so the far field evaluates two quadrature points per instruction (points 2p, 2p + 1 in
+// the .x / .y lanes of pair p; the 13th point runs alone).
+constexpr int kFarPairs = kFarPoints / 2;
+// Resident CTAs per SM of the FP32 far kernel: the packed loop keeps the column's 13 points, the
+// broadcast row terms and the lane sums in 168 registers without spills at 3 CTAs (measured at
+// N = 20480: 11.16 ms; 4 CTAs with spills 11.23 ms, 2 CTAs 12.24 ms).
+constexpr int kFar32MinBlocks = 3;
+static_assert(kFarPoints == 2 * kFarPairs + 1, "the packed far loop pairs all points but the last");
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Channel sums of one far pair in the pair-phase frame (see far32_tile).
+struct Far32Sums {
+    float gr, gi, hr, hi, tr, ti, er, ei;
+};
+
+// One quadrature point of a far pair, scalar (the point left over by the packed pairs).
+__device__ __forceinline__ void far32_point(Far32Sums& a, float px, float py, float pz, float pd, float pw, float pn,
+                                            float fx, float fy, float fz, float rc2f, float rcf, float kf, float k2f,
+                                            float fny, float fnx, float nxx, float nxy, float nxz, float nxny) {
+    const float num = fmaf(2.f, fx * px + fy * py + fz * pz, pd);
+    const float rq2 = rc2f + num;
+    const float rinv = rsqrtf(rq2);
+    const float t = kf * __fdividef(num, fmaf(rq2, rinv, rcf));
+    float st, ct;
+    if (fabsf(t) <= 3.14159265f) {
+        __sincosf(t, &st, &ct);
+    } else {
+        sincos_f32(t, &st, &ct);
+    }
+    const float gs = pw * rinv;
+    const float g_r = ct * gs, g_i = st * gs;
+    const float rny = (fny + pn) * rinv;
+    const float rnx = (fnx - (px * nxx + py * nxy + pz * nxz)) * rinv;
+    const float b_r = -fmaf(g_r, rinv, g_i * kf);
+    const float b_i = fmaf(g_r, kf, -g_i * rinv);
+    a.gr += g_r;
+    a.gi += g_i;
+    a.hr = fmaf(b_r, rny, a.hr);
+    a.hi = fmaf(b_i, rny, a.hi);
+    a.tr = fmaf(b_r, rnx, a.tr);
+    a.ti = fmaf(b_i, rnx, a.ti);
+    const float rqq = rny * rnx;
+    const float s3 = fmaf(3.f, rqq, nxny);
+    const float f_r = fmaf(rinv * rinv, s3, -k2f * rqq);
+    const float f_i = -kf * rinv * s3;
+    a.er = fmaf(g_r, f_r, fmaf(-g_i, f_i, a.er));
+    a.ei = fmaf(g_r, f_i, fmaf(g_i, f_r, a.ei));
+}
+
 // One (128-column tile, 64-row block) of the FP32 far field; all 128 threads of the CTA call it.
 template <bool kWithRhs>
 __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const double* __restrict__ elem,
@@ -641,20 +699,31 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
         sx[r][c] = (i < n) ? E(ECX + c, i) : 0.0;
         snx[r][c] = (i < n) ? static_cast<float>(E(ENX + c, i)) : 0.f;
     }
-    // The column's 13 points in registers.
-    float px[kFarPoints], py[kFarPoints], pz[kFarPoints], pd[kFarPoints], pw[kFarPoints], pn[kFarPoints];
+    // The column's 13 points in registers: points 2p, 2p + 1 in the lanes of pair p, the 13th alone.
+    float2 PX[kFarPairs], PY[kFarPairs], PZ[kFarPairs], PD[kFarPairs], PW[kFarPairs], PN[kFarPairs];
+    float lx, ly, lz, ld_, lw, ln;
     double cx = 0, cy = 0, cz = 0;
     float nyx = 0, nyy = 0, nyz = 0;
     const int64_t jj = j < n ? j : 0;
 #pragma unroll
-    for (int q = 0; q < kFarPoints; ++q) {
-        const float* src = qp32 + (int64_t)(q * kQ32) * ld + jj;
-        px[q] = src[0];
-        py[q] = src[ld];
-        pz[q] = src[2 * ld];
-        pd[q] = src[3 * ld];
-        pw[q] = src[4 * ld];
-        pn[q] = src[5 * ld];
+    for (int p = 0; p < kFarPairs; ++p) {
+        const float* s0 = qp32 + (int64_t)(2 * p * kQ32) * ld + jj;
+        const float* s1 = s0 + (int64_t)kQ32 * ld;
+        PX[p] = make_float2(s0[0], s1[0]);
+        PY[p] = make_float2(s0[ld], s1[ld]);
+        PZ[p] = make_float2(s0[2 * ld], s1[2 * ld]);
+        PD[p] = make_float2(s0[3 * ld], s1[3 * ld]);
+        PW[p] = make_float2(s0[4 * ld], s1[4 * ld]);
+        PN[p] = make_float2(s0[5 * ld], s1[5 * ld]);
+    }
+    {
+        const float* sl = qp32 + (int64_t)((kFarPoints - 1) * kQ32) * ld + jj;
+        lx = sl[0];
+        ly = sl[ld];
+        lz = sl[2 * ld];
+        ld_ = sl[3 * ld];
+        lw = sl[4 * ld];
+        ln = sl[5 * ld];
     }
     if (j < n) {
         cx = E(ECX, j); cy = E(ECY, j); cz = E(ECZ, j);
@@ -696,46 +765,62 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             const float nxny = nxx * nyx + nxy * nyy + nxz * nyz;
             const float fny = fx * nyx + fy * nyy + fz * nyz;       // d_c . n_y
             const float fnx = -(fx * nxx + fy * nxy + fz * nxz);    // -d_c . n_x
-            float ag_r = 0.f, ag_i = 0.f, ah_r = 0.f, ah_i = 0.f, at_r = 0.f, at_i = 0.f, ae_r = 0.f, ae_i = 0.f;
+            // Points in pairs: lane sums AGR = sum g_r, NAHR = -sum b_r r.n_y, NATR = -sum b_r (-r.n_x),
+            // AER - AEX = sum (g_r f_r - g_i f_i), with b = g (-1/r + i k) and the E factor f below.
+            const float2 FX = bc2(fx), FY = bc2(fy), FZ = bc2(fz), RC2 = bc2(rc2f), RC = bc2(rcf), KK = bc2(kf);
+            const float2 FNY = bc2(fny), FNX = bc2(fnx), NXX = bc2(nxx), NXY = bc2(nxy), NXZ = bc2(nxz);
+            const float2 NXNY = bc2(nxny), NK2 = bc2(-k2f), NK = bc2(-kf), M1 = bc2(-1.f);
+            const float2 Z = bc2(0.f);
+            float2 AGR = Z, AGI = Z, NAHR = Z, AHI = Z, NATR = Z, ATI = Z, AER = Z, AEX = Z, AEI = Z;
 #pragma unroll
-            for (int q = 0; q < kFarPoints; ++q) {
-                const float num = fmaf(2.f, fx * px[q] + fy * py[q] + fz * pz[q], pd[q]);
-                const float rq2 = rc2f + num;
-                const float rinv = rsqrtf(rq2);
-                const float t = kf * __fdividef(num, fmaf(rq2, rinv, rcf));
-                float st, ct;
-                // Every resolved mesh keeps the phase offset t = k (r_q - r_c) within one element
-                // size (|t| <= pi): the special-function unit's sine / cosine (documented absolute
-                // error 2^-21.4 on [-pi, pi], below the FP32 rounding of the sums) cost two issue
-                // slots instead of a polynomial; larger offsets take the quadrant-reduced version.
-                if (fabsf(t) <= 3.14159265f) {
-                    __sincosf(t, &st, &ct);
+            for (int p = 0; p < kFarPairs; ++p) {
+                float2 d = pmul(FX, PX[p]);
+                d = pfma(FY, PY[p], d);
+                d = pfma(FZ, PZ[p], d);
+                const float2 num = pfma(bc2(2.f), d, PD[p]);
+                const float2 rq2 = padd(RC2, num);
+                const float2 rinv = make_float2(rsqrtf(rq2.x), rsqrtf(rq2.y));
+                const float2 den = pfma(rq2, rinv, RC);
+                const float2 t = pmul(KK, pmul(num, make_float2(rcp_approx(den.x), rcp_approx(den.y))));
+                // Special-function sine / cosine while both phase offsets are within one element
+                // size (|t| <= pi, every resolved mesh), else the quadrant-reduced version.
+                float2 S, C;
+                if (fmaxf(fabsf(t.x), fabsf(t.y)) <= 3.14159265f) {
+                    __sincosf(t.x, &S.x, &C.x);
+                    __sincosf(t.y, &S.y, &C.y);
                 } else {
-                    sincos_f32(t, &st, &ct);
+                    sincos_f32(t.x, &S.x, &C.x);
+                    sincos_f32(t.y, &S.y, &C.y);
                 }
-                // The pair phase exp(i k r_c) is common to all points: the channel sums are
-                // accumulated in its frame and rotated once after the loop.
-                const float gs = pw[q] * rinv;
-                const float g_r = ct * gs, g_i = st * gs;
-                // r_hat . n_y and -r_hat . n_x from per-pair and per-point dot products
-                const float rny = (fny + pn[q]) * rinv;
-                const float rnx = (fnx - (px[q] * nxx + py[q] * nxy + pz[q] * nxz)) * rinv;
-                const float b_r = -fmaf(g_r, rinv, g_i * kf);
-                const float b_i = fmaf(g_r, kf, -g_i * rinv);
-                ag_r += g_r;
-                ag_i += g_i;
-                ah_r = fmaf(b_r, rny, ah_r);
-                ah_i = fmaf(b_i, rny, ah_i);
-                at_r = fmaf(b_r, rnx, at_r);
-                at_i = fmaf(b_i, rnx, at_i);
-                // E factor: ((3/r^2 - k^2) rq + nx.ny / r^2, -(k / r) (3 rq + nx.ny))
-                const float rqq = rny * rnx;
-                const float s3 = fmaf(3.f, rqq, nxny);
-                const float f_r = fmaf(rinv * rinv, s3, -k2f * rqq);
-                const float f_i = -kf * rinv * s3;
-                ae_r = fmaf(g_r, f_r, fmaf(-g_i, f_i, ae_r));
-                ae_i = fmaf(g_r, f_i, fmaf(g_i, f_r, ae_i));
+                const float2 gs = pmul(PW[p], rinv);
+                const float2 gr = pmul(C, gs), gi = pmul(S, gs);
+                const float2 rny = pmul(padd(FNY, PN[p]), rinv);
+                float2 pnx = pmul(PX[p], NXX);
+                pnx = pfma(PY[p], NXY, pnx);
+                pnx = pfma(PZ[p], NXZ, pnx);
+                const float2 rnx = pmul(pfma(pnx, M1, FNX), rinv);
+                const float2 u = pfma(gr, rinv, pmul(gi, KK));           // -b_r
+                const float2 bi = pfma(gi, pmul(rinv, M1), pmul(gr, KK));  // b_i
+                AGR = padd(AGR, gr);
+                AGI = padd(AGI, gi);
+                NAHR = pfma(u, rny, NAHR);
+                AHI = pfma(bi, rny, AHI);
+                NATR = pfma(u, rnx, NATR);
+                ATI = pfma(bi, rnx, ATI);
+                // E factor: f = ((3/r^2 - k^2) rq + nx.ny / r^2, -(k / r) (3 rq + nx.ny))
+                const float2 rqq = pmul(rny, rnx);
+                const float2 s3 = pfma(bc2(3.f), rqq, NXNY);
+                const float2 fr = pfma(pmul(rinv, rinv), s3, pmul(NK2, rqq));
+                const float2 fi = pmul(pmul(NK, rinv), s3);
+                AER = pfma(gr, fr, AER);
+                AEX = pfma(gi, fi, AEX);
+                AEI = pfma(gr, fi, pfma(gi, fr, AEI));
             }
+            Far32Sums sm{AGR.x + AGR.y, AGI.x + AGI.y, -(NAHR.x + NAHR.y), AHI.x + AHI.y, -(NATR.x + NATR.y),
+                         ATI.x + ATI.y, (AER.x + AER.y) - (AEX.x + AEX.y), AEI.x + AEI.y};
+            far32_point(sm, lx, ly, lz, ld_, lw, ln, fx, fy, fz, rc2f, rcf, kf, k2f, fny, fnx, nxx, nxy, nxz, nxny);
+            const float ag_r = sm.gr, ag_i = sm.gi, ah_r = sm.hr, ah_i = sm.hi, at_r = sm.tr, at_i = sm.ti,
+                        ae_r = sm.er, ae_i = sm.ei;
             const float cgr = scf[0][tid], cgi = scf[1][tid], chr = scf[2][tid], chi = scf[3][tid];
             const float ctr = scf[4][tid], cti = scf[5][tid], cer = scf[6][tid], cei = scf[7][tid];
             const float ur = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
@@ -772,7 +857,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
 }
 
 template <bool kWithRhs>
-__global__ void __launch_bounds__(kFarTile, 4) k_far32(const float* __restrict__ qp32,
+__global__ void __launch_bounds__(kFarTile, kFar32MinBlocks) k_far32(const float* __restrict__ qp32,
                                                     const double* __restrict__ elem, int64_t n,
                                                     int64_t ld, const double* __restrict__ coef,
                                                     double k, float2* __restrict__ A32, int64_t lda32,
