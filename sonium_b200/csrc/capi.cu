@@ -630,6 +630,7 @@ SB_API int sb_operator_destroy(sb_operator* op) {
             destroy_solve_work(*op->op);
             multi_release(*op->op);
             tensor_release(*op->op);
+            op->op->side.release();
             if (op->op->stream) cudaStreamDestroy(op->op->stream);
             delete op->op;
         }

@@ -176,6 +176,10 @@ struct Operator {
     // entries apart; half_aux holds the largest part's bits, the scale and its inverse (device).
     int inner = SB_INNER_FP32;
     DevBuf A16, half_aux;
+    // Near-pair and self kernels of the constant-basis Tri3 assembly run here, concurrently with
+    // the far kernel (they write disjoint entries; the far kernel is FMA / special-function bound,
+    // the near kernel FP64 and latency bound).
+    SideStream side;
     int64_t lda16 = 0;
     bool half_valid = false;
     cudaStream_t stream = nullptr;
