@@ -8,8 +8,9 @@ solve: re-assembly of the dense system on the device, the incident right-hand si
                 one (`headline_mode`): FP32 assembly (FP64 phase, near and self terms) and FP64
                 refinement to 1e-8 around an inner GMRES(50) with FP32 vectors, on the complex64
                 matrix (`mixed`, inner tolerance 1e-5) or on its power-of-two-scaled complex-half
-                copy (`mixed_half`, inner tolerance 1e-3); `mixed_fp64_matrix` refines on the
-                complex128 matrix. Inputs resident in HBM, device time by CUDA events on the
+                copy (`mixed_half`, inner tolerance 1e-3), the latter also with a block-Jacobi
+                right preconditioner of the inner solve (`mixed_half_bj`, blocks of 64 spatially
+                close elements); `mixed_fp64_matrix` refines on the complex128 matrix. Inputs resident in HBM, device time by CUDA events on the
                 operator's stream; every mode's error against the plain FP64 solution is reported.
   * `plain_fp64` -- the same solve with complex128 only and FP64 GMRES(50) to 1e-8.
   * `e2e`    -- the headline form through the C ABI with host buffers: mesh upload, assembly,
@@ -274,6 +275,7 @@ def reference_arm(a, dist: Dist):
 # ---------------------------------------------------------------------------------------------
 MODES = {
     # name: (assembly precision, solver)
+    "mixed_half_bj": ("SB_PRECISION_FP32", "ir16bj"),
     "mixed_half": ("SB_PRECISION_FP32", "ir16"),
     "mixed": ("SB_PRECISION_FP32", "ir"),
     "mixed_fp64_matrix": ("SB_PRECISION_FP64_FP32", "ir"),
@@ -287,7 +289,9 @@ HALF_INNER_TOL = 1e-3
 GEMV16_TRAFFIC_PER_ENTRY = 4.13
 # Modes that may carry the headline (fastest first when both meet the accuracy bar), with the
 # kernel class of their dominant matrix-vector product.
-HEADLINE_MODES = {"mixed_half": "SB_PROF_GEMV16", "mixed": "SB_PROF_GEMV32"}
+HEADLINE_MODES = {"mixed_half_bj": "SB_PROF_GEMV16", "mixed_half": "SB_PROF_GEMV16", "mixed": "SB_PROF_GEMV32"}
+# Block size of the block-Jacobi inner preconditioner of the `mixed_half_bj` form.
+BJ_BLOCK = 64
 
 
 def main():
@@ -340,8 +344,8 @@ def main():
         def step():
             L.check(lib.sb_assemble_into(op.handle, ct.byref(phys), bta))
             L.check(lib.sb_rhs_plane_wave_device(op.handle, dirs.ctypes.data, None, 1, b_d))
-            if solver in ("ir", "ir16"):
-                cfg = ir16 if solver == "ir16" else ir
+            if solver in ("ir", "ir16", "ir16bj"):
+                cfg = ir if solver == "ir" else ir16
                 L.check(lib.sb_gmres_mixed_device(op.handle, b_d, x_d, 0, ct.byref(cfg), ct.byref(st)))
             else:
                 L.check(lib.sb_gmres_device(op.handle, b_d, x_d, 0, ct.byref(gc), 0, ct.byref(st)))
@@ -362,11 +366,13 @@ def main():
 
     results, x_ref = {}, None
     live = {}  # per headline-capable mode: (live profile, class breakdown, clocks, launches)
-    for name in ("plain_fp64", "mixed_fp64_matrix", "mixed", "mixed_half"):
+    for name in ("plain_fp64", "mixed_fp64_matrix", "mixed", "mixed_half", "mixed_half_bj"):
         prec, solver = MODES[name]
         op = sb.build_tbem_system_with_beta(mesh, ph, beta, getattr(sb, prec))
-        if solver == "ir16":
+        if solver in ("ir16", "ir16bj"):
             op.set_inner_precision(sb.SB_INNER_FP16)
+        if solver == "ir16bj":
+            op.set_inner_preconditioner(sb.SB_INNER_PRECOND_BLOCK_JACOBI, BJ_BLOCK)
         step = make_step(op, solver)
         s0 = step()  # untimed: solution for the accuracy check
         x = _to_host(rt, x_d, n)
@@ -410,8 +416,10 @@ def main():
             "iterations": int(s0.iterations), "matvecs": int(s0.matvecs), "matvecs_fp32": int(s0.matvecs_fp32),
             "refinements": int(s0.refinements), "residual": s0.residual,
         }
-        if solver == "ir16":
+        if solver in ("ir16", "ir16bj"):
             results[name]["inner"] = "complex-half matrix, inner tolerance %g" % HALF_INNER_TOL
+        if solver == "ir16bj":
+            results[name]["inner"] += ", block-Jacobi right preconditioner (blocks of %d)" % BJ_BLOCK
         op.close()
     # Headline: the fastest mixed form whose solution is within 1e-5 of the FP64 one.
     ok = [m for m in HEADLINE_MODES if results[m]["error_vs_fp64"] <= 1e-5]
@@ -429,11 +437,13 @@ def main():
             t0 = time.perf_counter()
             m2 = sb.Mesh(nodes, tris, device=dev)
             o2 = sb.build_tbem_system_with_beta(m2, ph, beta, sb.SB_PRECISION_FP32)
-            if head_mode == "mixed_half":
+            if head_mode in ("mixed_half", "mixed_half_bj"):
                 o2.set_inner_precision(sb.SB_INNER_FP16)
+            if head_mode == "mixed_half_bj":
+                o2.set_inner_preconditioner(sb.SB_INNER_PRECOND_BLOCK_JACOBI, BJ_BLOCK)
             bh = sb.rhs_plane_wave(m2, ph, beta, dirs)[:, 0]
             sb.gmres_mixed(o2, bh, sb.IrConfig(20, TOL, RESTART, 20,
-                                               HALF_INNER_TOL if head_mode == "mixed_half" else 1e-5))
+                                               1e-5 if head_mode == "mixed" else HALF_INNER_TOL))
             o2.close()
             m2.close()
             rt.cudaDeviceSynchronize()
@@ -446,7 +456,9 @@ def main():
         e2e = {"value": dist.world * len(ts) / sum(ts), "unit": "solves/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "path": "sb_mesh_create + sb_assemble(SB_PRECISION_FP32) + "
-                       + ("sb_operator_set_inner_precision(SB_INNER_FP16) + " if head_mode == "mixed_half" else "")
+                       + ("sb_operator_set_inner_precision(SB_INNER_FP16) + " if head_mode != "mixed" else "")
+                       + ("sb_operator_set_inner_preconditioner(SB_INNER_PRECOND_BLOCK_JACOBI, %d) + " % BJ_BLOCK
+                          if head_mode == "mixed_half_bj" else "")
                        + "sb_rhs_plane_wave + sb_gmres_mixed (host buffers), wall clock"}
 
     # ---- batched frequency sweep ----
@@ -470,7 +482,7 @@ def main():
     # complex128: 16 N^2
     bytes_mv = {"gemv16": 4.0 * n * n + 16.0 * n, "gemv32": 8.0 * n * n + 16.0 * n,
                 "gemv64": 16.0 * n * n + 32.0 * n}
-    hbm_kind = "gemv16" if head_mode == "mixed_half" else "gemv32"
+    hbm_kind = "gemv32" if head_mode == "mixed" else "gemv16"
     hbm_cls = getattr(L, HEADLINE_MODES[head_mode])
     # average working launch of the matvec, from the events recorded inside the timed region
     live_ms = prof_live.ms[hbm_cls]
@@ -494,10 +506,21 @@ def main():
             "dominant_kernel_class": dominant}
     evals = 13.0 * n * (n - 1)
     far_avg = ms["far"] / max(launches["far"], 1) / 1e3
+    # Far-field roofline in the assembly convention: 90 FP64-equivalent flops per point
+    # evaluation (sincos, sqrt and reciprocals not counted). The FP32 far kernel has no measured
+    # peak to divide by: the nominal FP32 FMA rate of the part at its maximum SM clock stands in.
+    fp32_nominal = 148 * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    far_tflops = 90.0 * evals / far_avg / 1e12
     assembly = {"far_kernel_ms": far_avg * 1e3, "far_evals_per_s": evals / far_avg,
                 "near_kernel_ms": ms["near"] / max(launches["near"], 1),
                 "self_kernel_ms": ms["self"] / max(launches["self"], 1),
-                "share_of_kernel_time": (ms["far"] + ms["near"] + ms["self"]) / max(total_ms, 1e-9)}
+                "share_of_kernel_time": (ms["far"] + ms["near"] + ms["self"]) / max(total_ms, 1e-9),
+                "far_roofline": {"kernel": "k_far32 (FP32 far field, FP64 phase, packed f32x2)",
+                                 "bound": "FP32 FMA pipe + special-function unit",
+                                 "achieved": far_tflops, "unit": "TFLOP/s (90 FP64-equivalent flop per evaluation)",
+                                 "peak": fp32_nominal, "frac": far_tflops / fp32_nominal,
+                                 "peak_source": "nominal FP32 FMA rate, 148 SMs x 128 lanes x 2 flop x max SM "
+                                                "clock (no measured FP32 peak)"}}
 
     cpu = None
     if not a.no_cpu and dist.rank == 0:
@@ -511,8 +534,9 @@ def main():
         "data": "synthetic (icosphere geometry, analytic incident plane wave)",
         "config": {"workload": f"rigid sphere icosphere L{a.level} (N={n}), k={a.k}, beta=i/k, plane wave +z; "
                                f"one step = assembly + RHS + GMRES({RESTART}) inner solve on the "
-                               f"{'complex-half' if head_mode == 'mixed_half' else 'complex64'} matrix with FP32 "
-                               f"vectors / FP64-refined on the complex64 matrix to rtol {TOL}",
+                               f"{'complex64' if head_mode == 'mixed' else 'complex-half'} matrix with FP32 "
+                               f"vectors{' and block-Jacobi right preconditioning' if head_mode == 'mixed_half_bj' else ''}"
+                               f" / FP64-refined on the complex64 matrix to rtol {TOL}",
                    "N": n, "l2": "inputs larger than L2 (complex64 matrix %.1f GB)" % (8 * n * n / 1e9),
                    "parallelism": f"replicas x{dist.world}"},
         "headline_mode": head_mode,
@@ -823,11 +847,13 @@ def single_solves(sb, level, k, dev, modes=None):
     beta = ph.burton_miller_beta()
     mesh = sb.Mesh(nodes, tris, device=dev)
     b = sb.rhs_plane_wave(mesh, ph, beta, [0.0, 0.0, 1.0])[:, 0]
-    for name in (modes or ("mixed", "mixed_half", "plain_fp64")):
+    for name in (modes or ("mixed", "mixed_half", "mixed_half_bj", "plain_fp64")):
         prec, solver = MODES[name]
         op = sb.build_tbem_system_with_beta(mesh, ph, beta, getattr(sb, prec))
-        if solver == "ir16":
+        if solver in ("ir16", "ir16bj"):
             op.set_inner_precision(sb.SB_INNER_FP16)
+            if solver == "ir16bj":
+                op.set_inner_preconditioner(sb.SB_INNER_PRECOND_BLOCK_JACOBI, BJ_BLOCK)
             s = sb.gmres_mixed(op, b, sb.IrConfig(20, TOL, RESTART, 20, HALF_INNER_TOL))
         elif solver == "ir":
             s = sb.gmres_mixed(op, b, sb.IrConfig(20, TOL, RESTART, 20, 1e-5))

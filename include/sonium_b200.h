@@ -301,6 +301,19 @@ SB_API int sb_gmres_mixed(const sb_operator* op, const sb_complex* b, const sb_c
 #define SB_INNER_FP32 0
 #define SB_INNER_FP16 1
 SB_API int sb_operator_set_inner_precision(sb_operator* op, int inner);
+/* Right preconditioner of sb_gmres_mixed's inner GMRES (no reference counterpart: an inner-solver
+ * choice of this library; the reference's preconditioner interface is Preconditioner::apply_into,
+ * crates/sonium-solvers/crates/sonium-solvers-core/src/traits.rs:3645). SB_INNER_PRECOND_NONE
+ * (default) or SB_INNER_PRECOND_BLOCK_JACOBI: the unknowns in blocks of block_size (32, 64 or 128)
+ * spatially close elements (consecutive in the Morton order of the element centroids; index
+ * order for an operator without a mesh or with a discontinuous basis), each diagonal block of the
+ * complex64 matrix inverted on the device (Gauss-Jordan with partial pivoting, FP32; a singular
+ * block keeps the identity) on the first mixed solve after each assembly. The inner solve works
+ * on A M^-1 and the correction is M^-1 y, so the outer refinement and the converged solution are
+ * unchanged; fewer inner iterations are needed. Needs a complex64 matrix. */
+#define SB_INNER_PRECOND_NONE 0
+#define SB_INNER_PRECOND_BLOCK_JACOBI 1
+SB_API int sb_operator_set_inner_preconditioner(sb_operator* op, int kind, int block_size);
 SB_API int sb_gmres_mixed_device(const sb_operator* op, const sb_complex* b_dev,
                                  sb_complex* x_dev, int x0_given, const sb_ir_config* cfg,
                                  sb_gmres_stats* stats);

@@ -26,6 +26,8 @@ SB_PRECISION_FP64_FP32 = 1
 SB_PRECISION_FP32 = 2
 SB_INNER_FP32 = 0
 SB_INNER_FP16 = 1
+SB_INNER_PRECOND_NONE = 0
+SB_INNER_PRECOND_BLOCK_JACOBI = 1
 SB_OP_N, SB_OP_T, SB_OP_C = 0, 1, 2
 SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI = 0, 1
 SB_BC_VELOCITY, SB_BC_PRESSURE = 0, 1
@@ -146,6 +148,7 @@ _SIGNATURES = {
     "sb_gmres_mixed": ([P, P, P, ct.POINTER(SbIrConfig), P, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_mixed_device": ([P, P, P, ct.c_int, ct.POINTER(SbIrConfig), ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_operator_set_inner_precision": ([P, ct.c_int], ct.c_int),
+    "sb_operator_set_inner_preconditioner": ([P, ct.c_int, ct.c_int], ct.c_int),
     "sb_rhs_plane_wave_device": ([P, P, P, ct.c_int64, P], ct.c_int),
     "sb_gcro_subspace_create": ([ct.c_int, ct.c_int64, ct.POINTER(P)], ct.c_int),
     "sb_gcro_subspace_destroy": ([P], ct.c_int),

@@ -503,6 +503,7 @@ SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_compl
         check_beta(beta);
         tensor_release(*op->op);
         op->op->half_valid = false;
+        op->op->bj_valid = false;
         if (op->op->basis != SB_BASIS_CONSTANT)
             assemble_discontinuous(*op->op, *physics, beta.re, beta.im);
         else
@@ -1035,6 +1036,28 @@ SB_API int sb_operator_set_inner_precision(sb_operator* op, int inner) {
             op->op->A16.release();
             op->op->half_valid = false;
         }
+    });
+}
+
+SB_API int sb_operator_set_inner_preconditioner(sb_operator* op, int kind, int block_size) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op, SB_ERR_INVALID_ARGUMENT, "null argument");
+        SB_REQUIRE(kind == SB_INNER_PRECOND_NONE || kind == SB_INNER_PRECOND_BLOCK_JACOBI, SB_ERR_INVALID_ARGUMENT,
+                   "inner preconditioner must be SB_INNER_PRECOND_NONE or SB_INNER_PRECOND_BLOCK_JACOBI");
+        Operator& o = *op->op;
+        if (kind == SB_INNER_PRECOND_BLOCK_JACOBI) {
+            SB_REQUIRE(block_size == 32 || block_size == 64 || block_size == 128, SB_ERR_INVALID_ARGUMENT,
+                       "block_size must be 32, 64 or 128");
+            SB_REQUIRE(o.A32.p, SB_ERR_INVALID_ARGUMENT,
+                       "the block-Jacobi inner preconditioner needs a complex64 matrix (SB_PRECISION_FP64_FP32 or "
+                       "SB_PRECISION_FP32)");
+            if (block_size != o.bj_size) o.bj_valid = false;
+            o.bj_size = block_size;
+        } else {
+            o.bj_inv.release();
+            o.bj_valid = false;
+        }
+        o.inner_precond = kind;
     });
 }
 

@@ -74,6 +74,8 @@ struct KrylovWork {
     cudaGraphExec_t exec = nullptr;
     const void* key_A = nullptr;
     const void* key_jac = nullptr;  // the Jacobi diagonal the cycle reads, if any
+    const void* key_pre = nullptr;  // the block-Jacobi inverses the cycle reads, if any
+    int key_pre_bs = 0;
     int key_jacobi = -1;
     unsigned key_prof = 0;
     std::vector<ProfPair> prof_pairs;
@@ -118,7 +120,7 @@ struct KrylovWork {
 struct SolveWork {
     KrylovWork<double2> k64;
     KrylovWork<float2> k32;
-    DevBuf r64, r32, d32, partg, nrmg, one, ax;
+    DevBuf r64, r32, d32, t32, partg, nrmg, one, ax;
     PinnedBuf pin;
     DevBuf npart, nred;  // scratch of the ||b|| reduction
     int64_t n = 0;
@@ -133,6 +135,7 @@ struct SolveWork {
         r64.alloc(sizeof(double2) * n);
         r32.alloc(sizeof(float2) * n);
         d32.alloc(sizeof(float2) * n);
+        t32.alloc(sizeof(float2) * n);
         partg.alloc(sizeof(double) * gemv_partials(n));
         nrmg.alloc(sizeof(double) * 2);
         one.alloc(sizeof(double2));
@@ -224,6 +227,8 @@ struct Problem {
     std::function<void(const T*, T*, Gate)> apply;              // y = A x (gated)
     std::function<void(const T*, const T*, T*, double*)> residual;  // r = b - A x, partials
     int64_t partials = 0;                                       // partial norms residual writes
+    const void* key_pre = nullptr;                              // right preconditioner's data
+    int key_pre_bs = 0;
     const double2* jacobi = nullptr;                            // diagonal for Jacobi, or null
     cudaStream_t stream = nullptr;
 };
@@ -276,7 +281,8 @@ void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
 template <class T>
 void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
     const int jac = P.jacobi ? 1 : 0;
-    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_jac != P.jacobi || W.key_prof != prof_key()) {
+    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_jac != P.jacobi || W.key_prof != prof_key() ||
+        W.key_pre != P.key_pre || W.key_pre_bs != P.key_pre_bs) {
         W.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&W.prof_pairs);
@@ -299,6 +305,8 @@ void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
         W.key_jac = P.jacobi;
         W.key_jacobi = jac;
         W.key_prof = prof_key();
+        W.key_pre = P.key_pre;
+        W.key_pre_bs = P.key_pre_bs;
     }
     SB_CUDA(cudaGraphLaunch(W.exec, P.stream));
     add_kernel_count(W.graph_kernels);
@@ -601,6 +609,24 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
     const bool half = op.inner == SB_INNER_FP16;
     if (half) half_prepare(const_cast<Operator&>(op));
     Problem<float2> P = half ? problem16(op) : problem32(op);
+    // Right block-Jacobi preconditioning of the inner solve: (A M^-1) y = r, d = M^-1 y.
+    const bool bj = op.inner_precond == SB_INNER_PRECOND_BLOCK_JACOBI;
+    if (bj) {
+        bj_prepare(const_cast<Operator&>(op));
+        float2* t = sw.t32.as<float2>();
+        auto inner_apply = P.apply;
+        auto inner_res = P.residual;
+        P.apply = [&op, t, inner_apply](const float2* xi, float2* yo, Gate g) {
+            bj_apply(op, xi, t, g);
+            inner_apply(t, yo, g);
+        };
+        P.residual = [&op, t, inner_res](const float2* xi, const float2* bi, float2* ro, double* part) {
+            bj_apply(op, xi, t, Gate{});
+            inner_res(t, bi, ro, part);
+        };
+        P.key_pre = op.bj_inv.p;
+        P.key_pre_bs = op.bj_size;
+    }
     st = sb_gmres_stats{};
     // ||b|| by a norm kernel; with a zero initial guess the first residual is b itself.
     arnoldi_dots<double2>(b, n, 0, b, n, sw.k64_part(n), sw.k64_red(), op.stream);
@@ -646,7 +672,12 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
         st.restarts += R.restarts;
         st.matvecs += R.matvecs;
         st.matvecs_fp32 += R.matvecs;
-        basis_update<float2, double2>(sw.d32.as<float2>(), n, 1, nullptr, sw.one.as<double2>(), rn, x, n, op.stream);
+        const float2* dcorr = sw.d32.as<float2>();
+        if (bj) {
+            bj_apply(op, sw.d32.as<float2>(), sw.t32.as<float2>(), Gate{});
+            dcorr = sw.t32.as<float2>();
+        }
+        basis_update<float2, double2>(dcorr, n, 1, nullptr, sw.one.as<double2>(), rn, x, n, op.stream);
         r_valid = false;
         ++st.refinements;
         if (R.status == SB_SOLVER_BREAKDOWN && R.iterations == 0) {

@@ -1,0 +1,268 @@
+// Block-Jacobi preconditioner of the inner solve of the mixed solver (no reference counterpart:
+// an inner-solver choice of this library; the reference's preconditioned GMRES interface is
+// Preconditioner::apply_into, crates/sonium-solvers/crates/sonium-solvers-core/src/traits.rs:3645).
+//
+// The unknowns are grouped into blocks of spatially close elements (consecutive in the Morton
+// order of the element centroids; index order for an operator without a mesh). Each diagonal
+// block of the complex64 matrix is gathered into shared memory by one CTA and inverted in place
+// by Gauss-Jordan elimination with partial pivoting (FP32); the inverse is stored transposed so
+// that the apply kernel's loads are coalesced. The inner GMRES is preconditioned on the right:
+// it solves (A M^-1) y = r and the correction is d = M^-1 y, so the outer refinement (and the
+// converged answer) is unchanged; only the inner iteration count drops. The preconditioner is
+// rebuilt after each assembly on the first mixed solve that uses it.
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "sb_blas.cuh"
+#include "sb_device.cuh"
+#include "sb_internal.cuh"
+#include "sb_profile.cuh"
+
+namespace sb {
+
+namespace {
+
+// Threads of the inversion CTA: the elimination updates BS x BS entries per pivot.
+constexpr int bj_threads(int bs) { return bs >= 128 ? 512 : 256; }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// One CTA per block: gather M = A[p_i][p_j] (identity rows / columns past the last unknown),
+// invert in place (Gauss-Jordan, partial pivoting), store inv^T at out[blk]. A zero pivot (a
+// singular block) leaves the identity for that block and raises bit 0 of *status.
+template <int BS, int kBjThreads = bj_threads(BS)>
+__global__ void __launch_bounds__(kBjThreads) k_bj_invert(const float2* __restrict__ A, int64_t lda, int64_t n,
+                                                          const int32_t* __restrict__ perm, float2* __restrict__ out,
+                                                          int* __restrict__ status) {
+    extern __shared__ float2 M[];  // BS x BS, row-major
+    __shared__ int piv[BS];
+    __shared__ float2 fcol[BS];
+    __shared__ int s_p;
+    __shared__ float2 s_inv;
+    __shared__ int s_singular;
+    const int64_t base = blockIdx.x * (int64_t)BS;
+    const int rows = static_cast<int>(n - base < BS ? n - base : BS);
+    for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
+        const int i = t / BS, j = t % BS;
+        float2 v = make_float2(i == j ? 1.f : 0.f, 0.f);
+        if (i < rows && j < rows) v = A[(int64_t)perm[base + i] * lda + perm[base + j]];
+        M[t] = v;
+    }
+    if (threadIdx.x == 0) s_singular = 0;
+    __syncthreads();
+    for (int k = 0; k < BS; ++k) {
+        // pivot: the largest |M[i][k]|, i >= k (warp 0)
+        if (threadIdx.x < 32) {
+            float best = -1.f;
+            int bi = k;
+            for (int i = k + threadIdx.x; i < BS; i += 32) {
+                const float2 v = M[i * BS + k];
+                const float a = v.x * v.x + v.y * v.y;
+                if (a > best) {
+                    best = a;
+                    bi = i;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (threadIdx.x == 0) {
+                s_p = bi;
+                piv[k] = bi;
+                if (!(best > 0.f)) s_singular = 1;
+            }
+        }
+        __syncthreads();
+        if (s_singular) break;
+        const int p = s_p;
+        if (p != k)
+            for (int j = threadIdx.x; j < BS; j += kBjThreads) {
+                const float2 t = M[k * BS + j];
+                M[k * BS + j] = M[p * BS + j];
+                M[p * BS + j] = t;
+            }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const float2 v = M[k * BS + k];
+            const float d = 1.f / (v.x * v.x + v.y * v.y);
+            s_inv = make_float2(v.x * d, -v.y * d);
+        }
+        __syncthreads();
+        const float2 inv = s_inv;
+        // row k /= pivot, with M[k][k] taking 1 / pivot
+        for (int j = threadIdx.x; j < BS; j += kBjThreads)
+            M[k * BS + j] = (j == k) ? inv : cmul(M[k * BS + j], inv);
+        __syncthreads();
+        // rows i != k: M[i][j] -= M[i][k] M[k][j], with M[i][k] taking -M[i][k] / pivot (column k
+        // is read into fcol first: its entries are overwritten in the same pass)
+        for (int i = threadIdx.x; i < BS; i += kBjThreads) fcol[i] = M[i * BS + k];
+        __syncthreads();
+        for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
+            const int i = t / BS, j = t % BS;
+            if (i == k) continue;
+            const float2 f = fcol[i];
+            if (j == k) {
+                const float2 q = cmul(f, inv);
+                M[t] = make_float2(-q.x, -q.y);
+            } else {
+                const float2 pr = cmul(f, M[k * BS + j]);
+                M[t] = make_float2(M[t].x - pr.x, M[t].y - pr.y);
+            }
+        }
+        __syncthreads();
+    }
+    if (s_singular) {
+        if (threadIdx.x == 0) atomicOr(status, 1);
+        for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
+            const int i = t / BS, j = t % BS;
+            out[blockIdx.x * (int64_t)BS * BS + t] = make_float2(i == j ? 1.f : 0.f, 0.f);
+        }
+        return;
+    }
+    // Undo the row interchanges as column interchanges of the inverse, last first.
+    for (int k = BS - 1; k >= 0; --k) {
+        const int p = piv[k];
+        if (p != k)
+            for (int i = threadIdx.x; i < BS; i += kBjThreads) {
+                const float2 t = M[i * BS + k];
+                M[i * BS + k] = M[i * BS + p];
+                M[i * BS + p] = t;
+            }
+        __syncthreads();
+    }
+    // inv^T: out[blk][j][i] = M[i][j]
+    for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
+        const int j = t / BS, i = t % BS;
+        out[blockIdx.x * (int64_t)BS * BS + t] = M[i * BS + j];
+    }
+}
+
+// y = M^-1 x: one CTA of BS threads per block; thread i forms row i of the block from the
+// transposed inverse (coalesced over i) and the gathered x of the block.
+template <int BS>
+__global__ void __launch_bounds__(BS) k_bj_apply(const float2* __restrict__ invT, int64_t n,
+                                                 const int32_t* __restrict__ perm, const float2* __restrict__ x,
+                                                 float2* __restrict__ y, Gate gate) {
+    if ((gate.a && *gate.a == 0) || (gate.b && *gate.b == 0)) return;
+    __shared__ float2 xs[BS];
+    const int64_t base = blockIdx.x * (int64_t)BS;
+    const int rows = static_cast<int>(n - base < BS ? n - base : BS);
+    const int i = threadIdx.x;
+    xs[i] = i < rows ? x[perm[base + i]] : make_float2(0.f, 0.f);
+    __syncthreads();
+    const float2* blk = invT + blockIdx.x * (int64_t)BS * BS;
+    float re = 0.f, im = 0.f;
+#pragma unroll 8
+    for (int j = 0; j < BS; ++j) {
+        const float2 a = blk[j * BS + i], v = xs[j];
+        re = fmaf(a.x, v.x, fmaf(-a.y, v.y, re));
+        im = fmaf(a.x, v.y, fmaf(a.y, v.x, im));
+    }
+    if (i < rows) y[perm[base + i]] = make_float2(re, im);
+}
+
+// Morton (Z-order) permutation of points: 21 bits per axis of the normalised coordinates.
+std::vector<int32_t> morton_order(const std::vector<double>& xyz, int64_t n) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t e = 0; e < n; ++e)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], xyz[3 * e + d]);
+            hi[d] = std::max(hi[d], xyz[3 * e + d]);
+        }
+    const double span = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
+    std::vector<uint64_t> code(n);
+    for (int64_t e = 0; e < n; ++e) {
+        uint64_t c = 0;
+        uint64_t q[3];
+        for (int d = 0; d < 3; ++d) {
+            const double t = (xyz[3 * e + d] - lo[d]) / span;
+            q[d] = static_cast<uint64_t>(std::min(std::max(t, 0.0), 1.0) * 2097151.0);
+        }
+        for (int b = 0; b < 21; ++b)
+            for (int d = 0; d < 3; ++d) c |= ((q[d] >> b) & 1ull) << (3 * b + d);
+        code[e] = c;
+    }
+    std::vector<int32_t> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return code[a] < code[b]; });
+    return order;
+}
+
+template <int BS>
+void bj_build(Operator& op, int* status) {
+    const int64_t nb = (op.n + BS - 1) / BS;
+    const size_t smem = sizeof(float2) * BS * BS;
+    SB_CUDA(cudaFuncSetAttribute(k_bj_invert<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    k_bj_invert<BS><<<static_cast<unsigned>(nb), bj_threads(BS), smem, op.stream>>>(
+        op.A32.as<float2>(), op.lda32, op.n, op.bj_perm.as<int32_t>(), op.bj_inv.as<float2>(), status);
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+template <int BS>
+void bj_launch(const Operator& op, const float2* x, float2* y, cudaStream_t s, Gate g) {
+    const int64_t nb = (op.n + BS - 1) / BS;
+    k_bj_apply<BS><<<static_cast<unsigned>(nb), BS, 0, s>>>(op.bj_inv.as<float2>(), op.n, op.bj_perm.as<int32_t>(),
+                                                           x, y, g);
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void bj_prepare(Operator& op) {
+    if (op.bj_valid) return;
+    SB_REQUIRE(op.A32.p, SB_ERR_INVALID_ARGUMENT, "block-Jacobi inner preconditioner: no complex64 matrix");
+    const int bs = op.bj_size;
+    const int64_t n = op.n, nb = (n + bs - 1) / bs;
+    if (!op.bj_perm.p) {
+        std::vector<int32_t> perm(n);
+        if (op.mesh && op.basis == SB_BASIS_CONSTANT) {
+            const Mesh& m = *op.mesh;
+            std::vector<double> c(3 * n);
+            for (int64_t e = 0; e < n; ++e)
+                for (int d = 0; d < 3; ++d) c[3 * e + d] = m.h_elem[(ECX + d) * m.ld + e];
+            perm = morton_order(c, n);
+        } else {
+            std::iota(perm.begin(), perm.end(), 0);
+        }
+        op.bj_perm.alloc(sizeof(int32_t) * n);
+        h2d_sync(op.bj_perm.p, perm.data(), sizeof(int32_t) * n);
+    }
+    const size_t bytes = sizeof(float2) * static_cast<size_t>(nb) * bs * bs;
+    if (op.bj_inv.bytes != bytes) {
+        op.bj_inv.release();
+        op.bj_inv.alloc(bytes);
+    }
+    if (!op.bj_status.p) op.bj_status.alloc(sizeof(int));
+    ProfScope prof(SB_PROF_OTHER, op.stream);
+    SB_CUDA(cudaMemsetAsync(op.bj_status.p, 0, sizeof(int), op.stream));
+    switch (bs) {
+        case 32: bj_build<32>(op, op.bj_status.as<int>()); break;
+        case 64: bj_build<64>(op, op.bj_status.as<int>()); break;
+        default: bj_build<128>(op, op.bj_status.as<int>()); break;
+    }
+    op.bj_valid = true;
+}
+
+void bj_apply(const Operator& op, const float2* x, float2* y, Gate g) {
+    ProfScope prof(SB_PROF_ARNOLDI, op.stream);
+    switch (op.bj_size) {
+        case 32: bj_launch<32>(op, x, y, op.stream, g); break;
+        case 64: bj_launch<64>(op, x, y, op.stream, g); break;
+        default: bj_launch<128>(op, x, y, op.stream, g); break;
+    }
+}
+
+}  // namespace sb

@@ -176,6 +176,13 @@ struct Operator {
     // entries apart; half_aux holds the largest part's bits, the scale and its inverse (device).
     int inner = SB_INNER_FP32;
     DevBuf A16, half_aux;
+    // Block-Jacobi preconditioner of the inner solve (SB_INNER_PRECOND_BLOCK_JACOBI): unknowns in
+    // blocks of bj_size consecutive entries of bj_perm (Morton order of the element centroids),
+    // the transposed inverses of the complex64 diagonal blocks in bj_inv (rebuilt after assembly).
+    int inner_precond = SB_INNER_PRECOND_NONE;
+    int bj_size = 128;
+    DevBuf bj_perm, bj_inv, bj_status;
+    bool bj_valid = false;
     // Near-pair and self kernels of the constant-basis Tri3 assembly run here, concurrently with
     // the far kernel (they write disjoint entries; the far kernel is FMA / special-function bound,
     // the near kernel FP64 and latency bound).
@@ -249,6 +256,9 @@ void solve_work_pool_trim(int device);
 struct Gate;
 // Builds the complex-half copy of the complex64 matrix on the operator's stream (blas.cu).
 void half_prepare(Operator& op);
+// Block-Jacobi inner preconditioner (precond.cu): build the block inverses; y = M^-1 x (FP32).
+void bj_prepare(Operator& op);
+void bj_apply(const Operator& op, const float2* x, float2* y, Gate g);
 // Products with FP64 vectors on whichever matrix the operator holds (gmres.cu).
 void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g);
 void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part);

@@ -222,6 +222,13 @@ class TbemOperator(LinearOperator):
         with IrConfig(inner_tolerance=1e-3)). Needs a complex64 matrix."""
         check(L.load().sb_operator_set_inner_precision(self.handle, int(inner)))
 
+    def set_inner_preconditioner(self, kind: int, block_size: int = 128) -> None:
+        """Right preconditioner of gmres_mixed's inner GMRES: SB_INNER_PRECOND_NONE (default) or
+        SB_INNER_PRECOND_BLOCK_JACOBI (inverted diagonal blocks of block_size spatially close
+        elements; 32, 64 or 128). The converged solution is unchanged; the inner solves need fewer
+        iterations. Needs a complex64 matrix."""
+        check(L.load().sb_operator_set_inner_preconditioner(self.handle, int(kind), int(block_size)))
+
     def reassemble(self, physics: PhysicsParams, beta: complex) -> None:
         check(L.load().sb_assemble_into(self.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag)))
         self.physics, self.beta = physics, beta
