@@ -566,10 +566,11 @@ def sweep_leg(sb, a, dist, dev, rt):
 
     One step = batched assembly of all 64 complex64 matrices (the form the autotuner chose on the
     first, untimed step), the incident right-hand sides, and the batched mixed GMRES to rtol 1e-8
-    (FP64 refinement on the complex64 matrices around FP32-vector inner solves). Two forms of the
-    inner products are timed: on the complex64 matrices (inner tolerance 1e-5) and on complex-half
-    copies built inside each solve (inner tolerance 1e-3); `value` is the faster form whose
-    solutions are all within 1e-5 of the FP64 ones. Baseline: the same 64 instances solved one
+    (FP64 refinement on the complex64 matrices around FP32-vector inner solves). Three forms of
+    the inner solves are timed: products on the complex64 matrices (inner tolerance 1e-5), on
+    complex-half copies built inside each solve (inner tolerance 1e-3), and the latter with the
+    block-Jacobi right preconditioner (blocks of 64, inverted inside each solve); `value` is the
+    fastest form whose solutions are all within 1e-5 of the FP64 ones. Baseline: the same 64 instances solved one
     after another in plain FP64 (complex128 assembly re-done into one operator per mesh level,
     FP64 GMRES(50) to 1e-8), timed once. Wall clock around device-synchronised work on both sides;
     the per-instance error of the batched solution against the FP64 one is reported as its
@@ -596,8 +597,12 @@ def sweep_leg(sb, a, dist, dev, rt):
     # Two forms of the batched inner products: the complex64 matrices, and their complex-half
     # copies (built inside each solve, after each assembly).
     forms = {}
-    for form_name, inner, cfg_f in (("fp32_inner", sb.SB_INNER_FP32, cfg), ("half_inner", sb.SB_INNER_FP16, cfg16)):
+    for form_name, inner, bj, cfg_f in (("fp32_inner", sb.SB_INNER_FP32, False, cfg),
+                                        ("half_inner", sb.SB_INNER_FP16, False, cfg16),
+                                        ("half_inner_bj", sb.SB_INNER_FP16, True, cfg16)):
         batch.set_inner_precision(inner)
+        batch.set_inner_preconditioner(sb.SB_INNER_PRECOND_BLOCK_JACOBI if bj else sb.SB_INNER_PRECOND_NONE,
+                                       BJ_BLOCK)
 
         def step():
             batch.assemble()
@@ -665,7 +670,8 @@ def sweep_leg(sb, a, dist, dev, rt):
         "forms": {k: {"value": f["value"], "ms_per_step": 1e3 * f["t"] / a.steps, "assembly_ms": f["assembly_ms"],
                       "solve_ms": f["solve_ms"], "max_error_vs_fp64": max(f["errs"]),
                       "speedup_vs_plain_fp64": f["value"] / plain,
-                      "inner_tolerance": cfg16.inner_tolerance if k == "half_inner" else cfg.inner_tolerance,
+                      "inner_tolerance": cfg.inner_tolerance if k == "fp32_inner" else cfg16.inner_tolerance,
+                      "block_jacobi": BJ_BLOCK if k == "half_inner_bj" else None,
                       "iterations_total": int(sum(s.iterations for s in f["st0"]))}
                   for k, f in forms.items()},
         "timing": "wall clock around device-synchronised steps, max over ranks",

@@ -432,6 +432,10 @@ SB_API int sb_batch_solve(sb_batch* batch, const sb_ir_config* cfg, sb_gmres_sta
  * each with its own power-of-two scale, built on the device by the first solve after each
  * sb_batch_assemble and counted in its time; 4 bytes per entry of extra device memory). */
 SB_API int sb_batch_set_inner_precision(sb_batch* batch, int inner);
+/* Block-Jacobi right preconditioner of the batched inner solves, as
+ * sb_operator_set_inner_preconditioner: every instance's blocks of its own Morton order, inverted
+ * on the device by the first solve after each sb_batch_assemble (counted in its time). */
+SB_API int sb_batch_set_inner_preconditioner(sb_batch* batch, int kind, int block_size);
 SB_API int sb_batch_solution(const sb_batch* batch, int64_t index, sb_complex* x);
 /* The assembled complex64 matrix of one instance, row-major n x n. */
 SB_API int sb_batch_matrix_c64(const sb_batch* batch, int64_t index, sb_complex32* matrix);

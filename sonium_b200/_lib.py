@@ -172,6 +172,7 @@ _SIGNATURES = {
     "sb_batch_set_rhs": ([P, ct.c_int64, P], ct.c_int),
     "sb_batch_solve": ([P, ct.POINTER(SbIrConfig), P], ct.c_int),
     "sb_batch_set_inner_precision": ([P, ct.c_int], ct.c_int),
+    "sb_batch_set_inner_preconditioner": ([P, ct.c_int, ct.c_int], ct.c_int),
     "sb_batch_solution": ([P, ct.c_int64, P], ct.c_int),
     "sb_batch_matrix_c64": ([P, ct.c_int64, P], ct.c_int),
     "sb_batch_timings": ([P, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),

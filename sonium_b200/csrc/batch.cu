@@ -33,6 +33,7 @@
 #include "sb_gemv.cuh"
 #include "sb_internal.cuh"
 #include "sb_krylov.cuh"
+#include "sb_precond.cuh"
 #include "sb_profile.cuh"
 
 struct sb_mesh {
@@ -67,6 +68,11 @@ struct BInst {
     const uint32_t* A16;
     int64_t lda16;
     unsigned* aux16;
+    // Block-Jacobi right preconditioner of the inner solve (SB_INNER_PRECOND_BLOCK_JACOBI): the
+    // transposed block inverses, the Morton permutation, and t = M^-1 of the product's input.
+    const float2* bj_inv;
+    const int32_t* bj_perm;
+    float2* t;
 };
 
 namespace {
@@ -99,7 +105,8 @@ __device__ __forceinline__ bool open_gate(const BInst& I, int gk) {
 }
 
 // Matrix-vector products over the flattened row blocks (kGemvRows rows per CTA).
-// mode 0: w = A V_j; mode 1: rq = rb - A d (partial norms).
+// mode 0: w = A V_j; mode 1: rq = rb - A d (partial norms); modes 2 / 3: the same with t
+// (= M^-1 V_j or M^-1 d under the block-Jacobi preconditioner) in place of V_j / d.
 __global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restrict__ inst,
                                                           const int64_t* __restrict__ pre, int ninst, int mode,
                                                           int j, int gk) {
@@ -107,11 +114,11 @@ __global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restric
     const BInst& I = inst[b];
     if (!open_gate(I, gk)) return;
     const int64_t blk = blockIdx.x - pre[b];
-    if (mode == 0)
-        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.V + (int64_t)j * I.vs, I.w,
-                                                                    nullptr, nullptr, blk);
+    const float2* src = mode == 0 ? I.V + (int64_t)j * I.vs : (mode == 1 ? I.d : I.t);
+    if (mode == 0 || mode == 2)
+        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, src, I.w, nullptr, nullptr, blk);
     else
-        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, I.d, I.rq, I.rb, I.pnorm, blk);
+        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, src, I.rq, I.rb, I.pnorm, blk);
 }
 
 // The same products on the complex-half copies (kGemv16Rows rows per CTA).
@@ -123,12 +130,41 @@ __global__ void __launch_bounds__(kGemvThreads) k_bgemv16(const BInst* __restric
     if (!open_gate(I, gk)) return;
     const int64_t blk = blockIdx.x - pre[b];
     const float* inv = reinterpret_cast<const float*>(I.aux16 + 2);
-    if (mode == 0)
-        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, I.V + (int64_t)j * I.vs,
-                                                                 I.w, nullptr, nullptr, blk);
+    const float2* src = mode == 0 ? I.V + (int64_t)j * I.vs : (mode == 1 ? I.d : I.t);
+    if (mode == 0 || mode == 2)
+        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, src, I.w, nullptr,
+                                                                 nullptr, blk);
     else
-        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, I.d, I.rq, I.rb,
+        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, src, I.rq, I.rb,
                                                                  I.pnorm, blk);
+}
+
+// Block-Jacobi over the flattened blocks of every instance: inverses (one CTA per block) and
+// products. apply mode 0: t = M^-1 V_j; 1: t = M^-1 d; 2: d = M^-1 d (in place: a block's inputs
+// are gathered before its outputs are written, and blocks are disjoint).
+template <int BS>
+__global__ void __launch_bounds__(bj_threads(BS)) k_bbj_invert(const BInst* __restrict__ inst,
+                                                               const int64_t* __restrict__ pre, int ninst,
+                                                               int* __restrict__ status) {
+    extern __shared__ float2 Mbj[];
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    const int64_t blk = blockIdx.x - pre[b], base = blk * BS;
+    const int rows = static_cast<int>(I.n - base < BS ? I.n - base : BS);
+    bj_invert_block<BS, bj_threads(BS)>(I.A, I.lda, rows, I.bj_perm + base,
+                                        const_cast<float2*>(I.bj_inv) + blk * BS * BS, status, Mbj);
+}
+template <int BS>
+__global__ void __launch_bounds__(BS) k_bbj_apply(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+                                                  int ninst, int mode, int j, int gk) {
+    const int b = find_inst(pre, ninst, blockIdx.x);
+    const BInst& I = inst[b];
+    if (!open_gate(I, gk)) return;
+    const int64_t blk = blockIdx.x - pre[b], base = blk * BS;
+    const int rows = static_cast<int>(I.n - base < BS ? I.n - base : BS);
+    const float2* src = mode == 0 ? I.V + (int64_t)j * I.vs : I.d;
+    float2* dst = mode == 2 ? I.d : I.t;
+    bj_apply_block<BS>(I.bj_inv + blk * BS * BS, rows, I.bj_perm + base, src, dst);
 }
 
 // Complex-half copies of every instance's complex64 matrix: largest part, scale, conversion,
@@ -502,6 +538,13 @@ struct Batch {
     bool half_valid = false;
     DevBuf pool_half, pool_half_aux;
     int graph_inner = -1;
+    // Block-Jacobi right preconditioner of the inner solves (independent instances only).
+    int inner_precond = SB_INNER_PRECOND_NONE;
+    int bj_size = 64;
+    bool bj_valid = false;
+    std::vector<int64_t> prebj;
+    DevBuf pool_bj, pool_bj_perm, prebj_d, bj_status;
+    int graph_pre = -1;
     DevBuf pool_mat, pool_rhs, pool_f32, pool_f64, pool_small, pool_state;
     DevBuf gate;  // per group of kTensorRhsTile instances: any still in the Arnoldi cycle
     cudaStream_t stream = nullptr;
@@ -585,6 +628,85 @@ static void half_pointers(const Batch& B, int b, BInst& I) {
     I.aux16 = B.pool_half_aux.as<unsigned>() + 4 * b;
 }
 
+// Where instance b's block inverses and permutation live in the batch's pools (null before).
+static void bj_pointers(const Batch& B, int b, BInst& I) {
+    if (!B.pool_bj.p || !B.pool_bj_perm.p) {
+        I.bj_inv = nullptr;
+        I.bj_perm = nullptr;
+        return;
+    }
+    int64_t off_perm = 0;
+    for (int c = 0; c < b; ++c) off_perm += B.nvec[c];
+    I.bj_perm = B.pool_bj_perm.as<int32_t>() + off_perm;
+    I.bj_inv = B.pool_bj.as<float2>() + B.prebj[b] * B.bj_size * B.bj_size;
+}
+
+template <int BS>
+static void bj_invert_launch(Batch& B) {
+    const size_t smem = sizeof(float2) * BS * BS;
+    SB_CUDA(cudaFuncSetAttribute(k_bbj_invert<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    k_bbj_invert<BS><<<static_cast<unsigned>(B.prebj.back()), bj_threads(BS), smem, B.stream>>>(
+        B.inst_d.as<BInst>(), B.prebj_d.as<int64_t>(), B.ninst, B.bj_status.as<int>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+// Builds every instance's block-Jacobi inverses (after each assembly): Morton permutations once
+// per batch, the block layout per block size.
+static void batch_bj_prepare(Batch& B) {
+    if (B.bj_valid) return;
+    const int ni = B.ninst, bs = B.bj_size;
+    bool layout = false;
+    if (!B.pool_bj_perm.p) {
+        int64_t total = 0;
+        for (int b = 0; b < ni; ++b) total += B.nvec[b];
+        std::vector<int32_t> perm;
+        perm.reserve(total);
+        for (int b = 0; b < ni; ++b) {
+            const std::vector<int32_t> p = element_morton_order(*B.meshes[b]);
+            perm.insert(perm.end(), p.begin(), p.end());
+        }
+        B.pool_bj_perm.alloc(sizeof(int32_t) * total);
+        h2d_sync(B.pool_bj_perm.p, perm.data(), sizeof(int32_t) * total);
+        layout = true;
+    }
+    std::vector<int64_t> prebj(ni + 1, 0);
+    for (int b = 0; b < ni; ++b) prebj[b + 1] = prebj[b] + cdiv64(B.nvec[b], bs);
+    if (layout || prebj != B.prebj || !B.pool_bj.p) {
+        B.prebj = prebj;
+        B.pool_bj.release();
+        B.pool_bj.alloc(sizeof(float2) * prebj.back() * bs * bs);
+        B.prebj_d.alloc(sizeof(int64_t) * (ni + 1));
+        h2d_sync(B.prebj_d.p, prebj.data(), sizeof(int64_t) * (ni + 1));
+        for (int b = 0; b < ni; ++b) bj_pointers(B, b, B.h[b]);
+        h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
+    }
+    if (!B.bj_status.p) B.bj_status.alloc(sizeof(int));
+    ProfScope prof(SB_PROF_OTHER, B.stream);
+    SB_CUDA(cudaMemsetAsync(B.bj_status.p, 0, sizeof(int), B.stream));
+    switch (bs) {
+        case 32: bj_invert_launch<32>(B); break;
+        case 128: bj_invert_launch<128>(B); break;
+        default: bj_invert_launch<64>(B); break;
+    }
+    B.bj_valid = true;
+}
+
+// t = M^-1 V_j (mode 0), t = M^-1 d (1) or d = M^-1 d (2) for every instance whose gate is open.
+static void batch_bj_apply(Batch& B, int mode, int j, int gk) {
+    const unsigned g = static_cast<unsigned>(B.prebj.back());
+    const BInst* I = B.inst_d.as<BInst>();
+    const int64_t* p = B.prebj_d.as<int64_t>();
+    ProfScope prof(SB_PROF_ARNOLDI, B.stream);
+    switch (B.bj_size) {
+        case 32: k_bbj_apply<32><<<g, 32, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
+        case 128: k_bbj_apply<128><<<g, 128, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
+        default: k_bbj_apply<64><<<g, 64, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
+    }
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
 // Builds the complex-half copies of every instance's complex64 matrix (after each assembly).
 static void batch_half_prepare(Batch& B) {
     if (B.half_valid) return;
@@ -621,7 +743,7 @@ static void batch_workspace(Batch& B, int64_t m) {
     for (int b = 0; b < ni; ++b) {
         const int64_t n = B.nvec[b], ldv = (n + 1) / 2 * 2;
         const int64_t chunks = cdiv64(n, kChunk);
-        f32 += round256(sizeof(float2) * (m + 1) * ldv) + 4 * round256(sizeof(float2) * ldv);
+        f32 += round256(sizeof(float2) * (m + 1) * ldv) + 5 * round256(sizeof(float2) * ldv);
         f64 += 2 * round256(sizeof(double2) * ldv);
         small += round256(sizeof(double2) * (m + 1) * m) + 2 * round256(sizeof(double2) * m) +
                  2 * round256(sizeof(double2) * (m + 1)) + 2 * round256(sizeof(double2) * (m + 2)) +
@@ -691,6 +813,8 @@ static void batch_workspace(Batch& B, int64_t m) {
             I.rb = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
             I.d = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
             I.rq = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+            I.t = reinterpret_cast<float2*>(take(pf32, sizeof(float2) * ldv));
+            bj_pointers(B, b, I);
             I.x = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
             I.r = reinterpret_cast<double2*>(take(pf64, sizeof(double2) * ldv));
         }
@@ -747,14 +871,19 @@ static void batch_step(Batch& B, int j) {
         count_launch();
         tensor_block_product(*B.shared, B.v_all + (int64_t)j * ni * B.ld_all, B.ld_all, ni, B.w_all, B.ld_all, s,
                              B.gate.as<int>());
-    } else if (B.inner == SB_INNER_FP16) {
-        ProfScope prof(SB_PROF_GEMV16, s);
-        k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni, 0,
-                                                                                 j, G_ACTIVE);
-        count_launch();
     } else {
-        ProfScope prof(SB_PROF_GEMV32, s);
-        k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 0, j, G_ACTIVE);
+        // w = A V_j, or w = A (M^-1 V_j) under the block-Jacobi preconditioner
+        const bool bj = B.inner_precond == SB_INNER_PRECOND_BLOCK_JACOBI;
+        if (bj) batch_bj_apply(B, 0, j, G_ACTIVE);
+        const int mode = bj ? 2 : 0;
+        if (B.inner == SB_INNER_FP16) {
+            ProfScope prof(SB_PROF_GEMV16, s);
+            k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni,
+                                                                                     mode, j, G_ACTIVE);
+        } else {
+            ProfScope prof(SB_PROF_GEMV32, s);
+            k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, mode, j, G_ACTIVE);
+        }
         count_launch();
     }
     ProfScope prof(SB_PROF_ARNOLDI, s);
@@ -780,7 +909,9 @@ static void batch_step(Batch& B, int j) {
 // One restart cycle of the whole batch: m Arnoldi steps captured once into a CUDA graph.
 static void batch_cycle(Batch& B) {
     const uint64_t gen = B.shared ? tensor_generation(*B.shared) : 0;
-    if (!B.exec || B.graph_prof != prof_key() || B.graph_gen != gen || B.graph_inner != B.inner) {
+    const int pre_key = B.inner_precond * 1024 + B.bj_size;
+    if (!B.exec || B.graph_prof != prof_key() || B.graph_gen != gen || B.graph_inner != B.inner ||
+        B.graph_pre != pre_key) {
         B.reset_graph();
         const int64_t before = kernel_count();
         capture_begin(&B.prof_pairs);
@@ -802,6 +933,7 @@ static void batch_cycle(Batch& B) {
         B.graph_prof = prof_key();
         B.graph_gen = gen;
         B.graph_inner = B.inner;
+        B.graph_pre = pre_key;
     }
     SB_CUDA(cudaGraphLaunch(B.exec, B.stream));
     add_kernel_count(B.graph_kernels);
@@ -860,6 +992,7 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
     } evg{e0, e1};
     SB_CUDA(cudaEventRecord(e0, s));
     if (B.inner == SB_INNER_FP16) batch_half_prepare(B);
+    if (!B.shared && B.inner_precond == SB_INNER_PRECOND_BLOCK_JACOBI) batch_bj_prepare(B);
     for (int b = 0; b < ni; ++b) stats[b] = sb_gmres_stats{};
     // x = 0, r = b and ||b|| (with a zero initial guess the first residual needs no product).
     k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_B_TO_R, G_NONE);
@@ -948,20 +1081,25 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
                     k_bresid_w<<<g256, kChunk, 0, s>>>(I, p256, ni, G_RESTART);
                     k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_RESTART);
                     launched(2);
-                } else if (B.inner == SB_INNER_FP16) {
-                    {
-                        ProfScope prof(SB_PROF_GEMV16, s);
-                        k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(
-                            I, B.pre16_d.as<int64_t>(), ni, 1, 0, G_RESTART);
-                    }
-                    k_bsum_partials<<<ni, 32, 0, s>>>(I, B.pre16_d.as<int64_t>(), 2, G_RESTART);
-                    launched(2);
                 } else {
-                    {
-                        ProfScope prof(SB_PROF_GEMV32, s);
-                        k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, 1, 0, G_RESTART);
+                    // rq = rb - A d, or rb - A (M^-1 d) under the block-Jacobi preconditioner
+                    const bool bj = B.inner_precond == SB_INNER_PRECOND_BLOCK_JACOBI;
+                    if (bj) batch_bj_apply(B, 1, 0, G_RESTART);
+                    const int mode = bj ? 3 : 1;
+                    if (B.inner == SB_INNER_FP16) {
+                        {
+                            ProfScope prof(SB_PROF_GEMV16, s);
+                            k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(
+                                I, B.pre16_d.as<int64_t>(), ni, mode, 0, G_RESTART);
+                        }
+                        k_bsum_partials<<<ni, 32, 0, s>>>(I, B.pre16_d.as<int64_t>(), 2, G_RESTART);
+                    } else {
+                        {
+                            ProfScope prof(SB_PROF_GEMV32, s);
+                            k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, mode, 0, G_RESTART);
+                        }
+                        k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_RESTART);
                     }
-                    k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_RESTART);
                     launched(2);
                 }
             }
@@ -992,7 +1130,8 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
             profile_account(B.prof_pairs, steps_max);
             if (!running) break;
         }
-        // x += ||r|| d
+        // x += ||r|| d (d = M^-1 y under the block-Jacobi preconditioner)
+        if (!B.shared && B.inner_precond == SB_INNER_PRECOND_BLOCK_JACOBI) batch_bj_apply(B, 2, 0, G_OUTER);
         k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_X_UPDATE, G_OUTER);
         launched(1);
         for (int b = 0; b < ni; ++b) {
@@ -1307,6 +1446,23 @@ SB_API int sb_batch_assemble(sb_batch* batch) {
         B.asm_chosen = form;
         B.assembled = true;
         B.half_valid = false;
+        B.bj_valid = false;
+    });
+}
+
+SB_API int sb_batch_set_inner_preconditioner(sb_batch* batch, int kind, int block_size) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null argument");
+        SB_REQUIRE(kind == SB_INNER_PRECOND_NONE || kind == SB_INNER_PRECOND_BLOCK_JACOBI, SB_ERR_INVALID_ARGUMENT,
+                   "inner preconditioner must be SB_INNER_PRECOND_NONE or SB_INNER_PRECOND_BLOCK_JACOBI");
+        Batch& B = *batch->b;
+        if (kind == SB_INNER_PRECOND_BLOCK_JACOBI) {
+            SB_REQUIRE(block_size == 32 || block_size == 64 || block_size == 128, SB_ERR_INVALID_ARGUMENT,
+                       "block_size must be 32, 64 or 128");
+            if (block_size != B.bj_size) B.bj_valid = false;
+            B.bj_size = block_size;
+        }
+        B.inner_precond = kind;
     });
 }
 

@@ -19,158 +19,35 @@
 #include "sb_blas.cuh"
 #include "sb_device.cuh"
 #include "sb_internal.cuh"
+#include "sb_precond.cuh"
 #include "sb_profile.cuh"
 
 namespace sb {
 
 namespace {
 
-// Threads of the inversion CTA: the elimination updates BS x BS entries per pivot.
-constexpr int bj_threads(int bs) { return bs >= 128 ? 512 : 256; }
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-// One CTA per block: gather M = A[p_i][p_j] (identity rows / columns past the last unknown),
-// invert in place (Gauss-Jordan, partial pivoting), store inv^T at out[blk]. A zero pivot (a
-// singular block) leaves the identity for that block and raises bit 0 of *status.
-template <int BS, int kBjThreads = bj_threads(BS)>
-__global__ void __launch_bounds__(kBjThreads) k_bj_invert(const float2* __restrict__ A, int64_t lda, int64_t n,
-                                                          const int32_t* __restrict__ perm, float2* __restrict__ out,
-                                                          int* __restrict__ status) {
+template <int BS>
+__global__ void __launch_bounds__(bj_threads(BS)) k_bj_invert(const float2* __restrict__ A, int64_t lda, int64_t n,
+                                                              const int32_t* __restrict__ perm,
+                                                              float2* __restrict__ out, int* __restrict__ status) {
     extern __shared__ float2 M[];  // BS x BS, row-major
-    __shared__ int piv[BS];
-    __shared__ float2 fcol[BS];
-    __shared__ int s_p;
-    __shared__ float2 s_inv;
-    __shared__ int s_singular;
     const int64_t base = blockIdx.x * (int64_t)BS;
     const int rows = static_cast<int>(n - base < BS ? n - base : BS);
-    for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
-        const int i = t / BS, j = t % BS;
-        float2 v = make_float2(i == j ? 1.f : 0.f, 0.f);
-        if (i < rows && j < rows) v = A[(int64_t)perm[base + i] * lda + perm[base + j]];
-        M[t] = v;
-    }
-    if (threadIdx.x == 0) s_singular = 0;
-    __syncthreads();
-    for (int k = 0; k < BS; ++k) {
-        // pivot: the largest |M[i][k]|, i >= k (warp 0)
-        if (threadIdx.x < 32) {
-            float best = -1.f;
-            int bi = k;
-            for (int i = k + threadIdx.x; i < BS; i += 32) {
-                const float2 v = M[i * BS + k];
-                const float a = v.x * v.x + v.y * v.y;
-                if (a > best) {
-                    best = a;
-                    bi = i;
-                }
-            }
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                const float ob = __shfl_xor_sync(0xffffffffu, best, o);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (ob > best || (ob == best && oi < bi)) {
-                    best = ob;
-                    bi = oi;
-                }
-            }
-            if (threadIdx.x == 0) {
-                s_p = bi;
-                piv[k] = bi;
-                if (!(best > 0.f)) s_singular = 1;
-            }
-        }
-        __syncthreads();
-        if (s_singular) break;
-        const int p = s_p;
-        if (p != k)
-            for (int j = threadIdx.x; j < BS; j += kBjThreads) {
-                const float2 t = M[k * BS + j];
-                M[k * BS + j] = M[p * BS + j];
-                M[p * BS + j] = t;
-            }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const float2 v = M[k * BS + k];
-            const float d = 1.f / (v.x * v.x + v.y * v.y);
-            s_inv = make_float2(v.x * d, -v.y * d);
-        }
-        __syncthreads();
-        const float2 inv = s_inv;
-        // row k /= pivot, with M[k][k] taking 1 / pivot
-        for (int j = threadIdx.x; j < BS; j += kBjThreads)
-            M[k * BS + j] = (j == k) ? inv : cmul(M[k * BS + j], inv);
-        __syncthreads();
-        // rows i != k: M[i][j] -= M[i][k] M[k][j], with M[i][k] taking -M[i][k] / pivot (column k
-        // is read into fcol first: its entries are overwritten in the same pass)
-        for (int i = threadIdx.x; i < BS; i += kBjThreads) fcol[i] = M[i * BS + k];
-        __syncthreads();
-        for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
-            const int i = t / BS, j = t % BS;
-            if (i == k) continue;
-            const float2 f = fcol[i];
-            if (j == k) {
-                const float2 q = cmul(f, inv);
-                M[t] = make_float2(-q.x, -q.y);
-            } else {
-                const float2 pr = cmul(f, M[k * BS + j]);
-                M[t] = make_float2(M[t].x - pr.x, M[t].y - pr.y);
-            }
-        }
-        __syncthreads();
-    }
-    if (s_singular) {
-        if (threadIdx.x == 0) atomicOr(status, 1);
-        for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
-            const int i = t / BS, j = t % BS;
-            out[blockIdx.x * (int64_t)BS * BS + t] = make_float2(i == j ? 1.f : 0.f, 0.f);
-        }
-        return;
-    }
-    // Undo the row interchanges as column interchanges of the inverse, last first.
-    for (int k = BS - 1; k >= 0; --k) {
-        const int p = piv[k];
-        if (p != k)
-            for (int i = threadIdx.x; i < BS; i += kBjThreads) {
-                const float2 t = M[i * BS + k];
-                M[i * BS + k] = M[i * BS + p];
-                M[i * BS + p] = t;
-            }
-        __syncthreads();
-    }
-    // inv^T: out[blk][j][i] = M[i][j]
-    for (int t = threadIdx.x; t < BS * BS; t += kBjThreads) {
-        const int j = t / BS, i = t % BS;
-        out[blockIdx.x * (int64_t)BS * BS + t] = M[i * BS + j];
-    }
+    bj_invert_block<BS, bj_threads(BS)>(A, lda, rows, perm + base, out + blockIdx.x * (int64_t)BS * BS, status, M);
 }
 
-// y = M^-1 x: one CTA of BS threads per block; thread i forms row i of the block from the
-// transposed inverse (coalesced over i) and the gathered x of the block.
+// y = M^-1 x: one CTA of BS threads per block.
 template <int BS>
 __global__ void __launch_bounds__(BS) k_bj_apply(const float2* __restrict__ invT, int64_t n,
                                                  const int32_t* __restrict__ perm, const float2* __restrict__ x,
                                                  float2* __restrict__ y, Gate gate) {
     if ((gate.a && *gate.a == 0) || (gate.b && *gate.b == 0)) return;
-    __shared__ float2 xs[BS];
     const int64_t base = blockIdx.x * (int64_t)BS;
     const int rows = static_cast<int>(n - base < BS ? n - base : BS);
-    const int i = threadIdx.x;
-    xs[i] = i < rows ? x[perm[base + i]] : make_float2(0.f, 0.f);
-    __syncthreads();
-    const float2* blk = invT + blockIdx.x * (int64_t)BS * BS;
-    float re = 0.f, im = 0.f;
-#pragma unroll 8
-    for (int j = 0; j < BS; ++j) {
-        const float2 a = blk[j * BS + i], v = xs[j];
-        re = fmaf(a.x, v.x, fmaf(-a.y, v.y, re));
-        im = fmaf(a.x, v.y, fmaf(a.y, v.x, im));
-    }
-    if (i < rows) y[perm[base + i]] = make_float2(re, im);
+    bj_apply_block<BS>(invT + blockIdx.x * (int64_t)BS * BS, rows, perm + base, x, y);
 }
+
+}  // namespace
 
 // Morton (Z-order) permutation of points: 21 bits per axis of the normalised coordinates.
 std::vector<int32_t> morton_order(const std::vector<double>& xyz, int64_t n) {
@@ -198,6 +75,15 @@ std::vector<int32_t> morton_order(const std::vector<double>& xyz, int64_t n) {
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return code[a] < code[b]; });
     return order;
 }
+
+std::vector<int32_t> element_morton_order(const Mesh& m) {
+    std::vector<double> c(3 * m.n);
+    for (int64_t e = 0; e < m.n; ++e)
+        for (int d = 0; d < 3; ++d) c[3 * e + d] = m.h_elem[(ECX + d) * m.ld + e];
+    return morton_order(c, m.n);
+}
+
+namespace {
 
 template <int BS>
 void bj_build(Operator& op, int* status) {
@@ -229,11 +115,7 @@ void bj_prepare(Operator& op) {
     if (!op.bj_perm.p) {
         std::vector<int32_t> perm(n);
         if (op.mesh && op.basis == SB_BASIS_CONSTANT) {
-            const Mesh& m = *op.mesh;
-            std::vector<double> c(3 * n);
-            for (int64_t e = 0; e < n; ++e)
-                for (int d = 0; d < 3; ++d) c[3 * e + d] = m.h_elem[(ECX + d) * m.ld + e];
-            perm = morton_order(c, n);
+            perm = element_morton_order(*op.mesh);
         } else {
             std::iota(perm.begin(), perm.end(), 0);
         }

@@ -259,6 +259,8 @@ void half_prepare(Operator& op);
 // Block-Jacobi inner preconditioner (precond.cu): build the block inverses; y = M^-1 x (FP32).
 void bj_prepare(Operator& op);
 void bj_apply(const Operator& op, const float2* x, float2* y, Gate g);
+// Morton (Z-order) permutation of a mesh's element centroids (precond.cu).
+std::vector<int32_t> element_morton_order(const Mesh& m);
 // Products with FP64 vectors on whichever matrix the operator holds (gmres.cu).
 void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g);
 void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part);

@@ -1,0 +1,149 @@
+// Block-Jacobi preconditioner kernels' bodies (internal), shared by the single-operator solver
+// (precond.cu) and the batched solver (batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sb {
+
+// Threads of the inversion CTA: the elimination updates BS x BS entries per pivot.
+constexpr int bj_threads(int bs) { return bs >= 128 ? 512 : 256; }
+
+__device__ __forceinline__ float2 bj_cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// One CTA (THREADS threads, BS * BS float2 of dynamic shared memory at M) per block: gather the
+// diagonal block M = A[p_i][p_j], i, j < rows (identity beyond), invert it in place (Gauss-Jordan,
+// partial pivoting) and store its transpose at out. A zero pivot (a singular block) stores the
+// identity and raises bit 0 of *status.
+template <int BS, int THREADS>
+__device__ __forceinline__ void bj_invert_block(const float2* __restrict__ A, int64_t lda, int rows,
+                                                const int32_t* __restrict__ perm, float2* __restrict__ out,
+                                                int* __restrict__ status, float2* M) {
+    __shared__ int piv[BS];
+    __shared__ float2 fcol[BS];
+    __shared__ int s_p;
+    __shared__ float2 s_inv;
+    __shared__ int s_singular;
+    for (int t = threadIdx.x; t < BS * BS; t += THREADS) {
+        const int i = t / BS, j = t % BS;
+        float2 v = make_float2(i == j ? 1.f : 0.f, 0.f);
+        if (i < rows && j < rows) v = A[(int64_t)perm[i] * lda + perm[j]];
+        M[t] = v;
+    }
+    if (threadIdx.x == 0) s_singular = 0;
+    __syncthreads();
+    for (int k = 0; k < BS; ++k) {
+        // pivot: the largest |M[i][k]|, i >= k (warp 0)
+        if (threadIdx.x < 32) {
+            float best = -1.f;
+            int bi = k;
+            for (int i = k + threadIdx.x; i < BS; i += 32) {
+                const float2 v = M[i * BS + k];
+                const float a = v.x * v.x + v.y * v.y;
+                if (a > best) {
+                    best = a;
+                    bi = i;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (threadIdx.x == 0) {
+                s_p = bi;
+                piv[k] = bi;
+                if (!(best > 0.f)) s_singular = 1;
+            }
+        }
+        __syncthreads();
+        if (s_singular) break;
+        const int p = s_p;
+        if (p != k)
+            for (int j = threadIdx.x; j < BS; j += THREADS) {
+                const float2 t = M[k * BS + j];
+                M[k * BS + j] = M[p * BS + j];
+                M[p * BS + j] = t;
+            }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const float2 v = M[k * BS + k];
+            const float d = 1.f / (v.x * v.x + v.y * v.y);
+            s_inv = make_float2(v.x * d, -v.y * d);
+        }
+        __syncthreads();
+        const float2 inv = s_inv;
+        // row k /= pivot, with M[k][k] taking 1 / pivot
+        for (int j = threadIdx.x; j < BS; j += THREADS) M[k * BS + j] = (j == k) ? inv : bj_cmul(M[k * BS + j], inv);
+        __syncthreads();
+        // rows i != k: M[i][j] -= M[i][k] M[k][j], with M[i][k] taking -M[i][k] / pivot (column k
+        // is read into fcol first: its entries are overwritten in the same pass)
+        for (int i = threadIdx.x; i < BS; i += THREADS) fcol[i] = M[i * BS + k];
+        __syncthreads();
+        for (int t = threadIdx.x; t < BS * BS; t += THREADS) {
+            const int i = t / BS, j = t % BS;
+            if (i == k) continue;
+            const float2 f = fcol[i];
+            if (j == k) {
+                const float2 q = bj_cmul(f, inv);
+                M[t] = make_float2(-q.x, -q.y);
+            } else {
+                const float2 pr = bj_cmul(f, M[k * BS + j]);
+                M[t] = make_float2(M[t].x - pr.x, M[t].y - pr.y);
+            }
+        }
+        __syncthreads();
+    }
+    if (s_singular) {
+        if (threadIdx.x == 0) atomicOr(status, 1);
+        for (int t = threadIdx.x; t < BS * BS; t += THREADS) {
+            const int i = t / BS, j = t % BS;
+            out[t] = make_float2(i == j ? 1.f : 0.f, 0.f);
+        }
+        return;
+    }
+    // Undo the row interchanges as column interchanges of the inverse, last first.
+    for (int k = BS - 1; k >= 0; --k) {
+        const int p = piv[k];
+        if (p != k)
+            for (int i = threadIdx.x; i < BS; i += THREADS) {
+                const float2 t = M[i * BS + k];
+                M[i * BS + k] = M[i * BS + p];
+                M[i * BS + p] = t;
+            }
+        __syncthreads();
+    }
+    // inv^T: out[j][i] = M[i][j]
+    for (int t = threadIdx.x; t < BS * BS; t += THREADS) {
+        const int j = t / BS, i = t % BS;
+        out[t] = M[i * BS + j];
+    }
+}
+
+// y[p_i] = sum_j inv[i][j] x[p_j] for one block (BS threads, thread i = row i; the block's x is
+// gathered into shared memory before any y is written, so x and y may be the same vector).
+template <int BS>
+__device__ __forceinline__ void bj_apply_block(const float2* __restrict__ invT, int rows,
+                                               const int32_t* __restrict__ perm, const float2* x, float2* y) {
+    __shared__ float2 xs[BS];
+    const int i = threadIdx.x;
+    xs[i] = i < rows ? x[perm[i]] : make_float2(0.f, 0.f);
+    __syncthreads();
+    float re = 0.f, im = 0.f;
+#pragma unroll 8
+    for (int j = 0; j < BS; ++j) {
+        const float2 a = invT[j * BS + i], v = xs[j];
+        re = fmaf(a.x, v.x, fmaf(-a.y, v.y, re));
+        im = fmaf(a.x, v.y, fmaf(a.y, v.x, im));
+    }
+    if (i < rows) y[perm[i]] = make_float2(re, im);
+}
+
+}  // namespace sb

@@ -75,6 +75,11 @@ class SweepBatch:
         the first solve after each assembly; pair with IrConfig(inner_tolerance=1e-3))."""
         check(L.load().sb_batch_set_inner_precision(self.handle, int(inner)))
 
+    def set_inner_preconditioner(self, kind: int, block_size: int = 64) -> None:
+        """SB_INNER_PRECOND_NONE or SB_INNER_PRECOND_BLOCK_JACOBI (blocks of block_size spatially
+        close elements per instance, inverted by the first solve after each assembly)."""
+        check(L.load().sb_batch_set_inner_preconditioner(self.handle, int(kind), int(block_size)))
+
     def set_rhs_plane_wave(self, direction=(0.0, 0.0, 1.0)) -> None:
         d = np.ascontiguousarray(direction, np.float64)
         check(L.load().sb_batch_set_rhs_plane_wave(self.handle, _p(d)))

@@ -296,3 +296,48 @@ def test_batch_half_inner_matches_single_instance(gpu, oracle):
     with pytest.raises(gpu.SoniumError):
         batch.set_inner_precision(5)
     batch.close()
+
+
+def test_batch_block_jacobi_matches_single_instance(gpu, oracle):
+    """SB_INNER_PRECOND_BLOCK_JACOBI on a batch (FP32 and complex-half inner products): every
+    instance converges to the batch's unpreconditioned solution with no more inner iterations;
+    instance 4 matches the single-instance preconditioned solve; inner restarts (inner_restart 8)
+    take the preconditioned residual; an odd size covers the partial last block."""
+    from sonium_b200.sweep import SweepBatch
+
+    meshes, phys, betas = _instances(gpu, oracle, SPEC)
+    nodes, tris = oracle.icosphere(1.0, 2, (1.0, 0.6, 0.4))
+    meshes.append(gpu.Mesh(nodes, tris[:-1]))
+    ph = gpu.PhysicsParams.for_wavenumber(1.7)
+    phys.append(ph)
+    betas.append(ph.burton_miller_beta())
+    batch = SweepBatch(meshes, phys, betas)
+    batch.assemble()
+    batch.set_rhs_plane_wave([0.0, 0.0, 1.0])
+    for inner, tol in ((gpu.SB_INNER_FP32, 1e-5), (gpu.SB_INNER_FP16, 1e-3)):
+        batch.set_inner_precision(inner)
+        batch.set_inner_preconditioner(gpu.SB_INNER_PRECOND_NONE, 64)
+        cfg = gpu.IrConfig(tolerance=1e-8, inner_tolerance=tol)
+        s0 = batch.solve(cfg)
+        x0 = [batch.solution(i) for i in range(len(batch))]
+        for bs, restart in ((64, 50), (32, 8)):
+            batch.set_inner_preconditioner(gpu.SB_INNER_PRECOND_BLOCK_JACOBI, bs)
+            cfg_b = gpu.IrConfig(tolerance=1e-8, inner_tolerance=tol, inner_restart=restart)
+            s1 = batch.solve(cfg_b)
+            for i in range(len(batch)):
+                assert s1[i].converged and s1[i].residual < 1e-8, (i, s1[i])
+                assert np.linalg.norm(batch.solution(i) - x0[i]) / np.linalg.norm(x0[i]) < 1e-6, i
+            if restart == 50:
+                assert sum(s.iterations for s in s1) < sum(s.iterations for s in s0)
+                m, ph_i, be = meshes[4], phys[4], betas[4]
+                b = gpu.rhs_plane_wave(m, ph_i, be, [0, 0, 1])[:, 0]
+                op = gpu.build_tbem_system_with_beta(m, ph_i, be, precision=gpu.SB_PRECISION_FP32)
+                op.set_inner_precision(inner)
+                op.set_inner_preconditioner(gpu.SB_INNER_PRECOND_BLOCK_JACOBI, bs)
+                single = gpu.gmres_mixed(op, b, cfg_b)
+                assert abs(s1[4].iterations - single.iterations) <= max(2, single.iterations // 10)
+                assert np.linalg.norm(batch.solution(4) - single.x) / np.linalg.norm(single.x) < 1e-6
+                op.close()
+    with pytest.raises(gpu.SoniumError):
+        batch.set_inner_preconditioner(gpu.SB_INNER_PRECOND_BLOCK_JACOBI, 100)
+    batch.close()
