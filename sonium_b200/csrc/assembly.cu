@@ -2632,8 +2632,9 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     // Near pairs and self terms write entries disjoint from the far tiles. With the FP64 far kernel
     // they run on the side stream, concurrently with it (N = 20480: 38.9 -> 37.3 ms per assembly);
     // the FP32 far kernel fills every SM's register file (3 CTAs x 128 threads x 168 registers),
-    // so a concurrent near kernel only time-shares with it (14.13 ms either way) and they run in
-    // sequence on the operator's stream. The right-hand-side reduction waits for both.
+    // so a concurrent near kernel only time-shares with it (14.13 ms either way; capping the far
+    // kernel at 2 CTAs per SM to make room for near CTAs gave 15.53 ms) and they run in sequence
+    // on the operator's stream. The right-hand-side reduction waits for both.
     const bool overlap = !mixed;
     if (overlap) {
         op.side.ensure();
