@@ -765,19 +765,20 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             const float nxny = nxx * nyx + nxy * nyy + nxz * nyz;
             const float fny = fx * nyx + fy * nyy + fz * nyz;       // d_c . n_y
             const float fnx = -(fx * nxx + fy * nxy + fz * nxz);    // -d_c . n_x
-            // Points in pairs: lane sums AGR = sum g_r, NAHR = -sum b_r r.n_y, NATR = -sum b_r (-r.n_x),
-            // AER - AEX = sum (g_r f_r - g_i f_i), with b = g (-1/r + i k) and the E factor f below.
-            const float2 FX = bc2(fx), FY = bc2(fy), FZ = bc2(fz), RC2 = bc2(rc2f), RC = bc2(rcf), KK = bc2(kf);
+            // Points in pairs. With b = g (-1/r + i k) = -(u + i nbi), u = g_r / r + g_i k and
+            // nbi = g_i / r - g_r k, and the E factor f = (3 rq + nx.ny)(1/r)(1/r - i k) - k^2 rq:
+            //   H = -sum (u + i nbi) r.n_y, H^T = -sum (u + i nbi)(-r.n_x),
+            //   E = sum q1 (u + i nbi) - k^2 sum g rq, q1 = (3 rq + nx.ny) / r,
+            // so every channel is a lane sum of one fma per point and the k factors apply once.
+            const float2 FX2 = bc2(2.f * fx), FY2 = bc2(2.f * fy), FZ2 = bc2(2.f * fz);
+            const float2 RC2 = bc2(rc2f), RC = bc2(rcf), KK = bc2(kf), NK = bc2(-kf);
             const float2 FNY = bc2(fny), FNX = bc2(fnx), NXX = bc2(nxx), NXY = bc2(nxy), NXZ = bc2(nxz);
-            const float2 NXNY = bc2(nxny), NK2 = bc2(-k2f), NK = bc2(-kf), M1 = bc2(-1.f);
+            const float2 NXNY = bc2(nxny), M1 = bc2(-1.f), THREE = bc2(3.f);
             const float2 Z = bc2(0.f);
-            float2 AGR = Z, AGI = Z, NAHR = Z, AHI = Z, NATR = Z, ATI = Z, AER = Z, AEX = Z, AEI = Z;
+            float2 AGR = Z, AGI = Z, NAHR = Z, NAHI = Z, NATR = Z, NATI = Z, AER = Z, AEI = Z, GQR = Z, GQI = Z;
 #pragma unroll
             for (int p = 0; p < kFarPairs; ++p) {
-                float2 d = pmul(FX, PX[p]);
-                d = pfma(FY, PY[p], d);
-                d = pfma(FZ, PZ[p], d);
-                const float2 num = pfma(bc2(2.f), d, PD[p]);
+                const float2 num = pfma(FX2, PX[p], pfma(FY2, PY[p], pfma(FZ2, PZ[p], PD[p])));
                 const float2 rq2 = padd(RC2, num);
                 const float2 rinv = make_float2(rsqrtf(rq2.x), rsqrtf(rq2.y));
                 const float2 den = pfma(rq2, rinv, RC);
@@ -795,29 +796,31 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                 const float2 gs = pmul(PW[p], rinv);
                 const float2 gr = pmul(C, gs), gi = pmul(S, gs);
                 const float2 rny = pmul(padd(FNY, PN[p]), rinv);
-                float2 pnx = pmul(PX[p], NXX);
-                pnx = pfma(PY[p], NXY, pnx);
-                pnx = pfma(PZ[p], NXZ, pnx);
+                const float2 pnx = pfma(PZ[p], NXZ, pfma(PY[p], NXY, pmul(PX[p], NXX)));
                 const float2 rnx = pmul(pfma(pnx, M1, FNX), rinv);
-                const float2 u = pfma(gr, rinv, pmul(gi, KK));           // -b_r
-                const float2 bi = pfma(gi, pmul(rinv, M1), pmul(gr, KK));  // b_i
+                const float2 u = pfma(gr, rinv, pmul(gi, KK));
+                const float2 nbi = pfma(gi, rinv, pmul(gr, NK));
                 AGR = padd(AGR, gr);
                 AGI = padd(AGI, gi);
                 NAHR = pfma(u, rny, NAHR);
-                AHI = pfma(bi, rny, AHI);
+                NAHI = pfma(nbi, rny, NAHI);
                 NATR = pfma(u, rnx, NATR);
-                ATI = pfma(bi, rnx, ATI);
-                // E factor: f = ((3/r^2 - k^2) rq + nx.ny / r^2, -(k / r) (3 rq + nx.ny))
+                NATI = pfma(nbi, rnx, NATI);
                 const float2 rqq = pmul(rny, rnx);
-                const float2 s3 = pfma(bc2(3.f), rqq, NXNY);
-                const float2 fr = pfma(pmul(rinv, rinv), s3, pmul(NK2, rqq));
-                const float2 fi = pmul(pmul(NK, rinv), s3);
-                AER = pfma(gr, fr, AER);
-                AEX = pfma(gi, fi, AEX);
-                AEI = pfma(gr, fi, pfma(gi, fr, AEI));
+                const float2 q1 = pmul(rinv, pfma(THREE, rqq, NXNY));
+                AER = pfma(q1, u, AER);
+                AEI = pfma(q1, nbi, AEI);
+                GQR = pfma(gr, rqq, GQR);
+                GQI = pfma(gi, rqq, GQI);
             }
-            Far32Sums sm{AGR.x + AGR.y, AGI.x + AGI.y, -(NAHR.x + NAHR.y), AHI.x + AHI.y, -(NATR.x + NATR.y),
-                         ATI.x + ATI.y, (AER.x + AER.y) - (AEX.x + AEX.y), AEI.x + AEI.y};
+            Far32Sums sm{AGR.x + AGR.y,
+                         AGI.x + AGI.y,
+                         -(NAHR.x + NAHR.y),
+                         -(NAHI.x + NAHI.y),
+                         -(NATR.x + NATR.y),
+                         -(NATI.x + NATI.y),
+                         (AER.x + AER.y) - k2f * (GQR.x + GQR.y),
+                         (AEI.x + AEI.y) - k2f * (GQI.x + GQI.y)};
             far32_point(sm, lx, ly, lz, ld_, lw, ln, fx, fy, fz, rc2f, rcf, kf, k2f, fny, fnx, nxx, nxy, nxz, nxny);
             const float ag_r = sm.gr, ag_i = sm.gi, ah_r = sm.hr, ah_i = sm.hi, at_r = sm.tr, at_i = sm.ti,
                         ae_r = sm.er, ae_i = sm.ei;
