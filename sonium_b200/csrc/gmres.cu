@@ -69,9 +69,13 @@ template <class T>
 struct KrylovWork {
     int64_t n = 0, m = 0, ldv = 0;
     DevBuf V, w, opb, r, part, red, red2, nrm, ydev, H, cs, sn, g, st;
-    PinnedBuf host;  // KState + two doubles
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    PinnedBuf host;  // KState + two doubles, then two KState slots of the chunk checks
+    // The cycle is captured as chunks of kCycleChunk Arnoldi steps (one graph each), launched
+    // while the cycle is still active, so a converged cycle stops paying for gated launches.
+    std::vector<cudaGraph_t> graphs;
+    std::vector<cudaGraphExec_t> execs;
+    std::vector<int64_t> chunk_kernels;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
     const void* key_A = nullptr;
     const void* key_jac = nullptr;  // the Jacobi diagonal the cycle reads, if any
     const void* key_pre = nullptr;  // the block-Jacobi inverses the cycle reads, if any
@@ -79,16 +83,22 @@ struct KrylovWork {
     int key_jacobi = -1;
     unsigned key_prof = 0;
     std::vector<ProfPair> prof_pairs;
-    int64_t graph_kernels = 0;
 
     void reset_graph() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
+        for (cudaGraphExec_t e : execs)
+            if (e) cudaGraphExecDestroy(e);
+        for (cudaGraph_t g : graphs)
+            if (g) cudaGraphDestroy(g);
+        execs.clear();
+        graphs.clear();
+        chunk_kernels.clear();
         profile_release(prof_pairs);
     }
-    ~KrylovWork() { reset_graph(); }
+    ~KrylovWork() {
+        reset_graph();
+        for (cudaEvent_t& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
 
     void ensure(int64_t n_, int64_t m_) {
         if (n_ == n && m_ == m) return;
@@ -111,9 +121,14 @@ struct KrylovWork {
         sn.alloc(sizeof(double2) * m);
         g.alloc(sizeof(double2) * (m + 1));
         st.alloc(sizeof(KState));
-        host.alloc(sizeof(KState) + 64);
+        host.alloc(3 * sizeof(KState) + 64);
+        for (cudaEvent_t& e : ev)
+            if (!e) SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     KState* hstate() { return static_cast<KState*>(host.p); }
+    KState* hslot(int i) {
+        return reinterpret_cast<KState*>(static_cast<char*>(host.p) + sizeof(KState) + 64) + i;
+    }
     double* hscalar() { return reinterpret_cast<double*>(static_cast<char*>(host.p) + sizeof(KState)); }
 };
 
@@ -241,9 +256,9 @@ struct CoreResult {
     const void* r_last = nullptr;  // device b - A x for the returned x, when one was formed
 };
 
-// All Arnoldi steps of one cycle, every launch gated by st->active.
+// Arnoldi steps [j0, j1) of one cycle, every launch gated by st->active.
 template <class T>
-void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
+void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t j0, int64_t j1) {
     const int64_t n = P.n;
     const cudaStream_t s = P.stream;
     KState* st = W.st.template as<KState>();
@@ -252,7 +267,7 @@ void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
     T* Vp = W.V.template as<T>();
     T* w = W.w.template as<T>();
     double* nrm = W.nrm.template as<double>();
-    for (int64_t j = 0; j < m; ++j) {
+    for (int64_t j = j0; j < j1; ++j) {
         capture_step(static_cast<int>(j));
         const int k = static_cast<int>(j + 1);
         if (P.jacobi) {
@@ -277,30 +292,42 @@ void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
     SB_CUDA(cudaGetLastError());
 }
 
-// Replays the captured cycle (capturing it first when buffers, matrix or profiling changed).
+// Steps per captured chunk of a restart cycle.
+constexpr int64_t kCycleChunk = 8;
+
+// Replays the captured cycle (capturing it first when buffers, matrix or profiling changed):
+// chunk c + 1 is queued before the host reads chunk c's state, so the device never waits for the
+// host; launching stops once a chunk leaves the cycle inactive (the queued one returns at once).
 template <class T>
 void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
     const int jac = P.jacobi ? 1 : 0;
-    if (!W.exec || W.key_A != P.key_A || W.key_jacobi != jac || W.key_jac != P.jacobi || W.key_prof != prof_key() ||
-        W.key_pre != P.key_pre || W.key_pre_bs != P.key_pre_bs) {
+    const int64_t nch = (m + kCycleChunk - 1) / kCycleChunk;
+    if (W.execs.empty() || W.key_A != P.key_A || W.key_jacobi != jac || W.key_jac != P.jacobi ||
+        W.key_prof != prof_key() || W.key_pre != P.key_pre || W.key_pre_bs != P.key_pre_bs) {
         W.reset_graph();
-        const int64_t before = kernel_count();
         capture_begin(&W.prof_pairs);
-        SB_CUDA(cudaStreamBeginCapture(P.stream, cudaStreamCaptureModeThreadLocal));
-        try {
-            launch_cycle<T>(W, P, m);
-        } catch (...) {
+        for (int64_t c = 0; c < nch; ++c) {
+            const int64_t before = kernel_count();
             cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(P.stream, &g);
-            if (g) cudaGraphDestroy(g);
-            capture_end();
-            throw;
+            SB_CUDA(cudaStreamBeginCapture(P.stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                launch_cycle<T>(W, P, c * kCycleChunk, std::min(m, (c + 1) * kCycleChunk));
+            } catch (...) {
+                cudaStreamEndCapture(P.stream, &g);
+                if (g) cudaGraphDestroy(g);
+                capture_end();
+                W.reset_graph();
+                throw;
+            }
+            SB_CUDA(cudaStreamEndCapture(P.stream, &g));
+            W.graphs.push_back(g);
+            cudaGraphExec_t e = nullptr;
+            SB_CUDA(cudaGraphInstantiate(&e, g, 0));
+            W.execs.push_back(e);
+            W.chunk_kernels.push_back(kernel_count() - before);
+            add_kernel_count(-(kernel_count() - before));
         }
-        SB_CUDA(cudaStreamEndCapture(P.stream, &W.graph));
         capture_end();
-        SB_CUDA(cudaGraphInstantiate(&W.exec, W.graph, 0));
-        W.graph_kernels = kernel_count() - before;
-        add_kernel_count(-W.graph_kernels);
         W.key_A = P.key_A;
         W.key_jac = P.jacobi;
         W.key_jacobi = jac;
@@ -308,8 +335,20 @@ void run_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t m) {
         W.key_pre = P.key_pre;
         W.key_pre_bs = P.key_pre_bs;
     }
-    SB_CUDA(cudaGraphLaunch(W.exec, P.stream));
-    add_kernel_count(W.graph_kernels);
+    auto launch = [&](int64_t c) {
+        SB_CUDA(cudaGraphLaunch(W.execs[c], P.stream));
+        add_kernel_count(W.chunk_kernels[c]);
+        SB_CUDA(cudaMemcpyAsync(W.hslot(static_cast<int>(c & 1)), W.st.p, sizeof(KState), cudaMemcpyDeviceToHost,
+                                P.stream));
+        SB_CUDA(cudaEventRecord(W.ev[c & 1], P.stream));
+    };
+    launch(0);
+    if (nch > 1) launch(1);
+    for (int64_t c = 0; c + 1 < nch; ++c) {
+        SB_CUDA(cudaEventSynchronize(W.ev[c & 1]));
+        if (!W.hslot(static_cast<int>(c & 1))->active) break;
+        if (c + 2 < nch) launch(c + 2);
+    }
 }
 
 // gmres_core (gmres.rs:631-1047) with an identity or Jacobi left preconditioner.
