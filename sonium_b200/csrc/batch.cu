@@ -229,6 +229,14 @@ __global__ void __launch_bounds__(kChunk) k_bvnorm(const BInst* __restrict__ ins
     if (threadIdx.x == 0) I.pnorm[chunk] = v[0];
 }
 
+// *out = 1 when any instance still runs its Arnoldi cycle (one CTA).
+__global__ void __launch_bounds__(256) k_ball_active(const BInst* __restrict__ inst, int ninst, int* __restrict__ out) {
+    int on = 0;
+    for (int b = threadIdx.x; b < ninst; b += 256) on |= inst[b].st->active ? 1 : 0;
+    const int any = __syncthreads_or(on);
+    if (threadIdx.x == 0) *out = any;
+}
+
 // gate[g] = 1 when any instance of group g (kTensorRhsTile instances) still runs its Arnoldi
 // cycle: groups that are all done skip the step's block product.
 __global__ void __launch_bounds__(kTensorRhsTile) k_bany_active(const BInst* __restrict__ inst, int ninst,
@@ -548,9 +556,14 @@ struct Batch {
     DevBuf pool_mat, pool_rhs, pool_f32, pool_f64, pool_small, pool_state;
     DevBuf gate;  // per group of kTensorRhsTile instances: any still in the Arnoldi cycle
     cudaStream_t stream = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int64_t graph_kernels = 0;
+    // The restart cycle as graph chunks of kBatchChunk steps, launched while any instance is in
+    // its cycle (anyact: device flag, chk: its two pinned host copies, ev: their events).
+    std::vector<cudaGraph_t> graphs;
+    std::vector<cudaGraphExec_t> execs;
+    std::vector<int64_t> chunk_kernels;
+    DevBuf anyact;
+    Pinned chk;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
     unsigned graph_prof = 0;
     uint64_t graph_gen = 0;  // tensor-plane generation the captured cycle refers to
     std::vector<ProfPair> prof_pairs;
@@ -563,14 +576,19 @@ struct Batch {
     double tune_persistent_ms = 0.0, tune_streams_ms = 0.0;
     SideStream side;
     void reset_graph() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
+        for (cudaGraphExec_t e : execs)
+            if (e) cudaGraphExecDestroy(e);
+        for (cudaGraph_t g : graphs)
+            if (g) cudaGraphDestroy(g);
+        execs.clear();
+        graphs.clear();
+        chunk_kernels.clear();
         profile_release(prof_pairs);
     }
     ~Batch() {
         reset_graph();
+        for (cudaEvent_t& e : ev)
+            if (e) cudaEventDestroy(e);
         side.release();
         if (blas) cublasDestroy(blas);
         if (stream) cudaStreamDestroy(stream);
@@ -908,35 +926,64 @@ static void batch_step(Batch& B, int j) {
 
 // One restart cycle of the whole batch: m Arnoldi steps captured once into a CUDA graph.
 static void batch_cycle(Batch& B) {
+    constexpr int kBatchChunk = 8;
     const uint64_t gen = B.shared ? tensor_generation(*B.shared) : 0;
     const int pre_key = B.inner_precond * 1024 + B.bj_size;
-    if (!B.exec || B.graph_prof != prof_key() || B.graph_gen != gen || B.graph_inner != B.inner ||
+    const int nch = static_cast<int>((B.m + kBatchChunk - 1) / kBatchChunk);
+    if (B.execs.empty() || B.graph_prof != prof_key() || B.graph_gen != gen || B.graph_inner != B.inner ||
         B.graph_pre != pre_key) {
         B.reset_graph();
-        const int64_t before = kernel_count();
         capture_begin(&B.prof_pairs);
-        SB_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
-        try {
-            for (int j = 0; j < B.m; ++j) batch_step(B, j);
-        } catch (...) {
+        for (int c = 0; c < nch; ++c) {
+            const int64_t before = kernel_count();
             cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(B.stream, &g);
-            if (g) cudaGraphDestroy(g);
-            capture_end();
-            throw;
+            SB_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                for (int j = c * kBatchChunk; j < std::min<int64_t>(B.m, (c + 1) * kBatchChunk); ++j) batch_step(B, j);
+            } catch (...) {
+                cudaStreamEndCapture(B.stream, &g);
+                if (g) cudaGraphDestroy(g);
+                capture_end();
+                B.reset_graph();
+                throw;
+            }
+            SB_CUDA(cudaStreamEndCapture(B.stream, &g));
+            B.graphs.push_back(g);
+            cudaGraphExec_t e = nullptr;
+            SB_CUDA(cudaGraphInstantiate(&e, g, 0));
+            B.execs.push_back(e);
+            B.chunk_kernels.push_back(kernel_count() - before);
+            add_kernel_count(-(kernel_count() - before));
         }
-        SB_CUDA(cudaStreamEndCapture(B.stream, &B.graph));
         capture_end();
-        SB_CUDA(cudaGraphInstantiate(&B.exec, B.graph, 0));
-        B.graph_kernels = kernel_count() - before;
-        add_kernel_count(-B.graph_kernels);
         B.graph_prof = prof_key();
         B.graph_gen = gen;
         B.graph_inner = B.inner;
         B.graph_pre = pre_key;
     }
-    SB_CUDA(cudaGraphLaunch(B.exec, B.stream));
-    add_kernel_count(B.graph_kernels);
+    if (!B.anyact.p) {
+        B.anyact.alloc(sizeof(int));
+        B.chk.alloc(2 * sizeof(int));
+        for (cudaEvent_t& e : B.ev) SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    int* hchk = static_cast<int*>(B.chk.p);
+    // Chunk c + 1 is queued before the host reads chunk c's flag; launching stops once no instance
+    // is left in its cycle (the queued chunk's gated launches return at once).
+    auto launch = [&](int c) {
+        SB_CUDA(cudaGraphLaunch(B.execs[c], B.stream));
+        add_kernel_count(B.chunk_kernels[c]);
+        k_ball_active<<<1, 256, 0, B.stream>>>(B.inst_d.as<BInst>(), B.ninst, B.anyact.as<int>());
+        count_launch();
+        SB_CUDA(cudaMemcpyAsync(hchk + (c & 1), B.anyact.p, sizeof(int), cudaMemcpyDeviceToHost, B.stream));
+        SB_CUDA(cudaEventRecord(B.ev[c & 1], B.stream));
+    };
+    launch(0);
+    if (nch > 1) launch(1);
+    for (int c = 0; c + 1 < nch; ++c) {
+        SB_CUDA(cudaEventSynchronize(B.ev[c & 1]));
+        if (!hchk[c & 1]) break;
+        if (c + 2 < nch) launch(c + 2);
+    }
 }
 
 // r = b - A x for every right-hand side of a shared operator: one complex128 GEMM on the FP64
