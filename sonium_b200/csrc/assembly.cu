@@ -684,7 +684,8 @@ template <bool kWithRhs>
 __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const double* __restrict__ elem,
                                            int64_t n, int64_t ld, const double* __restrict__ coef, double k,
                                            float2* __restrict__ A32, int64_t lda32, double2* __restrict__ far_part,
-                                           int64_t n_tiles, int64_t tile, int64_t row0) {
+                                           int64_t n_tiles, int64_t tile, int64_t row0,
+                                           unsigned* __restrict__ amax = nullptr) {
     __shared__ double sx[kFar32Rows][3];
     __shared__ float snx[kFar32Rows][3];
     __shared__ double sg[4][kFarTile];    // column: level-0 centre and near threshold
@@ -743,6 +744,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
     __syncthreads();
     const float kf = static_cast<float>(k), k2f = kf * kf;
     const int64_t rows_here = (n - row0 < kFar32Rows) ? (n - row0) : kFar32Rows;
+    float vmax = 0.f;  // largest |re|, |im| this thread wrote (+inf for a non-finite part)
     for (int r = 0; r < rows_here; ++r) {
         const int64_t i = row0 + r;
         const double x0 = sx[r][0], x1 = sx[r][1], x2 = sx[r][2];
@@ -829,7 +831,10 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             const float ur = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
             const float ui = ag_r * cgi + ag_i * cgr + ah_r * chi + ah_i * chr + at_r * cti + at_i * ctr + ae_r * cei + ae_i * cer;
             // rotate by the pair phase exp(i k r_c) = (cc, sc)
-            A32[i * lda32 + j] = make_float2(ur * cc - ui * sc, ur * sc + ui * cc);
+            const float2 v = make_float2(ur * cc - ui * sc, ur * sc + ui * cc);
+            A32[i * lda32 + j] = v;
+            const float av = fmaxf(fabsf(v.x), fabsf(v.y));
+            vmax = (av <= 3.4e38f) ? fmaxf(vmax, av) : INFINITY;
             if (kWithRhs) {
                 Acc a;
                 a.gr = ag_r * cc - ag_i * sc; a.gi = ag_r * sc + ag_i * cc;
@@ -857,6 +862,14 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             __syncthreads();
         }
     }
+    // The largest part written, for the scale of the complex-half copy (one atomic per warp
+    // whose maximum exceeds the running one).
+    if (amax) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        if ((tid & 31) == 0 && __float_as_uint(vmax) > *reinterpret_cast<volatile unsigned*>(amax))
+            atomicMax(amax, __float_as_uint(vmax));
+    }
 }
 
 template <bool kWithRhs>
@@ -864,9 +877,30 @@ __global__ void __launch_bounds__(kFarTile, kFar32MinBlocks) k_far32(const float
                                                     const double* __restrict__ elem, int64_t n,
                                                     int64_t ld, const double* __restrict__ coef,
                                                     double k, float2* __restrict__ A32, int64_t lda32,
-                                                    double2* __restrict__ far_part, int64_t n_tiles) {
+                                                    double2* __restrict__ far_part, int64_t n_tiles,
+                                                    unsigned* __restrict__ amax) {
     far32_tile<kWithRhs>(qp32, elem, n, ld, coef, k, A32, lda32, far_part, n_tiles, blockIdx.x,
-                         blockIdx.y * (int64_t)kFar32Rows);
+                         blockIdx.y * (int64_t)kFar32Rows, amax);
+}
+
+// Largest |re|, |im| of the near-pair and diagonal entries of the complex64 matrix (the far
+// kernel covers the rest), atomically maxed into *amax as float bits.
+__global__ void __launch_bounds__(256) k_near_absmax(const float2* __restrict__ A32, int64_t lda32, int64_t n,
+                                                     const int64_t* __restrict__ near_ptr,
+                                                     const int32_t* __restrict__ near_col, unsigned* __restrict__ amax) {
+    float m = 0.f;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        for (int64_t p = near_ptr[i]; p <= near_ptr[i + 1]; ++p) {
+            const int64_t j = p < near_ptr[i + 1] ? near_col[p] : i;
+            const float2 v = A32[i * lda32 + j];
+            const float av = fmaxf(fabsf(v.x), fabsf(v.y));
+            m = (av <= 3.4e38f) ? fmaxf(m, av) : INFINITY;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(amax, __float_as_uint(m));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2663,14 +2697,19 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     if (mixed) {
         ProfScope prof(SB_PROF_FAR, op.stream);
         dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFar32Rows)));
+        // The far kernel also tracks the largest part it writes (the near and self entries are
+        // scanned after them): the complex-half copy's scale then needs no pass over the matrix.
+        if (!op.half_aux.p) op.half_aux.alloc(4 * sizeof(unsigned));
+        unsigned* amax = op.half_aux.as<unsigned>();
+        SB_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned), op.stream));
         if (with_rhs)
             k_far32<true><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
                                                              op.coef.as<double>(), k, A32, op.lda32,
-                                                             op.far_part.as<double2>(), m.n_tiles);
+                                                             op.far_part.as<double2>(), m.n_tiles, amax);
         else
             k_far32<false><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
                                                               op.coef.as<double>(), k, A32, op.lda32, nullptr,
-                                                              m.n_tiles);
+                                                              m.n_tiles, amax);
         count_launch();
         SB_CUDA(cudaGetLastError());
     } else {
@@ -2693,6 +2732,15 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     }
     if (overlap) op.side.end(op.stream);
     else near_and_self(op.stream);
+    if (mixed) {
+        ProfScope prof(SB_PROF_OTHER, op.stream);
+        const unsigned g = static_cast<unsigned>(std::min<int64_t>(cdiv(n, 256), 4 * device_sm_count(m.device)));
+        k_near_absmax<<<g, 256, 0, op.stream>>>(A32, op.lda32, n, m.near_ptr.as<int64_t>(), m.near_col.as<int32_t>(),
+                                                op.half_aux.as<unsigned>());
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+    }
+    op.amax_valid = mixed;
     k_rhs_reduce<<<cdiv(n, 256), 256, 0, op.stream>>>(n, ld, op.coef.as<double>(),
                                                        with_rhs ? op.self_rhs.as<double2>() : nullptr,
                                                        with_rhs ? op.far_part.as<double2>() : nullptr,
@@ -2908,7 +2956,7 @@ void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_
         ProfScope prof(SB_PROF_FAR, s);
         dim3 grid(static_cast<unsigned>(I.n_tiles), static_cast<unsigned>(cdiv(I.n, kFar32Rows)));
         k_far32<false><<<grid, kFarTile, 0, s>>>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr,
-                                                 I.n_tiles);
+                                                 I.n_tiles, nullptr);
         count_launch();
     }
     SB_CUDA(cudaGetLastError());

@@ -414,13 +414,15 @@ void half_prepare(Operator& op) {
     const cudaStream_t s = op.stream;
     unsigned* aux = op.half_aux.as<unsigned>();
     ProfScope prof(SB_PROF_OTHER, s);
-    SB_CUDA(cudaMemsetAsync(aux, 0, sizeof(unsigned), s));
     const int sms = device_sm_count(op.device);
     const unsigned grid = static_cast<unsigned>(std::min<int64_t>(n, 8 * sms));
-    k_absmax_c64<<<grid, kHalfThreads, 0, s>>>(op.A32.as<float2>(), n, op.lda32, aux);
+    if (!op.amax_valid) {  // the FP32 assembly tracks the largest part itself
+        SB_CUDA(cudaMemsetAsync(aux, 0, sizeof(unsigned), s));
+        k_absmax_c64<<<grid, kHalfThreads, 0, s>>>(op.A32.as<float2>(), n, op.lda32, aux);
+        count_launch();
+    }
     k_half_scale<<<1, 1, 0, s>>>(aux);
     k_c64_to_c16<<<grid, kHalfThreads, 0, s>>>(op.A32.as<float2>(), n, op.lda32, aux, op.A16.as<uint32_t>(), lda16);
-    count_launch();
     count_launch();
     count_launch();
     SB_CUDA(cudaGetLastError());

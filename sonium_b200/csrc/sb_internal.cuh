@@ -189,6 +189,7 @@ struct Operator {
     SideStream side;
     int64_t lda16 = 0;
     bool half_valid = false;
+    bool amax_valid = false;  // half_aux[0] holds the matrix's largest part (FP32 assembly)
     cudaStream_t stream = nullptr;
     double last_assembly_ms = 0.0;
 };

@@ -106,3 +106,26 @@ def test_half_inner_rejections(gpu):
     s = gpu.gmres_mixed(op, np.ones(8, complex), gpu.IrConfig(20, 1e-10, 50, 50, 1e-3))
     assert s.converged and np.allclose(s.x, 1.0 / 3.0, rtol=1e-9)
     op.close()
+
+
+@pytest.mark.gpu
+def test_half_scale_from_assembly_equals_full_scan(gpu):
+    # The FP32 assembly tracks the largest part while writing the matrix; a dense operator over
+    # the same complex64 matrix scans it. Equal scales give bit-identical FP16-inner solves.
+    nodes, tris = gpu.icosphere(1.0, 3, (1.0, 0.6, 0.4))
+    mesh = gpu.Mesh(nodes, tris)
+    ph = gpu.PhysicsParams.for_wavenumber(5.0)
+    beta = ph.burton_miller_beta()
+    b = gpu.rhs_plane_wave(mesh, ph, beta, [0.0, 0.0, 1.0])[:, 0]
+    op = gpu.build_tbem_system_with_beta(mesh, ph, beta, gpu.SB_PRECISION_FP32)
+    dense = gpu.DenseMatrixOperator(op.matrix_c64().astype(complex), gpu.SB_PRECISION_FP32)
+    cfg = gpu.IrConfig(20, 1e-8, 50, 50, 1e-3)
+    for o in (op, dense):
+        o.set_inner_precision(gpu.SB_INNER_FP16)
+    s1 = gpu.gmres_mixed(op, b, cfg)
+    s2 = gpu.gmres_mixed(dense, b, cfg)
+    assert s1.converged and s2.converged
+    assert s1.iterations == s2.iterations and np.array_equal(s1.x, s2.x)
+    op.close()
+    dense.close()
+    mesh.close()
