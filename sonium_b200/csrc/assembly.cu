@@ -2935,10 +2935,16 @@ void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst*
     SB_CUDA(cudaGetLastError());
 }
 
-void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_t s, SideStream& side) {
+void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_t s, SideStream& side,
+                            unsigned* amax) {
+    if (amax) SB_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned) * 4 * h_inst.size(), s));
     side.ensure();
     side.begin(s);
-    for (const BatchAsmInst& I : h_inst) {
+    int dev = 0;
+    SB_CUDA(cudaGetDevice(&dev));
+    const int sms = device_sm_count(dev);
+    for (size_t b = 0; b < h_inst.size(); ++b) {
+        const BatchAsmInst& I = h_inst[b];
         if (I.nnz > 0) {
             ProfScope prof(SB_PROF_NEAR, side.s);
             k_near<<<cdiv(I.nnz, kNearWarps), 32 * kNearWarps, 0, side.s>>>(I.elem, I.n, I.ld, I.near_ptr, I.near_col,
@@ -2950,13 +2956,19 @@ void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_
         k_self<<<cdiv(I.n, 4), 128, 0, side.s>>>(I.elem, I.n, I.ld, I.coef, I.k, nullptr, I.A32, I.lda32, nullptr,
                                                 I.diag);
         count_launch();
+        if (amax) {
+            const unsigned g = static_cast<unsigned>(std::min<int64_t>(cdiv(I.n, 256), 4 * sms));
+            k_near_absmax<<<g, 256, 0, side.s>>>(I.A32, I.lda32, I.n, I.near_ptr, I.near_col, amax + 4 * b);
+            count_launch();
+        }
     }
     SB_CUDA(cudaGetLastError());
-    for (const BatchAsmInst& I : h_inst) {
+    for (size_t b = 0; b < h_inst.size(); ++b) {
+        const BatchAsmInst& I = h_inst[b];
         ProfScope prof(SB_PROF_FAR, s);
         dim3 grid(static_cast<unsigned>(I.n_tiles), static_cast<unsigned>(cdiv(I.n, kFar32Rows)));
         k_far32<false><<<grid, kFarTile, 0, s>>>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr,
-                                                 I.n_tiles, nullptr);
+                                                 I.n_tiles, amax ? amax + 4 * b : nullptr);
         count_launch();
     }
     SB_CUDA(cudaGetLastError());

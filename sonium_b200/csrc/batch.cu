@@ -544,6 +544,7 @@ struct Batch {
     // after each assembly (SB_INNER_FP16; independent instances only).
     int inner = SB_INNER_FP32;
     bool half_valid = false;
+    bool amax_valid = false;  // pool_half_aux[4 b] holds instance b's largest part (streams assembly)
     DevBuf pool_half, pool_half_aux;
     int graph_inner = -1;
     // Block-Jacobi right preconditioner of the inner solves (independent instances only).
@@ -733,7 +734,7 @@ static void batch_half_prepare(Batch& B) {
         size_t bytes = 0;
         for (int b = 0; b < ni; ++b) bytes += round256(sizeof(uint32_t) * B.nvec[b] * ((B.nvec[b] + 3) / 4 * 4));
         B.pool_half.alloc(bytes);
-        B.pool_half_aux.alloc(sizeof(unsigned) * 4 * ni);
+        if (!B.pool_half_aux.p) B.pool_half_aux.alloc(sizeof(unsigned) * 4 * ni);
         for (int b = 0; b < ni; ++b) half_pointers(B, b, B.h[b]);
         h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
     }
@@ -741,11 +742,14 @@ static void batch_half_prepare(Batch& B) {
     const BInst* I = B.inst_d.as<BInst>();
     const unsigned g16 = static_cast<unsigned>(B.pre16.back());
     ProfScope prof(SB_PROF_OTHER, s);
-    SB_CUDA(cudaMemsetAsync(B.pool_half_aux.p, 0, sizeof(unsigned) * 4 * ni, s));
-    k_bhalf_absmax<<<g16, kHalfThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni);
+    if (!B.amax_valid) {
+        SB_CUDA(cudaMemsetAsync(B.pool_half_aux.p, 0, sizeof(unsigned) * 4 * ni, s));
+        k_bhalf_absmax<<<g16, kHalfThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni);
+        count_launch();
+    }
     k_bhalf_scale<<<static_cast<unsigned>(cdiv64(ni, 64)), 64, 0, s>>>(I, ni);
     k_bhalf_convert<<<g16, kHalfThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni);
-    for (int t = 0; t < 3; ++t) count_launch();
+    for (int t = 0; t < 2; ++t) count_launch();
     SB_CUDA(cudaGetLastError());
     B.half_valid = true;
 }
@@ -1467,10 +1471,16 @@ SB_API int sb_batch_assemble(sb_batch* batch) {
             for (int i = 0; i < B.ninst; ++i)
                 coefficients_for(*B.meshes[i], B.phys[i], B.beta[i].x, B.beta[i].y,
                                  const_cast<double*>(B.asm_h[i].coef), B.stream);
-            if (form == SB_BATCH_ASM_PERSISTENT)
+            if (form == SB_BATCH_ASM_PERSISTENT) {
                 assemble_batch(B.asm_h, B.asm_d.as<BatchAsmInst>(), B.pre_asm, B.stream, B.device);
-            else
-                assemble_batch_streams(B.asm_h, B.stream, B.side);
+                B.amax_valid = false;
+            } else {
+                // With complex-half inner products the kernels also record each matrix's largest part.
+                const bool track = B.inner == SB_INNER_FP16;
+                if (track && !B.pool_half_aux.p) B.pool_half_aux.alloc(sizeof(unsigned) * 4 * B.ninst);
+                assemble_batch_streams(B.asm_h, B.stream, B.side, track ? B.pool_half_aux.as<unsigned>() : nullptr);
+                B.amax_valid = track;
+            }
             SB_CUDA(cudaEventRecord(e1, B.stream));
             SB_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -1525,6 +1535,7 @@ SB_API int sb_batch_set_inner_precision(sb_batch* batch, int inner) {
             B.pool_half.release();
             B.pool_half_aux.release();
             B.half_valid = false;
+            B.amax_valid = false;
             if (!B.h.empty()) {
                 SB_CUDA(cudaSetDevice(B.device));
                 for (int b = 0; b < B.ninst; ++b) half_pointers(B, b, B.h[b]);

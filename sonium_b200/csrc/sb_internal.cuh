@@ -211,7 +211,10 @@ void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst*
                     cudaStream_t s, int device);
 // The same batch as per-instance launches: far tiles on s, near pairs and self terms on the side
 // stream (same device functions, so the same entries).
-void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_t s, SideStream& side);
+// With amax, instance b's largest matrix part lands in amax[4 b] (float bits; the complex-half
+// copies' scales then need no scan).
+void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_t s, SideStream& side,
+                            unsigned* amax = nullptr);
 void coefficients_for(const Mesh& m, const sb_physics& ph, double beta_re, double beta_im, double* coef,
                       cudaStream_t s);
 int coefficient_fields();
