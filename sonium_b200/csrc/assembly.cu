@@ -20,6 +20,7 @@
 #include <mutex>
 
 #include "sb_device.cuh"
+#include "sb_gemv.cuh"
 #include "sb_internal.cuh"
 #include "sb_profile.cuh"
 
@@ -685,7 +686,10 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                                            int64_t n, int64_t ld, const double* __restrict__ coef, double k,
                                            float2* __restrict__ A32, int64_t lda32, double2* __restrict__ far_part,
                                            int64_t n_tiles, int64_t tile, int64_t row0,
-                                           unsigned* __restrict__ amax = nullptr) {
+                                           unsigned* __restrict__ amax = nullptr, uint32_t* __restrict__ A16 = nullptr,
+                                           int64_t lda16 = 0, const float* __restrict__ hscale = nullptr,
+                                           int* __restrict__ hflag = nullptr) {
+    __shared__ float shs[kFar32Rows];  // the rows' complex-half scales (with A16)
     __shared__ double sx[kFar32Rows][3];
     __shared__ float snx[kFar32Rows][3];
     __shared__ double sg[4][kFarTile];    // column: level-0 centre and near threshold
@@ -700,6 +704,8 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
         sx[r][c] = (i < n) ? E(ECX + c, i) : 0.0;
         snx[r][c] = (i < n) ? static_cast<float>(E(ENX + c, i)) : 0.f;
     }
+    if (A16)
+        for (int r = tid; r < kFar32Rows; r += kFarTile) shs[r] = (row0 + r < n) ? hscale[row0 + r] : 1.f;
     // The column's 13 points in registers: points 2p, 2p + 1 in the lanes of pair p, the 13th alone.
     float2 PX[kFarPairs], PY[kFarPairs], PZ[kFarPairs], PD[kFarPairs], PW[kFarPairs], PN[kFarPairs];
     float lx, ly, lz, ld_, lw, ln;
@@ -745,6 +751,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
     const float kf = static_cast<float>(k), k2f = kf * kf;
     const int64_t rows_here = (n - row0 < kFar32Rows) ? (n - row0) : kFar32Rows;
     float vmax = 0.f;  // largest |re|, |im| this thread wrote (+inf for a non-finite part)
+    int hbad = 0;      // a complex-half entry this thread wrote left the FP16 range
     for (int r = 0; r < rows_here; ++r) {
         const int64_t i = row0 + r;
         const double x0 = sx[r][0], x1 = sx[r][1], x2 = sx[r][2];
@@ -835,6 +842,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             A32[i * lda32 + j] = v;
             const float av = fmaxf(fabsf(v.x), fabsf(v.y));
             vmax = (av <= 3.4e38f) ? fmaxf(vmax, av) : INFINITY;
+            if (A16) A16[i * lda16 + j] = half_pack(v, shs[r], &hbad);
             if (kWithRhs) {
                 Acc a;
                 a.gr = ag_r * cc - ag_i * sc; a.gi = ag_r * sc + ag_i * cc;
@@ -870,6 +878,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
         if ((tid & 31) == 0 && __float_as_uint(vmax) > *reinterpret_cast<volatile unsigned*>(amax))
             atomicMax(amax, __float_as_uint(vmax));
     }
+    if (A16 && __any_sync(0xffffffffu, hbad) && (tid & 31) == 0) atomicOr(hflag, 1);
 }
 
 template <bool kWithRhs>
@@ -878,9 +887,47 @@ __global__ void __launch_bounds__(kFarTile, kFar32MinBlocks) k_far32(const float
                                                     int64_t ld, const double* __restrict__ coef,
                                                     double k, float2* __restrict__ A32, int64_t lda32,
                                                     double2* __restrict__ far_part, int64_t n_tiles,
-                                                    unsigned* __restrict__ amax) {
+                                                    unsigned* __restrict__ amax, uint32_t* __restrict__ A16,
+                                                    int64_t lda16, const float* __restrict__ hscale,
+                                                    int* __restrict__ hflag) {
     far32_tile<kWithRhs>(qp32, elem, n, ld, coef, k, A32, lda32, far_part, n_tiles, blockIdx.x,
-                         blockIdx.y * (int64_t)kFar32Rows, amax);
+                         blockIdx.y * (int64_t)kFar32Rows, amax, A16, lda16, hscale, hflag);
+}
+
+// Complex-half copy during the FP32 assembly (after the near and self kernels): each row's scale
+// from its near and diagonal entries (the largest of a row on resolved meshes), then those
+// entries' FP16 values; the far kernel converts the rest with the same scales. Thread per row.
+__global__ void __launch_bounds__(256) k_near_row_scale(const float2* __restrict__ A32, int64_t lda32, int64_t n,
+                                                        const int64_t* __restrict__ near_ptr,
+                                                        const int32_t* __restrict__ near_col, float* __restrict__ s,
+                                                        float* __restrict__ inv) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float m = 0.f;
+    for (int64_t p = near_ptr[i]; p <= near_ptr[i + 1]; ++p) {
+        const int64_t j = p < near_ptr[i + 1] ? near_col[p] : i;
+        const float2 v = A32[i * lda32 + j];
+        const float av = fmaxf(fabsf(v.x), fabsf(v.y));
+        m = (av <= 3.4e38f) ? fmaxf(m, av) : INFINITY;
+    }
+    const float sc = half_scale_for(m);
+    s[i] = sc;
+    inv[i] = 1.f / sc;
+}
+__global__ void __launch_bounds__(256) k_near_to_half(const float2* __restrict__ A32, int64_t lda32, int64_t n,
+                                                      const int64_t* __restrict__ near_ptr,
+                                                      const int32_t* __restrict__ near_col,
+                                                      const float* __restrict__ s, uint32_t* __restrict__ A16,
+                                                      int64_t lda16, int* __restrict__ hflag) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float sc = s[i];
+    int bad = 0;
+    for (int64_t p = near_ptr[i]; p <= near_ptr[i + 1]; ++p) {
+        const int64_t j = p < near_ptr[i + 1] ? near_col[p] : i;
+        A16[i * lda16 + j] = half_pack(A32[i * lda32 + j], sc, &bad);
+    }
+    if (bad) atomicOr(hflag, 1);
 }
 
 // Largest |re|, |im| of the near-pair and diagonal entries of the complex64 matrix (the far
@@ -2670,8 +2717,8 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     // they run on the side stream, concurrently with it (N = 20480: 38.9 -> 37.3 ms per assembly);
     // the FP32 far kernel fills every SM's register file (3 CTAs x 128 threads x 168 registers),
     // so a concurrent near kernel only time-shares with it (14.13 ms either way; capping the far
-    // kernel at 2 CTAs per SM to make room for near CTAs gave 15.53 ms) and they run in sequence
-    // on the operator's stream. The right-hand-side reduction waits for both.
+    // kernel at 2 CTAs per SM to make room for near CTAs gave 15.53 ms) and they run before it on
+    // the operator's stream. The right-hand-side reduction waits for both.
     const bool overlap = !mixed;
     if (overlap) {
         op.side.ensure();
@@ -2695,23 +2742,48 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     };
     if (overlap) near_and_self(op.side.s);
     if (mixed) {
-        ProfScope prof(SB_PROF_FAR, op.stream);
-        dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFar32Rows)));
-        // The far kernel also tracks the largest part it writes (the near and self entries are
-        // scanned after them): the complex-half copy's scale then needs no pass over the matrix.
-        if (!op.half_aux.p) op.half_aux.alloc(4 * sizeof(unsigned));
-        unsigned* amax = op.half_aux.as<unsigned>();
-        SB_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned), op.stream));
-        if (with_rhs)
-            k_far32<true><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
-                                                             op.coef.as<double>(), k, A32, op.lda32,
-                                                             op.far_part.as<double2>(), m.n_tiles, amax);
-        else
-            k_far32<false><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
-                                                              op.coef.as<double>(), k, A32, op.lda32, nullptr,
-                                                              m.n_tiles, amax);
-        count_launch();
-        SB_CUDA(cudaGetLastError());
+        // Near pairs and self terms first; with complex-half inner products the rows' scales come
+        // from those entries and the far kernel writes the copy as it writes the matrix.
+        near_and_self(op.stream);
+        const bool half = op.inner == SB_INNER_FP16;
+        uint32_t* A16 = nullptr;
+        float* hs = nullptr;
+        int* hflag = nullptr;
+        if (half) {
+            half_alloc(op);
+            A16 = op.A16.as<uint32_t>();
+            hs = op.half_scale.as<float>();
+            hflag = op.half_flag.as<int>();
+            SB_CUDA(cudaMemsetAsync(hflag, 0, sizeof(int), op.stream));
+            ProfScope prof(SB_PROF_OTHER, op.stream);
+            k_near_row_scale<<<cdiv(n, 256), 256, 0, op.stream>>>(A32, op.lda32, n, m.near_ptr.as<int64_t>(),
+                                                                  m.near_col.as<int32_t>(), hs, hs + n);
+            count_launch();
+        }
+        {
+            ProfScope prof(SB_PROF_FAR, op.stream);
+            dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFar32Rows)));
+            if (with_rhs)
+                k_far32<true><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
+                                                                 op.coef.as<double>(), k, A32, op.lda32,
+                                                                 op.far_part.as<double2>(), m.n_tiles, nullptr, A16,
+                                                                 op.lda16, hs, hflag);
+            else
+                k_far32<false><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
+                                                                  op.coef.as<double>(), k, A32, op.lda32, nullptr,
+                                                                  m.n_tiles, nullptr, A16, op.lda16, hs, hflag);
+            count_launch();
+            SB_CUDA(cudaGetLastError());
+        }
+        if (half) {
+            ProfScope prof(SB_PROF_OTHER, op.stream);
+            k_near_to_half<<<cdiv(n, 256), 256, 0, op.stream>>>(A32, op.lda32, n, m.near_ptr.as<int64_t>(),
+                                                                m.near_col.as<int32_t>(), hs, A16, op.lda16, hflag);
+            count_launch();
+            SB_CUDA(cudaGetLastError());
+            op.half_valid = true;
+            op.half_check = true;
+        }
     } else {
         ProfScope prof(SB_PROF_FAR, op.stream);
         dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFarRows)));
@@ -2731,16 +2803,6 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
         SB_CUDA(cudaGetLastError());
     }
     if (overlap) op.side.end(op.stream);
-    else near_and_self(op.stream);
-    if (mixed) {
-        ProfScope prof(SB_PROF_OTHER, op.stream);
-        const unsigned g = static_cast<unsigned>(std::min<int64_t>(cdiv(n, 256), 4 * device_sm_count(m.device)));
-        k_near_absmax<<<g, 256, 0, op.stream>>>(A32, op.lda32, n, m.near_ptr.as<int64_t>(), m.near_col.as<int32_t>(),
-                                                op.half_aux.as<unsigned>());
-        count_launch();
-        SB_CUDA(cudaGetLastError());
-    }
-    op.amax_valid = mixed;
     k_rhs_reduce<<<cdiv(n, 256), 256, 0, op.stream>>>(n, ld, op.coef.as<double>(),
                                                        with_rhs ? op.self_rhs.as<double2>() : nullptr,
                                                        with_rhs ? op.far_part.as<double2>() : nullptr,
@@ -2968,7 +3030,8 @@ void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_
         ProfScope prof(SB_PROF_FAR, s);
         dim3 grid(static_cast<unsigned>(I.n_tiles), static_cast<unsigned>(cdiv(I.n, kFar32Rows)));
         k_far32<false><<<grid, kFarTile, 0, s>>>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr,
-                                                 I.n_tiles, amax ? amax + 4 * b : nullptr);
+                                                 I.n_tiles, amax ? amax + 4 * b : nullptr, nullptr, 0, nullptr,
+                                                 nullptr);
         count_launch();
     }
     SB_CUDA(cudaGetLastError());

@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(THREADS) k_gemv_n_c16(const uint32_t* __restri
                                                         const float2* __restrict__ b, double* __restrict__ part,
                                                         Gate gate) {
     if (closed(gate)) return;
-    gemv_c16_block<ROWS, THREADS, UNROLL>(A, n, lda, inv_scale, x, y, b, part, blockIdx.x);
+    gemv_c16_block<ROWS, THREADS, UNROLL, true>(A, n, lda, inv_scale, x, y, b, part, blockIdx.x);
 }
 
 int64_t gemv16_partials(int64_t n) { return cdiv(n, kGemv16Rows); }
@@ -386,22 +386,98 @@ void gemv_c16(const uint32_t* A, int64_t n, int64_t lda, const float* inv_scale,
     SB_CUDA(cudaGetLastError());
 }
 
-__global__ void __launch_bounds__(kHalfThreads) k_absmax_c64(const float2* __restrict__ A, int64_t n, int64_t lda,
-                                                             unsigned* __restrict__ out) {
-    half_absmax_rows(A, n, lda, blockIdx.x, n, gridDim.x, out);
+// Per-row scales of a complex64 matrix: one CTA per row (grid-stride) takes the row's largest
+// |re|, |im| and writes its power-of-two scale s[row] and inverse inv[row].
+__global__ void __launch_bounds__(kHalfThreads) k_row_scale_full(const float2* __restrict__ A, int64_t n,
+                                                                 int64_t lda, float* __restrict__ s,
+                                                                 float* __restrict__ inv) {
+    __shared__ float red[kHalfThreads / 32];
+    for (int64_t row = blockIdx.x; row < n; row += gridDim.x) {
+        float m = 0.f;
+        const float4* r4 = reinterpret_cast<const float4*>(A + row * lda);  // lda even
+        for (int64_t c = threadIdx.x; c < (n >> 1); c += kHalfThreads) {
+            const float4 v = __ldcs(r4 + c);
+            const float a = fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
+            m = (a <= 3.4e38f) ? fmaxf(m, a) : INFINITY;
+        }
+        if ((n & 1) && threadIdx.x == 0) {
+            const float2 v = A[row * lda + n - 1];
+            const float a = fmaxf(fabsf(v.x), fabsf(v.y));
+            m = (a <= 3.4e38f) ? fmaxf(m, a) : INFINITY;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < kHalfThreads / 32; ++w) m = fmaxf(m, red[w]);
+            const float sc = half_scale_for(m);
+            s[row] = sc;
+            inv[row] = 1.f / sc;
+        }
+        __syncthreads();
+    }
 }
 
-__global__ void k_half_scale(unsigned* aux) { half_scale_from_max(aux); }
-
-__global__ void __launch_bounds__(kHalfThreads) k_c64_to_c16(const float2* __restrict__ A, int64_t n, int64_t lda32,
-                                                             const unsigned* __restrict__ aux,
-                                                             uint32_t* __restrict__ H, int64_t lda16) {
-    half_convert_rows(A, n, lda32, aux, H, lda16, blockIdx.x, n, gridDim.x);
+// H[row][c] = FP16(s[row] A[row][c]) for c < n, four entries a thread, one CTA per row.
+__global__ void __launch_bounds__(kHalfThreads) k_c64_to_c16_rows(const float2* __restrict__ A, int64_t n,
+                                                                  int64_t lda32, const float* __restrict__ s,
+                                                                  uint32_t* __restrict__ H, int64_t lda16) {
+    const int64_t q = lda16 >> 2;
+    for (int64_t row = blockIdx.x; row < n; row += gridDim.x) {
+        const float sc = s[row];
+        int bad = 0;
+        for (int64_t c4 = threadIdx.x; c4 < q; c4 += kHalfThreads) {
+            const int64_t c = 4 * c4;
+            float2 v[4];
+            if (c + 3 < n) {
+                const float4* p = reinterpret_cast<const float4*>(A + row * lda32 + c);  // lda32 and c even
+                const float4 a = __ldcs(p), bq = __ldcs(p + 1);
+                v[0] = make_float2(a.x, a.y);
+                v[1] = make_float2(a.z, a.w);
+                v[2] = make_float2(bq.x, bq.y);
+                v[3] = make_float2(bq.z, bq.w);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) v[j] = (c + j < n) ? A[row * lda32 + c + j] : make_float2(0.f, 0.f);
+            }
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[j] = half_pack(v[j], sc, &bad);
+            __stcs(reinterpret_cast<uint4*>(H + row * lda16 + c), make_uint4(w[0], w[1], w[2], w[3]));
+        }
+    }
 }
 
 void half_prepare(Operator& op) {
+    const cudaStream_t s = op.stream;
+    if (op.half_valid && op.half_check) {
+        // The FP32 assembly wrote the copy with scales from each row's near and diagonal entries;
+        // a far entry beyond the FP16 range (never seen on resolved meshes) sends it to the full
+        // rebuild below.
+        int bad = 0;
+        SB_CUDA(cudaMemcpyAsync(&bad, op.half_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        op.half_check = false;
+        if (bad) op.half_valid = false;
+    }
     if (op.half_valid) return;
     SB_REQUIRE(op.A32.p, SB_ERR_INVALID_ARGUMENT, "FP16 inner solve: the operator has no complex64 matrix");
+    const int64_t n = op.n;
+    half_alloc(op);
+    ProfScope prof(SB_PROF_OTHER, s);
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(n, 8 * device_sm_count(op.device)));
+    float* sc = op.half_scale.as<float>();
+    k_row_scale_full<<<grid, kHalfThreads, 0, s>>>(op.A32.as<float2>(), n, op.lda32, sc, sc + n);
+    k_c64_to_c16_rows<<<grid, kHalfThreads, 0, s>>>(op.A32.as<float2>(), n, op.lda32, sc, op.A16.as<uint32_t>(),
+                                                    op.lda16);
+    count_launch();
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    op.half_valid = true;
+}
+
+void half_alloc(Operator& op) {
     const int64_t n = op.n;
     const int64_t lda16 = (n + 3) / 4 * 4;
     const size_t bytes = sizeof(uint32_t) * static_cast<size_t>(n) * lda16;
@@ -409,24 +485,12 @@ void half_prepare(Operator& op) {
         op.A16.release();
         op.A16.alloc(bytes);
     }
-    if (!op.half_aux.p) op.half_aux.alloc(4 * sizeof(unsigned));
-    op.lda16 = lda16;
-    const cudaStream_t s = op.stream;
-    unsigned* aux = op.half_aux.as<unsigned>();
-    ProfScope prof(SB_PROF_OTHER, s);
-    const int sms = device_sm_count(op.device);
-    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(n, 8 * sms));
-    if (!op.amax_valid) {  // the FP32 assembly tracks the largest part itself
-        SB_CUDA(cudaMemsetAsync(aux, 0, sizeof(unsigned), s));
-        k_absmax_c64<<<grid, kHalfThreads, 0, s>>>(op.A32.as<float2>(), n, op.lda32, aux);
-        count_launch();
+    if (op.half_scale.bytes != sizeof(float) * 2 * n) {
+        op.half_scale.release();
+        op.half_scale.alloc(sizeof(float) * 2 * n);
     }
-    k_half_scale<<<1, 1, 0, s>>>(aux);
-    k_c64_to_c16<<<grid, kHalfThreads, 0, s>>>(op.A32.as<float2>(), n, op.lda32, aux, op.A16.as<uint32_t>(), lda16);
-    count_launch();
-    count_launch();
-    SB_CUDA(cudaGetLastError());
-    op.half_valid = true;
+    if (!op.half_flag.p) op.half_flag.alloc(sizeof(int));
+    op.lda16 = lda16;
 }
 
 template <class T>

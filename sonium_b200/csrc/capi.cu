@@ -1035,6 +1035,7 @@ SB_API int sb_operator_set_inner_precision(sb_operator* op, int inner) {
         if (inner == SB_INNER_FP32) {
             op->op->A16.release();
             op->op->half_valid = false;
+            op->op->half_check = false;
         }
     });
 }

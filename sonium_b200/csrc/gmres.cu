@@ -591,7 +591,7 @@ Problem<float2> problem16(const Operator& op) {
     P.stream = op.stream;
     P.key_A = op.A16.p;
     P.partials = gemv16_partials(op.n);
-    const float* inv = reinterpret_cast<const float*>(op.half_aux.as<unsigned>() + 2);
+    const float* inv = op.half_scale.as<float>() + op.n;  // per-row inverse scales
     P.apply = [&op, inv](const float2* xi, float2* yo, Gate g) {
         gemv_c16(op.A16.as<uint32_t>(), op.n, op.lda16, inv, xi, yo, nullptr, nullptr, op.stream, g);
     };

@@ -187,8 +187,9 @@ __device__ __forceinline__ void cmac(float& re, float& im, float2 a, float xr, f
 }
 
 // Rows [blk * ROWS, blk * ROWS + ROWS) of y = (A x) / scale, or b - (A x) / scale with part[blk]
-// = the squared norm of those rows. Called by every thread of a THREADS-wide CTA.
-template <int ROWS, int THREADS, int UNROLL>
+// = the squared norm of those rows; the inverse scale is inv_scale[row] (kRowScale) or
+// inv_scale[0]. Called by every thread of a THREADS-wide CTA.
+template <int ROWS, int THREADS, int UNROLL, bool kRowScale = false>
 __device__ __forceinline__ void gemv_c16_block(const uint32_t* __restrict__ A, int64_t n, int64_t lda,
                                                const float* __restrict__ inv_scale, const float2* __restrict__ x,
                                                float2* __restrict__ y, const float2* __restrict__ b,
@@ -253,11 +254,11 @@ __device__ __forceinline__ void gemv_c16_block(const uint32_t* __restrict__ A, i
     for (int r = 0; r < 2 * ROWS; ++r) accd[r] = acc[r];
     block_sum<2 * ROWS, THREADS>(accd, red);
     if (threadIdx.x == 0) {
-        const float inv = *inv_scale;
         double nrm = 0.0;
 #pragma unroll
         for (int r = 0; r < ROWS; ++r) {
             if (r >= nr) break;
+            const float inv = kRowScale ? inv_scale[row0 + r] : *inv_scale;
             float vr = static_cast<float>(accd[2 * r]) * inv, vi = static_cast<float>(accd[2 * r + 1]) * inv;
             if (b) {
                 const float2 bb = b[row0 + r];
@@ -315,6 +316,25 @@ __device__ __forceinline__ void half_scale_from_max(unsigned* aux) {
     }
     aux[1] = __float_as_uint(sc);
     aux[2] = __float_as_uint(1.f / sc);
+}
+
+// Power-of-two scale of a row (or matrix) whose largest |re|, |im| is m: m times the scale lies in
+// [2^13, 2^14) (exact to apply and undo, a factor 4 below FP16 overflow); 1 for m = 0 or non-finite.
+__device__ __forceinline__ float half_scale_for(float m) {
+    if (!(m > 0.f && m <= 3.4e38f)) return 1.f;
+    int e = 13 - ilogbf(m);
+    e = e < -120 ? -120 : (e > 120 ? 120 : e);
+    return ldexpf(1.f, e);
+}
+
+// FP16 (re, im) of v times sc, packed as re | im << 16; *bad |= 1 when a part leaves the FP16 range.
+__device__ __forceinline__ uint32_t half_pack(float2 v, float sc, int* bad) {
+    const float a = v.x * sc, b = v.y * sc;
+    if (!(fabsf(a) <= 65504.f && fabsf(b) <= 65504.f)) *bad = 1;
+    const __half2 h = __floats2half2_rn(a, b);
+    uint32_t w;
+    memcpy(&w, &h, sizeof(w));
+    return w;
 }
 
 // H[row][c] = FP16(scale A[row][c]) (round to nearest) for c < n, 0 for n <= c < lda16, over rows

@@ -172,10 +172,12 @@ struct Operator {
     DevBuf lin_cp, lin_cn, lin_ptr, lin_col;
     int64_t lin_nnz = 0;
     // Complex-half copy of the complex64 matrix for the inner solve of the mixed solver
-    // (SB_INNER_FP16): FP16 (re, im) pairs of the entries times a power-of-two scale, rows lda16
-    // entries apart; half_aux holds the largest part's bits, the scale and its inverse (device).
+    // (SB_INNER_FP16): FP16 (re, im) pairs of row i's entries times a power-of-two scale s_i,
+    // rows lda16 entries apart; half_scale = [s (n floats), 1 / s (n floats)]; half_flag = 1 when
+    // an entry the assembly converted left the FP16 range (checked by the first solve).
     int inner = SB_INNER_FP32;
-    DevBuf A16, half_aux;
+    DevBuf A16, half_scale, half_flag;
+    bool half_check = false;
     // Block-Jacobi preconditioner of the inner solve (SB_INNER_PRECOND_BLOCK_JACOBI): unknowns in
     // blocks of bj_size consecutive entries of bj_perm (Morton order of the element centroids),
     // the transposed inverses of the complex64 diagonal blocks in bj_inv (rebuilt after assembly).
@@ -189,7 +191,6 @@ struct Operator {
     SideStream side;
     int64_t lda16 = 0;
     bool half_valid = false;
-    bool amax_valid = false;  // half_aux[0] holds the matrix's largest part (FP32 assembly)
     cudaStream_t stream = nullptr;
     double last_assembly_ms = 0.0;
 };
@@ -258,8 +259,10 @@ void destroy_solve_work(Operator& op);
 // Frees the kept solver workspaces of `device` (all devices when device < 0).
 void solve_work_pool_trim(int device);
 struct Gate;
-// Builds the complex-half copy of the complex64 matrix on the operator's stream (blas.cu).
+// Builds the complex-half copy of the complex64 matrix on the operator's stream, unless the FP32
+// assembly wrote it (blas.cu); half_alloc sizes its buffers.
 void half_prepare(Operator& op);
+void half_alloc(Operator& op);
 // Block-Jacobi inner preconditioner (precond.cu): build the block inverses; y = M^-1 x (FP32).
 void bj_prepare(Operator& op);
 void bj_apply(const Operator& op, const float2* x, float2* y, Gate g);

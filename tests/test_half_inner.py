@@ -109,9 +109,11 @@ def test_half_inner_rejections(gpu):
 
 
 @pytest.mark.gpu
-def test_half_scale_from_assembly_equals_full_scan(gpu):
-    # The FP32 assembly tracks the largest part while writing the matrix; a dense operator over
-    # the same complex64 matrix scans it. Equal scales give bit-identical FP16-inner solves.
+def test_half_copy_from_assembly_matches_rebuilt_copy(gpu):
+    # After a re-assembly with SB_INNER_FP16 set, the FP32 assembly writes the complex-half copy
+    # itself (row scales from each row's near and diagonal entries); a dense operator over the
+    # same complex64 matrix builds its copy from full-row scans. Both inner operators carry the
+    # same complex64 matrix to FP16 rounding, so the solves agree to the solver tolerance.
     nodes, tris = gpu.icosphere(1.0, 3, (1.0, 0.6, 0.4))
     mesh = gpu.Mesh(nodes, tris)
     ph = gpu.PhysicsParams.for_wavenumber(5.0)
@@ -122,10 +124,18 @@ def test_half_scale_from_assembly_equals_full_scan(gpu):
     cfg = gpu.IrConfig(20, 1e-8, 50, 50, 1e-3)
     for o in (op, dense):
         o.set_inner_precision(gpu.SB_INNER_FP16)
+    op.reassemble(ph, beta)  # the assembly writes the copy
+    assert np.array_equal(op.matrix_c64(), dense.matrix_c64())
     s1 = gpu.gmres_mixed(op, b, cfg)
     s2 = gpu.gmres_mixed(dense, b, cfg)
     assert s1.converged and s2.converged
-    assert s1.iterations == s2.iterations and np.array_equal(s1.x, s2.x)
+    assert abs(s1.iterations - s2.iterations) <= 2
+    assert _rel(s1.x, s2.x) < 1e-6
+    # the copy written by the assembly and a rebuilt one give the same solve
+    op.set_inner_precision(gpu.SB_INNER_FP32)
+    op.set_inner_precision(gpu.SB_INNER_FP16)  # no copy now: the next solve rebuilds it
+    s3 = gpu.gmres_mixed(op, b, cfg)
+    assert abs(s1.iterations - s3.iterations) <= 2 and _rel(s1.x, s3.x) < 1e-6
     op.close()
     dense.close()
     mesh.close()
