@@ -1250,7 +1250,10 @@ __device__ __forceinline__ Acc warp_reduce(const Acc& a) {
     return r;
 }
 
-__global__ void __launch_bounds__(32 * kNearWarps) k_near(const double* __restrict__ elem,
+// 5 resident CTAs (20 warps) per SM: 96 registers (8 bytes spilled); more warps hide the FP64
+// latency of the subdivision replay (N = 20480: 2.88 -> 2.56 ms; 6 CTAs 2.83 ms).
+constexpr int kNearMinBlocks = 5;
+__global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near(const double* __restrict__ elem,
                                                           int64_t n, int64_t ld,
                                                           const int64_t* __restrict__ row_ptr,
                                                           const int32_t* __restrict__ cols,

@@ -352,11 +352,16 @@ void gemv_c64(const float2* A, int64_t n, int64_t lda, const float2* x, float2* 
     SB_CUDA(cudaGetLastError());
 }
 
+// Rows a CTA of the FP64-vector product (measured at N = 20480: 8 rows, which halve its x traffic
+// from L2, made the mixed solve 0.3 ms slower than 4).
+constexpr int kGemvX64Rows = 4;
+int64_t gemv_x64_partials(int64_t n) { return cdiv(n, kGemvX64Rows); }
+
 void gemv_c64_x64(const float2* A, int64_t n, int64_t lda, const double2* x, double2* y,
                   const double2* b, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV32, s);
-    k_gemv_n_c64<kGemvRows, kGemvThreads, kGemvUnroll, true>
-        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part, gate);
+    k_gemv_n_c64<kGemvX64Rows, kGemvThreads, kGemvUnroll, true>
+        <<<cdiv(n, kGemvX64Rows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }

@@ -528,7 +528,7 @@ struct Ctx {
     // ||b - A x|| (residual vector left in opb)
     double residual(const double2* x, const double2* b) {
         op_residual64(op, x, b, S.opb.as<double2>(), S.part.as<double>());
-        sum_real(S.part.as<double>(), gemv_partials(n), S.nrm.as<double>() + 2, s);
+        sum_real(S.part.as<double>(), op_residual64_partials(op), S.nrm.as<double>() + 2, s);
         double h;
         to_host(&h, S.nrm.as<double>() + 2, 1);
         sync();

@@ -224,7 +224,11 @@ void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g) {
         gemv_c64_x64(op.A32.as<float2>(), op.n, op.lda32, x, y, nullptr, nullptr, op.stream, g);
 }
 
-// r = b - A x with FP64 vectors and per-CTA partial norms (gemv_partials(n) entries).
+int64_t op_residual64_partials(const Operator& op) {
+    return op.A64.p ? gemv_partials(op.n) : gemv_x64_partials(op.n);
+}
+
+// r = b - A x with FP64 vectors and per-CTA partial norms (op_residual64_partials entries).
 void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part) {
     if (op.A64.p)
         gemv_residual_c128(op.A64.as<double2>(), op.n, x, b, r, part, op.stream);
@@ -561,7 +565,7 @@ Problem<double2> problem64(const Operator& op) {
     P.n = op.n;
     P.stream = op.stream;
     P.key_A = op.A64.p ? op.A64.p : op.A32.p;
-    P.partials = gemv_partials(op.n);
+    P.partials = op_residual64_partials(op);
     P.apply = [&op](const double2* xi, double2* yo, Gate g) { op_gemv64(op, xi, yo, g); };
     P.residual = [&op](const double2* xi, const double2* bi, double2* ro, double* part) {
         op_residual64(op, xi, bi, ro, part);
@@ -640,7 +644,7 @@ void gmres_mixed_ir(const Operator& op, const double2* b, double2* x, bool x0_gi
     double* hsc = static_cast<double*>(sw.pin.p);
     auto residual64 = [&](const double2* xv) {
         op_residual64(op, xv, b, sw.r64.as<double2>(), sw.partg.as<double>());
-        sum_real(sw.partg.as<double>(), gemv_partials(n), sw.nrmg.as<double>(), op.stream);
+        sum_real(sw.partg.as<double>(), op_residual64_partials(op), sw.nrmg.as<double>(), op.stream);
         SB_CUDA(cudaMemcpyAsync(hsc, sw.nrmg.p, sizeof(double), cudaMemcpyDeviceToHost, op.stream));
         SB_CUDA(cudaStreamSynchronize(op.stream));
         return std::sqrt(hsc[0]);

@@ -31,6 +31,7 @@ void gemv_c64(const float2* A, int64_t n, int64_t lda, const float2* x, float2* 
               const float2* b, double* part, cudaStream_t s, Gate gate = {});
 void gemv_c64_x64(const float2* A, int64_t n, int64_t lda, const double2* x, double2* y,
                   const double2* b, double* part, cudaStream_t s, Gate gate = {});
+int64_t gemv_x64_partials(int64_t n);  // partial norms gemv_c64_x64 writes with b
 // Complex-half matrix (uint32 = FP16 re | FP16 im << 16; lda a multiple of 4), FP32 vectors and
 // accumulation: y_i = (A x)_i * inv_scale[i], or b_i - (A x)_i * inv_scale[i] with part = ||.||^2.
 void gemv_c16(const uint32_t* A, int64_t n, int64_t lda, const float* inv_scale, const float2* x, float2* y,

@@ -271,6 +271,7 @@ std::vector<int32_t> element_morton_order(const Mesh& m);
 // Products with FP64 vectors on whichever matrix the operator holds (gmres.cu).
 void op_gemv64(const Operator& op, const double2* x, double2* y, Gate g);
 void op_residual64(const Operator& op, const double2* x, const double2* b, double2* r, double* part);
+int64_t op_residual64_partials(const Operator& op);  // entries op_residual64 writes to part
 
 int device_sm_count(int device);
 
