@@ -626,10 +626,12 @@ constexpr int kFar32Rows = 64;
 // slot, so the far field evaluates two quadrature points per instruction (points 2p, 2p + 1 in
 // the .x / .y lanes of pair p; the 13th point runs alone).
 constexpr int kFarPairs = kFarPoints / 2;
-// Resident CTAs per SM of the FP32 far kernel: the packed loop keeps the column's 13 points, the
-// broadcast row terms and the lane sums in 168 registers without spills at 3 CTAs (measured at
-// N = 20480: 11.16 ms; 4 CTAs with spills 11.23 ms, 2 CTAs 12.24 ms).
-constexpr int kFar32MinBlocks = 3;
+// Resident CTAs per SM of the FP32 far kernel. With the columns' |delta|^2, weights and
+// delta . n_y in shared memory the packed loop fits 128 registers without spills: 4 CTAs per SM
+// (N = 20480: 10.28 ms; all point data in 168 registers at 3 CTAs 11.03 ms; 4 CTAs of that
+// layout with spills 11.23 ms, 2 CTAs 12.24 ms).
+constexpr bool kFar32SmemCols = true;
+constexpr int kFar32MinBlocks = kFar32SmemCols ? 4 : 3;
 static_assert(kFarPoints == 2 * kFarPairs + 1, "the packed far loop pairs all points but the last");
 __device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
@@ -681,7 +683,7 @@ __device__ __forceinline__ void far32_point(Far32Sums& a, float px, float py, fl
 }
 
 // One (128-column tile, 64-row block) of the FP32 far field; all 128 threads of the CTA call it.
-template <bool kWithRhs>
+template <bool kWithRhs, bool kSmemCols = true>
 __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const double* __restrict__ elem,
                                            int64_t n, int64_t ld, const double* __restrict__ coef, double k,
                                            float2* __restrict__ A32, int64_t lda32, double2* __restrict__ far_part,
@@ -707,7 +709,22 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
     if (A16)
         for (int r = tid; r < kFar32Rows; r += kFarTile) shs[r] = (row0 + r < n) ? hscale[row0 + r] : 1.f;
     // The column's 13 points in registers: points 2p, 2p + 1 in the lanes of pair p, the 13th alone.
-    float2 PX[kFarPairs], PY[kFarPairs], PZ[kFarPairs], PD[kFarPairs], PW[kFarPairs], PN[kFarPairs];
+    float2 PX[kFarPairs], PY[kFarPairs], PZ[kFarPairs];
+    // |delta|^2, weight and delta . n_y of the column's points: in shared memory with kSmemCols
+    // (each thread reads only its own column; 42 fewer registers, 4 CTAs per SM instead of 3),
+    // else in registers (the persistent batched kernel, whose static shared memory is full).
+    constexpr int kS = kSmemCols ? kFarPairs : 1, kR = kSmemCols ? 1 : kFarPairs;
+    __shared__ float2 sPD[kS][kFarTile], sPW[kS][kFarTile], sPN[kS][kFarTile];
+    float2 PD[kR], PW[kR], PN[kR];
+    auto PD_ = [&](int p) -> float2& {
+        if constexpr (kSmemCols) return sPD[p][tid]; else return PD[p];
+    };
+    auto PW_ = [&](int p) -> float2& {
+        if constexpr (kSmemCols) return sPW[p][tid]; else return PW[p];
+    };
+    auto PN_ = [&](int p) -> float2& {
+        if constexpr (kSmemCols) return sPN[p][tid]; else return PN[p];
+    };
     float lx, ly, lz, ld_, lw, ln;
     double cx = 0, cy = 0, cz = 0;
     float nyx = 0, nyy = 0, nyz = 0;
@@ -719,9 +736,9 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
         PX[p] = make_float2(s0[0], s1[0]);
         PY[p] = make_float2(s0[ld], s1[ld]);
         PZ[p] = make_float2(s0[2 * ld], s1[2 * ld]);
-        PD[p] = make_float2(s0[3 * ld], s1[3 * ld]);
-        PW[p] = make_float2(s0[4 * ld], s1[4 * ld]);
-        PN[p] = make_float2(s0[5 * ld], s1[5 * ld]);
+        PD_(p) = make_float2(s0[3 * ld], s1[3 * ld]);
+        PW_(p) = make_float2(s0[4 * ld], s1[4 * ld]);
+        PN_(p) = make_float2(s0[5 * ld], s1[5 * ld]);
     }
     {
         const float* sl = qp32 + (int64_t)((kFarPoints - 1) * kQ32) * ld + jj;
@@ -787,7 +804,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             float2 AGR = Z, AGI = Z, NAHR = Z, NAHI = Z, NATR = Z, NATI = Z, AER = Z, AEI = Z, GQR = Z, GQI = Z;
 #pragma unroll
             for (int p = 0; p < kFarPairs; ++p) {
-                const float2 num = pfma(FX2, PX[p], pfma(FY2, PY[p], pfma(FZ2, PZ[p], PD[p])));
+                const float2 num = pfma(FX2, PX[p], pfma(FY2, PY[p], pfma(FZ2, PZ[p], PD_(p))));
                 const float2 rq2 = padd(RC2, num);
                 const float2 rinv = make_float2(rsqrtf(rq2.x), rsqrtf(rq2.y));
                 const float2 den = pfma(rq2, rinv, RC);
@@ -802,9 +819,9 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                     sincos_f32(t.x, &S.x, &C.x);
                     sincos_f32(t.y, &S.y, &C.y);
                 }
-                const float2 gs = pmul(PW[p], rinv);
+                const float2 gs = pmul(PW_(p), rinv);
                 const float2 gr = pmul(C, gs), gi = pmul(S, gs);
-                const float2 rny = pmul(padd(FNY, PN[p]), rinv);
+                const float2 rny = pmul(padd(FNY, PN_(p)), rinv);
                 const float2 pnx = pfma(PZ[p], NXZ, pfma(PY[p], NXY, pmul(PX[p], NXX)));
                 const float2 rnx = pmul(pfma(pnx, M1, FNX), rinv);
                 const float2 u = pfma(gr, rinv, pmul(gi, KK));
@@ -890,8 +907,8 @@ __global__ void __launch_bounds__(kFarTile, kFar32MinBlocks) k_far32(const float
                                                     unsigned* __restrict__ amax, uint32_t* __restrict__ A16,
                                                     int64_t lda16, const float* __restrict__ hscale,
                                                     int* __restrict__ hflag) {
-    far32_tile<kWithRhs>(qp32, elem, n, ld, coef, k, A32, lda32, far_part, n_tiles, blockIdx.x,
-                         blockIdx.y * (int64_t)kFar32Rows, amax, A16, lda16, hscale, hflag);
+    far32_tile<kWithRhs, kFar32SmemCols>(qp32, elem, n, ld, coef, k, A32, lda32, far_part, n_tiles, blockIdx.x,
+                                         blockIdx.y * (int64_t)kFar32Rows, amax, A16, lda16, hscale, hflag);
 }
 
 // Complex-half copy during the FP32 assembly (after the near and self kernels): each row's scale
@@ -2330,7 +2347,7 @@ __global__ void __launch_bounds__(kFarTile, 4) k_assemble_batch(const BatchAsmIn
             const BatchAsmInst I = inst[b];
             const int64_t local = item - fpre[b];
             const int64_t nrb = (I.n + kFar32Rows - 1) / kFar32Rows;
-            far32_tile<false>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr, I.n_tiles,
+            far32_tile<false, false>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr, I.n_tiles,
                               local / nrb, (local % nrb) * kFar32Rows);
         } else if (item < nf + nn) {
             const int64_t it = item - nf;
