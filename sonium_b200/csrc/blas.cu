@@ -148,10 +148,15 @@ constexpr int kDotRows = 256;
 constexpr int kDotVecs = 8;
 
 // part[(chunk * (k + 1)) + i] = sum over the chunk of conj(V_i) w  (i < k), and |w|^2 at i = k.
+// With cnt (one counter per blockIdx.y, zero between launches) the last CTA of each column of the
+// grid also reduces the partials into out, in chunk order as k_reduce_part does, and resets the
+// counter: one launch instead of two.
 template <class T>
 __global__ void __launch_bounds__(kDotRows) k_dots(const T* __restrict__ V, int64_t ldv, int k,
                                                    const T* __restrict__ w, int64_t n,
-                                                   double2* __restrict__ part, Gate gate) {
+                                                   double2* __restrict__ part, Gate gate,
+                                                   double2* __restrict__ out = nullptr,
+                                                   unsigned* __restrict__ cnt = nullptr) {
     if (closed(gate)) return;
     __shared__ double red[(kDotRows / 32) * 2 * kDotVecs];
     const int64_t r = blockIdx.x * (int64_t)kDotRows + threadIdx.x;
@@ -180,7 +185,32 @@ __global__ void __launch_bounds__(kDotRows) k_dots(const T* __restrict__ V, int6
             if (i <= k) part[blockIdx.x * (int64_t)(k + 1) + i] = make_double2(acc[2 * t], acc[2 * t + 1]);
         }
     }
+    if (!cnt) return;
+    __shared__ int last;
+    if (threadIdx.x == 0) {
+        __threadfence();  // this CTA's partials are visible before its count
+        last = atomicAdd(&cnt[blockIdx.y], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // warp t reduces vector i0 + t (kDotRows / 32 == kDotVecs warps)
+    const int t = threadIdx.x >> 5, lane = threadIdx.x & 31, i = i0 + t;
+    if (i <= k) {
+        double sr = 0.0, si = 0.0;
+        for (int64_t c = lane; c < gridDim.x; c += 32) {
+            const double2 v = __ldcg(part + c * (k + 1) + i);
+            sr += v.x;
+            si += v.y;
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) out[i] = make_double2(sr, si);
+    }
+    if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
 }
+static_assert(kDotRows / 32 == kDotVecs, "one reducing warp per vector of a dots CTA");
+static_assert((kMaxKrylov + kDotVecs) / kDotVecs <= kArnoldiCounters, "a counter per column of the dots grid");
 
 // out[i] = sum over chunks of part[c][i], i <= k (one warp per output).
 __global__ void k_reduce_part(const double2* __restrict__ part, int64_t chunks, int kp1,
@@ -199,11 +229,14 @@ __global__ void k_reduce_part(const double2* __restrict__ part, int64_t chunks, 
 }
 
 // w -= sum_i coeff[i] V_i, and a per-CTA partial of |w|^2.
+// With cnt the last CTA also sums the partials into *out (as k_sum_real does) and resets *cnt.
 template <class T>
 __global__ void __launch_bounds__(256) k_project(const T* __restrict__ V, int64_t ldv, int k,
                                                  const double2* __restrict__ coeff,
                                                  T* __restrict__ w, int64_t n,
-                                                 double* __restrict__ part, Gate gate) {
+                                                 double* __restrict__ part, Gate gate,
+                                                 double* __restrict__ out = nullptr,
+                                                 unsigned* __restrict__ cnt = nullptr) {
     if (closed(gate)) return;
     __shared__ double2 sc[kMaxKrylov + 1];
     __shared__ double red[8];
@@ -238,6 +271,22 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ V, int64_
     }
     block_sum<1, 256>(nr2, red);
     if (threadIdx.x == 0) part[blockIdx.x] = nr2[0];
+    if (!cnt) return;
+    __shared__ int last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(cnt, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    double sum = 0.0;
+    for (int64_t c = threadIdx.x; c < gridDim.x; c += 32) sum += __ldcg(part + c);
+    sum = warp_sum(sum);
+    if (threadIdx.x == 0) {
+        *out = sum;
+        *cnt = 0;
+    }
 }
 
 __global__ void k_sum_real(const double* __restrict__ part, int64_t m, double* __restrict__ out,
@@ -500,13 +549,14 @@ void half_alloc(Operator& op) {
 
 template <class T>
 void arnoldi_dots(const T* V, int64_t ldv, int k, const T* w, int64_t n, double2* part,
-                  double2* out, cudaStream_t s, Gate gate) {
+                  double2* out, cudaStream_t s, Gate gate, unsigned* cnt) {
     ProfScope prof(SB_PROF_ARNOLDI, s);
     const int64_t chunks = cdiv(n, kDotRows);
     dim3 grid(static_cast<unsigned>(chunks), static_cast<unsigned>(cdiv(k + 1, kDotVecs)));
-    k_dots<T><<<grid, kDotRows, 0, s>>>(V, ldv, k, w, n, part, gate);
+    k_dots<T><<<grid, kDotRows, 0, s>>>(V, ldv, k, w, n, part, gate, out, cnt);
     count_launch();
     SB_CUDA(cudaGetLastError());
+    if (cnt) return;
     k_reduce_part<<<k + 1, 32, 0, s>>>(part, chunks, k + 1, out, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
@@ -515,12 +565,13 @@ int64_t arnoldi_dot_chunks(int64_t n) { return cdiv(n, kDotRows); }
 
 template <class T>
 void arnoldi_project(const T* V, int64_t ldv, int k, const double2* coeff, T* w, int64_t n,
-                     double* part, double* out_norm2, cudaStream_t s, Gate gate) {
+                     double* part, double* out_norm2, cudaStream_t s, Gate gate, unsigned* cnt) {
     ProfScope prof(SB_PROF_ARNOLDI, s);
     const int64_t nb = cdiv(n, 256);
-    k_project<T><<<nb, 256, 0, s>>>(V, ldv, k, coeff, w, n, part, gate);
+    k_project<T><<<nb, 256, 0, s>>>(V, ldv, k, coeff, w, n, part, gate, out_norm2, cnt);
     count_launch();
     SB_CUDA(cudaGetLastError());
+    if (cnt) return;
     k_sum_real<<<1, 32, 0, s>>>(part, nb, out_norm2, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
@@ -557,10 +608,10 @@ void jacobi_apply(const double2* d, const T* x, T* y, int64_t n, cudaStream_t s,
 }
 
 // Explicit instantiations.
-template void arnoldi_dots<double2>(const double2*, int64_t, int, const double2*, int64_t, double2*, double2*, cudaStream_t, Gate);
-template void arnoldi_dots<float2>(const float2*, int64_t, int, const float2*, int64_t, double2*, double2*, cudaStream_t, Gate);
-template void arnoldi_project<double2>(const double2*, int64_t, int, const double2*, double2*, int64_t, double*, double*, cudaStream_t, Gate);
-template void arnoldi_project<float2>(const float2*, int64_t, int, const double2*, float2*, int64_t, double*, double*, cudaStream_t, Gate);
+template void arnoldi_dots<double2>(const double2*, int64_t, int, const double2*, int64_t, double2*, double2*, cudaStream_t, Gate, unsigned*);
+template void arnoldi_dots<float2>(const float2*, int64_t, int, const float2*, int64_t, double2*, double2*, cudaStream_t, Gate, unsigned*);
+template void arnoldi_project<double2>(const double2*, int64_t, int, const double2*, double2*, int64_t, double*, double*, cudaStream_t, Gate, unsigned*);
+template void arnoldi_project<float2>(const float2*, int64_t, int, const double2*, float2*, int64_t, double*, double*, cudaStream_t, Gate, unsigned*);
 template void scale_vec<double2, double2>(const double2*, double, const double*, double2*, int64_t, cudaStream_t, Gate);
 template void scale_vec<float2, float2>(const float2*, double, const double*, float2*, int64_t, cudaStream_t, Gate);
 template void scale_vec<double2, float2>(const double2*, double, const double*, float2*, int64_t, cudaStream_t, Gate);

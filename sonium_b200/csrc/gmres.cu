@@ -69,6 +69,7 @@ template <class T>
 struct KrylovWork {
     int64_t n = 0, m = 0, ldv = 0;
     DevBuf V, w, opb, r, part, red, red2, nrm, ydev, H, cs, sn, g, st;
+    DevBuf cnt;  // last-CTA reduction counters of the Arnoldi kernels (zero between launches)
     PinnedBuf host;  // KState + two doubles, then two KState slots of the chunk checks
     // The cycle is captured as chunks of kCycleChunk Arnoldi steps (one graph each), launched
     // while the cycle is still active, so a converged cycle stops paying for gated launches.
@@ -121,6 +122,10 @@ struct KrylovWork {
         sn.alloc(sizeof(double2) * m);
         g.alloc(sizeof(double2) * (m + 1));
         st.alloc(sizeof(KState));
+        if (!cnt.p) {
+            cnt.alloc(sizeof(unsigned) * 2 * kArnoldiCounters);
+            memset_sync(cnt.p, 0, sizeof(unsigned) * 2 * kArnoldiCounters);
+        }
         host.alloc(3 * sizeof(KState) + 64);
         for (cudaEvent_t& e : ev)
             if (!e) SB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -280,13 +285,16 @@ void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t j0, int64_t j1)
         } else {
             P.apply(Vp + j * W.ldv, w, ga);
         }
-        arnoldi_dots<T>(Vp, W.ldv, k, w, n, W.part.template as<double2>(), W.red.template as<double2>(), s, ga);
-        arnoldi_project<T>(Vp, W.ldv, k, W.red.template as<double2>(), w, n, W.part.template as<double>(), nrm, s, ga);
+        unsigned* cd = W.cnt.template as<unsigned>();           // dots counters
+        unsigned* cp = cd + kArnoldiCounters;                    // projection counter
+        arnoldi_dots<T>(Vp, W.ldv, k, w, n, W.part.template as<double2>(), W.red.template as<double2>(), s, ga, cd);
+        arnoldi_project<T>(Vp, W.ldv, k, W.red.template as<double2>(), w, n, W.part.template as<double>(), nrm, s, ga,
+                           cp);
         k_after_first<<<1, 1, 0, s>>>(st, W.red.template as<double2>(), nrm, W.H.template as<double2>(), static_cast<int>(j));
         count_launch();
-        arnoldi_dots<T>(Vp, W.ldv, k, w, n, W.part.template as<double2>(), W.red2.template as<double2>(), s, gb);
+        arnoldi_dots<T>(Vp, W.ldv, k, w, n, W.part.template as<double2>(), W.red2.template as<double2>(), s, gb, cd);
         arnoldi_project<T>(Vp, W.ldv, k, W.red2.template as<double2>(), w, n, W.part.template as<double>(), nrm + 1,
-                           s, gb);
+                           s, gb, cp);
         k_givens<<<1, 1, 0, s>>>(st, W.red2.template as<double2>(), nrm + 1, W.H.template as<double2>(),
                                  W.cs.template as<double2>(), W.sn.template as<double2>(), W.g.template as<double2>(),
                                  static_cast<int>(j));

@@ -39,14 +39,17 @@ void gemv_c16(const uint32_t* A, int64_t n, int64_t lda, const float* inv_scale,
 int64_t gemv16_partials(int64_t n);
 
 // out[i] = V_i^H w (i < k), out[k].x = |w|^2; part holds arnoldi_dot_chunks(n) * (k + 1).
+// With cnt (kArnoldiCounters zeroed unsigned, owned by one stream's work) the reduction runs in
+// the same launch (the last CTA reduces).
+constexpr int kArnoldiCounters = 16;
 template <class T>
 void arnoldi_dots(const T* V, int64_t ldv, int k, const T* w, int64_t n, double2* part,
-                  double2* out, cudaStream_t s, Gate gate = {});
+                  double2* out, cudaStream_t s, Gate gate = {}, unsigned* cnt = nullptr);
 int64_t arnoldi_dot_chunks(int64_t n);
-// w -= sum_i coeff[i] V_i; *out_norm2 = |w|^2 (part holds ceil(n / 256) doubles).
+// w -= sum_i coeff[i] V_i; *out_norm2 = |w|^2 (part holds ceil(n / 256) doubles); cnt as above.
 template <class T>
 void arnoldi_project(const T* V, int64_t ldv, int k, const double2* coeff, T* w, int64_t n,
-                     double* part, double* out_norm2, cudaStream_t s, Gate gate = {});
+                     double* part, double* out_norm2, cudaStream_t s, Gate gate = {}, unsigned* cnt = nullptr);
 void sum_real(const double* part, int64_t m, double* out, cudaStream_t s, Gate gate = {});
 // y = alpha x (alpha_dev, when given, overrides alpha).
 template <class TI, class TO>
