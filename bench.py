@@ -436,9 +436,9 @@ def main():
             dist.barrier()
             t0 = time.perf_counter()
             m2 = sb.Mesh(nodes, tris, device=dev)
-            o2 = sb.build_tbem_system_with_beta(m2, ph, beta, sb.SB_PRECISION_FP32)
-            if head_mode in ("mixed_half", "mixed_half_bj"):
-                o2.set_inner_precision(sb.SB_INNER_FP16)
+            # the complex-half forms assemble with the half copy written by the first assembly
+            o2 = sb.build_tbem_system_with_beta(m2, ph, beta, sb.SB_PRECISION_FP32 if head_mode == "mixed"
+                                                else sb.SB_PRECISION_FP32_HALF)
             if head_mode == "mixed_half_bj":
                 o2.set_inner_preconditioner(sb.SB_INNER_PRECOND_BLOCK_JACOBI, BJ_BLOCK)
             bh = sb.rhs_plane_wave(m2, ph, beta, dirs)[:, 0]
@@ -455,8 +455,8 @@ def main():
         d2h = 16 * n + 16 * n                           # RHS and solution
         e2e = {"value": dist.world * len(ts) / sum(ts), "unit": "solves/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "path": "sb_mesh_create + sb_assemble(SB_PRECISION_FP32) + "
-                       + ("sb_operator_set_inner_precision(SB_INNER_FP16) + " if head_mode != "mixed" else "")
+               "path": "sb_mesh_create + sb_assemble("
+                       + ("SB_PRECISION_FP32) + " if head_mode == "mixed" else "SB_PRECISION_FP32_HALF) + ")
                        + ("sb_operator_set_inner_preconditioner(SB_INNER_PRECOND_BLOCK_JACOBI, %d) + " % BJ_BLOCK
                           if head_mode == "mixed_half_bj" else "")
                        + "sb_rhs_plane_wave + sb_gmres_mixed (host buffers), wall clock"}

@@ -131,6 +131,10 @@ SB_API int sb_mesh_set_bc(sb_mesh* mesh, const int32_t* kind, const sb_complex* 
 #define SB_PRECISION_FP32 2      /* complex64 matrix only: far pairs in FP32 with the phase
                                   * argument k r in FP64, near and self pairs in FP64; products
                                   * with FP64 vectors accumulate in FP64 */
+#define SB_PRECISION_FP32_HALF 3 /* SB_PRECISION_FP32 with SB_INNER_FP16 set from the start (accepted
+                                  * by sb_assemble only): the first assembly already writes the
+                                  * complex-half copy the mixed solver's inner products read;
+                                  * sb_operator_info_get reports SB_PRECISION_FP32 */
 
 typedef struct sb_operator sb_operator;
 

@@ -5,8 +5,8 @@ The compute path is the CUDA shared library built from ``sonium_b200/csrc`` (C A
 """
 from ._lib import (SB_INNER_FP16, SB_INNER_FP32, SB_INNER_PRECOND_BLOCK_JACOBI, SB_INNER_PRECOND_NONE,
                    SB_BASIS_CONSTANT, SB_BASIS_LINEAR, SB_BASIS_QUADRATIC, SB_BC_PRESSURE, SB_BC_VELOCITY, SB_INJECT_ALLOC, SB_INJECT_LAUNCH, SB_INJECT_NONE,
-                   SB_OP_C, SB_OP_N, SB_OP_T, SB_PRECISION_FP32, SB_PRECISION_FP64, SB_PRECISION_FP64_FP32,
-                   SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI, SoniumError)
+                   SB_OP_C, SB_OP_N, SB_OP_T, SB_PRECISION_FP32, SB_PRECISION_FP32_HALF, SB_PRECISION_FP64,
+                   SB_PRECISION_FP64_FP32, SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI, SoniumError)
 from .tbem import (DenseMatrixOperator, GcroDrConfig, GcroDrSubspace, build_tbem_system_linear, gcro_dr,
                    build_tbem_system_discontinuous_stabilized, build_tbem_system_quadratic_stabilized,
                    rhs_plane_wave_at,
@@ -30,5 +30,5 @@ __all__ = [
     "SB_BC_PRESSURE", "SB_BC_VELOCITY", "SB_INJECT_ALLOC", "SB_INJECT_LAUNCH", "SB_INJECT_NONE",
     "SB_OP_C", "SB_OP_N", "SB_OP_T", "SB_PRECISION_FP32", "SB_PRECISION_FP64", "SB_PRECISION_FP64_FP32",
     "SB_PRECOND_IDENTITY", "SB_PRECOND_JACOBI", "SB_INNER_FP16", "SB_INNER_FP32",
-    "SB_INNER_PRECOND_BLOCK_JACOBI", "SB_INNER_PRECOND_NONE",
+    "SB_INNER_PRECOND_BLOCK_JACOBI", "SB_INNER_PRECOND_NONE", "SB_PRECISION_FP32_HALF",
 ]

@@ -24,6 +24,7 @@ SB_ERR_NOT_FINITE = 7
 SB_PRECISION_FP64 = 0
 SB_PRECISION_FP64_FP32 = 1
 SB_PRECISION_FP32 = 2
+SB_PRECISION_FP32_HALF = 3
 SB_INNER_FP32 = 0
 SB_INNER_FP16 = 1
 SB_INNER_PRECOND_NONE = 0

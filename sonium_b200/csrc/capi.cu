@@ -416,10 +416,12 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
         SB_REQUIRE(mesh && mesh->m && physics && out, SB_ERR_INVALID_ARGUMENT, "null argument");
         *out = nullptr;
         SB_REQUIRE(precision == SB_PRECISION_FP64 || precision == SB_PRECISION_FP64_FP32 ||
-                       precision == SB_PRECISION_FP32,
+                       precision == SB_PRECISION_FP32 || precision == SB_PRECISION_FP32_HALF,
                    SB_ERR_INVALID_ARGUMENT, "unknown precision");
         SB_REQUIRE(sb_physics_validate(physics) == SB_OK, SB_ERR_INVALID_ARGUMENT, "invalid physics: " + t_err);
         check_beta(beta);
+        const bool half = precision == SB_PRECISION_FP32_HALF;
+        if (half) precision = SB_PRECISION_FP32;
         Mesh& m = *mesh->m;
         SB_REQUIRE(!m.quad || precision == SB_PRECISION_FP64, SB_ERR_INVALID_ARGUMENT,
                    "Quad4 mesh: only SB_PRECISION_FP64 is supported");
@@ -435,6 +437,7 @@ SB_API int sb_assemble(const sb_mesh* mesh, const sb_physics* physics, sb_comple
             SB_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
             if (precision != SB_PRECISION_FP32) op->A64.alloc(sizeof(double2) * m.n * m.n);
             if (precision != SB_PRECISION_FP64) op->A32.alloc(sizeof(float2) * m.n * op->lda32);
+            if (half) op->inner = SB_INNER_FP16;
             assemble(*op, *physics, beta.re, beta.im);
         } catch (...) {
             if (op->stream) cudaStreamDestroy(op->stream);

@@ -327,11 +327,14 @@ class JacobiPreconditioner:
 
 def build_tbem_system_with_beta(mesh: Mesh, physics: PhysicsParams, beta: complex,
                                 precision: int = L.SB_PRECISION_FP64) -> TbemOperator:
-    """build_tbem_system_with_beta (tbem.rs:1196-1203): assemble on the device."""
+    """build_tbem_system_with_beta (tbem.rs:1196-1203): assemble on the device.
+    SB_PRECISION_FP32_HALF: SB_PRECISION_FP32 whose first assembly also writes the complex-half
+    copy for gmres_mixed's inner products (SB_INNER_FP16 set from the start)."""
     h = ct.c_void_p()
     check(L.load().sb_assemble(mesh.handle, ct.byref(physics._struct()), L.SbComplex(beta.real, beta.imag),
                                precision, ct.byref(h)))
-    return TbemOperator(mesh, h, physics, beta, precision)
+    return TbemOperator(mesh, h, physics, beta,
+                        L.SB_PRECISION_FP32 if precision == L.SB_PRECISION_FP32_HALF else precision)
 
 
 def build_tbem_system_linear(mesh: Mesh, physics: PhysicsParams, beta: complex) -> TbemOperator:

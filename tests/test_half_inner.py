@@ -139,3 +139,27 @@ def test_half_copy_from_assembly_matches_rebuilt_copy(gpu):
     op.close()
     dense.close()
     mesh.close()
+
+
+@pytest.mark.gpu
+def test_precision_fp32_half_writes_copy_at_first_assembly(gpu):
+    # SB_PRECISION_FP32_HALF: the first assembly writes the complex-half copy; the operator is an
+    # SB_PRECISION_FP32 one with SB_INNER_FP16 set, and solves as one that switched later.
+    nodes, tris = gpu.icosphere(1.0, 3)
+    mesh = gpu.Mesh(nodes, tris)
+    ph = gpu.PhysicsParams.for_wavenumber(4.0)
+    beta = ph.burton_miller_beta()
+    b = gpu.rhs_plane_wave(mesh, ph, beta, [0.0, 0.0, 1.0])[:, 0]
+    cfg = gpu.IrConfig(20, 1e-8, 50, 50, 1e-3)
+    oh = gpu.build_tbem_system_with_beta(mesh, ph, beta, gpu.SB_PRECISION_FP32_HALF)
+    assert oh.info().precision == gpu.SB_PRECISION_FP32
+    o32 = gpu.build_tbem_system_with_beta(mesh, ph, beta, gpu.SB_PRECISION_FP32)
+    assert np.array_equal(oh.matrix_c64(), o32.matrix_c64())
+    o32.set_inner_precision(gpu.SB_INNER_FP16)
+    s1 = gpu.gmres_mixed(oh, b, cfg)
+    s2 = gpu.gmres_mixed(o32, b, cfg)
+    assert s1.converged and s2.converged
+    assert abs(s1.iterations - s2.iterations) <= 2 and _rel(s1.x, s2.x) < 1e-6
+    oh.close()
+    o32.close()
+    mesh.close()
