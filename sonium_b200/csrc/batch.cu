@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(bj_threads(BS)) k_bbj_invert(const BInst* __re
                                         const_cast<float2*>(I.bj_inv) + blk * BS * BS, status, Mbj);
 }
 template <int BS>
-__global__ void __launch_bounds__(BS) k_bbj_apply(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+__global__ void __launch_bounds__(BS * kBjSplit) k_bbj_apply(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
                                                   int ninst, int mode, int j, int gk) {
     const int b = find_inst(pre, ninst, blockIdx.x);
     const BInst& I = inst[b];
@@ -718,9 +718,9 @@ static void batch_bj_apply(Batch& B, int mode, int j, int gk) {
     const int64_t* p = B.prebj_d.as<int64_t>();
     ProfScope prof(SB_PROF_ARNOLDI, B.stream);
     switch (B.bj_size) {
-        case 32: k_bbj_apply<32><<<g, 32, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
-        case 128: k_bbj_apply<128><<<g, 128, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
-        default: k_bbj_apply<64><<<g, 64, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
+        case 32: k_bbj_apply<32><<<g, 32 * kBjSplit, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
+        case 128: k_bbj_apply<128><<<g, 128 * kBjSplit, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
+        default: k_bbj_apply<64><<<g, 64 * kBjSplit, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
     }
     count_launch();
     SB_CUDA(cudaGetLastError());

@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(bj_threads(BS)) k_bj_invert(const float2* __re
 
 // y = M^-1 x: one CTA of BS threads per block.
 template <int BS>
-__global__ void __launch_bounds__(BS) k_bj_apply(const float2* __restrict__ invT, int64_t n,
+__global__ void __launch_bounds__(BS * kBjSplit) k_bj_apply(const float2* __restrict__ invT, int64_t n,
                                                  const int32_t* __restrict__ perm, const float2* __restrict__ x,
                                                  float2* __restrict__ y, Gate gate) {
     if ((gate.a && *gate.a == 0) || (gate.b && *gate.b == 0)) return;
@@ -99,7 +99,7 @@ void bj_build(Operator& op, int* status) {
 template <int BS>
 void bj_launch(const Operator& op, const float2* x, float2* y, cudaStream_t s, Gate g) {
     const int64_t nb = (op.n + BS - 1) / BS;
-    k_bj_apply<BS><<<static_cast<unsigned>(nb), BS, 0, s>>>(op.bj_inv.as<float2>(), op.n, op.bj_perm.as<int32_t>(),
+    k_bj_apply<BS><<<static_cast<unsigned>(nb), BS * kBjSplit, 0, s>>>(op.bj_inv.as<float2>(), op.n, op.bj_perm.as<int32_t>(),
                                                            x, y, g);
     count_launch();
     SB_CUDA(cudaGetLastError());

@@ -127,23 +127,41 @@ __device__ __forceinline__ void bj_invert_block(const float2* __restrict__ A, in
     }
 }
 
-// y[p_i] = sum_j inv[i][j] x[p_j] for one block (BS threads, thread i = row i; the block's x is
-// gathered into shared memory before any y is written, so x and y may be the same vector).
+// Threads of the apply CTA: kBjSplit threads per row, each summing BS / kBjSplit columns (short
+// dependent chains, 4x the parallelism of one thread per row).
+constexpr int kBjSplit = 4;
+
+// y[p_i] = sum_j inv[i][j] x[p_j] for one block (BS * kBjSplit threads: thread i + BS q takes
+// row i, columns [q BS / kBjSplit, (q + 1) BS / kBjSplit)). The block's x is gathered into shared
+// memory before any y is written, so x and y may be the same vector.
 template <int BS>
 __device__ __forceinline__ void bj_apply_block(const float2* __restrict__ invT, int rows,
                                                const int32_t* __restrict__ perm, const float2* x, float2* y) {
     __shared__ float2 xs[BS];
-    const int i = threadIdx.x;
-    xs[i] = i < rows ? x[perm[i]] : make_float2(0.f, 0.f);
+    __shared__ float2 ps[kBjSplit][BS];
+    const int i = threadIdx.x % BS, q = threadIdx.x / BS;
+    if (threadIdx.x < BS) xs[i] = i < rows ? x[perm[i]] : make_float2(0.f, 0.f);
     __syncthreads();
+    constexpr int kCols = BS / kBjSplit;
     float re = 0.f, im = 0.f;
 #pragma unroll 8
-    for (int j = 0; j < BS; ++j) {
+    for (int jj = 0; jj < kCols; ++jj) {
+        const int j = q * kCols + jj;
         const float2 a = invT[j * BS + i], v = xs[j];
         re = fmaf(a.x, v.x, fmaf(-a.y, v.y, re));
         im = fmaf(a.x, v.y, fmaf(a.y, v.x, im));
     }
-    if (i < rows) y[perm[i]] = make_float2(re, im);
+    ps[q][i] = make_float2(re, im);
+    __syncthreads();
+    if (q == 0 && i < rows) {
+        float2 t = ps[0][i];
+#pragma unroll
+        for (int u = 1; u < kBjSplit; ++u) {
+            t.x += ps[u][i].x;
+            t.y += ps[u][i].y;
+        }
+        y[perm[i]] = t;
+    }
 }
 
 }  // namespace sb
