@@ -308,7 +308,7 @@ SB_API int sb_operator_set_inner_precision(sb_operator* op, int inner);
 /* Right preconditioner of sb_gmres_mixed's inner GMRES (no reference counterpart: an inner-solver
  * choice of this library; the reference's preconditioner interface is Preconditioner::apply_into,
  * crates/sonium-solvers/crates/sonium-solvers-core/src/traits.rs:3645). SB_INNER_PRECOND_NONE
- * (default) or SB_INNER_PRECOND_BLOCK_JACOBI: the unknowns in blocks of block_size (32, 64 or 128)
+ * (default) or SB_INNER_PRECOND_BLOCK_JACOBI: the unknowns in blocks of block_size (32, 64, 96 or 128)
  * spatially close elements (consecutive in the Morton order of the element centroids; index
  * order for an operator without a mesh or with a discontinuous basis), each diagonal block of the
  * complex64 matrix inverted on the device (Gauss-Jordan with partial pivoting, FP32; a singular

@@ -705,6 +705,7 @@ static void batch_bj_prepare(Batch& B) {
     SB_CUDA(cudaMemsetAsync(B.bj_status.p, 0, sizeof(int), B.stream));
     switch (bs) {
         case 32: bj_invert_launch<32>(B); break;
+        case 96: bj_invert_launch<96>(B); break;
         case 128: bj_invert_launch<128>(B); break;
         default: bj_invert_launch<64>(B); break;
     }
@@ -719,6 +720,7 @@ static void batch_bj_apply(Batch& B, int mode, int j, int gk) {
     ProfScope prof(SB_PROF_ARNOLDI, B.stream);
     switch (B.bj_size) {
         case 32: k_bbj_apply<32><<<g, 32 * kBjSplit, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
+        case 96: k_bbj_apply<96><<<g, 96 * kBjSplit, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
         case 128: k_bbj_apply<128><<<g, 128 * kBjSplit, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
         default: k_bbj_apply<64><<<g, 64 * kBjSplit, 0, B.stream>>>(I, p, B.ninst, mode, j, gk); break;
     }
@@ -1514,8 +1516,8 @@ SB_API int sb_batch_set_inner_preconditioner(sb_batch* batch, int kind, int bloc
                    "inner preconditioner must be SB_INNER_PRECOND_NONE or SB_INNER_PRECOND_BLOCK_JACOBI");
         Batch& B = *batch->b;
         if (kind == SB_INNER_PRECOND_BLOCK_JACOBI) {
-            SB_REQUIRE(block_size == 32 || block_size == 64 || block_size == 128, SB_ERR_INVALID_ARGUMENT,
-                       "block_size must be 32, 64 or 128");
+            SB_REQUIRE(block_size == 32 || block_size == 64 || block_size == 96 || block_size == 128,
+                       SB_ERR_INVALID_ARGUMENT, "block_size must be 32, 64, 96 or 128");
             if (block_size != B.bj_size) B.bj_valid = false;
             B.bj_size = block_size;
         }

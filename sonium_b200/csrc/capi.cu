@@ -1050,8 +1050,8 @@ SB_API int sb_operator_set_inner_preconditioner(sb_operator* op, int kind, int b
                    "inner preconditioner must be SB_INNER_PRECOND_NONE or SB_INNER_PRECOND_BLOCK_JACOBI");
         Operator& o = *op->op;
         if (kind == SB_INNER_PRECOND_BLOCK_JACOBI) {
-            SB_REQUIRE(block_size == 32 || block_size == 64 || block_size == 128, SB_ERR_INVALID_ARGUMENT,
-                       "block_size must be 32, 64 or 128");
+            SB_REQUIRE(block_size == 32 || block_size == 64 || block_size == 96 || block_size == 128,
+                       SB_ERR_INVALID_ARGUMENT, "block_size must be 32, 64, 96 or 128");
             SB_REQUIRE(o.A32.p, SB_ERR_INVALID_ARGUMENT,
                        "the block-Jacobi inner preconditioner needs a complex64 matrix (SB_PRECISION_FP64_FP32 or "
                        "SB_PRECISION_FP32)");

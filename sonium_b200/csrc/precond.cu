@@ -133,6 +133,7 @@ void bj_prepare(Operator& op) {
     switch (bs) {
         case 32: bj_build<32>(op, op.bj_status.as<int>()); break;
         case 64: bj_build<64>(op, op.bj_status.as<int>()); break;
+        case 96: bj_build<96>(op, op.bj_status.as<int>()); break;
         default: bj_build<128>(op, op.bj_status.as<int>()); break;
     }
     op.bj_valid = true;
@@ -143,6 +144,7 @@ void bj_apply(const Operator& op, const float2* x, float2* y, Gate g) {
     switch (op.bj_size) {
         case 32: bj_launch<32>(op, x, y, op.stream, g); break;
         case 64: bj_launch<64>(op, x, y, op.stream, g); break;
+        case 96: bj_launch<96>(op, x, y, op.stream, g); break;
         default: bj_launch<128>(op, x, y, op.stream, g); break;
     }
 }

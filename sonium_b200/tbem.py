@@ -225,7 +225,7 @@ class TbemOperator(LinearOperator):
     def set_inner_preconditioner(self, kind: int, block_size: int = 128) -> None:
         """Right preconditioner of gmres_mixed's inner GMRES: SB_INNER_PRECOND_NONE (default) or
         SB_INNER_PRECOND_BLOCK_JACOBI (inverted diagonal blocks of block_size spatially close
-        elements; 32, 64 or 128). The converged solution is unchanged; the inner solves need fewer
+        elements; 32, 64, 96 or 128). The converged solution is unchanged; the inner solves need fewer
         iterations. Needs a complex64 matrix."""
         check(L.load().sb_operator_set_inner_preconditioner(self.handle, int(kind), int(block_size)))
 

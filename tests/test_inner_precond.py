@@ -24,7 +24,7 @@ def _rel(a, b):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("inner,bs", [(0, 128), (1, 64), (1, 128), (0, 32)])
+@pytest.mark.parametrize("inner,bs", [(0, 128), (1, 64), (1, 96), (1, 128), (0, 32)])
 def test_block_jacobi_tbem(gpu, inner, bs):
     nodes, tris = gpu.icosphere(1.0, 4, (1.0, 0.6, 0.4))
     mesh = gpu.Mesh(nodes, tris)
@@ -71,7 +71,7 @@ def _block_diag(rng, n, bs, zero_diag=True):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,bs", [(300, 64), (256, 128), (97, 32)])
+@pytest.mark.parametrize("n,bs", [(300, 64), (256, 128), (97, 32), (200, 96)])
 def test_block_jacobi_exact_on_block_diagonal(gpu, n, bs):
     rng = np.random.default_rng(n + bs)
     A = _block_diag(rng, n, bs)
