@@ -60,7 +60,8 @@ def test_block_product_matches_complex128(gpu, oracle, level, k, r, drop):
 
 
 def test_block_product_plane_wave_rhs_block(gpu, oracle):
-    """The right-hand sides of a multi-direction incident field (SURVEY config 5 shape, smaller)."""
+    """The right-hand sides of a multi-direction incident field (the shape of the 256-direction
+    multi-right-hand-side workload, smaller)."""
     from sonium_b200 import _lib as L
 
     nodes, tris = oracle.icosphere(1.0, 3, (1.0, 0.6, 0.4))
