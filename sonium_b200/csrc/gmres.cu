@@ -304,8 +304,10 @@ void launch_cycle(KrylovWork<T>& W, const Problem<T>& P, int64_t j0, int64_t j1)
     SB_CUDA(cudaGetLastError());
 }
 
-// Steps per captured chunk of a restart cycle.
-constexpr int64_t kCycleChunk = 8;
+// Steps per captured chunk of a restart cycle: smaller chunks leave fewer gated launches after
+// convergence (N = 20480 mixed solve: 4 steps 13.43 ms, 6 steps 13.49 ms, 8 steps 13.64 ms, 12
+// steps 13.64 ms).
+constexpr int64_t kCycleChunk = 4;
 
 // Replays the captured cycle (capturing it first when buffers, matrix or profiling changed):
 // chunk c + 1 is queued before the host reads chunk c's state, so the device never waits for the
