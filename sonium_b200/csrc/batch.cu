@@ -932,7 +932,7 @@ static void batch_step(Batch& B, int j) {
 
 // One restart cycle of the whole batch: m Arnoldi steps captured once into a CUDA graph.
 static void batch_cycle(Batch& B) {
-    constexpr int kBatchChunk = 8;
+    constexpr int kBatchChunk = 4;  // 4 vs 8 steps: sweep 96.2 vs 96.0 solves/s
     const uint64_t gen = B.shared ? tensor_generation(*B.shared) : 0;
     const int pre_key = B.inner_precond * 1024 + B.bj_size;
     const int nch = static_cast<int>((B.m + kBatchChunk - 1) / kBatchChunk);
