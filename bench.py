@@ -12,16 +12,20 @@ solve: re-assembly of the dense system on the device, the incident right-hand si
                 right preconditioner of the inner solve (`mixed_half_bj`, blocks of 128 spatially
                 close elements); `mixed_fp64_matrix` refines on the complex128 matrix. Inputs resident in HBM, device time by CUDA events on the
                 operator's stream; every mode's error against the plain FP64 solution is reported.
-  * `plain_fp64` -- the same solve with complex128 only and FP64 GMRES(50) to 1e-8.
+  * `plain_fp64` -- the same solve with complex128 only and FP64 GMRES(50) to 1e-8; `plain_fp64_bj`
+                the same with the headline's block-Jacobi right preconditioner (blocks of 128), the
+                like-for-like FP64 form: the line reports the speed-up against both.
   * `e2e`    -- the headline form through the C ABI with host buffers: mesh upload, assembly,
                 host RHS, solve with host b / x (all copies inside the timed region).
-  * `cpu_baseline` / `--impl reference` -- the CPU restatement of the reference path (oracle),
-                timed on a bounded sample (assembly rows + a CPU matvec) and scaled to one solve.
+  * `cpu_baseline` / `--impl reference` -- the CPU restatement of the reference path (oracle) on
+                the host cores: whole solves (all N rows of the assembly, the RHS, GMRES(50) from
+                x0 = 0 to 1e-8 with its real iteration count), one per step, same metric string.
 
   * `sweep`  -- the batched frequency sweep: 64 instances (ka 1 -> 32 on the (1, 0.6, 0.4) ellipsoid,
                 levels 2-5) assembled together (the autotuned form: one persistent launch or
                 per-instance kernels on two streams) and solved by the batched mixed GMRES,
-                against the same instances solved one after another in plain FP64.
+                against the same instances solved one after another in plain FP64 (and in FP64 with
+                the sweep's block-Jacobi preconditioner).
   * `multi_rhs` -- 256 plane-wave right-hand sides of one operator (ellipsoid level 5, k = 16)
                 solved together with tensor-core block products, against plain FP64 GMRES per
                 right-hand side; carries the tensor kernel's roofline.
@@ -72,6 +76,8 @@ def parse():
                     help="run only the 256-right-hand-side tensor-core leg and print its JSON")
     ap.add_argument("--rhs", type=int, default=256, help="right-hand sides of the multi-RHS leg")
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-RHS leg in the default run")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the leg that times the reference's own CUDA assembly kernel beside ours")
     ap.add_argument("--precision-form", action="store_true",
                     help="run only the N = 81920, k = 40 precision-form leg (~165 GB) and print its JSON")
     ap.add_argument("--single", action="store_true",
@@ -203,9 +209,16 @@ def peaks():
 
 
 # ---------------------------------------------------------------------------------------------
-# CPU baseline (oracle restatement of the reference CPU path), bounded sample
+# CPU path (oracle restatement of the reference CPU code): whole solves, nothing extrapolated
 # ---------------------------------------------------------------------------------------------
-def cpu_baseline(level: int, k: float, fp64_matvecs: int, budget_s: float = 12.0):
+METRIC = "BEM solves/s at <=1e-5 rel err vs FP64 (mixed-precision solve, dense Burton-Miller TBEM)"
+
+
+def cpu_solve(level: int, k: float):
+    """One whole solve of the workload on the host cores by the oracle (C++ restatement of the
+    reference CPU path, OpenMP over rows): assembly of all N rows (build_tbem_system_with_beta_parallel,
+    tbem.rs:1284-1466), the incident right-hand side, and restarted GMRES(50) from x0 = 0 to rtol 1e-8
+    with its real iteration count (gmres.rs:631-1000). Returns the timings and counts."""
     from oracle import oracle as O
 
     O.build()
@@ -213,59 +226,67 @@ def cpu_baseline(level: int, k: float, fp64_matvecs: int, budget_s: float = 12.0
     n = tris.shape[0]
     ph = O.physics_for_k(k)
     beta = O.bm_beta(ph)
-    # assembly: time a block of rows, grow it until ~budget/2 seconds
-    rows, t_rows = 8, 0.0
-    while True:
-        r0 = min(n // 3, n - rows)
-        t0 = time.perf_counter()
-        O.assemble(nodes, tris, ph, beta, rows=(r0, r0 + rows))
-        t_rows = time.perf_counter() - t0
-        if t_rows > budget_s / 4 or rows >= n:
-            break
-        rows = min(n, rows * 4)
-    t_asm = t_rows * n / rows
-    # dense complex128 matvec on a sample matrix, scaled by bytes (16 n^2)
-    ns = 4096
-    rng = np.random.default_rng(0x5EED)
-    A = (rng.standard_normal((ns, ns)) + 1j * rng.standard_normal((ns, ns))).astype(np.complex128)
-    x = rng.standard_normal(ns) + 0j
-    O.matvec(A, x)
-    reps, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < budget_s / 4:
-        O.matvec(A, x)
-        reps += 1
-    t_mv_s = (time.perf_counter() - t0) / reps
-    t_mv = t_mv_s * (n / ns) ** 2
-    t_solve = t_asm + fp64_matvecs * t_mv
-    return {
-        "value": 1.0 / t_solve, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-        "sample": (f"oracle (C++ restatement, OpenMP {os.cpu_count()} threads): assembly of {rows} of {n} rows "
-                   f"({t_rows:.2f} s, scaled x{n / rows:.0f}) + complex128 matvec at n={ns} "
-                   f"({t_mv_s * 1e3:.1f} ms, scaled by bytes to n={n}) x {fp64_matvecs} matvecs of the FP64 GMRES"),
-        "assembly_s": t_asm, "matvec_s": t_mv,
-    }
+    t0 = time.perf_counter()
+    A, _ = O.assemble(nodes, tris, ph, beta)
+    t1 = time.perf_counter()
+    c, nrm, _ = O.element_geometry(nodes, tris)
+    b = O.rhs_plane_wave(c, nrm, ph, beta, np.array([[0.0, 0.0, 1.0]]))[:, 0]
+    x, res = O.gmres(A, b, restart=RESTART, max_iterations=100, tol=TOL)
+    t2 = time.perf_counter()
+    del A
+    return {"n": n, "s": t2 - t0, "assembly_s": t1 - t0, "solve_s": t2 - t1, "iterations": int(res.iterations),
+            "matvecs": int(res.matvecs), "converged": bool(res.converged), "residual": float(res.residual)}
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample_text(r) -> str:
+    return (f"oracle (C++ restatement of the reference CPU path, OpenMP {cpu_threads()} threads): one whole "
+            f"solve of N={r['n']}: assembly of all {r['n']} rows ({r['assembly_s']:.2f} s) + incident RHS + "
+            f"GMRES({RESTART}) from x0 = 0 to rtol {TOL}: {r['iterations']} iterations, {r['matvecs']} "
+            f"complex128 matvecs ({r['solve_s']:.2f} s), converged={r['converged']}")
+
+
+def cpu_baseline(level: int, k: float):
+    r = cpu_solve(level, k)
+    return {"value": 1.0 / r["s"], "unit": "solves/s", "cores": cpu_threads(), "kind": "port",
+            "sample": cpu_sample_text(r), "assembly_s": r["assembly_s"], "solve_s": r["solve_s"]}
 
 
 def reference_arm(a, dist: Dist):
-    """--impl reference: the CPU restatement of the reference path on this host, bounded samples."""
+    """--impl reference: the reference's CPU path (its C++ restatement, oracle/) on this host's
+    cores, one whole solve of the same workload per step (W untimed, K timed, wall clock)."""
     if dist.rank != 0:
         return
-    res = []
-    for _ in range(a.warmup + a.steps):
-        res.append(cpu_baseline(a.level, a.k, fp64_matvecs=40, budget_s=8.0))
-    timed = res[a.warmup:]
-    v = float(np.mean([r["value"] for r in timed]))
+    for _ in range(a.warmup):
+        cpu_solve(a.level, a.k)
+    t0 = time.perf_counter()
+    runs = [cpu_solve(a.level, a.k) for _ in range(a.steps)]
+    t = time.perf_counter() - t0
+    v = a.steps / t
+    n = runs[-1]["n"]
     line = {
-        "impl": "reference", "metric": "BEM solves/s (dense Burton-Miller TBEM assembly + GMRES)",
+        "impl": "reference", "metric": METRIC,
         "value": v, "unit": "solves/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "c128", "data": "synthetic (icosphere geometry, analytic plane wave)",
-        "config": {"workload": f"rigid sphere icosphere L{a.level} (N={20 * 4 ** a.level}), k={a.k}, "
-                               f"Burton-Miller beta=i/k, GMRES({RESTART}) rtol {TOL}"},
-        "cpu_baseline": {k: timed[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128", "data": "synthetic (icosphere geometry, analytic incident plane wave)",
+        "config": {"workload": f"rigid sphere icosphere L{a.level} (N={n}), k={a.k}, beta=i/k, plane wave +z; "
+                               f"one step = assembly of all rows + RHS + GMRES({RESTART}) from x0 = 0 to rtol {TOL} "
+                               "(FP64 throughout: error vs FP64 is zero)",
+                   "N": n, "parallelism": "host cores (rank 0 only)"},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cpu_threads(), "kind": "port",
+                         "sample": cpu_sample_text(runs[-1]) + f"; {a.steps} timed solves, wall clock"},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the Rust reference cannot be built here (no rustc/cargo); this arm times its C++ "
-                "restatement (oracle/) and assumes 40 FP64 matvecs per solve",
+        "iterations": [r["iterations"] for r in runs],
+        "assembly_s_median": float(np.median([r["assembly_s"] for r in runs])),
+        "solve_s_median": float(np.median([r["solve_s"] for r in runs])),
+        "note": "the Rust reference cannot be built here (no rustc/cargo); this arm times its C++ restatement "
+                "(oracle/), whole solves, on the host cores",
     }
     print(json.dumps(line), flush=True)
 
@@ -280,6 +301,9 @@ MODES = {
     "mixed": ("SB_PRECISION_FP32", "ir"),
     "mixed_fp64_matrix": ("SB_PRECISION_FP64_FP32", "ir"),
     "plain_fp64": ("SB_PRECISION_FP64", "fp64"),
+    # FP64 GMRES(50) with the same block-Jacobi right preconditioner as `mixed_half_bj` (blocks of
+    # BJ_BLOCK): the like-for-like FP64 form of the preconditioned headline
+    "plain_fp64_bj": ("SB_PRECISION_FP64", "fp64bj"),
 }
 # Inner tolerance of the refinement with the complex-half inner matrix: the half copy limits each
 # refinement to about three digits, so a tighter inner solve buys nothing.
@@ -329,6 +353,7 @@ def main():
     ph = sb.PhysicsParams.for_wavenumber(a.k)
     beta = ph.burton_miller_beta()
     mesh = sb.Mesh(nodes, tris, device=dev)
+    near_pairs = float(mesh.info().n_near_pairs)  # pairs the near kernel owns (the far kernel skips them)
     dirs = np.array([[0.0, 0.0, 1.0]])
     rt = _cudart()
     b_d = _dev_alloc(rt, 16 * n)  # device-resident b and x (caller-owned device memory)
@@ -351,7 +376,8 @@ def main():
                 cfg = ir if solver == "ir" else ir16
                 L.check(lib.sb_gmres_mixed_device(op.handle, b_d, x_d, 0, ct.byref(cfg), ct.byref(st)))
             else:
-                L.check(lib.sb_gmres_device(op.handle, b_d, x_d, 0, ct.byref(gc), 0, ct.byref(st)))
+                pk = L.SB_PRECOND_BLOCK_JACOBI if solver == "fp64bj" else L.SB_PRECOND_IDENTITY
+                L.check(lib.sb_gmres_device(op.handle, b_d, x_d, 0, ct.byref(gc), pk, ct.byref(st)))
             return L.SbGmresStats.from_buffer_copy(st)
         return step
 
@@ -369,9 +395,11 @@ def main():
 
     results, x_ref = {}, None
     live = {}  # per headline-capable mode: (live profile, class breakdown, clocks, launches)
-    for name in ("plain_fp64", "mixed_fp64_matrix", "mixed", "mixed_half", "mixed_half_bj"):
+    for name in ("plain_fp64", "plain_fp64_bj", "mixed_fp64_matrix", "mixed", "mixed_half", "mixed_half_bj"):
         prec, solver = MODES[name]
         op = sb.build_tbem_system_with_beta(mesh, ph, beta, getattr(sb, prec))
+        if solver == "fp64bj":
+            L.check(lib.sb_operator_set_block_jacobi_size(op.handle, BJ_BLOCK))
         if solver in ("ir16", "ir16bj"):
             op.set_inner_precision(sb.SB_INNER_FP16)
         if solver == "ir16bj":
@@ -399,7 +427,7 @@ def main():
             # that class on its stream; the kernel-class breakdown from a third repetition with
             # every class timed.
             live_prof = L.SbProfile()
-            L.check(lib.sb_profile_enable_classes(1 << getattr(L, cls)))
+            L.check(lib.sb_profile_enable_classes((1 << getattr(L, cls)) | (1 << L.SB_PROF_FAR)))
             for _ in range(a.steps):
                 step()
             rt.cudaDeviceSynchronize()
@@ -423,6 +451,8 @@ def main():
             results[name]["inner"] = "complex-half matrix, inner tolerance %g" % HALF_INNER_TOL
         if solver == "ir16bj":
             results[name]["inner"] += ", block-Jacobi right preconditioner (blocks of %d)" % BJ_BLOCK
+        if solver == "fp64bj":
+            results[name]["preconditioner"] = "block-Jacobi, right, blocks of %d (as mixed_half_bj)" % BJ_BLOCK
         op.close()
     # Headline: the fastest mixed form whose solution is within 1e-5 of the FP64 one.
     ok = [m for m in HEADLINE_MODES if results[m]["error_vs_fp64"] <= 1e-5]
@@ -473,6 +503,10 @@ def main():
         multi = multi_rhs_leg(sb, a, dist, dev, rt)
         a.level = lvl
 
+    extra_legs = {}
+    if not a.no_ref_gpu:
+        extra_legs["reference_gpu_assembly"] = reference_gpu_leg(sb, L, lib, dev)
+
     # ---- roofline of the dominant kernel of the headline step ----
     pk, pk_kind = peaks()
     names = L.PROF_NAMES
@@ -499,41 +533,67 @@ def main():
     traffic = None if tpe is None else tpe * n * n
     kernel_names = {"gemv16": "k_gemv_n_c16 (complex-half matrix, FP32 vectors)",
                     "gemv32": "k_gemv_n_c64 (complex64 matrix; FP32 or FP64 vectors)"}
-    roof = {"kernel": kernel_names[hbm_kind],
-            "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_source": pk_kind,
-            "bytes_per_launch": bytes_mv[hbm_kind], "avg_launch_ms": avg * 1e3,
-            "launches": int(live_n), "share_of_kernel_time": ms[hbm_kind] / max(total_ms, 1e-9),
-            "measured": "CUDA events on the operator's stream around each matvec launch, in a repetition of "
-                        "the K timed steps (the timed steps themselves carry no events)",
-            "dominant_kernel_class": dominant}
-    evals = 13.0 * n * (n - 1)
-    far_avg = ms["far"] / max(launches["far"], 1) / 1e3
-    # Far-field roofline in the assembly convention: 90 FP64-equivalent flops per point
-    # evaluation (sincos, sqrt and reciprocals not counted). The FP32 far kernel has no measured
-    # peak to divide by: the nominal FP32 FMA rate of the part at its maximum SM clock stands in.
-    fp32_nominal = 148 * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    roof_gemv = {"kernel": kernel_names[hbm_kind],
+                 "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                 "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_source": pk_kind,
+                 "bytes_per_launch": bytes_mv[hbm_kind], "avg_launch_ms": avg * 1e3,
+                 "launches": int(live_n), "share_of_kernel_time": ms[hbm_kind] / max(total_ms, 1e-9),
+                 "measured": "CUDA events on the operator's stream around each matvec launch, in a repetition of "
+                             "the K timed steps (the timed steps themselves carry no events)"}
+    # Far field (FP32 kernel): point evaluations of the 13-point far leaf over the far pairs, in
+    # the assembly convention of 90 FP64-equivalent flops per evaluation (sincos, sqrt and
+    # reciprocals not counted), against the FP32 FMA rate measured on this device.
+    far_pairs = float(n) * (n - 1) - near_pairs
+    evals = 13.0 * far_pairs
+    far_n = prof_live.launches[L.SB_PROF_FAR]
+    far_avg = prof_live.ms[L.SB_PROF_FAR] / max(far_n, 1) / 1e3
+    fp32_s, fp32_p = ct.c_double(), ct.c_double()
+    L.check(lib.sb_measure_fp32_rate(dev, ct.byref(fp32_s), ct.byref(fp32_p)))
+    fp32_peak = max(fp32_s.value, fp32_p.value)
     far_tflops = 90.0 * evals / far_avg / 1e12
+    # bytes the far kernel must write: the complex64 entries of the far pairs and, with the
+    # complex-half copy, their FP16 pairs
+    far_bytes = far_pairs * (8.0 + (0.0 if head_mode == "mixed" else 4.0))
+    roof_far = {"kernel": "k_far32 (FP32 far field, FP64 phase, packed f32x2)",
+                "bound": "fp32 (FMA pipe with the special-function unit)",
+                "achieved": far_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": far_tflops / fp32_peak, "traffic": None, "peak_source":
+                    "measured on this device (sb_measure_fp32_rate: FMA chains on every SM, best of scalar %.1f "
+                    "and packed f32x2 %.1f TFLOP/s)" % (fp32_s.value, fp32_p.value),
+                "flop_convention": "90 FP64-equivalent flop per point evaluation, 13 evaluations per far pair "
+                                   "(%.4g far pairs)" % far_pairs,
+                "evals_per_s": evals / far_avg, "avg_launch_ms": far_avg * 1e3, "launches": int(far_n),
+                "bytes_written_per_launch": far_bytes,
+                "write_gbs": far_bytes / far_avg / 1e9,
+                "share_of_kernel_time": ms["far"] / max(total_ms, 1e-9),
+                "measured": "CUDA events on the operator's stream around each far-kernel launch, in the same "
+                            "repetition of the K timed steps"}
+    if ms["far"] >= ms[hbm_kind]:
+        roof, roof2 = roof_far, roof_gemv
+    else:
+        roof, roof2 = roof_gemv, roof_far
+    roof["dominant_kernel_class"] = dominant
     assembly = {"far_kernel_ms": far_avg * 1e3, "far_evals_per_s": evals / far_avg,
                 "near_kernel_ms": ms["near"] / max(launches["near"], 1),
                 "self_kernel_ms": ms["self"] / max(launches["self"], 1),
+                "near_pairs": int(near_pairs),
                 "share_of_kernel_time": (ms["far"] + ms["near"] + ms["self"]) / max(total_ms, 1e-9),
-                "far_roofline": {"kernel": "k_far32 (FP32 far field, FP64 phase, packed f32x2)",
-                                 "bound": "FP32 FMA pipe + special-function unit",
-                                 "achieved": far_tflops, "unit": "TFLOP/s (90 FP64-equivalent flop per evaluation)",
-                                 "peak": fp32_nominal, "frac": far_tflops / fp32_nominal,
-                                 "peak_source": "nominal FP32 FMA rate, 148 SMs x 128 lanes x 2 flop x max SM "
-                                                "clock (no measured FP32 peak)"}}
+                "fp32_fma_rate_tflops": {"scalar": fp32_s.value, "packed": fp32_p.value}}
 
     cpu = None
     if not a.no_cpu and dist.rank == 0:
-        cpu = cpu_baseline(a.level, a.k, results["plain_fp64"]["matvecs"])
+        cpu = cpu_baseline(a.level, a.k)
     head = results[head_mode]
+    # The FP64 form with the same preconditioner as the headline's (like for like), else plain.
+    like = "plain_fp64_bj" if head_mode == "mixed_half_bj" else "plain_fp64"
     line = {
-        "metric": "BEM solves/s at <=1e-5 rel err vs FP64 (mixed-precision solve, dense Burton-Miller TBEM)",
+        "metric": METRIC,
         "value": head["value"], "unit": "solves/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64 (FP64 phase, near/self, refinement)",
+        "vs_baseline": None,
+        "dtype": ("c64 matrix (FP64 phase, near/self, refinement)" if head_mode == "mixed" else
+                  "c64 matrix + complex-half (FP16 pair, per-row power-of-two scale) inner copy; FP64 phase, "
+                  "near/self, refinement"),
         "data": "synthetic (icosphere geometry, analytic incident plane wave)",
         "config": {"workload": f"rigid sphere icosphere L{a.level} (N={n}), k={a.k}, beta=i/k, plane wave +z; "
                                f"one step = assembly + RHS + GMRES({RESTART}) inner solve on the "
@@ -545,22 +605,107 @@ def main():
         "headline_mode": head_mode,
         "error_vs_fp64": head["error_vs_fp64"],
         "speedup_vs_plain_fp64": head["value"] / results["plain_fp64"]["value"],
-        "modes": results,
+        "speedup_vs_plain_fp64_bj": head["value"] / results["plain_fp64_bj"]["value"],
         "roofline": roof,
-        "assembly": assembly,
-        "kernel_ms_per_step": {kk: v / a.steps for kk, v in ms.items() if v > 0},
+        "roofline_second": roof2,
         "gpu_launches": launches_timed,
         "clocks": clk,
         "e2e": e2e,
+        "cpu_baseline": None if cpu is None else {kk: cpu[kk] for kk in ("value", "unit", "cores", "kind", "sample")},
+        "modes": results,
+        "assembly": assembly,
+        "kernel_ms_per_step": {kk: v / a.steps for kk, v in ms.items() if v > 0},
         "sweep": sweep,
         "multi_rhs": multi,
-        "cpu_baseline": None if cpu is None else {kk: cpu[kk] for kk in ("value", "unit", "cores", "kind", "sample")},
     }
+    line.update(extra_legs)
+    # Compact summary last (the part of the line that a truncated log tail keeps).
+    summ = {"headline": head_mode, "like_for_like": like,
+            "ms_per_step": {m: round(r["ms_per_step"], 3) for m, r in results.items()},
+            "speedup_vs_plain_fp64": round(line["speedup_vs_plain_fp64"], 3),
+            "speedup_vs_plain_fp64_bj": round(line["speedup_vs_plain_fp64_bj"], 3),
+            "iterations": {m: r["iterations"] for m, r in results.items()},
+            "error_vs_fp64": {m: float("%.3g" % r["error_vs_fp64"]) for m, r in results.items()}}
+    if sweep:
+        summ["sweep"] = {"value": round(sweep["value"], 2), "form": sweep["inner_form"],
+                         "speedup_vs_plain_fp64": round(sweep["speedup_vs_plain_fp64"], 3),
+                         "speedup_vs_plain_fp64_bj": round(sweep["speedup_vs_plain_fp64_bj"], 3),
+                         "max_error_vs_fp64": float("%.3g" % sweep["max_error_vs_fp64"])}
+    if multi:
+        summ["multi_rhs"] = {"rhs_solves_per_s": round(multi["rhs_solves_per_s"], 1),
+                             "speedup_vs_plain_fp64": round(multi["speedup_vs_plain_fp64"], 2),
+                             "tensor_frac": round(multi["tensor_kernel"]["frac"], 3)}
+    summ["roofline_frac"] = {"gemv_hbm": round(roof_gemv["frac"], 3), "far32_fp32": round(roof_far["frac"], 3)}
+    summ["far32_ms"] = round(far_avg * 1e3, 3)
+    if cpu is not None:
+        summ["cpu_solves_per_s"] = float("%.4g" % cpu["value"])
+    rg = extra_legs.get("reference_gpu_assembly") or {}
+    if "N1280_k2_all_pairs" in rg:
+        summ["reference_gpu_assembly_speedup_per_pair"] = {
+            kk: round(rg[kk]["speedup_per_pair"], 1) for kk in ("N1280_k2_all_pairs", "N20480_k10_rows0_128") if kk in rg}
+    line["summary"] = summ
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
     rt.cudaFree(b_d)
     rt.cudaFree(x_d)
     dist.close()
+
+
+def reference_gpu_leg(sb, L, lib, dev):
+    """Baseline leg: the reference's CUDA assembly kernel on the same B200.
+
+    The reference's GPU path (tbem.rs:5165-5405) builds a quadrature chart per pair on the host
+    and integrates every pair with its kernel sonium_bem_quadrature_pair_c64 (bem_kernels.cu:
+    839-967), one thread per pair, 128 threads per block. That kernel, compiled from the reference's
+    source (oracle/_ref/), is timed here on the oracle's restatement of those charts (inputs
+    resident on the device, kernel time by CUDA events, best of a few launches) against this
+    library's FP64 assembly of the same system (far tiles + near-pair replay + self terms, device
+    time of sb_assemble_into). The small configuration (N = 1280, k = 2) runs in full; at N = 20480
+    the charts of all pairs would take 0.5 TB, so the reference kernel runs on the first 128 rows
+    (2.6 M pairs) and the per-pair rates are compared."""
+    from oracle import oracle as O
+    from oracle import ref_kernels as RK
+
+    try:
+        if RK.build() is None:
+            return {"unavailable": "oracle/_ref/bem_kernels.cubin is missing (built where the reference tree is)"}
+        kern = RK.RefPairKernel(dev)
+        out = {"kernel": "sonium_bem_quadrature_pair_c64 (reference source, compiled unchanged for compute_100)",
+               "timing": "kernel only, charts resident on the device, CUDA events, best of the launches"}
+        for name, level, k, rows in (("N1280_k2_all_pairs", 3, 2.0, None), ("N20480_k10_rows0_128", 5, 10.0, (0, 128))):
+            nodes, tris = O.icosphere(RADIUS, level)
+            n = tris.shape[0]
+            t0 = time.perf_counter()
+            pairs, samples = O.chart(nodes, tris, k, rows=rows)
+            t_chart = time.perf_counter() - t0
+            kern.run(pairs, samples, k, 1.0, reps=1)  # warm-up
+            ms_ref = min(kern.run(pairs, samples, k, 1.0, reps=1)[1] for _ in range(3))
+            npairs = pairs.shape[0]
+            nsamp = samples.shape[0]
+            del pairs, samples
+            mesh = sb.Mesh(nodes, tris, device=dev)
+            ph = sb.PhysicsParams.for_wavenumber(k)
+            beta = ph.burton_miller_beta()
+            op = sb.build_tbem_system_with_beta(mesh, ph, beta)
+            ours = []
+            for _ in range(3):
+                op.reassemble(ph, beta)
+                ours.append(op.info().assembly_ms)
+            ms_ours = min(ours)
+            op.close()
+            mesh.close()
+            ref_per_pair = ms_ref / npairs
+            ours_per_pair = ms_ours / (n * n)
+            out[name] = {"N": n, "k": k, "pairs": int(npairs), "samples": int(nsamp),
+                         "reference_kernel_ms": ms_ref, "reference_host_chart_s": t_chart,
+                         "ours_fp64_assembly_ms": ms_ours,
+                         "ns_per_pair": {"reference": 1e6 * ref_per_pair, "ours": 1e6 * ours_per_pair},
+                         "speedup_per_pair": ref_per_pair / ours_per_pair,
+                         "scope": ("all pairs" if rows is None else f"reference on rows {rows[0]}-{rows[1]} of {n} "
+                                   "(per-pair rate), ours on the whole matrix")}
+        return out
+    except Exception as e:  # a baseline leg never fails the bench line
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def sweep_leg(sb, a, dist, dev, rt):
@@ -621,10 +766,11 @@ def sweep_leg(sb, a, dist, dev, rt):
         forms[form_name] = {"t": t_batch, "st0": st0, "xb": xb, "assembly_ms": asm_ms, "solve_ms": solve_ms}
     form, tune_p, tune_s = batch.assembly_tuning()
     batch.close()
-    # plain FP64 baseline, one instance after another
+    # plain FP64 baseline, one instance after another; and the same with the sweep's block-Jacobi
+    # right preconditioner (blocks of BJ_BLOCK_SWEEP, as the half_inner_bj form)
     ops = {}
 
-    def fp64_sweep():
+    def fp64_sweep(bj=False):
         out = []
         for m, ph, be in zip(meshes, physics, betas):
             key = id(m)
@@ -633,18 +779,24 @@ def sweep_leg(sb, a, dist, dev, rt):
             else:
                 ops[key].reassemble(ph, be)
             b = sb.rhs_plane_wave(m, ph, be, [[0.0, 0.0, 1.0]])[:, 0]
-            out.append(sb.gmres(ops[key], b, sb.GmresConfig(100, RESTART, TOL)))
+            pre = sb.BlockJacobiPreconditioner(ops[key], BJ_BLOCK_SWEEP) if bj else None
+            out.append(sb.gmres(ops[key], b, sb.GmresConfig(100, RESTART, TOL), preconditioner=pre))
         return out
 
     fp64_sweep()  # warm-up: allocations, graphs
     t_fp64, sols = wall(fp64_sweep)
+    fp64_sweep(True)
+    t_fp64_bj, sols_bj = wall(lambda: fp64_sweep(True))
     fp64_iters = [int(s.iterations) for s in sols]
+    fp64_bj_iters = [int(s.iterations) for s in sols_bj]
+    bj_err = max(float(np.linalg.norm(sb_.x - s.x) / np.linalg.norm(s.x)) for sb_, s in zip(sols_bj, sols))
     for f in forms.values():
         f["errs"] = [float(np.linalg.norm(f["xb"][i] - s.x) / np.linalg.norm(s.x)) for i, s in enumerate(sols)]
         f["value"] = dist.world * len(sols) * a.steps / f["t"]
     for o in ops.values():
         o.close()
     plain = dist.world * len(sols) / t_fp64
+    plain_bj = dist.world * len(sols_bj) / t_fp64_bj
     # the fastest form within the metric's 1e-5 of the FP64 solutions
     ok = [k for k, f in forms.items() if max(f["errs"]) <= 1e-5]
     best = max(ok, key=lambda k: forms[k]["value"]) if ok else "fp32_inner"
@@ -661,6 +813,9 @@ def sweep_leg(sb, a, dist, dev, rt):
         "value": batched, "unit": "solves/s", "ms_per_step": 1e3 * t_batch / a.steps,
         "plain_fp64": plain, "plain_fp64_ms_per_sweep": 1e3 * t_fp64,
         "speedup_vs_plain_fp64": batched / plain,
+        "plain_fp64_bj": plain_bj, "plain_fp64_bj_ms_per_sweep": 1e3 * t_fp64_bj,
+        "speedup_vs_plain_fp64_bj": batched / plain_bj,
+        "plain_fp64_bj_max_error_vs_fp64": bj_err,
         "max_error_vs_fp64": max(errs), "median_error_vs_fp64": float(np.median(errs)),
         "all_converged": bool(all(s.converged for s in st0)),
         "max_residual": float(max(s.residual for s in st0)),
@@ -668,11 +823,13 @@ def sweep_leg(sb, a, dist, dev, rt):
         "assembly_ms": asm_ms, "solve_ms": solve_ms,
         "assembly_form": {1: "persistent", 2: "streams"}.get(form, str(form)),
         "assembly_autotune_ms": {"persistent": tune_p, "streams": tune_s},
-        "iterations_batched": [int(s.iterations) for s in st0], "iterations_fp64": fp64_iters,
+        "iterations_total": {"batched": int(sum(s.iterations for s in st0)), "fp64": int(sum(fp64_iters)),
+                             "fp64_bj": int(sum(fp64_bj_iters))},
         "inner_form": best,
         "forms": {k: {"value": f["value"], "ms_per_step": 1e3 * f["t"] / a.steps, "assembly_ms": f["assembly_ms"],
                       "solve_ms": f["solve_ms"], "max_error_vs_fp64": max(f["errs"]),
                       "speedup_vs_plain_fp64": f["value"] / plain,
+                      "speedup_vs_plain_fp64_bj": f["value"] / plain_bj,
                       "inner_tolerance": cfg.inner_tolerance if k == "fp32_inner" else cfg16.inner_tolerance,
                       "block_jacobi": BJ_BLOCK_SWEEP if k == "half_inner_bj" else None,
                       "iterations_total": int(sum(s.iterations for s in f["st0"]))}
@@ -867,7 +1024,8 @@ def single_solves(sb, level, k, dev, modes=None):
         elif solver == "ir":
             s = sb.gmres_mixed(op, b, sb.IrConfig(20, TOL, RESTART, 20, 1e-5))
         else:
-            s = sb.gmres(op, b, sb.GmresConfig(100, RESTART, TOL))
+            pre = sb.BlockJacobiPreconditioner(op, BJ_BLOCK) if solver == "fp64bj" else None
+            s = sb.gmres(op, b, sb.GmresConfig(100, RESTART, TOL), preconditioner=pre)
         print(f"{name}: N={tris.shape[0]} iterations {s.iterations} matvecs {s.matvecs} residual {s.residual:.2e}")
         op.close()
 

@@ -228,11 +228,22 @@ SB_API int sb_operator_apply_device(const sb_operator* op, int trans, const sb_c
 SB_API int sb_operator_apply_device_noalloc(const sb_operator* op, int trans,
                                             const sb_complex* x_dev, sb_complex* y_dev);
 
-/* Preconditioner<Complex64>::apply_into (traits.rs:3645-3720): identity or Jacobi (A_ii^-1). */
+/* Preconditioner<Complex64>::apply_into (traits.rs:3645-3720): identity or Jacobi (A_ii^-1).
+ * SB_PRECOND_BLOCK_JACOBI (no reference counterpart; the interface is the same apply_into):
+ * y = M^-1 x with M the block diagonal of the complex128 matrix in blocks of the size set by
+ * sb_operator_set_block_jacobi_size (default 128) spatially close elements (consecutive in the
+ * Morton order of the element centroids; index order without a mesh), each block rounded to
+ * complex64 and inverted on the device (Gauss-Jordan with partial pivoting, FP32; a singular
+ * block keeps the identity) after each assembly, applied with FP64 vectors and accumulation.
+ * Needs the complex128 matrix. */
 #define SB_PRECOND_IDENTITY 0
 #define SB_PRECOND_JACOBI 1
+#define SB_PRECOND_BLOCK_JACOBI 2
 SB_API int sb_preconditioner_apply(const sb_operator* op, int precond, const sb_complex* x,
                                    sb_complex* y);
+/* Block size (32, 64, 96 or 128) of SB_PRECOND_BLOCK_JACOBI and of the block-Jacobi inner
+ * preconditioner of sb_gmres_mixed (no reference counterpart). */
+SB_API int sb_operator_set_block_jacobi_size(sb_operator* op, int block_size);
 
 /* IncidentField::compute_rhs_with_beta for plane waves (incident.rs:216-245,315-331,807-833):
  * rhs[i*r+q] = -(gamma p_inc + beta tau dp_inc/dn) at the element centroids, for r directions
@@ -271,7 +282,10 @@ typedef struct sb_gmres_stats {
 } sb_gmres_stats;
 
 /* gmres / gmres_preconditioned (gmres.rs:286-305, 631-1047, finalize 159-247) with CGS + one
- * DGKS pass (0.707), Givens on the host in FP64. b, x0 (NULL = 0) and x are host buffers. */
+ * DGKS pass (0.707), Givens on the host in FP64. b, x0 (NULL = 0) and x are host buffers.
+ * precond: SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI (left, as gmres_preconditioned) or
+ * SB_PRECOND_BLOCK_JACOBI (right: GMRES on (A M^-1) z = b - A x0, x = x0 + M^-1 z; convergence is
+ * tested on b - A x relative to ||b|| as without a preconditioner). */
 SB_API int sb_gmres(const sb_operator* op, const sb_complex* b, const sb_complex* x0,
                     const sb_gmres_config* cfg, int precond, sb_complex* x, sb_gmres_stats* stats);
 /* Same with device-resident b / x (x holds x0 on entry when x0_given != 0). */
@@ -499,6 +513,10 @@ SB_API int sb_profile_enable(int on);
 SB_API int sb_profile_enable_classes(unsigned mask);
 /* Totals since the last reset (synchronises the recorded events); reset != 0 clears them. */
 SB_API int sb_profile_read(sb_profile* out, int reset);
+/* FP32 fused multiply-add rate of `device` in TFLOP/s (2 flop per lane and FMA), measured by a
+ * kernel of 8 independent FMA chains per thread on every SM, scalar (fmaf) and packed (sm_100's
+ * f32x2 FMA): the denominator of the FP32 far-field kernel's roofline. No reference counterpart. */
+SB_API int sb_measure_fp32_rate(int device, double* scalar_tflops, double* packed_tflops);
 /* CUDA event helpers on an operator's stream, for timing whole solves on the device. */
 SB_API int sb_event_create(void** event);
 SB_API int sb_event_destroy(void* event);

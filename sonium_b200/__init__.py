@@ -6,8 +6,9 @@ The compute path is the CUDA shared library built from ``sonium_b200/csrc`` (C A
 from ._lib import (SB_INNER_FP16, SB_INNER_FP32, SB_INNER_PRECOND_BLOCK_JACOBI, SB_INNER_PRECOND_NONE,
                    SB_BASIS_CONSTANT, SB_BASIS_LINEAR, SB_BASIS_QUADRATIC, SB_BC_PRESSURE, SB_BC_VELOCITY, SB_INJECT_ALLOC, SB_INJECT_LAUNCH, SB_INJECT_NONE,
                    SB_OP_C, SB_OP_N, SB_OP_T, SB_PRECISION_FP32, SB_PRECISION_FP32_HALF, SB_PRECISION_FP64,
-                   SB_PRECISION_FP64_FP32, SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI, SoniumError)
-from .tbem import (DenseMatrixOperator, GcroDrConfig, GcroDrSubspace, build_tbem_system_linear, gcro_dr,
+                   SB_PRECISION_FP64_FP32, SB_PRECOND_BLOCK_JACOBI, SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI,
+                   SoniumError)
+from .tbem import (BlockJacobiPreconditioner, DenseMatrixOperator, GcroDrConfig, GcroDrSubspace, build_tbem_system_linear, gcro_dr,
                    build_tbem_system_discontinuous_stabilized, build_tbem_system_quadratic_stabilized,
                    rhs_plane_wave_at,
                    GmresConfig, GmresSolution, IrConfig, JacobiPreconditioner, LinearOperator, Mesh,
@@ -29,6 +30,7 @@ __all__ = [
     "build_tbem_system_discontinuous_stabilized", "build_tbem_system_quadratic_stabilized",
     "SB_BC_PRESSURE", "SB_BC_VELOCITY", "SB_INJECT_ALLOC", "SB_INJECT_LAUNCH", "SB_INJECT_NONE",
     "SB_OP_C", "SB_OP_N", "SB_OP_T", "SB_PRECISION_FP32", "SB_PRECISION_FP64", "SB_PRECISION_FP64_FP32",
-    "SB_PRECOND_IDENTITY", "SB_PRECOND_JACOBI", "SB_INNER_FP16", "SB_INNER_FP32",
+    "SB_PRECOND_IDENTITY", "SB_PRECOND_JACOBI", "SB_PRECOND_BLOCK_JACOBI", "BlockJacobiPreconditioner",
+    "SB_INNER_FP16", "SB_INNER_FP32",
     "SB_INNER_PRECOND_BLOCK_JACOBI", "SB_INNER_PRECOND_NONE", "SB_PRECISION_FP32_HALF",
 ]

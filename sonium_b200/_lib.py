@@ -30,7 +30,7 @@ SB_INNER_FP16 = 1
 SB_INNER_PRECOND_NONE = 0
 SB_INNER_PRECOND_BLOCK_JACOBI = 1
 SB_OP_N, SB_OP_T, SB_OP_C = 0, 1, 2
-SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI = 0, 1
+SB_PRECOND_IDENTITY, SB_PRECOND_JACOBI, SB_PRECOND_BLOCK_JACOBI = 0, 1, 2
 SB_BC_VELOCITY, SB_BC_PRESSURE = 0, 1
 SB_INJECT_NONE, SB_INJECT_ALLOC, SB_INJECT_LAUNCH = 0, 1, 2
 SB_SOLVER_CONVERGED, SB_SOLVER_MAX_ITERATIONS, SB_SOLVER_BREAKDOWN, SB_SOLVER_NUMERICAL_ERROR = 0, 1, 2, 3
@@ -143,6 +143,8 @@ _SIGNATURES = {
     "sb_operator_apply_device": ([P, ct.c_int, P, P], ct.c_int),
     "sb_operator_apply_device_noalloc": ([P, ct.c_int, P, P], ct.c_int),
     "sb_preconditioner_apply": ([P, ct.c_int, P, P], ct.c_int),
+    "sb_operator_set_block_jacobi_size": ([P, ct.c_int], ct.c_int),
+    "sb_measure_fp32_rate": ([ct.c_int, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
     "sb_rhs_plane_wave": ([P, ct.POINTER(SbPhysics), SbComplex, P, P, ct.c_int64, P], ct.c_int),
     "sb_gmres": ([P, P, P, ct.POINTER(SbGmresConfig), ct.c_int, P, ct.POINTER(SbGmresStats)], ct.c_int),
     "sb_gmres_device": ([P, P, P, ct.c_int, ct.POINTER(SbGmresConfig), ct.c_int, ct.POINTER(SbGmresStats)], ct.c_int),

@@ -1294,20 +1294,7 @@ namespace {
 
 template <class F>
 int guarded_batch(F&& f) {
-    try {
-        clear_error();
-        f();
-        return SB_OK;
-    } catch (const Error& e) {
-        set_error(e.status, e.msg);
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        set_error(SB_ERR_OUT_OF_MEMORY, "host allocation failed");
-        return SB_ERR_OUT_OF_MEMORY;
-    } catch (...) {
-        set_error(SB_ERR_CUDA, "unknown failure");
-        return SB_ERR_CUDA;
-    }
+    return abi_guard(std::forward<F>(f));
 }
 
 }  // namespace

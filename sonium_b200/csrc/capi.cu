@@ -163,23 +163,7 @@ int device_sm_count(int device) {
 
 template <class F>
 static int guarded(F&& f) {
-    try {
-        clear_error();
-        f();
-        return SB_OK;
-    } catch (const Error& e) {
-        set_error(e.status, e.msg);
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        set_error(SB_ERR_OUT_OF_MEMORY, "host allocation failed");
-        return SB_ERR_OUT_OF_MEMORY;
-    } catch (const std::exception& e) {
-        set_error(SB_ERR_CUDA, e.what());
-        return SB_ERR_CUDA;
-    } catch (...) {
-        set_error(SB_ERR_CUDA, "unknown failure");
-        return SB_ERR_CUDA;
-    }
+    return abi_guard(std::forward<F>(f));
 }
 
 static bool all_finite(const sb_complex* v, int64_t n) {
@@ -507,6 +491,7 @@ SB_API int sb_assemble_into(sb_operator* op, const sb_physics* physics, sb_compl
         tensor_release(*op->op);
         op->op->half_valid = false;
         op->op->bj_valid = false;
+        op->op->bj64_valid = false;
         if (op->op->basis != SB_BASIS_CONSTANT)
             assemble_discontinuous(*op->op, *physics, beta.re, beta.im);
         else
@@ -867,21 +852,37 @@ SB_API int sb_gmres_multi_device(const sb_operator* op, const sb_complex* b_dev,
     });
 }
 
+// Preconditioners of the FP64 GMRES: identity, Jacobi (left) or block-Jacobi (right, needs the
+// complex128 matrix).
+static void check_gmres_precond(const Operator& o, int precond) {
+    SB_REQUIRE(precond == SB_PRECOND_IDENTITY || precond == SB_PRECOND_JACOBI || precond == SB_PRECOND_BLOCK_JACOBI,
+               SB_ERR_INVALID_ARGUMENT, "unknown preconditioner");
+    if (precond == SB_PRECOND_BLOCK_JACOBI)
+        SB_REQUIRE(o.A64.p, SB_ERR_INVALID_ARGUMENT,
+                   "SB_PRECOND_BLOCK_JACOBI needs the complex128 matrix (SB_PRECISION_FP64 or SB_PRECISION_FP64_FP32)");
+}
+
 SB_API int sb_preconditioner_apply(const sb_operator* op, int precond, const sb_complex* x, sb_complex* y) {
     return guarded([&] {
         SB_REQUIRE(op && op->op && x && y, SB_ERR_INVALID_ARGUMENT, "null argument");
-        SB_REQUIRE(precond == SB_PRECOND_IDENTITY || precond == SB_PRECOND_JACOBI, SB_ERR_INVALID_ARGUMENT,
-                   "unknown preconditioner");
         Operator& o = *op->op;
+        check_gmres_precond(o, precond);
         if (precond == SB_PRECOND_IDENTITY) {
             std::memcpy(y, x, sizeof(sb_complex) * o.n);
             return;
         }
         SB_CUDA(cudaSetDevice(o.device));
-        DevBuf dx;
+        DevBuf dx, dy;
         dx.alloc(sizeof(double2) * o.n);
         SB_CUDA(cudaMemcpyAsync(dx.p, x, sizeof(double2) * o.n, cudaMemcpyHostToDevice, o.stream));
-        jacobi_apply<double2>(o.diag.as<double2>(), dx.as<double2>(), dx.as<double2>(), o.n, o.stream);
+        if (precond == SB_PRECOND_BLOCK_JACOBI) {
+            bj64_prepare(o);
+            dy.alloc(sizeof(double2) * o.n);
+            bj64_apply(o, dx.as<double2>(), dy.as<double2>(), Gate{});
+            SB_CUDA(cudaMemcpyAsync(dx.p, dy.p, sizeof(double2) * o.n, cudaMemcpyDeviceToDevice, o.stream));
+        } else {
+            jacobi_apply<double2>(o.diag.as<double2>(), dx.as<double2>(), dx.as<double2>(), o.n, o.stream);
+        }
         SB_CUDA(cudaMemcpyAsync(y, dx.p, sizeof(double2) * o.n, cudaMemcpyDeviceToHost, o.stream));
         SB_CUDA(cudaStreamSynchronize(o.stream));
     });
@@ -954,8 +955,7 @@ SB_API int sb_gmres_device(const sb_operator* op, const sb_complex* b_dev, sb_co
     return guarded([&] {
         SB_REQUIRE(op && op->op && b_dev && x_dev && stats, SB_ERR_INVALID_ARGUMENT, "null argument");
         check_cfg(cfg);
-        SB_REQUIRE(precond == SB_PRECOND_IDENTITY || precond == SB_PRECOND_JACOBI, SB_ERR_INVALID_ARGUMENT,
-                   "unknown preconditioner");
+        check_gmres_precond(*op->op, precond);
         maybe_inject(SB_INJECT_LAUNCH);
         gmres_fp64(*op->op, reinterpret_cast<const double2*>(b_dev), reinterpret_cast<double2*>(x_dev), x0_given != 0,
                    *cfg, precond, *stats);
@@ -976,8 +976,7 @@ SB_API int sb_gmres(const sb_operator* op, const sb_complex* b, const sb_complex
         dx.alloc(sizeof(double2) * o.n);
         SB_CUDA(cudaMemcpyAsync(db.p, b, sizeof(double2) * o.n, cudaMemcpyHostToDevice, o.stream));
         if (x0) SB_CUDA(cudaMemcpyAsync(dx.p, x0, sizeof(double2) * o.n, cudaMemcpyHostToDevice, o.stream));
-        SB_REQUIRE(precond == SB_PRECOND_IDENTITY || precond == SB_PRECOND_JACOBI, SB_ERR_INVALID_ARGUMENT,
-                   "unknown preconditioner");
+        check_gmres_precond(o, precond);
         maybe_inject(SB_INJECT_LAUNCH);
         gmres_fp64(o, db.as<double2>(), dx.as<double2>(), x0 != nullptr, *cfg, precond, *stats);
         SB_CUDA(cudaMemcpyAsync(x, dx.p, sizeof(double2) * o.n, cudaMemcpyDeviceToHost, o.stream));
@@ -1055,13 +1054,24 @@ SB_API int sb_operator_set_inner_preconditioner(sb_operator* op, int kind, int b
             SB_REQUIRE(o.A32.p, SB_ERR_INVALID_ARGUMENT,
                        "the block-Jacobi inner preconditioner needs a complex64 matrix (SB_PRECISION_FP64_FP32 or "
                        "SB_PRECISION_FP32)");
-            if (block_size != o.bj_size) o.bj_valid = false;
+            if (block_size != o.bj_size) o.bj_valid = o.bj64_valid = false;
             o.bj_size = block_size;
         } else {
             o.bj_inv.release();
             o.bj_valid = false;
         }
         o.inner_precond = kind;
+    });
+}
+
+SB_API int sb_operator_set_block_jacobi_size(sb_operator* op, int block_size) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op, SB_ERR_INVALID_ARGUMENT, "null argument");
+        SB_REQUIRE(block_size == 32 || block_size == 64 || block_size == 96 || block_size == 128,
+                   SB_ERR_INVALID_ARGUMENT, "block_size must be 32, 64, 96 or 128");
+        Operator& o = *op->op;
+        if (block_size != o.bj_size) o.bj_valid = o.bj64_valid = false;
+        o.bj_size = block_size;
     });
 }
 

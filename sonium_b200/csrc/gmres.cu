@@ -141,6 +141,7 @@ struct SolveWork {
     KrylovWork<double2> k64;
     KrylovWork<float2> k32;
     DevBuf r64, r32, d32, t32, partg, nrmg, one, ax;
+    DevBuf t64, z64;  // the FP64 solver's block-Jacobi vectors (allocated on first use)
     PinnedBuf pin;
     DevBuf npart, nred;  // scratch of the ||b|| reduction
     int64_t n = 0;
@@ -162,6 +163,15 @@ struct SolveWork {
         const double2 h_one = make_double2(1.0, 0.0);
         SB_CUDA(cudaMemcpy(one.p, &h_one, sizeof(double2), cudaMemcpyHostToDevice)); SB_CUDA(cudaStreamSynchronize(0));
         ax.alloc(sizeof(double2) * n);
+        t64.release();
+        z64.release();
+    }
+    void ensure_bj64(int64_t n_) {
+        if (t64.bytes == sizeof(double2) * n_) return;
+        t64.release();
+        z64.release();
+        t64.alloc(sizeof(double2) * n_);
+        z64.alloc(sizeof(double2) * n_);
     }
 };
 
@@ -617,6 +627,72 @@ Problem<float2> problem16(const Operator& op) {
 
 }  // namespace
 
+namespace {
+
+// Right block-Jacobi preconditioning of the FP64 solver: GMRES on (A M^-1) z = b - A x0 from z = 0,
+// then x = x0 + M^-1 z. The restart and convergence tests of gmres_core see b - A M^-1 z, which is
+// b - A x for that x, so the tolerance keeps its meaning (relative to ||b||: the inner tolerance
+// is scaled by ||b|| / ||b - A x0|| when an initial guess is given).
+void gmres_fp64_block_jacobi(const Operator& op, SolveWork& sw, Problem<double2>& P, const double2* b, double2* x,
+                             bool x0_given, const sb_gmres_config& cfg, sb_gmres_stats& st) {
+    const int64_t n = op.n;
+    bj64_prepare(const_cast<Operator&>(op));
+    sw.ensure_bj64(n);
+    double2* t = sw.t64.as<double2>();
+    double2* z = sw.z64.as<double2>();
+    auto a_apply = P.apply;
+    auto a_res = P.residual;
+    P.apply = [&op, t, a_apply](const double2* xi, double2* yo, Gate g) {
+        bj64_apply(op, xi, t, g);
+        a_apply(t, yo, g);
+    };
+    P.residual = [&op, t, a_res](const double2* xi, const double2* bi, double2* ro, double* part) {
+        bj64_apply(op, xi, t, Gate{});
+        a_res(t, bi, ro, part);
+    };
+    P.key_pre = op.bj64_inv.p;
+    P.key_pre_bs = op.bj_size;
+    st = sb_gmres_stats{};
+    const double2* rhs = b;
+    double tol = cfg.tolerance;
+    if (x0_given) {
+        // r0 = b - A x0 (one product), and the tolerance relative to ||b||
+        double* hsc = static_cast<double*>(sw.pin.p);
+        arnoldi_dots<double2>(b, n, 0, b, n, sw.k64_part(n), sw.k64_red(), op.stream);
+        SB_CUDA(cudaMemcpyAsync(hsc, sw.k64_red(), sizeof(double), cudaMemcpyDeviceToHost, op.stream));
+        op_residual64(op, x, b, sw.r64.as<double2>(), sw.partg.as<double>());
+        sum_real(sw.partg.as<double>(), op_residual64_partials(op), sw.nrmg.as<double>(), op.stream);
+        SB_CUDA(cudaMemcpyAsync(hsc + 1, sw.nrmg.p, sizeof(double), cudaMemcpyDeviceToHost, op.stream));
+        SB_CUDA(cudaStreamSynchronize(op.stream));
+        ++st.matvecs;
+        const double bn = std::sqrt(hsc[0]), rn = std::sqrt(hsc[1]);
+        if (bn >= 1e-15 && rn > 0.0) tol = cfg.tolerance * bn / rn;
+        rhs = sw.r64.as<double2>();
+    }
+    // gmres_core accumulates its updates into z and takes it to be zero on entry
+    SB_CUDA(cudaMemsetAsync(z, 0, sizeof(double2) * n, op.stream));
+    CoreResult R = gmres_core<double2>(sw.k64, P, rhs, z, cfg.max_iterations, cfg.restart, tol,
+                                       cfg.convergence_check_interval, /*x_zero=*/true, false);
+    // x = x0 + M^-1 z (x = M^-1 z without an initial guess)
+    bj64_apply(op, z, t, Gate{});
+    if (x0_given) {
+        basis_update<double2, double2>(t, n, 1, nullptr, sw.one.as<double2>(), 1.0, x, n, op.stream);
+    } else {
+        SB_CUDA(cudaMemcpyAsync(x, t, sizeof(double2) * n, cudaMemcpyDeviceToDevice, op.stream));
+    }
+    st.iterations = R.iterations;
+    st.restarts = R.restarts;
+    st.matvecs += R.matvecs;
+    st.estimated_residual = R.estimated;
+    st.converged = R.converged ? 1 : 0;
+    st.status = R.status;
+    // Without an initial guess the last residual gmres_core formed is b - A x for this very x
+    // (the same M^-1 z, by the same kernel); otherwise finalize forms it.
+    finalize(op, sw, b, x, st, x0_given ? nullptr : static_cast<const double2*>(R.r_last));
+}
+
+}  // namespace
+
 void gmres_fp64(const Operator& op, const double2* b, double2* x, bool x0_given,
                 const sb_gmres_config& cfg, int precond, sb_gmres_stats& st) {
     SB_CUDA(cudaSetDevice(op.device));
@@ -626,6 +702,11 @@ void gmres_fp64(const Operator& op, const double2* b, double2* x, bool x0_given,
     if (!x0_given) SB_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * op.n, op.stream));
     Problem<double2> P = problem64(op);
     P.jacobi = precond == SB_PRECOND_JACOBI ? op.diag.as<double2>() : nullptr;
+    if (precond == SB_PRECOND_BLOCK_JACOBI) {
+        gmres_fp64_block_jacobi(op, sw, P, b, x, x0_given, cfg, st);
+        st.device_ms = timer.stop();
+        return;
+    }
     CoreResult R = gmres_core<double2>(sw.k64, P, b, x, cfg.max_iterations, cfg.restart, cfg.tolerance,
                                        cfg.convergence_check_interval, !x0_given, false);
     st = sb_gmres_stats{};

@@ -10,6 +10,11 @@
 // it solves (A M^-1) y = r and the correction is d = M^-1 y, so the outer refinement (and the
 // converged answer) is unchanged; only the inner iteration count drops. The preconditioner is
 // rebuilt after each assembly on the first mixed solve that uses it.
+//
+// The FP64 solver takes the same preconditioner on the right (SB_PRECOND_BLOCK_JACOBI): the
+// diagonal blocks of the complex128 matrix, rounded to complex64 and inverted by the same kernel,
+// applied to FP64 vectors with FP64 accumulation. Right preconditioning leaves the residual that
+// decides convergence, b - A x, untouched, so the FP64 solution meets the same tolerance.
 
 #include <algorithm>
 #include <cstring>
@@ -36,15 +41,29 @@ __global__ void __launch_bounds__(bj_threads(BS)) k_bj_invert(const float2* __re
     bj_invert_block<BS, bj_threads(BS)>(A, lda, rows, perm + base, out + blockIdx.x * (int64_t)BS * BS, status, M);
 }
 
-// y = M^-1 x: one CTA of BS threads per block.
+// The same blocks of the complex128 matrix (row-major, leading dimension n), rounded to complex64
+// before the inversion: the FP64 solver's right preconditioner is then the same linear map as the
+// mixed solver's.
 template <int BS>
+__global__ void __launch_bounds__(bj_threads(BS)) k_bj_invert64(const double2* __restrict__ A, int64_t n,
+                                                                const int32_t* __restrict__ perm,
+                                                                float2* __restrict__ out, int* __restrict__ status) {
+    extern __shared__ float2 M[];
+    const int64_t base = blockIdx.x * (int64_t)BS;
+    const int rows = static_cast<int>(n - base < BS ? n - base : BS);
+    bj_invert_block<BS, bj_threads(BS), double2>(A, n, rows, perm + base, out + blockIdx.x * (int64_t)BS * BS, status,
+                                                 M);
+}
+
+// y = M^-1 x: one CTA of BS * kBjSplit threads per block; V = float2 (FP32 vectors) or double2.
+template <int BS, class V>
 __global__ void __launch_bounds__(BS * kBjSplit) k_bj_apply(const float2* __restrict__ invT, int64_t n,
-                                                 const int32_t* __restrict__ perm, const float2* __restrict__ x,
-                                                 float2* __restrict__ y, Gate gate) {
+                                                 const int32_t* __restrict__ perm, const V* __restrict__ x,
+                                                 V* __restrict__ y, Gate gate) {
     if ((gate.a && *gate.a == 0) || (gate.b && *gate.b == 0)) return;
     const int64_t base = blockIdx.x * (int64_t)BS;
     const int rows = static_cast<int>(n - base < BS ? n - base : BS);
-    bj_apply_block<BS>(invT + blockIdx.x * (int64_t)BS * BS, rows, perm + base, x, y);
+    bj_apply_block<BS, V>(invT + blockIdx.x * (int64_t)BS * BS, rows, perm + base, x, y);
 }
 
 }  // namespace
@@ -97,31 +116,88 @@ void bj_build(Operator& op, int* status) {
 }
 
 template <int BS>
-void bj_launch(const Operator& op, const float2* x, float2* y, cudaStream_t s, Gate g) {
+void bj_build64(Operator& op, int* status) {
     const int64_t nb = (op.n + BS - 1) / BS;
-    k_bj_apply<BS><<<static_cast<unsigned>(nb), BS * kBjSplit, 0, s>>>(op.bj_inv.as<float2>(), op.n, op.bj_perm.as<int32_t>(),
-                                                           x, y, g);
+    const size_t smem = sizeof(float2) * BS * BS;
+    SB_CUDA(cudaFuncSetAttribute(k_bj_invert64<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    k_bj_invert64<BS><<<static_cast<unsigned>(nb), bj_threads(BS), smem, op.stream>>>(
+        op.A64.as<double2>(), op.n, op.bj_perm.as<int32_t>(), op.bj64_inv.as<float2>(), status);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
+template <int BS, class V>
+void bj_launch(const Operator& op, const float2* inv, const V* x, V* y, cudaStream_t s, Gate g) {
+    const int64_t nb = (op.n + BS - 1) / BS;
+    k_bj_apply<BS, V><<<static_cast<unsigned>(nb), BS * kBjSplit, 0, s>>>(inv, op.n, op.bj_perm.as<int32_t>(), x, y,
+                                                                          g);
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+template <class V>
+void bj_dispatch(const Operator& op, const float2* inv, const V* x, V* y, Gate g) {
+    ProfScope prof(SB_PROF_ARNOLDI, op.stream);
+    switch (op.bj_size) {
+        case 32: bj_launch<32, V>(op, inv, x, y, op.stream, g); break;
+        case 64: bj_launch<64, V>(op, inv, x, y, op.stream, g); break;
+        case 96: bj_launch<96, V>(op, inv, x, y, op.stream, g); break;
+        default: bj_launch<128, V>(op, inv, x, y, op.stream, g); break;
+    }
+}
+
+// The blocks' permutation (Morton order of the element centroids, else index order), built once
+// per operator.
+void bj_ensure_perm(Operator& op) {
+    if (op.bj_perm.p) return;
+    const int64_t n = op.n;
+    std::vector<int32_t> perm(n);
+    if (op.mesh && op.basis == SB_BASIS_CONSTANT) {
+        perm = element_morton_order(*op.mesh);
+    } else {
+        std::iota(perm.begin(), perm.end(), 0);
+    }
+    op.bj_perm.alloc(sizeof(int32_t) * n);
+    h2d_sync(op.bj_perm.p, perm.data(), sizeof(int32_t) * n);
+}
+
 }  // namespace
+
+void bj64_prepare(Operator& op) {
+    if (op.bj64_valid) return;
+    SB_REQUIRE(op.A64.p, SB_ERR_INVALID_ARGUMENT,
+               "block-Jacobi preconditioner of the FP64 solver: the operator has no complex128 matrix");
+    const int bs = op.bj_size;
+    const int64_t nb = (op.n + bs - 1) / bs;
+    bj_ensure_perm(op);
+    const size_t bytes = sizeof(float2) * static_cast<size_t>(nb) * bs * bs;
+    if (op.bj64_inv.bytes != bytes) {
+        op.bj64_inv.release();
+        op.bj64_inv.alloc(bytes);
+    }
+    if (!op.bj_status.p) op.bj_status.alloc(sizeof(int));
+    ProfScope prof(SB_PROF_OTHER, op.stream);
+    SB_CUDA(cudaMemsetAsync(op.bj_status.p, 0, sizeof(int), op.stream));
+    switch (bs) {
+        case 32: bj_build64<32>(op, op.bj_status.as<int>()); break;
+        case 64: bj_build64<64>(op, op.bj_status.as<int>()); break;
+        case 96: bj_build64<96>(op, op.bj_status.as<int>()); break;
+        default: bj_build64<128>(op, op.bj_status.as<int>()); break;
+    }
+    op.bj64_valid = true;
+}
+
+void bj64_apply(const Operator& op, const double2* x, double2* y, Gate g) {
+    bj_dispatch<double2>(op, op.bj64_inv.as<float2>(), x, y, g);
+}
 
 void bj_prepare(Operator& op) {
     if (op.bj_valid) return;
     SB_REQUIRE(op.A32.p, SB_ERR_INVALID_ARGUMENT, "block-Jacobi inner preconditioner: no complex64 matrix");
     const int bs = op.bj_size;
-    const int64_t n = op.n, nb = (n + bs - 1) / bs;
-    if (!op.bj_perm.p) {
-        std::vector<int32_t> perm(n);
-        if (op.mesh && op.basis == SB_BASIS_CONSTANT) {
-            perm = element_morton_order(*op.mesh);
-        } else {
-            std::iota(perm.begin(), perm.end(), 0);
-        }
-        op.bj_perm.alloc(sizeof(int32_t) * n);
-        h2d_sync(op.bj_perm.p, perm.data(), sizeof(int32_t) * n);
-    }
+    const int64_t nb = (op.n + bs - 1) / bs;
+    bj_ensure_perm(op);
     const size_t bytes = sizeof(float2) * static_cast<size_t>(nb) * bs * bs;
     if (op.bj_inv.bytes != bytes) {
         op.bj_inv.release();
@@ -140,13 +216,7 @@ void bj_prepare(Operator& op) {
 }
 
 void bj_apply(const Operator& op, const float2* x, float2* y, Gate g) {
-    ProfScope prof(SB_PROF_ARNOLDI, op.stream);
-    switch (op.bj_size) {
-        case 32: bj_launch<32>(op, x, y, op.stream, g); break;
-        case 64: bj_launch<64>(op, x, y, op.stream, g); break;
-        case 96: bj_launch<96>(op, x, y, op.stream, g); break;
-        default: bj_launch<128>(op, x, y, op.stream, g); break;
-    }
+    bj_dispatch<float2>(op, op.bj_inv.as<float2>(), x, y, g);
 }
 
 }  // namespace sb

@@ -6,6 +6,8 @@
 
 #include <cmath>
 #include <cstdio>
+#include <exception>
+#include <new>
 #include <string>
 #include <utility>
 #include <vector>
@@ -25,6 +27,30 @@ struct Error {
 
 void set_error(int status, const std::string& msg);
 void clear_error();
+
+// Runs the body of a C-ABI entry point and turns whatever it throws into a status code with its
+// message: Error as raised, a failed host allocation as SB_ERR_OUT_OF_MEMORY, any other standard
+// exception as SB_ERR_CUDA with its what().
+template <class F>
+int abi_guard(F&& f) {
+    try {
+        clear_error();
+        f();
+        return SB_OK;
+    } catch (const Error& e) {
+        set_error(e.status, e.msg);
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_error(SB_ERR_OUT_OF_MEMORY, "host allocation failed");
+        return SB_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        set_error(SB_ERR_CUDA, e.what());
+        return SB_ERR_CUDA;
+    } catch (...) {
+        set_error(SB_ERR_CUDA, "unknown failure");
+        return SB_ERR_CUDA;
+    }
+}
 
 #define SB_CUDA(call)                                                                        \
     do {                                                                                     \
@@ -185,6 +211,10 @@ struct Operator {
     int bj_size = 128;
     DevBuf bj_perm, bj_inv, bj_status;
     bool bj_valid = false;
+    // The FP64 solver's block-Jacobi right preconditioner (SB_PRECOND_BLOCK_JACOBI): the same
+    // blocks of the complex128 matrix, inverted in FP32 (rebuilt after assembly).
+    DevBuf bj64_inv;
+    bool bj64_valid = false;
     // Near-pair and self kernels of the constant-basis Tri3 assembly run here, concurrently with
     // the far kernel (they write disjoint entries; the far kernel is FMA / special-function bound,
     // the near kernel FP64 and latency bound).
@@ -266,6 +296,10 @@ void half_alloc(Operator& op);
 // Block-Jacobi inner preconditioner (precond.cu): build the block inverses; y = M^-1 x (FP32).
 void bj_prepare(Operator& op);
 void bj_apply(const Operator& op, const float2* x, float2* y, Gate g);
+// The FP64 solver's block-Jacobi right preconditioner: inverses of the complex128 matrix's blocks;
+// y = M^-1 x with FP64 vectors.
+void bj64_prepare(Operator& op);
+void bj64_apply(const Operator& op, const double2* x, double2* y, Gate g);
 // Morton (Z-order) permutation of a mesh's element centroids (precond.cu).
 std::vector<int32_t> element_morton_order(const Mesh& m);
 // Products with FP64 vectors on whichever matrix the operator holds (gmres.cu).

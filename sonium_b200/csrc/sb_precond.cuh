@@ -16,12 +16,18 @@ __device__ __forceinline__ float2 bj_cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+// Entries of the gathered block in FP32, from a complex64 or a complex128 matrix.
+__device__ __forceinline__ float2 bj_entry(float2 v) { return v; }
+__device__ __forceinline__ float2 bj_entry(double2 v) {
+    return make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+}
+
 // One CTA (THREADS threads, BS * BS float2 of dynamic shared memory at M) per block: gather the
-// diagonal block M = A[p_i][p_j], i, j < rows (identity beyond), invert it in place (Gauss-Jordan,
-// partial pivoting) and store its transpose at out. A zero pivot (a singular block) stores the
-// identity and raises bit 0 of *status.
-template <int BS, int THREADS>
-__device__ __forceinline__ void bj_invert_block(const float2* __restrict__ A, int64_t lda, int rows,
+// diagonal block M = A[p_i][p_j], i, j < rows (identity beyond), rounded to complex64 when A is
+// complex128, invert it in place (Gauss-Jordan, partial pivoting) and store its transpose at out.
+// A zero pivot (a singular block) stores the identity and raises bit 0 of *status.
+template <int BS, int THREADS, class TA = float2>
+__device__ __forceinline__ void bj_invert_block(const TA* __restrict__ A, int64_t lda, int rows,
                                                 const int32_t* __restrict__ perm, float2* __restrict__ out,
                                                 int* __restrict__ status, float2* M) {
     __shared__ int piv[BS];
@@ -32,7 +38,7 @@ __device__ __forceinline__ void bj_invert_block(const float2* __restrict__ A, in
     for (int t = threadIdx.x; t < BS * BS; t += THREADS) {
         const int i = t / BS, j = t % BS;
         float2 v = make_float2(i == j ? 1.f : 0.f, 0.f);
-        if (i < rows && j < rows) v = A[(int64_t)perm[i] * lda + perm[j]];
+        if (i < rows && j < rows) v = bj_entry(A[(int64_t)perm[i] * lda + perm[j]]);
         M[t] = v;
     }
     if (threadIdx.x == 0) s_singular = 0;
@@ -135,28 +141,33 @@ constexpr int kBjSplit = 4;
 
 // y[p_i] = sum_j inv[i][j] x[p_j] for one block (BS * kBjSplit threads: thread i + BS q takes
 // row i, columns [q BS / kBjSplit, (q + 1) BS / kBjSplit)). The block's x is gathered into shared
-// memory before any y is written, so x and y may be the same vector.
-template <int BS>
+// memory before any y is written, so x and y may be the same vector. V is float2 (FP32 vectors
+// and arithmetic) or double2 (FP64 vectors; the FP32 inverse entries are exact in FP64 and the
+// products are accumulated in FP64, so the preconditioner is the same linear map either way).
+template <int BS, class V = float2>
 __device__ __forceinline__ void bj_apply_block(const float2* __restrict__ invT, int rows,
-                                               const int32_t* __restrict__ perm, const float2* x, float2* y) {
-    __shared__ float2 xs[BS];
-    __shared__ float2 ps[kBjSplit][BS];
+                                               const int32_t* __restrict__ perm, const V* x, V* y) {
+    using R = decltype(V{}.x);
+    __shared__ V xs[BS];
+    __shared__ V ps[kBjSplit][BS];
     const int i = threadIdx.x % BS, q = threadIdx.x / BS;
-    if (threadIdx.x < BS) xs[i] = i < rows ? x[perm[i]] : make_float2(0.f, 0.f);
+    if (threadIdx.x < BS) xs[i] = i < rows ? x[perm[i]] : V{R(0), R(0)};
     __syncthreads();
     constexpr int kCols = BS / kBjSplit;
-    float re = 0.f, im = 0.f;
+    R re = R(0), im = R(0);
 #pragma unroll 8
     for (int jj = 0; jj < kCols; ++jj) {
         const int j = q * kCols + jj;
-        const float2 a = invT[j * BS + i], v = xs[j];
-        re = fmaf(a.x, v.x, fmaf(-a.y, v.y, re));
-        im = fmaf(a.x, v.y, fmaf(a.y, v.x, im));
+        const float2 a = invT[j * BS + i];
+        const V v = xs[j];
+        const R ax = static_cast<R>(a.x), ay = static_cast<R>(a.y);
+        re = fma(ax, v.x, fma(-ay, v.y, re));
+        im = fma(ax, v.y, fma(ay, v.x, im));
     }
-    ps[q][i] = make_float2(re, im);
+    ps[q][i] = V{re, im};
     __syncthreads();
     if (q == 0 && i < rows) {
-        float2 t = ps[0][i];
+        V t = ps[0][i];
 #pragma unroll
         for (int u = 1; u < kBjSplit; ++u) {
             t.x += ps[u][i].x;
