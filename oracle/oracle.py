@@ -93,6 +93,20 @@ def _declare(L):
                                             OrC128, ct.c_int, ct.c_double, ct.c_int, P, P]
     L.or_assemble_linear.argtypes = [ct.c_int64, P, ct.c_int64, P, ct.POINTER(OrBc), ct.POINTER(OrPhysics),
                                      OrC128, ct.c_int, P, P]
+    L.or_assemble_rows_from_channels.argtypes = [ct.c_int64, P, ct.c_int64, P, ct.POINTER(OrBc),
+                                                 ct.POINTER(OrPhysics), OrC128, ct.c_int64, ct.c_int64, P,
+                                                 ct.c_int, P, P]
+    L.or_chart_rows.argtypes = [ct.c_int64, P, ct.c_int64, P, ct.c_double, ct.c_int64, ct.c_int64, ct.c_int, P, P,
+                                ct.c_int64]
+    L.or_chart_rows.restype = ct.c_int64
+
+
+# Record layouts of the reference CUDA path's chart-driven pair kernel (bem_kernels.cu:818-833).
+CHART_SAMPLE = np.dtype([("position", "<f8", 3), ("field_normal", "<f8", 3), ("edge_direction", "<f8", 3),
+                         ("weight", "<f8"), ("basis_weight", "<f8"), ("kind", "<u4"), ("pad", "<u4")])
+CHART_PAIR = np.dtype([("source_point", "<f8", 3), ("source_normal", "<f8", 3), ("sample_offset", "<u8"),
+                       ("sample_count", "<u8")])
+assert CHART_SAMPLE.itemsize == 96 and CHART_PAIR.itemsize == 64
 
 
 def _p(a: np.ndarray):
@@ -172,6 +186,47 @@ def assemble(nodes, tris, ph: OrPhysics, beta: complex, rows=None, bc_kind=None,
     if rc:
         raise ValueError("oracle assembly rejected its input")
     return A, rhs
+
+
+def assemble_from_channels(nodes, tris, ph: OrPhysics, beta: complex, channels, rows=None, threads: int = 0):
+    """Rows of the TBEM matrix with the CPU path's free terms and coefficients over the given
+    (G, H, H^T, E) channels of every pair of the rows (rigid surface): channels is
+    (rows x n x 4) complex128."""
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    tris = np.ascontiguousarray(tris, np.uint32)
+    m = tris.shape[0]
+    r0, r1 = (0, m) if rows is None else rows
+    ch = np.ascontiguousarray(channels, np.complex128)
+    if ch.size != (r1 - r0) * m * 4:
+        raise ValueError("channels must hold 4 values per pair of the rows")
+    A = np.zeros((r1 - r0, m), np.complex128)
+    rhs = np.zeros(r1 - r0, np.complex128)
+    b = OrBc()
+    rc = lib().or_assemble_rows_from_channels(nodes.shape[0], _p(nodes), m, _p(tris), ct.byref(b), ct.byref(ph),
+                                              OrC128(beta.real, beta.imag), r0, r1, _p(ch), threads, _p(A),
+                                              _p(rhs))
+    if rc:
+        raise ValueError("oracle assembly rejected its input")
+    return A, rhs
+
+
+def chart(nodes, tris, k: float, rows=None, threads: int = 0):
+    """Quadrature charts of the reference CUDA assembly path for the pairs of rows [r0, r1) x all
+    elements (pair index (i - r0) * n + j): (pairs, samples) as CHART_PAIR / CHART_SAMPLE arrays."""
+    nodes = np.ascontiguousarray(nodes, np.float64)
+    tris = np.ascontiguousarray(tris, np.uint32)
+    m = tris.shape[0]
+    r0, r1 = (0, m) if rows is None else rows
+    L = lib()
+    total = L.or_chart_rows(nodes.shape[0], _p(nodes), m, _p(tris), k, r0, r1, threads, None, None, 0)
+    if total < 0:
+        raise ValueError("oracle chart rejected its input")
+    pairs = np.zeros((r1 - r0) * m, CHART_PAIR)
+    samples = np.zeros(total, CHART_SAMPLE)
+    got = L.or_chart_rows(nodes.shape[0], _p(nodes), m, _p(tris), k, r0, r1, threads, _p(pairs), _p(samples), total)
+    if got != total:
+        raise ValueError("oracle chart changed size between its two passes")
+    return pairs, samples
 
 
 def quad_geometry(nodes, quads):

@@ -535,6 +535,173 @@ void set_threads(int threads) {
 #endif
 }
 
+// build_tbem_system_with_beta_parallel (tbem.rs:1284-1466) for rows [row0, row1): free terms
+// and the per-field-BC coefficients over the channels that `channels(i, j, x, nx)` returns (the
+// CPU integration rules, or channels computed elsewhere for the same pairs).
+template <class ChannelFn>
+int assemble_rows_impl(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris, const or_bc* bc,
+                       const or_physics* ph, or_c128 beta_in, int64_t row0, int64_t row1, int threads,
+                       or_c128* A, or_c128* rhs, ChannelFn&& channels) {
+    if (m <= 0 || row0 < 0 || row1 > m || row0 > row1) return 1;
+    for (int64_t i = 0; i < 3 * m; ++i)
+        if (tris[i] >= static_cast<uint64_t>(n_nodes)) return 1;
+    std::vector<double> centers(3 * m), normals(3 * m), areas(m);
+    element_geometry(m, nodes, tris, centers.data(), normals.data(), areas.data());
+    const cd gamma(1.0, 0.0), tau(ph->tau, 0.0), iwr(0.0, ph->pressure_factor);
+    const cd beta = C(beta_in);
+    std::vector<BcView> bcs(m);
+    for (int64_t e = 0; e < m; ++e) bcs[e] = bc_at(bc, e);
+    const int64_t rows = row1 - row0;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t rr = 0; rr < rows; ++rr) {
+        const int64_t i = row0 + rr;
+        or_c128* row = A + rr * m;
+        std::vector<cd> local(m, cd(0, 0));
+        cd lrhs(0, 0);
+        const BcView& sb = bcs[i];
+        // Free terms (tbem.rs:1344-1358).
+        if (sb.kind == 0) {
+            local[i] -= gamma * 0.5;
+            if (sb.has_adm) local[i] -= sb.adm * iwr * beta * tau * 0.5;
+            lrhs += sb.value * iwr * beta * tau * 0.5;
+        } else if (sb.kind == 1) {
+            local[i] += beta * tau * 0.5;
+            lrhs -= sb.value * gamma * 0.5;
+        }
+        const double* x = &centers[3 * i];
+        const double* nx = &normals[3 * i];
+        for (int64_t j = 0; j < m; ++j) {
+            const BcView& fb = bcs[j];
+            const bool compute_rhs = std::abs(fb.value) > 1e-15;
+            const Channels r = channels(i, j, x, nx, areas[j]);
+            // Coefficient per field BC (tbem.rs:1404-1417).
+            cd coeff(0, 0);
+            if (fb.kind == 0) {
+                coeff = r.h * gamma * tau + r.e * beta;
+                if (fb.has_adm) coeff -= (r.g * gamma * tau + r.ht * beta) * fb.adm * iwr;
+            } else if (fb.kind == 1) {
+                coeff = -(r.g * gamma * tau + r.ht * beta);
+            }
+            local[j] += coeff;
+            if (compute_rhs) {
+                if (fb.kind == 0)
+                    lrhs += (r.g * gamma * tau + r.ht * beta) * fb.value * iwr;
+                else if (fb.kind == 1)
+                    lrhs += (r.h * gamma * tau + r.e * beta) * fb.value;
+            }
+        }
+        for (int64_t j = 0; j < m; ++j) row[j] = O(local[j]);
+        if (rhs) rhs[rr] = O(lrhs);
+    }
+    return 0;
+}
+
+std::vector<Coords> element_coords(int64_t m, const double* nodes, const uint32_t* tris) {
+    std::vector<Coords> coords(m);
+    for (int64_t e = 0; e < m; ++e)
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 3; ++j) coords[e].v[a][j] = nodes[3 * tris[3 * e + a] + j];
+    return coords;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Quadrature charts of the reference CUDA assembly path: the records that its chart-driven pair
+// kernel (sonium_bem_quadrature_pair_c64, crates/sonium-compute/src/cuda/kernels/bem_kernels.cu:
+// 839-967) integrates. The record layouts are the kernel's (bem_kernels.cu:818-833), so that the
+// reference kernel, compiled from its own source, can be run on them as a checker.
+// ---------------------------------------------------------------------------------------------
+static_assert(sizeof(or_chart_sample) == 96, "SoniumBemQuadratureSampleC64 layout");
+static_assert(sizeof(or_chart_pair) == 64, "SoniumBemQuadraturePairC64 layout");
+
+// append_regular_tri3_quadrature (tbem.rs:4998-5049): every leaf of generate_subelements, its
+// triangle rule mapped affinely by the leaf's vertices (weight times the map's determinant), the
+// point's position, Jacobian and normal from the element map; kind 0 (full channels).
+void chart_regular(const double x[3], const Coords& c, double area, std::vector<or_chart_sample>& out) {
+    for (const Leaf& lf : generate_subelements(x, c, area)) {
+        for (const TriPoint& p : triangle_quadrature(lf.order)) {
+            const double l0 = 1.0 - p.xi - p.eta;
+            const double mxi = lf.tv[0][0] * l0 + lf.tv[1][0] * p.xi + lf.tv[2][0] * p.eta;
+            const double meta = lf.tv[0][1] * l0 + lf.tv[1][1] * p.xi + lf.tv[2][1] * p.eta;
+            const double dx1 = lf.tv[1][0] - lf.tv[0][0], dy1 = lf.tv[1][1] - lf.tv[0][1];
+            const double dx2 = lf.tv[2][0] - lf.tv[0][0], dy2 = lf.tv[2][1] - lf.tv[0][1];
+            const double det = std::fabs(dx1 * dy2 - dx2 * dy1);
+            or_chart_sample smp{};
+            double jac;
+            tri_parameters(c, mxi, meta, smp.position, jac, smp.field_normal);
+            smp.weight = p.w * det * jac;
+            smp.basis_weight = 1.0;
+            smp.kind = 0;
+            out.push_back(smp);
+        }
+    }
+}
+
+// append_singular_tri3_quadrature(_with_params) (tbem.rs:5051-5161): the regularised edge line
+// integral (kind 2: position on the edge, unit edge direction, weight = GL weight times the
+// section's half length) and the Duffy-collapsed bulk of the sub-triangles (kind 1), with the rule
+// of QuadratureParams::for_ka at ka = k sqrt(area).
+void chart_singular(const Coords& c, double area, double k, std::vector<or_chart_sample>& out) {
+    static const double csi6[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+    static const double eta6[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
+    const double ka = k * std::max(std::sqrt(area), 1e-10);
+    SingularParams q;
+    if (ka < 0.3) q = {3, 4, 4, 2};
+    else if (ka < 1.0) q = {4, 5, 6, 2};
+    else if (ka < 2.0) q = {5, 6, 8, 3};
+    else q = {6, 7, 10, 4};
+    std::vector<double> ex, ew, sx, sw;
+    gauss_legendre(q.edge_order, ex, ew);
+    gauss_legendre(q.sub_order, sx, sw);
+    for (int edge = 0; edge < 3; ++edge) {
+        const int next = (edge + 1) % 3;
+        double d[3];
+        for (int j = 0; j < 3; ++j) d[j] = c.v[next][j] - c.v[edge][j];
+        const double len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        const double scale = len / (2.0 * q.sections);
+        for (int sec = 0; sec < q.sections; ++sec) {
+            const double mid = -1.0 + (sec + 0.5) * (2.0 / q.sections);
+            for (int g = 0; g < q.edge_order; ++g) {
+                const double loc = mid + ex[g] / q.sections;
+                or_chart_sample smp{};
+                for (int j = 0; j < 3; ++j) {
+                    smp.position[j] = c.v[edge][j] + d[j] * (loc + 1.0) / 2.0;
+                    smp.edge_direction[j] = d[j] / len;
+                }
+                smp.weight = ew[g] * scale;
+                smp.basis_weight = 1.0;
+                smp.kind = 2;
+                out.push_back(smp);
+            }
+        }
+    }
+    for (int edge = 0; edge < 3; ++edge) {
+        const int next = (edge + 1) % 3, ig2 = edge + 3;
+        for (int st = 0; st < q.subtri; ++st) {
+            const double area_scale = 1.0 / 24.0 / q.subtri;
+            const double ss[3] = {1.0 / 3.0, st == 0 ? csi6[edge] : csi6[ig2], st == 0 ? csi6[ig2] : csi6[next]};
+            const double ts[3] = {1.0 / 3.0, st == 0 ? eta6[edge] : eta6[ig2], st == 0 ? eta6[ig2] : eta6[next]};
+            for (int a = 0; a < q.sub_order; ++a) {
+                const double sga = sx[a];
+                for (int b = 0; b < q.sub_order; ++b) {
+                    const double tga = sx[b];
+                    const double xi = 0.5 * (1.0 - sga) * ss[0] +
+                                      0.25 * (1.0 + sga) * ((1.0 - tga) * ss[1] + (1.0 + tga) * ss[2]);
+                    const double eta = 0.5 * (1.0 - sga) * ts[0] +
+                                       0.25 * (1.0 + sga) * ((1.0 - tga) * ts[1] + (1.0 + tga) * ts[2]);
+                    or_chart_sample smp{};
+                    double jac;
+                    tri_parameters(c, xi, eta, smp.position, jac, smp.field_normal);
+                    smp.weight = sw[a] * sw[b] * (1.0 + sga) * area_scale * jac;
+                    smp.basis_weight = 1.0;
+                    smp.kind = 1;
+                    out.push_back(smp);
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -634,64 +801,81 @@ void or_element_geometry(int64_t n_tris, const double* nodes, const uint32_t* tr
 int or_assemble_rows(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris,
                      const or_bc* bc, const or_physics* ph, or_c128 beta_in, int64_t row0,
                      int64_t row1, int threads, or_c128* A, or_c128* rhs) {
-    if (m <= 0 || row0 < 0 || row1 > m || row0 > row1) return 1;
+    if (m <= 0) return 1;
     for (int64_t i = 0; i < 3 * m; ++i)
         if (tris[i] >= static_cast<uint64_t>(n_nodes)) return 1;
+    const std::vector<Coords> coords = element_coords(m, nodes, tris);
+    return assemble_rows_impl(n_nodes, nodes, m, tris, bc, ph, beta_in, row0, row1, threads, A, rhs,
+                              [&](int64_t i, int64_t j, const double* x, const double* nx, double area) {
+                                  return (j == i) ? singular_pair(x, nx, coords[j], *ph)
+                                                  : regular_pair(x, nx, coords[j], area, *ph);
+                              });
+}
+
+int or_assemble_rows_from_channels(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris,
+                                   const or_bc* bc, const or_physics* ph, or_c128 beta, int64_t row0,
+                                   int64_t row1, const or_c128* channels, int threads, or_c128* A, or_c128* rhs) {
+    if (!channels) return 1;
+    return assemble_rows_impl(n_nodes, nodes, m, tris, bc, ph, beta, row0, row1, threads, A, rhs,
+                              [&](int64_t i, int64_t j, const double*, const double*, double) {
+                                  const or_c128* c4 = channels + ((i - row0) * m + j) * 4;
+                                  Channels r;
+                                  r.g = C(c4[0]);
+                                  r.h = C(c4[1]);
+                                  r.ht = C(c4[2]);
+                                  r.e = C(c4[3]);
+                                  return r;
+                              });
+}
+
+int64_t or_chart_rows(int64_t n_nodes, const double* nodes, int64_t m, const uint32_t* tris, double k,
+                      int64_t row0, int64_t row1, int threads, or_chart_pair* pairs, or_chart_sample* samples,
+                      int64_t capacity) {
+    if (m <= 0 || row0 < 0 || row1 > m || row0 > row1) return -1;
+    for (int64_t i = 0; i < 3 * m; ++i)
+        if (tris[i] >= static_cast<uint64_t>(n_nodes)) return -1;
+    const std::vector<Coords> coords = element_coords(m, nodes, tris);
     std::vector<double> centers(3 * m), normals(3 * m), areas(m);
     element_geometry(m, nodes, tris, centers.data(), normals.data(), areas.data());
-    std::vector<Coords> coords(m);
-    for (int64_t e = 0; e < m; ++e)
-        for (int a = 0; a < 3; ++a)
-            for (int j = 0; j < 3; ++j) coords[e].v[a][j] = nodes[3 * tris[3 * e + a] + j];
-    const cd gamma(1.0, 0.0), tau(ph->tau, 0.0), iwr(0.0, ph->pressure_factor);
-    const cd beta = C(beta_in);
-    std::vector<BcView> bcs(m);
-    for (int64_t e = 0; e < m; ++e) bcs[e] = bc_at(bc, e);
     const int64_t rows = row1 - row0;
+    std::vector<std::vector<or_chart_sample>> per_row(rows);
+    std::vector<std::vector<int64_t>> counts(rows);
     set_threads(threads);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t rr = 0; rr < rows; ++rr) {
         const int64_t i = row0 + rr;
-        or_c128* row = A + rr * m;
-        std::vector<cd> local(m, cd(0, 0));
-        cd lrhs(0, 0);
-        const BcView& sb = bcs[i];
-        // Free terms (tbem.rs:1344-1358).
-        if (sb.kind == 0) {
-            local[i] -= gamma * 0.5;
-            if (sb.has_adm) local[i] -= sb.adm * iwr * beta * tau * 0.5;
-            lrhs += sb.value * iwr * beta * tau * 0.5;
-        } else if (sb.kind == 1) {
-            local[i] += beta * tau * 0.5;
-            lrhs -= sb.value * gamma * 0.5;
-        }
-        const double* x = &centers[3 * i];
-        const double* nx = &normals[3 * i];
+        auto& out = per_row[rr];
+        counts[rr].resize(m);
         for (int64_t j = 0; j < m; ++j) {
-            const BcView& fb = bcs[j];
-            const bool compute_rhs = std::abs(fb.value) > 1e-15;
-            Channels r = (j == i) ? singular_pair(x, nx, coords[j], *ph)
-                                  : regular_pair(x, nx, coords[j], areas[j], *ph);
-            // Coefficient per field BC (tbem.rs:1404-1417).
-            cd coeff(0, 0);
-            if (fb.kind == 0) {
-                coeff = r.h * gamma * tau + r.e * beta;
-                if (fb.has_adm) coeff -= (r.g * gamma * tau + r.ht * beta) * fb.adm * iwr;
-            } else if (fb.kind == 1) {
-                coeff = -(r.g * gamma * tau + r.ht * beta);
-            }
-            local[j] += coeff;
-            if (compute_rhs) {
-                if (fb.kind == 0)
-                    lrhs += (r.g * gamma * tau + r.ht * beta) * fb.value * iwr;
-                else if (fb.kind == 1)
-                    lrhs += (r.h * gamma * tau + r.e * beta) * fb.value;
-            }
+            const size_t before = out.size();
+            if (j == i)
+                chart_singular(coords[j], areas[j], k, out);
+            else
+                chart_regular(&centers[3 * i], coords[j], areas[j], out);
+            counts[rr][j] = static_cast<int64_t>(out.size() - before);
         }
-        for (int64_t j = 0; j < m; ++j) row[j] = O(local[j]);
-        if (rhs) rhs[rr] = O(lrhs);
     }
-    return 0;
+    int64_t total = 0;
+    for (const auto& v : per_row) total += static_cast<int64_t>(v.size());
+    if (!pairs || !samples) return total;
+    if (capacity < total) return -1;
+    int64_t off = 0;
+    for (int64_t rr = 0; rr < rows; ++rr) {
+        const int64_t i = row0 + rr;
+        for (int64_t j = 0; j < m; ++j) {
+            or_chart_pair& p = pairs[rr * m + j];
+            for (int d = 0; d < 3; ++d) {
+                p.source_point[d] = centers[3 * i + d];
+                p.source_normal[d] = normals[3 * i + d];
+            }
+            p.sample_offset = static_cast<uint64_t>(off);
+            p.sample_count = static_cast<uint64_t>(counts[rr][j]);
+            off += counts[rr][j];
+        }
+        std::memcpy(samples + (off - static_cast<int64_t>(per_row[rr].size())), per_row[rr].data(),
+                    per_row[rr].size() * sizeof(or_chart_sample));
+    }
+    return total;
 }
 
 void or_regular_pair(const double* x, const double* nx, const double* c9, double area,

@@ -65,6 +65,41 @@ int or_assemble_rows(int64_t n_nodes, const double* nodes, int64_t n_tris, const
                      const or_bc* bc, const or_physics* phys, or_c128 beta, int64_t row0,
                      int64_t row1, int threads, or_c128* A, or_c128* rhs);
 
+/* The same rows assembled from given channels instead of the CPU integration rules: channels holds
+ * (G, H, H^T, E) of every pair of the rows, ((i - row0) * n_tris + j) * 4, e.g. the reference CUDA
+ * kernel's output for the same pairs; the free terms and BC coefficients are the CPU path's. */
+int or_assemble_rows_from_channels(int64_t n_nodes, const double* nodes, int64_t n_tris, const uint32_t* tris,
+                                   const or_bc* bc, const or_physics* phys, or_c128 beta, int64_t row0,
+                                   int64_t row1, const or_c128* channels, int threads, or_c128* A,
+                                   or_c128* rhs);
+
+/* Quadrature charts of the reference CUDA assembly path (crates/sonium-bem/src/core/assembly/
+ * tbem.rs:4998-5161, pairs as at :5189-5275) in the record layouts of its chart-driven kernel
+ * (SoniumBemQuadratureSampleC64 / SoniumBemQuadraturePairC64, crates/sonium-compute/src/cuda/
+ * kernels/bem_kernels.cu:818-833): kind 0 = regular sample, 1 = singular bulk, 2 = hypersingular
+ * edge. */
+typedef struct or_chart_sample {
+    double position[3];
+    double field_normal[3];
+    double edge_direction[3];
+    double weight;
+    double basis_weight;
+    uint32_t kind;
+    uint32_t pad;
+} or_chart_sample;
+typedef struct or_chart_pair {
+    double source_point[3];
+    double source_normal[3];
+    uint64_t sample_offset;
+    uint64_t sample_count;
+} or_chart_pair;
+/* Charts of the pairs (i, j), i in [row0, row1), all j (pair index (i - row0) * n_tris + j).
+ * Returns the sample count; with null pairs / samples only counts; -1 on bad input or when
+ * capacity (samples) is too small. */
+int64_t or_chart_rows(int64_t n_nodes, const double* nodes, int64_t n_tris, const uint32_t* tris, double k,
+                      int64_t row0, int64_t row1, int threads, or_chart_pair* pairs, or_chart_sample* samples,
+                      int64_t capacity);
+
 /* Single-pair channel integrals (G, H, H^T, E) as 4 complex numbers, for unit tests.
  * regular_integration (crates/sonium-bem/src/core/integration/regular.rs:124-321) and
  * singular_integration (crates/sonium-bem/src/core/integration/singular.rs:297-614). */
