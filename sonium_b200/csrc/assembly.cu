@@ -504,7 +504,13 @@ __global__ void __launch_bounds__(kFarTile) k_far(const double* __restrict__ qp,
     }
     const bool ok = mbar_wait(bar_a, 0);
     if (__syncthreads_or(!ok)) {
+        // Timed out: report, skip the tile, and stay resident for a second bounded wait so that
+        // the bulk copy this CTA issued lands before its shared memory can pass to another CTA.
+        // (If that wait also runs out, the copy may still land late; the status word tells the
+        // host to discard the whole assembly either way.)
         if (tid == 0) atomicExch(status, 1);
+        mbar_wait(bar_a, 0);
+        __syncthreads();
         return;
     }
 

@@ -17,7 +17,10 @@
 //    whose kernels overlap on the GPU (different streams, different operators on one device, or
 //    different host threads) overwrite each other's partial sums and race.
 //  - the first call on a device looks up the array's device address (cudaGetSymbolAddress, with
-//    that device current) and keeps it; make that first call before any stream capture.
+//    that device current) and keeps it; make that first call before any stream capture. The kept
+//    address belongs to the device's current context: a host that calls cudaDeviceReset (which
+//    unloads the library's device code) must not call this entry point on that device again in
+//    the same process, since the kept address would then point at released memory.
 
 #include <mutex>
 
@@ -96,13 +99,13 @@ using namespace sb;
 
 extern "C" SB_API int sb_operator_apply_device_noalloc(const sb_operator* op, int trans, const sb_complex* x_dev,
                                                        sb_complex* y_dev) {
-    try {
-        clear_error();
+    return abi_guard([&] {
         SB_REQUIRE(op && op->op && x_dev && y_dev, SB_ERR_INVALID_ARGUMENT, "null argument");
         SB_REQUIRE(trans == SB_OP_N || trans == SB_OP_T || trans == SB_OP_C, SB_ERR_INVALID_ARGUMENT,
                    "trans must be N, T or C");
         Operator& o = *op->op;
         const int64_t n = o.n;
+        SB_REQUIRE(n > 0, SB_ERR_INVALID_ARGUMENT, "empty operator");
         SB_CUDA(cudaSetDevice(o.device));
         const double2* x = reinterpret_cast<const double2*>(x_dev);
         double2* y = reinterpret_cast<double2*>(y_dev);
@@ -132,12 +135,5 @@ extern "C" SB_API int sb_operator_apply_device_noalloc(const sb_operator* op, in
             SB_CUDA(cudaGetLastError());
         }
         SB_CUDA(cudaStreamSynchronize(o.stream));
-        return SB_OK;
-    } catch (const Error& e) {
-        set_error(e.status, e.msg);
-        return e.status;
-    } catch (...) {
-        set_error(SB_ERR_CUDA, "unknown failure");
-        return SB_ERR_CUDA;
-    }
+    });
 }
