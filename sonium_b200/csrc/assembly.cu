@@ -566,31 +566,52 @@ __global__ void __launch_bounds__(kFarTile) k_far(const double* __restrict__ qp,
 // delta_q = y_q - c_j precomputed per element, the distance change is formed without
 // cancellation as r_q - r_c = (2 d_c . delta_q + |delta_q|^2) / (r_q + r_c) and its small phase
 // k (r_q - r_c) rotates exp(i k r_c). Everything else (G, H, H^T, E factors and the sums) is
-// FP32; the near and self pairs keep the FP64 kernels.
+// FP32; the near and self pairs keep the FP64 kernels. (N = 20480, k = 10: per-entry error
+// against the FP64 matrix median 2e-7; the mixed solution within 3e-8 of the FP64 one.)
 // ---------------------------------------------------------------------------------------------
-constexpr int kQ32 = 6;  // per point: delta x, y, z, |delta|^2, w * J / (4 pi), delta . n_y
+// A flat triangle's quadrature points lie in its plane, so each offset delta_q = y_q - c_j is
+// two in-plane coordinates (a_q, b_q) on the element's orthonormal frame (e1, e2), e1 along the
+// first edge and e2 = n_y x e1: d_c . delta_q = a_q (d_c . e1) + b_q (d_c . e2), delta_q . n_x =
+// a_q (e1 . n_x) + b_q (e2 . n_x) and delta_q . n_y = 0, so r . n_y = d_c . n_y is one value per
+// pair. The point data per element is (a, b, |delta|^2, w J / 4 pi); the frame follows it.
+constexpr int kQ32 = 4;                              // per point: a, b, |delta|^2, w * J / (4 pi)
+constexpr int kQ32Frame = kFarPoints * kQ32;         // then e1 x, y, z, e2 x, y, z
+constexpr int kQ32Fields = kQ32Frame + 6;
 
-// Element point data for the FP32 far kernel: qp32[(q * 6 + c) * ld + e].
+// Element point data for the FP32 far kernel: qp32[(q * kQ32 + c) * ld + e], frame at
+// qp32[(kQ32Frame + c) * ld + e].
 __global__ void k_far_points32(const double* __restrict__ elem, int64_t n, int64_t ld,
                                float* __restrict__ qp32) {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= ld) return;
+    if (e >= n) {
+        for (int c = 0; c < kQ32Fields; ++c) qp32[(int64_t)c * ld + e] = 0.f;
+        return;
+    }
+    double e1[3], e2[3];
+    const double nx = E(ENX, e), ny = E(ENY, e), nz = E(ENZ, e);
+    for (int j = 0; j < 3; ++j) e1[j] = E(EV1X + j, e) - E(EV0X + j, e);
+    const double l1 = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    for (int j = 0; j < 3; ++j) e1[j] /= l1;
+    e2[0] = ny * e1[2] - nz * e1[1];
+    e2[1] = nz * e1[0] - nx * e1[2];
+    e2[2] = nx * e1[1] - ny * e1[0];
     const int o = c_tri_off[0];
     for (int q = 0; q < kFarPoints; ++q) {
         float* dst = qp32 + (int64_t)(q * kQ32) * ld + e;
-        if (e >= n) {
-            for (int c = 0; c < kQ32; ++c) dst[c * ld] = 0.f;
-            continue;
-        }
         const double s = c_tri_xi[o + q], t = c_tri_eta[o + q];
         const double sf0 = 1.0 - s - t;
         double dl[3];
         for (int j = 0; j < 3; ++j)
             dl[j] = sf0 * E(EV0X + j, e) + s * E(EV1X + j, e) + t * E(EV2X + j, e) - E(ECX + j, e);
-        for (int j = 0; j < 3; ++j) dst[j * ld] = static_cast<float>(dl[j]);
-        dst[3 * ld] = static_cast<float>(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
-        dst[4 * ld] = static_cast<float>(c_tri_w[o + q] * E(EJAC, e) * kInv4Pi);
-        dst[5 * ld] = static_cast<float>(dl[0] * E(ENX, e) + dl[1] * E(ENY, e) + dl[2] * E(ENZ, e));
+        dst[0] = static_cast<float>(dl[0] * e1[0] + dl[1] * e1[1] + dl[2] * e1[2]);
+        dst[ld] = static_cast<float>(dl[0] * e2[0] + dl[1] * e2[1] + dl[2] * e2[2]);
+        dst[2 * ld] = static_cast<float>(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
+        dst[3 * ld] = static_cast<float>(c_tri_w[o + q] * E(EJAC, e) * kInv4Pi);
+    }
+    for (int j = 0; j < 3; ++j) {
+        qp32[(int64_t)(kQ32Frame + j) * ld + e] = static_cast<float>(e1[j]);
+        qp32[(int64_t)(kQ32Frame + 3 + j) * ld + e] = static_cast<float>(e2[j]);
     }
 }
 
@@ -632,10 +653,9 @@ constexpr int kFar32Rows = 64;
 // slot, so the far field evaluates two quadrature points per instruction (points 2p, 2p + 1 in
 // the .x / .y lanes of pair p; the 13th point runs alone).
 constexpr int kFarPairs = kFarPoints / 2;
-// Resident CTAs per SM of the FP32 far kernel. With the columns' |delta|^2, weights and
-// delta . n_y in shared memory the packed loop fits 128 registers without spills: 4 CTAs per SM
-// (N = 20480: 10.28 ms; all point data in 168 registers at 3 CTAs 11.03 ms; 4 CTAs of that
-// layout with spills 11.23 ms, 2 CTAs 12.24 ms).
+// The columns' k |delta|^2 and weights sit in shared memory (each thread reads only its own
+// column), their in-plane coordinates in registers: 128 registers, 4 CTAs per SM (N = 20480:
+// 9.17 ms per assembly; capped at 96 registers for 5 CTAs per SM the loop spills, 9.55 ms).
 constexpr bool kFar32SmemCols = true;
 constexpr int kFar32MinBlocks = kFar32SmemCols ? 4 : 3;
 static_assert(kFarPoints == 2 * kFarPairs + 1, "the packed far loop pairs all points but the last");
@@ -654,14 +674,43 @@ struct Far32Sums {
     float gr, gi, hr, hi, tr, ti, er, ei;
 };
 
-// One quadrature point of a far pair, scalar (the point left over by the packed pairs).
-__device__ __forceinline__ void far32_point(Far32Sums& a, float px, float py, float pz, float pd, float pw, float pn,
-                                            float fx, float fy, float fz, float rc2f, float rcf, float kf, float k2f,
-                                            float fny, float fnx, float nxx, float nxy, float nxz, float nxny) {
-    const float num = fmaf(2.f, fx * px + fy * py + fz * pz, pd);
-    const float rq2 = rc2f + num;
+// FP32 constants of one far pair (row i, column j; d_c = c_j - x_i, column frame e1, e2, row
+// normal n_x, column normal n_y).
+struct Far32Pair {
+    float a2k, b2k;  // 2 k d_c . e1, 2 k d_c . e2
+    float rc2, rc;   // |d_c|^2, |d_c|
+    float ea, eb;    // -e1 . n_x, -e2 . n_x
+    float fnx;       // -d_c . n_x
+    float fny;       // d_c . n_y (= r_q n_y . r_hat for every point of the flat element)
+    float nxny;      // n_x . n_y
+};
+
+// FP32 margin test: true when the pair is certainly beyond the near-pair threshold, g = (level-0
+// centre of the column in FP32, thr_hi). thr_hi bounds (sqrt(thr) + the FP32 rounding of the
+// coordinates) squared from above (far32_col_threshold), so a pair this test calls far is far for
+// the correctly rounded FP64 test too; the FP64 test decides every pair this one does not.
+__device__ __forceinline__ bool far_by_margin(float4 g, float4 x) {
+    const float dx = g.x - x.x, dy = g.y - x.y, dz = g.z - x.z;
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > g.w;
+}
+
+// thr_hi of a column: (1 + 1e-6) (sqrt(thr) + 5e-7 R)^2 rounded up, R bounding every |coordinate|.
+// Per coordinate the FP32 difference of the rounded values is within 4.1 * 2^-24 R of the exact
+// difference, the FP32 distance within 4.3e-7 R of the exact one, and the FP32 square of it
+// (three roundings) within a factor 1 + 3 * 2^-24.
+__device__ __forceinline__ float far32_col_threshold(double thr, double bound) {
+    const double s = sqrt(fmax(thr, 0.0)) + 5e-7 * bound;
+    return __double2float_ru((1.0 + 1e-6) * s * s);
+}
+
+// One quadrature point (a, b, k |delta|^2, w J / 4 pi) of a far pair, scalar (the point left over
+// by the packed pairs). t = k (r_q - r_c) = k (2 d_c . delta + |delta|^2) / (r_q + r_c).
+__device__ __forceinline__ void far32_point(Far32Sums& s, float pa, float pb, float pdk, float pw,
+                                            const Far32Pair& c, float kf, float invk, float k2f) {
+    const float numk = fmaf(c.a2k, pa, fmaf(c.b2k, pb, pdk));
+    const float rq2 = fmaf(numk, invk, c.rc2);
     const float rinv = rsqrtf(rq2);
-    const float t = kf * __fdividef(num, fmaf(rq2, rinv, rcf));
+    const float t = numk * rcp_approx(fmaf(rq2, rinv, c.rc));
     float st, ct;
     if (fabsf(t) <= 3.14159265f) {
         __sincosf(t, &st, &ct);
@@ -670,38 +719,42 @@ __device__ __forceinline__ void far32_point(Far32Sums& a, float px, float py, fl
     }
     const float gs = pw * rinv;
     const float g_r = ct * gs, g_i = st * gs;
-    const float rny = (fny + pn) * rinv;
-    const float rnx = (fnx - (px * nxx + py * nxy + pz * nxz)) * rinv;
+    const float rny = c.fny * rinv;
+    const float rnx = fmaf(pb, c.eb, fmaf(pa, c.ea, c.fnx)) * rinv;
     const float b_r = -fmaf(g_r, rinv, g_i * kf);
     const float b_i = fmaf(g_r, kf, -g_i * rinv);
-    a.gr += g_r;
-    a.gi += g_i;
-    a.hr = fmaf(b_r, rny, a.hr);
-    a.hi = fmaf(b_i, rny, a.hi);
-    a.tr = fmaf(b_r, rnx, a.tr);
-    a.ti = fmaf(b_i, rnx, a.ti);
+    s.gr += g_r;
+    s.gi += g_i;
+    s.hr = fmaf(b_r, rny, s.hr);
+    s.hi = fmaf(b_i, rny, s.hi);
+    s.tr = fmaf(b_r, rnx, s.tr);
+    s.ti = fmaf(b_i, rnx, s.ti);
     const float rqq = rny * rnx;
-    const float s3 = fmaf(3.f, rqq, nxny);
+    const float s3 = fmaf(3.f, rqq, c.nxny);
     const float f_r = fmaf(rinv * rinv, s3, -k2f * rqq);
     const float f_i = -kf * rinv * s3;
-    a.er = fmaf(g_r, f_r, fmaf(-g_i, f_i, a.er));
-    a.ei = fmaf(g_r, f_i, fmaf(g_i, f_r, a.ei));
+    s.er = fmaf(g_r, f_r, fmaf(-g_i, f_i, s.er));
+    s.ei = fmaf(g_r, f_i, fmaf(g_i, f_r, s.ei));
 }
 
 // One (128-column tile, 64-row block) of the FP32 far field; all 128 threads of the CTA call it.
 template <bool kWithRhs, bool kSmemCols = true>
 __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const double* __restrict__ elem,
                                            int64_t n, int64_t ld, const double* __restrict__ coef, double k,
-                                           float2* __restrict__ A32, int64_t lda32, double2* __restrict__ far_part,
-                                           int64_t n_tiles, int64_t tile, int64_t row0,
-                                           unsigned* __restrict__ amax = nullptr, uint32_t* __restrict__ A16 = nullptr,
-                                           int64_t lda16 = 0, const float* __restrict__ hscale = nullptr,
+                                           double coord_bound, float2* __restrict__ A32, int64_t lda32,
+                                           double2* __restrict__ far_part, int64_t n_tiles, int64_t tile,
+                                           int64_t row0, unsigned* __restrict__ amax = nullptr,
+                                           uint32_t* __restrict__ A16 = nullptr, int64_t lda16 = 0,
+                                           const float* __restrict__ hscale = nullptr,
                                            int* __restrict__ hflag = nullptr) {
-    __shared__ float shs[kFar32Rows];  // the rows' complex-half scales (with A16)
-    __shared__ double sx[kFar32Rows][3];
-    __shared__ float snx[kFar32Rows][3];
-    __shared__ double sg[4][kFarTile];    // column: level-0 centre and near threshold
-    __shared__ float scf[8][kFarTile];    // column: matrix weights (cG, cH, cHt, cE)
+    __shared__ float shs[kFar32Rows];        // rows: complex-half scales (with A16)
+    __shared__ double sx[kFar32Rows][3];     // rows: collocation points
+    __shared__ float4 sxf[kFar32Rows];       // rows: collocation points in FP32 (margin test)
+    __shared__ float snx[kFar32Rows][3];     // rows: negated normals -n_x
+    __shared__ float4 sgf[kFarTile];         // column: level-0 centre in FP32, thr_hi
+    __shared__ float4 scf[2][kFarTile];      // column: matrix weights (cG, cH | cHt, cE)
+    __shared__ float4 sfa[kFarTile];         // column: e1 x, y, z, e2 x
+    __shared__ float2 sfb[kFarTile];         // column: e2 y, z
     __shared__ double sred[kFarTile / 32][2];
     const int tid = threadIdx.x;
     const int64_t j = tile * kFarTile + tid;
@@ -710,28 +763,28 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
         const int r = t / 3, c = t % 3;
         const int64_t i = row0 + r;
         sx[r][c] = (i < n) ? E(ECX + c, i) : 0.0;
-        snx[r][c] = (i < n) ? static_cast<float>(E(ENX + c, i)) : 0.f;
+        snx[r][c] = (i < n) ? -static_cast<float>(E(ENX + c, i)) : 0.f;
     }
-    if (A16)
-        for (int r = tid; r < kFar32Rows; r += kFarTile) shs[r] = (row0 + r < n) ? hscale[row0 + r] : 1.f;
-    // The column's 13 points in registers: points 2p, 2p + 1 in the lanes of pair p, the 13th alone.
-    float2 PX[kFarPairs], PY[kFarPairs], PZ[kFarPairs];
-    // |delta|^2, weight and delta . n_y of the column's points: in shared memory with kSmemCols
-    // (each thread reads only its own column; 42 fewer registers, 4 CTAs per SM instead of 3),
-    // else in registers (the persistent batched kernel, whose static shared memory is full).
-    constexpr int kS = kSmemCols ? kFarPairs : 1, kR = kSmemCols ? 1 : kFarPairs;
-    __shared__ float2 sPD[kS][kFarTile], sPW[kS][kFarTile], sPN[kS][kFarTile];
-    float2 PD[kR], PW[kR], PN[kR];
-    auto PD_ = [&](int p) -> float2& {
-        if constexpr (kSmemCols) return sPD[p][tid]; else return PD[p];
-    };
-    auto PW_ = [&](int p) -> float2& {
-        if constexpr (kSmemCols) return sPW[p][tid]; else return PW[p];
-    };
-    auto PN_ = [&](int p) -> float2& {
-        if constexpr (kSmemCols) return sPN[p][tid]; else return PN[p];
-    };
-    float lx, ly, lz, ld_, lw, ln;
+    for (int r = tid; r < kFar32Rows; r += kFarTile) {
+        const int64_t i = row0 + r;
+        sxf[r] = (i < n) ? make_float4(static_cast<float>(E(ECX, i)), static_cast<float>(E(ECY, i)),
+                                       static_cast<float>(E(ECZ, i)), 0.f)
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (A16) shs[r] = (i < n) ? hscale[i] : 1.f;
+    }
+    const float kf = static_cast<float>(k), k2f = kf * kf, invk = 1.f / kf;
+    // The column's 13 points: in-plane coordinates in registers (points 2p, 2p + 1 in the lanes of
+    // pair p, the 13th alone); k |delta|^2 and the weights in shared memory with kSmemCols, else in
+    // registers (the persistent batched kernel, whose static shared memory is full).
+    float2 PA[kFarPairs], PB[kFarPairs];
+    constexpr int kR = kSmemCols ? 1 : kFarPairs;
+    float4* sPDW = nullptr;  // (k |delta|^2, w J / 4 pi) of points 2p, 2p + 1 at [p * kFarTile + tid]
+    if constexpr (kSmemCols) {
+        __shared__ float4 sPDW_buf[kFarPairs * kFarTile];
+        sPDW = sPDW_buf;
+    }
+    float4 PDW[kR];
+    float la, lb, lpdk, lw;
     double cx = 0, cy = 0, cz = 0;
     float nyx = 0, nyy = 0, nyz = 0;
     const int64_t jj = j < n ? j : 0;
@@ -739,82 +792,93 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
     for (int p = 0; p < kFarPairs; ++p) {
         const float* s0 = qp32 + (int64_t)(2 * p * kQ32) * ld + jj;
         const float* s1 = s0 + (int64_t)kQ32 * ld;
-        PX[p] = make_float2(s0[0], s1[0]);
-        PY[p] = make_float2(s0[ld], s1[ld]);
-        PZ[p] = make_float2(s0[2 * ld], s1[2 * ld]);
-        PD_(p) = make_float2(s0[3 * ld], s1[3 * ld]);
-        PW_(p) = make_float2(s0[4 * ld], s1[4 * ld]);
-        PN_(p) = make_float2(s0[5 * ld], s1[5 * ld]);
+        PA[p] = make_float2(s0[0], s1[0]);
+        PB[p] = make_float2(s0[ld], s1[ld]);
+        const float4 v = make_float4(kf * s0[2 * ld], kf * s1[2 * ld], s0[3 * ld], s1[3 * ld]);
+        if constexpr (kSmemCols) sPDW[p * kFarTile + tid] = v; else PDW[p] = v;
     }
     {
         const float* sl = qp32 + (int64_t)((kFarPoints - 1) * kQ32) * ld + jj;
-        lx = sl[0];
-        ly = sl[ld];
-        lz = sl[2 * ld];
-        ld_ = sl[3 * ld];
-        lw = sl[4 * ld];
-        ln = sl[5 * ld];
+        la = sl[0];
+        lb = sl[ld];
+        lpdk = kf * sl[2 * ld];
+        lw = sl[3 * ld];
+        const float* fr = qp32 + (int64_t)kQ32Frame * ld + jj;
+        sfa[tid] = make_float4(fr[0], fr[ld], fr[2 * ld], fr[3 * ld]);
+        sfb[tid] = make_float2(fr[4 * ld], fr[5 * ld]);
     }
     if (j < n) {
         cx = E(ECX, j); cy = E(ECY, j); cz = E(ECZ, j);
         nyx = static_cast<float>(E(ENX, j));
         nyy = static_cast<float>(E(ENY, j));
         nyz = static_cast<float>(E(ENZ, j));
-        sg[0][tid] = E(EGX, j);
-        sg[1][tid] = E(EGY, j);
-        sg[2][tid] = E(EGZ, j);
-        sg[3][tid] = near_threshold(E(EAREA, j));
-        for (int f = 0; f < 8; ++f) scf[f][tid] = static_cast<float>(coef[(int64_t)(CF_CG + f) * ld + j]);
+        sgf[tid] = make_float4(static_cast<float>(E(EGX, j)), static_cast<float>(E(EGY, j)),
+                               static_cast<float>(E(EGZ, j)),
+                               far32_col_threshold(near_threshold(E(EAREA, j)), coord_bound));
+        float cw[8];
+        for (int f = 0; f < 8; ++f) cw[f] = static_cast<float>(coef[(int64_t)(CF_CG + f) * ld + j]);
+        scf[0][tid] = make_float4(cw[0], cw[1], cw[2], cw[3]);
+        scf[1][tid] = make_float4(cw[4], cw[5], cw[6], cw[7]);
     } else {
-        sg[0][tid] = sg[1][tid] = sg[2][tid] = 0.0;
-        sg[3][tid] = -1.0;
-        for (int f = 0; f < 8; ++f) scf[f][tid] = 0.f;
+        sgf[tid] = make_float4(0.f, 0.f, 0.f, INFINITY);
+        scf[0][tid] = scf[1][tid] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
-    const float kf = static_cast<float>(k), k2f = kf * kf;
     const int64_t rows_here = (n - row0 < kFar32Rows) ? (n - row0) : kFar32Rows;
     float vmax = 0.f;  // largest |re|, |im| this thread wrote (+inf for a non-finite part)
     int hbad = 0;      // a complex-half entry this thread wrote left the FP16 range
     for (int r = 0; r < rows_here; ++r) {
         const int64_t i = row0 + r;
-        const double x0 = sx[r][0], x1 = sx[r][1], x2 = sx[r][2];
-        const bool active = (j < n) && (j != i) && !near_superset(sg[0][tid], sg[1][tid], sg[2][tid], sg[3][tid], x0, x1, x2);
+        bool active = (j < n) && (j != i);
+        // the rare pairs the margin test leaves open: the FP64 test on the column's global data
+        if (active && !far_by_margin(sgf[tid], sxf[r]))
+            active = !near_superset(E(EGX, j), E(EGY, j), E(EGZ, j), near_threshold(E(EAREA, j)), sx[r][0], sx[r][1],
+                                    sx[r][2]);
         double2 rhs_c = make_double2(0.0, 0.0);
         if (active) {
             // FP64: centroid offset, distance and the reduced phase k r_c mod 2 pi.
-            const double dcx = cx - x0, dcy = cy - x1, dcz = cz - x2;
+            const double dcx = cx - sx[r][0], dcy = cy - sx[r][1], dcz = cz - sx[r][2];
             const double rc2 = dcx * dcx + dcy * dcy + dcz * dcz;
-            const double rc = rc2 * sb_rsqrt2(rc2);
+            const double rc = rc2 * sb_rsqrt1(rc2);
             const double ph = k * rc;
             const double nq = rint(ph * 0x1.45f306dc9c883p-3);  // 1 / (2 pi)
-            double red = fma(-nq, 0x1.921fb54442d18p+2, ph);    // 2 pi split in two doubles
-            red = fma(-nq, 0x1.1a62633145c07p-52, red);
+            // 2 pi rounded to FP64: |nq| (2 pi - that) stays below 1e-13 for |k r_c| < 1e3
+            const double red = fma(-nq, 0x1.921fb54442d18p+2, ph);
             float sc, cc;
             sincos_f32(static_cast<float>(red), &sc, &cc);
             const float fx = static_cast<float>(dcx), fy = static_cast<float>(dcy), fz = static_cast<float>(dcz);
-            const float rcf = static_cast<float>(rc), rc2f = static_cast<float>(rc2);
-            const float nxx = snx[r][0], nxy = snx[r][1], nxz = snx[r][2];
-            const float nxny = nxx * nyx + nxy * nyy + nxz * nyz;
-            const float fny = fx * nyx + fy * nyy + fz * nyz;       // d_c . n_y
-            const float fnx = -(fx * nxx + fy * nxy + fz * nxz);    // -d_c . n_x
-            // Points in pairs. With b = g (-1/r + i k) = -(u + i nbi), u = g_r / r + g_i k and
-            // nbi = g_i / r - g_r k, and the E factor f = (3 rq + nx.ny)(1/r)(1/r - i k) - k^2 rq:
-            //   H = -sum (u + i nbi) r.n_y, H^T = -sum (u + i nbi)(-r.n_x),
-            //   E = sum q1 (u + i nbi) - k^2 sum g rq, q1 = (3 rq + nx.ny) / r,
-            // so every channel is a lane sum of one fma per point and the k factors apply once.
-            const float2 FX2 = bc2(2.f * fx), FY2 = bc2(2.f * fy), FZ2 = bc2(2.f * fz);
-            const float2 RC2 = bc2(rc2f), RC = bc2(rcf), KK = bc2(kf), NK = bc2(-kf);
-            const float2 FNY = bc2(fny), FNX = bc2(fnx), NXX = bc2(nxx), NXY = bc2(nxy), NXZ = bc2(nxz);
-            const float2 NXNY = bc2(nxny), M1 = bc2(-1.f), THREE = bc2(3.f);
+            const float nnx = snx[r][0], nny = snx[r][1], nnz = snx[r][2];
+            const float4 fa = sfa[tid];
+            const float2 fb = sfb[tid];
+            Far32Pair c;
+            c.a2k = 2.f * kf * (fx * fa.x + fy * fa.y + fz * fa.z);
+            c.b2k = 2.f * kf * (fx * fa.w + fy * fb.x + fz * fb.y);
+            c.rc2 = static_cast<float>(rc2);
+            c.rc = static_cast<float>(rc);
+            c.ea = fa.x * nnx + fa.y * nny + fa.z * nnz;
+            c.eb = fa.w * nnx + fb.x * nny + fb.y * nnz;
+            c.fnx = fx * nnx + fy * nny + fz * nnz;
+            c.fny = fx * nyx + fy * nyy + fz * nyz;
+            c.nxny = -(nnx * nyx + nny * nyy + nnz * nyz);
+            // Points in pairs. With u = g_r / r + g_i k and nbi = g_i / r - g_r k (b = g (-1/r + i k) =
+            // -(u + i nbi)), r.n_y = fny / r and q1 = (3 r.n_y r.(-n_x) + n_x.n_y) / r:
+            //   H = -fny sum (u + i nbi) / r,  H^T = -sum (u + i nbi) r.(-n_x),
+            //   E = sum q1 (u + i nbi) - k^2 fny sum g r.(-n_x) / r,
+            // so every channel is a lane sum of one fma per point.
+            const float2 A2K = bc2(c.a2k), B2K = bc2(c.b2k), RC2 = bc2(c.rc2), RC = bc2(c.rc);
+            const float2 EA = bc2(c.ea), EB = bc2(c.eb), FNX = bc2(c.fnx), FNY3 = bc2(3.f * c.fny);
+            const float2 NXNY = bc2(c.nxny), KK = bc2(kf), NK = bc2(-kf), INVK = bc2(invk);
             const float2 Z = bc2(0.f);
-            float2 AGR = Z, AGI = Z, NAHR = Z, NAHI = Z, NATR = Z, NATI = Z, AER = Z, AEI = Z, GQR = Z, GQI = Z;
+            float2 AGR = Z, AGI = Z, SHR = Z, SHI = Z, NATR = Z, NATI = Z, AER = Z, AEI = Z, GQR = Z, GQI = Z;
 #pragma unroll
             for (int p = 0; p < kFarPairs; ++p) {
-                const float2 num = pfma(FX2, PX[p], pfma(FY2, PY[p], pfma(FZ2, PZ[p], PD_(p))));
-                const float2 rq2 = padd(RC2, num);
+                float4 dw;
+                if constexpr (kSmemCols) dw = sPDW[p * kFarTile + tid]; else dw = PDW[p];
+                const float2 numk = pfma(A2K, PA[p], pfma(B2K, PB[p], make_float2(dw.x, dw.y)));
+                const float2 rq2 = pfma(numk, INVK, RC2);
                 const float2 rinv = make_float2(rsqrtf(rq2.x), rsqrtf(rq2.y));
                 const float2 den = pfma(rq2, rinv, RC);
-                const float2 t = pmul(KK, pmul(num, make_float2(rcp_approx(den.x), rcp_approx(den.y))));
+                const float2 t = pmul(numk, make_float2(rcp_approx(den.x), rcp_approx(den.y)));
                 // Special-function sine / cosine while both phase offsets are within one element
                 // size (|t| <= pi, every resolved mesh), else the quadrant-reduced version.
                 float2 S, C;
@@ -825,41 +889,39 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                     sincos_f32(t.x, &S.x, &C.x);
                     sincos_f32(t.y, &S.y, &C.y);
                 }
-                const float2 gs = pmul(PW_(p), rinv);
+                const float2 gs = pmul(make_float2(dw.z, dw.w), rinv);
                 const float2 gr = pmul(C, gs), gi = pmul(S, gs);
-                const float2 rny = pmul(padd(FNY, PN_(p)), rinv);
-                const float2 pnx = pfma(PZ[p], NXZ, pfma(PY[p], NXY, pmul(PX[p], NXX)));
-                const float2 rnx = pmul(pfma(pnx, M1, FNX), rinv);
+                const float2 rnx = pmul(pfma(PB[p], EB, pfma(PA[p], EA, FNX)), rinv);
                 const float2 u = pfma(gr, rinv, pmul(gi, KK));
                 const float2 nbi = pfma(gi, rinv, pmul(gr, NK));
                 AGR = padd(AGR, gr);
                 AGI = padd(AGI, gi);
-                NAHR = pfma(u, rny, NAHR);
-                NAHI = pfma(nbi, rny, NAHI);
+                SHR = pfma(u, rinv, SHR);
+                SHI = pfma(nbi, rinv, SHI);
                 NATR = pfma(u, rnx, NATR);
                 NATI = pfma(nbi, rnx, NATI);
-                const float2 rqq = pmul(rny, rnx);
-                const float2 q1 = pmul(rinv, pfma(THREE, rqq, NXNY));
+                const float2 rq1 = pmul(rnx, rinv);
+                const float2 q1 = pmul(rinv, pfma(FNY3, rq1, NXNY));
                 AER = pfma(q1, u, AER);
                 AEI = pfma(q1, nbi, AEI);
-                GQR = pfma(gr, rqq, GQR);
-                GQI = pfma(gi, rqq, GQI);
+                GQR = pfma(gr, rq1, GQR);
+                GQI = pfma(gi, rq1, GQI);
             }
+            const float kfny = k2f * c.fny;
             Far32Sums sm{AGR.x + AGR.y,
                          AGI.x + AGI.y,
-                         -(NAHR.x + NAHR.y),
-                         -(NAHI.x + NAHI.y),
+                         -c.fny * (SHR.x + SHR.y),
+                         -c.fny * (SHI.x + SHI.y),
                          -(NATR.x + NATR.y),
                          -(NATI.x + NATI.y),
-                         (AER.x + AER.y) - k2f * (GQR.x + GQR.y),
-                         (AEI.x + AEI.y) - k2f * (GQI.x + GQI.y)};
-            far32_point(sm, lx, ly, lz, ld_, lw, ln, fx, fy, fz, rc2f, rcf, kf, k2f, fny, fnx, nxx, nxy, nxz, nxny);
-            const float ag_r = sm.gr, ag_i = sm.gi, ah_r = sm.hr, ah_i = sm.hi, at_r = sm.tr, at_i = sm.ti,
-                        ae_r = sm.er, ae_i = sm.ei;
-            const float cgr = scf[0][tid], cgi = scf[1][tid], chr = scf[2][tid], chi = scf[3][tid];
-            const float ctr = scf[4][tid], cti = scf[5][tid], cer = scf[6][tid], cei = scf[7][tid];
-            const float ur = ag_r * cgr - ag_i * cgi + ah_r * chr - ah_i * chi + at_r * ctr - at_i * cti + ae_r * cer - ae_i * cei;
-            const float ui = ag_r * cgi + ag_i * cgr + ah_r * chi + ah_i * chr + at_r * cti + at_i * ctr + ae_r * cei + ae_i * cer;
+                         (AER.x + AER.y) - kfny * (GQR.x + GQR.y),
+                         (AEI.x + AEI.y) - kfny * (GQI.x + GQI.y)};
+            far32_point(sm, la, lb, lpdk, lw, c, kf, invk, k2f);
+            const float4 w0 = scf[0][tid], w1 = scf[1][tid];  // (cG, cH), (cHt, cE)
+            const float ur = sm.gr * w0.x - sm.gi * w0.y + sm.hr * w0.z - sm.hi * w0.w + sm.tr * w1.x -
+                             sm.ti * w1.y + sm.er * w1.z - sm.ei * w1.w;
+            const float ui = sm.gr * w0.y + sm.gi * w0.x + sm.hr * w0.w + sm.hi * w0.z + sm.tr * w1.y +
+                             sm.ti * w1.x + sm.er * w1.w + sm.ei * w1.z;
             // rotate by the pair phase exp(i k r_c) = (cc, sc)
             const float2 v = make_float2(ur * cc - ui * sc, ur * sc + ui * cc);
             A32[i * lda32 + j] = v;
@@ -868,10 +930,10 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             if (A16) A16[i * lda16 + j] = half_pack(v, shs[r], &hbad);
             if (kWithRhs) {
                 Acc a;
-                a.gr = ag_r * cc - ag_i * sc; a.gi = ag_r * sc + ag_i * cc;
-                a.hr = ah_r * cc - ah_i * sc; a.hi = ah_r * sc + ah_i * cc;
-                a.tr = at_r * cc - at_i * sc; a.ti = at_r * sc + at_i * cc;
-                a.er = ae_r * cc - ae_i * sc; a.ei = ae_r * sc + ae_i * cc;
+                a.gr = sm.gr * cc - sm.gi * sc; a.gi = sm.gr * sc + sm.gi * cc;
+                a.hr = sm.hr * cc - sm.hi * sc; a.hi = sm.hr * sc + sm.hi * cc;
+                a.tr = sm.tr * cc - sm.ti * sc; a.ti = sm.tr * sc + sm.ti * cc;
+                a.er = sm.er * cc - sm.ei * sc; a.ei = sm.er * sc + sm.ei * cc;
                 rhs_c = combine(a, coef, ld, j, CF_DG);
             }
         }
@@ -908,13 +970,14 @@ template <bool kWithRhs>
 __global__ void __launch_bounds__(kFarTile, kFar32MinBlocks) k_far32(const float* __restrict__ qp32,
                                                     const double* __restrict__ elem, int64_t n,
                                                     int64_t ld, const double* __restrict__ coef,
-                                                    double k, float2* __restrict__ A32, int64_t lda32,
-                                                    double2* __restrict__ far_part, int64_t n_tiles,
+                                                    double k, double coord_bound, float2* __restrict__ A32,
+                                                    int64_t lda32, double2* __restrict__ far_part, int64_t n_tiles,
                                                     unsigned* __restrict__ amax, uint32_t* __restrict__ A16,
                                                     int64_t lda16, const float* __restrict__ hscale,
                                                     int* __restrict__ hflag) {
-    far32_tile<kWithRhs, kFar32SmemCols>(qp32, elem, n, ld, coef, k, A32, lda32, far_part, n_tiles, blockIdx.x,
-                                         blockIdx.y * (int64_t)kFar32Rows, amax, A16, lda16, hscale, hflag);
+    far32_tile<kWithRhs, kFar32SmemCols>(qp32, elem, n, ld, coef, k, coord_bound, A32, lda32, far_part, n_tiles,
+                                         blockIdx.x, blockIdx.y * (int64_t)kFar32Rows, amax, A16, lda16, hscale,
+                                         hflag);
 }
 
 // Complex-half copy during the FP32 assembly (after the near and self kernels): each row's scale
@@ -2353,8 +2416,8 @@ __global__ void __launch_bounds__(kFarTile, 4) k_assemble_batch(const BatchAsmIn
             const BatchAsmInst I = inst[b];
             const int64_t local = item - fpre[b];
             const int64_t nrb = (I.n + kFar32Rows - 1) / kFar32Rows;
-            far32_tile<false, false>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr, I.n_tiles,
-                              local / nrb, (local % nrb) * kFar32Rows);
+            far32_tile<false, false>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.coord_bound, I.A32, I.lda32, nullptr,
+                                     I.n_tiles, local / nrb, (local % nrb) * kFar32Rows);
         } else if (item < nf + nn) {
             const int64_t it = item - nf;
             const int b = find_instance(npre, ninst, it);
@@ -2479,11 +2542,12 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
         m->ld = m->n_tiles * kFarTile;
         m->h_nodes.assign(nodes, nodes + 3 * n_nodes);
         m->h_tris.assign(tris, tris + 3 * n_tris);
+        for (int64_t a = 0; a < 3 * n_nodes; ++a) m->coord_bound = std::max(m->coord_bound, std::fabs(nodes[a]));
         m->nodes.alloc(sizeof(double) * 3 * n_nodes);
         m->tris.alloc(sizeof(uint32_t) * 3 * n_tris);
         m->elem.alloc(sizeof(double) * EFIELDS * m->ld);
         m->qp.alloc(sizeof(double) * kQpTileDoubles * m->n_tiles);
-        m->qp32.alloc(sizeof(float) * kFarPoints * kQ32 * m->ld);
+        m->qp32.alloc(sizeof(float) * kQ32Fields * m->ld);
         h2d_sync(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes);
         h2d_sync(m->tris.p, tris, sizeof(uint32_t) * 3 * n_tris);
         const int64_t nb = cdiv(m->ld, 256);
@@ -2741,10 +2805,9 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     float2* A32 = (f32 || mixed) ? op.A32.as<float2>() : nullptr;
     // Near pairs and self terms write entries disjoint from the far tiles. With the FP64 far kernel
     // they run on the side stream, concurrently with it (N = 20480: 38.9 -> 37.3 ms per assembly);
-    // the FP32 far kernel fills every SM's register file (3 CTAs x 128 threads x 168 registers),
-    // so a concurrent near kernel only time-shares with it (14.13 ms either way; capping the far
-    // kernel at 2 CTAs per SM to make room for near CTAs gave 15.53 ms) and they run before it on
-    // the operator's stream. The right-hand-side reduction waits for both.
+    // the FP32 far kernel fills every SM's register file (4 CTAs x 128 threads x 128 registers),
+    // so a concurrent near kernel only time-shares with it, and they run before it on the
+    // operator's stream. The right-hand-side reduction waits for both.
     const bool overlap = !mixed;
     if (overlap) {
         op.side.ensure();
@@ -2791,12 +2854,13 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
             dim3 grid(static_cast<unsigned>(m.n_tiles), static_cast<unsigned>(cdiv(n, kFar32Rows)));
             if (with_rhs)
                 k_far32<true><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
-                                                                 op.coef.as<double>(), k, A32, op.lda32,
+                                                                 op.coef.as<double>(), k, m.coord_bound, A32, op.lda32,
                                                                  op.far_part.as<double2>(), m.n_tiles, nullptr, A16,
                                                                  op.lda16, hs, hflag);
             else
                 k_far32<false><<<grid, kFarTile, 0, op.stream>>>(m.qp32.as<float>(), m.elem.as<double>(), n, ld,
-                                                                  op.coef.as<double>(), k, A32, op.lda32, nullptr,
+                                                                  op.coef.as<double>(), k, m.coord_bound, A32,
+                                                                  op.lda32, nullptr,
                                                                   m.n_tiles, nullptr, A16, op.lda16, hs, hflag);
             count_launch();
             SB_CUDA(cudaGetLastError());
@@ -3055,7 +3119,8 @@ void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_
         const BatchAsmInst& I = h_inst[b];
         ProfScope prof(SB_PROF_FAR, s);
         dim3 grid(static_cast<unsigned>(I.n_tiles), static_cast<unsigned>(cdiv(I.n, kFar32Rows)));
-        k_far32<false><<<grid, kFarTile, 0, s>>>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.A32, I.lda32, nullptr,
+        k_far32<false><<<grid, kFarTile, 0, s>>>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.coord_bound, I.A32,
+                                                 I.lda32, nullptr,
                                                  I.n_tiles, amax ? amax + 4 * b : nullptr, nullptr, 0, nullptr,
                                                  nullptr);
         count_launch();

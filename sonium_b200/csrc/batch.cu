@@ -1357,6 +1357,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
                 BatchAsmInst A;
                 A.elem = m->elem.as<double>();
                 A.qp32 = m->qp32.as<float>();
+                A.coord_bound = m->coord_bound;
                 A.n = m->n;
                 A.ld = m->ld;
                 A.n_tiles = m->n_tiles;

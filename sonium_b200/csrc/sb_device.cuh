@@ -74,6 +74,13 @@ __device__ __forceinline__ double sb_rsqrt(double a) {
     return y;
 }
 
+// One Newton step from the FP32 estimate: relative error below 1e-13, enough for the FP64 phase
+// k r of the FP32 far field, whose entries carry FP32 rounding.
+__device__ __forceinline__ double sb_rsqrt1(double a) {
+    double y = static_cast<double>(rsqrtf(static_cast<float>(a)));
+    return y * fma(-0.5 * a * y, y, 1.5);
+}
+
 // The same with two Newton steps: relative error below 2e-14, enough for the phase k r and the
 // 1e-10 parity bar of the assembled entries.
 __device__ __forceinline__ double sb_rsqrt2(double a) {

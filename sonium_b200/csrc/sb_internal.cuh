@@ -143,6 +143,7 @@ constexpr int kFarTile = 128;  // field elements per far-kernel column tile
 struct Mesh {
     int device = 0;
     int64_t n = 0, n_nodes = 0, ld = 0, n_tiles = 0;
+    double coord_bound = 0.0;  // largest |coordinate| of the nodes (bounds FP32 rounding of positions)
     std::vector<double> h_nodes;
     std::vector<uint32_t> h_tris;
     std::vector<double> h_elem;  // host copy of the element SoA (ld stride)
@@ -229,6 +230,7 @@ struct Operator {
 struct BatchAsmInst {
     const double* elem;
     const float* qp32;
+    double coord_bound;  // the mesh's largest |coordinate| (FP32 near-pair margin test)
     const double* coef;
     double2* diag;
     float2* A32;
