@@ -36,6 +36,11 @@ __constant__ double c_tri_eta[kTriTotal];
 __constant__ double c_tri_w[kTriTotal];
 __constant__ int c_tri_off[kTriOrders];
 __constant__ int c_tri_cnt[kTriOrders];
+// (cos, sin)(m pi / 64), m = 0..127: the pair phase of the FP32 far field is a table angle plus a
+// remainder below pi / 128 (global memory, read through the read-only cache: the lanes of a warp
+// read different entries).
+constexpr int kPhaseTab = 128;
+__device__ float2 g_phase_tab[kPhaseTab];
 
 // Gauss-Legendre on [-1, 1] by Newton iteration on the Legendre three-term recurrence.
 void host_gauss_legendre(int n, double* x, double* w) {
@@ -142,6 +147,10 @@ void ensure_tables(int device) {
     SB_CUDA(cudaMemcpyToSymbol(c_tri_w, tw, sizeof(tw)));
     SB_CUDA(cudaMemcpyToSymbol(c_tri_off, off, sizeof(off)));
     SB_CUDA(cudaMemcpyToSymbol(c_tri_cnt, cnt, sizeof(cnt)));
+    float2 ph[kPhaseTab];
+    for (int m = 0; m < kPhaseTab; ++m)
+        ph[m] = make_float2(static_cast<float>(std::cos(m * (M_PI / 64.0))), static_cast<float>(std::sin(m * (M_PI / 64.0))));
+    SB_CUDA(cudaMemcpyToSymbol(g_phase_tab, ph, sizeof(ph)));
     SB_CUDA(cudaDeviceSynchronize());  // tables in place before kernels on any stream read them
     done[device] = true;
 }
@@ -618,7 +627,11 @@ __global__ void k_far_points32(const double* __restrict__ elem, int64_t n, int64
 // sin / cos in FP32 for |x| <= pi: quadrant reduction by pi/2 and Taylor series to x^9 / x^10
 // on |r| <= pi/4 (truncation below 2e-9).
 __device__ __forceinline__ void sincos_f32(float x, float* so, float* co) {
-    const float q = rintf(x * 0.636619772f);
+    // x 2/pi rounded to the nearest integer by adding 1.5 * 2^23 (one rounding, ties to even, as
+    // rintf), which also leaves the integer's low bits in the sum's mantissa: no conversion
+    // instructions on the special-function unit.
+    const float y = fmaf(x, 0.636619772f, 12582912.0f);
+    const float q = y - 12582912.0f;
     float r = fmaf(-q, 1.57079637f, x);
     r = fmaf(-q, -4.37113883e-8f, r);
     const float r2 = r * r;
@@ -633,7 +646,7 @@ __device__ __forceinline__ void sincos_f32(float x, float* so, float* co) {
     pc = fmaf(pc, r2, 4.16666667e-2f);
     pc = fmaf(pc, r2, -0.5f);
     const float cs = fmaf(pc, r2, 1.0f);
-    const int quad = static_cast<int>(q) & 3;
+    const int quad = __float_as_int(y) & 3;
     float sv = sn, cv = cs;
     if (quad & 1) {
         sv = cs;
@@ -841,11 +854,20 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             const double rc2 = dcx * dcx + dcy * dcy + dcz * dcz;
             const double rc = rc2 * sb_rsqrt1(rc2);
             const double ph = k * rc;
-            const double nq = rint(ph * 0x1.45f306dc9c883p-3);  // 1 / (2 pi)
-            // 2 pi rounded to FP64: |nq| (2 pi - that) stays below 1e-13 for |k r_c| < 1e3
-            const double red = fma(-nq, 0x1.921fb54442d18p+2, ph);
-            float sc, cc;
-            sincos_f32(static_cast<float>(red), &sc, &cc);
+            // exp(i k r_c): k r_c = m pi / 64 + b with m the nearest integer (found by adding
+            // 1.5 * 2^52, which leaves m in the low mantissa bits), |b| <= pi / 128 from an FP64 fma
+            // (pi / 64 rounded to FP64: m times its error stays below 1e-13 for k r_c < 1e3), then
+            // the table entry rotated by b's sine and cosine (Taylor to b^3 and b^4, truncation
+            // below 1e-10); error about 1e-7 from the FP32 table.
+            const double y = fma(ph, 0x1.45f306dc9c883p+4, 0x1.8p52);  // 64 / pi
+            const double nq = y - 0x1.8p52;
+            const int m = __double2loint(y) & (kPhaseTab - 1);
+            const float b = static_cast<float>(fma(-nq, 0x1.921fb54442d18p-5, ph));  // pi / 64
+            const float b2 = b * b;
+            const float sb = fmaf(b * b2, -1.f / 6.f, b);
+            const float cb = fmaf(b2, fmaf(b2, 1.f / 24.f, -0.5f), 1.f);
+            const float2 tab = __ldg(&g_phase_tab[m]);
+            const float cc = tab.x * cb - tab.y * sb, sc = tab.y * cb + tab.x * sb;
             const float fx = static_cast<float>(dcx), fy = static_cast<float>(dcy), fz = static_cast<float>(dcz);
             const float nnx = snx[r][0], nny = snx[r][1], nnz = snx[r][2];
             const float4 fa = sfa[tid];
@@ -868,8 +890,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             const float2 A2K = bc2(c.a2k), B2K = bc2(c.b2k), RC2 = bc2(c.rc2), RC = bc2(c.rc);
             const float2 EA = bc2(c.ea), EB = bc2(c.eb), FNX = bc2(c.fnx), FNY3 = bc2(3.f * c.fny);
             const float2 NXNY = bc2(c.nxny), KK = bc2(kf), NK = bc2(-kf), INVK = bc2(invk);
-            const float2 Z = bc2(0.f);
-            float2 AGR = Z, AGI = Z, SHR = Z, SHI = Z, NATR = Z, NATI = Z, AER = Z, AEI = Z, GQR = Z, GQI = Z;
+            float2 AGR, AGI, SHR, SHI, NATR, NATI, AER, AEI, GQR, GQI;  // set by the first pair
 #pragma unroll
             for (int p = 0; p < kFarPairs; ++p) {
                 float4 dw;
@@ -894,18 +915,31 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                 const float2 rnx = pmul(pfma(PB[p], EB, pfma(PA[p], EA, FNX)), rinv);
                 const float2 u = pfma(gr, rinv, pmul(gi, KK));
                 const float2 nbi = pfma(gi, rinv, pmul(gr, NK));
-                AGR = padd(AGR, gr);
-                AGI = padd(AGI, gi);
-                SHR = pfma(u, rinv, SHR);
-                SHI = pfma(nbi, rinv, SHI);
-                NATR = pfma(u, rnx, NATR);
-                NATI = pfma(nbi, rnx, NATI);
                 const float2 rq1 = pmul(rnx, rinv);
                 const float2 q1 = pmul(rinv, pfma(FNY3, rq1, NXNY));
-                AER = pfma(q1, u, AER);
-                AEI = pfma(q1, nbi, AEI);
-                GQR = pfma(gr, rq1, GQR);
-                GQI = pfma(gi, rq1, GQI);
+                if (p == 0) {
+                    AGR = gr;
+                    AGI = gi;
+                    SHR = pmul(u, rinv);
+                    SHI = pmul(nbi, rinv);
+                    NATR = pmul(u, rnx);
+                    NATI = pmul(nbi, rnx);
+                    AER = pmul(q1, u);
+                    AEI = pmul(q1, nbi);
+                    GQR = pmul(gr, rq1);
+                    GQI = pmul(gi, rq1);
+                } else {
+                    AGR = padd(AGR, gr);
+                    AGI = padd(AGI, gi);
+                    SHR = pfma(u, rinv, SHR);
+                    SHI = pfma(nbi, rinv, SHI);
+                    NATR = pfma(u, rnx, NATR);
+                    NATI = pfma(nbi, rnx, NATI);
+                    AER = pfma(q1, u, AER);
+                    AEI = pfma(q1, nbi, AEI);
+                    GQR = pfma(gr, rq1, GQR);
+                    GQI = pfma(gi, rq1, GQI);
+                }
             }
             const float kfny = k2f * c.fny;
             Far32Sums sm{AGR.x + AGR.y,

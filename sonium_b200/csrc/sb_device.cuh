@@ -74,10 +74,12 @@ __device__ __forceinline__ double sb_rsqrt(double a) {
     return y;
 }
 
-// One Newton step from the FP32 estimate: relative error below 1e-13, enough for the FP64 phase
-// k r of the FP32 far field, whose entries carry FP32 rounding.
+// One Newton step from the hardware's FP64 reciprocal square-root estimate (about 2^-22 relative,
+// from the special-function unit without FP32 conversions): relative error below 1e-13, enough
+// for the FP64 phase k r of the FP32 far field, whose entries carry FP32 rounding.
 __device__ __forceinline__ double sb_rsqrt1(double a) {
-    double y = static_cast<double>(rsqrtf(static_cast<float>(a)));
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
     return y * fma(-0.5 * a * y, y, 1.5);
 }
 
