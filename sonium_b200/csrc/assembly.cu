@@ -1333,9 +1333,10 @@ __device__ void near_channels_at(Acc* a, NearWarpSmem& S, const double* __restri
             const double py = sf0 * V[0][1] + xio * V[1][1] + eto * V[2][1];
             const double pz = sf0 * V[0][2] + xio * V[1][2] + eto * V[2][2];
             const double dx = px - x0, dy = py - x1, dz = pz - x2;
-            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
-            if (!(dis >= 1e-15)) continue;
-            const double rinv = 1.0 / dis;
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (!(d2 >= 1e-30)) continue;  // dis < 1e-15 (normalize, element.rs:304-311)
+            const double rinv = sb_rsqrt2(d2);
+            const double dis = d2 * rinv;
             if constexpr (NB == 1) {
                 point_channels(a[0], dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
             } else {
@@ -1370,12 +1371,14 @@ __device__ __forceinline__ Acc warp_reduce(const Acc& a) {
     return r;
 }
 
-// 5 resident CTAs (20 warps) per SM: 96 registers (8 bytes spilled); more warps hide the FP64
-// latency of the subdivision replay (N = 20480: 2.88 -> 2.56 ms; 6 CTAs 2.83 ms).
+// 5 resident CTAs (20 warps) per SM: 96 registers; more warps hide the FP64 latency of the
+// subdivision replay (N = 20480: 2.88 -> 2.56 ms; 6 CTAs 2.83 ms). The grid holds what is
+// resident and each warp strides over the pairs, so that the uneven trees (52 to over 400
+// points per pair) do not leave CTAs held by one slow warp.
 constexpr int kNearMinBlocks = 5;
 __global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near(const double* __restrict__ elem,
                                                           int64_t n, int64_t ld,
-                                                          const int64_t* __restrict__ row_ptr,
+                                                          const int32_t* __restrict__ rows,
                                                           const int32_t* __restrict__ cols,
                                                           int64_t nnz,
                                                           const double* __restrict__ coef,
@@ -1384,24 +1387,27 @@ __global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near(const 
                                                           double2* __restrict__ near_rhs) {
     __shared__ NearWarpSmem smem[kNearWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t p = blockIdx.x * (int64_t)kNearWarps + warp;
-    if (p >= nnz) return;
-    // Row of pair p by binary search in row_ptr.
-    int64_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int64_t mid = (lo + hi + 1) >> 1;
-        if (row_ptr[mid] <= p) lo = mid; else hi = mid - 1;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kNearWarps;
+    for (int64_t p = blockIdx.x * (int64_t)kNearWarps + warp; p < nnz; p += stride) {
+        const int64_t i = rows[p], j = cols[p];
+        Acc a;
+        near_pair_channels(a, smem[warp], elem, ld, i, j, k, k * k, lane);
+        const Acc t = warp_reduce(a);
+        if (lane == 0) {
+            const double2 v = combine(t, coef, ld, j, CF_CG);
+            if (A64) A64[i * n + j] = v;
+            if (A32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+            if (near_rhs) near_rhs[p] = combine(t, coef, ld, j, CF_DG);
+        }
+        __syncwarp();  // the warp's shared replay state is reused by its next pair
     }
-    const int64_t i = lo, j = cols[p];
-    Acc a;
-    near_pair_channels(a, smem[warp], elem, ld, i, j, k, k * k, lane);
-    const Acc t = warp_reduce(a);
-    if (lane == 0) {
-        const double2 v = combine(t, coef, ld, j, CF_CG);
-        if (A64) A64[i * n + j] = v;
-        if (A32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
-        if (near_rhs) near_rhs[p] = combine(t, coef, ld, j, CF_DG);
-    }
+}
+
+// Grid of k_near for nnz pairs: what is resident (kNearMinBlocks CTAs per SM), or fewer.
+static unsigned near_grid(int64_t nnz, int device) {
+    const int64_t need = (nnz + kNearWarps - 1) / kNearWarps;
+    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(kNearMinBlocks) *
+                                                                                  device_sm_count(device))));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2458,12 +2464,7 @@ __global__ void __launch_bounds__(kFarTile, 4) k_assemble_batch(const BatchAsmIn
             const BatchAsmInst I = inst[b];
             const int64_t p = (it - npre[b]) * kNearWarps + warp;
             if (p < I.nnz) {
-                int64_t lo = 0, hi = I.n - 1;
-                while (lo < hi) {
-                    const int64_t mid = (lo + hi + 1) >> 1;
-                    if (I.near_ptr[mid] <= p) lo = mid; else hi = mid - 1;
-                }
-                const int64_t i = lo, j = I.near_col[p];
+                const int64_t i = I.near_row[p], j = I.near_col[p];
                 Acc a;
                 near_pair_channels(a, nsm[warp], I.elem, I.ld, i, j, I.k, I.k * I.k, lane);
                 const Acc t = warp_reduce(a);
@@ -2546,6 +2547,16 @@ __global__ void k_sincos(const double* __restrict__ x, int64_t n, double* __rest
 // ---------------------------------------------------------------------------------------------
 static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Row of every near pair (the CSR's row index per entry), so that a near-pair kernel finds its
+// pair's row with one load instead of a search through the row pointers.
+static void set_near_rows(Mesh& m, const std::vector<int64_t>& ptr) {
+    std::vector<int32_t> row(std::max<int64_t>(m.nnz, 1), 0);
+    for (int64_t i = 0; i < m.n; ++i)
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) row[p] = static_cast<int32_t>(i);
+    m.near_row.alloc(sizeof(int32_t) * row.size());
+    h2d_sync(m.near_row.p, row.data(), sizeof(int32_t) * row.size());
+}
+
 Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, int64_t n_tris,
                   int device) {
     SB_REQUIRE(nodes && tris, SB_ERR_INVALID_ARGUMENT, "mesh: null nodes or connectivity");
@@ -2604,6 +2615,7 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
         m->nnz = ptr[m->n];
         m->near_ptr.alloc(sizeof(int64_t) * (m->n + 1));
         h2d_sync(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1));
+        set_near_rows(*m, ptr);
         m->near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m->nnz, 1));
         k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 1, nullptr, m->near_ptr.as<int64_t>(), m->near_col.as<int32_t>()); count_launch();
         SB_CUDA(cudaGetLastError());
@@ -2850,10 +2862,9 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     auto near_and_self = [&](cudaStream_t st) {
         if (m.nnz > 0) {
             ProfScope prof(SB_PROF_NEAR, st);
-            const int64_t nb = cdiv(m.nnz, kNearWarps);
-            k_near<<<nb, 32 * kNearWarps, 0, st>>>(m.elem.as<double>(), n, ld, m.near_ptr.as<int64_t>(),
-                                                   m.near_col.as<int32_t>(), m.nnz, op.coef.as<double>(), k, A64,
-                                                   A32, op.lda32, with_rhs ? op.near_rhs.as<double2>() : nullptr);
+            k_near<<<near_grid(m.nnz, op.device), 32 * kNearWarps, 0, st>>>(
+                m.elem.as<double>(), n, ld, m.near_row.as<int32_t>(), m.near_col.as<int32_t>(), m.nnz,
+                op.coef.as<double>(), k, A64, A32, op.lda32, with_rhs ? op.near_rhs.as<double2>() : nullptr);
             count_launch();
             SB_CUDA(cudaGetLastError());
         }
@@ -3133,9 +3144,9 @@ void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_
         const BatchAsmInst& I = h_inst[b];
         if (I.nnz > 0) {
             ProfScope prof(SB_PROF_NEAR, side.s);
-            k_near<<<cdiv(I.nnz, kNearWarps), 32 * kNearWarps, 0, side.s>>>(I.elem, I.n, I.ld, I.near_ptr, I.near_col,
-                                                                          I.nnz, I.coef, I.k, nullptr, I.A32, I.lda32,
-                                                                          nullptr);
+            k_near<<<near_grid(I.nnz, dev), 32 * kNearWarps, 0, side.s>>>(I.elem, I.n, I.ld, I.near_row, I.near_col,
+                                                                        I.nnz, I.coef, I.k, nullptr, I.A32, I.lda32,
+                                                                        nullptr);
             count_launch();
         }
         ProfScope prof(SB_PROF_SELF, side.s);

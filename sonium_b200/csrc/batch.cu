@@ -1371,6 +1371,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
                 A.k = B->phys[i].harmonic_factor * B->phys[i].wave_number;
                 A.near_ptr = m->near_ptr.as<int64_t>();
                 A.near_col = m->near_col.as<int32_t>();
+                A.near_row = m->near_row.as<int32_t>();
                 A.nnz = m->nnz;
                 B->asm_h.push_back(A);
                 B->rhs.push_back(reinterpret_cast<double2*>(pr));

@@ -150,7 +150,7 @@ struct Mesh {
     DevBuf nodes, tris, elem, qp, qp32;
     // near-pair CSR (superset of the reference's subdivision criterion; excludes the diagonal)
     int64_t nnz = 0;
-    DevBuf near_ptr, near_col;
+    DevBuf near_ptr, near_col, near_row;  // near_row: the row of each near pair
     // Quad4 meshes: four vertices per element (EV0..EV3), far points of the 4 x 4 rule with their
     // normals, qq[(q * 7 + f) * ld + e] for f = x, y, z, w J, nx, ny, nz.
     bool quad = false;
@@ -238,6 +238,7 @@ struct BatchAsmInst {
     double k;
     const int64_t* near_ptr;
     const int32_t* near_col;
+    const int32_t* near_row;
     int64_t nnz;
 };
 void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst* d_inst, DevBuf& pre_buf,
