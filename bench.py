@@ -29,7 +29,12 @@ solve: re-assembly of the dense system on the device, the incident right-hand si
   * `multi_rhs` -- 256 plane-wave right-hand sides of one operator (ellipsoid level 5, k = 16)
                 solved together with tensor-core block products, against plain FP64 GMRES per
                 right-hand side; carries the tensor kernel's roofline.
-  Opt-in legs: `--precision-form` (N = 81920, k = 40, ~165 GB), `--sweep-only`, `--multi-rhs`.
+  * `precision_form` -- N = 81920, k = 40 (complex128 + complex64, ~165 GB): FP64 and mixed solves
+                to 1e-10, their difference and both surface errors against the Mie series
+                (skipped with the free memory it found when the device has less).
+  * `reference_gpu_assembly` -- the reference's own CUDA pair kernel (compiled from its source) on
+                its quadrature charts, beside this library's FP64 assembly of the same system.
+  Legs alone: `--precision-form`, `--sweep-only`, `--multi-rhs`.
 
 With torchrun (N > 1 ranks) every rank solves its own copy of the workload (replicas: the path
 has no exchange step); value = all ranks' solves / max-over-ranks time.
@@ -76,6 +81,8 @@ def parse():
                     help="run only the 256-right-hand-side tensor-core leg and print its JSON")
     ap.add_argument("--rhs", type=int, default=256, help="right-hand sides of the multi-RHS leg")
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-RHS leg in the default run")
+    ap.add_argument("--no-precision-form", action="store_true",
+                    help="skip the N = 81920, k = 40 precision-form leg (~165 GB) in the default run")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the leg that times the reference's own CUDA assembly kernel beside ours")
     ap.add_argument("--precision-form", action="store_true",
@@ -199,6 +206,35 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
                 "samples": len(sm), "sm_mhz_min": min(sm), "period_ms": self.PERIOD_MS}
+
+
+def mie_rigid_surface(k: float, radius: float, theta: np.ndarray, terms: int) -> np.ndarray:
+    """Total surface pressure of a plane wave exp(i k z) on a rigid sphere (Mie series,
+    crates/sonium-wave/src/analytical/solutions_3d.rs:315-366, 769-806): sum over n of
+    (2n + 1) i^n (j_n(ka) - a_n h_n(ka)) P_n(cos theta), a_n = j_n'(ka) / h_n'(ka), h_n = j_n + i y_n."""
+    from scipy.special import eval_legendre, spherical_jn, spherical_yn
+
+    ka = k * radius
+    nn = np.arange(terms)
+    jp, yp = spherical_jn(nn, ka, derivative=True), spherical_yn(nn, ka, derivative=True)
+    j, y = spherical_jn(nn, ka), spherical_yn(nn, ka)
+    coef = (2 * nn + 1) * (1j ** nn) * (j - jp / (jp + 1j * yp) * (j + 1j * y))
+    ct_ = np.cos(theta)
+    out = np.zeros(theta.shape, complex)
+    for m in range(terms):
+        out += coef[m] * eval_legendre(m, ct_)
+    return out
+
+
+def mie_surface_error(x: np.ndarray, centers: np.ndarray, areas: np.ndarray, k: float, radius: float) -> float:
+    """Area-weighted relative L2 error of surface pressure x (element centroids) against the Mie
+    series (rigid_sphere_surface_relative_l2_error, crates/sonium-qa/src/lib.rs:319-358; terms
+    max(4 ceil(ka) + 16, 17) as suggested_sphere_terms, solutions_3d.rs:241-249)."""
+    ka = k * radius
+    terms = max(int(np.ceil(ka)) * 4 + 16, 17)
+    theta = np.arccos(np.clip(centers[:, 2] / np.linalg.norm(centers, axis=1), -1.0, 1.0))
+    ref = mie_rigid_surface(k, radius, theta, terms)
+    return float(np.sqrt(np.sum(areas * np.abs(x - ref) ** 2) / np.sum(areas * np.abs(ref) ** 2)))
 
 
 def peaks():
@@ -504,6 +540,8 @@ def main():
         a.level = lvl
 
     extra_legs = {}
+    if not a.no_precision_form:
+        extra_legs["precision_form"] = precision_leg(sb, a, dist, dev, rt, reps=1)
     if not a.no_ref_gpu:
         extra_legs["reference_gpu_assembly"] = reference_gpu_leg(sb, L, lib, dev)
 
@@ -639,6 +677,12 @@ def main():
     summ["far32_ms"] = round(far_avg * 1e3, 3)
     if cpu is not None:
         summ["cpu_solves_per_s"] = float("%.4g" % cpu["value"])
+    pf = extra_legs.get("precision_form") or {}
+    if "mixed_error_vs_fp64" in pf:
+        summ["precision_form"] = {"mixed_error_vs_fp64": float("%.3g" % pf["mixed_error_vs_fp64"]),
+                                  "mie_fp64": float("%.4g" % pf["mie_surface_error"]["fp64"]),
+                                  "mie_mixed": float("%.4g" % pf["mie_surface_error"]["mixed"]),
+                                  "solve_speedup": round(pf["solve_speedup"], 2)}
     rg = extra_legs.get("reference_gpu_assembly") or {}
     if "N1280_k2_all_pairs" in rg:
         summ["reference_gpu_assembly_speedup_per_pair"] = {
@@ -964,14 +1008,27 @@ def multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b
     }
 
 
-def precision_leg(sb, a, dist, dev, rt):
+def precision_leg(sb, a, dist, dev, rt, reps=None):
     """Precision form: rigid sphere, icosphere level 6 (N = 81920), k = 40, plane wave +z.
 
     The complex128 matrix (107 GB) and its complex64 copy (54 GB) come from one assembly; a step
     solves to rtol 1e-10 once in plain FP64 GMRES(50) and once with FP32-inner GMRES(50) to 1e-5 and
     FP64 refinement on the complex128 matrix. Device times from the solver statistics (CUDA events
-    on the operator's stream); error of the mixed solution against the FP64 one."""
+    on the operator's stream); error of the mixed solution against the FP64 one, and both
+    solutions' surface error against the Mie series (mie_surface_error)."""
+    reps = a.steps if reps is None else reps
+    from sonium_b200 import _lib as L
+
     level, k = 6, 40.0
+    import gc
+
+    gc.collect()
+    L.check(L.load().sb_memory_trim(-1))  # cached blocks of the other legs back to the driver
+    free, total = ct.c_size_t(), ct.c_size_t()
+    rt.cudaMemGetInfo.argtypes = [ct.POINTER(ct.c_size_t), ct.POINTER(ct.c_size_t)]
+    rt.cudaMemGetInfo(ct.byref(free), ct.byref(total))
+    if free.value < 170e9:
+        return {"unavailable": f"needs ~170 GB of free device memory, {free.value / 1e9:.1f} GB free"}
     nodes, tris = sb.icosphere(RADIUS, level)
     n = tris.shape[0]
     mesh = sb.Mesh(nodes, tris, device=dev)
@@ -985,17 +1042,22 @@ def precision_leg(sb, a, dist, dev, rt):
                      inner_tolerance=1e-5)
     t64, tmix = [], []
     s64 = mix = None
-    for i in range(max(1, a.steps)):
+    for i in range(max(1, reps)):
         s64 = sb.gmres(op, b, gc)
         mix = sb.gmres_mixed(op, b, ir)
         t64.append(s64.device_ms)
         tmix.append(mix.device_ms)
+    c, _, areas = mesh.element_geometry()
     op.close()
     mesh.close()
+    L.check(L.load().sb_memory_trim(-1))
     err = float(np.linalg.norm(mix.x - s64.x) / np.linalg.norm(s64.x))
+    e64 = mie_surface_error(s64.x, c, areas, k, RADIUS)
+    emix = mie_surface_error(mix.x, c, areas, k, RADIUS)
     return {
         "workload": f"rigid sphere icosphere L{level} (N={n}), k={k}, complex128 + complex64 matrices "
                     f"({16 * n * n / 1e9:.0f} + {8 * n * n / 1e9:.0f} GB), rtol 1e-10",
+        "mie_surface_error": {"fp64": e64, "mixed": emix, "difference": abs(emix - e64)},
         "assembly_ms": asm_ms,
         "fp64_solve_ms": float(np.median(t64)), "mixed_solve_ms": float(np.median(tmix)),
         "solve_speedup": float(np.median(t64) / np.median(tmix)),
