@@ -36,8 +36,10 @@ solve: re-assembly of the dense system on the device, the incident right-hand si
                 its quadrature charts, beside this library's FP64 assembly of the same system.
   Legs alone: `--precision-form`, `--sweep-only`, `--multi-rhs`.
 
-With torchrun (N > 1 ranks) every rank solves its own copy of the workload (replicas: the path
-has no exchange step); value = all ranks' solves / max-over-ranks time.
+With torchrun (N > 1 ranks): the single-solve headline runs one replica per rank (a solve has no
+exchange step to split); value = all ranks' solves / max-over-ranks time. The sweep shares its 64
+instances out over the ranks (balanced by N^2) and the multi-RHS leg its groups of 128
+right-hand sides (sonium_b200/shard.py): all instances / the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -769,7 +771,15 @@ def sweep_leg(sb, a, dist, dev, rt):
     maximum."""
     from sonium_b200.sweep import SweepBatch, build_ellipsoid_sweep, ellipsoid_sweep_plan
 
+    from sonium_b200 import shard
+
     plan = ellipsoid_sweep_plan(count=a.sweep_count)
+    # With several ranks each solves its share of the instances (balanced by N^2, no exchange
+    # until the end); the whole job's rate is all instances over the slowest rank's time.
+    levels_all = [p[2] for p in plan]
+    mine = shard.partition_by_cost(shard.dense_solve_costs([20 * 4 ** lv for lv in levels_all]),
+                                   dist.world)[dist.rank]
+    plan_all, plan = plan, [plan[i] for i in mine]
     meshes, physics, betas = build_ellipsoid_sweep(plan, device=dev)
     sizes = [m.num_elements for m in meshes]
     cfg = sb.IrConfig(20, TOL, RESTART, 20, 1e-5)
@@ -833,23 +843,24 @@ def sweep_leg(sb, a, dist, dev, rt):
     t_fp64_bj, sols_bj = wall(lambda: fp64_sweep(True))
     fp64_iters = [int(s.iterations) for s in sols]
     fp64_bj_iters = [int(s.iterations) for s in sols_bj]
-    bj_err = max(float(np.linalg.norm(sb_.x - s.x) / np.linalg.norm(s.x)) for sb_, s in zip(sols_bj, sols))
+    bj_err = dist.max(max(float(np.linalg.norm(sb_.x - s.x) / np.linalg.norm(s.x)) for sb_, s in zip(sols_bj, sols)))
     for f in forms.values():
         f["errs"] = [float(np.linalg.norm(f["xb"][i] - s.x) / np.linalg.norm(s.x)) for i, s in enumerate(sols)]
-        f["value"] = dist.world * len(sols) * a.steps / f["t"]
+        f["max_err"] = dist.max(max(f["errs"]))  # over every rank's instances
+        f["value"] = len(plan_all) * a.steps / f["t"]
     for o in ops.values():
         o.close()
-    plain = dist.world * len(sols) / t_fp64
-    plain_bj = dist.world * len(sols_bj) / t_fp64_bj
+    plain = len(plan_all) / t_fp64
+    plain_bj = len(plan_all) / t_fp64_bj
     # the fastest form within the metric's 1e-5 of the FP64 solutions
-    ok = [k for k, f in forms.items() if max(f["errs"]) <= 1e-5]
+    ok = [k for k, f in forms.items() if f["max_err"] <= 1e-5]
     best = max(ok, key=lambda k: forms[k]["value"]) if ok else "fp32_inner"
     fb = forms[best]
     batched, t_batch, st0, errs = fb["value"], fb["t"], fb["st0"], fb["errs"]
     asm_ms, solve_ms = fb["assembly_ms"], fb["solve_ms"]
-    levels = [p[2] for p in plan]
+    levels = levels_all
     return {
-        "workload": (f"{len(plan)} instances, ka log-spaced {plan[0][0]:g} -> {plan[-1][0]:g} on the ellipsoid "
+        "workload": (f"{len(plan_all)} instances, ka log-spaced {plan_all[0][0]:g} -> {plan_all[-1][0]:g} on the ellipsoid "
                      "(1, 0.6, 0.4), icosphere level per instance for >= 8 elements per wavelength "
                      f"(levels {min(levels)}-{max(levels)}: " +
                      ", ".join(f"L{lv} x{levels.count(lv)}" for lv in sorted(set(levels))) +
@@ -860,7 +871,7 @@ def sweep_leg(sb, a, dist, dev, rt):
         "plain_fp64_bj": plain_bj, "plain_fp64_bj_ms_per_sweep": 1e3 * t_fp64_bj,
         "speedup_vs_plain_fp64_bj": batched / plain_bj,
         "plain_fp64_bj_max_error_vs_fp64": bj_err,
-        "max_error_vs_fp64": max(errs), "median_error_vs_fp64": float(np.median(errs)),
+        "max_error_vs_fp64": fb["max_err"], "median_error_vs_fp64_this_rank": float(np.median(errs)),
         "all_converged": bool(all(s.converged for s in st0)),
         "max_residual": float(max(s.residual for s in st0)),
         "matrix_gb_c64": float(sum(8.0 * n * n for n in sizes) / 1e9),
@@ -871,7 +882,7 @@ def sweep_leg(sb, a, dist, dev, rt):
                              "fp64_bj": int(sum(fp64_bj_iters))},
         "inner_form": best,
         "forms": {k: {"value": f["value"], "ms_per_step": 1e3 * f["t"] / a.steps, "assembly_ms": f["assembly_ms"],
-                      "solve_ms": f["solve_ms"], "max_error_vs_fp64": max(f["errs"]),
+                      "solve_ms": f["solve_ms"], "max_error_vs_fp64": f["max_err"],
                       "speedup_vs_plain_fp64": f["value"] / plain,
                       "speedup_vs_plain_fp64_bj": f["value"] / plain_bj,
                       "inner_tolerance": cfg.inner_tolerance if k == "fp32_inner" else cfg16.inner_tolerance,
@@ -879,6 +890,10 @@ def sweep_leg(sb, a, dist, dev, rt):
                       "iterations_total": int(sum(s.iterations for s in f["st0"]))}
                   for k, f in forms.items()},
         "timing": "wall clock around device-synchronised steps, max over ranks",
+        "ranks": dist.world,
+        "scaling": "strong: the instances are shared out over the ranks (balanced by N^2), solutions gathered "
+                   "at the end" if dist.world > 1 else "one rank",
+        "instances_this_rank": len(plan),
     }
 
 
@@ -902,6 +917,14 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
     beta = ph.burton_miller_beta()
     op = sb.build_tbem_system_with_beta(mesh, ph, beta, sb.SB_PRECISION_FP64)
     B = sb.rhs_plane_wave(mesh, ph, beta, sb.fibonacci_sphere_directions(r))  # n x r
+    # With several ranks each solves its groups of 128 right-hand sides (no exchange); the whole
+    # job's rate is all right-hand sides over the slowest rank's time.
+    from sonium_b200 import shard
+
+    r_total = r
+    cols = [c for start, stop in shard.rhs_groups(r, dist.world)[dist.rank] for c in range(start, stop)]
+    B = np.ascontiguousarray(B[:, cols])
+    r = len(cols)
     lib = L.load()
     bt = np.ascontiguousarray(B.T)  # right-hand-side-major
     b_d = _dev_alloc(rt, bt.nbytes)
@@ -923,7 +946,7 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
     for _ in range(a.warmup):
         solve()
     times = [solve() for _ in range(a.steps)]
-    t_block = float(np.median(times)) / 1e3
+    t_block = dist.max(float(np.median(times)) / 1e3)
     # The block product alone, for its roofline: K launches on the operator's stream between two
     # CUDA events (all 256 right-hand sides, inputs resident, split planes 3.4 GB > L2).
     x32 = np.ascontiguousarray(bt.astype(np.complex64))
@@ -954,7 +977,14 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
         solve()
     L.check(lib.sb_profile_enable(0))
     L.check(lib.sb_profile_read(ct.byref(prof), 1))
-    return multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b_d, x_d, n, r, level, k)
+    out = multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b_d, x_d, n, r, level, k)
+    out["rhs_solves_per_s"] = r_total / t_block
+    out["speedup_vs_plain_fp64"] = out["rhs_solves_per_s"] / out["plain_fp64_rhs_solves_per_s"]
+    out["ranks"] = dist.world
+    out["rhs_this_rank"] = r
+    if dist.world > 1:
+        out["scaling"] = "strong: groups of 128 right-hand sides shared out over the ranks"
+    return out
 
 
 def multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b_d, x_d, n, r, level, k):
