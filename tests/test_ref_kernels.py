@@ -86,12 +86,13 @@ def test_reference_kernel_matches_oracle_pairs(oracle, refk, level, k, scale):
     selfm = np.array([i == j for i, j in ij])
     nearm = (counts > 13) & ~selfm
     assert nearm.any() and (~nearm & ~selfm).any()  # far and subdivided near pairs both present
-    # relative per entry, with a floor of 1e-6 of the pair's largest channel for channels that
-    # vanish up to rounding (H and H^T of a flat self element: r.n_y = 0 in the element's plane)
+    # relative per entry, with a floor of a fraction of the pair's largest channel for channels
+    # that vanish up to rounding (H and H^T of a flat self element: r.n_y = 0 in the element's
+    # plane, so both sums are rounding noise of the G-sized terms)
     pair_scale = np.abs(ref).max(axis=1)
-    for m, tol_e in ((~selfm, 1e-12), (selfm, 1e-11)):
+    for m, tol_e, floor in ((~selfm, 1e-12, 1e-6), (selfm, 1e-11, 1e-4)):
         for c in range(4):
-            d = np.abs(ch[m, c] - ref[m, c]) / np.maximum(np.abs(ref[m, c]), 1e-6 * pair_scale[m])
+            d = np.abs(ch[m, c] - ref[m, c]) / np.maximum(np.abs(ref[m, c]), floor * pair_scale[m])
             tol = tol_e if c == 3 else 1e-12
             assert d.max() < tol, (c, float(d.max()))
 
