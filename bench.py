@@ -903,9 +903,9 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
 
     A step = one sb_gmres_multi_device solve of all 256 right-hand sides (device-resident b and x):
     FP32-inner GMRES(50) with every step's 256 products as one tensor-core block product (BF16
-    hi/lo split, FP32 accumulation) and FP64 refinement to rtol 1e-8 by one complex128 GEMM per
-    refinement. Device time from the solver (CUDA events on its stream). Baseline: plain FP64
-    GMRES(50) to 1e-8, one right-hand side after another, timed on a sample of 16 directions and
+    hi/lo split, FP32 accumulation) and FP64 refinement to rtol 1e-8 by one integer-slice block
+    residual (INT8 tensor cores, FP64-grade) per refinement. Device time from the solver (CUDA
+    events on its stream). Baseline: plain FP64 GMRES(50) to 1e-8, one right-hand side after another, timed on a sample of 16 directions and
     reported per right-hand side; the error of the multi-RHS solutions against those FP64 solutions."""
     from sonium_b200 import _lib as L
 
@@ -965,11 +965,28 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
     L.check(lib.sb_event_record(e1, op.handle))
     ems = ct.c_float()
     L.check(lib.sb_event_elapsed_ms(e0, e1, ct.byref(ems)))
-    lib.sb_event_destroy(e0)
-    lib.sb_event_destroy(e1)
     rt.cudaFree(x32_d)
     rt.cudaFree(y32_d)
     live = (ems.value / reps, reps)
+    # The FP64-grade block residual alone (integer slices on the INT8 tensor cores), for its
+    # roofline: the same event bracket around back-to-back residuals of all right-hand sides.
+    res_d = _dev_alloc(rt, bt.nbytes)
+    for _ in range(2):
+        L.check(lib.sb_operator_block_residual_device(op.handle, b_d, x_d, r, res_d))
+    rreps = max(a.steps, 3) * 2
+    L.check(lib.sb_event_record(e0, op.handle))
+    for _ in range(rreps):
+        L.check(lib.sb_operator_block_residual_device(op.handle, b_d, x_d, r, res_d))
+    L.check(lib.sb_event_record(e1, op.handle))
+    L.check(lib.sb_event_elapsed_ms(e0, e1, ct.byref(ems)))
+    R = np.zeros((r, n), np.complex128)
+    Xr = np.zeros((r, n), np.complex128)
+    rt.cudaMemcpy(R.ctypes.data, res_d, R.nbytes, 2)
+    rt.cudaMemcpy(Xr.ctypes.data, x_d, Xr.nbytes, 2)
+    rt.cudaFree(res_d)
+    live_res = (ems.value / rreps, rreps, R, Xr)
+    lib.sb_event_destroy(e0)
+    lib.sb_event_destroy(e1)
     # all kernel classes from a separate profiled pass (their event pairs stay out of the timed solves)
     prof = L.SbProfile()
     L.check(lib.sb_profile_enable(1))
@@ -977,7 +994,8 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
         solve()
     L.check(lib.sb_profile_enable(0))
     L.check(lib.sb_profile_read(ct.byref(prof), 1))
-    out = multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b_d, x_d, n, r, level, k)
+    out = multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b_d, x_d, n, r, level, k,
+                           live_res)
     out["rhs_solves_per_s"] = r_total / t_block
     out["speedup_vs_plain_fp64"] = out["rhs_solves_per_s"] / out["plain_fp64_rhs_solves_per_s"]
     out["ranks"] = dist.world
@@ -987,9 +1005,20 @@ def multi_rhs_leg(sb, a, dist, dev, rt):
     return out
 
 
-def multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b_d, x_d, n, r, level, k):
-    """FP64 baseline on a sample of right-hand sides and the tensor-kernel roofline of the leg."""
+def multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b_d, x_d, n, r, level, k,
+                     live_res):
+    """FP64 baseline on a sample of right-hand sides and the tensor-kernel rooflines of the leg."""
     sample = list(range(0, r, max(1, r // 16)))[:16]
+    # the block residual of the solutions against numpy's FP64 residual on the same sample
+    A = op.matrix
+    absA = np.abs(A)
+    res_err = 0.0
+    for c in sample:
+        xr = live_res[3][c]
+        ref = B[:, c] - A @ xr
+        scale = absA @ np.abs(xr) + np.abs(B[:, c])
+        res_err = max(res_err, float(np.max(np.abs(live_res[2][c] - ref) / scale)))
+    del A, absA
     gc = sb.GmresConfig(100, RESTART, TOL)
     rt.cudaDeviceSynchronize()
     t0 = time.perf_counter()
@@ -1034,8 +1063,31 @@ def multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b
                           "peak_source": pk_kind, "executed_flop_per_launch": executed,
                           "algorithmic_complex_flop_per_launch": algorithmic,
                           "share_of_kernel_time": ms["tensor"] / max(sum(ms.values()), 1e-9)},
+        "residual_kernel": residual_roofline(n, r, live_res, pk, pk_kind, ms, launches, a.steps, res_err),
         "kernel_ms_per_solve": {kk: v / max(a.steps, 1) for kk, v in ms.items() if v > 0},
     }
+
+
+OZAKI_PRODUCTS = 36  # slice products of the block residual: diagonals 2..9 of 8 x 8 INT8 slices
+
+
+def residual_roofline(n, r, live_res, pk, pk_kind, ms, launches, steps, res_err):
+    """Roofline of the integer-slice block residual (k_ozaki_residual with its slicing and combine
+    kernels): INT8 tensor work = 36 slice products of the real 2N x 2R x N GEMM per launch; peak =
+    2 x the measured BF16 GEMM rate (the INT8 tensor rate per SM and clock is twice the BF16 one)."""
+    avg_s = live_res[0] / 1e3
+    ops = OZAKI_PRODUCTS * 2.0 * (2 * n) * (2 * r) * n
+    achieved = ops / max(avg_s, 1e-12) / 1e12
+    peak = 2.0 * pk["bf16_tflops"]
+    return {"kernel": "k_ozaki_residual (tcgen05 kind::i8, 8 INT8 slices, 36 products, TMA, TMEM) + slicing + combine",
+            "avg_launch_ms": live_res[0], "measured": f"{live_res[1]} back-to-back residuals of all {r} right-hand "
+                                                      "sides between CUDA events on the operator's stream",
+            "bound": "tensor", "achieved": achieved, "unit": "TOP/s (INT8)", "peak": peak,
+            "frac": achieved / peak, "peak_source": f"2 x {pk_kind} bf16 GEMM", "int8_ops_per_launch": ops,
+            "fp64_equivalent_tflops": 8.0 * n * n * r / max(avg_s, 1e-12) / 1e12,
+            "launches_per_solve": launches["residual"] / max(steps, 1),
+            "share_of_kernel_time": ms["residual"] / max(sum(ms.values()), 1e-9),
+            "max_error_vs_numpy_fp64": res_err}
 
 
 def precision_leg(sb, a, dist, dev, rt, reps=None):

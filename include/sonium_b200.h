@@ -407,6 +407,23 @@ SB_API int sb_operator_apply_block_tensor(const sb_operator* op, const sb_comple
 SB_API int sb_operator_apply_block_tensor_device(const sb_operator* op, const sb_complex32* x_dev,
                                                  sb_complex32* y_dev, int64_t r);
 
+/* ---- FP64-grade block residual ----
+ * R = B - A X for r right-hand sides on the operator's complex128 matrix: the block residual of
+ * block GMRES (crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:829 and
+ * block_true_metrics :571-620, one FP64 complex GEMM there) on the INT8 tensor cores. Every row
+ * of A and every vector is split into 8 signed 8-bit slices of a power-of-two scale (exact to
+ * 2^-56 of the scale); the slice products are exact in INT32 and summed by diagonal in FP64, 36
+ * of the 64 kept: per term an error below 9.05 * 2^-56 of (row scale x vector scale), the size of
+ * an FP64 rounding of a term near the largest entries (not bit-identical to an FP64 GEMM). The
+ * operator must hold the complex128 matrix; its slices (8 x 2 N^2 bytes) are built on first use
+ * and dropped by re-assembly. Host variant: b, x, res n x r row-major (b[i * r + c]). */
+SB_API int sb_operator_block_residual(const sb_operator* op, const sb_complex* b, const sb_complex* x, int64_t r,
+                                      sb_complex* res);
+/* Device-resident variant: vector c at + c * n (complex128), on the operator's device; complete on
+ * return. */
+SB_API int sb_operator_block_residual_device(const sb_operator* op, const sb_complex* b_dev, const sb_complex* x_dev,
+                                             int64_t r, sb_complex* res_dev);
+
 /* Many right-hand sides of one operator (the role of block_gmres_preconditioned,
  * crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:163, called via
  * solve_compressed_many, bem_solver.rs:4072-4110): r systems A x_c = b_c solved in lockstep by
@@ -414,8 +431,8 @@ SB_API int sb_operator_apply_block_tensor_device(const sb_operator* op, const sb
  * convergence state (the reference's block method shares one basis across right-hand sides; this
  * one shares the products instead). Each step's products for all right-hand sides are one
  * tensor-core block product (the BF16 split of sb_operator_apply_block_tensor); the refinement
- * residual of all of them is one complex128 GEMM on the FP64 matrix, so the operator must hold it
- * (SB_PRECISION_FP64 or SB_PRECISION_FP64_FP32). The split planes are built on first use. b and
+ * residual of all of them is one sb_operator_block_residual on the complex128 matrix, so the
+ * operator must hold it (SB_PRECISION_FP64 or SB_PRECISION_FP64_FP32). The split planes are built on first use. b and
  * x: n x r row-major (b[i * r + c], the reference's DenseMatrix block layout); stats: r entries,
  * the sb_gmres_mixed statistics per right-hand side (device_ms = the whole block's time). */
 SB_API int sb_gmres_multi(const sb_operator* op, const sb_complex* b, int64_t r, const sb_ir_config* cfg,
@@ -501,7 +518,8 @@ SB_API int sb_memory_stats(int device, int64_t* in_use_bytes, int64_t* cached_by
 #define SB_PROF_OTHER 6      /* geometry, coefficients, RHS reductions, plane waves */
 #define SB_PROF_TENSOR 7     /* tensor-core block product (BF16 split, tcgen05) */
 #define SB_PROF_GEMV16 8     /* complex-half matvec of the FP16 inner solve (incl. its copy) */
-#define SB_PROF_KINDS 9
+#define SB_PROF_RESIDUAL 9   /* integer-slice FP64 block residual (INT8 slices, tcgen05 kind::i8) */
+#define SB_PROF_KINDS 10
 typedef struct sb_profile {
     double ms[SB_PROF_KINDS];
     int64_t launches[SB_PROF_KINDS];

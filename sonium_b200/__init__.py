@@ -14,7 +14,7 @@ from .tbem import (BlockJacobiPreconditioner, DenseMatrixOperator, GcroDrConfig,
                    GmresConfig, GmresSolution, IrConfig, JacobiPreconditioner, LinearOperator, Mesh,
                    PhysicsParams, TbemOperator, build_tbem_system, build_tbem_system_with_beta,
                    compute_scattered_field, compute_total_field, device_count,
-                   fibonacci_sphere_directions, gmres, gmres_mixed, gmres_multi, icosphere,
+                   block_residual, fibonacci_sphere_directions, gmres, gmres_mixed, gmres_multi, icosphere,
                    inject_failure, rhs_plane_wave)
 from .sweep import (FrequencySweepConfig, FrequencySweepResult, SweepBatch, frequency_sweep,
                     frequency_sweep_batched)
@@ -23,7 +23,7 @@ __all__ = [
     "GmresConfig", "GmresSolution", "IrConfig", "JacobiPreconditioner", "LinearOperator", "Mesh",
     "PhysicsParams", "TbemOperator", "build_tbem_system", "build_tbem_system_with_beta", "device_count",
     "gmres", "gmres_mixed", "icosphere", "inject_failure", "rhs_plane_wave", "SoniumError",
-    "FrequencySweepConfig", "FrequencySweepResult", "SweepBatch", "frequency_sweep", "frequency_sweep_batched", "gmres_multi", "fibonacci_sphere_directions",
+    "FrequencySweepConfig", "FrequencySweepResult", "SweepBatch", "frequency_sweep", "frequency_sweep_batched", "gmres_multi", "block_residual", "fibonacci_sphere_directions",
     "compute_scattered_field", "compute_total_field",
     "DenseMatrixOperator", "GcroDrConfig", "GcroDrSubspace", "gcro_dr", "build_tbem_system_linear",
     "rhs_plane_wave_at", "SB_BASIS_CONSTANT", "SB_BASIS_LINEAR", "SB_BASIS_QUADRATIC",

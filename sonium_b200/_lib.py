@@ -92,9 +92,9 @@ class SbGmresStats(ct.Structure):
 
 
 (SB_PROF_FAR, SB_PROF_NEAR, SB_PROF_SELF, SB_PROF_GEMV64, SB_PROF_GEMV32, SB_PROF_ARNOLDI, SB_PROF_OTHER,
- SB_PROF_TENSOR, SB_PROF_GEMV16) = range(9)
-SB_PROF_KINDS = 9
-PROF_NAMES = ["far", "near", "self", "gemv64", "gemv32", "arnoldi", "other", "tensor", "gemv16"]
+ SB_PROF_TENSOR, SB_PROF_GEMV16, SB_PROF_RESIDUAL) = range(10)
+SB_PROF_KINDS = 10
+PROF_NAMES = ["far", "near", "self", "gemv64", "gemv32", "arnoldi", "other", "tensor", "gemv16", "residual"]
 
 
 class SbProfile(ct.Structure):
@@ -166,6 +166,8 @@ _SIGNATURES = {
     "sb_operator_prepare_block_tensor": ([P], ct.c_int),
     "sb_operator_apply_block_tensor": ([P, P, P, ct.c_int64], ct.c_int),
     "sb_operator_apply_block_tensor_device": ([P, P, P, ct.c_int64], ct.c_int),
+    "sb_operator_block_residual": ([P, P, P, ct.c_int64, P], ct.c_int),
+    "sb_operator_block_residual_device": ([P, P, P, ct.c_int64, P], ct.c_int),
     "sb_gmres_multi": ([P, P, ct.c_int64, ct.POINTER(SbIrConfig), P, P], ct.c_int),
     "sb_gmres_multi_device": ([P, P, ct.c_int64, ct.POINTER(SbIrConfig), P, P], ct.c_int),
     "sb_batch_create": ([ct.c_int64, P, P, P, ct.POINTER(P)], ct.c_int),

@@ -72,7 +72,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(compile_one, _sources()))
     tmp = LIB + ".tmp"
-    cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcublas", "-lcudart"]
+    cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

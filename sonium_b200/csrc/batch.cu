@@ -16,11 +16,11 @@
 // The same machinery solves many right-hand sides of ONE operator (sb_gmres_multi): the
 // instances are the right-hand sides, every vector family is stored right-hand-side-major so a
 // step's products for all of them are one block product on the tensor cores (tensor.cu: BF16
-// hi/lo split, FP32 accumulation), and the FP64 refinement residual of all of them is one complex128
-// GEMM (cuBLAS ZGEMM) on the FP64 matrix. Each right-hand side keeps its own Krylov basis and
+// hi/lo split, FP32 accumulation), and the FP64 refinement residual of all of them is one
+// integer-slice block residual on the complex128 matrix (ozaki.cu: INT8 slices, exact INT32
+// accumulation on the tensor cores, FP64-grade). Each right-hand side keeps its own Krylov basis and
 // convergence state (the reference's block_gmres, block_gmres.rs:163, shares one basis instead).
 
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cstring>
@@ -526,9 +526,9 @@ struct Batch {
     int64_t m = 0;  // Krylov dimension the workspace was sized for
     std::vector<int64_t> nvec;  // unknowns per instance
     // Many right-hand sides of one operator: products through `shared` (tensor-core block product
-    // for the inner solves, ZGEMM for the FP64 residual); vectors stored right-hand-side-major.
+    // for the inner solves, the integer-slice block residual for the FP64 one); vectors stored
+    // right-hand-side-major.
     Operator* shared = nullptr;
-    cublasHandle_t blas = nullptr;
     float2 *w_all = nullptr, *d_all = nullptr, *v_all = nullptr;
     double2 *x_all = nullptr, *r_all = nullptr, *b_all = nullptr;
     int64_t ld_all = 0;
@@ -591,7 +591,6 @@ struct Batch {
         for (cudaEvent_t& e : ev)
             if (e) cudaEventDestroy(e);
         side.release();
-        if (blas) cublasDestroy(blas);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -992,20 +991,11 @@ static void batch_cycle(Batch& B) {
     }
 }
 
-// r = b - A x for every right-hand side of a shared operator: one complex128 GEMM on the FP64
-// matrix (row-major A is the transpose of the column-major view cuBLAS takes).
+// r = b - A x for every right-hand side of a shared operator: the integer-slice block residual on
+// the complex128 matrix (FP64-grade, INT8 tensor cores; ozaki.cu).
 static void shared_residual64(Batch& B) {
     const Operator& op = *B.shared;
-    const int64_t n = op.n, ld = B.ld_all;
-    SB_CUDA(cudaMemcpyAsync(B.r_all, B.b_all, sizeof(double2) * B.ninst * ld, cudaMemcpyDeviceToDevice, B.stream));
-    ProfScope prof(SB_PROF_GEMV64, B.stream);
-    const cuDoubleComplex alpha = make_cuDoubleComplex(-1.0, 0.0), beta = make_cuDoubleComplex(1.0, 0.0);
-    const cublasStatus_t st = cublasZgemm(B.blas, CUBLAS_OP_T, CUBLAS_OP_N, static_cast<int>(n), B.ninst,
-                                          static_cast<int>(n), &alpha,
-                                          reinterpret_cast<const cuDoubleComplex*>(op.A64.p), static_cast<int>(n),
-                                          reinterpret_cast<const cuDoubleComplex*>(B.x_all), static_cast<int>(ld),
-                                          &beta, reinterpret_cast<cuDoubleComplex*>(B.r_all), static_cast<int>(ld));
-    SB_REQUIRE(st == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasZgemm failed (FP64 residual of the block)");
+    ozaki_residual(op, B.b_all, B.ld_all, B.x_all, B.ld_all, B.ninst, B.r_all, B.ld_all, B.stream);
 }
 
 // Mixed-precision iterative refinement of every instance in lockstep (gmres_mixed_ir semantics
@@ -1243,8 +1233,6 @@ static Batch& multi_batch(Operator& op, int r) {
     B->nvec.assign(r, op.n);
     B->ld_all = (op.n + 1) / 2 * 2;
     SB_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
-    SB_REQUIRE(cublasCreate(&B->blas) == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasCreate failed");
-    SB_REQUIRE(cublasSetStream(B->blas, B->stream) == CUBLAS_STATUS_SUCCESS, SB_ERR_CUDA, "cublasSetStream failed");
     B->gate.alloc(sizeof(int) * cdiv64(r, kTensorRhsTile));
     B->pool_rhs.alloc(sizeof(double2) * r * B->ld_all);
     memset_sync(B->pool_rhs.p, 0, sizeof(double2) * r * B->ld_all);
@@ -1277,6 +1265,8 @@ void multi_solve_device(Operator& op, const double2* b, int64_t ldb, int r, doub
     batch_solve(B, cfg, stats);
     SB_REQUIRE(tensor_status(op, true) == 0, SB_ERR_DEVICE_CHECK,
                "multi-RHS solve: a pipeline wait of the tensor-core kernel timed out");
+    SB_REQUIRE(ozaki_status(op, true) == 0, SB_ERR_DEVICE_CHECK,
+               "multi-RHS solve: a pipeline wait of the block-residual kernel timed out");
     SB_CUDA(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, B.x_all, sizeof(double2) * B.ld_all, sizeof(double2) * op.n,
                               r, cudaMemcpyDeviceToDevice, B.stream));
     SB_CUDA(cudaStreamSynchronize(B.stream));

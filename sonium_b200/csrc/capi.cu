@@ -813,6 +813,58 @@ SB_API int sb_operator_apply_block_tensor_device(const sb_operator* op, const sb
     });
 }
 
+SB_API int sb_operator_block_residual(const sb_operator* op, const sb_complex* b, const sb_complex* x, int64_t r,
+                                      sb_complex* res) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && b && x && res && r >= 1, SB_ERR_INVALID_ARGUMENT, "bad argument");
+        SB_REQUIRE(r <= 65536, SB_ERR_INVALID_ARGUMENT, "block_residual: at most 65536 vectors");
+        Operator& o = *op->op;
+        SB_REQUIRE(o.A64.p, SB_ERR_INVALID_ARGUMENT,
+                   "block_residual: needs the complex128 matrix (SB_PRECISION_FP64 or SB_PRECISION_FP64_FP32)");
+        const int64_t n = o.n;
+        SB_CUDA(cudaSetDevice(o.device));
+        maybe_inject(SB_INJECT_LAUNCH);
+        // n x r row-major blocks (the reference's DenseMatrix layout) <-> vector-major device copies
+        std::vector<sb_complex> t(n * r), u(n * r);
+        DevBuf db, dx, dr;
+        db.alloc(sizeof(double2) * n * r);
+        dx.alloc(sizeof(double2) * n * r);
+        dr.alloc(sizeof(double2) * n * r);
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t c = 0; c < r; ++c) {
+                t[c * n + i] = b[i * r + c];
+                u[c * n + i] = x[i * r + c];
+            }
+        SB_CUDA(cudaMemcpyAsync(db.p, t.data(), sizeof(double2) * n * r, cudaMemcpyHostToDevice, o.stream));
+        SB_CUDA(cudaMemcpyAsync(dx.p, u.data(), sizeof(double2) * n * r, cudaMemcpyHostToDevice, o.stream));
+        ozaki_residual(o, db.as<double2>(), n, dx.as<double2>(), n, static_cast<int>(r), dr.as<double2>(), n, o.stream);
+        SB_CUDA(cudaMemcpyAsync(t.data(), dr.p, sizeof(double2) * n * r, cudaMemcpyDeviceToHost, o.stream));
+        SB_CUDA(cudaStreamSynchronize(o.stream));
+        SB_REQUIRE(ozaki_status(o, true) == 0, SB_ERR_DEVICE_CHECK,
+                   "block_residual: a pipeline wait of the block-residual kernel timed out");
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t c = 0; c < r; ++c) res[i * r + c] = t[c * n + i];
+    });
+}
+
+SB_API int sb_operator_block_residual_device(const sb_operator* op, const sb_complex* b_dev, const sb_complex* x_dev,
+                                             int64_t r, sb_complex* res_dev) {
+    return guarded([&] {
+        SB_REQUIRE(op && op->op && b_dev && x_dev && res_dev && r >= 1, SB_ERR_INVALID_ARGUMENT, "bad argument");
+        SB_REQUIRE(r <= 65536, SB_ERR_INVALID_ARGUMENT, "block_residual: at most 65536 vectors");
+        Operator& o = *op->op;
+        SB_REQUIRE(o.A64.p, SB_ERR_INVALID_ARGUMENT,
+                   "block_residual: needs the complex128 matrix (SB_PRECISION_FP64 or SB_PRECISION_FP64_FP32)");
+        SB_CUDA(cudaSetDevice(o.device));
+        maybe_inject(SB_INJECT_LAUNCH);
+        ozaki_residual(o, reinterpret_cast<const double2*>(b_dev), o.n, reinterpret_cast<const double2*>(x_dev), o.n,
+                       static_cast<int>(r), reinterpret_cast<double2*>(res_dev), o.n, o.stream);
+        SB_CUDA(cudaStreamSynchronize(o.stream));
+        SB_REQUIRE(ozaki_status(o, true) == 0, SB_ERR_DEVICE_CHECK,
+                   "block_residual: a pipeline wait of the block-residual kernel timed out");
+    });
+}
+
 SB_API int sb_gmres_multi(const sb_operator* op, const sb_complex* b, int64_t r, const sb_ir_config* cfg,
                           sb_complex* x, sb_gmres_stats* stats) {
     return guarded([&] {

@@ -1,6 +1,7 @@
 // Internal declarations shared by the sonium-b200 CUDA sources (not part of the C ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -191,6 +192,7 @@ struct Operator {
     DevBuf coef, far_part, near_rhs, self_rhs, scratch, status;
     void* work = nullptr;        // solver workspace (gmres.cu), released by destroy_solve_work
     void* tensor = nullptr;      // BF16 split planes for the tensor-core block product (tensor.cu)
+    void* ozaki = nullptr;       // INT8 slices of the complex128 matrix for the block residual (ozaki.cu)
     void* multi = nullptr;       // many-right-hand-side solver workspace (batch.cu)
     // Discontinuous bases (n = 3 or 6 x elements): collocation points / normals (SoA) and the
     // near-pair CSR of the collocation rows.
@@ -321,6 +323,17 @@ void field_eval(const Mesh& mesh, const sb_physics& ph, const double2* pressure,
 // Y = A X for r complex64 vectors (vector c at x + c * ldx, result at y + c * ldy).
 void tensor_prepare(Operator& op);
 void tensor_release(Operator& op);
+// 2-D tiled TMA descriptor over rows x ldk elements of elem_bytes (row pitch ldk elements), box of
+// box_rows x box_inner elements, with the given swizzle.
+CUtensorMap make_tmap_2d(void* base, CUtensorMapDataType type, int elem_bytes, int64_t rows, int64_t ldk,
+                         int box_inner, int box_rows, CUtensorMapSwizzle swizzle);
+// R = B - A X for r complex128 vectors on the operator's complex128 matrix (ozaki.cu): integer
+// slices on the INT8 tensor cores, FP64-grade; b_c at b + c * ldb, x_c at x + c * ldx, r_c at
+// res + c * ldr. Builds the matrix slices on first use; tensor_release drops them.
+void ozaki_residual(const Operator& op, const double2* b, int64_t ldb, const double2* x, int64_t ldx, int r,
+                    double2* res, int64_t ldr, cudaStream_t s);
+void ozaki_release(Operator& op);
+int ozaki_status(const Operator& op, bool reset);
 bool tensor_ready(const Operator& op);
 // block_gate (optional, one int per group of kTensorRhsTile vectors): a group whose entry is 0
 // is skipped; its results are unspecified (zero or left as they were).

@@ -47,6 +47,15 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16_f32(int m, int n) {
            | ((uint32_t)(m >> 4) << 24);// M / 16, bits [24,29)
 }
 
+// Instruction descriptor of kind::i8 with signed 8-bit A and B, S32 accumulator, both K-major.
+__host__ __device__ constexpr uint32_t instr_desc_s8_s32(int m, int n) {
+    return (2u << 4)                    // D format S32, bits [4,6)
+           | (1u << 7)                  // A format signed 8-bit, bits [7,10)
+           | (1u << 10)                 // B format signed 8-bit, bits [10,13)
+           | ((uint32_t)(n >> 3) << 17) // N / 8, bits [17,23)
+           | ((uint32_t)(m >> 4) << 24);// M / 16, bits [24,29)
+}
+
 #if defined(__CUDA_ARCH__)
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -58,6 +67,10 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 }
 __device__ __forceinline__ void mbar_fence_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// One arrival (no transaction bytes).
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -118,16 +131,25 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
         ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
+// D[tmem] (+)= A[smem] * B[smem]^T with signed 8-bit operands and exact S32 accumulation.
+__device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
 // The mbarrier gets one arrival when every MMA issued so far by this thread has completed.
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
 }
 
-// 32 consecutive FP32 columns of this warp's 32 TMEM lanes (one lane per thread); the load and
+// 32 consecutive 32-bit columns of this warp's 32 TMEM lanes (one lane per thread); the load and
 // its completion wait are one asm statement, so no use of the registers can move above the wait.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+__device__ __forceinline__ void tmem_ld32_raw(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
@@ -140,6 +162,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
           "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr)
         : "memory");
+}
+// The same, as FP32 values.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    tmem_ld32_raw(taddr, r);
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }

@@ -255,20 +255,25 @@ EncodeTiled encode_fn() {
 
 // 2-D BF16 tensor map over rows x ldk (row pitch ldk elements), box of box_rows x 32, 64B swizzle.
 CUtensorMap make_map(void* base, int64_t rows, int64_t ldk, int box_rows) {
-    CUtensorMap m;
-    std::memset(&m, 0, sizeof(m));
-    const cuuint64_t dims[2] = {(cuuint64_t)ldk, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)ldk * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)kTileK, (cuuint32_t)box_rows};
-    const cuuint32_t elem[2] = {1, 1};
-    const CUresult rc = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, elem,
-                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    SB_REQUIRE(rc == CUDA_SUCCESS, SB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    return m;
+    return make_tmap_2d(base, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, rows, ldk, kTileK, box_rows,
+                        CU_TENSOR_MAP_SWIZZLE_64B);
 }
 
 }  // namespace
+
+CUtensorMap make_tmap_2d(void* base, CUtensorMapDataType type, int elem_bytes, int64_t rows, int64_t ldk,
+                         int box_inner, int box_rows, CUtensorMapSwizzle swizzle) {
+    CUtensorMap m;
+    std::memset(&m, 0, sizeof(m));
+    const cuuint64_t dims[2] = {(cuuint64_t)ldk, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldk * elem_bytes};
+    const cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_rows};
+    const cuuint32_t elem[2] = {1, 1};
+    const CUresult rc = encode_fn()(&m, type, 2, base, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                    swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    SB_REQUIRE(rc == CUDA_SUCCESS, SB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
 
 // Split planes of an operator's matrix and of the right-hand-side blocks (internal).
 struct TensorWork {
@@ -291,6 +296,7 @@ uint64_t tensor_generation(const Operator& op) {
 void tensor_release(Operator& op) {
     delete static_cast<TensorWork*>(op.tensor);
     op.tensor = nullptr;
+    ozaki_release(op);
 }
 
 bool tensor_ready(const Operator& op) { return op.tensor != nullptr; }

@@ -507,6 +507,19 @@ def gmres_mixed(operator: TbemOperator, b, config: IrConfig = IrConfig(), x0=Non
     return GmresSolution._from(x, st)
 
 
+def block_residual(operator: TbemOperator, B, X):
+    """R = B - A X for n x r blocks on the operator's complex128 matrix (the block residual of block
+    GMRES, crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:829): integer
+    slices on the INT8 tensor cores, FP64-grade (not bit-identical to an FP64 GEMM)."""
+    B = _c128(B)
+    X = _c128(X)
+    if B.ndim != 2 or B.shape[0] != operator.n or X.shape != B.shape:
+        raise SoniumError(L.SB_ERR_INVALID_ARGUMENT, "block_residual: B and X must be n x r")
+    R = np.zeros_like(B)
+    check(L.load().sb_operator_block_residual(operator.handle, _p(B), _p(X), B.shape[1], _p(R)))
+    return R
+
+
 def gmres_multi(operator: TbemOperator, B, config: IrConfig = IrConfig()):
     """Many right-hand sides of one operator (the block_gmres_preconditioned role,
     crates/sonium-solvers/crates/sonium-solvers-iterative/src/block_gmres.rs:163): B is n x r, returns

@@ -29,6 +29,15 @@ int main() {
             bad = 1;
         }
     }
+    {
+        const uint32_t ref = uint32_t(cute::UMMA::make_instr_desc<int8_t, int8_t, int32_t, 128, 256,
+                                                                  cute::UMMA::Major::K, cute::UMMA::Major::K>());
+        const uint32_t ours = sb::umma::instr_desc_s8_s32(128, 256);
+        if (ours != ref) {
+            std::printf("instr s8 128x256: ours %08x cutlass %08x\n", ours, ref);
+            bad = 1;
+        }
+    }
     for (uint32_t addr : {0x0u, 0x400u, 0x12340u, 0x3FFF0u}) {
         cute::UMMA::SmemDescriptor d;
         d.start_address_ = static_cast<uint16_t>(addr >> 4);
