@@ -53,10 +53,13 @@ namespace {
 constexpr int kSlices = 8;
 constexpr int kOzM = 128;                                // Ahat rows per tile (64 complex rows)
 constexpr int kOzRhs = 128;                              // right-hand sides per tile (256 Xhat rows)
-constexpr int kOzK = 64;                                 // K per stage: one 64-byte swizzle row of int8
-constexpr int kOzStages = 8;
-constexpr uint32_t kOzABytes = kOzM * kOzK;              // 8 KB
-constexpr uint32_t kOzXBytes = 2 * kOzRhs * kOzK;        // 16 KB
+#ifndef SB_OZ_K
+#define SB_OZ_K 128
+#endif
+constexpr int kOzK = SB_OZ_K;                            // K per stage: one swizzle row of int8 (128 B)
+constexpr int kOzStages = kOzK == 128 ? 4 : 8;
+constexpr uint32_t kOzABytes = kOzM * kOzK;              // 16 KB
+constexpr uint32_t kOzXBytes = 2 * kOzRhs * kOzK;        // 32 KB
 constexpr uint32_t kOzStageBytes = kOzABytes + kOzXBytes;
 constexpr uint32_t kOzSmem = kOzStages * kOzStageBytes + 1024;
 constexpr uint32_t kOzTmemCols = 512;
@@ -64,6 +67,13 @@ constexpr int kOzSegBlocks = (1 << 15) / kOzK;           // K blocks per exact I
 constexpr int kOzMaxPasses = 8;
 constexpr int kOzThreads = 192;
 constexpr int kOzMaxSplit = 4;
+
+constexpr CUtensorMapSwizzle kOzSwizzle = kOzK == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+
+// Shared-memory descriptor of a K-major tile row of kOzK bytes (the TMA box's swizzle).
+__device__ __forceinline__ uint64_t oz_desc(uint32_t addr) {
+    return kOzK == 128 ? umma::smem_desc_k_sw128(addr) : umma::smem_desc_k_sw64(addr);
+}
 
 constexpr int kErrOzProducer = 1;
 constexpr int kErrOzMma = 2;
@@ -328,13 +338,13 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                             const uint32_t sa = base + s * kOzStageBytes, sa_prev = base + sp * kOzStageBytes;
 #pragma unroll
                             for (int kk = 0; kk < kOzK / 32; ++kk) {
-                                const uint64_t xd = smem_desc_k_sw64(sa + kOzABytes + kk * 32);
+                                const uint64_t xd = oz_desc(sa + kOzABytes + kk * 32);
                                 if (hi) {
-                                    mma_s8(tacc + 256, smem_desc_k_sw64(sa + kk * 32), xd, idesc, acc_hi);
+                                    mma_s8(tacc + 256, oz_desc(sa + kk * 32), xd, idesc, acc_hi);
                                     acc_hi = 1;
                                 }
                                 if (lo && k >= 2) {
-                                    mma_s8(tacc, smem_desc_k_sw64(sa_prev + kk * 32), xd, idesc, acc_lo);
+                                    mma_s8(tacc, oz_desc(sa_prev + kk * 32), xd, idesc, acc_lo);
                                     acc_lo = 1;
                                 }
                             }
@@ -509,7 +519,7 @@ static OzakiWork& ozaki_prepare(const Operator& cop, cudaStream_t s) {
         count_launch();
         SB_CUDA(cudaGetLastError());
         w->tm_a = make_tmap_2d(w->a.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, (int64_t)kSlices * w->arows, w->ldk, kOzK,
-                               kOzM, CU_TENSOR_MAP_SWIZZLE_64B);
+                               kOzM, kOzSwizzle);
         SB_CUDA(cudaFuncSetAttribute(k_ozaki_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzSmem));
     } catch (...) {
         ozaki_release(op);
@@ -548,7 +558,7 @@ void ozaki_residual(const Operator& op, const double2* b, int64_t ldb, const dou
         SB_CUDA(cudaMemsetAsync(w.x.p, 0, bytes, s));
         w.rblocks = rblocks;
         w.tm_x = make_tmap_2d(w.x.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, (int64_t)kSlices * xrows_new, w.ldk, kOzK,
-                              2 * kOzRhs, CU_TENSOR_MAP_SWIZZLE_64B);
+                              2 * kOzRhs, kOzSwizzle);
     }
     const int64_t xrows = (int64_t)w.rblocks * 2 * kOzRhs;  // rows per plane of the allocated X slices
     const int64_t tiles = (int64_t)rblocks * (w.arows / kOzM);
