@@ -79,10 +79,17 @@ namespace {
 
 constexpr int kChunk = 256;  // vector rows per CTA of the vector kernels
 constexpr int kBDotVecs = 8;
-constexpr int kDotSpan = 8;  // kChunk row slices per CTA of the Gram-Schmidt dots
+constexpr int kDotSpan = 32;  // kChunk row slices per CTA of the Gram-Schmidt dots
+constexpr int kRowsPerThread = 4;  // rows per thread of the projection and next-vector kernels
+constexpr int kWide = kChunk * kRowsPerThread;
 constexpr int kScal = 5;
 
 __device__ __forceinline__ int find_inst(const int64_t* __restrict__ pre, int ninst, int64_t unit) {
+    // Instances of equal size (every right-hand side of one operator): the proportional guess is
+    // the answer, two dependent loads instead of a binary search's log2(ninst).
+    const int64_t total = pre[ninst];
+    const int guess = static_cast<int>(min((int64_t)ninst - 1, unit * ninst / max(total, (int64_t)1)));
+    if (pre[guess] <= unit && unit < pre[guess + 1]) return guess;
     int lo = 0, hi = ninst - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -333,7 +340,8 @@ __global__ void k_breduce(const BInst* __restrict__ inst, const int64_t* __restr
     if (threadIdx.x == 0) (second ? I.red2 : I.red)[i] = make_double2(sr, si);
 }
 
-// w -= sum_{i<k} coeff[i] V_i (coeff = red or red2), partial |w|^2 per chunk.
+// w -= sum_{i<k} coeff[i] V_i (coeff = red or red2), partial |w|^2 per chunk of kWide rows
+// (kRowsPerThread rows per thread, kChunk apart: every basis load of a warp stays coalesced).
 __global__ void __launch_bounds__(kChunk) k_bproject(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
                                                      int ninst, int k, int second, int gk) {
     __shared__ double2 sc[kMaxKrylov + 1];
@@ -345,20 +353,37 @@ __global__ void __launch_bounds__(kChunk) k_bproject(const BInst* __restrict__ i
     for (int t = threadIdx.x; t < k; t += kChunk) sc[t] = coeff[t];
     __syncthreads();
     const int64_t chunk = blockIdx.x - pre[b];
-    const int64_t r = chunk * kChunk + threadIdx.x;
-    double nr2[1] = {0.0};
-    if (r < I.n) {
-        const float2 w0 = I.w[r];
-        double ar = w0.x, ai = w0.y;
-        for (int i = 0; i < k; ++i) {
-            const float2 v = I.V[i * I.vs + r];
-            ar -= sc[i].x * v.x - sc[i].y * v.y;
-            ai -= sc[i].x * v.y + sc[i].y * v.x;
-        }
-        const float2 o = make_float2(static_cast<float>(ar), static_cast<float>(ai));
-        I.w[r] = o;
-        nr2[0] = (double)o.x * o.x + (double)o.y * o.y;
+    const int64_t n = I.n;
+    const float2* __restrict__ V = I.V;
+    const int64_t vs = I.vs;
+    int64_t rr[kRowsPerThread];
+    double ar[kRowsPerThread], ai[kRowsPerThread];
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) {
+        rr[q] = chunk * kWide + q * kChunk + threadIdx.x;
+        const float2 w0 = rr[q] < n ? I.w[rr[q]] : make_float2(0.f, 0.f);
+        ar[q] = w0.x;
+        ai[q] = w0.y;
     }
+    for (int i = 0; i < k; ++i) {
+        const double2 c = sc[i];
+        float2 v[kRowsPerThread];
+#pragma unroll
+        for (int q = 0; q < kRowsPerThread; ++q) v[q] = rr[q] < n ? V[i * vs + rr[q]] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < kRowsPerThread; ++q) {
+            ar[q] -= c.x * v[q].x - c.y * v[q].y;
+            ai[q] -= c.x * v[q].y + c.y * v[q].x;
+        }
+    }
+    double nr2[1] = {0.0};
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q)
+        if (rr[q] < n) {
+            const float2 o = make_float2(static_cast<float>(ar[q]), static_cast<float>(ai[q]));
+            I.w[rr[q]] = o;
+            nr2[0] += (double)o.x * o.x + (double)o.y * o.y;
+        }
     block_sum<1, kChunk>(nr2, red);
     if (threadIdx.x == 0) I.pnorm[chunk] = nr2[0];
 }
@@ -377,17 +402,27 @@ __global__ void k_bgivens(const BInst* __restrict__ inst, int ninst, int j) {
     givens_step_dev(I.st, I.red2, I.nrm + 1, I.H, I.cs, I.sn, I.g, j);
 }
 
-// V_{j+1} = w / ||w|| for the instances still running.
+// V_{j+1} = w / ||w|| for the instances still running (chunks of kWide rows).
 __global__ void __launch_bounds__(kChunk) k_bnext(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
                                                   int ninst, int j) {
     const int b = find_inst(pre, ninst, blockIdx.x);
     const BInst& I = inst[b];
     if (!I.st->active) return;
-    const int64_t r = (blockIdx.x - pre[b]) * kChunk + threadIdx.x;
-    if (r >= I.n) return;
     const double s = I.st->inv_wn;
-    const float2 v = I.w[r];
-    I.V[(int64_t)(j + 1) * I.vs + r] = make_float2(static_cast<float>(v.x * s), static_cast<float>(v.y * s));
+    const int64_t n = I.n;
+    float2* __restrict__ dst = I.V + (int64_t)(j + 1) * I.vs;
+    const int64_t r0 = (blockIdx.x - pre[b]) * kWide + threadIdx.x;
+    float2 v[kRowsPerThread];
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) {
+        const int64_t r = r0 + q * kChunk;
+        v[q] = r < n ? I.w[r] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) {
+        const int64_t r = r0 + q * kChunk;
+        if (r < n) dst[r] = make_float2(static_cast<float>(v[q].x * s), static_cast<float>(v[q].y * s));
+    }
 }
 
 // Vector updates over the flattened chunks.
@@ -538,8 +573,8 @@ struct Batch {
     std::vector<BatchAsmInst> asm_h;
     std::vector<double2*> rhs;  // per-instance right-hand side (pool_rhs)
     std::vector<BInst> h;
-    std::vector<int64_t> pre4, pre16, pre256, predot;
-    DevBuf asm_d, inst_d, pre4_d, pre16_d, pre256_d, predot_d, pre_asm;
+    std::vector<int64_t> pre4, pre16, pre256, predot, prewide;
+    DevBuf asm_d, inst_d, pre4_d, pre16_d, pre256_d, predot_d, prewide_d, pre_asm;
     // Inner products on the complex64 matrices (SB_INNER_FP32) or on complex-half copies built
     // after each assembly (SB_INNER_FP16; independent instances only).
     int inner = SB_INNER_FP32;
@@ -820,6 +855,7 @@ static void batch_workspace(Batch& B, int64_t m) {
     B.pre16.assign(ni + 1, 0);
     B.pre256.assign(ni + 1, 0);
     B.predot.assign(ni + 1, 0);
+    B.prewide.assign(ni + 1, 0);
     for (int b = 0; b < ni; ++b) {
         const int64_t n = B.nvec[b], ldv = (n + 1) / 2 * 2;
         const int64_t chunks = cdiv64(n, kChunk);
@@ -861,6 +897,7 @@ static void batch_workspace(Batch& B, int64_t m) {
         B.pre16[b + 1] = B.pre16[b] + cdiv64(n, kGemv16Rows);
         B.pre256[b + 1] = B.pre256[b] + chunks;
         B.predot[b + 1] = B.predot[b] + cdiv64(n, (int64_t)kChunk * kDotSpan);
+        B.prewide[b + 1] = B.prewide[b] + cdiv64(n, (int64_t)kWide);
     }
     B.inst_d.alloc(sizeof(BInst) * ni);
     B.pre4_d.alloc(sizeof(int64_t) * (ni + 1));
@@ -868,6 +905,8 @@ static void batch_workspace(Batch& B, int64_t m) {
     B.pre256_d.alloc(sizeof(int64_t) * (ni + 1));
     B.predot_d.alloc(sizeof(int64_t) * (ni + 1));
     h2d_sync(B.predot_d.p, B.predot.data(), sizeof(int64_t) * (ni + 1));
+    B.prewide_d.alloc(sizeof(int64_t) * (ni + 1));
+    h2d_sync(B.prewide_d.p, B.prewide.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
     h2d_sync(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.pre16_d.p, B.pre16.data(), sizeof(int64_t) * (ni + 1));
@@ -915,15 +954,17 @@ static void batch_step(Batch& B, int j) {
     const dim3 gr(static_cast<unsigned>(k + 1), static_cast<unsigned>(ni));
     k_bdots<<<gd, kChunk, 0, s>>>(I, pdot, ni, k, G_ACTIVE);
     k_breduce<<<gr, 32, 0, s>>>(I, pdot, k, 0, G_ACTIVE);
-    k_bproject<<<g256, kChunk, 0, s>>>(I, p256, ni, k, 0, G_ACTIVE);
-    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 0, G_ACTIVE);
+    const unsigned gw = static_cast<unsigned>(B.prewide.back());
+    const int64_t* pw = B.prewide_d.as<int64_t>();
+    k_bproject<<<gw, kChunk, 0, s>>>(I, pw, ni, k, 0, G_ACTIVE);
+    k_bsum_partials<<<ni, 32, 0, s>>>(I, pw, 0, G_ACTIVE);
     k_bafter_first<<<gi, 64, 0, s>>>(I, ni, j);
     k_bdots<<<gd, kChunk, 0, s>>>(I, pdot, ni, k, G_REORTH);
     k_breduce<<<gr, 32, 0, s>>>(I, pdot, k, 1, G_REORTH);
-    k_bproject<<<g256, kChunk, 0, s>>>(I, p256, ni, k, 1, G_REORTH);
-    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 1, G_REORTH);
+    k_bproject<<<gw, kChunk, 0, s>>>(I, pw, ni, k, 1, G_REORTH);
+    k_bsum_partials<<<ni, 32, 0, s>>>(I, pw, 1, G_REORTH);
     k_bgivens<<<gi, 64, 0, s>>>(I, ni, j);
-    k_bnext<<<g256, kChunk, 0, s>>>(I, p256, ni, j);
+    k_bnext<<<gw, kChunk, 0, s>>>(I, pw, ni, j);
     for (int t = 0; t < 11; ++t) count_launch();
     (void)g4;
     SB_CUDA(cudaGetLastError());
