@@ -718,6 +718,7 @@ __device__ __forceinline__ float far32_col_threshold(double thr, double bound) {
 
 // One quadrature point (a, b, k |delta|^2, w J / 4 pi) of a far pair, scalar (the point left over
 // by the packed pairs). t = k (r_q - r_c) = k (2 d_c . delta + |delta|^2) / (r_q + r_c).
+template <bool kChecked>
 __device__ __forceinline__ void far32_point(Far32Sums& s, float pa, float pb, float pdk, float pw,
                                             const Far32Pair& c, float kf, float invk, float k2f) {
     const float numk = fmaf(c.a2k, pa, fmaf(c.b2k, pb, pdk));
@@ -725,7 +726,7 @@ __device__ __forceinline__ void far32_point(Far32Sums& s, float pa, float pb, fl
     const float rinv = rsqrtf(rq2);
     const float t = numk * rcp_approx(fmaf(rq2, rinv, c.rc));
     float st, ct;
-    if (fabsf(t) <= 3.14159265f) {
+    if (!kChecked || fabsf(t) <= 3.14159265f) {
         __sincosf(t, &st, &ct);
     } else {
         sincos_f32(t, &st, &ct);
@@ -748,6 +749,84 @@ __device__ __forceinline__ void far32_point(Far32Sums& s, float pa, float pb, fl
     const float f_i = -kf * rinv * s3;
     s.er = fmaf(g_r, f_r, fmaf(-g_i, f_i, s.er));
     s.ei = fmaf(g_r, f_i, fmaf(g_i, f_r, s.ei));
+}
+
+// The 12 packed points of a far pair (the 13th is far32_point). kChecked: test every pair's
+// phase offsets against pi and take the quadrant-reduced sine / cosine beyond it; without it the
+// caller has shown |t| <= k max |delta| < 3 for every point of the column (|r_q - r_c| <= |delta|).
+template <bool kChecked, bool kSmemCols>
+__device__ __forceinline__ Far32Sums far32_pairs(const Far32Pair& c, const float2 (&PA)[kFarPairs],
+                                                 const float2 (&PB)[kFarPairs], const float4* sPDW,
+                                                 const float4 (&PDW)[kSmemCols ? 1 : kFarPairs], int tid, float kf,
+                                                 float invk, float k2f) {
+    // Points in pairs. With u = g_r / r + g_i k and nbi = g_i / r - g_r k (b = g (-1/r + i k) =
+    // -(u + i nbi)), r.n_y = fny / r and q1 = (3 r.n_y r.(-n_x) + n_x.n_y) / r:
+    //   H = -fny sum (u + i nbi) / r,  H^T = -sum (u + i nbi) r.(-n_x),
+    //   E = sum q1 (u + i nbi) - k^2 fny sum g r.(-n_x) / r,
+    // so every channel is a lane sum of one fma per point.
+    const float2 A2K = bc2(c.a2k), B2K = bc2(c.b2k), RC2 = bc2(c.rc2), RC = bc2(c.rc);
+    const float2 EA = bc2(c.ea), EB = bc2(c.eb), FNX = bc2(c.fnx), FNY3 = bc2(3.f * c.fny);
+    const float2 NXNY = bc2(c.nxny), KK = bc2(kf), NK = bc2(-kf), INVK = bc2(invk);
+    float2 AGR, AGI, SHR, SHI, NATR, NATI, AER, AEI, GQR, GQI;  // set by the first pair
+#pragma unroll
+    for (int p = 0; p < kFarPairs; ++p) {
+        float4 dw;
+        if constexpr (kSmemCols) dw = sPDW[p * kFarTile + tid]; else dw = PDW[p];
+        const float2 numk = pfma(A2K, PA[p], pfma(B2K, PB[p], make_float2(dw.x, dw.y)));
+        const float2 rq2 = pfma(numk, INVK, RC2);
+        const float2 rinv = make_float2(rsqrtf(rq2.x), rsqrtf(rq2.y));
+        const float2 den = pfma(rq2, rinv, RC);
+        const float2 t = pmul(numk, make_float2(rcp_approx(den.x), rcp_approx(den.y)));
+        // Special-function sine / cosine while both phase offsets are within one element
+        // size (|t| <= pi, every resolved mesh), else the quadrant-reduced version.
+        float2 S, C;
+        if (!kChecked || fmaxf(fabsf(t.x), fabsf(t.y)) <= 3.14159265f) {
+            __sincosf(t.x, &S.x, &C.x);
+            __sincosf(t.y, &S.y, &C.y);
+        } else {
+            sincos_f32(t.x, &S.x, &C.x);
+            sincos_f32(t.y, &S.y, &C.y);
+        }
+        const float2 gs = pmul(make_float2(dw.z, dw.w), rinv);
+        const float2 gr = pmul(C, gs), gi = pmul(S, gs);
+        const float2 rnx = pmul(pfma(PB[p], EB, pfma(PA[p], EA, FNX)), rinv);
+        const float2 u = pfma(gr, rinv, pmul(gi, KK));
+        const float2 nbi = pfma(gi, rinv, pmul(gr, NK));
+        const float2 rq1 = pmul(rnx, rinv);
+        const float2 q1 = pmul(rinv, pfma(FNY3, rq1, NXNY));
+        if (p == 0) {
+            AGR = gr;
+            AGI = gi;
+            SHR = pmul(u, rinv);
+            SHI = pmul(nbi, rinv);
+            NATR = pmul(u, rnx);
+            NATI = pmul(nbi, rnx);
+            AER = pmul(q1, u);
+            AEI = pmul(q1, nbi);
+            GQR = pmul(gr, rq1);
+            GQI = pmul(gi, rq1);
+        } else {
+            AGR = padd(AGR, gr);
+            AGI = padd(AGI, gi);
+            SHR = pfma(u, rinv, SHR);
+            SHI = pfma(nbi, rinv, SHI);
+            NATR = pfma(u, rnx, NATR);
+            NATI = pfma(nbi, rnx, NATI);
+            AER = pfma(q1, u, AER);
+            AEI = pfma(q1, nbi, AEI);
+            GQR = pfma(gr, rq1, GQR);
+            GQI = pfma(gi, rq1, GQI);
+        }
+    }
+    const float kfny = k2f * c.fny;
+    return Far32Sums{AGR.x + AGR.y,
+                     AGI.x + AGI.y,
+                     -c.fny * (SHR.x + SHR.y),
+                     -c.fny * (SHI.x + SHI.y),
+                     -(NATR.x + NATR.y),
+                     -(NATI.x + NATI.y),
+                     (AER.x + AER.y) - kfny * (GQR.x + GQR.y),
+                     (AEI.x + AEI.y) - kfny * (GQI.x + GQI.y)};
 }
 
 // One (128-column tile, 64-row block) of the FP32 far field; all 128 threads of the CTA call it.
@@ -801,12 +880,16 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
     double cx = 0, cy = 0, cz = 0;
     float nyx = 0, nyy = 0, nyz = 0;
     const int64_t jj = j < n ? j : 0;
+    // |t| = k |r_q - r_c| <= k |delta| for every point: a column with k max |delta| below 3 needs no
+    // per-point range test of the special-function sine / cosine (decided per warp).
+    float dmax2 = 0.f;
 #pragma unroll
     for (int p = 0; p < kFarPairs; ++p) {
         const float* s0 = qp32 + (int64_t)(2 * p * kQ32) * ld + jj;
         const float* s1 = s0 + (int64_t)kQ32 * ld;
         PA[p] = make_float2(s0[0], s1[0]);
         PB[p] = make_float2(s0[ld], s1[ld]);
+        dmax2 = fmaxf(dmax2, fmaxf(s0[2 * ld], s1[2 * ld]));
         const float4 v = make_float4(kf * s0[2 * ld], kf * s1[2 * ld], s0[3 * ld], s1[3 * ld]);
         if constexpr (kSmemCols) sPDW[p * kFarTile + tid] = v; else PDW[p] = v;
     }
@@ -816,6 +899,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
         lb = sl[ld];
         lpdk = kf * sl[2 * ld];
         lw = sl[3 * ld];
+        dmax2 = sl[2 * ld];
         const float* fr = qp32 + (int64_t)kQ32Frame * ld + jj;
         sfa[tid] = make_float4(fr[0], fr[ld], fr[2 * ld], fr[3 * ld]);
         sfb[tid] = make_float2(fr[4 * ld], fr[5 * ld]);
@@ -836,6 +920,7 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
         sgf[tid] = make_float4(0.f, 0.f, 0.f, INFINITY);
         scf[0][tid] = scf[1][tid] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
+    const bool warp_fast = __all_sync(0xffffffffu, kf * kf * dmax2 < 9.f);
     __syncthreads();
     const int64_t rows_here = (n - row0 < kFar32Rows) ? (n - row0) : kFar32Rows;
     float vmax = 0.f;  // largest |re|, |im| this thread wrote (+inf for a non-finite part)
@@ -882,75 +967,12 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
             c.fnx = fx * nnx + fy * nny + fz * nnz;
             c.fny = fx * nyx + fy * nyy + fz * nyz;
             c.nxny = -(nnx * nyx + nny * nyy + nnz * nyz);
-            // Points in pairs. With u = g_r / r + g_i k and nbi = g_i / r - g_r k (b = g (-1/r + i k) =
-            // -(u + i nbi)), r.n_y = fny / r and q1 = (3 r.n_y r.(-n_x) + n_x.n_y) / r:
-            //   H = -fny sum (u + i nbi) / r,  H^T = -sum (u + i nbi) r.(-n_x),
-            //   E = sum q1 (u + i nbi) - k^2 fny sum g r.(-n_x) / r,
-            // so every channel is a lane sum of one fma per point.
-            const float2 A2K = bc2(c.a2k), B2K = bc2(c.b2k), RC2 = bc2(c.rc2), RC = bc2(c.rc);
-            const float2 EA = bc2(c.ea), EB = bc2(c.eb), FNX = bc2(c.fnx), FNY3 = bc2(3.f * c.fny);
-            const float2 NXNY = bc2(c.nxny), KK = bc2(kf), NK = bc2(-kf), INVK = bc2(invk);
-            float2 AGR, AGI, SHR, SHI, NATR, NATI, AER, AEI, GQR, GQI;  // set by the first pair
-#pragma unroll
-            for (int p = 0; p < kFarPairs; ++p) {
-                float4 dw;
-                if constexpr (kSmemCols) dw = sPDW[p * kFarTile + tid]; else dw = PDW[p];
-                const float2 numk = pfma(A2K, PA[p], pfma(B2K, PB[p], make_float2(dw.x, dw.y)));
-                const float2 rq2 = pfma(numk, INVK, RC2);
-                const float2 rinv = make_float2(rsqrtf(rq2.x), rsqrtf(rq2.y));
-                const float2 den = pfma(rq2, rinv, RC);
-                const float2 t = pmul(numk, make_float2(rcp_approx(den.x), rcp_approx(den.y)));
-                // Special-function sine / cosine while both phase offsets are within one element
-                // size (|t| <= pi, every resolved mesh), else the quadrant-reduced version.
-                float2 S, C;
-                if (fmaxf(fabsf(t.x), fabsf(t.y)) <= 3.14159265f) {
-                    __sincosf(t.x, &S.x, &C.x);
-                    __sincosf(t.y, &S.y, &C.y);
-                } else {
-                    sincos_f32(t.x, &S.x, &C.x);
-                    sincos_f32(t.y, &S.y, &C.y);
-                }
-                const float2 gs = pmul(make_float2(dw.z, dw.w), rinv);
-                const float2 gr = pmul(C, gs), gi = pmul(S, gs);
-                const float2 rnx = pmul(pfma(PB[p], EB, pfma(PA[p], EA, FNX)), rinv);
-                const float2 u = pfma(gr, rinv, pmul(gi, KK));
-                const float2 nbi = pfma(gi, rinv, pmul(gr, NK));
-                const float2 rq1 = pmul(rnx, rinv);
-                const float2 q1 = pmul(rinv, pfma(FNY3, rq1, NXNY));
-                if (p == 0) {
-                    AGR = gr;
-                    AGI = gi;
-                    SHR = pmul(u, rinv);
-                    SHI = pmul(nbi, rinv);
-                    NATR = pmul(u, rnx);
-                    NATI = pmul(nbi, rnx);
-                    AER = pmul(q1, u);
-                    AEI = pmul(q1, nbi);
-                    GQR = pmul(gr, rq1);
-                    GQI = pmul(gi, rq1);
-                } else {
-                    AGR = padd(AGR, gr);
-                    AGI = padd(AGI, gi);
-                    SHR = pfma(u, rinv, SHR);
-                    SHI = pfma(nbi, rinv, SHI);
-                    NATR = pfma(u, rnx, NATR);
-                    NATI = pfma(nbi, rnx, NATI);
-                    AER = pfma(q1, u, AER);
-                    AEI = pfma(q1, nbi, AEI);
-                    GQR = pfma(gr, rq1, GQR);
-                    GQI = pfma(gi, rq1, GQI);
-                }
-            }
-            const float kfny = k2f * c.fny;
-            Far32Sums sm{AGR.x + AGR.y,
-                         AGI.x + AGI.y,
-                         -c.fny * (SHR.x + SHR.y),
-                         -c.fny * (SHI.x + SHI.y),
-                         -(NATR.x + NATR.y),
-                         -(NATI.x + NATI.y),
-                         (AER.x + AER.y) - kfny * (GQR.x + GQR.y),
-                         (AEI.x + AEI.y) - kfny * (GQI.x + GQI.y)};
-            far32_point(sm, la, lb, lpdk, lw, c, kf, invk, k2f);
+            Far32Sums sm = warp_fast ? far32_pairs<false, kSmemCols>(c, PA, PB, sPDW, PDW, tid, kf, invk, k2f)
+                                     : far32_pairs<true, kSmemCols>(c, PA, PB, sPDW, PDW, tid, kf, invk, k2f);
+            if (warp_fast)
+                far32_point<false>(sm, la, lb, lpdk, lw, c, kf, invk, k2f);
+            else
+                far32_point<true>(sm, la, lb, lpdk, lw, c, kf, invk, k2f);
             const float4 w0 = scf[0][tid], w1 = scf[1][tid];  // (cG, cH), (cHt, cE)
             const float ur = sm.gr * w0.x - sm.gi * w0.y + sm.hr * w0.z - sm.hi * w0.w + sm.tr * w1.x -
                              sm.ti * w1.y + sm.er * w1.z - sm.ei * w1.w;
