@@ -22,6 +22,156 @@ __device__ __forceinline__ float2 bj_entry(double2 v) {
     return make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
 }
 
+// Blocks of 128 with 1024 threads, in registers: thread (ty, tx) = (tid / 32, tid % 32) holds rows
+// 4 ty .. 4 ty + 3 and columns 4 tx .. 4 tx + 3 of the block. Gauss-Jordan with implicit partial
+// pivoting: step k takes as pivot p_k the largest |M[i][k]| among rows not yet pivots (the lowest
+// index on ties) and exchanges it in place, with no row interchange (a_pk <- 1 / a_pk, a_pj <-
+// a_pj / a_pk, a_ik <- -a_ik / a_pk, a_ij <- a_ij - a_ik a_pj / a_pk). Row p_k then holds x_k's
+// equation and column c the coefficient of y_{p_c}, so inv[k][m] = M[p_k][c] with p_c = m. Only
+// the step's column and scaled pivot row pass through shared memory (double-buffered by the step's
+// parity, three barriers per step); a step costs 16 complex updates per thread.
+template <class TA>
+__device__ __forceinline__ void bj_invert128_reg(const TA* __restrict__ A, int64_t lda, int rows,
+                                                 const int32_t* __restrict__ perm, float2* __restrict__ out,
+                                                 int* __restrict__ status) {
+    constexpr int BS = 128;
+    __shared__ float2 s_col[2][BS];
+    __shared__ float2 s_row[2][BS];
+    __shared__ int s_piv[BS];             // p_k
+    __shared__ int s_step[BS];            // the step at which row r was the pivot
+    __shared__ unsigned char s_used[BS];
+    __shared__ int s_p;
+    __shared__ float2 s_inv;
+    __shared__ int s_singular;
+    const int tid = threadIdx.x, ty = tid >> 5, tx = tid & 31;
+    float2 m[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int i = 4 * ty + a;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int j = 4 * tx + b;
+            float2 v = make_float2(i == j ? 1.f : 0.f, 0.f);
+            if (i < rows && j < rows) v = bj_entry(A[(int64_t)perm[i] * lda + perm[j]]);
+            m[a][b] = v;
+        }
+    }
+    if (tid < BS) s_used[tid] = 0;
+    if (tid == 0) s_singular = 0;
+    __syncthreads();
+    for (int k = 0; k < BS; ++k) {
+        const int buf = k & 1, kc = k & 3;
+        // the column before the step
+        if (tx == (k >> 2)) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                float2 v = m[a][0];
+#pragma unroll
+                for (int b = 1; b < 4; ++b)
+                    if (b == kc) v = m[a][b];
+                s_col[buf][4 * ty + a] = v;
+            }
+        }
+        __syncthreads();
+        // pivot: warp 0
+        if (ty == 0) {
+            float best = -1.f;
+            int bi = BS;
+#pragma unroll
+            for (int q = 0; q < BS / 32; ++q) {
+                const int i = tx + 32 * q;
+                if (!s_used[i]) {
+                    const float2 v = s_col[buf][i];
+                    const float a = v.x * v.x + v.y * v.y;
+                    if (a > best) {
+                        best = a;
+                        bi = i;
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (tx == 0) {
+                if (!(best > 0.f)) {
+                    s_singular = 1;
+                } else {
+                    s_p = bi;
+                    s_piv[k] = bi;
+                    s_step[bi] = k;
+                    s_used[bi] = 1;
+                    const float2 v = s_col[buf][bi];
+                    const float d = 1.f / (v.x * v.x + v.y * v.y);
+                    s_inv = make_float2(v.x * d, -v.y * d);
+                }
+            }
+        }
+        __syncthreads();
+        if (s_singular) break;
+        const int p = s_p;
+        const float2 inv = s_inv;
+        // the pivot row, scaled
+        if (ty == (p >> 2)) {
+            const int pa = p & 3;
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+                if (a == pa) {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const float2 nv = (4 * tx + b == k) ? inv : bj_cmul(m[a][b], inv);
+                        m[a][b] = nv;
+                        s_row[buf][4 * tx + b] = nv;
+                    }
+                }
+        }
+        __syncthreads();
+        float2 rv[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) rv[b] = s_row[buf][4 * tx + b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = 4 * ty + a;
+            if (i == p) continue;
+            const float2 f = s_col[buf][i];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                if (4 * tx + b == k) {
+                    const float2 q = bj_cmul(f, inv);
+                    m[a][b] = make_float2(-q.x, -q.y);
+                } else {
+                    const float2 pr = bj_cmul(f, rv[b]);
+                    m[a][b] = make_float2(m[a][b].x - pr.x, m[a][b].y - pr.y);
+                }
+            }
+        }
+    }
+    if (s_singular) {
+        if (tid == 0) atomicOr(status, 1);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int i = 4 * ty + a, j = 4 * tx + b;
+                out[j * BS + i] = make_float2(i == j ? 1.f : 0.f, 0.f);
+            }
+        return;
+    }
+    // inv^T: out[m][k] = inv[k][m] = M[p_k][c], p_c = m
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int r = 4 * ty + a;
+        const int kr = s_step[r];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out[s_piv[4 * tx + b] * BS + kr] = m[a][b];
+    }
+}
+
 // One CTA (THREADS threads, BS * BS float2 of dynamic shared memory at M) per block: gather the
 // diagonal block M = A[p_i][p_j], i, j < rows (identity beyond), rounded to complex64 when A is
 // complex128, invert it in place (Gauss-Jordan, partial pivoting) and store its transpose at out.
@@ -30,6 +180,10 @@ template <int BS, int THREADS, class TA = float2>
 __device__ __forceinline__ void bj_invert_block(const TA* __restrict__ A, int64_t lda, int rows,
                                                 const int32_t* __restrict__ perm, float2* __restrict__ out,
                                                 int* __restrict__ status, float2* M) {
+    if constexpr (BS == 128 && THREADS == 1024) {
+        bj_invert128_reg<TA>(A, lda, rows, perm, out, status);
+        return;
+    }
     __shared__ int piv[BS];
     __shared__ float2 fcol[BS];
     __shared__ int s_p;
