@@ -1064,8 +1064,30 @@ def multi_rhs_report(sb, L, a, op, mesh, B, X, first, prof, live, t_block, rt, b
                           "algorithmic_complex_flop_per_launch": algorithmic,
                           "share_of_kernel_time": ms["tensor"] / max(sum(ms.values()), 1e-9)},
         "residual_kernel": residual_roofline(n, r, live_res, pk, pk_kind, ms, launches, a.steps, res_err),
+        "gram_schmidt_kernels": gram_schmidt_roofline(n, first, ms["arnoldi"] / max(a.steps, 1), pk, pk_kind),
         "kernel_ms_per_solve": {kk: v / max(a.steps, 1) for kk, v in ms.items() if v > 0},
     }
+
+
+def gram_schmidt_roofline(n, stats, ms_per_solve, pk, pk_kind):
+    """Roofline of the many-right-hand-side Gram-Schmidt (k_bdots, k_bproject and their small
+    reductions, the `arnoldi` kernel class). Algorithmic bytes per right-hand side and Arnoldi step
+    with k basis vectors: two classical Gram-Schmidt passes (the DGKS second pass, which these
+    solves take at every step), each reading the k complex64 basis vectors twice (dots, projection)
+    plus w three times (8 bytes per entry): 2 (2 k + 3) 8 n. A right-hand side's inner iterations
+    are split evenly over its refinements (k counts from 1 in every inner solve)."""
+    total = 0.0
+    for st in stats:
+        solves = max(int(st.refinements), 1)
+        its = int(st.iterations)
+        for q in range(solves):
+            steps = its // solves + (1 if q < its % solves else 0)
+            total += sum(2.0 * (2 * k + 3) * 8.0 * n for k in range(1, steps + 1))
+    achieved = total / max(ms_per_solve / 1e3, 1e-12) / 1e9
+    return {"kernels": "k_bdots + k_bproject (+ k_breduce, k_bsum_partials, k_bnext, Givens / control)",
+            "bound": "hbm", "algorithmic_bytes_per_solve": total, "ms_per_solve": ms_per_solve,
+            "achieved": achieved, "unit": "GB/s", "peak": pk["hbm_gbs"], "frac": achieved / pk["hbm_gbs"],
+            "peak_source": pk_kind}
 
 
 OZAKI_PRODUCTS = 36  # slice products of the block residual: diagonals 2..9 of 8 x 8 INT8 slices

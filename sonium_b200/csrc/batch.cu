@@ -286,8 +286,10 @@ __global__ void k_bsum_partials(const BInst* __restrict__ inst, const int64_t* _
 }
 
 // Gram-Schmidt dots over the flattened chunks of kDotSpan * kChunk rows:
-// part[chunk * (k + 1) + i] = V_i^H w (i < k), |w|^2 at i = k.
-__global__ void __launch_bounds__(kChunk) k_bdots(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
+// part[chunk * (k + 1) + i] = V_i^H w (i < k), |w|^2 at i = k. A thread takes two adjacent rows per
+// 16-byte load (vectors have an even leading dimension; a row at n or beyond counts as zero) and
+// sums its kDotSpan / 2 row pairs in FP32 (the vectors are complex64); the CTA sum is FP64.
+__global__ void __launch_bounds__(kChunk, 4) k_bdots(const BInst* __restrict__ inst, const int64_t* __restrict__ pre,
                                                   int ninst, int k, int gk) {
     __shared__ double red[(kChunk / 32) * 2 * kBDotVecs];
     const int b = find_inst(pre, ninst, blockIdx.x);
@@ -295,31 +297,40 @@ __global__ void __launch_bounds__(kChunk) k_bdots(const BInst* __restrict__ inst
     if (!open_gate(I, gk)) return;
     const int64_t chunk = blockIdx.x - pre[b];
     const int i0 = blockIdx.y * kBDotVecs;
-    double acc[2 * kBDotVecs];
+    const int64_t n = I.n, vs = I.vs;
+    const float4* __restrict__ W = reinterpret_cast<const float4*>(I.w);
+    const float2* __restrict__ V = I.V;
+    float acc[2 * kBDotVecs];
 #pragma unroll
-    for (int t = 0; t < 2 * kBDotVecs; ++t) acc[t] = 0.0;
-    // kDotSpan row slices of kChunk per CTA: one block reduction per kDotSpan * kChunk rows
-    for (int sl = 0; sl < kDotSpan; ++sl) {
-        const int64_t r = (chunk * kDotSpan + sl) * kChunk + threadIdx.x;
-        if (r >= I.n) break;
-        const float2 wv = I.w[r];
+    for (int t = 0; t < 2 * kBDotVecs; ++t) acc[t] = 0.f;
+    for (int sl = 0; sl < kDotSpan / 2; ++sl) {
+        const int64_t r = (chunk * kDotSpan + 2 * sl) * kChunk + 2 * threadIdx.x;  // rows r, r + 1
+        if (r >= n) break;
+        const bool two = r + 1 < n;
+        float4 wv = W[r >> 1];
+        if (!two) wv.z = wv.w = 0.f;
 #pragma unroll
         for (int t = 0; t < kBDotVecs; ++t) {
             const int i = i0 + t;
             if (i < k) {
-                const float2 v = I.V[i * I.vs + r];
-                acc[2 * t] = fma((double)v.x, wv.x, fma((double)v.y, wv.y, acc[2 * t]));
-                acc[2 * t + 1] = fma((double)v.x, wv.y, fma(-(double)v.y, wv.x, acc[2 * t + 1]));
+                float4 v = *reinterpret_cast<const float4*>(V + i * vs + r);
+                if (!two) v.z = v.w = 0.f;
+                acc[2 * t] = fmaf(v.x, wv.x, fmaf(v.y, wv.y, fmaf(v.z, wv.z, fmaf(v.w, wv.w, acc[2 * t]))));
+                acc[2 * t + 1] =
+                    fmaf(v.x, wv.y, fmaf(-v.y, wv.x, fmaf(v.z, wv.w, fmaf(-v.w, wv.z, acc[2 * t + 1]))));
             } else if (i == k) {
-                acc[2 * t] = fma((double)wv.x, wv.x, fma((double)wv.y, wv.y, acc[2 * t]));
+                acc[2 * t] = fmaf(wv.x, wv.x, fmaf(wv.y, wv.y, fmaf(wv.z, wv.z, fmaf(wv.w, wv.w, acc[2 * t]))));
             }
         }
     }
-    block_sum<2 * kBDotVecs, kChunk>(acc, red);
+    double accd[2 * kBDotVecs];
+#pragma unroll
+    for (int t = 0; t < 2 * kBDotVecs; ++t) accd[t] = acc[t];
+    block_sum<2 * kBDotVecs, kChunk>(accd, red);
     if (threadIdx.x == 0)
         for (int t = 0; t < kBDotVecs; ++t) {
             const int i = i0 + t;
-            if (i <= k) I.part[chunk * (k + 1) + i] = make_double2(acc[2 * t], acc[2 * t + 1]);
+            if (i <= k) I.part[chunk * (k + 1) + i] = make_double2(accd[2 * t], accd[2 * t + 1]);
         }
 }
 
