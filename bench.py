@@ -819,6 +819,7 @@ def sweep_leg(sb, a, dist, dev, rt):
         asm_ms, solve_ms = batch.timings()  # the last timed step
         forms[form_name] = {"t": t_batch, "st0": st0, "xb": xb, "assembly_ms": asm_ms, "solve_ms": solve_ms}
     form, tune_p, tune_s = batch.assembly_tuning()
+    split, layout_ms = batch.assembly_split()
     batch.close()
     # plain FP64 baseline, one instance after another; and the same with the sweep's block-Jacobi
     # right preconditioner (blocks of BJ_BLOCK_SWEEP, as the half_inner_bj form)
@@ -878,6 +879,7 @@ def sweep_leg(sb, a, dist, dev, rt):
         "assembly_ms": asm_ms, "solve_ms": solve_ms,
         "assembly_form": {1: "persistent", 2: "streams"}.get(form, str(form)),
         "assembly_autotune_ms": {"persistent": tune_p, "streams": tune_s},
+        "assembly_persistent_layout": {"far_slots_per_sm": split, "autotune_ms": layout_ms},
         "iterations_total": {"batched": int(sum(s.iterations for s in st0)), "fp64": int(sum(fp64_iters)),
                              "fp64_bj": int(sum(fp64_bj_iters))},
         "inner_form": best,

@@ -475,13 +475,17 @@ SB_API int sb_batch_solution(const sb_batch* batch, int64_t index, sb_complex* x
 /* The assembled complex64 matrix of one instance, row-major n x n. */
 SB_API int sb_batch_matrix_c64(const sb_batch* batch, int64_t index, sb_complex32* matrix);
 /* Assembly form of sb_batch_assemble (no reference counterpart: the execution choice of this
- * implementation). SB_BATCH_ASM_PERSISTENT: one persistent launch walks a flattened work list of
- * every instance's far tiles, near pairs and self terms. SB_BATCH_ASM_STREAMS: per-instance far
- * kernels on the batch's stream with the near and self kernels on a second, higher-priority
- * stream beside them. Both run the same device functions and write the same entries.
- * SB_BATCH_ASM_AUTO (default): the first assembly of a batch shape (device, unknowns and near
- * pairs per instance) runs both forms, keeps the faster one for every later batch of that shape
- * in the process, and reports both times through sb_batch_assembly_tuning. */
+ * implementation). SB_BATCH_ASM_PERSISTENT: persistent CTAs walk flattened work lists of every
+ * instance's far tiles, near pairs and self terms, either as one launch (each CTA alternating far
+ * tiles with near / self items) or as two persistent launches side by side (the far tiles on some
+ * of each SM's CTA slots, the near / self items on the others; sb_batch_assembly_split).
+ * SB_BATCH_ASM_STREAMS: per-instance far kernels on the batch's stream with the near and self
+ * kernels on a second, higher-priority stream beside them. All run the same device functions and
+ * write the same entries. SB_BATCH_ASM_AUTO (default): the first assembly of a batch shape
+ * (device, unknowns and near pairs per instance) runs one untimed assembly, then times the
+ * persistent layouts and the streams form once each, keeps the fastest for every later batch of
+ * that shape in the process, and reports the times through sb_batch_assembly_tuning and
+ * sb_batch_assembly_split. */
 #define SB_BATCH_ASM_AUTO 0
 #define SB_BATCH_ASM_PERSISTENT 1
 #define SB_BATCH_ASM_STREAMS 2
@@ -490,6 +494,13 @@ SB_API int sb_batch_set_assembly_mode(sb_batch* batch, int mode);
  * milliseconds (0 when this batch did not run the autotuner). Any pointer may be NULL. */
 SB_API int sb_batch_assembly_tuning(const sb_batch* batch, int* chosen, double* persistent_ms,
                                     double* streams_ms);
+/* The persistent form's layout: far CTA slots per SM when it runs as two persistent launches (the
+ * far tiles of every instance on those slots, the near pairs and self terms on the SM's other slots,
+ * or, with all slots, on the slots the far launch frees at its end; 0 = one launch alternating
+ * both), and in layout_ms[0..4] (may be NULL) the autotuner's times of the one-launch layout (index
+ * 0) and of far tiles on 2, 3 and 4 slots (indices 2..4; 0 when it did not run). No counterpart in
+ * the reference (its sweep assembles one frequency after another). */
+SB_API int sb_batch_assembly_split(const sb_batch* batch, int* far_slots_per_sm, double* layout_ms);
 /* Device time of the last sb_batch_assemble and sb_batch_solve, milliseconds. */
 SB_API int sb_batch_timings(const sb_batch* batch, double* assembly_ms, double* solve_ms);
 

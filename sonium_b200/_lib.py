@@ -184,6 +184,7 @@ _SIGNATURES = {
     "sb_batch_set_assembly_mode": ([P, ct.c_int], ct.c_int),
     "sb_batch_assembly_tuning": ([P, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)],
                                  ct.c_int),
+    "sb_batch_assembly_split": ([P, ct.POINTER(ct.c_int), P], ct.c_int),
     "sb_memory_trim": ([ct.c_int], ct.c_int),
     "sb_memory_stats": ([ct.c_int, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)], ct.c_int),
     "sb_profile_enable": ([ct.c_int], ct.c_int),

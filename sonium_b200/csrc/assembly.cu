@@ -829,6 +829,21 @@ __device__ __forceinline__ Far32Sums far32_pairs(const Far32Pair& c, const float
                      (AEI.x + AEI.y) - kfny * (GQI.x + GQI.y)};
 }
 
+// Shared memory of one FP32 far tile (the persistent batched kernel overlays it with the near
+// pairs' subdivision buffers).
+struct Far32Smem {
+    float shs[kFar32Rows];        // rows: complex-half scales (with A16)
+    double sx[kFar32Rows][3];     // rows: collocation points
+    float4 sxf[kFar32Rows];       // rows: collocation points in FP32 (margin test)
+    float snx[kFar32Rows][3];     // rows: negated normals -n_x
+    float4 sgf[kFarTile];         // column: level-0 centre in FP32, thr_hi
+    float4 scf[2][kFarTile];      // column: matrix weights (cG, cH | cHt, cE)
+    float4 sfa[kFarTile];         // column: e1 x, y, z, e2 x
+    float2 sfb[kFarTile];         // column: e2 y, z
+    double sred[kFarTile / 32][2];
+    float4 sPDW[kFarPairs * kFarTile];  // (k |delta|^2, w J / 4 pi) of points 2p, 2p + 1 at [p * kFarTile + tid]
+};
+
 // One (128-column tile, 64-row block) of the FP32 far field; all 128 threads of the CTA call it.
 template <bool kWithRhs, bool kSmemCols = true>
 __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const double* __restrict__ elem,
@@ -838,16 +853,17 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
                                            int64_t row0, unsigned* __restrict__ amax = nullptr,
                                            uint32_t* __restrict__ A16 = nullptr, int64_t lda16 = 0,
                                            const float* __restrict__ hscale = nullptr,
-                                           int* __restrict__ hflag = nullptr) {
-    __shared__ float shs[kFar32Rows];        // rows: complex-half scales (with A16)
-    __shared__ double sx[kFar32Rows][3];     // rows: collocation points
-    __shared__ float4 sxf[kFar32Rows];       // rows: collocation points in FP32 (margin test)
-    __shared__ float snx[kFar32Rows][3];     // rows: negated normals -n_x
-    __shared__ float4 sgf[kFarTile];         // column: level-0 centre in FP32, thr_hi
-    __shared__ float4 scf[2][kFarTile];      // column: matrix weights (cG, cH | cHt, cE)
-    __shared__ float4 sfa[kFarTile];         // column: e1 x, y, z, e2 x
-    __shared__ float2 sfb[kFarTile];         // column: e2 y, z
-    __shared__ double sred[kFarTile / 32][2];
+                                           int* __restrict__ hflag = nullptr, Far32Smem* smem = nullptr) {
+    Far32Smem& S = *smem;
+    auto& shs = S.shs;
+    auto& sx = S.sx;
+    auto& sxf = S.sxf;
+    auto& snx = S.snx;
+    auto& sgf = S.sgf;
+    auto& scf = S.scf;
+    auto& sfa = S.sfa;
+    auto& sfb = S.sfb;
+    auto& sred = S.sred;
     const int tid = threadIdx.x;
     const int64_t j = tile * kFarTile + tid;
     __syncthreads();  // a previous tile of a persistent CTA may still read the shared arrays
@@ -867,14 +883,11 @@ __device__ __forceinline__ void far32_tile(const float* __restrict__ qp32, const
     const float kf = static_cast<float>(k), k2f = kf * kf, invk = 1.f / kf;
     // The column's 13 points: in-plane coordinates in registers (points 2p, 2p + 1 in the lanes of
     // pair p, the 13th alone); k |delta|^2 and the weights in shared memory with kSmemCols, else in
-    // registers (the persistent batched kernel, whose static shared memory is full).
+    // registers.
     float2 PA[kFarPairs], PB[kFarPairs];
     constexpr int kR = kSmemCols ? 1 : kFarPairs;
     float4* sPDW = nullptr;  // (k |delta|^2, w J / 4 pi) of points 2p, 2p + 1 at [p * kFarTile + tid]
-    if constexpr (kSmemCols) {
-        __shared__ float4 sPDW_buf[kFarPairs * kFarTile];
-        sPDW = sPDW_buf;
-    }
+    if constexpr (kSmemCols) sPDW = S.sPDW;
     float4 PDW[kR];
     float la, lb, lpdk, lw;
     double cx = 0, cy = 0, cz = 0;
@@ -1031,9 +1044,10 @@ __global__ void __launch_bounds__(kFarTile, kFar32MinBlocks) k_far32(const float
                                                     unsigned* __restrict__ amax, uint32_t* __restrict__ A16,
                                                     int64_t lda16, const float* __restrict__ hscale,
                                                     int* __restrict__ hflag) {
+    __shared__ Far32Smem fs;
     far32_tile<kWithRhs, kFar32SmemCols>(qp32, elem, n, ld, coef, k, coord_bound, A32, lda32, far_part, n_tiles,
                                          blockIdx.x, blockIdx.y * (int64_t)kFar32Rows, amax, A16, lda16, hscale,
-                                         hflag);
+                                         hflag, &fs);
 }
 
 // Complex-half copy during the FP32 assembly (after the near and self kernels): each row's scale
@@ -2464,48 +2478,135 @@ __device__ __forceinline__ int find_instance(const int64_t* __restrict__ pre, in
     return lo;
 }
 
+// Shared memory of the persistent kernel: a CTA works on one item at a time, so the far tile's
+// arrays and the near pairs' subdivision buffers share the same bytes.
+union BatchAsmSmem {
+    Far32Smem far;
+    NearWarpSmem near[kNearWarps];
+};
+
+// Largest |re|, |im| of the entries a warp wrote for one instance, kept in registers while the
+// warp's items stay in that instance and merged into the instance's word when it moves on.
+struct WarpAmax {
+    unsigned* dst = nullptr;
+    float m = 0.f;
+    __device__ __forceinline__ void add(unsigned* to, float v) {
+        if (to != dst) {
+            flush();
+            dst = to;
+        }
+        m = (v <= 3.4e38f) ? fmaxf(m, v) : INFINITY;
+    }
+    __device__ __forceinline__ void flush() {
+        if (dst && m > 0.f) atomicMax(dst, __float_as_uint(m));
+        m = 0.f;
+    }
+};
+
+constexpr int kBatchPerWarp = 4;  // near pairs / self elements per warp and item of the persistent kernel
+
+// kPart: 0 = every item (far tiles alternating with near / self items), 1 = the far tiles only,
+// 2 = the near pairs and self elements only.
+template <int kPart>
 __global__ void __launch_bounds__(kFarTile, 4) k_assemble_batch(const BatchAsmInst* __restrict__ inst, int ninst,
-                                                             const int64_t* __restrict__ pre) {
-    __shared__ NearWarpSmem nsm[kNearWarps];
+                                                             const int64_t* __restrict__ pre, int near_per_far) {
+    extern __shared__ __align__(16) unsigned char batch_smem[];
+    BatchAsmSmem& sm = *reinterpret_cast<BatchAsmSmem*>(batch_smem);
+    // The loop state is the same for the whole CTA and lives in shared memory, so no register holds
+    // it across a far tile (whose packed loop uses all 128).
+    __shared__ int64_t st_fi, st_qi;
+    __shared__ int st_bf, st_bn, st_bs, st_npf;
     const int64_t* fpre = pre;
     const int64_t* npre = pre + (ninst + 1);
     const int64_t* spre = pre + 2 * (ninst + 1);
-    const int64_t nf = fpre[ninst], nn = npre[ninst], ns = spre[ninst];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int64_t item = blockIdx.x; item < nf + nn + ns; item += gridDim.x) {
-        if (item < nf) {
-            const int b = find_instance(fpre, ninst, item);
-            const BatchAsmInst I = inst[b];
-            const int64_t local = item - fpre[b];
-            const int64_t nrb = (I.n + kFar32Rows - 1) / kFar32Rows;
-            far32_tile<false, false>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.coord_bound, I.A32, I.lda32, nullptr,
-                                     I.n_tiles, local / nrb, (local % nrb) * kFar32Rows);
-        } else if (item < nf + nn) {
-            const int64_t it = item - nf;
-            const int b = find_instance(npre, ninst, it);
-            const BatchAsmInst I = inst[b];
-            const int64_t p = (it - npre[b]) * kNearWarps + warp;
-            if (p < I.nnz) {
-                const int64_t i = I.near_row[p], j = I.near_col[p];
-                Acc a;
-                near_pair_channels(a, nsm[warp], I.elem, I.ld, i, j, I.k, I.k * I.k, lane);
-                const Acc t = warp_reduce(a);
-                if (lane == 0) {
-                    const double2 v = combine(t, I.coef, I.ld, j, CF_CG);
-                    I.A32[i * I.lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+    if (threadIdx.x == 0) {
+        st_fi = kPart == 2 ? fpre[ninst] : blockIdx.x;
+        st_qi = kPart == 1 ? npre[ninst] + spre[ninst] : blockIdx.x;
+        st_bf = st_bn = st_bs = 0;
+        st_npf = near_per_far;
+    }
+    __syncthreads();
+    // Each CTA alternates one far tile with near_per_far near / self items (both lists walked with
+    // the grid stride), so the far tiles and the FP64 near pairs share the SMs for the whole
+    // launch. Items only move forward, so each list's instance is kept and advanced, not searched.
+    for (;;) {
+        const int64_t nf = fpre[ninst], nq = npre[ninst] + spre[ninst];
+        if (st_fi >= nf && st_qi >= nq) break;
+        if (kPart != 2 && st_fi < nf) {
+            const int64_t fi = st_fi;
+            int bf = st_bf;
+            while (fpre[bf + 1] <= fi) ++bf;
+            const BatchAsmInst& I = inst[bf];
+            // column tiles fastest, as the per-instance launch's grid: the CTAs running side by side
+            // write neighbouring column blocks of the same rows
+            const int64_t local = fi - fpre[bf];
+            far32_tile<false, true>(I.qp32, I.elem, I.n, I.ld, I.coef, I.k, I.coord_bound, I.A32, I.lda32, nullptr,
+                                    I.n_tiles, local % I.n_tiles, (local / I.n_tiles) * kFar32Rows, I.amax, nullptr,
+                                    0, nullptr, nullptr, &sm.far);
+            // every warp is done with the tile before the next item reuses its shared memory
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                st_fi = fi + gridDim.x;
+                st_bf = bf;
+            }
+            __syncthreads();
+        }
+        if (kPart != 1) {
+            const int64_t nn = npre[ninst];
+            int64_t qi = st_qi;
+            int bn = st_bn, bs = st_bs;
+            const int npf = st_npf;
+            WarpAmax wam;  // lane 0's running maximum of the near and self entries
+            for (int rep = 0; rep < npf && qi < nq; ++rep, qi += gridDim.x) {
+                if (qi < nn) {
+                    while (npre[bn + 1] <= qi) ++bn;
+                    const BatchAsmInst& I = inst[bn];
+                    const int64_t p0 = (qi - npre[bn]) * (kNearWarps * kBatchPerWarp) + warp * kBatchPerWarp;
+                    for (int u = 0; u < kBatchPerWarp; ++u) {
+                        const int64_t p = p0 + u;
+                        if (p >= I.nnz) break;
+                        const int64_t i = I.near_row[p], j = I.near_col[p];
+                        Acc a;
+                        near_pair_channels(a, sm.near[warp], I.elem, I.ld, i, j, I.k, I.k * I.k, lane);
+                        const Acc t = warp_reduce(a);
+                        if (lane == 0) {
+                            const double2 v = combine(t, I.coef, I.ld, j, CF_CG);
+                            const float2 f = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+                            I.A32[i * I.lda32 + j] = f;
+                            if (I.amax) wam.add(I.amax, fmaxf(fabsf(f.x), fabsf(f.y)));
+                        }
+                    }
+                } else {
+                    const int64_t it = qi - nn;
+                    while (spre[bs + 1] <= it) ++bs;
+                    const BatchAsmInst& I = inst[bs];
+                    const int64_t e0 = (it - spre[bs]) * (kNearWarps * kBatchPerWarp) + warp * kBatchPerWarp;
+                    for (int u = 0; u < kBatchPerWarp; ++u) {
+                        const int64_t e = e0 + u;
+                        if (e >= I.n) break;
+                        Acc a;
+                        self_channels(a, I.elem, I.ld, e, I.k, lane);
+                        const Acc t = warp_reduce(a);
+                        if (lane == 0) {
+                            self_store(t, I.coef, I.ld, I.n, e, nullptr, I.A32, I.lda32, nullptr, I.diag);
+                            if (I.amax) {
+                                const float2 f = I.A32[e * I.lda32 + e];
+                                wam.add(I.amax, fmaxf(fabsf(f.x), fabsf(f.y)));
+                            }
+                        }
+                    }
                 }
             }
-        } else {
-            const int64_t it = item - nf - nn;
-            const int b = find_instance(spre, ninst, it);
-            const BatchAsmInst I = inst[b];
-            const int64_t e = (it - spre[b]) * kNearWarps + warp;
-            if (e < I.n) {
-                Acc a;
-                self_channels(a, I.elem, I.ld, e, I.k, lane);
-                const Acc t = warp_reduce(a);
-                if (lane == 0) self_store(t, I.coef, I.ld, I.n, e, nullptr, I.A32, I.lda32, nullptr, I.diag);
+            if (lane == 0) wam.flush();
+            __syncthreads();  // every warp read the state and finished its items
+            if (threadIdx.x == 0) {
+                st_qi = qi;
+                st_bn = bn;
+                st_bs = bs;
+                if (st_fi >= nf) st_npf = 1 << 30;  // far list done: the rest of the near / self list
             }
+            __syncthreads();
         }
     }
 }
@@ -3132,26 +3233,58 @@ void incident_plane_wave_at(int device, const double* pts_dev, const double* nrm
 }
 
 void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst* d_inst, DevBuf& pre_buf,
-                    cudaStream_t s, int device) {
+                    cudaStream_t s, int device, SideStream* side, int far_per_sm) {
     const int ninst = static_cast<int>(h_inst.size());
     std::vector<int64_t> pre(3 * (ninst + 1), 0);
     for (int b = 0; b < ninst; ++b) {
         const BatchAsmInst& I = h_inst[b];
         pre[b + 1] = pre[b] + I.n_tiles * cdiv(I.n, kFar32Rows);
-        pre[(ninst + 1) + b + 1] = pre[(ninst + 1) + b] + cdiv(I.nnz, kNearWarps);
-        pre[2 * (ninst + 1) + b + 1] = pre[2 * (ninst + 1) + b] + cdiv(I.n, kNearWarps);
+        pre[(ninst + 1) + b + 1] = pre[(ninst + 1) + b] + cdiv(I.nnz, kNearWarps * kBatchPerWarp);
+        pre[2 * (ninst + 1) + b + 1] = pre[2 * (ninst + 1) + b] + cdiv(I.n, kNearWarps * kBatchPerWarp);
     }
     if (pre_buf.bytes < sizeof(int64_t) * pre.size()) pre_buf.alloc(sizeof(int64_t) * pre.size());
     SB_CUDA(cudaMemcpyAsync(pre_buf.p, pre.data(), sizeof(int64_t) * pre.size(), cudaMemcpyHostToDevice, s));
+    const int smem = static_cast<int>(sizeof(BatchAsmSmem));
+    for (auto kern : {k_assemble_batch<0>, k_assemble_batch<1>, k_assemble_batch<2>})
+        SB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int per_sm = 0;
-    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_batch, kFarTile, 0));
-    const int64_t items = pre[ninst] + pre[2 * (ninst + 1) - 1] + pre[3 * (ninst + 1) - 1];
-    const int64_t grid = std::min<int64_t>(items, static_cast<int64_t>(std::max(per_sm, 1)) * device_sm_count(device));
-    ProfScope prof(SB_PROF_FAR, s);
-    k_assemble_batch<<<static_cast<unsigned>(std::max<int64_t>(grid, 1)), kFarTile, 0, s>>>(d_inst, ninst,
-                                                                                           pre_buf.as<int64_t>());
-    count_launch();
+    SB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_batch<0>, kFarTile, smem));
+    per_sm = std::max(per_sm, 1);
+    const int64_t sms = device_sm_count(device);
+    const int64_t nf = pre[ninst], nq = pre[2 * (ninst + 1) - 1] + pre[3 * (ninst + 1) - 1];
+    const int64_t* d_pre = pre_buf.as<int64_t>();
+    if (!side || far_per_sm <= 0) {
+        // one launch: every CTA alternates far tiles with near / self items (both lists end together)
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(nf + nq, per_sm * sms));
+        const int near_per_far = static_cast<int>(std::max<int64_t>(1, nf > 0 ? cdiv(nq, nf) : 1));
+        ProfScope prof(SB_PROF_FAR, s);
+        k_assemble_batch<0><<<static_cast<unsigned>(grid), kFarTile, smem, s>>>(d_inst, ninst, d_pre, near_per_far);
+        count_launch();
+        SB_CUDA(cudaGetLastError());
+        return;
+    }
+    // Two persistent launches: the far tiles of every instance on far_per_sm CTA slots per SM, the
+    // near pairs and self elements on the remaining slots (on the high-priority side stream; with
+    // far_per_sm = all of them, its CTAs take the slots the far launch's CTAs free at its end). A
+    // CTA of a persistent launch keeps its slot to the end, so the split is fixed.
+    const int far_slots = std::min(far_per_sm, per_sm);
+    const int near_slots = far_slots < per_sm ? per_sm - far_slots : per_sm;
+    side->ensure();
+    side->begin(s);
+    {
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(nf, far_slots * sms));
+        ProfScope prof(SB_PROF_FAR, s);
+        k_assemble_batch<1><<<static_cast<unsigned>(grid), kFarTile, smem, s>>>(d_inst, ninst, d_pre, 1);
+        count_launch();
+    }
+    {
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(nq, near_slots * sms));
+        ProfScope prof(SB_PROF_NEAR, side->s);
+        k_assemble_batch<2><<<static_cast<unsigned>(grid), kFarTile, smem, side->s>>>(d_inst, ninst, d_pre, 1);
+        count_launch();
+    }
     SB_CUDA(cudaGetLastError());
+    side->end(s);
 }
 
 void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_t s, SideStream& side,

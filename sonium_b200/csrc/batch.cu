@@ -620,7 +620,10 @@ struct Batch {
     // Assembly form: SB_BATCH_ASM_AUTO (the autotuner's choice for this batch shape), _PERSISTENT
     // or _STREAMS; the autotuner's two measurements when it ran for this batch.
     int asm_mode = SB_BATCH_ASM_AUTO, asm_chosen = 0;
+    // Persistent form: far CTA slots per SM of its split form (0 = one launch); set by the autotuner.
+    int asm_split = 3;
     double tune_persistent_ms = 0.0, tune_streams_ms = 0.0;
+    double tune_split_ms[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     SideStream side;
     void reset_graph() {
         for (cudaGraphExec_t e : execs)
@@ -1415,6 +1418,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
                 A.near_col = m->near_col.as<int32_t>();
                 A.near_row = m->near_row.as<int32_t>();
                 A.nnz = m->nnz;
+                A.amax = nullptr;
                 B->asm_h.push_back(A);
                 B->rhs.push_back(reinterpret_cast<double2*>(pr));
                 pr += round256(sizeof(double2) * ((m->n + 1) / 2 * 2));
@@ -1453,15 +1457,19 @@ static std::vector<int64_t> batch_shape_key(const Batch& B) {
     return key;
 }
 
-static int tuned_assembly_form(const Batch& B) {
+// The remembered choice of a batch shape: form + 16 * (far CTA slots per SM of the split
+// persistent form, 0 = its single launch).
+static int tuned_assembly_form(const Batch& B, int* split) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune.find(batch_shape_key(B));
-    return it == g_tune.end() ? SB_BATCH_ASM_AUTO : it->second;
+    if (it == g_tune.end()) return SB_BATCH_ASM_AUTO;
+    *split = it->second / 16;
+    return it->second % 16;
 }
 
-static void remember_assembly_form(const Batch& B, int form) {
+static void remember_assembly_form(const Batch& B, int form, int split) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tune[batch_shape_key(B)] = form;
+    g_tune[batch_shape_key(B)] = form + 16 * split;
 }
 
 SB_API int sb_batch_set_assembly_mode(sb_batch* batch, int mode) {
@@ -1470,6 +1478,16 @@ SB_API int sb_batch_set_assembly_mode(sb_batch* batch, int mode) {
         SB_REQUIRE(mode == SB_BATCH_ASM_AUTO || mode == SB_BATCH_ASM_PERSISTENT || mode == SB_BATCH_ASM_STREAMS,
                    SB_ERR_INVALID_ARGUMENT, "batch: unknown assembly mode");
         batch->b->asm_mode = mode;
+    });
+}
+
+SB_API int sb_batch_assembly_split(const sb_batch* batch, int* far_slots_per_sm, double* layout_ms) {
+    return guarded_batch([&] {
+        SB_REQUIRE(batch && batch->b, SB_ERR_INVALID_ARGUMENT, "batch: null handle");
+        const Batch& B = *batch->b;
+        if (far_slots_per_sm) *far_slots_per_sm = B.asm_split;
+        if (layout_ms)
+            for (int t = 0; t < 5; ++t) layout_ms[t] = B.tune_split_ms[t];
     });
 }
 
@@ -1499,18 +1517,32 @@ SB_API int sb_batch_assemble(sb_batch* batch) {
                 cudaEventDestroy(b);
             }
         } evg{e0, e1};
-        auto run = [&](int form) -> double {
+        auto run = [&](int form, int split) -> double {
             SB_CUDA(cudaEventRecord(e0, B.stream));
             for (int i = 0; i < B.ninst; ++i)
                 coefficients_for(*B.meshes[i], B.phys[i], B.beta[i].x, B.beta[i].y,
                                  const_cast<double*>(B.asm_h[i].coef), B.stream);
+            // With complex-half inner products the kernels also record each matrix's largest part.
+            const bool track = B.inner == SB_INNER_FP16;
+            if (track && !B.pool_half_aux.p) B.pool_half_aux.alloc(sizeof(unsigned) * 4 * B.ninst);
             if (form == SB_BATCH_ASM_PERSISTENT) {
-                assemble_batch(B.asm_h, B.asm_d.as<BatchAsmInst>(), B.pre_asm, B.stream, B.device);
-                B.amax_valid = false;
+                unsigned* aux = track ? B.pool_half_aux.as<unsigned>() : nullptr;
+                bool changed = false;
+                for (int i = 0; i < B.ninst; ++i) {
+                    unsigned* want = aux ? aux + 4 * i : nullptr;
+                    if (B.asm_h[i].amax != want) {
+                        B.asm_h[i].amax = want;
+                        changed = true;
+                    }
+                }
+                if (changed) {
+                    SB_CUDA(cudaStreamSynchronize(B.stream));  // no earlier launch still reads the descriptors
+                    h2d_sync(B.asm_d.p, B.asm_h.data(), sizeof(BatchAsmInst) * B.ninst);
+                }
+                if (aux) SB_CUDA(cudaMemsetAsync(aux, 0, sizeof(unsigned) * 4 * B.ninst, B.stream));
+                assemble_batch(B.asm_h, B.asm_d.as<BatchAsmInst>(), B.pre_asm, B.stream, B.device, &B.side, split);
+                B.amax_valid = track;
             } else {
-                // With complex-half inner products the kernels also record each matrix's largest part.
-                const bool track = B.inner == SB_INNER_FP16;
-                if (track && !B.pool_half_aux.p) B.pool_half_aux.alloc(sizeof(unsigned) * 4 * B.ninst);
                 assemble_batch_streams(B.asm_h, B.stream, B.side, track ? B.pool_half_aux.as<unsigned>() : nullptr);
                 B.amax_valid = track;
             }
@@ -1520,19 +1552,33 @@ SB_API int sb_batch_assemble(sb_batch* batch) {
             SB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             return ms;
         };
-        int form = B.asm_mode;
-        if (form == SB_BATCH_ASM_AUTO) form = tuned_assembly_form(B);
+        int form = B.asm_mode, split = B.asm_split;
+        if (form == SB_BATCH_ASM_AUTO) form = tuned_assembly_form(B, &split);
         if (form == SB_BATCH_ASM_AUTO) {
-            // Autotune: both forms once (each writes the complete matrices), keep the faster one
-            // for every batch of this shape on this device.
-            B.tune_persistent_ms = run(SB_BATCH_ASM_PERSISTENT);
-            B.tune_streams_ms = run(SB_BATCH_ASM_STREAMS);
+            // Autotune, after one untimed assembly (first touches): the persistent form as one launch
+            // and as two launches (far tiles on 4, 3 or 2 CTA slots per SM), and the per-instance
+            // streams form,
+            // each once (every run writes the complete matrices); the fastest is kept for every
+            // batch of this shape on this device.
+            run(SB_BATCH_ASM_STREAMS, 0);
+            double best = 1e300;
+            for (int sp : {0, 4, 3, 2}) {
+                const double t = run(SB_BATCH_ASM_PERSISTENT, sp);
+                B.tune_split_ms[sp] = t;
+                if (t < best) {
+                    best = t;
+                    split = sp;
+                }
+            }
+            B.tune_persistent_ms = best;
+            B.tune_streams_ms = run(SB_BATCH_ASM_STREAMS, 0);
             form = B.tune_streams_ms < B.tune_persistent_ms ? SB_BATCH_ASM_STREAMS : SB_BATCH_ASM_PERSISTENT;
-            remember_assembly_form(B, form);
+            remember_assembly_form(B, form, split);
             B.last_assembly_ms = std::min(B.tune_persistent_ms, B.tune_streams_ms);
         } else {
-            B.last_assembly_ms = run(form);
+            B.last_assembly_ms = run(form, split);
         }
+        B.asm_split = split;
         B.asm_chosen = form;
         B.assembled = true;
         B.half_valid = false;

@@ -242,9 +242,13 @@ struct BatchAsmInst {
     const int32_t* near_col;
     const int32_t* near_row;
     int64_t nnz;
+    unsigned* amax;  // when set: the largest |re|, |im| written (FP32 bits), for the complex-half copy
 };
+// The persistent form: one launch over every instance's far tiles, near pairs and self elements
+// (far_per_sm = 0), or two persistent launches side by side, the far tiles on far_per_sm CTA slots
+// per SM and the near / self items on the rest (side stream).
 void assemble_batch(const std::vector<BatchAsmInst>& h_inst, const BatchAsmInst* d_inst, DevBuf& pre_buf,
-                    cudaStream_t s, int device);
+                    cudaStream_t s, int device, SideStream* side = nullptr, int far_per_sm = 0);
 // The same batch as per-instance launches: far tiles on s, near pairs and self terms on the side
 // stream (same device functions, so the same entries).
 // With amax, instance b's largest matrix part lands in amax[4 b] (float bits; the complex-half

@@ -70,6 +70,14 @@ class SweepBatch:
         check(L.load().sb_batch_assembly_tuning(self.handle, ct.byref(c), ct.byref(a), ct.byref(b)))
         return c.value, a.value, b.value
 
+    def assembly_split(self):
+        """(far CTA slots per SM of the persistent form's two-launch layout, 0 = one launch;
+        {layout: autotuner ms}, layouts "one_launch", "far_2", "far_3", "far_4", 0 when it did not run)."""
+        c = ct.c_int()
+        t = np.zeros(5, np.float64)
+        check(L.load().sb_batch_assembly_split(self.handle, ct.byref(c), _p(t)))
+        return c.value, {"one_launch": t[0], "far_2": t[2], "far_3": t[3], "far_4": t[4]}
+
     def set_inner_precision(self, inner: int) -> None:
         """SB_INNER_FP32 (the complex64 matrices) or SB_INNER_FP16 (complex-half copies, built by
         the first solve after each assembly; pair with IrConfig(inner_tolerance=1e-3))."""
