@@ -16,18 +16,21 @@
 //   Re Y_ic = D[2i][c] - D[2i+1][128+c],   Im Y_ic = D[2i][128+c] + D[2i+1][c],
 // combined in the epilogue between neighbouring TMEM lanes with one shuffle.
 //
-// Kernel structure: one CTA per (128 Ahat rows, 128 right-hand sides); 4 warps. Warp 0 allocates
-// 256 TMEM columns (the 128 x 256 FP32 accumulator), lane 0 of warp 0 issues the TMA loads of a
-// four-stage ring (per stage: Ahat hi/lo 128 x 32 and Xhat hi/lo 256 x 32 BF16 tiles, 64-byte
-// swizzle, 48 KB), lane 0 of warp 1 issues 6 MMAs (128 x 256 x 16) per stage and commits them to
-// the stage's "empty" barrier; after the last stage all four warps read the accumulator
-// (tcgen05.ld) and write Y. Consecutive CTAs take the right-hand-side blocks of one row tile, so
-// the second read of an Ahat tile comes from L2. All waits are bounded; a timeout records an
-// error in the status word, skips the stores and still releases tensor memory.
+// Kernel structure: persistent, one CTA per SM walking the work units (128 Ahat rows, 128
+// right-hand sides, K half; right-hand-side block fastest, so the CTAs running side by side read an
+// Ahat tile's second use from L2). 6 warps: lane 0 of warp 0 issues the TMA loads of a four-stage
+// ring that runs on across units (per stage: Ahat hi/lo 128 x 32 and Xhat hi/lo 256 x 32 BF16
+// tiles, 64-byte swizzle, 48 KB), lane 0 of warp 1 issues 6 MMAs (128 x 256 x 16) per stage and
+// commits them to the stage's "empty" barrier, and warps 2-5 read the accumulator (tcgen05.ld) and
+// write Y. TMEM holds two 128 x 256 FP32 accumulators (all 512 columns) used by alternate units,
+// so the epilogue of one unit overlaps the K loop of the next. All waits are bounded; a timeout
+// records an error in the status word, skips the stores, waits for its copies and MMAs in flight
+// and still releases tensor memory.
 
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "sb_device.cuh"
@@ -56,30 +59,48 @@ constexpr int kErrTimeoutProducer = 1;
 constexpr int kErrTimeoutMma = 2;
 constexpr int kErrTimeoutEpilogue = 4;
 
-__global__ void __launch_bounds__(128, 1)
+// Persistent: grid = one CTA per SM; the CTA walks the work units u = blockIdx.x + t gridDim.x
+// (unit = right-hand-side block fastest, then row tile, then K half). 6 warps: warp 0 lane 0 the
+// TMA producer (the stage ring runs on across units), warp 1 lane 0 the MMA issuer, warps 2-5 the
+// epilogue. Two 256-column accumulators (all 512 TMEM columns) alternate between units, so the
+// epilogue of unit t overlaps the K loop of unit t + 1.
+constexpr int kPThreads = 192;
+constexpr uint32_t kPTmemCols = 2 * kTmemCols;
+
+__device__ __forceinline__ void unit_coords(int64_t u, int rblocks, int mtiles, int& rb, int& mt, int& kz) {
+    rb = static_cast<int>(u % rblocks);
+    const int64_t rest = u / rblocks;
+    mt = static_cast<int>(rest % mtiles);
+    kz = static_cast<int>(rest / mtiles);
+}
+
+__global__ void __launch_bounds__(kPThreads, 1)
     k_block_bf16x3(const __grid_constant__ CUtensorMap tm_a_hi, const __grid_constant__ CUtensorMap tm_a_lo,
                    const __grid_constant__ CUtensorMap tm_x_hi, const __grid_constant__ CUtensorMap tm_x_lo,
                    int ldk, int64_t n, int r, float* __restrict__ y, int64_t ldy, int* __restrict__ status,
-                   const int* __restrict__ block_gate, int ksplit) {
+                   const int* __restrict__ block_gate, int ksplit, int rblocks, int mtiles) {
 #if defined(__CUDA_ARCH__)
-    // A group of right-hand sides with nothing left to compute: the whole CTA returns before it
-    // allocates or initialises anything.
-    if (block_gate && block_gate[blockIdx.x] == 0) return;
     using namespace umma;
     extern __shared__ uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], acc_bar;
+    __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], acc_full[2], acc_empty[2], final_bar;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
     __shared__ volatile int consumed;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rblock = blockIdx.x, mtile = blockIdx.y;
     const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    const int64_t units = (int64_t)rblocks * mtiles * ksplit;
+    const int nkb_all = ldk / kTileK;
+    const int per = (nkb_all + ksplit - 1) / ksplit;
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(smem_u32(&full_bar[s]), 1);
             mbar_init(smem_u32(&empty_bar[s]), 1);
         }
-        mbar_init(smem_u32(&acc_bar), 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&acc_full[b]), 1);
+            mbar_init(smem_u32(&acc_empty[b]), 4);
+        }
+        mbar_init(smem_u32(&final_bar), 1);
         mbar_fence_init();
         abort_flag = 0;
         consumed = 0;
@@ -88,106 +109,156 @@ __global__ void __launch_bounds__(128, 1)
         prefetch_tmap(&tm_x_hi);
         prefetch_tmap(&tm_x_lo);
     }
-    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), kTmemCols);
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), kPTmemCols);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tacc = tmem_base;
-    // K blocks of this CTA: split blockIdx.z of ksplit; partial sums are added into y (zeroed by the
-    // host), two of them exactly (fl(a + b) either order), so the result does not depend on timing.
-    const int nkb_all = ldk / kTileK;
-    const int per = (nkb_all + ksplit - 1) / ksplit;
-    const int kb0 = blockIdx.z * per;
-    const int nkb = (nkb_all - kb0) < per ? (nkb_all - kb0) : per;
     int err = 0;
-    if (warp == 0 && lane == 0) {
-        // TMA producer
-        int issued = 0;
-        for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb % kStages, use = kb / kStages;
-            if (kb >= kStages && !mbar_wait(smem_u32(&empty_bar[s]), (use - 1) & 1)) {
-                err |= kErrTimeoutProducer;
-                abort_flag = 1;
-                break;
-            }
-            if (abort_flag) break;
-            const uint32_t st = base + s * kStageBytes;
-            const uint32_t fb = smem_u32(&full_bar[s]);
-            mbar_expect_tx(fb, kStageBytes);
-            const int kx = (kb0 + kb) * kTileK;
-            tma_load_2d(st, &tm_a_hi, fb, kx, mtile * kTileM);
-            tma_load_2d(st + kABytes, &tm_a_lo, fb, kx, mtile * kTileM);
-            tma_load_2d(st + 2 * kABytes, &tm_x_hi, fb, kx, rblock * 2 * kTileRhs);
-            tma_load_2d(st + 2 * kABytes + kXBytes, &tm_x_lo, fb, kx, rblock * 2 * kTileRhs);
-            ++issued;
-        }
-        // Loads still in flight land before the CTA may exit.
-        if (abort_flag) {
-            __threadfence_block();
-            for (int kb = consumed; kb < issued; ++kb)
-                if (!mbar_wait(smem_u32(&full_bar[kb % kStages]), (kb / kStages) & 1)) err |= kErrTimeoutProducer;
-        }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        const uint32_t idesc = instr_desc_bf16_f32(kTileM, 2 * kTileRhs);
-        for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb % kStages, use = kb / kStages;
-            if (abort_flag || !mbar_wait(smem_u32(&full_bar[s]), use & 1)) {
-                if (!abort_flag) err |= kErrTimeoutMma;
-                abort_flag = 1;
-                break;
-            }
-            consumed = kb + 1;
-            tc_fence_after();
-            const uint32_t st = base + s * kStageBytes;
-#pragma unroll
-            for (int kk = 0; kk < kTileK / 16; ++kk) {
-                const uint64_t a_hi = smem_desc_k_sw64(st + kk * 32);
-                const uint64_t a_lo = smem_desc_k_sw64(st + kABytes + kk * 32);
-                const uint64_t x_hi = smem_desc_k_sw64(st + 2 * kABytes + kk * 32);
-                const uint64_t x_lo = smem_desc_k_sw64(st + 2 * kABytes + kXBytes + kk * 32);
-                mma_bf16(tacc, a_hi, x_hi, idesc, (kb | kk) != 0 ? 1u : 0u);
-                mma_bf16(tacc, a_hi, x_lo, idesc, 1u);
-                mma_bf16(tacc, a_lo, x_hi, idesc, 1u);
-            }
-            mma_commit(smem_u32(&empty_bar[s]));
-        }
-        // Tracks every MMA issued above, on the normal and on the error path.
-        mma_commit(smem_u32(&acc_bar));
-    }
-    // Epilogue: all four warps.
-    __syncwarp();
-    const bool done = mbar_wait(smem_u32(&acc_bar), 0);
-    if (!done) err |= kErrTimeoutEpilogue;
-    tc_fence_after();
-    // tcgen05.ld is warp-collective: the decision to read the accumulator is made per warp.
-    if (__all_sync(0xffffffffu, done && !abort_flag)) {
-        const int t = warp * 32 + lane;                 // TMEM lane = Ahat row within the tile
-        const int64_t row = (int64_t)mtile * kTileM + t;
-        const int64_t i = row >> 1;
-        const int parity = static_cast<int>(row & 1);
-        const uint32_t lane_addr = tacc + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-        for (int g = 0; g < kTileRhs / 32; ++g) {
-            float a[32], b[32];
-            tmem_ld32(lane_addr + g * 32, a);              // D[t][c]       (Re X part)
-            tmem_ld32(lane_addr + kTileRhs + g * 32, b);   // D[t][128 + c] (Im X part)
-#pragma unroll
-            for (int c = 0; c < 32; ++c) {
-                const float v = __shfl_xor_sync(0xffffffffu, b[c], 1);
-                const float out = parity ? a[c] + v : a[c] - v;
-                const int rhs = rblock * kTileRhs + g * 32 + c;
-                if (i < n && rhs < r) {
-                    float* dst = y + ((int64_t)rhs * ldy + i) * 2 + parity;
-                    if (ksplit > 1) atomicAdd(dst, out);
-                    else *dst = out;
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer: every unit's K blocks, one ring across the units.
+            int issued = 0;
+            bool stop = false;
+            for (int64_t u = blockIdx.x; u < units && !stop; u += gridDim.x) {
+                int rb, mt, kz;
+                unit_coords(u, rblocks, mtiles, rb, mt, kz);
+                if (block_gate && block_gate[rb] == 0) continue;
+                const int kb0 = kz * per;
+                const int nkb = min(per, nkb_all - kb0);
+                for (int kb = 0; kb < nkb; ++kb) {
+                    const int s = issued % kStages, use = issued / kStages;
+                    if (issued >= kStages && !mbar_wait(smem_u32(&empty_bar[s]), (use - 1) & 1)) {
+                        err |= kErrTimeoutProducer;
+                        abort_flag = 1;
+                    }
+                    if (abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    const uint32_t st = base + s * kStageBytes;
+                    const uint32_t fb = smem_u32(&full_bar[s]);
+                    mbar_expect_tx(fb, kStageBytes);
+                    const int kx = (kb0 + kb) * kTileK;
+                    tma_load_2d(st, &tm_a_hi, fb, kx, mt * kTileM);
+                    tma_load_2d(st + kABytes, &tm_a_lo, fb, kx, mt * kTileM);
+                    tma_load_2d(st + 2 * kABytes, &tm_x_hi, fb, kx, rb * 2 * kTileRhs);
+                    tma_load_2d(st + 2 * kABytes + kXBytes, &tm_x_lo, fb, kx, rb * 2 * kTileRhs);
+                    ++issued;
                 }
             }
+            // Loads still in flight land before the CTA may exit.
+            if (abort_flag) {
+                __threadfence_block();
+                for (int q = consumed; q < issued; ++q)
+                    if (!mbar_wait(smem_u32(&full_bar[q % kStages]), (q / kStages) & 1)) err |= kErrTimeoutProducer;
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer: unit t into accumulator t & 1, once the epilogue has read it out.
+            const uint32_t idesc = instr_desc_bf16_f32(kTileM, 2 * kTileRhs);
+            int g = 0, t = 0;
+            bool stop = false;
+            for (int64_t u = blockIdx.x; u < units && !stop; u += gridDim.x) {
+                int rb, mt, kz;
+                unit_coords(u, rblocks, mtiles, rb, mt, kz);
+                if (block_gate && block_gate[rb] == 0) continue;
+                const int buf = t & 1;
+                if (t >= 2 && (abort_flag || !mbar_wait(smem_u32(&acc_empty[buf]), ((t >> 1) - 1) & 1))) {
+                    if (!abort_flag) err |= kErrTimeoutMma;
+                    abort_flag = 1;
+                    mma_commit(smem_u32(&acc_full[buf]));  // the epilogue wakes and sees the flag
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t acc = tacc + buf * kTmemCols;
+                const int nkb = min(per, nkb_all - kz * per);
+                for (int kb = 0; kb < nkb; ++kb) {
+                    const int s = g % kStages;
+                    if (abort_flag || !mbar_wait(smem_u32(&full_bar[s]), (g / kStages) & 1)) {
+                        if (!abort_flag) err |= kErrTimeoutMma;
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    consumed = g + 1;
+                    tc_fence_after();
+                    const uint32_t st = base + s * kStageBytes;
+#pragma unroll
+                    for (int kk = 0; kk < kTileK / 16; ++kk) {
+                        const uint64_t a_hi = smem_desc_k_sw64(st + kk * 32);
+                        const uint64_t a_lo = smem_desc_k_sw64(st + kABytes + kk * 32);
+                        const uint64_t x_hi = smem_desc_k_sw64(st + 2 * kABytes + kk * 32);
+                        const uint64_t x_lo = smem_desc_k_sw64(st + 2 * kABytes + kXBytes + kk * 32);
+                        mma_bf16(acc, a_hi, x_hi, idesc, (kb | kk) != 0 ? 1u : 0u);
+                        mma_bf16(acc, a_hi, x_lo, idesc, 1u);
+                        mma_bf16(acc, a_lo, x_hi, idesc, 1u);
+                    }
+                    mma_commit(smem_u32(&empty_bar[s]));
+                    ++g;
+                }
+                // The unit's accumulator is complete (on the error path: the epilogue wakes and
+                // sees the abort flag).
+                mma_commit(smem_u32(&acc_full[buf]));
+                ++t;
+            }
+            // Every MMA issued above has completed before tensor memory is released.
+            mma_commit(smem_u32(&final_bar));
+            if (!mbar_wait(smem_u32(&final_bar), 0)) err |= kErrTimeoutMma;
+        }
+        __syncwarp();
+    } else {
+        // Epilogue: warps 2..5; warp w reads TMEM lanes 32 (w % 4) .. + 31.
+        const int quad = warp & 3;
+        const int tl = quad * 32 + lane;  // TMEM lane = Ahat row within the tile
+        int t = 0;
+        for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+            int rb, mt, kz;
+            unit_coords(u, rblocks, mtiles, rb, mt, kz);
+            if (block_gate && block_gate[rb] == 0) continue;
+            if (abort_flag) break;
+            const int buf = t & 1;
+            const bool ok = mbar_wait(smem_u32(&acc_full[buf]), (t >> 1) & 1);
+            if (!ok) {
+                err |= kErrTimeoutEpilogue;
+                abort_flag = 1;
+            }
+            tc_fence_after();
+            // tcgen05.ld is warp-collective: the decision to read the accumulator is made per warp.
+            if (__all_sync(0xffffffffu, ok && !abort_flag)) {
+                const int64_t row = (int64_t)mt * kTileM + tl;
+                const int64_t i = row >> 1;
+                const int parity = static_cast<int>(row & 1);
+                const uint32_t lane_addr = tacc + buf * kTmemCols + ((uint32_t)(quad * 32) << 16);
+#pragma unroll 1
+                for (int gq = 0; gq < kTileRhs / 32; ++gq) {
+                    float a[32], b[32];
+                    tmem_ld32(lane_addr + gq * 32, a);              // D[t][c]       (Re X part)
+                    tmem_ld32(lane_addr + kTileRhs + gq * 32, b);   // D[t][128 + c] (Im X part)
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        const float v = __shfl_xor_sync(0xffffffffu, b[c], 1);
+                        const float out = parity ? a[c] + v : a[c] - v;
+                        const int rhs = rb * kTileRhs + gq * 32 + c;
+                        if (i < n && rhs < r) {
+                            float* dst = y + ((int64_t)rhs * ldy + i) * 2 + parity;
+                            if (ksplit > 1) atomicAdd(dst, out);
+                            else *dst = out;
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&acc_empty[buf]));
+            ++t;
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tacc, kTmemCols);
+    if (warp == 0) tmem_dealloc(tacc, kPTmemCols);
     if (err) atomicOr(status, err);
 #endif
 }
@@ -375,11 +446,12 @@ void tensor_block_product(const Operator& op, const float2* x, int64_t ldx, int 
     if (ksplit > 1)
         SB_CUDA(cudaMemset2DAsync(y, sizeof(float2) * ldy, 0, sizeof(float2) * w->n, r, s));
     ProfScope prof(SB_PROF_TENSOR, s);
-    const dim3 grid(static_cast<unsigned>(rblocks), static_cast<unsigned>(w->rows / kTileM),
-                    static_cast<unsigned>(ksplit));
-    k_block_bf16x3<<<grid, 128, kSmemBytes, s>>>(w->tm_a_hi, w->tm_a_lo, w->tm_x_hi, w->tm_x_lo,
-                                                  static_cast<int>(w->ldk), w->n, r, reinterpret_cast<float*>(y), ldy,
-                                                  w->status.as<int>(), block_gate, ksplit);
+    const int mtiles = static_cast<int>(w->rows / kTileM);
+    const int64_t units = ctas * ksplit;
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(units, device_sm_count(op.device)));
+    k_block_bf16x3<<<grid, kPThreads, kSmemBytes, s>>>(w->tm_a_hi, w->tm_a_lo, w->tm_x_hi, w->tm_x_lo,
+                                                        static_cast<int>(w->ldk), w->n, r, reinterpret_cast<float*>(y),
+                                                        ldy, w->status.as<int>(), block_gate, ksplit, rblocks, mtiles);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }
