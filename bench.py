@@ -85,6 +85,8 @@ def parse():
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-RHS leg in the default run")
     ap.add_argument("--no-precision-form", action="store_true",
                     help="skip the N = 81920, k = 40 precision-form leg (~165 GB) in the default run")
+    ap.add_argument("--no-gemv-bar", action="store_true",
+                    help="skip the cuBLAS Cgemv / Zgemv comparison of the matrix-vector products")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the leg that times the reference's own CUDA assembly kernel beside ours")
     ap.add_argument("--precision-form", action="store_true",
@@ -546,6 +548,8 @@ def main():
         extra_legs["precision_form"] = precision_leg(sb, a, dist, dev, rt, reps=1)
     if not a.no_ref_gpu:
         extra_legs["reference_gpu_assembly"] = reference_gpu_leg(sb, L, lib, dev)
+    if not a.no_gemv_bar:
+        extra_legs["gemv_bar"] = gemv_bar_leg(sb, L, lib, dev, rt)
 
     # ---- roofline of the dominant kernel of the headline step ----
     pk, pk_kind = peaks()
@@ -689,12 +693,78 @@ def main():
     if "N1280_k2_all_pairs" in rg:
         summ["reference_gpu_assembly_speedup_per_pair"] = {
             kk: round(rg[kk]["speedup_per_pair"], 1) for kk in ("N1280_k2_all_pairs", "N20480_k10_rows0_128") if kk in rg}
+    gb = extra_legs.get("gemv_bar") or {}
+    if "c64" in gb:
+        summ["gemv_vs_cublas"] = {kk: round(gb[kk]["ours_over_cublas"], 3) for kk in ("c64", "c128")}
     line["summary"] = summ
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
     rt.cudaFree(b_d)
     rt.cudaFree(x_d)
     dist.close()
+
+
+def gemv_bar_leg(sb, L, lib, dev, rt, reps=20):
+    """The matrix-vector products against cuBLAS on the same device (the reference's backend calls
+    cublasCgemv / cublasZgemv, crates/sonium-compute/src/cuda/cublas_blas23.rs:126,165): at the
+    config-2 size (N = 20480), torch.mv on random complex64 / complex128 device matrices (cuBLAS)
+    and this library's product on the assembled complex64 / complex128 operators of the headline
+    mesh (sb_operator_apply_device, complex128 vectors), each timed over back-to-back calls between
+    CUDA events after warm-up; matrix bytes per product over the time, against the measured HBM
+    copy bandwidth."""
+    import torch
+
+    n = 20 * 4 ** LEVEL
+    pk, pk_kind = peaks()
+    out = {"n": n, "peak_gbs": pk["hbm_gbs"], "peak_source": pk_kind}
+    torch.cuda.set_device(dev)
+    for key, dt in (("c64", torch.complex64), ("c128", torch.complex128)):
+        A = torch.randn(n, n, dtype=dt, device=f"cuda:{dev}")
+        x = torch.randn(n, dtype=dt, device=f"cuda:{dev}")
+        for _ in range(3):
+            y = torch.mv(A, x)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            y = torch.mv(A, x)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        nbytes = A.element_size() * n * n
+        out[key] = {"cublas_ms": ms, "cublas_gbs": nbytes / ms / 1e6}
+        del A, x, y
+        torch.cuda.empty_cache()
+    nodes, tris = sb.icosphere(RADIUS, LEVEL)
+    mesh = sb.Mesh(nodes, tris, device=dev)
+    ph = sb.PhysicsParams.for_wavenumber(K)
+    beta = ph.burton_miller_beta()
+    xv = np.ascontiguousarray(np.exp(1j * np.arange(n) * 0.37))
+    x_d, y_d = _dev_alloc(rt, xv.nbytes), _dev_alloc(rt, xv.nbytes)
+    rt.cudaMemcpy(x_d, xv.ctypes.data, xv.nbytes, 1)
+    e0, e1 = ct.c_void_p(), ct.c_void_p()
+    L.check(lib.sb_event_create(ct.byref(e0)))
+    L.check(lib.sb_event_create(ct.byref(e1)))
+    for key, prec, esize in (("c64", sb.SB_PRECISION_FP32, 8), ("c128", sb.SB_PRECISION_FP64, 16)):
+        op = sb.build_tbem_system_with_beta(mesh, ph, beta, prec)
+        for _ in range(3):
+            L.check(lib.sb_operator_apply_device(op.handle, 0, x_d, y_d))
+        L.check(lib.sb_event_record(e0, op.handle))
+        for _ in range(reps):
+            L.check(lib.sb_operator_apply_device(op.handle, 0, x_d, y_d))
+        L.check(lib.sb_event_record(e1, op.handle))
+        ems = ct.c_float()
+        L.check(lib.sb_event_elapsed_ms(e0, e1, ct.byref(ems)))
+        ms = ems.value / reps
+        gbs = esize * n * n / ms / 1e6
+        out[key].update({"ours_ms": ms, "ours_gbs": gbs, "ours_over_cublas": out[key]["cublas_ms"] / ms,
+                         "ours_frac": gbs / pk["hbm_gbs"], "cublas_frac": out[key]["cublas_gbs"] / pk["hbm_gbs"]})
+        op.close()
+    lib.sb_event_destroy(e0)
+    lib.sb_event_destroy(e1)
+    rt.cudaFree(x_d)
+    rt.cudaFree(y_d)
+    mesh.close()
+    return out
 
 
 def reference_gpu_leg(sb, L, lib, dev):

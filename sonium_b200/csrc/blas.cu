@@ -289,13 +289,22 @@ __global__ void __launch_bounds__(256) k_project(const T* __restrict__ V, int64_
     }
 }
 
-__global__ void k_sum_real(const double* __restrict__ part, int64_t m, double* __restrict__ out,
-                           Gate gate) {
+// One CTA sums m partial norms (m up to one per row of the residual products).
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_sum_real(const double* __restrict__ part, int64_t m,
+                                                          double* __restrict__ out, Gate gate) {
     if (closed(gate)) return;
+    __shared__ double red[kSumThreads / 32];
     double s = 0.0;
-    for (int64_t c = threadIdx.x; c < m; c += 32) s += part[c];
+    for (int64_t c = threadIdx.x; c < m; c += kSumThreads) s += part[c];
     s = warp_sum(s);
-    if (threadIdx.x == 0) *out = s;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < kSumThreads / 32 ? red[threadIdx.x] : 0.0;
+        s = warp_sum(s);
+        if (threadIdx.x == 0) *out = s;
+    }
 }
 
 // y = alpha * x with type conversion; alpha from the host, or *alpha_dev when given.
@@ -354,12 +363,27 @@ __global__ void k_jacobi(const double2* __restrict__ d, const T* __restrict__ x,
 // Host launchers
 // ---------------------------------------------------------------------------------------------
 
+// Launch shapes of the single-operator products (rows per CTA, 16-byte loads in flight per row
+// and thread; 256 threads). Measured at N = 20480 on B200 against 4 rows x 2 loads: the complex128
+// product 1 x 4 (0.93-0.99 ms, 4 x 2 0.98-1.02 ms); the complex64 product with FP32 vectors
+// 1 x 4 (0.49 ms, 4 x 2 0.51-0.52 ms) and with FP64 vectors 2 x 4 (0.49-0.53 ms, 4 x 2
+// 0.55-0.60 ms: its x is twice the row's bytes, so two rows share each x load). Few rows and many
+// CTAs keep more loads in flight per SM than wide row blocks with their register cost.
+constexpr int kGemv128Rows = 1, kGemv128Unroll = 4;
+constexpr int kGemv64Rows = 1, kGemv64Unroll = 4;
+constexpr int kGemvX64Rows = 2, kGemvX64Unroll = 4;
+// gemv_partials counts the partial norms of both the complex128 and the FP32-vector complex64
+// residuals, and callers size partial-norm buffers by it for every residual product.
+static_assert(kGemv64Rows == kGemv128Rows, "one partial count for the c128 and c64 residuals");
+static_assert(kGemvX64Rows >= kGemv128Rows && kGemv16Rows >= kGemv128Rows,
+              "gemv_partials bounds every residual's partial count");
+
 void gemv_c128(const double2* A, int64_t n, const double2* x, double2* y, Trans t,
                cudaStream_t s, DevBuf& scratch, Gate gate) {
     ProfScope prof(SB_PROF_GEMV64, s);
     if (t == Trans::N) {
-        k_gemv_n_c128<kGemvRows, kGemvThreads, kGemvUnroll>
-            <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, y, nullptr, nullptr, gate);
+        k_gemv_n_c128<kGemv128Rows, kGemvThreads, kGemv128Unroll>
+            <<<cdiv(n, kGemv128Rows), kGemvThreads, 0, s>>>(A, n, x, y, nullptr, nullptr, gate);
         count_launch();
         SB_CUDA(cudaGetLastError());
         return;
@@ -385,31 +409,28 @@ void gemv_c128(const double2* A, int64_t n, const double2* x, double2* y, Trans 
 void gemv_residual_c128(const double2* A, int64_t n, const double2* x, const double2* b,
                         double2* r, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV64, s);
-    k_gemv_n_c128<kGemvRows, kGemvThreads, kGemvUnroll>
-        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, x, r, b, part, gate);
+    k_gemv_n_c128<kGemv128Rows, kGemvThreads, kGemv128Unroll>
+        <<<cdiv(n, kGemv128Rows), kGemvThreads, 0, s>>>(A, n, x, r, b, part, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }
-int64_t gemv_partials(int64_t n) { return cdiv(n, kGemvRows); }
+int64_t gemv_partials(int64_t n) { return cdiv(n, kGemv128Rows); }
 
 void gemv_c64(const float2* A, int64_t n, int64_t lda, const float2* x, float2* y,
               const float2* b, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV32, s);
-    k_gemv_n_c64<kGemvRows, kGemvThreads, kGemvUnroll, false>
-        <<<cdiv(n, kGemvRows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part, gate);
+    k_gemv_n_c64<kGemv64Rows, kGemvThreads, kGemv64Unroll, false>
+        <<<cdiv(n, kGemv64Rows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
-// Rows a CTA of the FP64-vector product (measured at N = 20480: 8 rows, which halve its x traffic
-// from L2, made the mixed solve 0.3 ms slower than 4).
-constexpr int kGemvX64Rows = 4;
 int64_t gemv_x64_partials(int64_t n) { return cdiv(n, kGemvX64Rows); }
 
 void gemv_c64_x64(const float2* A, int64_t n, int64_t lda, const double2* x, double2* y,
                   const double2* b, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV32, s);
-    k_gemv_n_c64<kGemvX64Rows, kGemvThreads, kGemvUnroll, true>
+    k_gemv_n_c64<kGemvX64Rows, kGemvThreads, kGemvX64Unroll, true>
         <<<cdiv(n, kGemvX64Rows), kGemvThreads, 0, s>>>(A, n, lda, x, y, b, part, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
@@ -572,13 +593,13 @@ void arnoldi_project(const T* V, int64_t ldv, int k, const double2* coeff, T* w,
     count_launch();
     SB_CUDA(cudaGetLastError());
     if (cnt) return;
-    k_sum_real<<<1, 32, 0, s>>>(part, nb, out_norm2, gate);
+    k_sum_real<<<1, kSumThreads, 0, s>>>(part, nb, out_norm2, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }
 
 void sum_real(const double* part, int64_t m, double* out, cudaStream_t s, Gate gate) {
-    k_sum_real<<<1, 32, 0, s>>>(part, m, out, gate);
+    k_sum_real<<<1, kSumThreads, 0, s>>>(part, m, out, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }

@@ -17,7 +17,8 @@
 
 namespace sb {
 
-// Launch shape of the matrix-vector products: rows per CTA, threads per CTA, loads in flight.
+// Launch shape of the batched solver's complex64 products (rows per CTA, threads per CTA, loads
+// in flight); the single-operator products set their own row and load counts on these threads.
 constexpr int kGemvRows = 4;
 constexpr int kGemvThreads = 256;
 constexpr int kGemvUnroll = 2;
