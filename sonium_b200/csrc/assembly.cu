@@ -250,16 +250,59 @@ __device__ __forceinline__ double near_threshold(double area) {
 }
 
 constexpr int kNearRows = 32;
+constexpr int kNearCols = 256;  // columns per chunk of the classifier, one per thread
+
+// Bounds of every chunk of kNearCols columns: box[8 t + 0..2] the lower and [8 t + 3..5] the upper
+// corner of the chunk's level-0 subdivision centres, [8 t + 6] its largest near threshold.
+__global__ void __launch_bounds__(kNearCols) k_near_chunk_bounds(const double* __restrict__ elem, int64_t n,
+                                                                 int64_t ld, double* __restrict__ box) {
+    __shared__ double red[kNearCols / 32][7];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t j = blockIdx.x * (int64_t)kNearCols + tid;
+    double v[7];
+    if (j < n) {
+        v[0] = v[3] = E(EGX, j);
+        v[1] = v[4] = E(EGY, j);
+        v[2] = v[5] = E(EGZ, j);
+        v[6] = near_threshold(E(EAREA, j));
+    } else {
+        v[0] = v[1] = v[2] = INFINITY;
+        v[3] = v[4] = v[5] = v[6] = -INFINITY;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = fmin(v[c], __shfl_xor_sync(0xffffffffu, v[c], o));
+#pragma unroll
+        for (int c = 3; c < 7; ++c) v[c] = fmax(v[c], __shfl_xor_sync(0xffffffffu, v[c], o));
+    }
+    if (lane == 0)
+        for (int c = 0; c < 7; ++c) red[warp][c] = v[c];
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < kNearCols / 32; ++w) {
+            for (int c = 0; c < 3; ++c) v[c] = fmin(v[c], red[w][c]);
+            for (int c = 3; c < 7; ++c) v[c] = fmax(v[c], red[w][c]);
+        }
+        for (int c = 0; c < 7; ++c) box[8 * blockIdx.x + c] = v[c];
+        box[8 * blockIdx.x + 7] = 0.0;
+    }
+}
 
 // Near-pair classification, one CTA per 32 source rows. pass 0 counts per row, pass 1 writes
-// the column indices in increasing order (row_ptr from the host-side scan).
-__global__ void __launch_bounds__(256) k_near_pass(const double* __restrict__ elem, int64_t n,
-                                                   int64_t ld, int pass,
-                                                   int64_t* __restrict__ counts,
-                                                   const int64_t* __restrict__ row_ptr,
-                                                   int32_t* __restrict__ cols) {
+// the column indices in increasing order and the row of every pair (row_ptr from the scan). A
+// chunk of columns whose box lies farther from the box of the CTA's rows than its largest
+// threshold allows is skipped: every pair in it would test far (the 1e-9 margin covers the
+// rounding of both squared distances), so both passes and the decisions stay those of the full
+// test.
+__global__ void __launch_bounds__(kNearCols) k_near_pass(const double* __restrict__ elem, int64_t n,
+                                                         int64_t ld, int pass, const double* __restrict__ box,
+                                                         int64_t* __restrict__ counts,
+                                                         const int64_t* __restrict__ row_ptr,
+                                                         int32_t* __restrict__ cols, int32_t* __restrict__ rows) {
     __shared__ double sx[kNearRows][3];
-    __shared__ unsigned sball[8][kNearRows];
+    __shared__ double srb[6];
+    __shared__ unsigned sball[kNearCols / 32][kNearRows];
     __shared__ int64_t sbase[kNearRows];
     __shared__ int scount[kNearRows];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -271,7 +314,27 @@ __global__ void __launch_bounds__(256) k_near_pass(const double* __restrict__ el
         sbase[tid] = (pass == 1 && i < n) ? row_ptr[i] : 0;
     }
     __syncthreads();
-    for (int64_t c0 = 0; c0 < n; c0 += 256) {
+    if (tid == 0) {
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int r = 0; r < kNearRows && row0 + r < n; ++r)
+            for (int c = 0; c < 3; ++c) {
+                lo[c] = fmin(lo[c], sx[r][c]);
+                hi[c] = fmax(hi[c], sx[r][c]);
+            }
+        for (int c = 0; c < 3; ++c) {
+            srb[c] = lo[c];
+            srb[3 + c] = hi[c];
+        }
+    }
+    __syncthreads();
+    for (int64_t c0 = 0; c0 < n; c0 += kNearCols) {
+        const double* B = box + 8 * (c0 / kNearCols);
+        double gap2 = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            const double g = fmax(0.0, fmax(B[c] - srb[3 + c], srb[c] - B[3 + c]));
+            gap2 += g * g;
+        }
+        if (gap2 > B[6] * (1.0 + 1e-9)) continue;  // the same decision in every thread
         const int64_t j = c0 + tid;
         double gx = 0, gy = 0, gz = 0, thr = -1.0;
         if (j < n) {
@@ -300,12 +363,13 @@ __global__ void __launch_bounds__(256) k_near_pass(const double* __restrict__ el
                     for (int w = 0; w < warp; ++w) pos += __popc(sball[w][r]);
                     pos += __popc(b & ((1u << lane) - 1u));
                     cols[pos] = static_cast<int32_t>(j);
+                    rows[pos] = static_cast<int32_t>(row0 + r);
                 }
             }
             __syncthreads();
             if (tid < kNearRows) {
                 int64_t t = 0;
-                for (int w = 0; w < 8; ++w) t += __popc(sball[w][tid]);
+                for (int w = 0; w < kNearCols / 32; ++w) t += __popc(sball[w][tid]);
                 sbase[tid] += t;
             }
             __syncthreads();
@@ -313,6 +377,46 @@ __global__ void __launch_bounds__(256) k_near_pass(const double* __restrict__ el
     }
     __syncthreads();
     if (pass == 0 && tid < kNearRows && row0 + tid < n) counts[row0 + tid] = scount[tid];
+}
+
+// Exclusive scan of the per-row pair counts into the CSR row pointers (one CTA): ptr[n] = *total
+// = the number of pairs.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) k_scan_counts(const int64_t* __restrict__ counts, int64_t n,
+                                                              int64_t* __restrict__ ptr, long long* __restrict__ total) {
+    __shared__ long long wsum[kScanThreads / 32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t per = (n + kScanThreads - 1) / kScanThreads;
+    const int64_t b = min(n, tid * per), e = min(n, b + per);
+    long long s = 0;
+    for (int64_t i = b; i < e; ++i) s += counts[i];
+    long long incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        wsum[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    long long run = incl - s + (warp ? wsum[warp - 1] : 0);
+    for (int64_t i = b; i < e; ++i) {
+        ptr[i] = run;
+        run += counts[i];
+    }
+    if (tid == kScanThreads - 1) {
+        ptr[n] = run;
+        *total = run;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2670,14 +2774,58 @@ __global__ void k_sincos(const double* __restrict__ x, int64_t n, double* __rest
 // ---------------------------------------------------------------------------------------------
 static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// Row of every near pair (the CSR's row index per entry), so that a near-pair kernel finds its
-// pair's row with one load instead of a search through the row pointers.
-static void set_near_rows(Mesh& m, const std::vector<int64_t>& ptr) {
-    std::vector<int32_t> row(std::max<int64_t>(m.nnz, 1), 0);
-    for (int64_t i = 0; i < m.n; ++i)
-        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) row[p] = static_cast<int32_t>(i);
-    m.near_row.alloc(sizeof(int32_t) * row.size());
-    h2d_sync(m.near_row.p, row.data(), sizeof(int32_t) * row.size());
+// Area of a triangle as compute_element_geometry (generators.rs:771-830) takes it: half the
+// length of the cross product of the two edges from the first vertex (host input validation).
+static double host_triangle_area(const double* nodes, const uint32_t* t) {
+    double a1[3], a2[3];
+    for (int j = 0; j < 3; ++j) {
+        a1[j] = nodes[3 * t[1] + j] - nodes[3 * t[0] + j];
+        a2[j] = nodes[3 * t[2] + j] - nodes[3 * t[0] + j];
+    }
+    const double c0 = a1[1] * a2[2] - a1[2] * a2[1];
+    const double c1 = a1[2] * a2[0] - a1[0] * a2[2];
+    const double c2 = a1[0] * a2[1] - a1[1] * a2[0];
+    return std::sqrt(c0 * c0 + c1 * c1 + c2 * c2) / 2.0;
+}
+
+// Near-pair CSR of a mesh built on the device: chunk bounds, per-row counts, the scan (the pair
+// count is the one value read back), then the columns (increasing) and the row of every pair.
+static void build_near_csr(Mesh& m) {
+    const int64_t nchunk = cdiv(m.n, kNearCols);
+    const int64_t nblk = cdiv(m.n, kNearRows);
+    DevBuf box, counts, total;
+    box.alloc(sizeof(double) * 8 * nchunk);
+    counts.alloc(sizeof(int64_t) * m.n);
+    total.alloc(sizeof(long long));
+    k_near_chunk_bounds<<<nchunk, kNearCols>>>(m.elem.as<double>(), m.n, m.ld, box.as<double>()); count_launch();
+    SB_CUDA(cudaGetLastError());
+    k_near_pass<<<nblk, kNearCols>>>(m.elem.as<double>(), m.n, m.ld, 0, box.as<double>(), counts.as<int64_t>(),
+                                     nullptr, nullptr, nullptr); count_launch();
+    SB_CUDA(cudaGetLastError());
+    m.near_ptr.alloc(sizeof(int64_t) * (m.n + 1));
+    k_scan_counts<<<1, kScanThreads>>>(counts.as<int64_t>(), m.n, m.near_ptr.as<int64_t>(), total.as<long long>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    long long nnz = 0;
+    SB_CUDA(cudaMemcpy(&nnz, total.p, sizeof(nnz), cudaMemcpyDeviceToHost));
+    m.nnz = nnz;
+    m.near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m.nnz, 1));
+    m.near_row.alloc(sizeof(int32_t) * std::max<int64_t>(m.nnz, 1));
+    k_near_pass<<<nblk, kNearCols>>>(m.elem.as<double>(), m.n, m.ld, 1, box.as<double>(), nullptr,
+                                     m.near_ptr.as<int64_t>(), m.near_col.as<int32_t>(), m.near_row.as<int32_t>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+}
+
+const std::vector<double>& mesh_host_elem(const Mesh& m) {
+    std::lock_guard<std::mutex> lock(m.h_elem_mu);
+    if (m.h_elem.empty()) {
+        std::vector<double> h(static_cast<size_t>(EFIELDS) * m.ld);
+        SB_CUDA(cudaSetDevice(m.device));
+        SB_CUDA(cudaMemcpy(h.data(), m.elem.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+        m.h_elem.swap(h);
+    }
+    return m.h_elem;
 }
 
 Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, int64_t n_tris,
@@ -2690,11 +2838,11 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
     for (int64_t a = 0; a < 3 * n_tris; ++a)
         SB_REQUIRE(tris[a] < static_cast<uint64_t>(n_nodes), SB_ERR_INVALID_ARGUMENT,
                    "mesh: connectivity index out of range");
-    std::vector<double> c(3 * n_tris), nr(3 * n_tris), ar(n_tris);
-    host_element_geometry(nodes, tris, n_tris, c.data(), nr.data(), ar.data());
-    for (int64_t e = 0; e < n_tris; ++e)
-        SB_REQUIRE(ar[e] > 1e-300 && std::isfinite(ar[e]), SB_ERR_UNSUPPORTED_ELEMENT,
+    for (int64_t e = 0; e < n_tris; ++e) {
+        const double ar = host_triangle_area(nodes, tris + 3 * e);
+        SB_REQUIRE(ar > 1e-300 && std::isfinite(ar), SB_ERR_UNSUPPORTED_ELEMENT,
                    "mesh: degenerate triangle " + std::to_string(e));
+    }
     int ndev = 0;
     SB_CUDA(cudaGetDeviceCount(&ndev));
     SB_REQUIRE(device >= 0 && device < ndev, SB_ERR_CUDA, "mesh: CUDA device not available");
@@ -2719,31 +2867,14 @@ Mesh* mesh_create(const double* nodes, int64_t n_nodes, const uint32_t* tris, in
         h2d_sync(m->nodes.p, nodes, sizeof(double) * 3 * n_nodes);
         h2d_sync(m->tris.p, tris, sizeof(uint32_t) * 3 * n_tris);
         const int64_t nb = cdiv(m->ld, 256);
-        k_element_geometry<<<nb, 256>>>(m->nodes.as<double>(), m->tris.as<uint32_t>(), m->n, m->ld, m->elem.as<double>()); count_launch();
+        k_element_geometry<<<nb, 256>>>(m->nodes.as<double>(), m->tris.as<uint32_t>(), m->n, m->ld, m->elem.as<double>());
+        count_launch();
         SB_CUDA(cudaGetLastError());
         k_far_points<<<nb, 256>>>(m->elem.as<double>(), m->n, m->ld, m->qp.as<double>()); count_launch();
         SB_CUDA(cudaGetLastError());
         k_far_points32<<<nb, 256>>>(m->elem.as<double>(), m->n, m->ld, m->qp32.as<float>()); count_launch();
         SB_CUDA(cudaGetLastError());
-        // Near-pair CSR.
-        DevBuf counts;
-        counts.alloc(sizeof(int64_t) * (m->n + 1));
-        const int64_t nblk = cdiv(m->n, kNearRows);
-        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 0, counts.as<int64_t>(), nullptr, nullptr); count_launch();
-        SB_CUDA(cudaGetLastError());
-        std::vector<int64_t> cnt(m->n), ptr(m->n + 1);
-        SB_CUDA(cudaMemcpy(cnt.data(), counts.p, sizeof(int64_t) * m->n, cudaMemcpyDeviceToHost));
-        ptr[0] = 0;
-        for (int64_t i = 0; i < m->n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
-        m->nnz = ptr[m->n];
-        m->near_ptr.alloc(sizeof(int64_t) * (m->n + 1));
-        h2d_sync(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1));
-        set_near_rows(*m, ptr);
-        m->near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m->nnz, 1));
-        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 1, nullptr, m->near_ptr.as<int64_t>(), m->near_col.as<int32_t>()); count_launch();
-        SB_CUDA(cudaGetLastError());
-        m->h_elem.resize(static_cast<size_t>(EFIELDS) * m->ld);
-        SB_CUDA(cudaMemcpy(m->h_elem.data(), m->elem.p, sizeof(double) * m->h_elem.size(), cudaMemcpyDeviceToHost));
+        build_near_csr(*m);
         SB_CUDA(cudaDeviceSynchronize());
         m->h_bc_kind.assign(m->n, SB_BC_VELOCITY);
         m->h_bc_value.assign(2 * m->n, 0.0);
@@ -2803,24 +2934,7 @@ Mesh* mesh_create_quad(const double* nodes, int64_t n_nodes, const uint32_t* qua
             SB_REQUIRE(ar > 1e-300 && std::isfinite(ar), SB_ERR_UNSUPPORTED_ELEMENT,
                        "mesh: degenerate quadrilateral " + std::to_string(e));
         }
-        DevBuf counts;
-        counts.alloc(sizeof(int64_t) * (m->n + 1));
-        const int64_t nblk = cdiv(m->n, kNearRows);
-        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 0, counts.as<int64_t>(), nullptr, nullptr);
-        count_launch();
-        SB_CUDA(cudaGetLastError());
-        std::vector<int64_t> cnt(m->n), ptr(m->n + 1);
-        SB_CUDA(cudaMemcpy(cnt.data(), counts.p, sizeof(int64_t) * m->n, cudaMemcpyDeviceToHost));
-        ptr[0] = 0;
-        for (int64_t i = 0; i < m->n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
-        m->nnz = ptr[m->n];
-        m->near_ptr.alloc(sizeof(int64_t) * (m->n + 1));
-        h2d_sync(m->near_ptr.p, ptr.data(), sizeof(int64_t) * (m->n + 1));
-        m->near_col.alloc(sizeof(int32_t) * std::max<int64_t>(m->nnz, 1));
-        k_near_pass<<<nblk, 256>>>(m->elem.as<double>(), m->n, m->ld, 1, nullptr, m->near_ptr.as<int64_t>(),
-                                   m->near_col.as<int32_t>());
-        count_launch();
-        SB_CUDA(cudaGetLastError());
+        build_near_csr(*m);
         SB_CUDA(cudaDeviceSynchronize());
         m->h_bc_kind.assign(m->n, SB_BC_VELOCITY);
         m->h_bc_value.assign(2 * m->n, 0.0);
@@ -3399,33 +3513,6 @@ void device_sincos(int device, const double* x, int64_t n, double* s, double* c)
     SB_CUDA(cudaGetLastError());
     SB_CUDA(cudaMemcpy(s, ds.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
     SB_CUDA(cudaMemcpy(c, dc.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
-}
-
-// compute_element_geometry (generators.rs:771-830) on the host, for input validation.
-void host_element_geometry(const double* nodes, const uint32_t* tris, int64_t n, double* c,
-                           double* nrm, double* area) {
-    for (int64_t e = 0; e < n; ++e) {
-        const uint32_t* t = tris + 3 * e;
-        for (int j = 0; j < 3; ++j)
-            c[3 * e + j] = (((0.0 + nodes[3 * t[0] + j]) + nodes[3 * t[1] + j]) + nodes[3 * t[2] + j]) / 3.0;
-        double a1[3], a2[3];
-        for (int j = 0; j < 3; ++j) {
-            a1[j] = nodes[3 * t[1] + j] - nodes[3 * t[0] + j];
-            a2[j] = nodes[3 * t[2] + j] - nodes[3 * t[0] + j];
-        }
-        const double c0 = a1[1] * a2[2] - a1[2] * a2[1];
-        const double c1 = a1[2] * a2[0] - a1[0] * a2[2];
-        const double c2 = a1[0] * a2[1] - a1[1] * a2[0];
-        const double len = std::sqrt(c0 * c0 + c1 * c1 + c2 * c2);
-        area[e] = len / 2.0;
-        if (len > 1e-15) {
-            nrm[3 * e] = c0 / len;
-            nrm[3 * e + 1] = c1 / len;
-            nrm[3 * e + 2] = c2 / len;
-        } else {
-            nrm[3 * e] = nrm[3 * e + 1] = nrm[3 * e + 2] = 0.0;
-        }
-    }
 }
 
 }  // namespace sb

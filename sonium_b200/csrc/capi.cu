@@ -372,12 +372,13 @@ SB_API int sb_mesh_element_geometry(const sb_mesh* mesh, double* centers, double
     return guarded([&] {
         SB_REQUIRE(mesh && mesh->m, SB_ERR_INVALID_ARGUMENT, "null mesh");
         const Mesh& m = *mesh->m;
+        const std::vector<double>& he = mesh_host_elem(m);
         for (int64_t e = 0; e < m.n; ++e) {
             for (int c = 0; c < 3; ++c) {
-                if (centers) centers[3 * e + c] = m.h_elem[(ECX + c) * m.ld + e];
-                if (normals) normals[3 * e + c] = m.h_elem[(ENX + c) * m.ld + e];
+                if (centers) centers[3 * e + c] = he[(ECX + c) * m.ld + e];
+                if (normals) normals[3 * e + c] = he[(ENX + c) * m.ld + e];
             }
-            if (areas) areas[e] = m.h_elem[EAREA * m.ld + e];
+            if (areas) areas[e] = he[EAREA * m.ld + e];
         }
     });
 }
@@ -553,10 +554,11 @@ SB_API int sb_mesh_collocation(const sb_mesh* mesh, int basis, double* points, d
         SB_REQUIRE(basis == SB_BASIS_CONSTANT || !m.quad, SB_ERR_UNSUPPORTED_ELEMENT,
                    "discontinuous bases: Tri3 meshes only");
         if (basis == SB_BASIS_CONSTANT) {
+            const std::vector<double>& he = mesh_host_elem(m);
             for (int64_t e = 0; e < m.n; ++e)
                 for (int c = 0; c < 3; ++c) {
-                    points[3 * e + c] = m.h_elem[(ECX + c) * m.ld + e];
-                    normals[3 * e + c] = m.h_elem[(ENX + c) * m.ld + e];
+                    points[3 * e + c] = he[(ECX + c) * m.ld + e];
+                    normals[3 * e + c] = he[(ENX + c) * m.ld + e];
                 }
             return;
         }

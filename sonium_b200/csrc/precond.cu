@@ -68,38 +68,107 @@ __global__ void __launch_bounds__(BS * kBjSplit) k_bj_apply(const float2* __rest
 
 }  // namespace
 
-// Morton (Z-order) permutation of points: 21 bits per axis of the normalised coordinates.
-std::vector<int32_t> morton_order(const std::vector<double>& xyz, int64_t n) {
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int64_t e = 0; e < n; ++e)
+namespace {
+
+// Bounds of the element centroids: one CTA, bounds[0..2] the smallest and [3..5] the largest
+// coordinate along each axis.
+constexpr int kMortonThreads = 1024;
+__global__ void __launch_bounds__(kMortonThreads) k_centroid_bounds(const double* __restrict__ elem, int64_t n,
+                                                                     int64_t ld, double* __restrict__ bounds) {
+    __shared__ double red[kMortonThreads / 32][6];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (int64_t e = tid; e < n; e += kMortonThreads)
         for (int d = 0; d < 3; ++d) {
-            lo[d] = std::min(lo[d], xyz[3 * e + d]);
-            hi[d] = std::max(hi[d], xyz[3 * e + d]);
+            const double x = elem[(ECX + d) * ld + e];
+            v[d] = fmin(v[d], x);
+            v[3 + d] = fmax(v[3 + d], x);
         }
-    const double span = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
-    std::vector<uint64_t> code(n);
-    for (int64_t e = 0; e < n; ++e) {
-        uint64_t c = 0;
-        uint64_t q[3];
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const double t = (xyz[3 * e + d] - lo[d]) / span;
-            q[d] = static_cast<uint64_t>(std::min(std::max(t, 0.0), 1.0) * 2097151.0);
+            v[d] = fmin(v[d], __shfl_xor_sync(0xffffffffu, v[d], o));
+            v[3 + d] = fmax(v[3 + d], __shfl_xor_sync(0xffffffffu, v[3 + d], o));
         }
-        for (int b = 0; b < 21; ++b)
-            for (int d = 0; d < 3; ++d) c |= ((q[d] >> b) & 1ull) << (3 * b + d);
-        code[e] = c;
+    if (lane == 0)
+        for (int c = 0; c < 6; ++c) red[warp][c] = v[c];
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < kMortonThreads / 32; ++w)
+            for (int d = 0; d < 3; ++d) {
+                v[d] = fmin(v[d], red[w][d]);
+                v[3 + d] = fmax(v[3 + d], red[w][3 + d]);
+            }
+        for (int c = 0; c < 6; ++c) bounds[c] = v[c];
     }
-    std::vector<int32_t> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return code[a] < code[b]; });
-    return order;
 }
 
+// Two zero bits after each of the low 21 bits of x (bit b moves to bit 3 b).
+__device__ __forceinline__ uint64_t spread3(uint64_t x) {
+    x &= 0x1fffffull;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+// Morton (Z-order) code of every element centroid: each coordinate normalised by the largest
+// extent of the box, clamped to [0, 1], scaled to 21 bits (truncated), bits interleaved x, y, z
+// from the lowest. Correctly rounded operations, so the code does not depend on contraction.
+__global__ void k_morton_codes(const double* __restrict__ elem, int64_t n, int64_t ld,
+                               const double* __restrict__ bounds, uint64_t* __restrict__ code) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const double span = fmax(fmax(fmax(__dsub_rn(bounds[3], bounds[0]), __dsub_rn(bounds[4], bounds[1])),
+                                  __dsub_rn(bounds[5], bounds[2])), 1e-300);
+    uint64_t c = 0;
+    for (int d = 0; d < 3; ++d) {
+        const double t = __ddiv_rn(__dsub_rn(elem[(ECX + d) * ld + e], bounds[d]), span);
+        const uint64_t q = static_cast<uint64_t>(__dmul_rn(fmin(fmax(t, 0.0), 1.0), 2097151.0));
+        c |= spread3(q) << d;
+    }
+    code[e] = c;
+}
+
+// Indices sorted by code, equal codes in index order (least-significant-digit radix sort, 8 bits
+// a pass over the 63 code bits).
+std::vector<int32_t> order_by_code(const std::vector<uint64_t>& code) {
+    const size_t n = code.size();
+    std::vector<int32_t> a(n), b(n);
+    std::iota(a.begin(), a.end(), 0);
+    if (n == 0) return a;
+    for (int shift = 0; shift < 64; shift += 8) {
+        size_t cnt[257] = {0};
+        for (size_t i = 0; i < n; ++i) ++cnt[((code[a[i]] >> shift) & 0xff) + 1];
+        if (cnt[1 + ((code[a[0]] >> shift) & 0xff)] == n) continue;  // one digit value: order kept
+        for (int d = 0; d < 256; ++d) cnt[d + 1] += cnt[d];
+        for (size_t i = 0; i < n; ++i) b[cnt[(code[a[i]] >> shift) & 0xff]++] = a[i];
+        a.swap(b);
+    }
+    return a;
+}
+
+}  // namespace
+
+// Morton order of a mesh's element centroids: codes on the device, the stable sort on the host.
 std::vector<int32_t> element_morton_order(const Mesh& m) {
-    std::vector<double> c(3 * m.n);
-    for (int64_t e = 0; e < m.n; ++e)
-        for (int d = 0; d < 3; ++d) c[3 * e + d] = m.h_elem[(ECX + d) * m.ld + e];
-    return morton_order(c, m.n);
+    SB_CUDA(cudaSetDevice(m.device));
+    DevBuf bounds, dcode;
+    bounds.alloc(sizeof(double) * 6);
+    dcode.alloc(sizeof(uint64_t) * std::max<int64_t>(m.n, 1));
+    k_centroid_bounds<<<1, kMortonThreads>>>(m.elem.as<double>(), m.n, m.ld, bounds.as<double>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    k_morton_codes<<<static_cast<unsigned>((m.n + 255) / 256), 256>>>(m.elem.as<double>(), m.n, m.ld,
+                                                                      bounds.as<double>(), dcode.as<uint64_t>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    std::vector<uint64_t> code(m.n);
+    SB_CUDA(cudaMemcpy(code.data(), dcode.p, sizeof(uint64_t) * m.n, cudaMemcpyDeviceToHost));
+    return order_by_code(code);
 }
 
 namespace {

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <exception>
+#include <mutex>
 #include <new>
 #include <string>
 #include <utility>
@@ -147,7 +148,9 @@ struct Mesh {
     double coord_bound = 0.0;  // largest |coordinate| of the nodes (bounds FP32 rounding of positions)
     std::vector<double> h_nodes;
     std::vector<uint32_t> h_tris;
-    std::vector<double> h_elem;  // host copy of the element SoA (ld stride)
+    // host copy of the element SoA (ld stride), read back on first use (mesh_host_elem)
+    mutable std::vector<double> h_elem;
+    mutable std::mutex h_elem_mu;
     DevBuf nodes, tris, elem, qp, qp32;
     // near-pair CSR (superset of the reference's subdivision criterion; excludes the diagonal)
     int64_t nnz = 0;
@@ -283,8 +286,8 @@ Mesh* mesh_create_quad(const double* nodes, int64_t n_nodes, const uint32_t* qua
 void assemble_quad(Operator& op, const sb_physics& ph, double beta_re, double beta_im);
 void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const uint8_t* has_adm,
                  const sb_complex* adm);
-void host_element_geometry(const double* nodes, const uint32_t* tris, int64_t n, double* c,
-                           double* nrm, double* area);
+// The element SoA on the host (EFIELDS x ld doubles), copied from the device on first use.
+const std::vector<double>& mesh_host_elem(const Mesh& m);
 
 enum class Trans { N = 0, T = 1, C = 2 };
 
