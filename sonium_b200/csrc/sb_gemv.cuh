@@ -169,9 +169,9 @@ __device__ __forceinline__ void gemv_c64_block(const float2* __restrict__ A, int
 // apart (lda a multiple of 4). FP32 vectors and accumulation; results times the inverse scale
 // (exact). 4 bytes per entry: half the HBM traffic of the complex64 product.
 // ---------------------------------------------------------------------------------------------
-// 16 rows a CTA, one 16-byte load per row in flight per thread: 16 loads in flight per thread
-// and each x chunk reused across 16 rows (measured at N = 20480: 0.257 ms a launch, the HBM copy
-// rate; 8 rows x 2 loads 0.291 ms, 16 x 2 0.348 ms).
+// The batched solver's shape: 16 rows a CTA, one 16-byte load per row in flight per thread, each
+// x chunk reused across 16 rows (measured at N = 20480: 0.250-0.253 ms a launch; 8 rows x 2 loads
+// 0.291 ms, 16 x 2 0.348 ms). The single-operator product runs 2 rows x 4 loads (blas.cu).
 constexpr int kGemv16Rows = 16;
 constexpr int kGemv16Unroll = 1;
 constexpr int kHalfThreads = 256;  // threads of the largest-part scan and the conversion
