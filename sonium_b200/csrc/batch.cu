@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restric
         gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, src, I.rq, I.rb, I.pnorm, blk);
 }
 
-// The same products on the complex-half copies (kGemv16Rows rows per CTA).
+// The same products on the complex-half copies (kGemv16PRows rows per CTA).
 __global__ void __launch_bounds__(kGemvThreads) k_bgemv16(const BInst* __restrict__ inst,
                                                           const int64_t* __restrict__ pre, int ninst, int mode,
                                                           int j, int gk) {
@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(kGemvThreads) k_bgemv16(const BInst* __restric
     const float* inv = reinterpret_cast<const float*>(I.aux16 + 2);
     const float2* src = mode == 0 ? I.V + (int64_t)j * I.vs : (mode == 1 ? I.d : I.t);
     if (mode == 0 || mode == 2)
-        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, src, I.w, nullptr,
-                                                                 nullptr, blk);
+        gemv_c16_block<kGemv16PRows, kGemvThreads, kGemv16PUnroll>(I.A16, I.n, I.lda16, inv, src, I.w, nullptr,
+                                                                   nullptr, blk);
     else
-        gemv_c16_block<kGemv16Rows, kGemvThreads, kGemv16Unroll>(I.A16, I.n, I.lda16, inv, src, I.rq, I.rb,
-                                                                 I.pnorm, blk);
+        gemv_c16_block<kGemv16PRows, kGemvThreads, kGemv16PUnroll>(I.A16, I.n, I.lda16, inv, src, I.rq, I.rb,
+                                                                   I.pnorm, blk);
 }
 
 // Block-Jacobi over the flattened blocks of every instance: inverses (one CTA per block) and
@@ -584,8 +584,8 @@ struct Batch {
     std::vector<BatchAsmInst> asm_h;
     std::vector<double2*> rhs;  // per-instance right-hand side (pool_rhs)
     std::vector<BInst> h;
-    std::vector<int64_t> pre4, pre16, pre256, predot, prewide;
-    DevBuf asm_d, inst_d, pre4_d, pre16_d, pre256_d, predot_d, prewide_d, pre_asm;
+    std::vector<int64_t> pre4, pre16, pre16p, pre256, predot, prewide;
+    DevBuf asm_d, inst_d, pre4_d, pre16_d, pre16p_d, pre256_d, predot_d, prewide_d, pre_asm;
     // Inner products on the complex64 matrices (SB_INNER_FP32) or on complex-half copies built
     // after each assembly (SB_INNER_FP16; independent instances only).
     int inner = SB_INNER_FP32;
@@ -820,7 +820,7 @@ static void batch_workspace(Batch& B, int64_t m) {
         small += round256(sizeof(double2) * (m + 1) * m) + 2 * round256(sizeof(double2) * m) +
                  2 * round256(sizeof(double2) * (m + 1)) + 2 * round256(sizeof(double2) * (m + 2)) +
                  round256(sizeof(double2) * chunks * (m + 2)) +
-                 round256(sizeof(double) * std::max(cdiv64(n, kGemvRows), chunks));
+                 round256(sizeof(double) * std::max({cdiv64(n, kGemvRows), cdiv64(n, kGemv16PRows), chunks}));
     }
     B.pool_f32.alloc(f32);
     B.pool_f64.alloc(f64);
@@ -867,6 +867,7 @@ static void batch_workspace(Batch& B, int64_t m) {
     }
     B.pre4.assign(ni + 1, 0);
     B.pre16.assign(ni + 1, 0);
+    B.pre16p.assign(ni + 1, 0);
     B.pre256.assign(ni + 1, 0);
     B.predot.assign(ni + 1, 0);
     B.prewide.assign(ni + 1, 0);
@@ -900,7 +901,7 @@ static void batch_workspace(Batch& B, int64_t m) {
         I.red = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 2)));
         I.red2 = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 2)));
         I.part = reinterpret_cast<double2*>(take(ps, sizeof(double2) * chunks * (m + 2)));
-        I.pnorm = reinterpret_cast<double*>(take(ps, sizeof(double) * std::max(cdiv64(n, kGemvRows), chunks)));
+        I.pnorm = reinterpret_cast<double*>(take(ps, sizeof(double) * std::max({cdiv64(n, kGemvRows), cdiv64(n, kGemv16PRows), chunks})));
         I.st = dv.st + b;
         I.nrm = dv.nrm + 3 * b;
         I.scal = dv.scal + kScal * b;
@@ -909,6 +910,7 @@ static void batch_workspace(Batch& B, int64_t m) {
         I.brk = dv.brk + b;
         B.pre4[b + 1] = B.pre4[b] + cdiv64(n, kGemvRows);
         B.pre16[b + 1] = B.pre16[b] + cdiv64(n, kGemv16Rows);
+        B.pre16p[b + 1] = B.pre16p[b] + cdiv64(n, kGemv16PRows);
         B.pre256[b + 1] = B.pre256[b] + chunks;
         B.predot[b + 1] = B.predot[b] + cdiv64(n, (int64_t)kChunk * kDotSpan);
         B.prewide[b + 1] = B.prewide[b] + cdiv64(n, (int64_t)kWide);
@@ -916,6 +918,7 @@ static void batch_workspace(Batch& B, int64_t m) {
     B.inst_d.alloc(sizeof(BInst) * ni);
     B.pre4_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre16_d.alloc(sizeof(int64_t) * (ni + 1));
+    B.pre16p_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre256_d.alloc(sizeof(int64_t) * (ni + 1));
     B.predot_d.alloc(sizeof(int64_t) * (ni + 1));
     h2d_sync(B.predot_d.p, B.predot.data(), sizeof(int64_t) * (ni + 1));
@@ -924,6 +927,7 @@ static void batch_workspace(Batch& B, int64_t m) {
     h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
     h2d_sync(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.pre16_d.p, B.pre16.data(), sizeof(int64_t) * (ni + 1));
+    h2d_sync(B.pre16p_d.p, B.pre16p.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.pre256_d.p, B.pre256.data(), sizeof(int64_t) * (ni + 1));
     B.m = m;
 }
@@ -954,8 +958,8 @@ static void batch_step(Batch& B, int j) {
         const int mode = bj ? 2 : 0;
         if (B.inner == SB_INNER_FP16) {
             ProfScope prof(SB_PROF_GEMV16, s);
-            k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(I, B.pre16_d.as<int64_t>(), ni,
-                                                                                     mode, j, G_ACTIVE);
+            k_bgemv16<<<static_cast<unsigned>(B.pre16p.back()), kGemvThreads, 0, s>>>(I, B.pre16p_d.as<int64_t>(), ni,
+                                                                                      mode, j, G_ACTIVE);
         } else {
             ProfScope prof(SB_PROF_GEMV32, s);
             k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, mode, j, G_ACTIVE);
@@ -1187,10 +1191,10 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
                     if (B.inner == SB_INNER_FP16) {
                         {
                             ProfScope prof(SB_PROF_GEMV16, s);
-                            k_bgemv16<<<static_cast<unsigned>(B.pre16.back()), kGemvThreads, 0, s>>>(
-                                I, B.pre16_d.as<int64_t>(), ni, mode, 0, G_RESTART);
+                            k_bgemv16<<<static_cast<unsigned>(B.pre16p.back()), kGemvThreads, 0, s>>>(
+                                I, B.pre16p_d.as<int64_t>(), ni, mode, 0, G_RESTART);
                         }
-                        k_bsum_partials<<<ni, 32, 0, s>>>(I, B.pre16_d.as<int64_t>(), 2, G_RESTART);
+                        k_bsum_partials<<<ni, 32, 0, s>>>(I, B.pre16p_d.as<int64_t>(), 2, G_RESTART);
                     } else {
                         {
                             ProfScope prof(SB_PROF_GEMV32, s);

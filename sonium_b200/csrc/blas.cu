@@ -372,14 +372,11 @@ __global__ void k_jacobi(const double2* __restrict__ d, const T* __restrict__ x,
 constexpr int kGemv128Rows = 1, kGemv128Unroll = 4;
 constexpr int kGemv64Rows = 1, kGemv64Unroll = 4;
 constexpr int kGemvX64Rows = 2, kGemvX64Unroll = 4;
-// The complex-half product of the inner solve: 2 rows x 4 loads (0.244-0.245 ms at N = 20480,
-// against 0.250-0.253 ms for 16 rows x 1 load, whose x chunk is shared by more rows but whose 128
-// registers allow 2 CTAs per SM; the batched solver keeps kGemv16Rows).
-constexpr int kGemv16OpRows = 2, kGemv16OpUnroll = 4;
+
 // gemv_partials counts the partial norms of both the complex128 and the FP32-vector complex64
 // residuals, and callers size partial-norm buffers by it for every residual product.
 static_assert(kGemv64Rows == kGemv128Rows, "one partial count for the c128 and c64 residuals");
-static_assert(kGemvX64Rows >= kGemv128Rows && kGemv16OpRows >= kGemv128Rows,
+static_assert(kGemvX64Rows >= kGemv128Rows && kGemv16PRows >= kGemv128Rows,
               "gemv_partials bounds every residual's partial count");
 
 void gemv_c128(const double2* A, int64_t n, const double2* x, double2* y, Trans t,
@@ -454,13 +451,13 @@ __global__ void __launch_bounds__(THREADS) k_gemv_n_c16(const uint32_t* __restri
     gemv_c16_block<ROWS, THREADS, UNROLL, true>(A, n, lda, inv_scale, x, y, b, part, blockIdx.x);
 }
 
-int64_t gemv16_partials(int64_t n) { return cdiv(n, kGemv16OpRows); }
+int64_t gemv16_partials(int64_t n) { return cdiv(n, kGemv16PRows); }
 
 void gemv_c16(const uint32_t* A, int64_t n, int64_t lda, const float* inv_scale, const float2* x, float2* y,
               const float2* b, double* part, cudaStream_t s, Gate gate) {
     ProfScope prof(SB_PROF_GEMV16, s);
-    k_gemv_n_c16<kGemv16OpRows, kGemvThreads, kGemv16OpUnroll>
-        <<<cdiv(n, kGemv16OpRows), kGemvThreads, 0, s>>>(A, n, lda, inv_scale, x, y, b, part, gate);
+    k_gemv_n_c16<kGemv16PRows, kGemvThreads, kGemv16PUnroll>
+        <<<cdiv(n, kGemv16PRows), kGemvThreads, 0, s>>>(A, n, lda, inv_scale, x, y, b, part, gate);
     count_launch();
     SB_CUDA(cudaGetLastError());
 }

@@ -169,11 +169,14 @@ __device__ __forceinline__ void gemv_c64_block(const float2* __restrict__ A, int
 // apart (lda a multiple of 4). FP32 vectors and accumulation; results times the inverse scale
 // (exact). 4 bytes per entry: half the HBM traffic of the complex64 product.
 // ---------------------------------------------------------------------------------------------
-// The batched solver's shape: 16 rows a CTA, one 16-byte load per row in flight per thread, each
-// x chunk reused across 16 rows (measured at N = 20480: 0.250-0.253 ms a launch; 8 rows x 2 loads
-// 0.291 ms, 16 x 2 0.348 ms). The single-operator product runs 2 rows x 4 loads (blas.cu).
+// Launch shape of the complex-half products (single operator and batched): 2 rows a CTA, 4 loads
+// of 16 bytes in flight per row and thread (measured at N = 20480: 0.244-0.245 ms a launch; 16
+// rows x 1 load, which shares each x chunk across 16 rows but needs 128 registers, 2 CTAs per SM,
+// 0.250-0.253 ms; 8 x 2 0.291 ms; 16 x 2 0.348 ms; 4 x 4 0.342 ms).
+constexpr int kGemv16PRows = 2;
+constexpr int kGemv16PUnroll = 4;
+// Row blocks of the batched solver's largest-part scan and conversion to the complex-half copy.
 constexpr int kGemv16Rows = 16;
-constexpr int kGemv16Unroll = 1;
 constexpr int kHalfThreads = 256;  // threads of the largest-part scan and the conversion
 
 __device__ __forceinline__ float2 half_pair(uint32_t u) {
