@@ -111,7 +111,12 @@ __device__ __forceinline__ bool open_gate(const BInst& I, int gk) {
     }
 }
 
-// Matrix-vector products over the flattened row blocks (kGemvRows rows per CTA).
+// The batched FP32-vector complex64 product keeps 4 rows x 2 loads per CTA: at the single
+// operator's 1 x 4 the sweep's flattened grid (one CTA per row of every instance) made the
+// FP32-inner sweep solve slower (711 against 646 ms for 64 instances).
+constexpr int kBGemv64Rows = 4, kBGemv64Unroll = 2;
+
+// Matrix-vector products over the flattened row blocks (kBGemv64Rows rows per CTA).
 // mode 0: w = A V_j; mode 1: rq = rb - A d (partial norms); modes 2 / 3: the same with t
 // (= M^-1 V_j or M^-1 d under the block-Jacobi preconditioner) in place of V_j / d.
 __global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restrict__ inst,
@@ -123,9 +128,11 @@ __global__ void __launch_bounds__(kGemvThreads) k_bgemv32(const BInst* __restric
     const int64_t blk = blockIdx.x - pre[b];
     const float2* src = mode == 0 ? I.V + (int64_t)j * I.vs : (mode == 1 ? I.d : I.t);
     if (mode == 0 || mode == 2)
-        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, src, I.w, nullptr, nullptr, blk);
+        gemv_c64_block<kBGemv64Rows, kGemvThreads, kBGemv64Unroll, false>(I.A, I.n, I.lda, src, I.w, nullptr,
+                                                                           nullptr, blk);
     else
-        gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, false>(I.A, I.n, I.lda, src, I.rq, I.rb, I.pnorm, blk);
+        gemv_c64_block<kBGemv64Rows, kGemvThreads, kBGemv64Unroll, false>(I.A, I.n, I.lda, src, I.rq, I.rb, I.pnorm,
+                                                                           blk);
 }
 
 // The same products on the complex-half copies (kGemv16PRows rows per CTA).
@@ -196,14 +203,15 @@ __global__ void __launch_bounds__(kHalfThreads) k_bhalf_convert(const BInst* __r
                       r0 + kGemv16Rows < I.n ? r0 + kGemv16Rows : I.n, 1);
 }
 
-// r = b - A x with FP64 vectors and FP64 accumulation on the complex64 matrix, partial norms.
+// r = b - A x with FP64 vectors and FP64 accumulation on the complex64 matrix, partial norms
+// (kGemvX64Rows rows per CTA).
 __global__ void __launch_bounds__(kGemvThreads) k_bres64(const BInst* __restrict__ inst,
                                                          const int64_t* __restrict__ pre, int ninst, int gk) {
     const int b = find_inst(pre, ninst, blockIdx.x);
     const BInst& I = inst[b];
     if (!open_gate(I, gk)) return;
-    gemv_c64_block<kGemvRows, kGemvThreads, kGemvUnroll, true>(I.A, I.n, I.lda, I.x, I.r, I.b, I.pnorm,
-                                                               blockIdx.x - pre[b]);
+    gemv_c64_block<kGemvX64Rows, kGemvThreads, kGemvX64Unroll, true>(I.A, I.n, I.lda, I.x, I.r, I.b, I.pnorm,
+                                                                     blockIdx.x - pre[b]);
 }
 
 // Per-chunk squared norms: sel 0 = rb, 1 = b, 2 = b - r (= A x), 3 = r.
@@ -275,14 +283,24 @@ __global__ void __launch_bounds__(kChunk) k_bresid_w(const BInst* __restrict__ i
 }
 
 // nrm[slot] = sum of the instance's partials (their count is the instance's span of `pre`).
-__global__ void k_bsum_partials(const BInst* __restrict__ inst, const int64_t* __restrict__ pre, int slot, int gk) {
+// One CTA per instance sums its partial norms (up to one per row of its residual product).
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_bsum_partials(const BInst* __restrict__ inst,
+                                                               const int64_t* __restrict__ pre, int slot, int gk) {
+    __shared__ double red[kSumThreads / 32];
     const BInst& I = inst[blockIdx.x];
     if (!open_gate(I, gk)) return;
     const int64_t cnt = pre[blockIdx.x + 1] - pre[blockIdx.x];
     double s = 0.0;
-    for (int64_t c = threadIdx.x; c < cnt; c += 32) s += I.pnorm[c];
+    for (int64_t c = threadIdx.x; c < cnt; c += kSumThreads) s += I.pnorm[c];
     s = warp_sum(s);
-    if (threadIdx.x == 0) I.nrm[slot] = s;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < kSumThreads / 32 ? red[threadIdx.x] : 0.0;
+        s = warp_sum(s);
+        if (threadIdx.x == 0) I.nrm[slot] = s;
+    }
 }
 
 // Gram-Schmidt dots over the flattened chunks of kDotSpan * kChunk rows:
@@ -584,8 +602,8 @@ struct Batch {
     std::vector<BatchAsmInst> asm_h;
     std::vector<double2*> rhs;  // per-instance right-hand side (pool_rhs)
     std::vector<BInst> h;
-    std::vector<int64_t> pre4, pre16, pre16p, pre256, predot, prewide;
-    DevBuf asm_d, inst_d, pre4_d, pre16_d, pre16p_d, pre256_d, predot_d, prewide_d, pre_asm;
+    std::vector<int64_t> pre64, prex, pre16, pre16p, pre256, predot, prewide;
+    DevBuf asm_d, inst_d, pre64_d, prex_d, pre16_d, pre16p_d, pre256_d, predot_d, prewide_d, pre_asm;
     // Inner products on the complex64 matrices (SB_INNER_FP32) or on complex-half copies built
     // after each assembly (SB_INNER_FP16; independent instances only).
     int inner = SB_INNER_FP32;
@@ -820,7 +838,7 @@ static void batch_workspace(Batch& B, int64_t m) {
         small += round256(sizeof(double2) * (m + 1) * m) + 2 * round256(sizeof(double2) * m) +
                  2 * round256(sizeof(double2) * (m + 1)) + 2 * round256(sizeof(double2) * (m + 2)) +
                  round256(sizeof(double2) * chunks * (m + 2)) +
-                 round256(sizeof(double) * std::max({cdiv64(n, kGemvRows), cdiv64(n, kGemv16PRows), chunks}));
+                 round256(sizeof(double) * std::max({cdiv64(n, kBGemv64Rows), cdiv64(n, kGemvX64Rows), cdiv64(n, kGemv16PRows), chunks}));
     }
     B.pool_f32.alloc(f32);
     B.pool_f64.alloc(f64);
@@ -865,7 +883,8 @@ static void batch_workspace(Batch& B, int64_t m) {
             I.r = B.r_all + b * ld;
         }
     }
-    B.pre4.assign(ni + 1, 0);
+    B.pre64.assign(ni + 1, 0);
+    B.prex.assign(ni + 1, 0);
     B.pre16.assign(ni + 1, 0);
     B.pre16p.assign(ni + 1, 0);
     B.pre256.assign(ni + 1, 0);
@@ -901,14 +920,15 @@ static void batch_workspace(Batch& B, int64_t m) {
         I.red = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 2)));
         I.red2 = reinterpret_cast<double2*>(take(ps, sizeof(double2) * (m + 2)));
         I.part = reinterpret_cast<double2*>(take(ps, sizeof(double2) * chunks * (m + 2)));
-        I.pnorm = reinterpret_cast<double*>(take(ps, sizeof(double) * std::max({cdiv64(n, kGemvRows), cdiv64(n, kGemv16PRows), chunks})));
+        I.pnorm = reinterpret_cast<double*>(take(ps, sizeof(double) * std::max({cdiv64(n, kBGemv64Rows), cdiv64(n, kGemvX64Rows), cdiv64(n, kGemv16PRows), chunks})));
         I.st = dv.st + b;
         I.nrm = dv.nrm + 3 * b;
         I.scal = dv.scal + kScal * b;
         I.outer = dv.outer + b;
         I.live = dv.live + b;
         I.brk = dv.brk + b;
-        B.pre4[b + 1] = B.pre4[b] + cdiv64(n, kGemvRows);
+        B.pre64[b + 1] = B.pre64[b] + cdiv64(n, kBGemv64Rows);
+        B.prex[b + 1] = B.prex[b] + cdiv64(n, kGemvX64Rows);
         B.pre16[b + 1] = B.pre16[b] + cdiv64(n, kGemv16Rows);
         B.pre16p[b + 1] = B.pre16p[b] + cdiv64(n, kGemv16PRows);
         B.pre256[b + 1] = B.pre256[b] + chunks;
@@ -916,7 +936,8 @@ static void batch_workspace(Batch& B, int64_t m) {
         B.prewide[b + 1] = B.prewide[b] + cdiv64(n, (int64_t)kWide);
     }
     B.inst_d.alloc(sizeof(BInst) * ni);
-    B.pre4_d.alloc(sizeof(int64_t) * (ni + 1));
+    B.pre64_d.alloc(sizeof(int64_t) * (ni + 1));
+    B.prex_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre16_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre16p_d.alloc(sizeof(int64_t) * (ni + 1));
     B.pre256_d.alloc(sizeof(int64_t) * (ni + 1));
@@ -925,7 +946,8 @@ static void batch_workspace(Batch& B, int64_t m) {
     B.prewide_d.alloc(sizeof(int64_t) * (ni + 1));
     h2d_sync(B.prewide_d.p, B.prewide.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.inst_d.p, B.h.data(), sizeof(BInst) * ni);
-    h2d_sync(B.pre4_d.p, B.pre4.data(), sizeof(int64_t) * (ni + 1));
+    h2d_sync(B.pre64_d.p, B.pre64.data(), sizeof(int64_t) * (ni + 1));
+    h2d_sync(B.prex_d.p, B.prex.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.pre16_d.p, B.pre16.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.pre16p_d.p, B.pre16p.data(), sizeof(int64_t) * (ni + 1));
     h2d_sync(B.pre256_d.p, B.pre256.data(), sizeof(int64_t) * (ni + 1));
@@ -936,8 +958,8 @@ static void batch_workspace(Batch& B, int64_t m) {
 static void batch_step(Batch& B, int j) {
     const BInst* I = B.inst_d.as<BInst>();
     const int ni = B.ninst;
-    const unsigned g4 = static_cast<unsigned>(B.pre4.back()), g256 = static_cast<unsigned>(B.pre256.back());
-    const int64_t* p4 = B.pre4_d.as<int64_t>();
+    const unsigned g64 = static_cast<unsigned>(B.pre64.back()), g256 = static_cast<unsigned>(B.pre256.back());
+    const int64_t* p64 = B.pre64_d.as<int64_t>();
     const int64_t* p256 = B.pre256_d.as<int64_t>();
     const int k = j + 1;
     const cudaStream_t s = B.stream;
@@ -962,7 +984,7 @@ static void batch_step(Batch& B, int j) {
                                                                                       mode, j, G_ACTIVE);
         } else {
             ProfScope prof(SB_PROF_GEMV32, s);
-            k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, mode, j, G_ACTIVE);
+            k_bgemv32<<<g64, kGemvThreads, 0, s>>>(I, p64, ni, mode, j, G_ACTIVE);
         }
         count_launch();
     }
@@ -975,16 +997,16 @@ static void batch_step(Batch& B, int j) {
     const unsigned gw = static_cast<unsigned>(B.prewide.back());
     const int64_t* pw = B.prewide_d.as<int64_t>();
     k_bproject<<<gw, kChunk, 0, s>>>(I, pw, ni, k, 0, G_ACTIVE);
-    k_bsum_partials<<<ni, 32, 0, s>>>(I, pw, 0, G_ACTIVE);
+    k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, pw, 0, G_ACTIVE);
     k_bafter_first<<<gi, 64, 0, s>>>(I, ni, j);
     k_bdots<<<gd, kChunk, 0, s>>>(I, pdot, ni, k, G_REORTH);
     k_breduce<<<gr, 32, 0, s>>>(I, pdot, k, 1, G_REORTH);
     k_bproject<<<gw, kChunk, 0, s>>>(I, pw, ni, k, 1, G_REORTH);
-    k_bsum_partials<<<ni, 32, 0, s>>>(I, pw, 1, G_REORTH);
+    k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, pw, 1, G_REORTH);
     k_bgivens<<<gi, 64, 0, s>>>(I, ni, j);
     k_bnext<<<gw, kChunk, 0, s>>>(I, pw, ni, j);
     for (int t = 0; t < 11; ++t) count_launch();
-    (void)g4;
+    (void)g64;
     SB_CUDA(cudaGetLastError());
 }
 
@@ -1064,9 +1086,9 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
     batch_workspace(B, cfg.inner_restart);
     const int ni = B.ninst;
     const BInst* I = B.inst_d.as<BInst>();
-    const unsigned g4 = static_cast<unsigned>(B.pre4.back()), g256 = static_cast<unsigned>(B.pre256.back());
+    const unsigned g64 = static_cast<unsigned>(B.pre64.back()), g256 = static_cast<unsigned>(B.pre256.back());
     const unsigned gi = static_cast<unsigned>(cdiv64(ni, 64));
-    const int64_t* p4 = B.pre4_d.as<int64_t>();
+    const int64_t* p64 = B.pre64_d.as<int64_t>();
     const int64_t* p256 = B.pre256_d.as<int64_t>();
     const cudaStream_t s = B.stream;
     const StateView hv = state_view(B.pin.p, ni);
@@ -1099,7 +1121,7 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
     // x = 0, r = b and ||b|| (with a zero initial guess the first residual needs no product).
     k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_B_TO_R, G_NONE);
     k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 1, G_NONE);
-    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_NONE);
+    k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, p256, 2, G_NONE);
     launched(3);
     d2h(hv.nrm, dv.nrm, sizeof(double) * 3 * ni);
     SB_CUDA(cudaStreamSynchronize(s));
@@ -1116,14 +1138,15 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
             if (B.shared) {
                 shared_residual64(B);
                 k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 3, G_OUTER);
-                k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_OUTER);
+                k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, p256, 2, G_OUTER);
                 launched(2);
             } else {
                 {
                     ProfScope prof(SB_PROF_GEMV32, s);
-                    k_bres64<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, G_OUTER);
+                    k_bres64<<<static_cast<unsigned>(B.prex.back()), kGemvThreads, 0, s>>>(I, B.prex_d.as<int64_t>(),
+                                                                                         ni, G_OUTER);
                 }
-                k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_OUTER);
+                k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, B.prex_d.as<int64_t>(), 2, G_OUTER);
                 launched(2);
             }
             d2h(hv.nrm, dv.nrm, sizeof(double) * 3 * ni);
@@ -1163,7 +1186,7 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
         // Inner FP32 solves of A d = r / ||r||, in lockstep.
         k_bvec<<<g256, kChunk, 0, s>>>(I, p256, ni, OP_R_TO_RB, G_OUTER);
         k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 0, G_OUTER);
-        k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_OUTER);
+        k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, p256, 2, G_OUTER);
         k_bcontrol<<<gi, 64, 0, s>>>(I, ni, 0, 0);
         launched(4);
         for (int b = 0; b < ni; ++b) was_live[b] = outer[b];
@@ -1181,7 +1204,7 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
                 if (B.shared) {
                     tensor_block_product(*B.shared, B.d_all, B.ld_all, ni, B.w_all, B.ld_all, s);
                     k_bresid_w<<<g256, kChunk, 0, s>>>(I, p256, ni, G_RESTART);
-                    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 2, G_RESTART);
+                    k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, p256, 2, G_RESTART);
                     launched(2);
                 } else {
                     // rq = rb - A d, or rb - A (M^-1 d) under the block-Jacobi preconditioner
@@ -1194,13 +1217,13 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
                             k_bgemv16<<<static_cast<unsigned>(B.pre16p.back()), kGemvThreads, 0, s>>>(
                                 I, B.pre16p_d.as<int64_t>(), ni, mode, 0, G_RESTART);
                         }
-                        k_bsum_partials<<<ni, 32, 0, s>>>(I, B.pre16p_d.as<int64_t>(), 2, G_RESTART);
+                        k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, B.pre16p_d.as<int64_t>(), 2, G_RESTART);
                     } else {
                         {
                             ProfScope prof(SB_PROF_GEMV32, s);
-                            k_bgemv32<<<g4, kGemvThreads, 0, s>>>(I, p4, ni, mode, 0, G_RESTART);
+                            k_bgemv32<<<g64, kGemvThreads, 0, s>>>(I, p64, ni, mode, 0, G_RESTART);
                         }
-                        k_bsum_partials<<<ni, 32, 0, s>>>(I, p4, 2, G_RESTART);
+                        k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, p64, 2, G_RESTART);
                     }
                     launched(2);
                 }
@@ -1248,7 +1271,7 @@ static void batch_solve(Batch& B, const sb_ir_config& cfg, sb_gmres_stats* stats
     // Every instance stopped right after its residual was formed, so r = b - A x is current:
     // ||A x|| = ||b - r|| gives the backward error without another product.
     k_bvnorm<<<g256, kChunk, 0, s>>>(I, p256, ni, 2, G_NONE);
-    k_bsum_partials<<<ni, 32, 0, s>>>(I, p256, 0, G_NONE);
+    k_bsum_partials<<<ni, kSumThreads, 0, s>>>(I, p256, 0, G_NONE);
     launched(2);
     d2h(hv.nrm, dv.nrm, sizeof(double) * 3 * ni);
     SB_CUDA(cudaEventRecord(e1, s));

@@ -363,15 +363,9 @@ __global__ void k_jacobi(const double2* __restrict__ d, const T* __restrict__ x,
 // Host launchers
 // ---------------------------------------------------------------------------------------------
 
-// Launch shapes of the single-operator products (rows per CTA, 16-byte loads in flight per row
-// and thread; 256 threads). Measured at N = 20480 on B200 against 4 rows x 2 loads: the complex128
-// product 1 x 4 (0.93-0.99 ms, 4 x 2 0.98-1.02 ms); the complex64 product with FP32 vectors
-// 1 x 4 (0.49 ms, 4 x 2 0.51-0.52 ms) and with FP64 vectors 2 x 4 (0.49-0.53 ms, 4 x 2
-// 0.55-0.60 ms: its x is twice the row's bytes, so two rows share each x load). Few rows and many
-// CTAs keep more loads in flight per SM than wide row blocks with their register cost.
+// Launch shape of the complex128 product (rows per CTA, 16-byte loads in flight per row and
+// thread): 1 x 4, measured at N = 20480 on B200 0.93-0.99 ms against 0.98-1.02 ms for 4 x 2.
 constexpr int kGemv128Rows = 1, kGemv128Unroll = 4;
-constexpr int kGemv64Rows = 1, kGemv64Unroll = 4;
-constexpr int kGemvX64Rows = 2, kGemvX64Unroll = 4;
 
 // gemv_partials counts the partial norms of both the complex128 and the FP32-vector complex64
 // residuals, and callers size partial-norm buffers by it for every residual product.

@@ -17,11 +17,15 @@
 
 namespace sb {
 
-// Launch shape of the batched solver's complex64 products (rows per CTA, threads per CTA, loads
-// in flight); the single-operator products set their own row and load counts on these threads.
-constexpr int kGemvRows = 4;
+// Threads of every matrix-vector product CTA.
 constexpr int kGemvThreads = 256;
-constexpr int kGemvUnroll = 2;
+// Rows per CTA and 16-byte loads in flight per row and thread of the complex64 products, single
+// operator and batched (measured at N = 20480 against 4 rows x 2 loads: FP32 vectors 1 x 4, 0.49
+// ms against 0.51-0.52 ms; FP64 vectors 2 x 4, 0.49-0.53 ms against 0.55-0.60 ms: their x is
+// twice a row's bytes, so two rows share each x load). Few rows and many CTAs keep more loads in
+// flight per SM than wide row blocks with their register cost.
+constexpr int kGemv64Rows = 1, kGemv64Unroll = 4;
+constexpr int kGemvX64Rows = 2, kGemvX64Unroll = 4;
 
 __device__ __forceinline__ double2 ld_stream(const double2* p) { return __ldcs(p); }
 __device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
