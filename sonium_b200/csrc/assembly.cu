@@ -3016,6 +3016,28 @@ void assemble_quad(Operator& op, const sb_physics& ph, double beta_re, double be
 
 void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const uint8_t* has_adm,
                  const sb_complex* adm) {
+    if (!kind && !value && !has_adm && !adm) {
+        // The default (rigid: velocity 0, no admittance everywhere): every field is zero.
+        static_assert(SB_BC_VELOCITY == 0, "the rigid default is the zero kind");
+        SB_CUDA(cudaSetDevice(m.device));
+        m.any_bc_value = false;
+        m.any_adm = false;
+        m.h_bc_kind.assign(m.n, SB_BC_VELOCITY);
+        m.h_bc_value.assign(2 * m.n, 0.0);
+        m.h_has_adm.assign(m.n, 0);
+        m.h_adm.assign(2 * m.n, 0.0);
+        if (!m.bc_kind.p) {
+            m.bc_kind.alloc(sizeof(int32_t) * m.n);
+            m.bc_value.alloc(sizeof(double2) * m.n);
+            m.has_adm.alloc(m.n);
+            m.adm.alloc(sizeof(double2) * m.n);
+        }
+        SB_CUDA(cudaMemset(m.bc_kind.p, 0, sizeof(int32_t) * m.n));
+        SB_CUDA(cudaMemset(m.bc_value.p, 0, sizeof(double2) * m.n));
+        SB_CUDA(cudaMemset(m.has_adm.p, 0, m.n));
+        memset_sync(m.adm.p, 0, sizeof(double2) * m.n);
+        return;
+    }
     for (int64_t e = 0; e < m.n; ++e) {
         const int k = kind ? kind[e] : SB_BC_VELOCITY;
         SB_REQUIRE(k == SB_BC_VELOCITY || k == SB_BC_PRESSURE, SB_ERR_INVALID_ARGUMENT,

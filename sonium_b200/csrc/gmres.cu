@@ -18,6 +18,7 @@
 #include <mutex>
 
 #include "sb_blas.cuh"
+#include "sb_device.cuh"
 #include "sb_internal.cuh"
 #include "sb_krylov.cuh"
 #include "sb_profile.cuh"
@@ -49,6 +50,49 @@ __global__ void k_givens(KState* __restrict__ st, const double2* __restrict__ re
 __global__ void k_upper_solve(const KState* __restrict__ st, const double2* __restrict__ H,
                               const double2* __restrict__ g, double2* __restrict__ y) {
     upper_solve_dev(st, H, g, y);
+}
+
+// Final statistics of a solve: per-CTA sums of |b - A x|^2, |A x|^2, |b|^2 and the count of
+// non-finite x or A x entries (from A x itself, or from a residual r as A x = b - r), then one warp
+// adds the CTAs' sums in CTA order.
+constexpr int kFinThreads = 256, kFinBlocks = 296;
+__global__ void __launch_bounds__(kFinThreads) k_final_sums(const double2* __restrict__ b,
+                                                            const double2* __restrict__ axr, bool is_r,
+                                                            const double2* __restrict__ x, int64_t n,
+                                                            double* __restrict__ part) {
+    __shared__ double red[kFinThreads / 32][4];
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t i = blockIdx.x * (int64_t)kFinThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kFinThreads) {
+        const double2 bb = b[i];
+        double2 ax = axr[i];
+        if (is_r) ax = make_double2(bb.x - ax.x, bb.y - ax.y);
+        const double dr = bb.x - ax.x, di = bb.y - ax.y;
+        v[0] += dr * dr + di * di;
+        v[1] += ax.x * ax.x + ax.y * ax.y;
+        v[2] += bb.x * bb.x + bb.y * bb.y;
+        const double2 xx = x[i];
+        if (!isfinite(xx.x) || !isfinite(xx.y) || !isfinite(ax.x) || !isfinite(ax.y)) v[3] += 1.0;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) v[c] = warp_sum(v[c]);
+    if (lane == 0)
+        for (int c = 0; c < 4; ++c) red[warp][c] = v[c];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0.0;
+        for (int w = 0; w < kFinThreads / 32; ++w) t += red[w][threadIdx.x];
+        part[4 * blockIdx.x + threadIdx.x] = t;
+    }
+}
+
+__global__ void k_final_reduce(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c = threadIdx.x; c < nb; c += 32)
+        for (int t = 0; t < 4; ++t) v[t] += part[4 * c + t];
+    for (int t = 0; t < 4; ++t) v[t] = warp_sum(v[t]);
+    if (threadIdx.x == 0)
+        for (int t = 0; t < 4; ++t) out[t] = v[t];
 }
 
 struct PinnedBuf {
@@ -144,6 +188,7 @@ struct SolveWork {
     DevBuf t64, z64;  // the FP64 solver's block-Jacobi vectors (allocated on first use)
     PinnedBuf pin;
     DevBuf npart, nred;  // scratch of the ||b|| reduction
+    DevBuf fin;          // partial sums of the final statistics (k_final_sums) and their totals
     int64_t n = 0;
     double2* k64_part(int64_t) { return npart.as<double2>(); }
     double2* k64_red() { return nred.as<double2>(); }
@@ -153,6 +198,7 @@ struct SolveWork {
         pin.alloc(64);
         npart.alloc(sizeof(double2) * arnoldi_dot_chunks(n));
         nred.alloc(sizeof(double2) * 2);
+        fin.alloc(sizeof(double) * 4 * (kFinBlocks + 1));
         r64.alloc(sizeof(double2) * n);
         r32.alloc(sizeof(float2) * n);
         d32.alloc(sizeof(float2) * n);
@@ -523,30 +569,23 @@ CoreResult gmres_core(KrylovWork<T>& W, const Problem<T>& P, const T* b, T* x, i
 void finalize(const Operator& op, SolveWork& sw, const double2* b, const double2* x, sb_gmres_stats& st,
               const double2* r = nullptr) {
     const int64_t n = op.n;
-    std::vector<double2> hb(n), hax(n), hx(n);
-    if (r) {
-        SB_CUDA(cudaMemcpyAsync(hax.data(), r, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
-    } else {
+    const double2* axr = r;
+    if (!r) {
         op_gemv64(op, x, sw.ax.as<double2>(), Gate{});
         ++st.matvecs;
-        SB_CUDA(cudaMemcpyAsync(hax.data(), sw.ax.p, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
+        axr = sw.ax.as<double2>();
     }
-    SB_CUDA(cudaMemcpyAsync(hb.data(), b, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
-    SB_CUDA(cudaMemcpyAsync(hx.data(), x, sizeof(double2) * n, cudaMemcpyDeviceToHost, op.stream));
+    k_final_sums<<<kFinBlocks, kFinThreads, 0, op.stream>>>(b, axr, r != nullptr, x, n, sw.fin.as<double>());
+    count_launch();
+    k_final_reduce<<<1, 32, 0, op.stream>>>(sw.fin.as<double>(), kFinBlocks, sw.fin.as<double>() + 4 * kFinBlocks);
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    double* h = static_cast<double*>(sw.pin.p) + 2;
+    SB_CUDA(cudaMemcpyAsync(h, sw.fin.as<double>() + 4 * kFinBlocks, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                            op.stream));
     SB_CUDA(cudaStreamSynchronize(op.stream));
-    if (r)
-        for (int64_t i = 0; i < n; ++i) hax[i] = make_double2(hb[i].x - hax[i].x, hb[i].y - hax[i].y);
-    double rs = 0, as = 0, bs = 0;
-    bool finite = true;
-    for (int64_t i = 0; i < n; ++i) {
-        const double dr = hb[i].x - hax[i].x, di = hb[i].y - hax[i].y;
-        rs += dr * dr + di * di;
-        as += hax[i].x * hax[i].x + hax[i].y * hax[i].y;
-        bs += hb[i].x * hb[i].x + hb[i].y * hb[i].y;
-        if (!std::isfinite(hx[i].x) || !std::isfinite(hx[i].y) || !std::isfinite(hax[i].x) ||
-            !std::isfinite(hax[i].y))
-            finite = false;
-    }
+    const double rs = h[0], as = h[1], bs = h[2];
+    const bool finite = h[3] == 0.0;
     if (!finite || !std::isfinite(rs)) {
         st.status = SB_SOLVER_NUMERICAL_ERROR;
         st.converged = 0;
