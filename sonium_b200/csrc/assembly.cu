@@ -1311,13 +1311,85 @@ __device__ __forceinline__ void panel_basis_deriv(double s, double t, double (*d
     }
 }
 
+// One kept leaf of a near pair's subdivision: its vertices in the field element's reference
+// coordinates (s, t of each of the three), its Gauss order, and the leaves its subdivision level
+// kept (low 16 bits; bit 16 set at level 0, the element itself), the same in every leaf of a level.
+struct NearLeaf {
+    double lv[6];
+    int order, group;
+};
+
+// The points of the kept leaves of one subdivision level (S.lv / S.lorder, keep of them) into the
+// lane-partial sums: lane 0 lays out the leaves' point offsets, the lanes stride over the points.
+// iforie: the level-0 leaf, the element itself (its reference coordinates are the points').
+template <int NB>
+__device__ __forceinline__ void near_eval_kept(Acc* a, NearWarpSmem& S, int keep, bool iforie,
+                                               const double (&V)[3][3], double x0, double x1, double x2,
+                                               double nxx, double nxy, double nxz, double nyx, double nyy,
+                                               double nyz, double jac, double k, double k2, int lane) {
+    // Point offsets of the kept leaves (serial scan by lane 0: at most 60 leaves).
+    if (lane == 0) {
+        int o = 0;
+        for (int l = 0; l < keep; ++l) {
+            S.loff[l] = o;
+            o += c_tri_cnt[S.lorder[l] - 4];
+        }
+        S.loff[keep] = o;
+    }
+    __syncwarp();
+    const int npts = S.loff[keep];
+    for (int f = lane; f < npts; f += 32) {
+        int lo = 0, hi = keep - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (S.loff[mid] <= f) lo = mid; else hi = mid - 1;
+        }
+        const int l = lo;
+        const int q = f - S.loff[l];
+        const int ti = c_tri_off[S.lorder[l] - 4] + q;
+        const double xi = c_tri_xi[ti], et = c_tri_eta[ti], wq = c_tri_w[ti];
+        double xio, eto, weih2;
+        if (iforie) {
+            xio = xi;
+            eto = et;
+            weih2 = wq;
+        } else {
+            const double* lv = S.lv[l];
+            const double lam = 1.0 - xi - et;
+            xio = lv[0] * lam + lv[2] * xi + lv[4] * et;
+            eto = lv[1] * lam + lv[3] * xi + lv[5] * et;
+            const double det = fabs((lv[2] - lv[0]) * (lv[5] - lv[1]) - (lv[4] - lv[0]) * (lv[3] - lv[1]));
+            weih2 = wq * det;
+        }
+        const double sf0 = 1.0 - xio - eto;
+        const double px = sf0 * V[0][0] + xio * V[1][0] + eto * V[2][0];
+        const double py = sf0 * V[0][1] + xio * V[1][1] + eto * V[2][1];
+        const double pz = sf0 * V[0][2] + xio * V[1][2] + eto * V[2][2];
+        const double dx = px - x0, dy = py - x1, dz = pz - x2;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 >= 1e-30)) continue;  // dis < 1e-15 (normalize, element.rs:304-311)
+        const double rinv = sb_rsqrt2(d2);
+        const double dis = d2 * rinv;
+        if constexpr (NB == 1) {
+            point_channels(a[0], dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
+        } else {
+            double nb[NB];
+            panel_basis<NB>(xio, eto, nb);
+            point_channels_w<NB>(a, nb, dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k,
+                                 k2);
+        }
+    }
+}
+
 // Evaluates the regular-integration channels of field element j seen from the point x with
 // normal nx into lane-partial sums: NB = 1 the constant basis, NB = 3 / 6 the discontinuous
 // linear / quadratic basis weights.
-template <int NB>
-__device__ void near_channels_at(Acc* a, NearWarpSmem& S, const double* __restrict__ elem, int64_t ld,
-                                 double x0, double x1, double x2, double nxx, double nxy, double nxz,
-                                 int64_t j, double k, double k2, int lane) {
+// kMode 0 evaluates as it subdivides; kMode 1 only counts the kept leaves (returned by lane 0's
+// call, the others return the same); kMode 2 writes them, level by level, to plan[0 .. count).
+template <int NB, int kMode = 0>
+__device__ int near_channels_at(Acc* a, NearWarpSmem& S, const double* __restrict__ elem, int64_t ld,
+                                double x0, double x1, double x2, double nxx, double nxy, double nxz,
+                                int64_t j, double k, double k2, int lane, NearLeaf* __restrict__ plan = nullptr) {
     double V[3][3];
     for (int t = 0; t < 3; ++t)
         for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, j);
@@ -1433,57 +1505,15 @@ __device__ void near_channels_at(Acc* a, NearWarpSmem& S, const double* __restri
             }
         }
         __syncwarp();
-        // Point offsets of the kept leaves (serial scan by lane 0: at most 60 leaves).
-        if (lane == 0) {
-            int o = 0;
-            for (int l = 0; l < keep; ++l) {
-                S.loff[l] = o;
-                o += c_tri_cnt[S.lorder[l] - 4];
-            }
-            S.loff[keep] = o;
-        }
-        __syncwarp();
-        const int npts = S.loff[keep];
-        const bool iforie = fabs(fabs(faclin) - 1.0) < 1e-10;
-        for (int f = lane; f < npts; f += 32) {
-            int lo = 0, hi = keep - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (S.loff[mid] <= f) lo = mid; else hi = mid - 1;
-            }
-            const int l = lo;
-            const int q = f - S.loff[l];
-            const int ti = c_tri_off[S.lorder[l] - 4] + q;
-            const double xi = c_tri_xi[ti], et = c_tri_eta[ti], wq = c_tri_w[ti];
-            double xio, eto, weih2;
-            if (iforie) {
-                xio = xi;
-                eto = et;
-                weih2 = wq;
-            } else {
-                const double* lv = S.lv[l];
-                const double lam = 1.0 - xi - et;
-                xio = lv[0] * lam + lv[2] * xi + lv[4] * et;
-                eto = lv[1] * lam + lv[3] * xi + lv[5] * et;
-                const double det = fabs((lv[2] - lv[0]) * (lv[5] - lv[1]) - (lv[4] - lv[0]) * (lv[3] - lv[1]));
-                weih2 = wq * det;
-            }
-            const double sf0 = 1.0 - xio - eto;
-            const double px = sf0 * V[0][0] + xio * V[1][0] + eto * V[2][0];
-            const double py = sf0 * V[0][1] + xio * V[1][1] + eto * V[2][1];
-            const double pz = sf0 * V[0][2] + xio * V[1][2] + eto * V[2][2];
-            const double dx = px - x0, dy = py - x1, dz = pz - x2;
-            const double d2 = dx * dx + dy * dy + dz * dz;
-            if (!(d2 >= 1e-30)) continue;  // dis < 1e-15 (normalize, element.rs:304-311)
-            const double rinv = sb_rsqrt2(d2);
-            const double dis = d2 * rinv;
-            if constexpr (NB == 1) {
-                point_channels(a[0], dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k, k2);
-            } else {
-                double nb[NB];
-                panel_basis<NB>(xio, eto, nb);
-                point_channels_w<NB>(a, nb, dx, dy, dz, dis, rinv, weih2 * jac, nyx, nyy, nyz, nxx, nxy, nxz, k,
-                                     k2);
+        if constexpr (kMode == 0) {
+            near_eval_kept<NB>(a, S, keep, fabs(fabs(faclin) - 1.0) < 1e-10, V, x0, x1, x2, nxx, nxy, nxz, nyx,
+                               nyy, nyz, jac, k, k2, lane);
+        } else if constexpr (kMode == 2) {
+            for (int l = lane; l < keep; l += 32) {
+                NearLeaf& o = plan[total + l];
+                for (int t = 0; t < 6; ++t) o.lv[t] = S.lv[l][t];
+                o.order = S.lorder[l];
+                o.group = keep | (level == 0 ? 1 << 16 : 0);
             }
         }
         total += keep;
@@ -1492,6 +1522,7 @@ __device__ void near_channels_at(Acc* a, NearWarpSmem& S, const double* __restri
         nsel = min(nsub, 15) * 4;
         cur = nxt;
     }
+    return total;
 }
 
 // The constant basis: pair (i, j) seen from the centroid of element i.
@@ -1540,6 +1571,82 @@ __global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near(const 
             if (near_rhs) near_rhs[p] = combine(t, coef, ld, j, CF_DG);
         }
         __syncwarp();  // the warp's shared replay state is reused by its next pair
+    }
+}
+
+// The near pairs' subdivision plan of a mesh. Which leaves a pair keeps depends on the geometry
+// alone (the collocation point, the field element), not on the wave number, so a mesh records them
+// once and later assemblies evaluate the recorded leaves (k_near_cached) instead of repeating the
+// subdivision tests. kPass 0 counts each pair's kept leaves into counts[p]; kPass 1 writes them,
+// level by level in the order k_near keeps them, to plan[off[p] .. off[p + 1]).
+template <int kPass>
+__global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near_plan(
+    const double* __restrict__ elem, int64_t n, int64_t ld, const int32_t* __restrict__ rows,
+    const int32_t* __restrict__ cols, int64_t nnz, int64_t* __restrict__ counts, const int64_t* __restrict__ off,
+    NearLeaf* __restrict__ plan) {
+    __shared__ NearWarpSmem smem[kNearWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kNearWarps;
+    for (int64_t p = blockIdx.x * (int64_t)kNearWarps + warp; p < nnz; p += stride) {
+        const int64_t i = rows[p], j = cols[p];
+        if constexpr (kPass == 0) {
+            const int t = near_channels_at<1, 1>(nullptr, smem[warp], elem, ld, E(ECX, i), E(ECY, i), E(ECZ, i),
+                                                 E(ENX, i), E(ENY, i), E(ENZ, i), j, 0.0, 0.0, lane);
+            if (lane == 0) counts[p] = t;
+        } else {
+            near_channels_at<1, 2>(nullptr, smem[warp], elem, ld, E(ECX, i), E(ECY, i), E(ECZ, i), E(ENX, i),
+                                   E(ENY, i), E(ENZ, i), j, 0.0, 0.0, lane, plan + off[p]);
+        }
+        __syncwarp();
+    }
+}
+
+// k_near from a recorded plan: the same leaves, levels and per-lane point order as the
+// subdividing kernel, so the same sums bit for bit.
+__global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near_cached(
+    const double* __restrict__ elem, int64_t n, int64_t ld, const int32_t* __restrict__ rows,
+    const int32_t* __restrict__ cols, int64_t nnz, const int64_t* __restrict__ off,
+    const NearLeaf* __restrict__ plan, const double* __restrict__ coef, double k, double2* __restrict__ A64,
+    float2* __restrict__ A32, int64_t lda32, double2* __restrict__ near_rhs) {
+    __shared__ NearWarpSmem smem[kNearWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    NearWarpSmem& S = smem[warp];
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kNearWarps;
+    const double k2 = k * k;
+    for (int64_t p = blockIdx.x * (int64_t)kNearWarps + warp; p < nnz; p += stride) {
+        const int64_t i = rows[p], j = cols[p];
+        double V[3][3];
+        for (int t = 0; t < 3; ++t)
+            for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, j);
+        const double nyx = E(ENX, j), nyy = E(ENY, j), nyz = E(ENZ, j), jac = E(EJAC, j);
+        const double x0 = E(ECX, i), x1 = E(ECY, i), x2 = E(ECZ, i);
+        const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
+        Acc a;
+        const int64_t end = off[p + 1];
+        for (int64_t g = off[p]; g < end;) {
+            const int grp = plan[g].group;
+            // a level keeps 1 to kMaxNse leaves; the bound only guards the loop against a bad plan
+            const int64_t room = end - g < kMaxNse ? end - g : kMaxNse;
+            const int keep = (grp & 0xffff) < room ? (grp & 0xffff) : static_cast<int>(room);
+            if (keep <= 0) break;
+            for (int l = lane; l < keep; l += 32) {
+                const NearLeaf& f = plan[g + l];
+                for (int t = 0; t < 6; ++t) S.lv[l][t] = f.lv[t];
+                S.lorder[l] = f.order;
+            }
+            __syncwarp();
+            near_eval_kept<1>(&a, S, keep, (grp >> 16) != 0, V, x0, x1, x2, nxx, nxy, nxz, nyx, nyy, nyz, jac, k, k2,
+                              lane);
+            __syncwarp();  // the level's leaves and offsets are read before the next level replaces them
+            g += keep;
+        }
+        const Acc t = warp_reduce(a);
+        if (lane == 0) {
+            const double2 v = combine(t, coef, ld, j, CF_CG);
+            if (A64) A64[i * n + j] = v;
+            if (A32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+            if (near_rhs) near_rhs[p] = combine(t, coef, ld, j, CF_DG);
+        }
     }
 }
 
@@ -3073,6 +3180,48 @@ void mesh_set_bc(Mesh& m, const int32_t* kind, const sb_complex* value, const ui
     h2d_sync(m.adm.p, m.h_adm.data(), sizeof(double2) * m.n);
 }
 
+// The near pairs' subdivision plan (k_near_plan): recorded on the second near-pair assembly of a
+// mesh (one assembly of a new mesh keeps the subdividing kernel, which costs less than recording
+// and evaluating), and only while the device keeps 2 GiB free beside it. Runs on `st`, reads the
+// leaf count back once and waits for the plan before marking it ready, so that an assembly of
+// another operator of the same mesh on another stream finds it complete.
+static void near_plan_prepare(Mesh& m, int device, cudaStream_t st) {
+    std::lock_guard<std::mutex> lock(m.near_plan_mu);
+    if (m.near_plan_ready || m.near_plan_declined || m.quad || ++m.near_assemblies < 2) return;
+    const unsigned grid = near_grid(m.nnz, device);
+    DevBuf counts, total;
+    counts.alloc(sizeof(int64_t) * m.nnz);
+    total.alloc(sizeof(long long));
+    m.near_plan_off.alloc(sizeof(int64_t) * (m.nnz + 1));
+    k_near_plan<0><<<grid, 32 * kNearWarps, 0, st>>>(m.elem.as<double>(), m.n, m.ld, m.near_row.as<int32_t>(),
+                                                     m.near_col.as<int32_t>(), m.nnz, counts.as<int64_t>(), nullptr,
+                                                     nullptr);
+    count_launch();
+    k_scan_counts<<<1, kScanThreads, 0, st>>>(counts.as<int64_t>(), m.nnz, m.near_plan_off.as<int64_t>(),
+                                              total.as<long long>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    long long leaves = 0;
+    SB_CUDA(cudaMemcpyAsync(&leaves, total.p, sizeof(leaves), cudaMemcpyDeviceToHost, st));
+    SB_CUDA(cudaStreamSynchronize(st));
+    const size_t bytes = sizeof(NearLeaf) * static_cast<size_t>(std::max<long long>(leaves, 1));
+    size_t free_b = 0, total_b = 0;
+    SB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (free_b < bytes + (size_t(2) << 30)) {
+        m.near_plan_off.release();
+        m.near_plan_declined = true;
+        return;
+    }
+    m.near_plan.alloc(bytes);
+    k_near_plan<1><<<grid, 32 * kNearWarps, 0, st>>>(m.elem.as<double>(), m.n, m.ld, m.near_row.as<int32_t>(),
+                                                     m.near_col.as<int32_t>(), m.nnz, nullptr,
+                                                     m.near_plan_off.as<int64_t>(), m.near_plan.as<NearLeaf>());
+    count_launch();
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaStreamSynchronize(st));
+    m.near_plan_ready = true;
+}
+
 void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im) {
     if (op.mesh->quad) {
         assemble_quad(op, ph, beta_re, beta_im);
@@ -3120,10 +3269,22 @@ void assemble(Operator& op, const sb_physics& ph, double beta_re, double beta_im
     }
     auto near_and_self = [&](cudaStream_t st) {
         if (m.nnz > 0) {
+            near_plan_prepare(m, op.device, st);
             ProfScope prof(SB_PROF_NEAR, st);
-            k_near<<<near_grid(m.nnz, op.device), 32 * kNearWarps, 0, st>>>(
-                m.elem.as<double>(), n, ld, m.near_row.as<int32_t>(), m.near_col.as<int32_t>(), m.nnz,
-                op.coef.as<double>(), k, A64, A32, op.lda32, with_rhs ? op.near_rhs.as<double2>() : nullptr);
+            bool cached;
+            {
+                std::lock_guard<std::mutex> lock(m.near_plan_mu);
+                cached = m.near_plan_ready;
+            }
+            if (cached)
+                k_near_cached<<<near_grid(m.nnz, op.device), 32 * kNearWarps, 0, st>>>(
+                    m.elem.as<double>(), n, ld, m.near_row.as<int32_t>(), m.near_col.as<int32_t>(), m.nnz,
+                    m.near_plan_off.as<int64_t>(), m.near_plan.as<NearLeaf>(), op.coef.as<double>(), k, A64, A32,
+                    op.lda32, with_rhs ? op.near_rhs.as<double2>() : nullptr);
+            else
+                k_near<<<near_grid(m.nnz, op.device), 32 * kNearWarps, 0, st>>>(
+                    m.elem.as<double>(), n, ld, m.near_row.as<int32_t>(), m.near_col.as<int32_t>(), m.nnz,
+                    op.coef.as<double>(), k, A64, A32, op.lda32, with_rhs ? op.near_rhs.as<double2>() : nullptr);
             count_launch();
             SB_CUDA(cudaGetLastError());
         }

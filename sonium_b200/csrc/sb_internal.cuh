@@ -155,6 +155,12 @@ struct Mesh {
     // near-pair CSR (superset of the reference's subdivision criterion; excludes the diagonal)
     int64_t nnz = 0;
     DevBuf near_ptr, near_col, near_row;  // near_row: the row of each near pair
+    // The near pairs' recorded subdivision leaves (geometry only), built on the mesh's second
+    // near-pair assembly when memory allows; near_plan_off has nnz + 1 entries.
+    DevBuf near_plan, near_plan_off;
+    int near_assemblies = 0;
+    bool near_plan_ready = false, near_plan_declined = false;
+    std::mutex near_plan_mu;
     // Quad4 meshes: four vertices per element (EV0..EV3), far points of the 4 x 4 rule with their
     // normals, qq[(q * 7 + f) * ld + e] for f = x, y, z, w J, nx, ny, nz.
     bool quad = false;
