@@ -3595,10 +3595,21 @@ void assemble_batch_streams(const std::vector<BatchAsmInst>& h_inst, cudaStream_
     for (size_t b = 0; b < h_inst.size(); ++b) {
         const BatchAsmInst& I = h_inst[b];
         if (I.nnz > 0) {
+            bool cached = false;
+            if (I.mesh) {
+                near_plan_prepare(*I.mesh, dev, side.s);
+                std::lock_guard<std::mutex> lock(I.mesh->near_plan_mu);
+                cached = I.mesh->near_plan_ready;
+            }
             ProfScope prof(SB_PROF_NEAR, side.s);
-            k_near<<<near_grid(I.nnz, dev), 32 * kNearWarps, 0, side.s>>>(I.elem, I.n, I.ld, I.near_row, I.near_col,
-                                                                        I.nnz, I.coef, I.k, nullptr, I.A32, I.lda32,
-                                                                        nullptr);
+            if (cached)
+                k_near_cached<<<near_grid(I.nnz, dev), 32 * kNearWarps, 0, side.s>>>(
+                    I.elem, I.n, I.ld, I.near_row, I.near_col, I.nnz, I.mesh->near_plan_off.as<int64_t>(),
+                    I.mesh->near_plan.as<NearLeaf>(), I.coef, I.k, nullptr, I.A32, I.lda32, nullptr);
+            else
+                k_near<<<near_grid(I.nnz, dev), 32 * kNearWarps, 0, side.s>>>(I.elem, I.n, I.ld, I.near_row,
+                                                                            I.near_col, I.nnz, I.coef, I.k, nullptr,
+                                                                            I.A32, I.lda32, nullptr);
             count_launch();
         }
         ProfScope prof(SB_PROF_SELF, side.s);

@@ -1446,6 +1446,7 @@ SB_API int sb_batch_create(int64_t count, sb_mesh* const* meshes, const sb_physi
                 A.near_row = m->near_row.as<int32_t>();
                 A.nnz = m->nnz;
                 A.amax = nullptr;
+                A.mesh = m;
                 B->asm_h.push_back(A);
                 B->rhs.push_back(reinterpret_cast<double2*>(pr));
                 pr += round256(sizeof(double2) * ((m->n + 1) / 2 * 2));

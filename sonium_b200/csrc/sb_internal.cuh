@@ -252,6 +252,7 @@ struct BatchAsmInst {
     const int32_t* near_row;
     int64_t nnz;
     unsigned* amax;  // when set: the largest |re|, |im| written (FP32 bits), for the complex-half copy
+    Mesh* mesh;      // host side only: the instance's mesh (its recorded near-pair plan)
 };
 // The persistent form: one launch over every instance's far tiles, near pairs and self elements
 // (far_per_sm = 0), or two persistent launches side by side, the far tiles on far_per_sm CTA slots
