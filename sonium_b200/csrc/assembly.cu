@@ -1319,11 +1319,12 @@ struct NearLeaf {
     int order, group;
 };
 
-// The points of the kept leaves of one subdivision level (S.lv / S.lorder, keep of them) into the
+// The points of the kept leaves of one subdivision level (lvs / lorder, keep of them) into the
 // lane-partial sums: lane 0 lays out the leaves' point offsets, the lanes stride over the points.
 // iforie: the level-0 leaf, the element itself (its reference coordinates are the points').
 template <int NB>
-__device__ __forceinline__ void near_eval_kept(Acc* a, NearWarpSmem& S, int keep, bool iforie,
+__device__ __forceinline__ void near_eval_kept(Acc* a, const double (*lvs)[6], const int* lorder, int* loff,
+                                               int keep, bool iforie,
                                                const double (&V)[3][3], double x0, double x1, double x2,
                                                double nxx, double nxy, double nxz, double nyx, double nyy,
                                                double nyz, double jac, double k, double k2, int lane) {
@@ -1331,22 +1332,22 @@ __device__ __forceinline__ void near_eval_kept(Acc* a, NearWarpSmem& S, int keep
     if (lane == 0) {
         int o = 0;
         for (int l = 0; l < keep; ++l) {
-            S.loff[l] = o;
-            o += c_tri_cnt[S.lorder[l] - 4];
+            loff[l] = o;
+            o += c_tri_cnt[lorder[l] - 4];
         }
-        S.loff[keep] = o;
+        loff[keep] = o;
     }
     __syncwarp();
-    const int npts = S.loff[keep];
+    const int npts = loff[keep];
     for (int f = lane; f < npts; f += 32) {
         int lo = 0, hi = keep - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (S.loff[mid] <= f) lo = mid; else hi = mid - 1;
+            if (loff[mid] <= f) lo = mid; else hi = mid - 1;
         }
         const int l = lo;
-        const int q = f - S.loff[l];
-        const int ti = c_tri_off[S.lorder[l] - 4] + q;
+        const int q = f - loff[l];
+        const int ti = c_tri_off[lorder[l] - 4] + q;
         const double xi = c_tri_xi[ti], et = c_tri_eta[ti], wq = c_tri_w[ti];
         double xio, eto, weih2;
         if (iforie) {
@@ -1354,7 +1355,7 @@ __device__ __forceinline__ void near_eval_kept(Acc* a, NearWarpSmem& S, int keep
             eto = et;
             weih2 = wq;
         } else {
-            const double* lv = S.lv[l];
+            const double* lv = lvs[l];
             const double lam = 1.0 - xi - et;
             xio = lv[0] * lam + lv[2] * xi + lv[4] * et;
             eto = lv[1] * lam + lv[3] * xi + lv[5] * et;
@@ -1506,8 +1507,8 @@ __device__ int near_channels_at(Acc* a, NearWarpSmem& S, const double* __restric
         }
         __syncwarp();
         if constexpr (kMode == 0) {
-            near_eval_kept<NB>(a, S, keep, fabs(fabs(faclin) - 1.0) < 1e-10, V, x0, x1, x2, nxx, nxy, nxz, nyx,
-                               nyy, nyz, jac, k, k2, lane);
+            near_eval_kept<NB>(a, S.lv, S.lorder, S.loff, keep, fabs(fabs(faclin) - 1.0) < 1e-10, V, x0, x1, x2, nxx,
+                               nxy, nxz, nyx, nyy, nyz, jac, k, k2, lane);
         } else if constexpr (kMode == 2) {
             for (int l = lane; l < keep; l += 32) {
                 NearLeaf& o = plan[total + l];
@@ -1601,20 +1602,45 @@ __global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near_plan(
     }
 }
 
+// Shared memory of one warp of k_near_cached: a pair's whole recorded leaf list and the point
+// offsets of the level being evaluated.
+struct NearPlanSmem {
+    double lv[kMaxLeaves][6];
+    int lorder[kMaxLeaves];
+    int group[kMaxLeaves];
+    int loff[kMaxNse + 1];
+};
+static_assert(sizeof(NearLeaf) == 7 * sizeof(double), "a leaf is seven 8-byte words");
+
 // k_near from a recorded plan: the same leaves, levels and per-lane point order as the
-// subdividing kernel, so the same sums bit for bit.
+// subdividing kernel, so the same sums bit for bit. The warp reads the pair's leaves into shared
+// memory in one coalesced pass, then evaluates them level by level.
 __global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near_cached(
     const double* __restrict__ elem, int64_t n, int64_t ld, const int32_t* __restrict__ rows,
     const int32_t* __restrict__ cols, int64_t nnz, const int64_t* __restrict__ off,
     const NearLeaf* __restrict__ plan, const double* __restrict__ coef, double k, double2* __restrict__ A64,
     float2* __restrict__ A32, int64_t lda32, double2* __restrict__ near_rhs) {
-    __shared__ NearWarpSmem smem[kNearWarps];
+    __shared__ NearPlanSmem smem[kNearWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    NearWarpSmem& S = smem[warp];
+    NearPlanSmem& S = smem[warp];
     const int64_t stride = static_cast<int64_t>(gridDim.x) * kNearWarps;
     const double k2 = k * k;
+    const uint64_t* __restrict__ words = reinterpret_cast<const uint64_t*>(plan);
     for (int64_t p = blockIdx.x * (int64_t)kNearWarps + warp; p < nnz; p += stride) {
         const int64_t i = rows[p], j = cols[p];
+        const int64_t o0 = off[p];
+        const int64_t cnt64 = off[p + 1] - o0;
+        const int cnt = static_cast<int>(cnt64 < kMaxLeaves ? cnt64 : kMaxLeaves);
+        for (int w = lane; w < 7 * cnt; w += 32) {
+            const int l = w / 7, c = w - 7 * l;
+            const uint64_t v = __ldg(words + (o0 + l) * 7 + c);
+            if (c < 6) {
+                S.lv[l][c] = __longlong_as_double(static_cast<long long>(v));
+            } else {
+                S.lorder[l] = static_cast<int>(static_cast<uint32_t>(v));
+                S.group[l] = static_cast<int>(static_cast<uint32_t>(v >> 32));
+            }
+        }
         double V[3][3];
         for (int t = 0; t < 3; ++t)
             for (int c = 0; c < 3; ++c) V[t][c] = E(EV0X + 3 * t + c, j);
@@ -1622,22 +1648,16 @@ __global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near_cached
         const double x0 = E(ECX, i), x1 = E(ECY, i), x2 = E(ECZ, i);
         const double nxx = E(ENX, i), nxy = E(ENY, i), nxz = E(ENZ, i);
         Acc a;
-        const int64_t end = off[p + 1];
-        for (int64_t g = off[p]; g < end;) {
-            const int grp = plan[g].group;
-            // a level keeps 1 to kMaxNse leaves; the bound only guards the loop against a bad plan
-            const int64_t room = end - g < kMaxNse ? end - g : kMaxNse;
-            const int keep = (grp & 0xffff) < room ? (grp & 0xffff) : static_cast<int>(room);
+        __syncwarp();
+        for (int g = 0; g < cnt;) {
+            const int grp = S.group[g];
+            // a level keeps 1 to kMaxNse leaves; the bounds only guard the loop against a bad plan
+            const int room = cnt - g < kMaxNse ? cnt - g : kMaxNse;
+            const int keep = (grp & 0xffff) < room ? (grp & 0xffff) : room;
             if (keep <= 0) break;
-            for (int l = lane; l < keep; l += 32) {
-                const NearLeaf& f = plan[g + l];
-                for (int t = 0; t < 6; ++t) S.lv[l][t] = f.lv[t];
-                S.lorder[l] = f.order;
-            }
-            __syncwarp();
-            near_eval_kept<1>(&a, S, keep, (grp >> 16) != 0, V, x0, x1, x2, nxx, nxy, nxz, nyx, nyy, nyz, jac, k, k2,
-                              lane);
-            __syncwarp();  // the level's leaves and offsets are read before the next level replaces them
+            near_eval_kept<1>(&a, S.lv + g, S.lorder + g, S.loff, keep, (grp >> 16) != 0, V, x0, x1, x2, nxx, nxy,
+                              nxz, nyx, nyy, nyz, jac, k, k2, lane);
+            __syncwarp();  // the level's offsets are read before the next level replaces them
             g += keep;
         }
         const Acc t = warp_reduce(a);
@@ -1647,6 +1667,7 @@ __global__ void __launch_bounds__(32 * kNearWarps, kNearMinBlocks) k_near_cached
             if (A32) A32[i * lda32 + j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
             if (near_rhs) near_rhs[p] = combine(t, coef, ld, j, CF_DG);
         }
+        __syncwarp();  // the pair's leaves are read before the next pair's replace them
     }
 }
 
